@@ -1,0 +1,287 @@
+"""Benchmark: D3Q19 lattice updates per second on the sphere tunnel.
+
+Workload (one bench step = one reference sample chunk): 50 fused pull-stream + collide steps of
+a 256 x 128 x 128 D3Q19 tunnel (FP16 shifted population storage, f32 arithmetic, Smagorinsky
+Cs = 0.1, regularized BGK) around a sphere of diameter 24 at (64, 64, 64) with Bouzidi walls,
+inlet u = 0.05, Re = 300 (nu = 0.004), rest initial state with seeded 1e-4 velocity noise; then
+the macro pass (momentum-exchange force, FP64 sums) and the 64-byte statistics readback.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` = lattice updates (all ranks) / device time of the timed steps (CUDA events, max over
+ranks). `e2e` = the same metric through the public API with host buffers: every step uploads the
+body's flags and wall distances from pinned host memory, runs stepAndSample(50) and reads the
+velocity field back. `roofline` = algorithmic bytes of one stream-collide launch
+(19 x (2 + 2) B per cell) over its mean duration, timed with events on the solver's stream.
+Multi-GPU: independent tunnel replicas, one per rank (no data-path collective).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DIMS = (256, 128, 128)
+CHUNK = 50
+U = 0.05
+D = 24
+PARAMS = dict(u=U, nu=U * D / 300, cs=0.1, ground="freeslip", sides="freeslip", spongeNu=0.03, spongeStart=0.85,
+              emaAlpha=0.0, precision="f16", init="rest_noise", initNoise=1e-4, initSeed=1)
+BYTES_PER_UPDATE = 19 * 2 * 2  # D3Q19, FP16: each population read once and written once
+METRIC = "D3Q19 MLUPS"
+WORKLOAD = "D3Q19 sphere tunnel 256x128x128, FP16 shifted storage, Smagorinsky Cs=0.1, Bouzidi, Re=300"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def geometry():
+    from windtunnel_vis_b200.validation import round_flags
+
+    return round_flags(DIMS, (64, 64.37, 64.21), D / 2, False)
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv",
+                                          "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+            self.fh.close()
+
+    def summary(self):
+        if not self.proc:
+            return None
+        rows = [r.split(", ") for r in open(self.path).read().strip().split("\n")[1:] if r.strip()]
+        if not rows:
+            return None
+        sm = [float(r[1].split()[0]) for r in rows]
+        mx = float(rows[0][2].split()[0])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        loaded = [v for v in sm if v > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_port_mlups(seconds=12.0, threads=0, steps_cap=None):
+    """The oracle (CPU restatement of the reference's shader) on the same workload, all host
+    threads, bounded to about `seconds` of work. Returns (MLUPS, threads, steps run)."""
+    from oracle import oracle as O
+
+    th = O.threads(threads)
+    flags, _, sdf = geometry()
+    s = O.OracleSolver(DIMS, PARAMS)
+    s.upload_flags(flags)
+    s.upload_sdf(sdf)
+    s.step(1)  # init + warm-up
+    n = DIMS[0] * DIMS[1] * DIMS[2]
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds and (steps_cap is None or done < steps_cap):
+        s.step(1)
+        done += 1
+    dt = time.perf_counter() - t0
+    return n * done / dt / 1e6, th, done
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference's WGSL path cannot run here (TypeScript + WebGPU; no Node
+    and no graphics stack), so its algorithm runs as the CPU restatement on the host cores."""
+    if rank != 0:
+        return
+    n = DIMS[0] * DIMS[1] * DIMS[2]
+    from oracle import oracle as O
+
+    th = O.threads(0)
+    flags, _, sdf = geometry()
+    s = O.OracleSolver(DIMS, PARAMS)
+    s.upload_flags(flags)
+    s.upload_sdf(sdf)
+    for _ in range(max(args.warmup, 0)):
+        s.step(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.step(1)
+    dt = time.perf_counter() - t0
+    v = n * args.steps / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": list(DIMS), "bench_step": "1 lattice update of the full grid"},
+        "cpu_baseline": {"value": round(v, 3), "unit": "MLUPS", "cores": th, "kind": "port",
+                         "sample": f"{args.steps} full-grid D3Q19 steps (FP16 storage) on {th} threads"},
+        "e2e": {"value": round(v, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank, dist):
+    import torch
+
+    from windtunnel_vis_b200.solver import Solver
+
+    torch.cuda.set_device(local_rank)
+    flags, frontal, sdf = geometry()
+    n = DIMS[0] * DIMS[1] * DIMS[2]
+    s = Solver(DIMS, PARAMS)
+    s.upload_flags(flags)
+    s.upload_sdf(sdf)
+    stream = torch.cuda.ExternalStream(s.stream)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        s.step_and_sample(CHUNK)
+    torch.cuda.synchronize()
+    barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = s.launches
+    with Clocks(local_rank) as clk:
+        torch.cuda.synchronize()
+        barrier()
+        with torch.cuda.stream(stream):
+            t_start.record(stream)
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            s.step(CHUNK)
+            ev[k][1].record(stream)
+            s.sample()
+        t_end.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    launches = s.launches - launches0
+    ms = t_start.elapsed_time(t_end)
+    sc_ms = sum(a.elapsed_time(b) for a, b in ev) / (args.steps * CHUNK)
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * n * CHUNK * args.steps / (ms_max / 1e3) / 1e6
+
+    # end to end through the public API with host buffers
+    fl_h = torch.from_numpy(flags).pin_memory()
+    sd_h = torch.from_numpy(sdf).pin_memory()
+    vel_bytes = n * 16
+    e2e_steps = max(2, min(args.steps, 10))
+    s.step_and_sample(CHUNK)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.upload_flags(fl_h.numpy())
+        s.upload_sdf(sd_h.numpy())
+        st = s.step_and_sample(CHUNK)
+        s.read_velocity()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * n * CHUNK * e2e_steps / e2e_s / 1e6
+
+    if rank != 0:
+        s.destroy()
+        return
+    peak, peak_kind = peaks()
+    achieved = n * BYTES_PER_UPDATE / (sc_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "stream_collide_d3q19_f16_traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get("bytes_per_launch")
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        mlups, th, done = cpu_port_mlups(args.cpu_seconds)
+        cpu = {"value": round(mlups, 3), "unit": "MLUPS", "cores": th, "kind": "port",
+               "sample": f"{done} full-grid D3Q19 steps (FP16 storage) of the same workload, ~{args.cpu_seconds:.0f} s"}
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": list(DIMS), "storage": "f16 shifted (f - w)",
+                   "bench_step": f"{CHUNK} lattice updates + macro/force pass + stats readback",
+                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2: 2 x 159 MB population buffers"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "k_stream_collide<D3Q19,StF16>", "bytes_per_launch_alg": n * BYTES_PER_UPDATE,
+                     "launch_ms": round(sc_ms, 5)},
+        "cpu_baseline": cpu,
+        "e2e": {"value": round(e2e, 1), "unit": "MLUPS", "h2d_bytes_per_step": n * 8,
+                "d2h_bytes_per_step": 64 + vel_bytes},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    s.destroy()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    try:
+        run_ours(args, rank, world, local_rank, dist)
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

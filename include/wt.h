@@ -1,0 +1,232 @@
+/*
+ * wt.h — C ABI of the B200 lattice Boltzmann wind-tunnel compute path.
+ *
+ * This is the drop-in boundary for the reference's compute path. Every entry point replaces one
+ * method of the reference's solver / backend objects (TypeScript over WebGPU); the citation on
+ * each line names the interface it stands in for (paths relative to the reference project).
+ *
+ *   LbmSolver / SolverFactory ............ src/backend/types.ts:7-18
+ *   Backend (fits, voxelize, setParams…) . src/backend/types.ts:24-53
+ *   SolverGPU (the WebGPU solver object) . src/solver/SolverGPU.ts:12-444
+ *   VoxelizerGPU.voxelize ................ src/voxelize/VoxelizerGPU.ts:48-151
+ *   particle tracers ..................... src/render/tracers.ts:3-106, RendererGPU.ts:505-527
+ *
+ * Conventions
+ *   - Cell index everywhere: cell = x + nx * (y + ny * z). D2Q9 when nz == 1, D3Q19 otherwise.
+ *   - Populations are structure-of-arrays: f[i * N + cell]. FP16 storage holds (f_i - w_i) as IEEE
+ *     binary16, which is byte-for-byte the reference's packed pair layout (two cells per u32 word,
+ *     low half = even cell).
+ *   - Host pointers are borrowed for the duration of the call only (copied, never retained).
+ *   - Device memory is owned by the handle and released by wt_destroy.
+ *   - Every function returns WT_OK (0) or a negative WT_E_* code and stores a message retrievable
+ *     with wt_last_error(); nothing aborts or throws across the ABI.
+ *   - Calls on one handle must be serialised by the caller. Each handle owns one CUDA stream on the
+ *     device that was current when it was created, so handles are independent of each other.
+ */
+#ifndef WT_H
+#define WT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WT_ABI_VERSION 1
+
+enum {
+  WT_OK = 0,
+  WT_E_INVALID = -1,     /* bad argument: null pointer, size mismatch, unsupported dims */
+  WT_E_CUDA = -2,        /* CUDA runtime error (message holds cudaGetErrorString) */
+  WT_E_OOM = -3,         /* device allocation failed */
+  WT_E_STATE = -4,       /* call not valid in the handle's current state */
+  WT_E_UNSUPPORTED = -5, /* feature not available for this precision / lattice */
+  WT_E_NO_DEVICE = -6    /* no CUDA device visible */
+};
+
+enum { WT_GROUND_FREESLIP = 0, WT_GROUND_NOSLIP = 1, WT_GROUND_MOVING = 2 };
+enum { WT_SIDES_FREESLIP = 0, WT_SIDES_PERIODIC = 1 };
+enum { WT_PREC_F32 = 0, WT_PREC_F16 = 1, WT_PREC_F64 = 2 };
+enum { WT_COLL_REGULARIZED = 0, WT_COLL_BGK = 1 };
+enum { WT_INIT_FREESTREAM = 0, WT_INIT_REST_NOISE = 1 };
+
+typedef struct wt_dims {
+  int32_t nx, ny, nz;
+} wt_dims;
+
+/* SolverParams (src/solver/types.ts:3-29). Real-valued fields are doubles because the reference
+ * holds them as JS numbers and rounds only the derived values to f32 when it packs the uniform. */
+typedef struct wt_params {
+  double u;            /* lattice inlet velocity (cells / step) */
+  double nu;           /* molecular lattice viscosity */
+  double cs;           /* Smagorinsky constant */
+  double sponge_nu;    /* extra viscosity in the outlet sponge */
+  double sponge_start; /* fraction of nx where the outlet sponge starts */
+  double sponge_in;    /* width (fraction of nx) of the inlet absorbing layer; 0 = off */
+  double tau_wall;     /* minimum relaxation time on floor-wall cells (reference default 0.5) */
+  double ema_alpha;    /* EMA weight of the time averages, applied at each sample */
+  double init_noise;   /* WT_INIT_REST_NOISE: amplitude of the seeded velocity noise */
+  int32_t ground;      /* WT_GROUND_* */
+  int32_t sides;       /* WT_SIDES_* (3-D z boundaries) */
+  int32_t precision;   /* WT_PREC_*; fixed at creation */
+  int32_t interp;      /* 1 = Bouzidi interpolated bounce-back (default), 0 = halfway */
+  int32_t collision;   /* WT_COLL_* */
+  int32_t init_mode;   /* WT_INIT_*: reference free-stream equilibrium, or rest + seeded noise */
+  uint32_t init_seed;  /* WT_INIT_REST_NOISE seed */
+  uint32_t reserved;
+} wt_params;
+
+/* The 96-byte kernel parameter block: Params uniform (src/solver/wgslLbm.ts:6-15) as packed by
+ * SolverGPU.writeParams (src/solver/SolverGPU.ts:160-187). */
+typedef struct wt_kparams {
+  uint32_t nx, ny, nz, n;
+  float tau0, csmag2, uin, rho_in;
+  uint32_t ground, stride_x;
+  float sponge_start, sponge_nu;
+  float u_ground, ema_alpha, u_ref;
+  uint32_t ref_x;
+  uint32_t side_mode, collision;
+  float tau_wall;
+  uint32_t pad2;
+  float sponge_in, contact_h;
+  uint32_t interp, stride_p;
+} wt_kparams;
+
+/* SolverStats (src/solver/types.ts:31-42), decoded as SolverGPU.stepAndSample does
+ * (src/solver/SolverGPU.ts:302-308). raw[] is the 8-slot reduction result:
+ * [ΣFx, ΣFy, ΣFz, max|u|², Σρ on x = refX, n_ref, nan count, solid count]. The force sum is
+ * accumulated in FP64. */
+typedef struct wt_stats {
+  double fx, fy, fz;
+  double max_u;
+  double rho_ref;
+  int64_t step;
+  int32_t unstable;
+  int32_t reserved;
+  double raw[8];
+} wt_stats;
+
+/* WheelDef (src/voxelize/mesh.ts:54-60), grid space. */
+typedef struct wt_wheel {
+  double c[3];
+  double axis[3];
+  double r;
+  double hw;
+} wt_wheel;
+
+/* VoxelInfo (src/voxelize/VoxelizerGPU.ts:6-12). */
+typedef struct wt_voxel_info {
+  int32_t frontal;
+  int32_t solid_cells;
+  int32_t min[3];
+  int32_t max[3];
+} wt_voxel_info;
+
+/* Particle uniform PU (src/render/tracers.ts:5-12) as packed by RendererGPU
+ * (src/render/RendererGPU.ts:511-520). */
+typedef struct wt_tracer_params {
+  uint32_t count, trail, head, emitter; /* emitter: 0 inlet band, 1 rake */
+  float steps;
+  uint32_t seed;
+  float max_age;
+  uint32_t nozzles;
+  float rake_a[4];
+  float rake_b[4];
+  uint32_t advance, fill, lines, pad;
+  float rake_d[4];
+} wt_tracer_params;
+
+typedef struct wt_solver wt_solver;
+
+/* ---- library ---------------------------------------------------------------------------- */
+int wt_version(void);
+const char* wt_error_string(int code);
+/* Backend.fits (src/backend/webgpu.ts:58-61): bytes the handle would allocate for these dims,
+ * and whether they fit in the free memory of the current device (1 yes, 0 no). */
+int wt_fits(const wt_dims* dims, int32_t precision, int64_t* bytes_needed, int32_t* fits);
+/* SolverGPU.writeParams (src/solver/SolverGPU.ts:160-187). Pure host function. */
+int wt_pack_params(const wt_dims* dims, const wt_params* p, wt_kparams* out);
+
+/* ---- solver lifecycle ------------------------------------------------------------------- */
+/* SolverFactory (src/backend/types.ts:18) / new SolverGPU (src/solver/SolverGPU.ts:61-144). */
+int wt_create(const wt_dims* dims, const wt_params* p, wt_solver** out);
+/* LbmSolver.destroy (src/backend/types.ts:15). Accepts NULL. */
+void wt_destroy(wt_solver* s);
+/* Message of the last failing call on this handle (or of the last failing wt_create when s is
+ * NULL). Valid until the next call on the handle. */
+const char* wt_last_error(const wt_solver* s);
+/* Backend.setParams (src/backend/types.ts:30) / SolverGPU.setParams (SolverGPU.ts:155-158).
+ * precision must equal the creation precision. */
+int wt_set_params(wt_solver* s, const wt_params* p);
+int wt_get_params(const wt_solver* s, wt_params* out);
+int wt_get_kparams(const wt_solver* s, wt_kparams* out);
+/* SolverGPU.reset (SolverGPU.ts:190-194): populations re-initialised before the next step. */
+int wt_reset(wt_solver* s);
+/* SolverGPU.clearStats (SolverGPU.ts:196-201). */
+int wt_clear_stats(wt_solver* s);
+int64_t wt_step_count(const wt_solver* s);
+
+/* ---- geometry --------------------------------------------------------------------------- */
+/* LbmSolver.uploadFlags (types.ts:11): bit 0 solid, bits 8..15 wheel tag k+1. */
+int wt_upload_flags(wt_solver* s, const uint32_t* flags, int64_t n);
+/* LbmSolver.uploadSdf (types.ts:13) / SolverGPU.uploadSdf (SolverGPU.ts:312-322): wall
+ * distances in cells; negative or NaN = unknown. */
+int wt_upload_sdf(wt_solver* s, const float* d, int64_t n);
+/* SolverGPU.setWheels (SolverGPU.ts:325-335): at most 16 wheels, extra entries are ignored. */
+int wt_set_wheels(wt_solver* s, const wt_wheel* w, int32_t count);
+/* Backend.voxelize (types.ts:36) / VoxelizerGPU.voxelize (VoxelizerGPU.ts:48-151): voxelizes an
+ * indexed triangle mesh (positions xyz f32, u32 indices) through the column-major 4x4 mesh->grid
+ * matrix into the solver's flags and wall-distance buffers, tags wheel cells, and returns the
+ * frontal projection and bounding box. ntri == 0 clears the geometry. */
+int wt_voxelize(wt_solver* s, const float* pos, int64_t nverts, const uint32_t* idx, int64_t ntri,
+                const float m[16], const wt_wheel* wheels, int32_t nwheels, wt_voxel_info* info);
+
+/* ---- time stepping ---------------------------------------------------------------------- */
+/* SolverGPU.encodeSteps (SolverGPU.ts:204-222): `steps` fused pull-stream + collide steps. */
+int wt_step(wt_solver* s, int32_t steps);
+/* SolverGPU.encodePost(enc, false) + result read (SolverGPU.ts:225-247, 292-309): macroscopic
+ * fields, EMA statistics, momentum-exchange force and reductions of the current populations. */
+int wt_sample(wt_solver* s, wt_stats* out);
+/* LbmSolver.stepAndSample (types.ts:14, SolverGPU.ts:292-309). */
+int wt_step_and_sample(wt_solver* s, int32_t steps, wt_stats* out);
+
+/* ---- readback / checkpoint -------------------------------------------------------------- */
+/* SolverGPU.readFlags (SolverGPU.ts:347-356). */
+int wt_read_flags(wt_solver* s, uint32_t* out, int64_t n);
+/* Encoded wall distances (~bits(d), 0 = unknown) as stored on the device. */
+int wt_read_sdf(wt_solver* s, uint32_t* out, int64_t n);
+/* SolverGPU.readPopulations (SolverGPU.ts:359-369): the raw current buffer (f32: 4 B, f16: 2 B
+ * of f - w, f64: 8 B per population). bytes must equal the buffer size. */
+int64_t wt_population_bytes(const wt_solver* s);
+int wt_read_populations(wt_solver* s, void* out, int64_t bytes);
+/* Checkpoint resume: overwrite the current buffer (same raw layout). Clears any pending reset. */
+int wt_write_populations(wt_solver* s, const void* in, int64_t bytes);
+/* velTex of the last sample (wgslLbm.ts:439-468): (ux, uy, uz, rho) per cell, stored as FP16 like
+ * the reference's rgba16float texture, returned as f32. */
+int wt_read_velocity(wt_solver* s, float* out4, int64_t n);
+/* meanA (ux, uy, uz, rho EMA, 4 f32 per cell) and meanB (<u.u> EMA, 1 f32 per cell). */
+int wt_read_means(wt_solver* s, float* mean4, float* meanb, int64_t n);
+
+/* ---- tracer particles ------------------------------------------------------------------- */
+/* PARTICLES_WGSL (src/render/tracers.ts:3-106): one dispatch of the particle kernel against the
+ * velocity field of the last sample. Tracer state (count vec4) and trail history (count * trail
+ * vec4) live on the device and are (re)allocated when count or trail change (RendererGPU
+ * ensureTracers). */
+int wt_advect_tracers(wt_solver* s, const wt_tracer_params* p);
+int wt_read_tracers(wt_solver* s, float* state4, int64_t count, float* hist4, int64_t hist_len);
+int wt_write_tracers(wt_solver* s, const float* state4, int64_t count, const float* hist4,
+                     int64_t hist_len, uint32_t trail);
+
+/* ---- device plumbing -------------------------------------------------------------------- */
+/* The handle's cudaStream_t (for event timing by the caller) and its device ordinal. */
+void* wt_stream(const wt_solver* s);
+int32_t wt_device(const wt_solver* s);
+/* Number of kernel launches this handle has issued since creation. */
+int64_t wt_launch_count(const wt_solver* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WT_H */

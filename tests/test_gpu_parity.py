@@ -1,0 +1,195 @@
+"""CUDA path (through libwt.so) against the CPU oracle on the same seeded inputs.
+
+Tolerances (the LBM kernels keep FMA contraction; the oracle evaluates the WGSL expression order
+without it, so single-precision results differ by a few ulp per step):
+  f64 populations ............ |Δ| <= 1e-12 after 1 and 30 steps
+  f32 populations ............ |Δ| <= 1e-6 after 1 step, <= 2e-5 after 30 steps
+  f16 (f - w) populations .... |Δ| <= 2e-5 after 1 step (about 2 half ulps), <= 3e-4 after 30
+  force sum / max|u|² ........ relative 1e-4 (f32, f16), 1e-10 (f64); counts exact
+  voxelizer flags, sdf, info . bit-exact (compiled without contraction)
+  tracers .................... bit-exact state and trail
+"""
+import numpy as np
+import pytest
+
+from windtunnel_vis_b200 import abi, mesh as Mh
+from windtunnel_vis_b200.solver import Solver, WtError
+
+from .scenes import PARAM_SETS, scene
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"f64": (1e-12, 1e-12), "f32": (1e-6, 2e-5), "f16": (2e-5, 3e-4)}
+STAT_RTOL = {"f64": 1e-10, "f32": 1e-4, "f16": 1e-4}
+
+
+def _pair(oracle, dims, params):
+    flags, sdf, wheels = scene(dims)
+    g = Solver(dims, params)
+    o = oracle.OracleSolver(dims, params)
+    for s in (g, o):
+        s.upload_flags(flags)
+        s.upload_sdf(sdf)
+        s.set_wheels(wheels)
+    return g, o, flags
+
+
+def _as_float(a):
+    return a.astype(np.float64)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f16", "f64"])
+@pytest.mark.parametrize("pset", list(PARAM_SETS))
+@pytest.mark.parametrize("dims", [(24, 14, 12), (40, 16, 1)])
+def test_stream_collide_matches_oracle(gpu, oracle, dims, pset, prec):
+    params = dict(PARAM_SETS[pset], precision=prec)
+    g, o, flags = _pair(oracle, dims, params)
+    t1, t30 = TOL[prec]
+    g.step(1)
+    o.step(1)
+    d1 = np.abs(_as_float(g.read_populations()) - _as_float(o.current)).max()
+    assert d1 <= t1, f"1 step: max |diff| {d1:.3e}"
+    g.step(29)
+    o.step(29)
+    d30 = np.abs(_as_float(g.read_populations()) - _as_float(o.current)).max()
+    assert d30 <= t30, f"30 steps: max |diff| {d30:.3e}"
+    # macro pass: stats, velocity field, EMA statistics
+    sg, so = g.sample(), o.sample()
+    rt = STAT_RTOL[prec]
+    scale = max(np.abs(so["raw"][:3]).max(), 1e-3)
+    assert np.abs(sg["raw"][:3] - so["raw"][:3]).max() <= rt * scale + 1e-9, (sg["raw"], so["raw"])
+    assert abs(sg["raw"][3] - so["raw"][3]) <= rt * so["raw"][3] + 1e-12
+    assert abs(sg["rhoRef"] - so["rhoRef"]) <= 1e-5
+    assert sg["raw"][5:].tolist() == so["raw"][5:].tolist()
+    assert sg["step"] == so["step"] == 30 and not sg["unstable"]
+    vg = g.read_velocity()
+    vo = o.vel.reshape(-1, 4)
+    np.testing.assert_allclose(vg, vo, rtol=2e-3, atol=2e-6)
+    ma, mb = g.read_means()
+    np.testing.assert_allclose(ma, o.meanA.reshape(-1, 4), rtol=1e-4, atol=1e-7)
+    np.testing.assert_allclose(mb, o.meanB, rtol=1e-3, atol=1e-9)
+    g.destroy()
+
+
+def test_solid_cells_and_init(gpu, oracle):
+    dims = (16, 8, 8)
+    params = dict(PARAM_SETS["freeslip_reg"], precision="f32")
+    g, o, flags = _pair(oracle, dims, params)
+    # before any step the init runs on first access, equal to the oracle's equilibrium
+    o._init()
+    np.testing.assert_allclose(g.read_populations(), o.current, atol=1e-7)
+    g.step(3)
+    f = g.read_populations().reshape(19, -1)
+    solid = flags != 0
+    w = oracle.lattice(3)["w"].astype(np.float32)
+    np.testing.assert_array_equal(f[:, solid], np.repeat(w[:, None], solid.sum(), 1))
+
+
+def test_determinism_and_checkpoint(gpu):
+    dims = (32, 16, 16)
+    flags, sdf, wheels = scene(dims)
+    params = dict(PARAM_SETS["belt_periodic_les"], precision="f16")
+    runs = []
+    for _ in range(2):
+        s = Solver(dims, params)
+        s.upload_flags(flags)
+        s.upload_sdf(sdf)
+        s.set_wheels(wheels)
+        s.step(20)
+        runs.append((s, s.read_populations()))
+    np.testing.assert_array_equal(runs[0][1], runs[1][1])
+    # resume from a checkpoint into a fresh handle: same trajectory
+    a = runs[0][0]
+    b = Solver(dims, params)
+    b.upload_flags(flags)
+    b.upload_sdf(sdf)
+    b.set_wheels(wheels)
+    b.write_populations(runs[0][1])
+    a.step(7)
+    b.step(7)
+    np.testing.assert_array_equal(a.read_populations(), b.read_populations())
+
+
+def test_reset_restarts_from_init(gpu):
+    dims = (24, 12, 1)
+    s = Solver(dims, dict(u=0.05, nu=0.02))
+    s.step(1)
+    first = s.read_populations()
+    s.step(10)
+    s.reset()
+    assert s.step_count == 0
+    s.step(1)
+    np.testing.assert_array_equal(s.read_populations(), first)
+
+
+def test_errors_are_reported(gpu):
+    s = Solver((16, 8, 4), dict(u=0.05, nu=0.02))
+    with pytest.raises(WtError) as e:
+        s.upload_flags(np.zeros(10, np.uint32))
+    assert e.value.code == abi.WT_E_INVALID
+    with pytest.raises(WtError):
+        s.set_params(dict(precision="f16"))
+    with pytest.raises(WtError):
+        Solver((0, 8, 8), dict(u=0.05, nu=0.02))
+
+
+# ---- voxelizer -------------------------------------------------------------------------------
+def _sphere(dims):
+    pos, idx = Mh.uv_sphere()
+    p, lo, hi, _ = Mh.normalize_mesh(pos)
+    M16, _, full = Mh.placement_matrix(p, lo, hi, dims, dict(mode="center", lengthFrac=1 / 3, diamFrac=0.3, xFrac=0.35))
+    return p, idx, M16, []
+
+
+def _vehicle(dims, tris=20000):
+    p, idx, wheels, lo, hi = Mh.vehicle_body(target_tris=tris)
+    M16, _, full = Mh.placement_matrix(p, lo, hi, dims, dict(mode="ground", lengthFrac=1 / 3, diamFrac=0.3,
+                                                             xFrac=0.34, rideCells=0.08 * dims[1]))
+    return p, idx, M16, Mh.grid_wheels(wheels, full)
+
+
+@pytest.mark.parametrize("kind,dims", [("sphere", (128, 64, 64)), ("sphere", (512, 192, 1)), ("vehicle", (96, 48, 48)),
+                                       ("vehicle", (160, 64, 1))])
+def test_voxelizer_bit_exact(gpu, oracle, kind, dims):
+    p, idx, M16, wheels = (_sphere if kind == "sphere" else _vehicle)(dims)
+    s = Solver(dims, dict(u=0.05, nu=0.02))
+    info = s.voxelize(p, idx, M16, wheels)
+    fo, so, io = oracle.voxelize_f32(dims, p, idx, M16, wheels)
+    assert info == io
+    np.testing.assert_array_equal(s.read_flags(), fo)
+    np.testing.assert_array_equal(s.read_sdf_encoded(), so)
+    if wheels and dims[2] > 1:
+        assert ((s.read_flags() >> 8) != 0).sum() > 0
+    # empty mesh clears the geometry
+    info0 = s.voxelize(np.zeros((0, 3), np.float32), np.zeros(0, np.uint32), M16)
+    assert info0["solidCells"] == 0 and s.read_flags().sum() == 0
+
+
+# ---- tracers ---------------------------------------------------------------------------------
+@pytest.mark.parametrize("dims,emitter", [((48, 24, 16), 0), ((48, 24, 16), 1), ((64, 32, 1), 0), ((64, 32, 1), 1)])
+def test_tracers_bit_exact(gpu, oracle, dims, emitter):
+    flags, sdf, wheels = scene(dims)
+    s = Solver(dims, dict(PARAM_SETS["freeslip_reg"], init="rest_noise", initNoise=0.02))
+    s.upload_flags(flags)
+    s.upload_sdf(sdf)
+    s.step_and_sample(40)
+    vel = s.read_velocity().astype(np.float16)
+    count, trail = 3000, 5
+    tp = abi.TracerParams(count=count, trail=trail, head=0, emitter=emitter, steps=6.0, seed=11, max_age=12.0,
+                          nozzles=7)
+    tp.lines = 3
+    tp.rake_a[:] = [2.0, 3.0, 1.0, 0.0]
+    tp.rake_b[:] = [2.0, dims[1] - 3.0, max(dims[2] - 1.0, 0.5), 0.0]
+    tp.rake_d[:] = [0.0, 0.0, 1.5, 0.0]
+    st = np.zeros((count, 4), np.float32)
+    hi = np.zeros((count * trail, 4), np.float32)
+    for frame in range(6):
+        tp.fill = 1 if frame == 0 else 0
+        tp.advance = 0 if frame == 0 else 1
+        tp.head = frame % trail
+        tp.seed = 11 + frame
+        s.advect_tracers(tp)
+        oracle.tracers(dims, tp, vel, flags, st, hi)
+        gs, gh = s.read_tracers(count, trail)
+        np.testing.assert_array_equal(gs, st, err_msg=f"frame {frame}")
+        np.testing.assert_array_equal(gh, hi, err_msg=f"frame {frame}")

@@ -1,0 +1,149 @@
+"""Pins the CPU oracle to the reference: its lattice tables (extracted from the reference's
+src/solver/lattice.ts into tests/golden/lattice.json) and the pass bands / published results of
+the reference's own validation cases (src/analysis/validation.ts, src/test/harness.ts:20-39,
+README.md:174-176). The reference has no golden vectors, so these are the pins available."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from windtunnel_vis_b200 import mesh as Mh
+from windtunnel_vis_b200 import validation as V
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "lattice.json")
+
+
+@pytest.mark.parametrize("name,dim", [("D2Q9", 2), ("D3Q19", 3)])
+def test_lattice_tables_match_reference(oracle, name, dim):
+    ref = json.load(open(GOLDEN))[name]
+    L = oracle.lattice(dim)
+    assert L["q"] == ref["q"]
+    assert L["c"].tolist() == ref["c"]
+    np.testing.assert_array_equal(L["w"], np.array(ref["w_num"]) / np.array(ref["w_den"]))
+    for k in ("opp", "mirrorY", "mirrorZ", "mirrorYZ"):
+        assert L[k].tolist() == ref[k], k
+
+
+def test_pack_params_matches_write_params(oracle):
+    # SolverGPU.writeParams (SolverGPU.ts:160-187) for the Ahmed case parameters
+    k = oracle.pack_params((224, 70, 96), dict(u=0.06, nu=0.06 * 64 / 20000, cs=0.14, ground="noslip",
+                                              sides="freeslip", spongeNu=0.04, spongeStart=0.84, emaAlpha=0,
+                                              tauWall=0.53, spongeIn=0.03))
+    assert (k.nx, k.ny, k.nz, k.n) == (224, 70, 96, 224 * 70 * 96)
+    assert k.tau0 == np.float32(3 * (0.06 * 64 / 20000) + 0.5)
+    assert k.csmag2 == np.float32(0.14 * 0.14)
+    assert k.uin == np.float32(0.06) and k.rho_in == 1.0
+    assert k.ground == 1 and k.u_ground == 0.0
+    assert k.sponge_start == np.float32(0.84 * 224) and k.sponge_nu == np.float32(0.04)
+    assert k.u_ref == np.float32(0.06) and k.ref_x == 4
+    assert k.side_mode == 0 and k.collision == 0
+    assert k.tau_wall == np.float32(0.53) and k.sponge_in == np.float32(0.03 * 224)
+    assert k.contact_h == 2.0 and k.interp == 1
+    k2 = oracle.pack_params((3, 8, 1), dict(u=0.00001, nu=0.01, ground="moving", sides="periodic", interp=False,
+                                            collision="bgk"))
+    assert k2.ref_x == 2 and k2.u_ref == np.float32(1e-4) and k2.u_ground == np.float32(0.00001)
+    assert k2.side_mode == 1 and k2.collision == 1 and k2.interp == 0 and k2.tau_wall == 0.5
+
+
+def test_encode_sdf(oracle):
+    d = np.array([0.0, 1.5, -1.0, np.nan, 2.4], np.float32)
+    e = oracle.encode_sdf(d)
+    assert e[2] == 0 and e[3] == 0
+    np.testing.assert_array_equal((~e[[0, 1, 4]]).view(np.float32), d[[0, 1, 4]])
+
+
+def test_freestream_case_published(oracle):
+    # validation.ts:61-88; published 1.0000 / 1.0000 (README.md:174)
+    r = V.freestream(oracle.OracleSolver)
+    assert r["passed"]
+    assert abs(r["metrics"]["maxU_over_U"] - 1) < 1e-4
+    assert abs(r["metrics"]["rhoRef"] - 1) < 1e-4
+
+
+def test_cylinder_case_band(oracle):
+    # validation.ts:89-136 at valscale 0.5 (the reference's CI setting, scripts/harness.mjs:15):
+    # St in [0.16, 0.20] with >= 4 cycles; published St 0.173, C_D ~ 1.5 (README.md:175)
+    r = V.cylinder(oracle.OracleSolver, 0.5)
+    m = r["metrics"]
+    assert r["passed"], m
+    assert abs(m["St"] - 0.173) < 0.005
+    assert 1.3 < m["cd_mean"] < 1.7
+
+
+@pytest.mark.parametrize("dims", [(128, 64, 64), (512, 192, 1)])
+def test_voxcheck_band_and_f32_f64_agree(oracle, dims):
+    # harness.ts:20-39: preset sphere (96 x 64 segments), 'center' placement, diamFrac 0.3,
+    # xFrac 0.35: volume within 3 %, frontal within 5 % of analytic
+    pos, idx = Mh.uv_sphere()
+    p, lo, hi, _ = Mh.normalize_mesh(pos)
+    M16, _, _ = Mh.placement_matrix(p, lo, hi, dims, dict(mode="center", lengthFrac=1 / 3, diamFrac=0.3, xFrac=0.35))
+    f32, sdf32, info = oracle.voxelize_f32(dims, p, idx, M16)
+    r = 0.3 * dims[1] / 2
+    is3 = dims[2] > 1
+    ev = 4 / 3 * math.pi * r ** 3 if is3 else math.pi * r * r
+    ea = math.pi * r * r if is3 else 2 * r
+    assert abs(info["solidCells"] / ev - 1) < 0.03
+    assert abs(info["frontal"] / ea - 1) < 0.05
+    f64, sdf64, info64 = oracle.voxelize_f64(dims, p, idx, M16)
+    assert info64 == info
+    np.testing.assert_array_equal(f32 != 0, f64 != 0)
+    k32, k64 = sdf32 != 0, sdf64 >= 0
+    np.testing.assert_array_equal(k32, k64)
+    d32 = (~sdf32[k32]).view(np.float32)
+    assert np.abs(d32 - sdf64[k64]).max() < 1e-4
+
+
+def test_f16_storage_tracks_f32(oracle):
+    # shifted FP16 storage with f32 arithmetic stays close to f32 storage (D3Q19, 200 steps)
+    d = (32, 16, 16)
+    flags, frontal, sdf = V.round_flags(d, (10, 8.37, 8.21), 3, False)
+    base = dict(u=0.05, nu=0.02, cs=0.1, ground="freeslip", sides="freeslip", spongeNu=0.03, spongeStart=0.85,
+                emaAlpha=0)
+    L = oracle.lattice(3)
+    n = d[0] * d[1] * d[2]
+    out = {}
+    for prec in ("f32", "f16", "f64"):
+        s = oracle.OracleSolver(d, dict(base, precision=prec))
+        s.upload_flags(flags)
+        s.upload_sdf(sdf)
+        s.step(200)
+        st = s.sample()
+        f = s.current.astype(np.float64).reshape(19, n)
+        if prec == "f16":
+            f = f + L["w"][:, None]
+        ux = (L["c"][:, 0:1] * f).sum(0) / f.sum(0)
+        out[prec] = (st, ux)
+    f32, f16, f64 = out["f32"], out["f16"], out["f64"]
+    fluid = flags == 0
+    e16 = np.abs(f16[1][fluid] - f64[1][fluid]).max()
+    e32 = np.abs(f32[1][fluid] - f64[1][fluid]).max()
+    assert e32 < 1e-4 * 0.05 and e16 < 2e-3 * 0.05, (e32, e16)
+    assert abs(f32[0]["fx"] - f64[0]["fx"]) < 1e-4 * abs(f64[0]["fx"]) + 1e-7
+    assert abs(f16[0]["fx"] - f64[0]["fx"]) < 2e-2 * abs(f64[0]["fx"]) + 1e-6
+
+
+def test_tracer_oracle_fill_and_spawn(oracle):
+    from windtunnel_vis_b200 import abi
+
+    d = (32, 16, 8)
+    n = d[0] * d[1] * d[2]
+    vel = np.zeros((n, 4), np.float16)
+    vel[:, 0] = 0.05
+    vel[:, 3] = 1
+    flags = np.zeros(n, np.uint32)
+    tp = abi.TracerParams(count=1000, trail=4, head=0, emitter=0, steps=8.0, seed=7, max_age=50.0, nozzles=8)
+    tp.fill = 1
+    state = np.zeros((1000, 4), np.float32)
+    hist = np.zeros((4000, 4), np.float32)
+    oracle.tracers(d, tp, vel, flags, state, hist)
+    assert (state[:, 0] >= 1).all() and (state[:, 0] <= d[0] - 1).all()
+    assert (state[:, 3] == 4).all()
+    tp.fill = 0
+    tp.advance = 1
+    tp.head = 1
+    x0 = state[:, 0].copy()
+    oracle.tracers(d, tp, vel, flags, state, hist)
+    moved = state[:, 3] == 5
+    np.testing.assert_allclose(state[moved, 0] - x0[moved], 0.05 * 8, rtol=1e-3)

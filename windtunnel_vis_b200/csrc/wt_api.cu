@@ -1,0 +1,545 @@
+// wt_api.cu — the extern "C" entry points of libwt.so (declared in include/wt.h).
+//
+// One handle = one tunnel on the device that was current at creation, with its own stream. The
+// handle owns every device buffer; host pointers passed in are only read/written during the
+// call. Errors never abort: each entry point returns a WT_E_* code and records a message.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "wt_internal.h"
+
+namespace {
+
+thread_local std::string g_create_err;
+
+int fail(wt_solver* s, int code, const std::string& msg) {
+  if (s) s->err = msg;
+  else g_create_err = msg;
+  return code;
+}
+
+int cuda_fail(wt_solver* s, cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();  // clear a non-sticky error
+  return fail(s, e == cudaErrorMemoryAllocation ? WT_E_OOM : WT_E_CUDA, m);
+}
+
+#define WT_CUDA(s, call, what)                         \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_fail(s, e_, what); \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+size_t elem_bytes(int prec) { return prec == WT_PREC_F16 ? 2 : (prec == WT_PREC_F64 ? 8 : 4); }
+
+bool dims_ok(const wt_dims* d) {
+  if (!d || d->nx < 1 || d->ny < 1 || d->nz < 1) return false;
+  if (d->ny > 65535 || d->nz > 65535) return false;  // grid.y / grid.z of the row launches
+  const uint64_t n = (uint64_t)d->nx * (uint64_t)d->ny * (uint64_t)d->nz;
+  return n < (1ull << 32);  // the kernel parameter block carries n as u32, like the reference
+}
+
+int64_t bytes_for(const wt_dims* d, int prec) {
+  const int64_t n = (int64_t)d->nx * d->ny * d->nz;
+  const int64_t q = d->nz > 1 ? 19 : 9;
+  // 2 population buffers + flags + sdf + class byte + half4 velocity + meanA + meanB
+  return n * (2 * q * (int64_t)elem_bytes(prec) + 4 + 4 + 1 + 8 + 16 + 4);
+}
+
+void free_all(wt_solver* s) {
+  void* bufs[] = {s->f[0], s->f[1], s->flags, s->sdf, s->cls, s->vel, s->meanA, s->meanB,
+                  s->partials, s->result_dev, s->tr_state, s->tr_hist};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  if (s->result_host) cudaFreeHost(s->result_host);
+  if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+// ---- small device helpers used only by the API -----------------------------------------------
+__global__ void k_encode_sdf(uint32_t* __restrict__ buf, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float v = __uint_as_float(buf[i]);
+    buf[i] = v >= 0.0f ? ~__float_as_uint(v) : 0u;  // negative or NaN -> unknown
+  }
+}
+
+__global__ void k_clear_stats(float4* __restrict__ meanA, float* __restrict__ meanB, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    meanA[i] = make_float4(0.f, 0.f, 0.f, 1.f);
+    meanB[i] = 0.f;
+  }
+}
+
+unsigned grid_for(size_t n) {
+  size_t b = (n + 255) / 256;
+  return (unsigned)(b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b));
+}
+
+int ensure_classified(wt_solver* s) {
+  if (!s->cls_dirty) return WT_OK;
+  WT_CUDA(s, wt::launch_classify(s), "classify");
+  s->cls_dirty = false;
+  return WT_OK;
+}
+
+int ensure_init(wt_solver* s) {
+  if (!s->pending_init) return WT_OK;
+  WT_CUDA(s, wt::launch_init(s), "init");
+  s->pending_init = false;
+  return WT_OK;
+}
+
+void decode(const wt_solver* s, const double* d, wt_stats* out) {
+  std::memset(out, 0, sizeof *out);
+  for (int k = 0; k < 8; k++) out->raw[k] = d[k];
+  out->fx = d[0];
+  out->fy = d[1];
+  out->fz = d[2];
+  out->max_u = std::sqrt(d[3] > 0 ? d[3] : 0.0);
+  out->rho_ref = d[5] > 0 ? d[4] / d[5] : 1.0;
+  out->unstable = (d[6] > 0 || !std::isfinite(d[0]) || d[3] > 0.25) ? 1 : 0;
+  out->step = s->step_count;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wt_version(void) { return WT_ABI_VERSION; }
+
+const char* wt_error_string(int code) {
+  switch (code) {
+    case WT_OK: return "ok";
+    case WT_E_INVALID: return "invalid argument";
+    case WT_E_CUDA: return "CUDA error";
+    case WT_E_OOM: return "out of device memory";
+    case WT_E_STATE: return "invalid state";
+    case WT_E_UNSUPPORTED: return "unsupported";
+    case WT_E_NO_DEVICE: return "no CUDA device";
+    default: return "unknown error";
+  }
+}
+
+int wt_pack_params(const wt_dims* d, const wt_params* p, wt_kparams* k) {
+  if (!d || !p || !k) return WT_E_INVALID;
+  std::memset(k, 0, sizeof *k);
+  const uint32_t nx = (uint32_t)d->nx, ny = (uint32_t)d->ny, nz = (uint32_t)d->nz;
+  k->nx = nx;
+  k->ny = ny;
+  k->nz = nz;
+  k->n = nx * ny * nz;
+  k->tau0 = (float)(3.0 * p->nu + 0.5);
+  k->csmag2 = (float)(p->cs * p->cs);
+  k->uin = (float)p->u;
+  k->rho_in = 1.0f;
+  k->ground = p->ground == WT_GROUND_NOSLIP ? 1u : (p->ground == WT_GROUND_MOVING ? 2u : 0u);
+  k->sponge_start = (float)(p->sponge_start * nx);
+  k->sponge_nu = (float)p->sponge_nu;
+  k->u_ground = p->ground == WT_GROUND_MOVING ? (float)p->u : 0.0f;
+  k->ema_alpha = (float)p->ema_alpha;
+  k->u_ref = (float)(p->u > 1e-4 ? p->u : 1e-4);
+  k->ref_x = nx - 1 < 4u ? nx - 1 : 4u;
+  k->side_mode = p->sides == WT_SIDES_PERIODIC ? 1u : 0u;
+  k->collision = p->collision == WT_COLL_BGK ? 1u : 0u;
+  k->tau_wall = (float)p->tau_wall;
+  k->sponge_in = (float)(p->sponge_in * nx);
+  k->contact_h = 2.0f;
+  k->interp = p->interp ? 1u : 0u;
+  return WT_OK;
+}
+
+int wt_fits(const wt_dims* d, int32_t precision, int64_t* bytes_needed, int32_t* fits) {
+  if (!dims_ok(d) || precision < 0 || precision > 2) return fail(nullptr, WT_E_INVALID, "wt_fits: bad dims/precision");
+  const int64_t b = bytes_for(d, precision);
+  if (bytes_needed) *bytes_needed = b;
+  if (fits) {
+    size_t fr = 0, tot = 0;
+    cudaError_t e = cudaMemGetInfo(&fr, &tot);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaMemGetInfo");
+    *fits = (int64_t)fr > b + (b >> 3) ? 1 : 0;
+  }
+  return WT_OK;
+}
+
+int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
+  if (!out) return fail(nullptr, WT_E_INVALID, "wt_create: out is NULL");
+  *out = nullptr;
+  if (!p || !dims_ok(d)) return fail(nullptr, WT_E_INVALID, "wt_create: bad dims (need nx,ny,nz >= 1, ny,nz <= 65535, cells < 2^32)");
+  if (p->precision < 0 || p->precision > 2) return fail(nullptr, WT_E_INVALID, "wt_create: bad precision");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(nullptr, WT_E_NO_DEVICE, "wt_create: no CUDA device visible");
+  }
+  wt_solver* s = new (std::nothrow) wt_solver();
+  if (!s) return fail(nullptr, WT_E_OOM, "wt_create: host allocation failed");
+  cudaGetDevice(&s->device);
+  s->dims = *d;
+  s->params = *p;
+  s->prec = p->precision;
+  s->is3d = d->nz > 1;
+  s->q = s->is3d ? 19 : 9;
+  s->n = (size_t)d->nx * d->ny * d->nz;
+  s->pop_elem = elem_bytes(s->prec);
+  wt_pack_params(d, p, &s->kp);
+  std::string where;
+  auto alloc = [&](void** ptr, size_t bytes, const char* name) -> bool {
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) {
+      where = std::string("cudaMalloc(") + name + ", " + std::to_string(bytes) + " B): " + cudaGetErrorString(e);
+      cudaGetLastError();
+      return false;
+    }
+    return true;
+  };
+  const size_t fbytes = (size_t)s->q * s->n * s->pop_elem;
+  s->partial_blocks = (int)std::min<size_t>((s->n + 255) / 256, 148 * 8);
+  bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            alloc(&s->f[0], fbytes, "populations A") && alloc(&s->f[1], fbytes, "populations B") &&
+            alloc((void**)&s->flags, s->n * 4, "flags") && alloc((void**)&s->sdf, s->n * 4, "sdf") &&
+            alloc((void**)&s->cls, s->n, "cell class") && alloc((void**)&s->vel, s->n * 8, "velocity") &&
+            alloc((void**)&s->meanA, s->n * 16, "meanA") && alloc((void**)&s->meanB, s->n * 4, "meanB") &&
+            alloc((void**)&s->partials, (size_t)s->partial_blocks * 64, "partials") &&
+            alloc((void**)&s->result_dev, 64, "result");
+  if (ok && cudaMallocHost((void**)&s->result_host, 64) != cudaSuccess) {
+    where = "cudaMallocHost(result)";
+    ok = false;
+  }
+  if (!ok) {
+    int code = where.find("out of memory") != std::string::npos ? WT_E_OOM : WT_E_CUDA;
+    free_all(s);
+    delete s;
+    return fail(nullptr, code, "wt_create: " + (where.empty() ? std::string("stream creation failed") : where));
+  }
+  cudaMemsetAsync(s->flags, 0, s->n * 4, s->stream);
+  cudaMemsetAsync(s->sdf, 0, s->n * 4, s->stream);
+  cudaMemsetAsync(s->vel, 0, s->n * 8, s->stream);
+  k_clear_stats<<<grid_for(s->n), 256, 0, s->stream>>>(s->meanA, s->meanB, s->n);
+  s->launches++;
+  cudaError_t e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) {
+    std::string m = std::string("wt_create: ") + cudaGetErrorString(e);
+    free_all(s);
+    delete s;
+    return fail(nullptr, WT_E_CUDA, m);
+  }
+  s->pending_init = true;
+  s->cls_dirty = true;
+  *out = s;
+  return WT_OK;
+}
+
+void wt_destroy(wt_solver* s) {
+  if (!s) return;
+  DeviceGuard g(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  free_all(s);
+  delete s;
+}
+
+const char* wt_last_error(const wt_solver* s) { return s ? s->err.c_str() : g_create_err.c_str(); }
+
+int wt_set_params(wt_solver* s, const wt_params* p) {
+  if (!s || !p) return WT_E_INVALID;
+  if (p->precision != s->prec) return fail(s, WT_E_INVALID, "wt_set_params: precision is fixed at creation");
+  s->params = *p;
+  wt_pack_params(&s->dims, p, &s->kp);
+  return WT_OK;
+}
+
+int wt_get_params(const wt_solver* s, wt_params* out) {
+  if (!s || !out) return WT_E_INVALID;
+  *out = s->params;
+  return WT_OK;
+}
+
+int wt_get_kparams(const wt_solver* s, wt_kparams* out) {
+  if (!s || !out) return WT_E_INVALID;
+  *out = s->kp;
+  return WT_OK;
+}
+
+int wt_reset(wt_solver* s) {
+  if (!s) return WT_E_INVALID;
+  s->pending_init = true;
+  s->step_count = 0;
+  return wt_clear_stats(s);
+}
+
+int wt_clear_stats(wt_solver* s) {
+  if (!s) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  k_clear_stats<<<grid_for(s->n), 256, 0, s->stream>>>(s->meanA, s->meanB, s->n);
+  s->launches++;
+  WT_CUDA(s, cudaGetLastError(), "clear_stats");
+  return WT_OK;
+}
+
+int64_t wt_step_count(const wt_solver* s) { return s ? s->step_count : -1; }
+
+int wt_upload_flags(wt_solver* s, const uint32_t* flags, int64_t n) {
+  if (!s || !flags) return WT_E_INVALID;
+  if ((size_t)n != s->n) return fail(s, WT_E_INVALID, "wt_upload_flags: n != nx*ny*nz");
+  DeviceGuard g(s->device);
+  WT_CUDA(s, cudaMemcpyAsync(s->flags, flags, s->n * 4, cudaMemcpyHostToDevice, s->stream), "upload flags");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "upload flags");
+  s->cls_dirty = true;
+  return WT_OK;
+}
+
+int wt_upload_sdf(wt_solver* s, const float* d, int64_t n) {
+  if (!s || !d) return WT_E_INVALID;
+  if ((size_t)n != s->n) return fail(s, WT_E_INVALID, "wt_upload_sdf: n != nx*ny*nz");
+  DeviceGuard g(s->device);
+  WT_CUDA(s, cudaMemcpyAsync(s->sdf, d, s->n * 4, cudaMemcpyHostToDevice, s->stream), "upload sdf");
+  k_encode_sdf<<<grid_for(s->n), 256, 0, s->stream>>>(s->sdf, s->n);
+  s->launches++;
+  WT_CUDA(s, cudaGetLastError(), "encode sdf");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "upload sdf");
+  return WT_OK;
+}
+
+int wt_set_wheels(wt_solver* s, const wt_wheel* w, int32_t count) {
+  if (!s || (count > 0 && !w) || count < 0) return WT_E_INVALID;
+  std::memset(&s->wheels, 0, sizeof s->wheels);
+  const int n = count < 16 ? count : 16;
+  s->wheels.count = (uint32_t)n;
+  for (int k = 0; k < n; k++) {
+    const double r = w[k].r > 1e-3 ? w[k].r : 1e-3;
+    s->wheels.w[2 * k] = make_float4((float)w[k].c[0], (float)w[k].c[1], (float)w[k].c[2], (float)(1.0 / r));
+    s->wheels.w[2 * k + 1] = make_float4((float)w[k].axis[0], (float)w[k].axis[1], (float)w[k].axis[2], (float)w[k].hw);
+  }
+  return WT_OK;
+}
+
+int wt_voxelize(wt_solver* s, const float* pos, int64_t nverts, const uint32_t* idx, int64_t ntri, const float m[16],
+                const wt_wheel* wheels, int32_t nwheels, wt_voxel_info* info) {
+  if (!s || !info || !m || ntri < 0 || nverts < 0 || (ntri > 0 && (!pos || !idx))) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  int rc = wt_set_wheels(s, wheels, nwheels);
+  if (rc) return rc;
+  std::memset(info, 0, sizeof *info);
+  if (ntri == 0) {
+    WT_CUDA(s, cudaMemsetAsync(s->flags, 0, s->n * 4, s->stream), "voxelize clear");
+    WT_CUDA(s, cudaMemsetAsync(s->sdf, 0, s->n * 4, s->stream), "voxelize clear");
+    WT_CUDA(s, cudaStreamSynchronize(s->stream), "voxelize clear");
+    s->cls_dirty = true;
+    return WT_OK;
+  }
+  for (int64_t i = 0; i < 3 * ntri; i++)
+    if ((int64_t)idx[i] >= nverts) return fail(s, WT_E_INVALID, "wt_voxelize: index out of range of the vertex array");
+  void *dpos = nullptr, *didx = nullptr, *hits = nullptr, *vote = nullptr, *dinfo = nullptr;
+  auto cleanup = [&]() {
+    for (void* b : {dpos, didx, hits, vote, dinfo})
+      if (b) cudaFree(b);
+  };
+  cudaError_t e = cudaSuccess;
+  if ((e = cudaMalloc(&dpos, (size_t)nverts * 12 + 16)) != cudaSuccess ||
+      (e = cudaMalloc(&didx, (size_t)ntri * 12 + 16)) != cudaSuccess ||
+      (e = cudaMalloc(&hits, 3 * s->n * 4)) != cudaSuccess || (e = cudaMalloc(&vote, s->n * 4)) != cudaSuccess ||
+      (e = cudaMalloc(&dinfo, 32)) != cudaSuccess) {
+    cleanup();
+    return cuda_fail(s, e, "wt_voxelize: scratch allocation");
+  }
+  const uint32_t info_init[8] = {0, 0, 0xffffffffu, 0xffffffffu, 0xffffffffu, 0, 0, 0};
+  uint32_t info_h[8];
+  wt::VoxelJob job;
+  job.pos = (const float*)dpos;
+  job.idx = (const uint32_t*)didx;
+  job.ntri = ntri;
+  std::memcpy(job.M, m, sizeof job.M);
+  job.hits = (int32_t*)hits;
+  job.vote = (uint32_t*)vote;
+  job.info = (uint32_t*)dinfo;
+  if ((e = cudaMemcpyAsync(dpos, pos, (size_t)nverts * 12, cudaMemcpyHostToDevice, s->stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(didx, idx, (size_t)ntri * 12, cudaMemcpyHostToDevice, s->stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(dinfo, info_init, 32, cudaMemcpyHostToDevice, s->stream)) != cudaSuccess ||
+      (e = wt::launch_voxelize(s, job)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(info_h, dinfo, 32, cudaMemcpyDeviceToHost, s->stream)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s->stream)) != cudaSuccess) {
+    cudaStreamSynchronize(s->stream);
+    cleanup();
+    return cuda_fail(s, e, "wt_voxelize");
+  }
+  cleanup();
+  s->cls_dirty = true;
+  const bool ok = info_h[1] > 0;
+  info->frontal = (int32_t)info_h[0];
+  info->solid_cells = (int32_t)info_h[1];
+  for (int k = 0; k < 3; k++) {
+    info->min[k] = ok ? (int32_t)info_h[2 + k] : 0;
+    info->max[k] = ok ? (int32_t)info_h[5 + k] + 1 : 0;
+  }
+  return WT_OK;
+}
+
+int wt_step(wt_solver* s, int32_t steps) {
+  if (!s || steps < 0) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  int rc = ensure_classified(s);
+  if (!rc) rc = ensure_init(s);
+  if (rc) return rc;
+  for (int32_t k = 0; k < steps; k++) {
+    cudaError_t e = wt::launch_stream_collide(s, s->f[s->parity], s->f[s->parity ^ 1]);
+    if (e != cudaSuccess) return cuda_fail(s, e, "stream_collide");
+    s->parity ^= 1;
+  }
+  s->step_count += steps;
+  return WT_OK;
+}
+
+int wt_sample(wt_solver* s, wt_stats* out) {
+  if (!s || !out) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  int rc = ensure_init(s);
+  if (rc) return rc;
+  WT_CUDA(s, wt::launch_macro(s), "macro");
+  WT_CUDA(s, cudaMemcpyAsync(s->result_host, s->result_dev, 64, cudaMemcpyDeviceToHost, s->stream), "read result");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "sample");
+  decode(s, s->result_host, out);
+  return WT_OK;
+}
+
+int wt_step_and_sample(wt_solver* s, int32_t steps, wt_stats* out) {
+  int rc = wt_step(s, steps);
+  if (rc) return rc;
+  return wt_sample(s, out);
+}
+
+int wt_read_flags(wt_solver* s, uint32_t* out, int64_t n) {
+  if (!s || !out || (size_t)n != s->n) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  WT_CUDA(s, cudaMemcpyAsync(out, s->flags, s->n * 4, cudaMemcpyDeviceToHost, s->stream), "read flags");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "read flags");
+  return WT_OK;
+}
+
+int wt_read_sdf(wt_solver* s, uint32_t* out, int64_t n) {
+  if (!s || !out || (size_t)n != s->n) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  WT_CUDA(s, cudaMemcpyAsync(out, s->sdf, s->n * 4, cudaMemcpyDeviceToHost, s->stream), "read sdf");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "read sdf");
+  return WT_OK;
+}
+
+int64_t wt_population_bytes(const wt_solver* s) { return s ? (int64_t)(s->q * s->n * s->pop_elem) : -1; }
+
+int wt_read_populations(wt_solver* s, void* out, int64_t bytes) {
+  if (!s || !out || bytes != wt_population_bytes(s)) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  int rc = ensure_init(s);
+  if (rc) return rc;
+  WT_CUDA(s, cudaMemcpyAsync(out, s->f[s->parity], (size_t)bytes, cudaMemcpyDeviceToHost, s->stream), "read populations");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "read populations");
+  return WT_OK;
+}
+
+int wt_write_populations(wt_solver* s, const void* in, int64_t bytes) {
+  if (!s || !in || bytes != wt_population_bytes(s)) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  WT_CUDA(s, cudaMemcpyAsync(s->f[s->parity], in, (size_t)bytes, cudaMemcpyHostToDevice, s->stream), "write populations");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "write populations");
+  s->pending_init = false;
+  return WT_OK;
+}
+
+int wt_read_velocity(wt_solver* s, float* out4, int64_t n) {
+  if (!s || !out4 || (size_t)n != s->n) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  std::vector<__half> h(4 * s->n);
+  WT_CUDA(s, cudaMemcpyAsync(h.data(), s->vel, s->n * 8, cudaMemcpyDeviceToHost, s->stream), "read velocity");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "read velocity");
+  for (size_t i = 0; i < 4 * s->n; i++) out4[i] = __half2float(h[i]);
+  return WT_OK;
+}
+
+int wt_read_means(wt_solver* s, float* mean4, float* meanb, int64_t n) {
+  if (!s || (size_t)n != s->n) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  if (mean4) WT_CUDA(s, cudaMemcpyAsync(mean4, s->meanA, s->n * 16, cudaMemcpyDeviceToHost, s->stream), "read meanA");
+  if (meanb) WT_CUDA(s, cudaMemcpyAsync(meanb, s->meanB, s->n * 4, cudaMemcpyDeviceToHost, s->stream), "read meanB");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "read means");
+  return WT_OK;
+}
+
+static int ensure_tracers(wt_solver* s, uint32_t count, uint32_t trail) {
+  if (s->tr_state && s->tr_count == count && s->tr_trail == trail) return WT_OK;
+  if (s->tr_state) cudaFree(s->tr_state);
+  if (s->tr_hist) cudaFree(s->tr_hist);
+  s->tr_state = nullptr;
+  s->tr_hist = nullptr;
+  s->tr_count = s->tr_trail = 0;
+  WT_CUDA(s, cudaMalloc((void**)&s->tr_state, (size_t)(count ? count : 1) * 16), "tracer state");
+  WT_CUDA(s, cudaMalloc((void**)&s->tr_hist, (size_t)(count ? count : 1) * (trail ? trail : 1) * 16), "tracer trail");
+  WT_CUDA(s, cudaMemsetAsync(s->tr_state, 0, (size_t)(count ? count : 1) * 16, s->stream), "tracer state");
+  WT_CUDA(s, cudaMemsetAsync(s->tr_hist, 0, (size_t)(count ? count : 1) * (trail ? trail : 1) * 16, s->stream), "tracer trail");
+  s->tr_count = count;
+  s->tr_trail = trail;
+  return WT_OK;
+}
+
+int wt_advect_tracers(wt_solver* s, const wt_tracer_params* p) {
+  if (!s || !p) return WT_E_INVALID;
+  if (p->trail == 0 || p->head >= p->trail) return fail(s, WT_E_INVALID, "wt_advect_tracers: need trail >= 1 and head < trail");
+  if (p->emitter == 1 && p->nozzles == 0) return fail(s, WT_E_INVALID, "wt_advect_tracers: rake emitter needs nozzles >= 1");
+  DeviceGuard g(s->device);
+  int rc = ensure_tracers(s, p->count, p->trail);
+  if (rc) return rc;
+  if (p->count == 0) return WT_OK;
+  WT_CUDA(s, wt::launch_tracers(s, *p), "tracers");
+  return WT_OK;
+}
+
+int wt_read_tracers(wt_solver* s, float* state4, int64_t count, float* hist4, int64_t hist_len) {
+  if (!s || count != (int64_t)s->tr_count) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  if (state4 && count)
+    WT_CUDA(s, cudaMemcpyAsync(state4, s->tr_state, (size_t)count * 16, cudaMemcpyDeviceToHost, s->stream), "read tracers");
+  if (hist4) {
+    if (hist_len != (int64_t)s->tr_count * s->tr_trail) return fail(s, WT_E_INVALID, "wt_read_tracers: hist_len != count*trail");
+    if (hist_len)
+      WT_CUDA(s, cudaMemcpyAsync(hist4, s->tr_hist, (size_t)hist_len * 16, cudaMemcpyDeviceToHost, s->stream), "read trail");
+  }
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "read tracers");
+  return WT_OK;
+}
+
+int wt_write_tracers(wt_solver* s, const float* state4, int64_t count, const float* hist4, int64_t hist_len,
+                     uint32_t trail) {
+  if (!s || count < 0 || trail == 0 || (count > 0 && !state4)) return WT_E_INVALID;
+  if (hist4 && hist_len != count * (int64_t)trail) return fail(s, WT_E_INVALID, "wt_write_tracers: hist_len != count*trail");
+  DeviceGuard g(s->device);
+  int rc = ensure_tracers(s, (uint32_t)count, trail);
+  if (rc) return rc;
+  if (count) WT_CUDA(s, cudaMemcpyAsync(s->tr_state, state4, (size_t)count * 16, cudaMemcpyHostToDevice, s->stream), "write tracers");
+  if (hist4 && hist_len)
+    WT_CUDA(s, cudaMemcpyAsync(s->tr_hist, hist4, (size_t)hist_len * 16, cudaMemcpyHostToDevice, s->stream), "write trail");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "write tracers");
+  return WT_OK;
+}
+
+void* wt_stream(const wt_solver* s) { return s ? (void*)s->stream : nullptr; }
+int32_t wt_device(const wt_solver* s) { return s ? s->device : -1; }
+int64_t wt_launch_count(const wt_solver* s) { return s ? s->launches : -1; }
+
+}  // extern "C"

@@ -1,0 +1,73 @@
+// wt_internal.h — handle layout and kernel launchers shared by the translation units of libwt.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/wt.h"
+#include "wt_common.cuh"
+
+struct wt_solver {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  wt_dims dims{};
+  wt_params params{};
+  wt_kparams kp{};
+  int prec = WT_PREC_F32;
+  int q = 9;
+  bool is3d = false;
+  size_t n = 0;
+  size_t pop_elem = 4;  // bytes per stored population
+  void* f[2] = {nullptr, nullptr};
+  int parity = 0;  // current populations in f[parity]
+  int64_t step_count = 0;
+  bool pending_init = true;
+  uint32_t* flags = nullptr;
+  uint32_t* sdf = nullptr;
+  uint8_t* cls = nullptr;
+  bool cls_dirty = true;
+  uint2* vel = nullptr;  // half4 (ux, uy, uz, rho) per cell
+  float4* meanA = nullptr;
+  float* meanB = nullptr;
+  double* partials = nullptr;  // per-block partial reductions of the macro pass
+  int partial_blocks = 0;
+  double* result_dev = nullptr;  // 8 doubles
+  double* result_host = nullptr; // pinned
+  wt::Wheels wheels{};
+  // tracers
+  float4* tr_state = nullptr;
+  float4* tr_hist = nullptr;
+  uint32_t tr_count = 0, tr_trail = 0;
+  // step launch shape (chosen per lattice by the tuner, see wt_lbm.cu)
+  int block_x = 0;
+  int64_t launches = 0;
+  std::string err;
+};
+
+namespace wt {
+
+int lbm_block_x(const wt_solver* s);
+cudaError_t launch_classify(wt_solver* s);
+cudaError_t launch_init(wt_solver* s);
+cudaError_t launch_stream_collide(wt_solver* s, const void* fin, void* fout);
+cudaError_t launch_macro(wt_solver* s);
+
+// voxelizer (wt_voxel.cu). Scratch buffers hits (3n i32), vote (n u32), info (8 u32) are
+// allocated by the caller.
+struct VoxelJob {
+  const float* pos;     // device, 3 * nverts
+  const uint32_t* idx;  // device, 3 * ntri
+  int64_t ntri;
+  float M[16];
+  int32_t* hits;
+  uint32_t* vote;
+  uint32_t* info;
+};
+cudaError_t launch_voxelize(wt_solver* s, const VoxelJob& job);
+
+// tracers (wt_tracer.cu)
+cudaError_t launch_tracers(wt_solver* s, const wt_tracer_params& p);
+
+}  // namespace wt

@@ -1,0 +1,653 @@
+// wt_lbm.cu — lattice Boltzmann kernels for sm_100a: cell classification, initialisation,
+// fused pull-stream + collide (D2Q9 / D3Q19; f32, shifted-f16 and f64 storage), and the macro
+// pass (velocity field, EMA statistics, momentum-exchange force, reductions).
+//
+// Physics follows the reference's generated WGSL (paths relative to the reference project):
+//   stream + collide ... src/solver/wgslLbm.ts:134-293     init ... wgslLbm.ts:296-341
+//   macro / force ...... src/solver/wgslLbm.ts:347-489     reduce . wgslLbm.ts:491-521
+//
+// Layout: populations SoA, f[i * N + cell], cell = x + nx * (y + ny * z). One thread per cell;
+// a block covers a run of consecutive x in one (y, z) row, so the 19 loads and 19 stores of a
+// warp are contiguous 64-byte (f16) / 128-byte (f32) segments. Cells whose pull stencil stays
+// inside the domain and touches no solid (the bulk of the tunnel) take a branch-free pull; the
+// reference's full boundary logic runs only for cells next to walls, the floor, the roof and
+// the z sides.
+#include <cuda_fp16.h>
+
+#include "wt_internal.h"
+
+namespace wt {
+
+// ---------------------------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------------------------
+template <class R>
+__device__ __forceinline__ R sdf_at(const uint32_t* __restrict__ sdf, size_t id) {
+  uint32_t s = __ldg(sdf + id);
+  if (s == 0u) return (R)-1;
+  return (R)__uint_as_float(~s);
+}
+
+// linkQ (wgslLbm.ts:37-43)
+template <class R>
+__device__ __forceinline__ R link_q(const wt_kparams& P, const uint32_t* __restrict__ sdf, size_t fluid, size_t solid) {
+  if (P.interp == 0u) return (R)0.5;
+  R a = sdf_at<R>(sdf, fluid);
+  R b = sdf_at<R>(sdf, solid);
+  if (a < (R)0 || b < (R)0 || a + b < (R)1e-6f) return (R)0.5;
+  R q = a / (a + b);
+  return q < (R)0.01f ? (R)0.01f : (q > (R)0.99f ? (R)0.99f : q);
+}
+
+// wheelVel (wgslLbm.ts:21-28): u_w = U_g * (1/R) * axis x (p - c)
+template <class R>
+__device__ __forceinline__ void wheel_vel(const wt_kparams& P, const Wheels& W, uint32_t k, R px, R py, R pz, R& ux,
+                                          R& uy, R& uz) {
+  const float4 a = W.w[2 * k];
+  const float4 b = W.w[2 * k + 1];
+  R dx = px - (R)a.x, dy = py - (R)a.y, dz = pz - (R)a.z;
+  R s = (R)P.u_ground * (R)a.w;
+  ux = s * ((R)b.y * dz - (R)b.z * dy);
+  uy = s * ((R)b.z * dx - (R)b.x * dz);
+  uz = s * ((R)b.x * dy - (R)b.y * dx);
+}
+
+__device__ __forceinline__ size_t cell_id(int x, int y, int z, int NX, int NY) {
+  return (size_t)x + (size_t)NX * ((size_t)y + (size_t)NY * (size_t)z);
+}
+
+// ---------------------------------------------------------------------------------------------
+// classify: per-cell class byte (solid / fluid next to a solid pull source)
+// ---------------------------------------------------------------------------------------------
+template <class L>
+__global__ void __launch_bounds__(256) k_classify(const wt_kparams P, const uint32_t* __restrict__ flags,
+                                                  uint8_t* __restrict__ cls) {
+  const int NX = P.nx, NY = P.ny, NZ = P.nz;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y, iz = blockIdx.z;
+  if (ix >= NX) return;
+  const size_t idx = cell_id(ix, iy, iz, NX, NY);
+  if (flags[idx] != 0u) {
+    cls[idx] = CLS_SOLID;
+    return;
+  }
+  uint8_t c = 0;
+  static_for<L::Q>([&](auto I) {
+    constexpr int i = I;
+    if constexpr (i > 0) {
+      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+      int sx = ix - cx, sy = iy - cy, sz = L::DIM == 3 ? iz - cz : 0;
+      if (cx < 0) sx = min(sx, NX - 1);
+      const bool inlet = cx > 0 && sx < 0;
+      const bool yOut = sy < 0 || sy >= NY;
+      const bool zOut = L::DIM == 3 && (sz < 0 || sz >= NZ);
+      if (!inlet && !yOut && !zOut) {
+        const int sxc = min(max(sx, 0), NX - 1);
+        if (flags[cell_id(sxc, sy, sz, NX, NY)] != 0u) c = CLS_NEAR_SOLID;
+      }
+    }
+  });
+  cls[idx] = c;
+}
+
+// ---------------------------------------------------------------------------------------------
+// init (wgslLbm.ts:296-341) + rest-state-with-noise extension
+// ---------------------------------------------------------------------------------------------
+template <class L, class S>
+__global__ void __launch_bounds__(256) k_init(const wt_kparams P, typename S::T* __restrict__ fa,
+                                              typename S::T* __restrict__ fb, const uint32_t* __restrict__ flags,
+                                              int mode, uint32_t seed, float amp) {
+  typedef typename S::R R;
+  const size_t N = P.n;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < N; idx += (size_t)gridDim.x * blockDim.x) {
+    const bool solid = flags[idx] != 0u;
+    float un[3] = {0.f, 0.f, 0.f};
+    if (mode == WT_INIT_FREESTREAM) {
+      un[0] = solid ? 0.0f : P.uin;
+    } else if (!solid) {
+      for (int a = 0; a < L::DIM; a++) un[a] = noise_component(seed, idx, a, amp);
+    }
+    static_for<L::Q>([&](auto I) {
+      constexpr int i = I;
+      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+      typename S::T v;
+      if constexpr (S::PREC == WT_PREC_F16) {
+        // shifted storage: f - w written directly (wgslLbm.ts:297-303)
+        float r;
+        if (mode == WT_INIT_FREESTREAM) {
+          const float ua = un[0];
+          r = (float)Wc<L, i>::v * ((float)(3 * cx) * ua + (float)(4.5 * cx * cx) * ua * ua - 1.5f * ua * ua);
+        } else {
+          float cu = (float)cx * un[0] + (float)cy * un[1] + (float)cz * un[2];
+          float usq = un[0] * un[0] + un[1] * un[1] + un[2] * un[2];
+          r = (float)Wc<L, i>::v * (3.0f * cu + 4.5f * cu * cu - 1.5f * usq);
+        }
+        v = __float2half_rn(r);
+      } else {
+        R r;
+        if (mode == WT_INIT_FREESTREAM) {
+          const R U = (R)un[0];
+          r = (R)Wc<L, i>::v * ((R)1 + (R)(3 * cx) * U + (R)(4.5 * cx * cx) * U * U - (R)1.5 * U * U);
+        } else {
+          float cu = (float)cx * un[0] + (float)cy * un[1] + (float)cz * un[2];
+          float usq = un[0] * un[0] + un[1] * un[1] + un[2] * un[2];
+          r = (R)(float)Wc<L, i>::v * ((R)1 + (R)3 * (R)cu + (R)4.5 * (R)cu * (R)cu - (R)1.5 * (R)usq);
+        }
+        v = (typename S::T)r;
+      }
+      fa[(size_t)i * N + idx] = v;
+      fb[(size_t)i * N + idx] = v;
+    });
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// fused pull-stream + collide
+// ---------------------------------------------------------------------------------------------
+template <class L, class S>
+__global__ void __launch_bounds__(256) k_stream_collide(const wt_kparams P, const typename S::T* __restrict__ fin,
+                                                        typename S::T* __restrict__ fout,
+                                                        const uint8_t* __restrict__ cls,
+                                                        const uint32_t* __restrict__ flags,
+                                                        const uint32_t* __restrict__ sdf, const Wheels W) {
+  typedef typename S::R R;
+  constexpr int Q = L::Q;
+  constexpr bool D3 = L::DIM == 3;
+  const int NX = P.nx, NY = P.ny, NZ = P.nz;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y, iz = blockIdx.z;
+  if (ix >= NX) return;
+  const size_t N = P.n;
+  const size_t idx = cell_id(ix, iy, iz, NX, NY);
+  const uint8_t cl = __ldg(cls + idx);
+  if (cl & CLS_SOLID) {
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      fout[(size_t)i * N + idx] = S::solid((R)Wc<L, i>::v);
+    });
+    return;
+  }
+  const R U = (R)P.uin;
+  R f[Q];
+  bool wall = false, gwall = false;
+  f[0] = S::ld(fin, idx, (R)Wc<L, 0>::v);
+  const bool fast = cl == 0 && iy > 0 && iy < NY - 1 && (!D3 || (iz > 0 && iz < NZ - 1));
+  if (fast) {
+    // bulk: every pull source is an in-domain fluid cell, except the inlet / outlet columns
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      if constexpr (i > 0) {
+        constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+        const R w = (R)Wc<L, i>::v;
+        int sx = ix - cx;
+        if constexpr (cx < 0) sx = min(sx, NX - 1);
+        const size_t src = cell_id(max(sx, 0), iy - cy, D3 ? iz - cz : 0, NX, NY);
+        R v = S::ld(fin, (size_t)i * N + src, w);
+        if constexpr (cx > 0) {
+          if (sx < 0) {
+            const R cu = (R)1 * U;
+            v = w * (R)P.rho_in * ((R)1 + (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * U * U);
+          }
+        }
+        f[i] = v;
+      }
+    });
+  } else {
+    R mvSum = 0, mvW = 0;
+    uint32_t wm = 0;
+    R belt = P.ground == 2u ? (R)1 : (R)0;
+    if (belt > (R)0 && iy == 0) {
+      // tyre contact patches: belt held still near non-wheel solids (wgslLbm.ts:276-287)
+      const int r = (int)P.contact_h;
+      for (int dz = -r; dz <= r; dz++)
+        for (int dx = -r; dx <= r; dx++)
+          for (int dy = 0; dy <= 1 && dy < NY; dy++) {
+            const int qx = ix + dx, qz = iz + dz;
+            if (qx >= 0 && qx < NX && qz >= 0 && qz < NZ) {
+              const uint32_t fq = flags[cell_id(qx, dy, qz, NX, NY)];
+              if (fq != 0u && (fq >> 8u) == 0u) belt = (R)0;
+            }
+          }
+    }
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      if constexpr (i > 0) {
+        constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+        constexpr int io = opp<L>(i);
+        const R w = (R)Wc<L, i>::v;
+        int sx = ix - cx;
+        const int sy = iy - cy, sz = D3 ? iz - cz : 0;
+        if constexpr (cx < 0) sx = min(sx, NX - 1);
+        const bool yOut = cy > 0 ? sy < 0 : (cy < 0 ? sy >= NY : false);
+        const bool zOut = D3 ? (cz > 0 ? sz < 0 : (cz < 0 ? sz >= NZ : false)) : false;
+        R v;
+        if (cx > 0 && sx < 0) {
+          const R cu = (R)1 * U;
+          v = w * (R)P.rho_in * ((R)1 + (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * U * U);
+        } else if (cy > 0 && yOut && P.ground != 0u) {
+          wall = true;
+          gwall = true;
+          v = S::ld(fin, (size_t)io * N + idx, (R)Wc<L, io>::v);
+          if constexpr (cx != 0) v = v + belt * ((R)(6.0 * Wc<L, i>::v * cx) * (R)P.u_ground);
+        } else {
+          const int sxc = min(max(sx, 0), NX - 1);
+          if (D3 && yOut && zOut) {
+            constexpr int k = mirYZ<L>(i);
+            v = S::ld(fin, (size_t)k * N + cell_id(sxc, iy, iz, NX, NY), (R)Wc<L, k>::v);
+          } else if (yOut) {
+            constexpr int k = mirY<L>(i);
+            const int zz = D3 ? min(max(sz, 0), NZ - 1) : 0;
+            v = S::ld(fin, (size_t)k * N + cell_id(sxc, iy, zz, NX, NY), (R)Wc<L, k>::v);
+          } else if (D3 && zOut) {
+            if (P.side_mode == 1u) {
+              v = S::ld(fin, (size_t)i * N + cell_id(sxc, sy, (sz + NZ) % NZ, NX, NY), w);
+            } else {
+              constexpr int k = mirZ<L>(i);
+              v = S::ld(fin, (size_t)k * N + cell_id(sxc, sy, iz, NX, NY), (R)Wc<L, k>::v);
+            }
+          } else {
+            const size_t sc = cell_id(sxc, sy, sz, NX, NY);
+            const uint32_t fs = flags[sc];
+            if (fs != 0u) {
+              // interpolated bounce-back (Bouzidi)
+              wall = true;
+              const R fb = S::ld(fin, (size_t)io * N + idx, (R)Wc<L, io>::v);
+              R q = link_q<R>(P, sdf, idx, sc);
+              v = fb;
+              if (q < (R)0.5) {
+                const int ax = ix + cx, ay = iy + cy, az = D3 ? iz + cz : 0;
+                if (ax >= 0 && ay >= 0 && az >= 0 && ax < NX && ay < NY && az < NZ &&
+                    flags[cell_id(ax, ay, az, NX, NY)] == 0u) {
+                  v = (R)2 * q * fb + ((R)1 - (R)2 * q) * S::ld(fin, (size_t)io * N + cell_id(ax, ay, az, NX, NY), (R)Wc<L, io>::v);
+                } else {
+                  q = (R)0.5;
+                }
+              } else if (q > (R)0.5) {
+                v = ((R)0.5 / q) * fb + ((R)1 - (R)0.5 / q) * S::ld(fin, (size_t)i * N + idx, w);
+              }
+              if ((fs >> 8u) != 0u) {
+                R ux, uy, uz;
+                wheel_vel<R>(P, W, (fs >> 8u) - 1u, (R)0.5 * (R)(ix + sxc) + (R)0.5, (R)0.5 * (R)(iy + sy) + (R)0.5,
+                             (R)0.5 * (R)(iz + sz) + (R)0.5, ux, uy, uz);
+                const R dot = (R)cx * ux + (R)cy * uy + (R)cz * uz;
+                const R mv = (R)(6.0 * Wc<L, i>::v) * dot * (q > (R)0.5 ? (R)0.5 / q : (R)1);
+                v += mv;
+                mvSum += mv;
+                mvW += w;
+                wm |= 1u << i;
+              }
+            } else {
+              v = S::ld(fin, (size_t)i * N + sc, w);
+            }
+          }
+        }
+        f[i] = v;
+      }
+    });
+    // wheel links: remove the net mass of the moving-wall terms (wgslLbm.ts:289-291)
+    if (mvW > (R)0) {
+      const R corr = mvSum / mvW;
+      static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        if constexpr (i > 0)
+          if (wm & (1u << i)) f[i] -= (R)Wc<L, i>::v * corr;
+      });
+    }
+  }
+
+  // ---- collision: regularized BGK / BGK with Smagorinsky (wgslLbm.ts:177-240) ----
+  R rho = f[0];
+  R jx = 0, jy = 0, jz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+    if constexpr (i > 0) rho += f[i];
+    if constexpr (cx != 0) jx += (R)cx * f[i];
+    if constexpr (cy != 0) jy += (R)cy * f[i];
+    if constexpr (cz != 0) jz += (R)cz * f[i];
+    if constexpr (cx != 0) sxx += f[i];
+    if constexpr (cy != 0) syy += f[i];
+    if constexpr (cz != 0) szz += f[i];
+    if constexpr (cx * cy != 0) sxy += (R)(cx * cy) * f[i];
+    if constexpr (cx * cz != 0) sxz += (R)(cx * cz) * f[i];
+    if constexpr (cy * cz != 0) syz += (R)(cy * cz) * f[i];
+  });
+  const R irho = (R)1 / rho;
+  const R ux = jx * irho, uy = jy * irho, uz = D3 ? jz * irho : (R)0;
+  const R usq = ux * ux + uy * uy + uz * uz;
+  const R third = (R)(1.0 / 3.0);
+  const R pxx = sxx - rho * (ux * ux + third);
+  const R pyy = syy - rho * (uy * uy + third);
+  const R pxy = sxy - rho * ux * uy;
+  R pzz = 0, pxz = 0, pyz = 0;
+  if constexpr (D3) {
+    pzz = szz - rho * (uz * uz + third);
+    pxz = sxz - rho * ux * uz;
+    pyz = syz - rho * uy * uz;
+  }
+  R pn = pxx * pxx + (R)2 * pxy * pxy + pyy * pyy;
+  if constexpr (D3) pn = pxx * pxx + (R)2 * pxy * pxy + (R)2 * pxz * pxz + pyy * pyy + (R)2 * pyz * pyz + pzz * pzz;
+  const R piN = sqrt(pn);
+  const R fx = (R)ix;
+  const R den = (R)NX - (R)P.sponge_start;
+  R sp = (fx - (R)P.sponge_start) / (den > (R)1 ? den : (R)1);
+  sp = sp < (R)0 ? (R)0 : (sp > (R)1 ? (R)1 : sp);
+  R t0 = (R)P.tau0 + (R)3 * (R)P.sponge_nu * sp * sp;
+  if (gwall) t0 = t0 > (R)P.tau_wall ? t0 : (R)P.tau_wall;
+  const R tau = (R)0.5 * (t0 + sqrt(t0 * t0 + (R)(18.0 * 1.4142135623730951) * (R)P.csmag2 * piN * irho));
+  const R omega = (R)1 - (R)1 / tau;
+  const R k1 = omega * (R)4.5;
+  const bool useBGK = wall || P.collision == 1u;
+  const R sInDen = (R)P.sponge_in > (R)1 ? (R)P.sponge_in : (R)1;
+  R si = (R)1 - fx / sInDen;
+  si = si < (R)0 ? (R)0 : (si > (R)1 ? (R)1 : si);
+  const R sIn = (R)P.sponge_in > (R)0 ? (R)0.08 * si * si : (R)0;
+  const R trP = (pxx + pyy + pzz) * third;
+  const R base = (R)1 - (R)1.5 * usq;
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+    const R w = (R)Wc<L, i>::v;
+    const R cu = (R)cx * ux + (R)cy * uy + (R)cz * uz;
+    const R feq = w * rho * (base + cu * ((R)3 + (R)4.5 * cu));
+    const R qpi = (R)(cx * cx) * pxx + (R)(cy * cy) * pyy + (R)(cz * cz) * pzz + (R)(2 * cx * cy) * pxy +
+                  (R)(2 * cx * cz) * pxz + (R)(2 * cy * cz) * pyz - trP;
+    R fo = feq + (useBGK ? omega * (f[i] - feq) : w * k1 * qpi);
+    if (sIn > (R)0) {
+      const R eq = w * ((R)1 + (R)(3 * cx) * U + (R)(4.5 * cx * cx) * U * U - (R)1.5 * U * U);
+      fo = fo * ((R)1 - sIn) + eq * sIn;
+    }
+    S::st(fout, (size_t)i * N + idx, fo, w);
+  });
+}
+
+// ---------------------------------------------------------------------------------------------
+// macro pass: velocity field, EMA statistics, momentum-exchange force, partial reductions
+// ---------------------------------------------------------------------------------------------
+constexpr int MACRO_THREADS = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+template <class L, class S>
+__global__ void __launch_bounds__(MACRO_THREADS) k_macro(const wt_kparams P, const typename S::T* __restrict__ fin,
+                                                         const uint32_t* __restrict__ flags,
+                                                         const uint32_t* __restrict__ sdf, const Wheels W,
+                                                         uint2* __restrict__ vel, float4* __restrict__ meanA,
+                                                         float* __restrict__ meanB, double* __restrict__ partials) {
+  typedef typename S::R R;
+  constexpr int Q = L::Q;
+  constexpr bool D3 = L::DIM == 3;
+  const int NX = P.nx, NY = P.ny, NZ = P.nz;
+  const size_t N = P.n;
+  const float a = P.ema_alpha;
+  double accF[3] = {0, 0, 0}, accRho = 0, accNref = 0, accNan = 0, accSolid = 0;
+  float accMax = 0.0f;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < N; idx += (size_t)gridDim.x * blockDim.x) {
+    const int ix = (int)(idx % (size_t)NX);
+    const int iy = (int)((idx / (size_t)NX) % (size_t)NY);
+    const int iz = (int)(idx / ((size_t)NX * NY));
+    auto safe = [&](int x, int y, int z) -> int64_t {
+      if (x < 0 || y < 0 || z < 0 || x >= NX || y >= NY || z >= NZ) return -1;
+      return (int64_t)cell_id(x, y, z, NX, NY);
+    };
+    float out[4] = {0.f, 0.f, 0.f, 1.f};
+    if (flags[idx] == 0u) {
+      R f[Q];
+      static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        f[i] = S::ld(fin, (size_t)i * N + idx, (R)Wc<L, i>::v);
+      });
+      R rho = f[0], jx = 0, jy = 0, jz = 0;
+      static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+        if constexpr (i > 0) rho += f[i];
+        if constexpr (cx != 0) jx += (R)cx * f[i];
+        if constexpr (cy != 0) jy += (R)cy * f[i];
+        if constexpr (cz != 0) jz += (R)cz * f[i];
+      });
+      const R ux = jx / rho, uy = jy / rho, uz = D3 ? jz / rho : (R)0;
+      R Fx = 0, Fy = 0, Fz = 0, mvSum = 0, mvW = 0, Cwx = 0, Cwy = 0, Cwz = 0;
+      static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        if constexpr (i > 0) {
+          constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+          constexpr R w = (R)Wc<L, i>::v;
+          const int64_t s = safe(ix + cx, iy + cy, iz + cz);
+          if (s >= 0 && flags[s] != 0u) {
+            R q = link_q<R>(P, sdf, idx, (size_t)s);
+            R fr = f[i];
+            if (q < (R)0.5) {
+              const int64_t bk = safe(ix - cx, iy - cy, iz - cz);
+              if (bk >= 0 && flags[bk] == 0u) fr = (R)2 * q * f[i] + ((R)1 - (R)2 * q) * S::ld(fin, (size_t)i * N + (size_t)bk, w);
+              else q = (R)0.5;
+            } else if (q > (R)0.5) {
+              constexpr int oi = opp<L>(i);
+              fr = ((R)0.5 / q) * f[i] + ((R)1 - (R)0.5 / q) * f[oi];
+            }
+            const uint32_t tg = flags[s] >> 8u;
+            if (tg != 0u) {
+              R wx, wy, wz;
+              wheel_vel<R>(P, W, tg - 1u, (R)ix + (R)(0.5 + cx / 2.0), (R)iy + (R)(0.5 + cy / 2.0),
+                           (R)iz + (R)(0.5 + cz / 2.0), wx, wy, wz);
+              const R dot = (R)cx * wx + (R)cy * wy + (R)cz * wz;
+              const R mv = -(R)(6.0 * Wc<L, i>::v) * (q > (R)0.5 ? (R)0.5 / q : (R)1) * dot;
+              fr += mv;
+              mvSum += mv;
+              mvW += w;
+              Cwx += (R)cx * w;
+              Cwy += (R)cy * w;
+              Cwz += (R)cz * w;
+            }
+            const R t = f[i] + fr - (R)(2.0 * Wc<L, i>::v);
+            Fx += (R)cx * t;
+            Fy += (R)cy * t;
+            Fz += (R)cz * t;
+          }
+        }
+      });
+      if (mvW > (R)0) {
+        const R k = mvSum / mvW;
+        Fx -= Cwx * k;
+        Fy -= Cwy * k;
+        Fz -= Cwz * k;
+      }
+      const R uu = ux * ux + uy * uy + uz * uz;
+      const bool bad = !(uu < (R)1.0e6) || !(rho > (R)0);
+      out[0] = (float)ux;
+      out[1] = (float)uy;
+      out[2] = (float)uz;
+      out[3] = (float)rho;
+      accF[0] += (double)Fx;
+      accF[1] += (double)Fy;
+      accF[2] += (double)Fz;
+      accMax = fmaxf(accMax, bad ? 1.0e6f : (float)uu);
+      if ((uint32_t)ix == P.ref_x) {
+        accRho += (double)rho;
+        accNref += 1.0;
+      }
+      accNan += bad ? 1.0 : 0.0;
+      float4 m = meanA[idx];
+      m.x = m.x * (1.0f - a) + out[0] * a;
+      m.y = m.y * (1.0f - a) + out[1] * a;
+      m.z = m.z * (1.0f - a) + out[2] * a;
+      m.w = m.w * (1.0f - a) + out[3] * a;
+      meanA[idx] = m;
+      meanB[idx] = meanB[idx] * (1.0f - a) + (float)uu * a;
+    } else {
+      // density extrapolated into the solid from fluid face neighbours (wgslLbm.ts:460-466)
+      R rs = 0, rn = 0;
+      const int nb[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+#pragma unroll
+      for (int k = 0; k < (D3 ? 6 : 4); k++) {
+        const int64_t s = safe(ix + nb[k][0], iy + nb[k][1], iz + nb[k][2]);
+        if (s >= 0 && flags[s] == 0u) {
+          R r = 0;
+          static_for<Q>([&](auto I) {
+            constexpr int j = I;
+            r += S::ld(fin, (size_t)j * N + (size_t)s, (R)Wc<L, j>::v);
+          });
+          rs += r;
+          rn += (R)1;
+        }
+      }
+      if (rn > (R)0) out[3] = (float)(rs / rn);
+      float4 m = meanA[idx];
+      m.x = m.x * (1.0f - a) + out[0] * a;
+      m.y = m.y * (1.0f - a) + out[1] * a;
+      m.z = m.z * (1.0f - a) + out[2] * a;
+      m.w = m.w * (1.0f - a) + out[3] * a;
+      meanA[idx] = m;
+      meanB[idx] = 0.0f;
+      accSolid += 1.0;
+    }
+    __half2 h01 = __floats2half2_rn(out[0], out[1]);
+    __half2 h23 = __floats2half2_rn(out[2], out[3]);
+    uint2 pk;
+    pk.x = *reinterpret_cast<uint32_t*>(&h01);
+    pk.y = *reinterpret_cast<uint32_t*>(&h23);
+    vel[idx] = pk;
+  }
+  // block reduction: warp shuffles, then one warp over the per-warp values
+  __shared__ double sh[MACRO_THREADS / 32][8];
+  double v[8] = {accF[0], accF[1], accF[2], 0.0, accRho, accNref, accNan, accSolid};
+  float mx = warp_max(accMax);
+#pragma unroll
+  for (int k = 0; k < 8; k++)
+    if (k != 3) v[k] = warp_sum(v[k]);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) sh[wid][k] = k == 3 ? (double)mx : v[k];
+  }
+  __syncthreads();
+  if (wid == 0) {
+    constexpr int NW = MACRO_THREADS / 32;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      double x = lane < NW ? sh[lane][k] : 0.0;
+      if (k == 3) {
+        float m = warp_max((float)x);
+        x = (double)m;
+      } else {
+        x = warp_sum(x);
+      }
+      if (lane == 0) partials[(size_t)blockIdx.x * 8 + k] = x;
+    }
+  }
+}
+
+// final reduction of the per-block partials (one block; fixed order, deterministic)
+__global__ void __launch_bounds__(256) k_reduce_partials(const double* __restrict__ partials, int nblocks,
+                                                        double* __restrict__ result) {
+  __shared__ double sh[8][8];
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const double x = partials[(size_t)b * 8 + k];
+      v[k] = k == 3 ? fmax(v[k], x) : v[k] + x;
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    if (k == 3) v[k] = (double)warp_max((float)v[k]);
+    else v[k] = warp_sum(v[k]);
+  }
+  if (lane == 0)
+    for (int k = 0; k < 8; k++) sh[wid][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    const int k = threadIdx.x;
+    double x = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) x = k == 3 ? fmax(x, sh[w][k]) : x + sh[w][k];
+    result[k] = x;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------------------------
+int lbm_block_x(const wt_solver* s) {
+  if (s->block_x > 0) return s->block_x;
+  const int nx = s->dims.nx;
+  const int nb = (nx + 255) / 256;
+  int bx = (nx + nb - 1) / nb;
+  bx = (bx + 31) / 32 * 32;
+  return bx < 32 ? 32 : bx;
+}
+
+static dim3 row_grid(const wt_solver* s, int bx) {
+  return dim3((unsigned)((s->dims.nx + bx - 1) / bx), (unsigned)s->dims.ny, (unsigned)s->dims.nz);
+}
+
+template <class L>
+static cudaError_t classify_t(wt_solver* s) {
+  const int bx = lbm_block_x(s);
+  k_classify<L><<<row_grid(s, bx), bx, 0, s->stream>>>(s->kp, s->flags, s->cls);
+  s->launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_classify(wt_solver* s) { return s->is3d ? classify_t<D3Q19>(s) : classify_t<D2Q9>(s); }
+
+template <class L, class S>
+static cudaError_t init_t(wt_solver* s) {
+  const int threads = 256;
+  size_t blocks = (s->n + threads - 1) / threads;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  const int mode = s->params.init_mode == WT_INIT_REST_NOISE ? WT_INIT_REST_NOISE : WT_INIT_FREESTREAM;
+  k_init<L, S><<<(unsigned)blocks, threads, 0, s->stream>>>(s->kp, (typename S::T*)s->f[0], (typename S::T*)s->f[1],
+                                                            s->flags, mode, s->params.init_seed,
+                                                            (float)s->params.init_noise);
+  s->launches++;
+  return cudaGetLastError();
+}
+
+template <class L, class S>
+static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
+  const int bx = lbm_block_x(s);
+  k_stream_collide<L, S><<<row_grid(s, bx), bx, 0, s->stream>>>(
+      s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->flags, s->sdf, s->wheels);
+  s->launches++;
+  return cudaGetLastError();
+}
+
+template <class L, class S>
+static cudaError_t macro_t(wt_solver* s) {
+  k_macro<L, S><<<s->partial_blocks, MACRO_THREADS, 0, s->stream>>>(
+      s->kp, (const typename S::T*)s->f[s->parity], s->flags, s->sdf, s->wheels, s->vel, s->meanA, s->meanB,
+      s->partials);
+  s->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_reduce_partials<<<1, 256, 0, s->stream>>>(s->partials, s->partial_blocks, s->result_dev);
+  s->launches++;
+  return cudaGetLastError();
+}
+
+#define WT_DISPATCH(FN, ...)                                                                  \
+  do {                                                                                        \
+    if (s->is3d) {                                                                            \
+      if (s->prec == WT_PREC_F16) return FN<D3Q19, StF16>(__VA_ARGS__);                      \
+      if (s->prec == WT_PREC_F64) return FN<D3Q19, StF64>(__VA_ARGS__);                      \
+      return FN<D3Q19, StF32>(__VA_ARGS__);                                                  \
+    }                                                                                         \
+    if (s->prec == WT_PREC_F16) return FN<D2Q9, StF16>(__VA_ARGS__);                         \
+    if (s->prec == WT_PREC_F64) return FN<D2Q9, StF64>(__VA_ARGS__);                         \
+    return FN<D2Q9, StF32>(__VA_ARGS__);                                                     \
+  } while (0)
+
+cudaError_t launch_init(wt_solver* s) { WT_DISPATCH(init_t, s); }
+cudaError_t launch_stream_collide(wt_solver* s, const void* fin, void* fout) { WT_DISPATCH(sc_t, s, fin, fout); }
+cudaError_t launch_macro(wt_solver* s) { WT_DISPATCH(macro_t, s); }
+
+}  // namespace wt

@@ -1,0 +1,288 @@
+"""Host-side mirror of the reference's solver interface, over the C ABI of libwt.so.
+
+    LbmSolver / SolverFactory ... src/backend/types.ts:7-18   -> Solver / solver_factory
+    Backend ..................... src/backend/types.ts:24-53  -> Backend
+    SolverGPU extras ............ src/solver/SolverGPU.ts     -> Solver.read_* / set_wheels / ...
+    VoxelizerGPU.voxelize ....... src/voxelize/VoxelizerGPU.ts:48-151 -> Solver.voxelize
+
+Method names are the reference's in snake_case (uploadFlags -> upload_flags, stepAndSample ->
+step_and_sample); parameters are the reference's SolverParams dict (u, nu, cs, ground, sides,
+spongeNu, spongeStart, spongeIn, tauWall, precision, interp, collision, emaAlpha) and stats come
+back as the SolverStats dict (fx, fy, fz, maxU, rhoRef, unstable, step). Errors raise WtError
+with the library's message. Every call runs on the GPU through libwt.so; there is no CPU path.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+POP_DTYPE = {0: np.float32, 1: np.float16, 2: np.float64}
+
+
+class WtError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{abi.load().wt_error_string(code).decode()} ({code}): {msg}")
+        self.code = code
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _stats_dict(st: abi.Stats):
+    return {
+        "fx": st.fx, "fy": st.fy, "fz": st.fz, "maxU": st.max_u, "rhoRef": st.rho_ref,
+        "unstable": bool(st.unstable), "step": int(st.step), "raw": np.array(st.raw[:], np.float64),
+    }
+
+
+class Solver:
+    """One wind tunnel on the current CUDA device (LbmSolver + the SolverGPU extras)."""
+
+    def __init__(self, dims, params: dict):
+        self._lib = abi.load()
+        self.dims = tuple(int(v) for v in dims)
+        nx, ny, nz = self.dims
+        self.n = nx * ny * nz
+        self.is3d = nz > 1
+        self.q = 19 if self.is3d else 9
+        self.params = dict(params)
+        self.precision = abi.PRECISION[self.params.get("precision", "f32") or "f32"]
+        h = C.c_void_p()
+        d = abi.Dims(nx, ny, nz)
+        rc = self._lib.wt_create(C.byref(d), C.byref(abi.make_params(self.params)), C.byref(h))
+        if rc != 0:
+            raise WtError(rc, self._lib.wt_last_error(None).decode())
+        self._h = h
+
+    # ---- plumbing ----------------------------------------------------------------------------
+    def _check(self, rc):
+        if rc != 0:
+            raise WtError(rc, self._lib.wt_last_error(self._h).decode())
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of this tunnel (for torch.cuda.ExternalStream event timing)."""
+        return int(self._lib.wt_stream(self._h) or 0)
+
+    @property
+    def device(self) -> int:
+        return int(self._lib.wt_device(self._h))
+
+    @property
+    def launches(self) -> int:
+        return int(self._lib.wt_launch_count(self._h))
+
+    @property
+    def step_count(self) -> int:
+        return int(self._lib.wt_step_count(self._h))
+
+    def destroy(self):
+        if getattr(self, "_h", None):
+            self._lib.wt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    # ---- parameters --------------------------------------------------------------------------
+    def set_params(self, p: dict):
+        self.params.update(p)
+        self._check(self._lib.wt_set_params(self._h, C.byref(abi.make_params(self.params))))
+
+    def kparams(self) -> abi.KParams:
+        k = abi.KParams()
+        self._check(self._lib.wt_get_kparams(self._h, C.byref(k)))
+        return k
+
+    def reset(self):
+        self._check(self._lib.wt_reset(self._h))
+
+    def clear_stats(self):
+        self._check(self._lib.wt_clear_stats(self._h))
+
+    # ---- geometry ----------------------------------------------------------------------------
+    def upload_flags(self, flags):
+        f = np.ascontiguousarray(np.asarray(flags).ravel(), np.uint32)
+        self._check(self._lib.wt_upload_flags(self._h, _ptr(f), f.size))
+
+    def upload_sdf(self, d):
+        a = np.ascontiguousarray(np.asarray(d).ravel(), np.float32)
+        self._check(self._lib.wt_upload_sdf(self._h, _ptr(a), a.size))
+
+    def set_wheels(self, wheels):
+        arr, n = abi.make_wheels(list(wheels))
+        self._check(self._lib.wt_set_wheels(self._h, arr, n))
+
+    def voxelize(self, positions, indices, matrix, wheels=()):
+        """Backend.voxelize / VoxelizerGPU.voxelize: mesh (f32 xyz, u32 indices), column-major
+        4x4 mesh->grid matrix, grid-space wheels -> VoxelInfo dict."""
+        pos = np.ascontiguousarray(np.asarray(positions).ravel(), np.float32)
+        idx = np.ascontiguousarray(np.asarray(indices).ravel(), np.uint32)
+        m = np.ascontiguousarray(np.asarray(matrix, np.float64).ravel(), np.float32)
+        if m.size != 16:
+            raise ValueError("matrix must have 16 elements (column-major 4x4)")
+        arr, nw = abi.make_wheels(list(wheels))
+        info = abi.VoxelInfo()
+        self._check(self._lib.wt_voxelize(self._h, _ptr(pos), pos.size // 3, _ptr(idx), idx.size // 3, _ptr(m), arr,
+                                          nw, C.byref(info)))
+        return {"frontal": info.frontal, "solidCells": info.solid_cells, "min": list(info.min), "max": list(info.max)}
+
+    # ---- stepping ----------------------------------------------------------------------------
+    def step(self, steps: int):
+        self._check(self._lib.wt_step(self._h, int(steps)))
+
+    def sample(self):
+        st = abi.Stats()
+        self._check(self._lib.wt_sample(self._h, C.byref(st)))
+        return _stats_dict(st)
+
+    def step_and_sample(self, steps: int):
+        st = abi.Stats()
+        self._check(self._lib.wt_step_and_sample(self._h, int(steps), C.byref(st)))
+        return _stats_dict(st)
+
+    # ---- readback / checkpoint ---------------------------------------------------------------
+    def read_flags(self):
+        out = np.empty(self.n, np.uint32)
+        self._check(self._lib.wt_read_flags(self._h, _ptr(out), self.n))
+        return out
+
+    def read_sdf_encoded(self):
+        out = np.empty(self.n, np.uint32)
+        self._check(self._lib.wt_read_sdf(self._h, _ptr(out), self.n))
+        return out
+
+    def read_populations(self):
+        """Raw current buffer: float32 / float16 (f - w) / float64, shape (q * n,)."""
+        out = np.empty(self.q * self.n, POP_DTYPE[self.precision])
+        self._check(self._lib.wt_read_populations(self._h, _ptr(out), out.nbytes))
+        return out
+
+    def write_populations(self, a):
+        a = np.ascontiguousarray(a, POP_DTYPE[self.precision]).ravel()
+        self._check(self._lib.wt_write_populations(self._h, _ptr(a), a.nbytes))
+
+    def read_velocity(self):
+        out = np.empty((self.n, 4), np.float32)
+        self._check(self._lib.wt_read_velocity(self._h, _ptr(out), self.n))
+        return out
+
+    def read_means(self):
+        a = np.empty((self.n, 4), np.float32)
+        b = np.empty(self.n, np.float32)
+        self._check(self._lib.wt_read_means(self._h, _ptr(a), _ptr(b), self.n))
+        return a, b
+
+    # ---- tracers -----------------------------------------------------------------------------
+    def advect_tracers(self, tp: abi.TracerParams):
+        self._check(self._lib.wt_advect_tracers(self._h, C.byref(tp)))
+
+    def read_tracers(self, count, trail):
+        s = np.empty((count, 4), np.float32)
+        h = np.empty((count * trail, 4), np.float32)
+        self._check(self._lib.wt_read_tracers(self._h, _ptr(s), count, _ptr(h), count * trail))
+        return s, h
+
+    def write_tracers(self, state, hist, trail):
+        s = np.ascontiguousarray(state, np.float32).reshape(-1, 4)
+        h = np.ascontiguousarray(hist, np.float32).reshape(-1, 4)
+        self._check(self._lib.wt_write_tracers(self._h, _ptr(s), s.shape[0], _ptr(h), h.shape[0], int(trail)))
+
+
+def solver_factory(dims, params: dict) -> Solver:
+    """SolverFactory (src/backend/types.ts:18)."""
+    return Solver(dims, params)
+
+
+def pack_params(dims, params: dict) -> abi.KParams:
+    """SolverGPU.writeParams (src/solver/SolverGPU.ts:160-187) through the library."""
+    k = abi.KParams()
+    nx, ny, nz = dims
+    rc = abi.load().wt_pack_params(C.byref(abi.Dims(nx, ny, nz)), C.byref(abi.make_params(params)), C.byref(k))
+    if rc != 0:
+        raise WtError(rc, "wt_pack_params")
+    return k
+
+
+def fits(dims, precision="f32"):
+    """Backend.fits (src/backend/webgpu.ts:58-61): (fits, bytes_needed) on the current device."""
+    nx, ny, nz = dims
+    need = C.c_int64()
+    ok = C.c_int32()
+    rc = abi.load().wt_fits(C.byref(abi.Dims(nx, ny, nz)), abi.PRECISION[precision], C.byref(need), C.byref(ok))
+    if rc != 0:
+        raise WtError(rc, abi.load().wt_last_error(None).decode())
+    return bool(ok.value), int(need.value)
+
+
+class Backend:
+    """Compute half of the reference's Backend (src/backend/types.ts:24-53): owns one solver and
+    runs frames of `steps` steps with a statistics sample, plus voxelization and tracers.
+    Rendering members of the reference (canvas, pixelSize, draw) have no counterpart here."""
+
+    kind = "cuda"
+    supports3D = True
+
+    def __init__(self):
+        self.solver = None
+        self.particles = None
+
+    @property
+    def label(self):
+        return "CUDA sm_100a"
+
+    @property
+    def step_count(self):
+        return self.solver.step_count if self.solver else 0
+
+    @property
+    def cells(self):
+        return self.solver.n if self.solver else 0
+
+    def fits(self, dims, precision="f32"):
+        return fits(dims, precision)[0]
+
+    def create_solver(self, dims, params: dict):
+        if self.solver:
+            self.solver.destroy()
+        self.solver = Solver(dims, params)
+        return self.solver
+
+    def set_params(self, p: dict):
+        self.solver.set_params(p)
+
+    def reset(self):
+        self.solver.reset()
+
+    def clear_stats(self):
+        self.solver.clear_stats()
+
+    def voxelize(self, positions, indices, matrix, wheels=()):
+        return self.solver.voxelize(positions, indices, matrix, wheels)
+
+    def frame(self, steps, on_stats=None, tracers: abi.TracerParams = None):
+        """`steps` solver steps, the macro / statistics pass, and (optionally) one tracer
+        dispatch against the fresh velocity field. Returns SolverStats."""
+        st = self.solver.step_and_sample(steps)
+        if tracers is not None:
+            self.solver.advect_tracers(tracers)
+        if on_stats:
+            on_stats(st)
+        return st
+
+    def solver_factory(self):
+        return solver_factory
+
+    def destroy(self):
+        if self.solver:
+            self.solver.destroy()
+            self.solver = None

@@ -1,0 +1,137 @@
+"""The reference's validation cases, driven through a solver factory.
+
+round_flags .... src/analysis/validation.ts:35-53 (analytic circle / sphere flags + exact sdf)
+freestream ..... src/analysis/validation.ts:61-88
+cylinder ....... src/analysis/validation.ts:89-136
+sphere ......... src/analysis/validation.ts:137-184
+
+A factory is any callable make(dims, params) returning an object with the LbmSolver surface
+(upload_flags, upload_sdf, step_and_sample, destroy) — windtunnel_vis_b200.solver.SolverFactory
+for the CUDA path. Sizes scale with `valscale` like the reference's ?valscale= query.
+"""
+import math
+import time
+
+import numpy as np
+
+from .analysis import coefficients, crossing_frequency, cylinder_st_ref, sphere_cd_ref
+
+
+def js_round(x):
+    """Math.round: halves round towards +infinity."""
+    return int(math.floor(x + 0.5))
+
+
+def round_flags(dims, c, r, cylinder):
+    """Analytic obstacle flags for a circle (2-D) or sphere (3-D): flags u32, frontal cell count,
+    sdf f32 (distance |‖p − c‖ − r| where < 2.5, else −1), all in f64 like the reference."""
+    nx, ny, nz = dims
+    z, y, x = np.meshgrid(np.arange(nz, dtype=np.float64), np.arange(ny, dtype=np.float64),
+                          np.arange(nx, dtype=np.float64), indexing="ij")
+    dx = x + 0.5 - c[0]
+    dy = y + 0.5 - c[1]
+    dz = np.zeros_like(dx) if cylinder else z + 0.5 - c[2]
+    r2 = dx * dx + dy * dy + dz * dz
+    dist = np.abs(np.sqrt(r2) - r)
+    sdf = np.where(dist < 2.5, dist, -1.0).astype(np.float32).ravel()
+    inside = r2 < r * r
+    flags = inside.astype(np.uint32).ravel()
+    frontal = int(inside.any(axis=2).sum())
+    return flags, frontal, sdf
+
+
+def freestream(make, valscale=1.0):
+    t0 = time.perf_counter()
+    d = (256, 96, 1)
+    U = 0.08
+    s = make(d, dict(u=U, nu=0.01, cs=0.1, ground="freeslip", sides="freeslip", spongeNu=0.05, spongeStart=0.85,
+                     emaAlpha=0.02))
+    s.upload_flags(np.zeros(d[0] * d[1], np.uint32))
+    st = s.step_and_sample(1)
+    for _ in range(20):
+        st = s.step_and_sample(50)
+    s.destroy()
+    err = abs(st["maxU"] - U) / U
+    drho = abs(st["rhoRef"] - 1)
+    return {"id": "freestream", "passed": err < 0.01 and drho < 0.01 and not st["unstable"],
+            "seconds": time.perf_counter() - t0,
+            "metrics": {"maxU_over_U": st["maxU"] / U, "rhoRef": st["rhoRef"]}}
+
+
+def cylinder(make, valscale=1.0):
+    t0 = time.perf_counter()
+    D = js_round(24 * valscale)
+    d = (js_round(25 * D), 10 * D, 1)
+    U = 0.06
+    Re = 100
+    nu = U * D / Re
+    s = make(d, dict(u=U, nu=nu, cs=0, ground="freeslip", sides="freeslip", spongeNu=0.03, spongeStart=0.85,
+                     emaAlpha=0.0))
+    flags, _, sdf = round_flags(d, (6 * D, d[1] / 2 + 0.37, 0), D / 2, True)
+    s.upload_flags(flags)
+    s.upload_sdf(sdf)
+    period = D / (0.17 * U)
+    total = js_round(period * 16)
+    measure_from = js_round(period * 6)
+    chunk = max(5, js_round(period / 40))
+    tt, cl, cd = [], [], []
+    step = 0
+    while step < total:
+        st = s.step_and_sample(chunk)
+        if st["unstable"]:
+            break
+        c = coefficients(st["fx"], st["fy"], 0, U, D)
+        if step >= measure_from:
+            tt.append(st["step"])
+            cl.append(c["cl"])
+            cd.append(c["cd"])
+        step += chunk
+    s.destroy()
+    fr = crossing_frequency(tt, cl)
+    St = fr["f"] * D / U
+    cd_mean = sum(cd) / max(len(cd), 1)
+    passed = (0.16 <= St <= 0.2) and fr["cycles"] >= 4
+    return {"id": "cylinder", "passed": bool(passed), "seconds": time.perf_counter() - t0,
+            "series": {"t": tt, "v": cl},
+            "metrics": {"St": St, "St_ref": cylinder_st_ref(Re), "cd_mean": cd_mean, "cl_amplitude": fr["amplitude"],
+                        "cycles": fr["cycles"], "grid": d, "tau": 3 * nu + 0.5}}
+
+
+def sphere(make, valscale=1.0):
+    t0 = time.perf_counter()
+    D = js_round(20 * valscale)
+    d = (js_round(9.6 * D), js_round(4.8 * D), js_round(4.8 * D))
+    U = 0.05
+    Re = 100
+    nu = U * D / Re
+    s = make(d, dict(u=U, nu=nu, cs=0, ground="freeslip", sides="freeslip", spongeNu=0.03, spongeStart=0.85,
+                     emaAlpha=0))
+    flags, frontal, sdf = round_flags(d, (2.8 * D, d[1] / 2 + 0.37, d[2] / 2 + 0.21), D / 2, False)
+    s.upload_flags(flags)
+    s.upload_sdf(sdf)
+    flow_through = d[0] / U
+    total = js_round(flow_through * 2.2)
+    measure_from = js_round(flow_through * 1.4)
+    chunk = 50
+    tt, cds = [], []
+    step = 0
+    while step < total:
+        st = s.step_and_sample(chunk)
+        if st["unstable"]:
+            break
+        c = coefficients(st["fx"], st["fy"], st["fz"], U, frontal)
+        tt.append(st["step"])
+        cds.append(c["cd"])
+        step += chunk
+    s.destroy()
+    sel = [v for t, v in zip(tt, cds) if t >= measure_from]
+    cd = sum(sel) / max(len(sel), 1)
+    ref = sphere_cd_ref(Re)
+    err = (cd - ref) / ref
+    return {"id": "sphere", "passed": abs(err) < 0.2, "seconds": time.perf_counter() - t0,
+            "series": {"t": tt, "v": cds},
+            "metrics": {"cd": cd, "cd_ref": ref, "deviation": err, "grid": d, "frontal": frontal,
+                        "blockage": frontal / (d[1] * d[2])}}
+
+
+CASES = {"freestream": freestream, "cylinder": cylinder, "sphere": sphere}
