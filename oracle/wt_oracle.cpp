@@ -423,14 +423,15 @@ template <int PREC> static void init_cell(const Ctx& X, const Pops<PREC>& F, siz
   if (!solid)
     for (int a = 0; a < L.dim; a++) un[a] = noise_component(seed, idx, a, amp);
   for (int i = 0; i < L.q; i++) {
-    float cu = (float)L.c[i][0] * un[0] + (float)L.c[i][1] * un[1] + (float)L.c[i][2] * un[2];
-    float usq = un[0] * un[0] + un[1] * un[1] + un[2] * un[2];
-    float w = (float)L.w[i];
     if (PREC == WT_PREC_F16) {
-      float v = w * (3.0f * cu + 4.5f * cu * cu - 1.5f * usq);
+      float cu = (float)L.c[i][0] * un[0] + (float)L.c[i][1] * un[1] + (float)L.c[i][2] * un[2];
+      float usq = un[0] * un[0] + un[1] * un[1] + un[2] * un[2];
+      float v = (float)L.w[i] * (3.0f * cu + 4.5f * cu * cu - 1.5f * usq);
       ((_Float16*)F.out)[(size_t)i * F.N + idx] = (_Float16)v;
     } else {
-      R v = (R)w * ((R)1 + (R)3 * (R)cu + (R)4.5 * (R)cu * (R)cu - (R)1.5 * (R)usq);
+      R cu = (R)L.c[i][0] * (R)un[0] + (R)L.c[i][1] * (R)un[1] + (R)L.c[i][2] * (R)un[2];
+      R usq = (R)un[0] * (R)un[0] + (R)un[1] * (R)un[1] + (R)un[2] * (R)un[2];
+      R v = wconst<R>(L.w[i]) * ((R)1 + (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * usq);
       F.st(i, idx, v);
     }
   }

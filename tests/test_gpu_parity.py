@@ -5,7 +5,10 @@ without it, so single-precision results differ by a few ulp per step):
   f64 populations ............ |Δ| <= 1e-12 after 1 and 30 steps
   f32 populations ............ |Δ| <= 1e-6 after 1 step, <= 2e-5 after 30 steps
   f16 (f - w) populations .... |Δ| <= 2e-5 after 1 step (about 2 half ulps), <= 3e-4 after 30
-  force sum / max|u|² ........ relative 1e-4 (f32, f16), 1e-10 (f64); counts exact
+  force sum / max|u|² ........ relative 1e-4 (f32), 5e-3 (f16: a one-ulp f32 difference can flip
+                                the rounding of a stored half, and the force sums hundreds of
+                                wall links), 1e-10 (f64); counts exact
+  EMA means .................. relative 1e-4 (f32, f64), 5e-3 (f16)
   voxelizer flags, sdf, info . bit-exact (compiled without contraction)
   tracers .................... bit-exact state and trail
 """
@@ -20,7 +23,8 @@ from .scenes import PARAM_SETS, scene
 pytestmark = pytest.mark.gpu
 
 TOL = {"f64": (1e-12, 1e-12), "f32": (1e-6, 2e-5), "f16": (2e-5, 3e-4)}
-STAT_RTOL = {"f64": 1e-10, "f32": 1e-4, "f16": 1e-4}
+STAT_RTOL = {"f64": 1e-10, "f32": 1e-4, "f16": 5e-3}
+MEAN_TOL = {"f64": (1e-4, 1e-7), "f32": (1e-4, 1e-7), "f16": (5e-3, 1e-5)}
 
 
 def _pair(oracle, dims, params):
@@ -38,12 +42,14 @@ def _as_float(a):
     return a.astype(np.float64)
 
 
-@pytest.mark.parametrize("prec", ["f32", "f16", "f64"])
+@pytest.mark.parametrize("prec,v", [("f32", 1), ("f32", 2), ("f32", 4), ("f16", 1), ("f16", 2), ("f16", 4),
+                                    ("f64", 1)])
 @pytest.mark.parametrize("pset", list(PARAM_SETS))
 @pytest.mark.parametrize("dims", [(24, 14, 12), (40, 16, 1)])
-def test_stream_collide_matches_oracle(gpu, oracle, dims, pset, prec):
+def test_stream_collide_matches_oracle(gpu, oracle, dims, pset, prec, v):
     params = dict(PARAM_SETS[pset], precision=prec)
     g, o, flags = _pair(oracle, dims, params)
+    g.set_launch(v, 32 if v > 1 else 0, 4 if v > 1 else 0)
     t1, t30 = TOL[prec]
     g.step(1)
     o.step(1)
@@ -66,8 +72,9 @@ def test_stream_collide_matches_oracle(gpu, oracle, dims, pset, prec):
     vo = o.vel.reshape(-1, 4)
     np.testing.assert_allclose(vg, vo, rtol=2e-3, atol=2e-6)
     ma, mb = g.read_means()
-    np.testing.assert_allclose(ma, o.meanA.reshape(-1, 4), rtol=1e-4, atol=1e-7)
-    np.testing.assert_allclose(mb, o.meanB, rtol=1e-3, atol=1e-9)
+    mr, ma_tol = MEAN_TOL[prec]
+    np.testing.assert_allclose(ma, o.meanA.reshape(-1, 4), rtol=mr, atol=ma_tol)
+    np.testing.assert_allclose(mb, o.meanB, rtol=max(mr, 1e-3), atol=ma_tol * 1e-2)
     g.destroy()
 
 

@@ -538,6 +538,80 @@ int wt_write_tracers(wt_solver* s, const float* state4, int64_t count, const flo
   return WT_OK;
 }
 
+int wt_set_launch(wt_solver* s, int32_t v, int32_t bx, int32_t by) {
+  if (!s) return WT_E_INVALID;
+  if (!(v == 1 || v == 2 || v == 4) || bx < 0 || by < 0 || bx * by > 1024 || (bx % 32) != 0 || ((bx == 0) != (by == 0)))
+    return fail(s, WT_E_INVALID, "wt_set_launch: need v in {1,2,4}, bx a multiple of 32, bx*by <= 1024");
+  s->sc_v = v;
+  s->sc_bx = bx;
+  s->sc_by = by;
+  return WT_OK;
+}
+
+int wt_autotune(wt_solver* s, int32_t iters, int32_t* out3) {
+  if (!s || iters < 1) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  int rc = ensure_classified(s);
+  if (!rc) rc = ensure_init(s);
+  if (rc) return rc;
+  struct Cand {
+    int v, bx, by;
+  };
+  std::vector<Cand> cands;
+  const bool vec = s->prec == WT_PREC_F16 || s->prec == WT_PREC_F32;
+  for (int v : {2, 4}) {
+    if (!vec || s->dims.nx % v) continue;
+    const int runs = s->dims.nx / v;
+    for (int bx : {32, 64, 128, 256}) {
+      if (bx > ((runs + 31) / 32) * 32) continue;
+      for (int threads : {128, 256}) {
+        if (threads % bx) continue;
+        cands.push_back({v, bx, threads / bx});
+      }
+    }
+  }
+  cands.push_back({1, 0, 0});
+  cudaEvent_t e0, e1;
+  WT_CUDA(s, cudaEventCreate(&e0), "autotune");
+  WT_CUDA(s, cudaEventCreate(&e1), "autotune");
+  float best = 1e30f;
+  Cand pick = {s->sc_v, s->sc_bx, s->sc_by};
+  for (const Cand& c : cands) {
+    s->sc_v = c.v;
+    s->sc_bx = c.bx;
+    s->sc_by = c.by;
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) e = wt::launch_stream_collide(s, s->f[s->parity], s->f[s->parity ^ 1]);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, s->stream);
+    for (int k = 0; k < iters && e == cudaSuccess; k++)
+      e = wt::launch_stream_collide(s, s->f[s->parity], s->f[s->parity ^ 1]);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return cuda_fail(s, e, "autotune");
+    }
+    if (ms < best) {
+      best = ms;
+      pick = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  s->sc_v = pick.v;
+  s->sc_bx = pick.bx;
+  s->sc_by = pick.by;
+  if (out3) {
+    out3[0] = pick.v;
+    out3[1] = pick.bx;
+    out3[2] = pick.by;
+  }
+  return WT_OK;
+}
+
 void* wt_stream(const wt_solver* s) { return s ? (void*)s->stream : nullptr; }
 int32_t wt_device(const wt_solver* s) { return s ? s->device : -1; }
 int64_t wt_launch_count(const wt_solver* s) { return s ? s->launches : -1; }

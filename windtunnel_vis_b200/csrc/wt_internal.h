@@ -40,8 +40,10 @@ struct wt_solver {
   float4* tr_state = nullptr;
   float4* tr_hist = nullptr;
   uint32_t tr_count = 0, tr_trail = 0;
-  // step launch shape (chosen per lattice by the tuner, see wt_lbm.cu)
+  // step launch shape (chosen per lattice by the tuner, see wt_lbm.cu): cells per thread along x
+  // (1 = scalar kernel) and the block shape of the vectorised kernel (0 = default)
   int block_x = 0;
+  int sc_v = 2, sc_bx = 0, sc_by = 0;
   int64_t launches = 0;
   std::string err;
 };

@@ -129,9 +129,9 @@ __global__ void __launch_bounds__(256) k_init(const wt_kparams P, typename S::T*
           const R U = (R)un[0];
           r = (R)Wc<L, i>::v * ((R)1 + (R)(3 * cx) * U + (R)(4.5 * cx * cx) * U * U - (R)1.5 * U * U);
         } else {
-          float cu = (float)cx * un[0] + (float)cy * un[1] + (float)cz * un[2];
-          float usq = un[0] * un[0] + un[1] * un[1] + un[2] * un[2];
-          r = (R)(float)Wc<L, i>::v * ((R)1 + (R)3 * (R)cu + (R)4.5 * (R)cu * (R)cu - (R)1.5 * (R)usq);
+          const R cu = (R)cx * (R)un[0] + (R)cy * (R)un[1] + (R)cz * (R)un[2];
+          const R usq = (R)un[0] * (R)un[0] + (R)un[1] * (R)un[1] + (R)un[2] * (R)un[2];
+          r = (R)Wc<L, i>::v * ((R)1 + (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * usq);
         }
         v = (typename S::T)r;
       }
@@ -144,158 +144,16 @@ __global__ void __launch_bounds__(256) k_init(const wt_kparams P, typename S::T*
 // ---------------------------------------------------------------------------------------------
 // fused pull-stream + collide
 // ---------------------------------------------------------------------------------------------
-template <class L, class S>
-__global__ void __launch_bounds__(256) k_stream_collide(const wt_kparams P, const typename S::T* __restrict__ fin,
-                                                        typename S::T* __restrict__ fout,
-                                                        const uint8_t* __restrict__ cls,
-                                                        const uint32_t* __restrict__ flags,
-                                                        const uint32_t* __restrict__ sdf, const Wheels W) {
-  typedef typename S::R R;
+
+// Collision on full populations, in the reference's formulation: regularized BGK (or BGK on wall
+// cells / collision = bgk) with the Smagorinsky relaxation time and the outlet / inlet sponges
+// (wgslLbm.ts:177-240). fo receives the post-collision populations.
+template <class L, class R>
+__device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L::Q], int ix, bool wall, bool gwall,
+                                             R (&fo)[L::Q]) {
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
-  const int NX = P.nx, NY = P.ny, NZ = P.nz;
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-  const int iy = blockIdx.y, iz = blockIdx.z;
-  if (ix >= NX) return;
-  const size_t N = P.n;
-  const size_t idx = cell_id(ix, iy, iz, NX, NY);
-  const uint8_t cl = __ldg(cls + idx);
-  if (cl & CLS_SOLID) {
-    static_for<Q>([&](auto I) {
-      constexpr int i = I;
-      fout[(size_t)i * N + idx] = S::solid((R)Wc<L, i>::v);
-    });
-    return;
-  }
   const R U = (R)P.uin;
-  R f[Q];
-  bool wall = false, gwall = false;
-  f[0] = S::ld(fin, idx, (R)Wc<L, 0>::v);
-  const bool fast = cl == 0 && iy > 0 && iy < NY - 1 && (!D3 || (iz > 0 && iz < NZ - 1));
-  if (fast) {
-    // bulk: every pull source is an in-domain fluid cell, except the inlet / outlet columns
-    static_for<Q>([&](auto I) {
-      constexpr int i = I;
-      if constexpr (i > 0) {
-        constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
-        const R w = (R)Wc<L, i>::v;
-        int sx = ix - cx;
-        if constexpr (cx < 0) sx = min(sx, NX - 1);
-        const size_t src = cell_id(max(sx, 0), iy - cy, D3 ? iz - cz : 0, NX, NY);
-        R v = S::ld(fin, (size_t)i * N + src, w);
-        if constexpr (cx > 0) {
-          if (sx < 0) {
-            const R cu = (R)1 * U;
-            v = w * (R)P.rho_in * ((R)1 + (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * U * U);
-          }
-        }
-        f[i] = v;
-      }
-    });
-  } else {
-    R mvSum = 0, mvW = 0;
-    uint32_t wm = 0;
-    R belt = P.ground == 2u ? (R)1 : (R)0;
-    if (belt > (R)0 && iy == 0) {
-      // tyre contact patches: belt held still near non-wheel solids (wgslLbm.ts:276-287)
-      const int r = (int)P.contact_h;
-      for (int dz = -r; dz <= r; dz++)
-        for (int dx = -r; dx <= r; dx++)
-          for (int dy = 0; dy <= 1 && dy < NY; dy++) {
-            const int qx = ix + dx, qz = iz + dz;
-            if (qx >= 0 && qx < NX && qz >= 0 && qz < NZ) {
-              const uint32_t fq = flags[cell_id(qx, dy, qz, NX, NY)];
-              if (fq != 0u && (fq >> 8u) == 0u) belt = (R)0;
-            }
-          }
-    }
-    static_for<Q>([&](auto I) {
-      constexpr int i = I;
-      if constexpr (i > 0) {
-        constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
-        constexpr int io = opp<L>(i);
-        const R w = (R)Wc<L, i>::v;
-        int sx = ix - cx;
-        const int sy = iy - cy, sz = D3 ? iz - cz : 0;
-        if constexpr (cx < 0) sx = min(sx, NX - 1);
-        const bool yOut = cy > 0 ? sy < 0 : (cy < 0 ? sy >= NY : false);
-        const bool zOut = D3 ? (cz > 0 ? sz < 0 : (cz < 0 ? sz >= NZ : false)) : false;
-        R v;
-        if (cx > 0 && sx < 0) {
-          const R cu = (R)1 * U;
-          v = w * (R)P.rho_in * ((R)1 + (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * U * U);
-        } else if (cy > 0 && yOut && P.ground != 0u) {
-          wall = true;
-          gwall = true;
-          v = S::ld(fin, (size_t)io * N + idx, (R)Wc<L, io>::v);
-          if constexpr (cx != 0) v = v + belt * ((R)(6.0 * Wc<L, i>::v * cx) * (R)P.u_ground);
-        } else {
-          const int sxc = min(max(sx, 0), NX - 1);
-          if (D3 && yOut && zOut) {
-            constexpr int k = mirYZ<L>(i);
-            v = S::ld(fin, (size_t)k * N + cell_id(sxc, iy, iz, NX, NY), (R)Wc<L, k>::v);
-          } else if (yOut) {
-            constexpr int k = mirY<L>(i);
-            const int zz = D3 ? min(max(sz, 0), NZ - 1) : 0;
-            v = S::ld(fin, (size_t)k * N + cell_id(sxc, iy, zz, NX, NY), (R)Wc<L, k>::v);
-          } else if (D3 && zOut) {
-            if (P.side_mode == 1u) {
-              v = S::ld(fin, (size_t)i * N + cell_id(sxc, sy, (sz + NZ) % NZ, NX, NY), w);
-            } else {
-              constexpr int k = mirZ<L>(i);
-              v = S::ld(fin, (size_t)k * N + cell_id(sxc, sy, iz, NX, NY), (R)Wc<L, k>::v);
-            }
-          } else {
-            const size_t sc = cell_id(sxc, sy, sz, NX, NY);
-            const uint32_t fs = flags[sc];
-            if (fs != 0u) {
-              // interpolated bounce-back (Bouzidi)
-              wall = true;
-              const R fb = S::ld(fin, (size_t)io * N + idx, (R)Wc<L, io>::v);
-              R q = link_q<R>(P, sdf, idx, sc);
-              v = fb;
-              if (q < (R)0.5) {
-                const int ax = ix + cx, ay = iy + cy, az = D3 ? iz + cz : 0;
-                if (ax >= 0 && ay >= 0 && az >= 0 && ax < NX && ay < NY && az < NZ &&
-                    flags[cell_id(ax, ay, az, NX, NY)] == 0u) {
-                  v = (R)2 * q * fb + ((R)1 - (R)2 * q) * S::ld(fin, (size_t)io * N + cell_id(ax, ay, az, NX, NY), (R)Wc<L, io>::v);
-                } else {
-                  q = (R)0.5;
-                }
-              } else if (q > (R)0.5) {
-                v = ((R)0.5 / q) * fb + ((R)1 - (R)0.5 / q) * S::ld(fin, (size_t)i * N + idx, w);
-              }
-              if ((fs >> 8u) != 0u) {
-                R ux, uy, uz;
-                wheel_vel<R>(P, W, (fs >> 8u) - 1u, (R)0.5 * (R)(ix + sxc) + (R)0.5, (R)0.5 * (R)(iy + sy) + (R)0.5,
-                             (R)0.5 * (R)(iz + sz) + (R)0.5, ux, uy, uz);
-                const R dot = (R)cx * ux + (R)cy * uy + (R)cz * uz;
-                const R mv = (R)(6.0 * Wc<L, i>::v) * dot * (q > (R)0.5 ? (R)0.5 / q : (R)1);
-                v += mv;
-                mvSum += mv;
-                mvW += w;
-                wm |= 1u << i;
-              }
-            } else {
-              v = S::ld(fin, (size_t)i * N + sc, w);
-            }
-          }
-        }
-        f[i] = v;
-      }
-    });
-    // wheel links: remove the net mass of the moving-wall terms (wgslLbm.ts:289-291)
-    if (mvW > (R)0) {
-      const R corr = mvSum / mvW;
-      static_for<Q>([&](auto I) {
-        constexpr int i = I;
-        if constexpr (i > 0)
-          if (wm & (1u << i)) f[i] -= (R)Wc<L, i>::v * corr;
-      });
-    }
-  }
-
-  // ---- collision: regularized BGK / BGK with Smagorinsky (wgslLbm.ts:177-240) ----
   R rho = f[0];
   R jx = 0, jy = 0, jz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
   static_for<Q>([&](auto I) {
@@ -329,7 +187,7 @@ __global__ void __launch_bounds__(256) k_stream_collide(const wt_kparams P, cons
   if constexpr (D3) pn = pxx * pxx + (R)2 * pxy * pxy + (R)2 * pxz * pxz + pyy * pyy + (R)2 * pyz * pyz + pzz * pzz;
   const R piN = sqrt(pn);
   const R fx = (R)ix;
-  const R den = (R)NX - (R)P.sponge_start;
+  const R den = (R)P.nx - (R)P.sponge_start;
   R sp = (fx - (R)P.sponge_start) / (den > (R)1 ? den : (R)1);
   sp = sp < (R)0 ? (R)0 : (sp > (R)1 ? (R)1 : sp);
   R t0 = (R)P.tau0 + (R)3 * (R)P.sponge_nu * sp * sp;
@@ -352,12 +210,461 @@ __global__ void __launch_bounds__(256) k_stream_collide(const wt_kparams P, cons
     const R feq = w * rho * (base + cu * ((R)3 + (R)4.5 * cu));
     const R qpi = (R)(cx * cx) * pxx + (R)(cy * cy) * pyy + (R)(cz * cz) * pzz + (R)(2 * cx * cy) * pxy +
                   (R)(2 * cx * cz) * pxz + (R)(2 * cy * cz) * pyz - trP;
-    R fo = feq + (useBGK ? omega * (f[i] - feq) : w * k1 * qpi);
+    R v = feq + (useBGK ? omega * (f[i] - feq) : w * k1 * qpi);
     if (sIn > (R)0) {
       const R eq = w * ((R)1 + (R)(3 * cx) * U + (R)(4.5 * cx * cx) * U * U - (R)1.5 * U * U);
-      fo = fo * ((R)1 - sIn) + eq * sIn;
+      v = v * ((R)1 - sIn) + eq * sIn;
     }
-    S::st(fout, (size_t)i * N + idx, fo, w);
+    fo[i] = v;
+  });
+}
+
+// Reference-exact update of one fluid cell with every boundary rule of the pull (inlet
+// equilibrium, zero-gradient outlet, free-slip / no-slip / moving-belt floor with tyre contact
+// patches, specular or periodic sides, Bouzidi walls, rotating wheels with their mass fix;
+// wgslLbm.ts:138-175, 276-291). Kept out of line: it runs only for cells next to walls and
+// domain faces, and must not inflate the register budget of the bulk path.
+template <class L, class S>
+__device__ __noinline__ void cell_general(const wt_kparams& P, const typename S::T* __restrict__ fin,
+                                          const uint32_t* __restrict__ flags, const uint32_t* __restrict__ sdf,
+                                          const Wheels& W, int ix, int iy, int iz, typename S::R* out) {
+  typedef typename S::R R;
+  constexpr int Q = L::Q;
+  constexpr bool D3 = L::DIM == 3;
+  const int NX = P.nx, NY = P.ny, NZ = P.nz;
+  const size_t N = P.n;
+  const size_t idx = cell_id(ix, iy, iz, NX, NY);
+  const R U = (R)P.uin;
+  R f[Q];
+  bool wall = false, gwall = false;
+  f[0] = S::ld(fin, idx, (R)Wc<L, 0>::v);
+  R mvSum = 0, mvW = 0;
+  uint32_t wm = 0;
+  R belt = P.ground == 2u ? (R)1 : (R)0;
+  if (belt > (R)0 && iy == 0) {
+    // tyre contact patches: belt held still near non-wheel solids (wgslLbm.ts:276-287)
+    const int r = (int)P.contact_h;
+    for (int dz = -r; dz <= r; dz++)
+      for (int dx = -r; dx <= r; dx++)
+        for (int dy = 0; dy <= 1 && dy < NY; dy++) {
+          const int qx = ix + dx, qz = iz + dz;
+          if (qx >= 0 && qx < NX && qz >= 0 && qz < NZ) {
+            const uint32_t fq = flags[cell_id(qx, dy, qz, NX, NY)];
+            if (fq != 0u && (fq >> 8u) == 0u) belt = (R)0;
+          }
+        }
+  }
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    if constexpr (i > 0) {
+      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+      constexpr int io = opp<L>(i);
+      const R w = (R)Wc<L, i>::v;
+      int sx = ix - cx;
+      const int sy = iy - cy, sz = D3 ? iz - cz : 0;
+      if constexpr (cx < 0) sx = min(sx, NX - 1);
+      const bool yOut = cy > 0 ? sy < 0 : (cy < 0 ? sy >= NY : false);
+      const bool zOut = D3 ? (cz > 0 ? sz < 0 : (cz < 0 ? sz >= NZ : false)) : false;
+      R v;
+      if (cx > 0 && sx < 0) {
+        const R cu = (R)1 * U;
+        v = w * (R)P.rho_in * ((R)1 + (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * U * U);
+      } else if (cy > 0 && yOut && P.ground != 0u) {
+        wall = true;
+        gwall = true;
+        v = S::ld(fin, (size_t)io * N + idx, (R)Wc<L, io>::v);
+        if constexpr (cx != 0) v = v + belt * ((R)(6.0 * Wc<L, i>::v * cx) * (R)P.u_ground);
+      } else {
+        const int sxc = min(max(sx, 0), NX - 1);
+        if (D3 && yOut && zOut) {
+          constexpr int k = mirYZ<L>(i);
+          v = S::ld(fin, (size_t)k * N + cell_id(sxc, iy, iz, NX, NY), (R)Wc<L, k>::v);
+        } else if (yOut) {
+          constexpr int k = mirY<L>(i);
+          const int zz = D3 ? min(max(sz, 0), NZ - 1) : 0;
+          v = S::ld(fin, (size_t)k * N + cell_id(sxc, iy, zz, NX, NY), (R)Wc<L, k>::v);
+        } else if (D3 && zOut) {
+          if (P.side_mode == 1u) {
+            v = S::ld(fin, (size_t)i * N + cell_id(sxc, sy, (sz + NZ) % NZ, NX, NY), w);
+          } else {
+            constexpr int k = mirZ<L>(i);
+            v = S::ld(fin, (size_t)k * N + cell_id(sxc, sy, iz, NX, NY), (R)Wc<L, k>::v);
+          }
+        } else {
+          const size_t sc = cell_id(sxc, sy, sz, NX, NY);
+          const uint32_t fs = flags[sc];
+          if (fs != 0u) {
+            // interpolated bounce-back (Bouzidi)
+            wall = true;
+            const R fb = S::ld(fin, (size_t)io * N + idx, (R)Wc<L, io>::v);
+            R q = link_q<R>(P, sdf, idx, sc);
+            v = fb;
+            if (q < (R)0.5) {
+              const int ax = ix + cx, ay = iy + cy, az = D3 ? iz + cz : 0;
+              if (ax >= 0 && ay >= 0 && az >= 0 && ax < NX && ay < NY && az < NZ &&
+                  flags[cell_id(ax, ay, az, NX, NY)] == 0u) {
+                v = (R)2 * q * fb +
+                    ((R)1 - (R)2 * q) * S::ld(fin, (size_t)io * N + cell_id(ax, ay, az, NX, NY), (R)Wc<L, io>::v);
+              } else {
+                q = (R)0.5;
+              }
+            } else if (q > (R)0.5) {
+              v = ((R)0.5 / q) * fb + ((R)1 - (R)0.5 / q) * S::ld(fin, (size_t)i * N + idx, w);
+            }
+            if ((fs >> 8u) != 0u) {
+              R ux, uy, uz;
+              wheel_vel<R>(P, W, (fs >> 8u) - 1u, (R)0.5 * (R)(ix + sxc) + (R)0.5, (R)0.5 * (R)(iy + sy) + (R)0.5,
+                           (R)0.5 * (R)(iz + sz) + (R)0.5, ux, uy, uz);
+              const R dot = (R)cx * ux + (R)cy * uy + (R)cz * uz;
+              const R mv = (R)(6.0 * Wc<L, i>::v) * dot * (q > (R)0.5 ? (R)0.5 / q : (R)1);
+              v += mv;
+              mvSum += mv;
+              mvW += w;
+              wm |= 1u << i;
+            }
+          } else {
+            v = S::ld(fin, (size_t)i * N + sc, w);
+          }
+        }
+      }
+      f[i] = v;
+    }
+  });
+  // wheel links: remove the net mass of the moving-wall terms (wgslLbm.ts:289-291)
+  if (mvW > (R)0) {
+    const R corr = mvSum / mvW;
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      if constexpr (i > 0)
+        if (wm & (1u << i)) f[i] -= (R)Wc<L, i>::v * corr;
+    });
+  }
+  R fo[Q];
+  collide_full<L, R>(P, f, ix, wall, gwall, fo);
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    out[i] = fo[i];
+  });
+}
+
+// One cell per thread; any storage. Used for f64 and for odd nx.
+template <class L, class S>
+__global__ void __launch_bounds__(256) k_stream_collide(const __grid_constant__ wt_kparams P,
+                                                        const typename S::T* __restrict__ fin,
+                                                        typename S::T* __restrict__ fout,
+                                                        const uint8_t* __restrict__ cls,
+                                                        const uint32_t* __restrict__ flags,
+                                                        const uint32_t* __restrict__ sdf,
+                                                        const __grid_constant__ Wheels W) {
+  typedef typename S::R R;
+  constexpr int Q = L::Q;
+  constexpr bool D3 = L::DIM == 3;
+  const int NX = P.nx, NY = P.ny, NZ = P.nz;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y, iz = blockIdx.z;
+  if (ix >= NX) return;
+  const size_t N = P.n;
+  const size_t idx = cell_id(ix, iy, iz, NX, NY);
+  const uint8_t cl = __ldg(cls + idx);
+  if (cl & CLS_SOLID) {
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      fout[(size_t)i * N + idx] = S::solid((R)Wc<L, i>::v);
+    });
+    return;
+  }
+  R fo[Q];
+  const bool fast = cl == 0 && iy > 0 && iy < NY - 1 && (!D3 || (iz > 0 && iz < NZ - 1));
+  if (fast) {
+    // bulk: every pull source is an in-domain fluid cell, except the inlet / outlet columns
+    const R U = (R)P.uin;
+    R f[Q];
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+      const R w = (R)Wc<L, i>::v;
+      int sx = ix - cx;
+      if constexpr (cx < 0) sx = min(sx, NX - 1);
+      const size_t src = cell_id(max(sx, 0), iy - cy, D3 ? iz - cz : 0, NX, NY);
+      R v = S::ld(fin, (size_t)i * N + src, w);
+      if constexpr (cx > 0) {
+        if (sx < 0) {
+          const R cu = (R)1 * U;
+          v = w * (R)P.rho_in * ((R)1 + (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * U * U);
+        }
+      }
+      f[i] = v;
+    });
+    collide_full<L, R>(P, f, ix, false, false, fo);
+  } else {
+    cell_general<L, S>(P, fin, flags, sdf, W, ix, iy, iz, fo);
+  }
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    S::st(fout, (size_t)i * N + idx, fo[i], (R)Wc<L, i>::v);
+  });
+}
+
+// ---- vectorised bulk kernel: V consecutive cells per thread ---------------------------------
+//
+// Works on shifted populations h = f - w throughout (the FP16 storage format): with
+// drho = sum h, j = sum c h and S = sum c c h, the reference's regularized collision becomes
+//   out_i - w_i = w_i (drho - 1.5 j.u + 4.5 (c_i.j)(c_i.u) + 3 c_i.j + k1 (Q_i : Pi_neq))
+//   Pi_neq = S - j u^T - I drho / 3,   k1 = 4.5 (1 - 1/tau)
+// which is the same algebra as wgslLbm.ts:177-240 without the +w / -w round trip. Moments are
+// built from opposite-direction pair sums h_i + h_opp and differences h_i - h_opp.
+template <class S, int V> struct VecIO;
+template <> struct VecIO<StF16, 2> {
+  __device__ __forceinline__ static void ld(const __half* __restrict__ p, uint32_t o, float (&h)[2], float /*w*/) {
+    const uint32_t u = __ldg(reinterpret_cast<const unsigned int*>(p + o));
+    const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&u));
+    h[0] = f.x;
+    h[1] = f.y;
+  }
+  __device__ __forceinline__ static void st(__half* __restrict__ p, uint32_t o, const float (&h)[2], float /*w*/) {
+    const __half2 v = __floats2half2_rn(h[0], h[1]);
+    *reinterpret_cast<__half2*>(p + o) = v;
+  }
+};
+template <> struct VecIO<StF16, 4> {
+  __device__ __forceinline__ static void ld(const __half* __restrict__ p, uint32_t o, float (&h)[4], float /*w*/) {
+    const uint2 u = __ldg(reinterpret_cast<const uint2*>(p + o));
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+    h[0] = a.x;
+    h[1] = a.y;
+    h[2] = b.x;
+    h[3] = b.y;
+  }
+  __device__ __forceinline__ static void st(__half* __restrict__ p, uint32_t o, const float (&h)[4], float /*w*/) {
+    const __half2 a = __floats2half2_rn(h[0], h[1]);
+    const __half2 b = __floats2half2_rn(h[2], h[3]);
+    uint2 u;
+    u.x = *reinterpret_cast<const uint32_t*>(&a);
+    u.y = *reinterpret_cast<const uint32_t*>(&b);
+    *reinterpret_cast<uint2*>(p + o) = u;
+  }
+};
+template <> struct VecIO<StF32, 2> {
+  __device__ __forceinline__ static void ld(const float* __restrict__ p, uint32_t o, float (&h)[2], float w) {
+    const float2 f = __ldg(reinterpret_cast<const float2*>(p + o));
+    h[0] = f.x - w;
+    h[1] = f.y - w;
+  }
+  __device__ __forceinline__ static void st(float* __restrict__ p, uint32_t o, const float (&h)[2], float w) {
+    *reinterpret_cast<float2*>(p + o) = make_float2(h[0] + w, h[1] + w);
+  }
+};
+template <> struct VecIO<StF32, 4> {
+  __device__ __forceinline__ static void ld(const float* __restrict__ p, uint32_t o, float (&h)[4], float w) {
+    const float4 f = __ldg(reinterpret_cast<const float4*>(p + o));
+    h[0] = f.x - w;
+    h[1] = f.y - w;
+    h[2] = f.z - w;
+    h[3] = f.w - w;
+  }
+  __device__ __forceinline__ static void st(float* __restrict__ p, uint32_t o, const float (&h)[4], float w) {
+    *reinterpret_cast<float4*>(p + o) = make_float4(h[0] + w, h[1] + w, h[2] + w, h[3] + w);
+  }
+};
+__device__ __forceinline__ float ld_shift(const __half* __restrict__ p, uint32_t o, float /*w*/) {
+  return __half2float(__ldg(p + o));
+}
+__device__ __forceinline__ float ld_shift(const float* __restrict__ p, uint32_t o, float w) { return __ldg(p + o) - w; }
+
+// Regularized / BGK collision of one bulk cell on shifted populations (see the block comment).
+template <class L>
+__device__ __forceinline__ void collide_shifted(const wt_kparams& P, const float (&h)[L::Q], int ix, float (&o)[L::Q]) {
+  constexpr int Q = L::Q;
+  constexpr bool D3 = L::DIM == 3;
+  float drho = h[0];
+  float jx = 0.f, jy = 0.f, jz = 0.f, sxx = 0.f, syy = 0.f, szz = 0.f, sxy = 0.f, sxz = 0.f, syz = 0.f;
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    constexpr int io = opp<L>(i);
+    if constexpr (i > 0 && i < io) {
+      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+      const float s = h[i] + h[io];
+      const float d = h[i] - h[io];
+      drho += s;
+      if constexpr (cx > 0) jx += d;
+      if constexpr (cx < 0) jx -= d;
+      if constexpr (cy > 0) jy += d;
+      if constexpr (cy < 0) jy -= d;
+      if constexpr (cz > 0) jz += d;
+      if constexpr (cz < 0) jz -= d;
+      if constexpr (cx != 0) sxx += s;
+      if constexpr (cy != 0) syy += s;
+      if constexpr (cz != 0) szz += s;
+      if constexpr (cx * cy > 0) sxy += s;
+      if constexpr (cx * cy < 0) sxy -= s;
+      if constexpr (cx * cz > 0) sxz += s;
+      if constexpr (cx * cz < 0) sxz -= s;
+      if constexpr (cy * cz > 0) syz += s;
+      if constexpr (cy * cz < 0) syz -= s;
+    }
+  });
+  const float rho = 1.0f + drho;
+  const float irho = __frcp_rn(rho);
+  const float ux = jx * irho, uy = jy * irho, uz = D3 ? jz * irho : 0.0f;
+  const float d3 = drho * (1.0f / 3.0f);
+  const float pxx = sxx - jx * ux - d3;
+  const float pyy = syy - jy * uy - d3;
+  const float pxy = sxy - jx * uy;
+  float pzz = 0.f, pxz = 0.f, pyz = 0.f;
+  if constexpr (D3) {
+    pzz = szz - jz * uz - d3;
+    pxz = sxz - jx * uz;
+    pyz = syz - jy * uz;
+  }
+  float pn = pxx * pxx + 2.0f * pxy * pxy + pyy * pyy;
+  if constexpr (D3) pn += 2.0f * pxz * pxz + pzz * pzz + 2.0f * pyz * pyz;
+  const float fx = (float)ix;
+  const float den = (float)P.nx - P.sponge_start;
+  const float sp = fminf(fmaxf((fx - P.sponge_start) / (den > 1.0f ? den : 1.0f), 0.0f), 1.0f);
+  const float t0 = P.tau0 + 3.0f * P.sponge_nu * sp * sp;
+  const float tau = 0.5f * (t0 + sqrtf(t0 * t0 + (float)(18.0 * 1.4142135623730951) * P.csmag2 * sqrtf(pn) * irho));
+  const float omega = 1.0f - __frcp_rn(tau);
+  const float k1 = 4.5f * omega;
+  const float trP = (pxx + pyy + pzz) * (1.0f / 3.0f);
+  const float ju = jx * ux + jy * uy + jz * uz;
+  const float base = drho - 1.5f * ju;
+  const bool bgk = P.collision == 1u;
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    constexpr int io = opp<L>(i);
+    if constexpr (i == 0 || i < io) {
+      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+      constexpr float w = (float)Wc<L, i>::v;
+      const float cj = (float)cx * jx + (float)cy * jy + (float)cz * jz;
+      const float cu = (float)cx * ux + (float)cy * uy + (float)cz * uz;
+      const float qp = (float)(cx * cx) * pxx + (float)(cy * cy) * pyy + (float)(cz * cz) * pzz +
+                       (float)(2 * cx * cy) * pxy + (float)(2 * cx * cz) * pxz + (float)(2 * cy * cz) * pyz - trP;
+      const float e = base + 4.5f * cj * cu;  // even part of (feq - w) / w
+      const float od = 3.0f * cj;             // odd part
+      if (!bgk) {
+        const float t = e + k1 * qp;
+        o[i] = w * (t + od);
+        if constexpr (i > 0) o[io] = w * (t - od);
+      } else {
+        const float a = 1.0f - omega;
+        o[i] = a * (w * (e + od)) + omega * h[i];
+        if constexpr (i > 0) o[io] = a * (w * (e - od)) + omega * h[io];
+      }
+    }
+  });
+  // inlet absorbing layer: blend towards the free-stream equilibrium (wgslLbm.ts:224-237)
+  if (P.sponge_in > 0.0f) {
+    const float si = fminf(fmaxf(1.0f - fx / fmaxf(P.sponge_in, 1.0f), 0.0f), 1.0f);
+    const float sIn = 0.08f * si * si;
+    if (sIn > 0.0f) {
+      const float U = P.uin;
+      static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        constexpr int cx = L::c[i][0];
+        constexpr float w = (float)Wc<L, i>::v;
+        const float eqw = w * ((float)(3 * cx) * U + (float)(4.5 * cx * cx) * U * U - 1.5f * U * U);
+        o[i] = o[i] * (1.0f - sIn) + eqw * sIn;
+      });
+    }
+  }
+}
+
+template <class L, class S, int V>
+__global__ void __launch_bounds__(256) k_stream_collide_v(const __grid_constant__ wt_kparams P,
+                                                          const typename S::T* __restrict__ fin,
+                                                          typename S::T* __restrict__ fout,
+                                                          const uint8_t* __restrict__ cls,
+                                                          const uint32_t* __restrict__ flags,
+                                                          const uint32_t* __restrict__ sdf,
+                                                          const __grid_constant__ Wheels W) {
+  constexpr int Q = L::Q;
+  constexpr bool D3 = L::DIM == 3;
+  const int NX = P.nx, NY = P.ny, NZ = P.nz;
+  const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z;
+  if (x0 >= NX || iy >= NY) return;
+  const uint32_t N = P.n;
+  const uint32_t sy = (uint32_t)NX, sz = (uint32_t)NX * (uint32_t)NY;
+  const uint32_t idx0 = (uint32_t)x0 + sy * (uint32_t)iy + sz * (uint32_t)iz;
+  uint32_t cv;
+  if constexpr (V == 2) cv = __ldg(reinterpret_cast<const unsigned short*>(cls + idx0));
+  else cv = __ldg(reinterpret_cast<const unsigned int*>(cls + idx0));
+  const bool fast = cv == 0u && iy > 0 && iy < NY - 1 && (!D3 || (iz > 0 && iz < NZ - 1));
+  float o[Q][V];
+  if (fast) {
+    float h[Q][V];
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+      constexpr float w = (float)Wc<L, i>::v;
+      // source row of direction i (bulk cells: y - cy and z - cz are inside the domain)
+      const uint32_t src = i * N + idx0 - (uint32_t)(cy * (int)sy) - (uint32_t)(cz * (int)sz);
+      float cur[V];
+      VecIO<S, V>::ld(fin, src, cur, w);
+      if constexpr (cx == 0) {
+#pragma unroll
+        for (int v = 0; v < V; v++) h[i][v] = cur[v];
+      } else if constexpr (cx > 0) {
+        // pull from x - 1: the last element of the previous run, then cur shifted by one
+        const float prev = ld_shift(fin, x0 > 0 ? src - 1u : src, w);
+        h[i][0] = prev;
+#pragma unroll
+        for (int v = 1; v < V; v++) h[i][v] = cur[v - 1];
+      } else {
+        // pull from x + 1, clamped to the outlet column (zero gradient)
+        const bool last = x0 + V >= NX;
+        const float next = ld_shift(fin, last ? src + (V - 1) : src + V, w);
+#pragma unroll
+        for (int v = 0; v < V - 1; v++) h[i][v] = cur[v + 1];
+        h[i][V - 1] = next;
+      }
+    });
+    if (x0 == 0) {
+      // inlet column: populations entering from x < 0 are the free-stream equilibrium
+      const float U = P.uin;
+      static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        constexpr int cx = L::c[i][0];
+        if constexpr (cx > 0) {
+          constexpr float w = (float)Wc<L, i>::v;
+          h[i][0] = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
+        }
+      });
+    }
+#pragma unroll
+    for (int v = 0; v < V; v++) {
+      float hv[Q], ov[Q];
+#pragma unroll
+      for (int i = 0; i < Q; i++) hv[i] = h[i][v];
+      collide_shifted<L>(P, hv, x0 + v, ov);
+#pragma unroll
+      for (int i = 0; i < Q; i++) o[i][v] = ov[i];
+    }
+  } else {
+#pragma unroll 1
+    for (int v = 0; v < V; v++) {
+      if ((cv >> (8 * v)) & CLS_SOLID) {
+#pragma unroll
+        for (int i = 0; i < Q; i++) o[i][v] = 0.0f;  // solids hold f = w
+      } else {
+        float fo[Q];
+        cell_general<L, S>(P, fin, flags, sdf, W, x0 + v, iy, iz, fo);
+        static_for<Q>([&](auto I) {
+          constexpr int i = I;
+          o[i][v] = fo[i] - (float)Wc<L, i>::v;
+        });
+      }
+    }
+  }
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    constexpr float w = (float)Wc<L, i>::v;
+    float ov[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) ov[v] = o[i][v];
+    VecIO<S, V>::st(fout, i * N + idx0, ov, w);
   });
 }
 
@@ -614,6 +921,30 @@ static cudaError_t init_t(wt_solver* s) {
 
 template <class L, class S>
 static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
+  constexpr bool vec_ok = S::PREC == WT_PREC_F16 || S::PREC == WT_PREC_F32;
+  if constexpr (vec_ok) {
+    const int V = s->sc_v;
+    if ((V == 2 || V == 4) && s->dims.nx % V == 0) {
+      const int runs = s->dims.nx / V;
+      int bx = s->sc_bx, by = s->sc_by;
+      if (bx <= 0 || by <= 0) {
+        bx = runs >= 128 ? 128 : ((runs + 31) / 32) * 32;
+        by = 256 / bx;
+      }
+      const dim3 block(bx, by);
+      const dim3 grid((runs + bx - 1) / bx, (s->dims.ny + by - 1) / by, s->dims.nz);
+      if (V == 2)
+        k_stream_collide_v<L, S, 2><<<grid, block, 0, s->stream>>>(s->kp, (const typename S::T*)fin,
+                                                                    (typename S::T*)fout, s->cls, s->flags, s->sdf,
+                                                                    s->wheels);
+      else
+        k_stream_collide_v<L, S, 4><<<grid, block, 0, s->stream>>>(s->kp, (const typename S::T*)fin,
+                                                                    (typename S::T*)fout, s->cls, s->flags, s->sdf,
+                                                                    s->wheels);
+      s->launches++;
+      return cudaGetLastError();
+    }
+  }
   const int bx = lbm_block_x(s);
   k_stream_collide<L, S><<<row_grid(s, bx), bx, 0, s->stream>>>(
       s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->flags, s->sdf, s->wheels);

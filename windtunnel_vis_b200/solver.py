@@ -182,6 +182,15 @@ class Solver:
         self._check(self._lib.wt_read_means(self._h, _ptr(a), _ptr(b), self.n))
         return a, b
 
+    # ---- launch shape ------------------------------------------------------------------------
+    def set_launch(self, v, bx=0, by=0):
+        self._check(self._lib.wt_set_launch(self._h, int(v), int(bx), int(by)))
+
+    def autotune(self, iters=20):
+        out = (C.c_int32 * 3)()
+        self._check(self._lib.wt_autotune(self._h, int(iters), out))
+        return tuple(out)
+
     # ---- tracers -----------------------------------------------------------------------------
     def advect_tracers(self, tp: abi.TracerParams):
         self._check(self._lib.wt_advect_tracers(self._h, C.byref(tp)))
