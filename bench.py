@@ -70,7 +70,7 @@ class Clocks:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv",
-                                          "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+                                          "-lms", "50"], stdout=self.fh, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
