@@ -218,15 +218,19 @@ int wt_read_tracers(wt_solver* s, float* state4, int64_t count, float* hist4, in
 int wt_write_tracers(wt_solver* s, const float* state4, int64_t count, const float* hist4,
                      int64_t hist_len, uint32_t trail);
 
-/* ---- launch shape (extension; no counterpart in the reference) ------------------------------ */
-/* Forces the stream-collide launch shape: v cells per thread along x (1, 2 or 4; 2 and 4 need
- * f16/f32 storage and nx % v == 0, otherwise the scalar kernel runs), block bx x by threads
- * (0, 0 = default). */
-int wt_set_launch(wt_solver* s, int32_t v, int32_t bx, int32_t by);
-/* Times every candidate launch shape on this handle's grid (iters launches each, reading the
- * current populations and writing the other buffer, so the state does not change) and keeps the
- * fastest. out3 (may be NULL) receives {v, bx, by}. */
-int wt_autotune(wt_solver* s, int32_t iters, int32_t* out3);
+/* ---- launch selection (extension; no counterpart in the reference) ------------------------ */
+/* Selects the stream-collide kernel. kernel 0: register-fed, `param` cells per thread along x
+ * (1, 2 or 4; 2 and 4 need f16/f32 storage and nx % param == 0, otherwise the scalar kernel
+ * runs), block bx x by threads (0, 0 = default). kernel 1: TMA-staged persistent kernel with
+ * `param` pipeline stages (2..4) and bx threads per CTA (0 = default); needs f16 (nx % 8 == 0) or
+ * f32 (nx % 4 == 0) storage and a row of all directions per stage in shared memory. */
+int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32_t by);
+int wt_get_launch(const wt_solver* s, int32_t* out4);
+/* The project's launch tuner: times every applicable candidate of both kernels on this handle's
+ * grid (iters launches each, reading the current populations and writing the other buffer, so
+ * the state does not change) and keeps the fastest. out4 (may be NULL) receives
+ * {kernel, param, bx, by}. */
+int wt_autotune(wt_solver* s, int32_t iters, int32_t* out4);
 
 /* ---- device plumbing -------------------------------------------------------------------- */
 /* The handle's cudaStream_t (for event timing by the caller) and its device ordinal. */

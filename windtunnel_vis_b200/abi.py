@@ -151,7 +151,8 @@ def _sig(lib):
         "wt_advect_tracers": ([S, P(TracerParams)], C.c_int),
         "wt_read_tracers": ([S, v, i64, v, i64], C.c_int),
         "wt_write_tracers": ([S, v, i64, v, i64, C.c_uint32], C.c_int),
-        "wt_set_launch": ([S, i32, i32, i32], C.c_int),
+        "wt_set_launch": ([S, i32, i32, i32, i32], C.c_int),
+        "wt_get_launch": ([S, P(i32)], C.c_int),
         "wt_autotune": ([S, i32, P(i32)], C.c_int),
         "wt_stream": ([S], v),
         "wt_device": ([S], i32),

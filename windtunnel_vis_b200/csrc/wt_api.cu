@@ -68,10 +68,11 @@ int64_t bytes_for(const wt_dims* d, int prec) {
 
 void free_all(wt_solver* s) {
   void* bufs[] = {s->f[0], s->f[1], s->flags, s->sdf, s->cls, s->vel, s->meanA, s->meanB,
-                  s->partials, s->result_dev, s->tr_state, s->tr_hist};
+                  s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->result_host) cudaFreeHost(s->result_host);
+  if (s->err_host) cudaFreeHost(s->err_host);
   if (s->stream) cudaStreamDestroy(s->stream);
 }
 
@@ -106,6 +107,19 @@ int ensure_init(wt_solver* s) {
   if (!s->pending_init) return WT_OK;
   WT_CUDA(s, wt::launch_init(s), "init");
   s->pending_init = false;
+  return WT_OK;
+}
+
+// Reads (and clears) the device error word set by kernels whose bounded waits gave up.
+int check_err_flag(wt_solver* s) {
+  WT_CUDA(s, cudaMemcpyAsync(s->err_host, s->err_dev, 4, cudaMemcpyDeviceToHost, s->stream), "read error word");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "read error word");
+  if (*s->err_host != 0) {
+    const int code = *s->err_host;
+    *s->err_host = 0;
+    cudaMemsetAsync(s->err_dev, 0, 4, s->stream);
+    return fail(s, WT_E_CUDA, "a kernel's bounded wait timed out (device error word " + std::to_string(code) + ")");
+  }
   return WT_OK;
 }
 
@@ -220,8 +234,9 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
             alloc((void**)&s->cls, s->n, "cell class") && alloc((void**)&s->vel, s->n * 8, "velocity") &&
             alloc((void**)&s->meanA, s->n * 16, "meanA") && alloc((void**)&s->meanB, s->n * 4, "meanB") &&
             alloc((void**)&s->partials, (size_t)s->partial_blocks * 64, "partials") &&
-            alloc((void**)&s->result_dev, 64, "result");
-  if (ok && cudaMallocHost((void**)&s->result_host, 64) != cudaSuccess) {
+            alloc((void**)&s->result_dev, 64, "result") && alloc((void**)&s->err_dev, 4, "error word");
+  if (ok && (cudaMallocHost((void**)&s->result_host, 64) != cudaSuccess ||
+             cudaMallocHost((void**)&s->err_host, 4) != cudaSuccess)) {
     where = "cudaMallocHost(result)";
     ok = false;
   }
@@ -234,6 +249,8 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
   cudaMemsetAsync(s->flags, 0, s->n * 4, s->stream);
   cudaMemsetAsync(s->sdf, 0, s->n * 4, s->stream);
   cudaMemsetAsync(s->vel, 0, s->n * 8, s->stream);
+  cudaMemsetAsync(s->err_dev, 0, 4, s->stream);
+  *s->err_host = 0;
   k_clear_stats<<<grid_for(s->n), 256, 0, s->stream>>>(s->meanA, s->meanB, s->n);
   s->launches++;
   cudaError_t e = cudaStreamSynchronize(s->stream);
@@ -415,7 +432,9 @@ int wt_sample(wt_solver* s, wt_stats* out) {
   if (rc) return rc;
   WT_CUDA(s, wt::launch_macro(s), "macro");
   WT_CUDA(s, cudaMemcpyAsync(s->result_host, s->result_dev, 64, cudaMemcpyDeviceToHost, s->stream), "read result");
+  WT_CUDA(s, cudaMemcpyAsync(s->err_host, s->err_dev, 4, cudaMemcpyDeviceToHost, s->stream), "read error word");
   WT_CUDA(s, cudaStreamSynchronize(s->stream), "sample");
+  if (*s->err_host != 0) return check_err_flag(s);
   decode(s, s->result_host, out);
   return WT_OK;
 }
@@ -451,7 +470,7 @@ int wt_read_populations(wt_solver* s, void* out, int64_t bytes) {
   if (rc) return rc;
   WT_CUDA(s, cudaMemcpyAsync(out, s->f[s->parity], (size_t)bytes, cudaMemcpyDeviceToHost, s->stream), "read populations");
   WT_CUDA(s, cudaStreamSynchronize(s->stream), "read populations");
-  return WT_OK;
+  return check_err_flag(s);
 }
 
 int wt_write_populations(wt_solver* s, const void* in, int64_t bytes) {
@@ -538,24 +557,35 @@ int wt_write_tracers(wt_solver* s, const float* state4, int64_t count, const flo
   return WT_OK;
 }
 
-int wt_set_launch(wt_solver* s, int32_t v, int32_t bx, int32_t by) {
+int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32_t by) {
   if (!s) return WT_E_INVALID;
-  if (!(v == 1 || v == 2 || v == 4) || bx < 0 || by < 0 || bx * by > 1024 || (bx % 32) != 0 || ((bx == 0) != (by == 0)))
-    return fail(s, WT_E_INVALID, "wt_set_launch: need v in {1,2,4}, bx a multiple of 32, bx*by <= 1024");
-  s->sc_v = v;
+  if (kernel == 0) {
+    if (!(param == 1 || param == 2 || param == 4) || bx < 0 || by < 0 || bx * by > 1024 || (bx % 32) != 0 ||
+        ((bx == 0) != (by == 0)))
+      return fail(s, WT_E_INVALID, "wt_set_launch: register-fed kernel needs v in {1,2,4}, bx % 32 == 0, bx*by <= 1024");
+  } else if (kernel == 1) {
+    if (param < 2 || param > 4 || bx < 0 || bx > 512 || (bx % 32) != 0)
+      return fail(s, WT_E_INVALID, "wt_set_launch: TMA-staged kernel needs 2..4 stages and bx % 32 == 0, bx <= 512");
+    if (!wt::sc_tma_ok(s, param))
+      return fail(s, WT_E_UNSUPPORTED, "wt_set_launch: TMA-staged kernel needs f16 (nx % 8 == 0) or f32 (nx % 4 == 0) and a row that fits in shared memory");
+  } else {
+    return fail(s, WT_E_INVALID, "wt_set_launch: kernel must be 0 (register-fed) or 1 (TMA-staged)");
+  }
+  s->sc_kernel = kernel;
+  s->sc_param = param;
   s->sc_bx = bx;
   s->sc_by = by;
   return WT_OK;
 }
 
-int wt_autotune(wt_solver* s, int32_t iters, int32_t* out3) {
+int wt_autotune(wt_solver* s, int32_t iters, int32_t* out4) {
   if (!s || iters < 1) return WT_E_INVALID;
   DeviceGuard g(s->device);
   int rc = ensure_classified(s);
   if (!rc) rc = ensure_init(s);
   if (rc) return rc;
   struct Cand {
-    int v, bx, by;
+    int kernel, param, bx, by;
   };
   std::vector<Cand> cands;
   const bool vec = s->prec == WT_PREC_F16 || s->prec == WT_PREC_F32;
@@ -566,18 +596,26 @@ int wt_autotune(wt_solver* s, int32_t iters, int32_t* out3) {
       if (bx > ((runs + 31) / 32) * 32) continue;
       for (int threads : {128, 256}) {
         if (threads % bx) continue;
-        cands.push_back({v, bx, threads / bx});
+        cands.push_back({0, v, bx, threads / bx});
       }
     }
   }
-  cands.push_back({1, 0, 0});
+  for (int st : {2, 3, 4}) {
+    if (!wt::sc_tma_ok(s, st)) continue;
+    for (int bx : {128, 256, 384, 512}) {
+      if (bx > ((s->dims.nx + 31) / 32) * 32 + 31) continue;
+      cands.push_back({1, st, bx, 0});
+    }
+  }
+  cands.push_back({0, 1, 0, 0});
   cudaEvent_t e0, e1;
   WT_CUDA(s, cudaEventCreate(&e0), "autotune");
   WT_CUDA(s, cudaEventCreate(&e1), "autotune");
   float best = 1e30f;
-  Cand pick = {s->sc_v, s->sc_bx, s->sc_by};
+  Cand pick = {s->sc_kernel, s->sc_param, s->sc_bx, s->sc_by};
   for (const Cand& c : cands) {
-    s->sc_v = c.v;
+    s->sc_kernel = c.kernel;
+    s->sc_param = c.param;
     s->sc_bx = c.bx;
     s->sc_by = c.by;
     cudaError_t e = cudaSuccess;
@@ -601,14 +639,25 @@ int wt_autotune(wt_solver* s, int32_t iters, int32_t* out3) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  s->sc_v = pick.v;
+  s->sc_kernel = pick.kernel;
+  s->sc_param = pick.param;
   s->sc_bx = pick.bx;
   s->sc_by = pick.by;
-  if (out3) {
-    out3[0] = pick.v;
-    out3[1] = pick.bx;
-    out3[2] = pick.by;
+  if (out4) {
+    out4[0] = pick.kernel;
+    out4[1] = pick.param;
+    out4[2] = pick.bx;
+    out4[3] = pick.by;
   }
+  return check_err_flag(s);
+}
+
+int wt_get_launch(const wt_solver* s, int32_t* out4) {
+  if (!s || !out4) return WT_E_INVALID;
+  out4[0] = s->sc_kernel;
+  out4[1] = s->sc_param;
+  out4[2] = s->sc_bx;
+  out4[3] = s->sc_by;
   return WT_OK;
 }
 

@@ -14,6 +14,8 @@
 // the z sides.
 #include <cuda_fp16.h>
 
+#include <algorithm>
+
 #include "wt_internal.h"
 
 namespace wt {
@@ -668,6 +670,178 @@ __global__ void __launch_bounds__(256) k_stream_collide_v(const __grid_constant_
   });
 }
 
+// ---- TMA-staged persistent kernel ----------------------------------------------------------
+//
+// The memory-level parallelism of the register-fed kernels is capped by their register budget.
+// Here each CTA walks a strided set of (y, z) rows. For every row a single thread issues one 1-D
+// bulk copy (cp.async.bulk, completion counted on an mbarrier) per direction: the whole source
+// row (y - c_y, z - c_z) of that direction, NX populations, into a shared-memory stage. STAGES
+// rows are in flight per CTA while the threads collide the oldest one out of shared memory,
+// where the x shift of the pull is a plain index offset. Rows on the domain faces and cells next
+// to a solid take the reference-exact per-cell path from global memory. Every wait is bounded:
+// on timeout the kernel records an error code, drains its copies (also bounded) and returns.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: gives up after ~2 s of SM clock (returns false)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > 4000000000ll) return false;
+  return true;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+constexpr int WT_ERR_PIPELINE_TIMEOUT = 1;
+
+template <class S>
+__device__ __forceinline__ float sm_shift(const typename S::T* p, int k, float w);
+template <>
+__device__ __forceinline__ float sm_shift<StF16>(const __half* p, int k, float /*w*/) {
+  return __half2float(p[k]);
+}
+template <>
+__device__ __forceinline__ float sm_shift<StF32>(const float* p, int k, float w) {
+  return p[k] - w;
+}
+template <class S>
+__device__ __forceinline__ void st_shift(typename S::T* p, uint32_t o, float v, float w);
+template <>
+__device__ __forceinline__ void st_shift<StF16>(__half* p, uint32_t o, float v, float /*w*/) {
+  p[o] = __float2half_rn(v);
+}
+template <>
+__device__ __forceinline__ void st_shift<StF32>(float* p, uint32_t o, float v, float w) {
+  p[o] = v + w;
+}
+
+template <class L, class S, int STAGES>
+__global__ void __launch_bounds__(512) k_stream_collide_tma(const __grid_constant__ wt_kparams P,
+                                                            const typename S::T* __restrict__ fin,
+                                                            typename S::T* __restrict__ fout,
+                                                            const uint8_t* __restrict__ cls,
+                                                            const uint32_t* __restrict__ flags,
+                                                            const uint32_t* __restrict__ sdf,
+                                                            const __grid_constant__ Wheels W, int* __restrict__ err) {
+  typedef typename S::T T;
+  constexpr int Q = L::Q;
+  constexpr bool D3 = L::DIM == 3;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int NX = P.nx, NY = P.ny, NZ = P.nz;
+  const uint32_t N = P.n;
+  const uint32_t rows = (uint32_t)NY * (uint32_t)NZ;
+  T* buf = reinterpret_cast<T*>(smem);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + (((size_t)STAGES * Q * NX * sizeof(T) + 15) & ~(size_t)15));
+  const uint32_t row_bytes = (uint32_t)NX * (uint32_t)sizeof(T);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) mbar_init(&full[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const uint32_t first = blockIdx.x, stride = gridDim.x;
+  const uint32_t ntiles = first < rows ? (rows - first + stride - 1) / stride : 0;
+  auto issue = [&](uint32_t k) {
+    const uint32_t r = first + k * stride;
+    const int y = (int)(r % (uint32_t)NY), z = (int)(r / (uint32_t)NY);
+    const int s = (int)(k % STAGES);
+    mbar_expect_tx(&full[s], (uint32_t)Q * row_bytes);
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      constexpr int cy = L::c[i][1], cz = L::c[i][2];
+      const int sy = min(max(y - cy, 0), NY - 1);
+      const int sz = D3 ? min(max(z - cz, 0), NZ - 1) : 0;
+      const T* src = fin + (size_t)i * N + ((size_t)sy + (size_t)NY * (size_t)sz) * (size_t)NX;
+      bulk_g2s(buf + ((size_t)s * Q + i) * NX, src, row_bytes, &full[s]);
+    });
+  };
+  if (threadIdx.x == 0)
+    for (uint32_t k = 0; k < ntiles && k < (uint32_t)STAGES; k++) issue(k);
+
+  const float U = P.uin;
+  for (uint32_t k = 0; k < ntiles; k++) {
+    const int s = (int)(k % STAGES);
+    const bool ok = mbar_wait_bounded(&full[s], (k / STAGES) & 1u);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, WT_ERR_PIPELINE_TIMEOUT);
+        // drain the copies still in flight (bounded) before leaving
+        for (uint32_t j = k + 1; j < ntiles && j < k + STAGES; j++) mbar_wait_bounded(&full[j % STAGES], (j / STAGES) & 1u);
+      }
+      return;
+    }
+    const uint32_t r = first + k * stride;
+    const int iy = (int)(r % (uint32_t)NY), iz = (int)(r / (uint32_t)NY);
+    const uint32_t rowbase = r * (uint32_t)NX;
+    const bool face = iy == 0 || iy == NY - 1 || (D3 && (iz == 0 || iz == NZ - 1));
+    const T* st = buf + (size_t)s * Q * NX;
+    for (int x = threadIdx.x; x < NX; x += blockDim.x) {
+      const uint32_t idx = rowbase + (uint32_t)x;
+      const uint8_t cl = __ldg(cls + idx);
+      float o[Q];
+      if (cl == 0 && !face) {
+        float h[Q];
+        static_for<Q>([&](auto I) {
+          constexpr int i = I;
+          constexpr int cx = L::c[i][0];
+          constexpr float w = (float)Wc<L, i>::v;
+          int xs = x - cx;
+          if constexpr (cx < 0) xs = min(xs, NX - 1);
+          if constexpr (cx > 0) xs = max(xs, 0);
+          float v = sm_shift<S>(st + i * NX, xs, w);
+          if constexpr (cx > 0) {
+            if (x == 0) v = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
+          }
+          h[i] = v;
+        });
+        collide_shifted<L>(P, h, x, o);
+      } else if (cl & CLS_SOLID) {
+#pragma unroll
+        for (int i = 0; i < Q; i++) o[i] = 0.0f;
+      } else {
+        float fo[Q];
+        cell_general<L, S>(P, fin, flags, sdf, W, x, iy, iz, fo);
+        static_for<Q>([&](auto I) {
+          constexpr int i = I;
+          o[i] = fo[i] - (float)Wc<L, i>::v;
+        });
+      }
+      static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        st_shift<S>(fout, i * N + idx, o[i], (float)Wc<L, i>::v);
+      });
+    }
+    __syncthreads();  // every thread is done with stage s
+    if (threadIdx.x == 0 && k + STAGES < ntiles) {
+      fence_proxy_async();
+      issue(k + STAGES);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // macro pass: velocity field, EMA statistics, momentum-exchange force, partial reductions
 // ---------------------------------------------------------------------------------------------
@@ -919,14 +1093,56 @@ static cudaError_t init_t(wt_solver* s) {
   return cudaGetLastError();
 }
 
+template <class L, class S, int STAGES>
+static cudaError_t sc_tma_launch(wt_solver* s, const void* fin, void* fout, int threads) {
+  typedef typename S::T T;
+  auto kern = k_stream_collide_tma<L, S, STAGES>;
+  const size_t smem = (((size_t)STAGES * L::Q * s->dims.nx * sizeof(T) + 15) & ~(size_t)15) + 8 * STAGES;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0, sms = 0, dev = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem)) != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const uint32_t rows = (uint32_t)s->dims.ny * (uint32_t)s->dims.nz;
+  const uint32_t grid = (uint32_t)std::min<uint64_t>(rows, (uint64_t)sms * per_sm);
+  kern<<<grid, threads, smem, s->stream>>>(s->kp, (const T*)fin, (T*)fout, s->cls, s->flags, s->sdf, s->wheels,
+                                           s->err_dev);
+  s->launches++;
+  return cudaGetLastError();
+}
+
+// bytes of shared memory the TMA-staged kernel needs for `stages` stages (0 if not applicable)
+size_t sc_tma_smem(const wt_solver* s, int stages) {
+  if (s->prec == WT_PREC_F16 && s->dims.nx % 8 == 0) return (size_t)stages * s->q * s->dims.nx * 2 + 8 * stages + 16;
+  if (s->prec == WT_PREC_F32 && s->dims.nx % 4 == 0) return (size_t)stages * s->q * s->dims.nx * 4 + 8 * stages + 16;
+  return 0;
+}
+
+// the vectorised and TMA-staged kernels index populations with 32-bit element offsets
+static bool offsets32(const wt_solver* s) { return (uint64_t)s->q * (uint64_t)s->n < (1ull << 32); }
+
+bool sc_tma_ok(const wt_solver* s, int stages) {
+  const size_t b = sc_tma_smem(s, stages);
+  return stages >= 2 && stages <= 4 && b > 0 && b <= 200 * 1024 && offsets32(s);
+}
+
 template <class L, class S>
 static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
   constexpr bool vec_ok = S::PREC == WT_PREC_F16 || S::PREC == WT_PREC_F32;
   if constexpr (vec_ok) {
-    const int V = s->sc_v;
-    if ((V == 2 || V == 4) && s->dims.nx % V == 0) {
+    if (s->sc_kernel == 1 && sc_tma_ok(s, s->sc_param)) {
+      int threads = s->sc_bx;
+      if (threads <= 0) threads = std::min(512, ((s->dims.nx + 31) / 32) * 32);
+      if (s->sc_param == 2) return sc_tma_launch<L, S, 2>(s, fin, fout, threads);
+      if (s->sc_param == 3) return sc_tma_launch<L, S, 3>(s, fin, fout, threads);
+      return sc_tma_launch<L, S, 4>(s, fin, fout, threads);
+    }
+    const int V = s->sc_kernel == 0 ? s->sc_param : 2;
+    if ((V == 2 || V == 4) && s->dims.nx % V == 0 && offsets32(s)) {
       const int runs = s->dims.nx / V;
-      int bx = s->sc_bx, by = s->sc_by;
+      int bx = s->sc_kernel == 0 ? s->sc_bx : 0, by = s->sc_kernel == 0 ? s->sc_by : 0;
       if (bx <= 0 || by <= 0) {
         bx = runs >= 128 ? 128 : ((runs + 31) / 32) * 32;
         by = 256 / bx;

@@ -183,11 +183,19 @@ class Solver:
         return a, b
 
     # ---- launch shape ------------------------------------------------------------------------
-    def set_launch(self, v, bx=0, by=0):
-        self._check(self._lib.wt_set_launch(self._h, int(v), int(bx), int(by)))
+    def set_launch(self, kernel, param, bx=0, by=0):
+        """kernel 0: register-fed, param = cells per thread (1, 2, 4); kernel 1: TMA-staged,
+        param = pipeline stages (2..4)."""
+        self._check(self._lib.wt_set_launch(self._h, int(kernel), int(param), int(bx), int(by)))
+
+    def get_launch(self):
+        out = (C.c_int32 * 4)()
+        self._check(self._lib.wt_get_launch(self._h, out))
+        return tuple(out)
 
     def autotune(self, iters=20):
-        out = (C.c_int32 * 3)()
+        """The launch tuner: returns the chosen (kernel, param, bx, by)."""
+        out = (C.c_int32 * 4)()
         self._check(self._lib.wt_autotune(self._h, int(iters), out))
         return tuple(out)
 
