@@ -572,6 +572,176 @@ __device__ __forceinline__ void collide_shifted(const wt_kparams& P, const float
   }
 }
 
+// ---- packed two-cell collision (sm_100 f32x2 arithmetic) ------------------------------------
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// relaxation time of one bulk cell: molecular tau0 + outlet sponge, Smagorinsky closure
+__device__ __forceinline__ void relax_cell(const wt_kparams& P, float fx, float pn, float irho, float& omega) {
+  float t0 = P.tau0;
+  if (fx > P.sponge_start) {
+    const float den = (float)P.nx - P.sponge_start;
+    const float sp = fminf((fx - P.sponge_start) / (den > 1.0f ? den : 1.0f), 1.0f);
+    t0 += 3.0f * P.sponge_nu * sp * sp;
+  }
+  float tau = t0;
+  if (P.csmag2 > 0.0f) {
+    const float k = (float)(18.0 * 1.4142135623730951) * P.csmag2;
+    tau = 0.5f * (t0 + sqrtf(t0 * t0 + k * sqrtf(pn) * irho));
+  }
+  omega = 1.0f - __fdividef(1.0f, tau);
+}
+
+// Regularized / BGK collision of two bulk cells at once on shifted populations (lanes .x, .y),
+// same algebra as collide_shifted.
+template <class L>
+__device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const float2 (&h)[L::Q], int x, float2 (&o)[L::Q]) {
+  constexpr int Q = L::Q;
+  constexpr bool D3 = L::DIM == 3;
+  float2 drho = h[0];
+  float2 jx = f2(0.f), jy = f2(0.f), jz = f2(0.f), sxx = f2(0.f), syy = f2(0.f), szz = f2(0.f), sxy = f2(0.f),
+         sxz = f2(0.f), syz = f2(0.f);
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    constexpr int io = opp<L>(i);
+    if constexpr (i > 0 && i < io) {
+      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+      const float2 s = add2(h[i], h[io]);
+      const float2 d = sub2(h[i], h[io]);
+      drho = add2(drho, s);
+      if constexpr (cx > 0) jx = add2(jx, d);
+      if constexpr (cx < 0) jx = sub2(jx, d);
+      if constexpr (cy > 0) jy = add2(jy, d);
+      if constexpr (cy < 0) jy = sub2(jy, d);
+      if constexpr (cz > 0) jz = add2(jz, d);
+      if constexpr (cz < 0) jz = sub2(jz, d);
+      if constexpr (cx != 0) sxx = add2(sxx, s);
+      if constexpr (cy != 0) syy = add2(syy, s);
+      if constexpr (cz != 0) szz = add2(szz, s);
+      if constexpr (cx * cy > 0) sxy = add2(sxy, s);
+      if constexpr (cx * cy < 0) sxy = sub2(sxy, s);
+      if constexpr (cx * cz > 0) sxz = add2(sxz, s);
+      if constexpr (cx * cz < 0) sxz = sub2(sxz, s);
+      if constexpr (cy * cz > 0) syz = add2(syz, s);
+      if constexpr (cy * cz < 0) syz = sub2(syz, s);
+    }
+  });
+  const float2 rho = add2(f2(1.0f), drho);
+  const float2 irho = make_float2(__fdividef(1.0f, rho.x), __fdividef(1.0f, rho.y));
+  const float2 ux = mul2(jx, irho), uy = mul2(jy, irho), uz = D3 ? mul2(jz, irho) : f2(0.f);
+  const float2 nux = mul2(ux, f2(-1.f)), nuy = mul2(uy, f2(-1.f)), nuz = mul2(uz, f2(-1.f));
+  const float2 d3 = mul2(drho, f2(1.0f / 3.0f));
+  const float2 pxx = fma2(jx, nux, sub2(sxx, d3));
+  const float2 pyy = fma2(jy, nuy, sub2(syy, d3));
+  const float2 pxy = fma2(jx, nuy, sxy);
+  float2 pzz = f2(0.f), pxz = f2(0.f), pyz = f2(0.f);
+  if constexpr (D3) {
+    pzz = fma2(jz, nuz, sub2(szz, d3));
+    pxz = fma2(jx, nuz, sxz);
+    pyz = fma2(jy, nuz, syz);
+  }
+  float2 omega, k1;
+  if (P.csmag2 > 0.0f || P.sponge_start < (float)P.nx) {
+    float2 pn = fma2(pxx, pxx, fma2(pyy, pyy, mul2(f2(2.f), mul2(pxy, pxy))));
+    if constexpr (D3) pn = fma2(pzz, pzz, fma2(f2(2.f), fma2(pxz, pxz, mul2(pyz, pyz)), pn));
+    relax_cell(P, (float)x, pn.x, irho.x, omega.x);
+    relax_cell(P, (float)(x + 1), pn.y, irho.y, omega.y);
+  } else {
+    const float om = 1.0f - __fdividef(1.0f, P.tau0);
+    omega = f2(om);
+  }
+  k1 = mul2(f2(4.5f), omega);
+  const float2 trP = mul2(add2(add2(pxx, pyy), pzz), f2(1.0f / 3.0f));
+  // Q_i : Pi - trP for axis directions (Daa) and for two-component directions (Eab +- 2 Pab)
+  const float2 Dxx = sub2(pxx, trP), Dyy = sub2(pyy, trP), Dzz = sub2(pzz, trP);
+  const float2 Exy = add2(Dxx, pyy), Exz = add2(Dxx, pzz), Eyz = add2(Dyy, pzz);
+  const float2 ju = fma2(jx, ux, fma2(jy, uy, mul2(jz, uz)));
+  const float2 base = fma2(f2(-1.5f), ju, drho);
+  const bool bgk = P.collision == 1u;
+  const float2 a = sub2(f2(1.0f), omega);
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    constexpr int io = opp<L>(i);
+    if constexpr (i == 0 || i < io) {
+      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+      constexpr int nc = (cx != 0) + (cy != 0) + (cz != 0);
+      constexpr float w = (float)Wc<L, i>::v;
+      float2 cj = f2(0.f), cu = f2(0.f), qp;
+      if constexpr (nc == 0) {
+        qp = mul2(trP, f2(-1.f));
+      } else if constexpr (nc == 1) {
+        cj = cx > 0 ? jx : (cx < 0 ? mul2(jx, f2(-1.f)) : cy > 0 ? jy : (cy < 0 ? mul2(jy, f2(-1.f)) : cz > 0 ? jz : mul2(jz, f2(-1.f))));
+        cu = cx > 0 ? ux : (cx < 0 ? nux : cy > 0 ? uy : (cy < 0 ? nuy : cz > 0 ? uz : nuz));
+        qp = cx != 0 ? Dxx : (cy != 0 ? Dyy : Dzz);
+      } else {
+        // two non-zero components (a, b) with signs (sa, sb)
+        constexpr int ax = cx != 0 ? 0 : 1;
+        constexpr int bx = cz != 0 ? 2 : 1;
+        constexpr int sa = ax == 0 ? cx : cy;
+        constexpr int sb = bx == 2 ? cz : cy;
+        const float2 ja = ax == 0 ? jx : jy, jb = bx == 2 ? jz : jy;
+        const float2 ua = ax == 0 ? ux : uy, ub = bx == 2 ? uz : uy;
+        cj = sa > 0 ? (sb > 0 ? add2(ja, jb) : sub2(ja, jb)) : (sb > 0 ? sub2(jb, ja) : mul2(add2(ja, jb), f2(-1.f)));
+        cu = sa > 0 ? (sb > 0 ? add2(ua, ub) : sub2(ua, ub)) : (sb > 0 ? sub2(ub, ua) : mul2(add2(ua, ub), f2(-1.f)));
+        const float2 E = ax == 0 ? (bx == 1 ? Exy : Exz) : Eyz;
+        const float2 Pab = ax == 0 ? (bx == 1 ? pxy : pxz) : pyz;
+        qp = fma2(f2((float)(2 * sa * sb)), Pab, E);
+      }
+      const float2 e = fma2(mul2(f2(4.5f), cj), cu, base);  // even part of (feq - w) / w
+      if (!bgk) {
+        const float2 wt = mul2(f2(w), fma2(k1, qp, e));
+        o[i] = fma2(f2(3.0f * w), cj, wt);
+        if constexpr (i > 0) o[io] = fma2(f2(-3.0f * w), cj, wt);
+      } else {
+        const float2 we = mul2(f2(w), e);
+        o[i] = fma2(a, fma2(f2(3.0f * w), cj, we), mul2(omega, h[i]));
+        if constexpr (i > 0) o[io] = fma2(a, fma2(f2(-3.0f * w), cj, we), mul2(omega, h[io]));
+      }
+    }
+  });
+  // inlet absorbing layer: blend towards the free-stream equilibrium (wgslLbm.ts:224-237)
+  if (P.sponge_in > 0.0f && (float)x < P.sponge_in) {
+    float2 sIn;
+    const float inv = __fdividef(1.0f, fmaxf(P.sponge_in, 1.0f));
+    const float s0 = fminf(fmaxf(1.0f - (float)x * inv, 0.0f), 1.0f);
+    const float s1 = fminf(fmaxf(1.0f - (float)(x + 1) * inv, 0.0f), 1.0f);
+    sIn = make_float2(0.08f * s0 * s0, 0.08f * s1 * s1);
+    const float2 keep = sub2(f2(1.0f), sIn);
+    const float U = P.uin;
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      constexpr int cx = L::c[i][0];
+      constexpr float w = (float)Wc<L, i>::v;
+      const float eqw = w * ((float)(3 * cx) * U + (float)(4.5 * cx * cx) * U * U - 1.5f * U * U);
+      o[i] = fma2(o[i], keep, mul2(f2(eqw), sIn));
+    });
+  }
+}
+
+// two-cell loads / stores of shifted populations: elements (o, o + 1), o even
+template <class S> struct PairIO;
+template <> struct PairIO<StF16> {
+  __device__ __forceinline__ static float2 ld(const __half* __restrict__ p, uint32_t o, float /*w*/) {
+    const uint32_t u = __ldg(reinterpret_cast<const unsigned int*>(p + o));
+    return __half22float2(*reinterpret_cast<const __half2*>(&u));
+  }
+  __device__ __forceinline__ static void st(__half* __restrict__ p, uint32_t o, float2 v, float /*w*/) {
+    *reinterpret_cast<__half2*>(p + o) = __float22half2_rn(v);
+  }
+};
+template <> struct PairIO<StF32> {
+  __device__ __forceinline__ static float2 ld(const float* __restrict__ p, uint32_t o, float w) {
+    const float2 f = __ldg(reinterpret_cast<const float2*>(p + o));
+    return make_float2(f.x - w, f.y - w);
+  }
+  __device__ __forceinline__ static void st(float* __restrict__ p, uint32_t o, float2 v, float w) {
+    *reinterpret_cast<float2*>(p + o) = make_float2(v.x + w, v.y + w);
+  }
+};
+
 template <class L, class S, int V>
 __global__ void __launch_bounds__(256) k_stream_collide_v(const __grid_constant__ wt_kparams P,
                                                           const typename S::T* __restrict__ fin,
@@ -582,6 +752,7 @@ __global__ void __launch_bounds__(256) k_stream_collide_v(const __grid_constant_
                                                           const __grid_constant__ Wheels W) {
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
+  constexpr int G = V / 2;  // groups of two cells collided together in f32x2 lanes
   const int NX = P.nx, NY = P.ny, NZ = P.nz;
   const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -594,33 +765,34 @@ __global__ void __launch_bounds__(256) k_stream_collide_v(const __grid_constant_
   if constexpr (V == 2) cv = __ldg(reinterpret_cast<const unsigned short*>(cls + idx0));
   else cv = __ldg(reinterpret_cast<const unsigned int*>(cls + idx0));
   const bool fast = cv == 0u && iy > 0 && iy < NY - 1 && (!D3 || (iz > 0 && iz < NZ - 1));
-  float o[Q][V];
+  float2 o[G][Q];
   if (fast) {
-    float h[Q][V];
+    float2 h[G][Q];
     static_for<Q>([&](auto I) {
       constexpr int i = I;
       constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
       constexpr float w = (float)Wc<L, i>::v;
       // source row of direction i (bulk cells: y - cy and z - cz are inside the domain)
       const uint32_t src = i * N + idx0 - (uint32_t)(cy * (int)sy) - (uint32_t)(cz * (int)sz);
-      float cur[V];
-      VecIO<S, V>::ld(fin, src, cur, w);
+      float2 cur[G];
+#pragma unroll
+      for (int g = 0; g < G; g++) cur[g] = PairIO<S>::ld(fin, src + 2 * g, w);
       if constexpr (cx == 0) {
 #pragma unroll
-        for (int v = 0; v < V; v++) h[i][v] = cur[v];
+        for (int g = 0; g < G; g++) h[g][i] = cur[g];
       } else if constexpr (cx > 0) {
-        // pull from x - 1: the last element of the previous run, then cur shifted by one
+        // pull from x - 1: the last element of the previous run, then the run shifted by one
         const float prev = ld_shift(fin, x0 > 0 ? src - 1u : src, w);
-        h[i][0] = prev;
+        h[0][i] = make_float2(prev, cur[0].x);
 #pragma unroll
-        for (int v = 1; v < V; v++) h[i][v] = cur[v - 1];
+        for (int g = 1; g < G; g++) h[g][i] = make_float2(cur[g - 1].y, cur[g].x);
       } else {
         // pull from x + 1, clamped to the outlet column (zero gradient)
         const bool last = x0 + V >= NX;
         const float next = ld_shift(fin, last ? src + (V - 1) : src + V, w);
 #pragma unroll
-        for (int v = 0; v < V - 1; v++) h[i][v] = cur[v + 1];
-        h[i][V - 1] = next;
+        for (int g = 0; g < G - 1; g++) h[g][i] = make_float2(cur[g].y, cur[g + 1].x);
+        h[G - 1][i] = make_float2(cur[G - 1].y, next);
       }
     });
     if (x0 == 0) {
@@ -631,42 +803,39 @@ __global__ void __launch_bounds__(256) k_stream_collide_v(const __grid_constant_
         constexpr int cx = L::c[i][0];
         if constexpr (cx > 0) {
           constexpr float w = (float)Wc<L, i>::v;
-          h[i][0] = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
+          h[0][i].x = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
         }
       });
     }
 #pragma unroll
-    for (int v = 0; v < V; v++) {
-      float hv[Q], ov[Q];
-#pragma unroll
-      for (int i = 0; i < Q; i++) hv[i] = h[i][v];
-      collide_shifted<L>(P, hv, x0 + v, ov);
-#pragma unroll
-      for (int i = 0; i < Q; i++) o[i][v] = ov[i];
-    }
+    for (int g = 0; g < G; g++) collide_shifted2<L>(P, h[g], x0 + 2 * g, o[g]);
   } else {
-#pragma unroll 1
+#pragma unroll
     for (int v = 0; v < V; v++) {
+      float ov[Q];
       if ((cv >> (8 * v)) & CLS_SOLID) {
 #pragma unroll
-        for (int i = 0; i < Q; i++) o[i][v] = 0.0f;  // solids hold f = w
+        for (int i = 0; i < Q; i++) ov[i] = 0.0f;  // solids hold f = w
       } else {
         float fo[Q];
         cell_general<L, S>(P, fin, flags, sdf, W, x0 + v, iy, iz, fo);
         static_for<Q>([&](auto I) {
           constexpr int i = I;
-          o[i][v] = fo[i] - (float)Wc<L, i>::v;
+          ov[i] = fo[i] - (float)Wc<L, i>::v;
         });
+      }
+#pragma unroll
+      for (int i = 0; i < Q; i++) {
+        if (v & 1) o[v / 2][i].y = ov[i];
+        else o[v / 2][i].x = ov[i];
       }
     }
   }
   static_for<Q>([&](auto I) {
     constexpr int i = I;
     constexpr float w = (float)Wc<L, i>::v;
-    float ov[V];
 #pragma unroll
-    for (int v = 0; v < V; v++) ov[v] = o[i][v];
-    VecIO<S, V>::st(fout, i * N + idx0, ov, w);
+    for (int g = 0; g < G; g++) PairIO<S>::st(fout, i * N + idx0 + 2 * g, o[g][i], w);
   });
 }
 
