@@ -226,10 +226,12 @@ __device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L
 // patches, specular or periodic sides, Bouzidi walls, rotating wheels with their mass fix;
 // wgslLbm.ts:138-175, 276-291). Kept out of line: it runs only for cells next to walls and
 // domain faces, and must not inflate the register budget of the bulk path.
+// `near` = the cell's class byte says some in-domain pull source is solid; without it the
+// solid checks (and their dependent loads) are skipped, which keeps the face rows cheap.
 template <class L, class S>
 __device__ __noinline__ void cell_general(const wt_kparams& P, const typename S::T* __restrict__ fin,
                                           const uint32_t* __restrict__ flags, const uint32_t* __restrict__ sdf,
-                                          const Wheels& W, int ix, int iy, int iz, typename S::R* out) {
+                                          const Wheels& W, int ix, int iy, int iz, bool near, typename S::R* out) {
   typedef typename S::R R;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
@@ -294,7 +296,7 @@ __device__ __noinline__ void cell_general(const wt_kparams& P, const typename S:
           }
         } else {
           const size_t sc = cell_id(sxc, sy, sz, NX, NY);
-          const uint32_t fs = flags[sc];
+          const uint32_t fs = near ? flags[sc] : 0u;
           if (fs != 0u) {
             // interpolated bounce-back (Bouzidi)
             wall = true;
@@ -399,7 +401,7 @@ __global__ void __launch_bounds__(256) k_stream_collide(const __grid_constant__ 
     });
     collide_full<L, R>(P, f, ix, false, false, fo);
   } else {
-    cell_general<L, S>(P, fin, flags, sdf, W, ix, iy, iz, fo);
+    cell_general<L, S>(P, fin, flags, sdf, W, ix, iy, iz, (cl & CLS_NEAR_SOLID) != 0, fo);
   }
   static_for<Q>([&](auto I) {
     constexpr int i = I;
@@ -818,7 +820,7 @@ __global__ void __launch_bounds__(256) k_stream_collide_v(const __grid_constant_
         for (int i = 0; i < Q; i++) ov[i] = 0.0f;  // solids hold f = w
       } else {
         float fo[Q];
-        cell_general<L, S>(P, fin, flags, sdf, W, x0 + v, iy, iz, fo);
+        cell_general<L, S>(P, fin, flags, sdf, W, x0 + v, iy, iz, ((cv >> (8 * v)) & CLS_NEAR_SOLID) != 0, fo);
         static_for<Q>([&](auto I) {
           constexpr int i = I;
           ov[i] = fo[i] - (float)Wc<L, i>::v;
@@ -992,7 +994,7 @@ __global__ void __launch_bounds__(512) k_stream_collide_tma(const __grid_constan
         for (int i = 0; i < Q; i++) o[i] = 0.0f;
       } else {
         float fo[Q];
-        cell_general<L, S>(P, fin, flags, sdf, W, x, iy, iz, fo);
+        cell_general<L, S>(P, fin, flags, sdf, W, x, iy, iz, (cl & CLS_NEAR_SOLID) != 0, fo);
         static_for<Q>([&](auto I) {
           constexpr int i = I;
           o[i] = fo[i] - (float)Wc<L, i>::v;
