@@ -45,15 +45,16 @@ def _as_float(a):
 
 
 # (kernel, param, bx, by): register-fed kernel with 1 / 2 / 4 cells per thread, TMA-staged kernel
-# with 2 / 3 / 4 stages (bx = 32 makes rows longer than the CTA loop over x)
-LAUNCHES = {"reg1": (0, 1, 0, 0), "reg2": (0, 2, 32, 4), "reg4": (0, 4, 32, 4), "tma2": (1, 2, 32, 0),
-            "tma3": (1, 3, 0, 0), "tma4": (1, 4, 32, 0)}
+# with 2 / 3 / 4 stages and 1 / default / 2 consumer warps (one consumer warp covers 64 cells per
+# pass, so the 160-wide grid loops over its rows)
+LAUNCHES = {"reg1": (0, 1, 0, 0), "reg2": (0, 2, 32, 4), "reg4": (0, 4, 32, 4), "tma2": (1, 2, 64, 0),
+            "tma3": (1, 3, 0, 0), "tma4": (1, 4, 96, 0)}
 CASES = [(p, k) for p in ("f32", "f16") for k in LAUNCHES] + [("f64", "reg1")]
 
 
 @pytest.mark.parametrize("prec,launch", CASES)
 @pytest.mark.parametrize("pset", list(PARAM_SETS))
-@pytest.mark.parametrize("dims", [(24, 14, 12), (40, 16, 1)])
+@pytest.mark.parametrize("dims", [(32, 14, 12), (48, 16, 1), (160, 12, 1)])
 def test_stream_collide_matches_oracle(gpu, oracle, dims, pset, prec, launch):
     params = dict(PARAM_SETS[pset], precision=prec)
     g, o, flags = _pair(oracle, dims, params)

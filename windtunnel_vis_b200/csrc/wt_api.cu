@@ -564,8 +564,8 @@ int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32
         ((bx == 0) != (by == 0)))
       return fail(s, WT_E_INVALID, "wt_set_launch: register-fed kernel needs v in {1,2,4}, bx % 32 == 0, bx*by <= 1024");
   } else if (kernel == 1) {
-    if (param < 2 || param > 4 || bx < 0 || bx > 512 || (bx % 32) != 0)
-      return fail(s, WT_E_INVALID, "wt_set_launch: TMA-staged kernel needs 2..4 stages and bx % 32 == 0, bx <= 512");
+    if (param < 2 || param > 4 || bx < 0 || bx == 32 || bx > 544 || (bx % 32) != 0)
+      return fail(s, WT_E_INVALID, "wt_set_launch: TMA-staged kernel needs 2..4 stages and bx = 0 or 64..544, bx % 32 == 0");
     if (!wt::sc_tma_ok(s, param))
       return fail(s, WT_E_UNSUPPORTED, "wt_set_launch: TMA-staged kernel needs f16 (nx % 8 == 0) or f32 (nx % 4 == 0) and a row that fits in shared memory");
   } else {
@@ -602,9 +602,9 @@ int wt_autotune(wt_solver* s, int32_t iters, int32_t* out4) {
   }
   for (int st : {2, 3, 4}) {
     if (!wt::sc_tma_ok(s, st)) continue;
-    for (int bx : {128, 256, 384, 512}) {
-      if (bx > ((s->dims.nx + 31) / 32) * 32 + 31) continue;
-      cands.push_back({1, st, bx, 0});
+    for (int cw : {2, 4, 8}) {  // consumer warps (+1 producer warp)
+      if (cw > 1 && 64 * (cw / 2) >= s->dims.nx) continue;
+      cands.push_back({1, st, 32 * (cw + 1), 0});
     }
   }
   cands.push_back({0, 1, 0, 0});
