@@ -237,12 +237,10 @@ def run_ours(args, rank, world, local_rank, dist):
         "config": {"workload": WORKLOAD, "grid": list(DIMS), "storage": "f16 shifted (f - w)",
                    "bench_step": f"{CHUNK} lattice updates + macro/force pass + stats readback",
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2: 2 x 159 MB population buffers",
-                   "launch": {"kernel": ["register-fed", "tma-staged"][shape[0]],
-                              "param": shape[1], "block": [shape[2], shape[3]]}},
+                   "launch": {"cells_per_thread": shape[1], "block": [shape[2], shape[3]]}},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": ("k_stream_collide_tma<D3Q19,StF16>" if shape[0] == 1 else
-                                "k_stream_collide_v<D3Q19,StF16>" if shape[1] > 1 else "k_stream_collide<D3Q19,StF16>"), "bytes_per_launch_alg": n * BYTES_PER_UPDATE,
+                     "kernel": "k_stream_collide_v<D3Q19,StF16>" if shape[1] > 1 else "k_stream_collide<D3Q19,StF16>", "bytes_per_launch_alg": n * BYTES_PER_UPDATE,
                      "launch_ms": round(sc_ms, 5)},
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e, 1), "unit": "MLUPS", "h2d_bytes_per_step": n * 8,

@@ -219,15 +219,12 @@ int wt_write_tracers(wt_solver* s, const float* state4, int64_t count, const flo
                      int64_t hist_len, uint32_t trail);
 
 /* ---- launch selection (extension; no counterpart in the reference) ------------------------ */
-/* Selects the stream-collide kernel. kernel 0: register-fed, `param` cells per thread along x
- * (1, 2 or 4; 2 and 4 need f16/f32 storage and nx % param == 0, otherwise the scalar kernel
- * runs), block bx x by threads (0, 0 = default). kernel 1: TMA-staged persistent kernel with
- * `param` pipeline stages (2..4) and bx threads per CTA: one producer warp plus bx/32 - 1
- * consumer warps (0 = default); needs f16 or f32 storage, nx % 16 == 0, and a row of all
- * directions per stage in shared memory. */
+/* Selects the stream-collide launch. kernel must be 0. `param` cells per thread along x (1, 2 or
+ * 4; 2 and 4 need f16/f32 storage and nx % param == 0, otherwise the scalar kernel runs), block
+ * bx x by threads (0, 0 = default). */
 int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32_t by);
 int wt_get_launch(const wt_solver* s, int32_t* out4);
-/* The project's launch tuner: times every applicable candidate of both kernels on this handle's
+/* The project's launch tuner: times every applicable launch candidate on this handle's
  * grid (iters launches each, reading the current populations and writing the other buffer, so
  * the state does not change) and keeps the fastest. out4 (may be NULL) receives
  * {kernel, param, bx, by}. */

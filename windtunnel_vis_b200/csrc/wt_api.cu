@@ -563,13 +563,8 @@ int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32
     if (!(param == 1 || param == 2 || param == 4) || bx < 0 || by < 0 || bx * by > 1024 || (bx % 32) != 0 ||
         ((bx == 0) != (by == 0)))
       return fail(s, WT_E_INVALID, "wt_set_launch: register-fed kernel needs v in {1,2,4}, bx % 32 == 0, bx*by <= 1024");
-  } else if (kernel == 1) {
-    if (param < 2 || param > 4 || bx < 0 || bx == 32 || bx > 544 || (bx % 32) != 0)
-      return fail(s, WT_E_INVALID, "wt_set_launch: TMA-staged kernel needs 2..4 stages and bx = 0 or 64..544, bx % 32 == 0");
-    if (!wt::sc_tma_ok(s, param))
-      return fail(s, WT_E_UNSUPPORTED, "wt_set_launch: TMA-staged kernel needs f16 (nx % 8 == 0) or f32 (nx % 4 == 0) and a row that fits in shared memory");
   } else {
-    return fail(s, WT_E_INVALID, "wt_set_launch: kernel must be 0 (register-fed) or 1 (TMA-staged)");
+    return fail(s, WT_E_INVALID, "wt_set_launch: kernel must be 0 (register-fed)");
   }
   s->sc_kernel = kernel;
   s->sc_param = param;
@@ -598,13 +593,6 @@ int wt_autotune(wt_solver* s, int32_t iters, int32_t* out4) {
         if (threads % bx) continue;
         cands.push_back({0, v, bx, threads / bx});
       }
-    }
-  }
-  for (int st : {2, 3, 4}) {
-    if (!wt::sc_tma_ok(s, st)) continue;
-    for (int cw : {2, 4, 8}) {  // consumer warps (+1 producer warp)
-      if (cw > 1 && 64 * (cw / 2) >= s->dims.nx) continue;
-      cands.push_back({1, st, 32 * (cw + 1), 0});
     }
   }
   cands.push_back({0, 1, 0, 0});

@@ -40,12 +40,10 @@ struct wt_solver {
   float4* tr_state = nullptr;
   float4* tr_hist = nullptr;
   uint32_t tr_count = 0, tr_trail = 0;
-  // stream-collide launch (chosen per lattice by the tuner, see wt_lbm.cu): sc_kernel 0 =
-  // register-fed kernel with sc_param cells per thread along x (1 = scalar), block sc_bx x sc_by
-  // (0 = default); sc_kernel 1 = TMA-staged persistent kernel with sc_param pipeline stages and
-  // sc_bx threads per CTA (0 = default)
+  // stream-collide launch (chosen per lattice by the tuner, see wt_lbm.cu): sc_param cells per
+  // thread along x (1 = scalar kernel), block sc_bx x sc_by of the vectorised kernel (0 = default)
   int block_x = 0;
-  int sc_kernel = 1, sc_param = 3, sc_bx = 0, sc_by = 0;
+  int sc_kernel = 0, sc_param = 2, sc_bx = 0, sc_by = 0;
   int* err_dev = nullptr;   // device-side error word written by kernels with bounded waits
   int* err_host = nullptr;  // pinned copy
   int64_t launches = 0;
@@ -58,7 +56,6 @@ int lbm_block_x(const wt_solver* s);
 cudaError_t launch_classify(wt_solver* s);
 cudaError_t launch_init(wt_solver* s);
 cudaError_t launch_stream_collide(wt_solver* s, const void* fin, void* fout);
-bool sc_tma_ok(const wt_solver* s, int stages);
 cudaError_t launch_macro(wt_solver* s);
 
 // voxelizer (wt_voxel.cu). Scratch buffers hits (3n i32), vote (n u32), info (8 u32) are

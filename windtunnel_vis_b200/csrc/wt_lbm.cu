@@ -841,235 +841,6 @@ __global__ void __launch_bounds__(256) k_stream_collide_v(const __grid_constant_
   });
 }
 
-// ---- TMA-staged persistent kernel (warp-specialised) ----------------------------------------
-//
-// The memory-level parallelism of the register-fed kernels is capped by their register budget.
-// Here warp 0 of each CTA is a producer: one lane streams, for each (y, z) row the CTA owns,
-// one 1-D bulk copy per direction (cp.async.bulk, completion counted on the stage's `full`
-// mbarrier) of the whole source row (y - c_y, z - c_z), plus the row's class bytes, into a ring
-// of STAGES shared-memory stages. The other warps are consumers: they collide two cells per
-// thread in f32x2 lanes straight out of shared memory (the x shift of the pull is an index
-// offset), store to global memory, and release the stage with an arrive on its `empty`
-// mbarrier. No CTA-wide barrier is involved, so a slow row only delays the reuse of its own
-// stage. Rows on the domain faces and cells next to a solid take the reference-exact per-cell
-// path from global memory. Every wait is bounded (about 2 s of SM clock): on timeout the kernel
-// records an error code in `err`, the producer drains its copies (bounded) and all warps return.
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded wait: gives up after ~2 s of SM clock (returns false)
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity))
-    if (clock64() - t0 > 4000000000ll) return false;
-  return true;
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(bar))
-               : "memory");
-}
-
-constexpr int WT_ERR_PIPELINE_TIMEOUT = 1;
-
-template <class S>
-__device__ __forceinline__ float sm_shift(const typename S::T* p, int k, float w);
-template <>
-__device__ __forceinline__ float sm_shift<StF16>(const __half* p, int k, float /*w*/) {
-  return __half2float(p[k]);
-}
-template <>
-__device__ __forceinline__ float sm_shift<StF32>(const float* p, int k, float w) {
-  return p[k] - w;
-}
-template <class S>
-__device__ __forceinline__ float2 sm_pair(const typename S::T* p, int k, float w);  // k even
-template <>
-__device__ __forceinline__ float2 sm_pair<StF16>(const __half* p, int k, float /*w*/) {
-  return __half22float2(*reinterpret_cast<const __half2*>(p + k));
-}
-template <>
-__device__ __forceinline__ float2 sm_pair<StF32>(const float* p, int k, float w) {
-  const float2 f = *reinterpret_cast<const float2*>(p + k);
-  return make_float2(f.x - w, f.y - w);
-}
-
-// bytes of one pipeline stage: Q rows of populations + the row's class bytes (16-byte padded)
-template <class L, class S>
-__host__ __device__ __forceinline__ size_t tma_stage_bytes(int nx) {
-  return (size_t)L::Q * nx * sizeof(typename S::T) + (((size_t)nx + 15) & ~(size_t)15);
-}
-
-template <class L, class S, int STAGES>
-__global__ void __launch_bounds__(544) k_stream_collide_tma(const __grid_constant__ wt_kparams P,
-                                                            const typename S::T* __restrict__ fin,
-                                                            typename S::T* __restrict__ fout,
-                                                            const uint8_t* __restrict__ cls,
-                                                            const uint32_t* __restrict__ flags,
-                                                            const uint32_t* __restrict__ sdf,
-                                                            const __grid_constant__ Wheels W, int* __restrict__ err) {
-  typedef typename S::T T;
-  constexpr int Q = L::Q;
-  constexpr bool D3 = L::DIM == 3;
-  extern __shared__ __align__(128) unsigned char smem[];
-  const int NX = P.nx, NY = P.ny, NZ = P.nz;
-  const uint32_t N = P.n;
-  const uint32_t rows = (uint32_t)NY * (uint32_t)NZ;
-  const size_t stage_bytes = tma_stage_bytes<L, S>(NX);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * stage_bytes);
-  uint64_t* empty = full + STAGES;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int consumers = (int)(blockDim.x >> 5) - 1;
-  const uint32_t row_bytes = (uint32_t)NX * (uint32_t)sizeof(T);
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; s++) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], (uint32_t)consumers);
-    }
-    mbar_fence_init();
-  }
-  __syncthreads();
-  const uint32_t first = blockIdx.x, stride = gridDim.x;
-  const uint32_t ntiles = first < rows ? (rows - first + stride - 1) / stride : 0;
-
-  if (warp == 0) {
-    // ---------------- producer ----------------
-    if (lane == 0) {
-      uint32_t issued = 0;
-      bool ok = true;
-      for (uint32_t k = 0; k < ntiles && ok; k++) {
-        const int s = (int)(k % STAGES);
-        if (k >= (uint32_t)STAGES) ok = mbar_wait_bounded(&empty[s], (k / STAGES - 1) & 1u);
-        if (!ok) break;
-        const uint32_t r = first + k * stride;
-        const int y = (int)(r % (uint32_t)NY), z = (int)(r / (uint32_t)NY);
-        unsigned char* st = smem + s * stage_bytes;
-        fence_proxy_async();
-        mbar_expect_tx(&full[s], (uint32_t)Q * row_bytes + (uint32_t)NX);
-        static_for<Q>([&](auto I) {
-          constexpr int i = I;
-          constexpr int cy = L::c[i][1], cz = L::c[i][2];
-          const int sy = min(max(y - cy, 0), NY - 1);
-          const int sz = D3 ? min(max(z - cz, 0), NZ - 1) : 0;
-          const T* src = fin + (size_t)i * N + ((size_t)sy + (size_t)NY * (size_t)sz) * (size_t)NX;
-          bulk_g2s(st + (size_t)i * row_bytes, src, row_bytes, &full[s]);
-        });
-        bulk_g2s(st + (size_t)Q * row_bytes, cls + (size_t)r * NX, (uint32_t)NX, &full[s]);
-        issued = k + 1;
-      }
-      if (!ok) {
-        atomicExch(err, WT_ERR_PIPELINE_TIMEOUT);
-        // drain copies still in flight (bounded)
-        for (uint32_t j = issued > (uint32_t)STAGES ? issued - STAGES : 0; j < issued; j++)
-          mbar_wait_bounded(&full[j % STAGES], (j / STAGES) & 1u);
-      }
-    }
-    return;
-  }
-
-  // ---------------- consumers ----------------
-  const int t = threadIdx.x - 32;
-  const int T2 = 64 * consumers;  // cells per pass of all consumer threads
-  const float U = P.uin;
-  for (uint32_t k = 0; k < ntiles; k++) {
-    const int s = (int)(k % STAGES);
-    if (!mbar_wait_bounded(&full[s], (k / STAGES) & 1u)) {
-      if (lane == 0) atomicExch(err, WT_ERR_PIPELINE_TIMEOUT);
-      return;
-    }
-    const uint32_t r = first + k * stride;
-    const int iy = (int)(r % (uint32_t)NY), iz = (int)(r / (uint32_t)NY);
-    const uint32_t rowbase = r * (uint32_t)NX;
-    const bool face = iy == 0 || iy == NY - 1 || (D3 && (iz == 0 || iz == NZ - 1));
-    const T* st = reinterpret_cast<const T*>(smem + s * stage_bytes);
-    const uint8_t* scls = smem + s * stage_bytes + (size_t)Q * row_bytes;
-    for (int x0 = 2 * t; x0 < NX; x0 += T2) {
-      const uint32_t idx0 = rowbase + (uint32_t)x0;
-      const uint32_t cv = *reinterpret_cast<const unsigned short*>(scls + x0);
-      float2 o[Q];
-      if (cv == 0u && !face) {
-        float2 h[Q];
-        static_for<Q>([&](auto I) {
-          constexpr int i = I;
-          constexpr int cx = L::c[i][0];
-          constexpr float w = (float)Wc<L, i>::v;
-          const T* row = st + i * NX;
-          if constexpr (cx == 0) {
-            h[i] = sm_pair<S>(row, x0, w);
-          } else if constexpr (cx > 0) {
-            h[i] = make_float2(sm_shift<S>(row, max(x0 - 1, 0), w), sm_shift<S>(row, x0, w));
-          } else {
-            h[i] = make_float2(sm_shift<S>(row, x0 + 1, w), sm_shift<S>(row, min(x0 + 2, NX - 1), w));
-          }
-        });
-        if (x0 == 0) {
-          // inlet column: populations entering from x < 0 are the free-stream equilibrium
-          static_for<Q>([&](auto I) {
-            constexpr int i = I;
-            constexpr int cx = L::c[i][0];
-            if constexpr (cx > 0) {
-              constexpr float w = (float)Wc<L, i>::v;
-              h[i].x = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
-            }
-          });
-        }
-        collide_shifted2<L>(P, h, x0, o);
-      } else {
-#pragma unroll
-        for (int v = 0; v < 2; v++) {
-          const uint32_t cb = (cv >> (8 * v)) & 0xffu;
-          float ov[Q];
-          if (cb & CLS_SOLID) {
-#pragma unroll
-            for (int i = 0; i < Q; i++) ov[i] = 0.0f;  // solids hold f = w
-          } else {
-            float fo[Q];
-            cell_general<L, S>(P, fin, flags, sdf, W, x0 + v, iy, iz, (cb & CLS_NEAR_SOLID) != 0, fo);
-            static_for<Q>([&](auto I) {
-              constexpr int i = I;
-              ov[i] = fo[i] - (float)Wc<L, i>::v;
-            });
-          }
-#pragma unroll
-          for (int i = 0; i < Q; i++) {
-            if (v) o[i].y = ov[i];
-            else o[i].x = ov[i];
-          }
-        }
-      }
-      static_for<Q>([&](auto I) {
-        constexpr int i = I;
-        PairIO<S>::st(fout, i * N + idx0, o[i], (float)Wc<L, i>::v);
-      });
-    }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s]);
-  }
-}
-
 // ---------------------------------------------------------------------------------------------
 // macro pass: velocity field, EMA statistics, momentum-exchange force, partial reductions
 // ---------------------------------------------------------------------------------------------
@@ -1321,61 +1092,17 @@ static cudaError_t init_t(wt_solver* s) {
   return cudaGetLastError();
 }
 
-template <class L, class S, int STAGES>
-static cudaError_t sc_tma_launch(wt_solver* s, const void* fin, void* fout, int threads) {
-  typedef typename S::T T;
-  auto kern = k_stream_collide_tma<L, S, STAGES>;
-  const size_t smem = STAGES * tma_stage_bytes<L, S>(s->dims.nx) + 16 * STAGES;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  int per_sm = 0, sms = 0, dev = 0;
-  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem)) != cudaSuccess) return e;
-  if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  const uint32_t rows = (uint32_t)s->dims.ny * (uint32_t)s->dims.nz;
-  const uint32_t grid = (uint32_t)std::min<uint64_t>(rows, (uint64_t)sms * per_sm);
-  kern<<<grid, threads, smem, s->stream>>>(s->kp, (const T*)fin, (T*)fout, s->cls, s->flags, s->sdf, s->wheels,
-                                           s->err_dev);
-  s->launches++;
-  return cudaGetLastError();
-}
-
-// bytes of shared memory the TMA-staged kernel needs for `stages` stages (0 if not applicable)
-size_t sc_tma_smem(const wt_solver* s, int stages) {
-  const int nx = s->dims.nx;
-  if (nx % 16 != 0) return 0;  // 16-byte aligned rows of class bytes and f16 populations
-  if (s->prec == WT_PREC_F16)
-    return stages * (s->is3d ? tma_stage_bytes<D3Q19, StF16>(nx) : tma_stage_bytes<D2Q9, StF16>(nx)) + 16 * stages;
-  if (s->prec == WT_PREC_F32)
-    return stages * (s->is3d ? tma_stage_bytes<D3Q19, StF32>(nx) : tma_stage_bytes<D2Q9, StF32>(nx)) + 16 * stages;
-  return 0;
-}
-
-// the vectorised and TMA-staged kernels index populations with 32-bit element offsets
+// the vectorised kernel indexes populations with 32-bit element offsets
 static bool offsets32(const wt_solver* s) { return (uint64_t)s->q * (uint64_t)s->n < (1ull << 32); }
-
-bool sc_tma_ok(const wt_solver* s, int stages) {
-  const size_t b = sc_tma_smem(s, stages);
-  return stages >= 2 && stages <= 4 && b > 0 && b <= 200 * 1024 && offsets32(s);
-}
 
 template <class L, class S>
 static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
   constexpr bool vec_ok = S::PREC == WT_PREC_F16 || S::PREC == WT_PREC_F32;
   if constexpr (vec_ok) {
-    if (s->sc_kernel == 1 && sc_tma_ok(s, s->sc_param)) {
-      // one producer warp + consumer warps (default: enough for one pass over the row, <= 8)
-      int threads = s->sc_bx;
-      if (threads <= 0) threads = 32 * (1 + std::min(8, std::max(1, (s->dims.nx / 2 + 31) / 32)));
-      if (s->sc_param == 2) return sc_tma_launch<L, S, 2>(s, fin, fout, threads);
-      if (s->sc_param == 3) return sc_tma_launch<L, S, 3>(s, fin, fout, threads);
-      return sc_tma_launch<L, S, 4>(s, fin, fout, threads);
-    }
-    const int V = s->sc_kernel == 0 ? s->sc_param : 2;
+    const int V = s->sc_param;
     if ((V == 2 || V == 4) && s->dims.nx % V == 0 && offsets32(s)) {
       const int runs = s->dims.nx / V;
-      int bx = s->sc_kernel == 0 ? s->sc_bx : 0, by = s->sc_kernel == 0 ? s->sc_by : 0;
+      int bx = s->sc_bx, by = s->sc_by;
       if (bx <= 0 || by <= 0) {
         bx = runs >= 128 ? 128 : ((runs + 31) / 32) * 32;
         by = 256 / bx;
