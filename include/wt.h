@@ -219,9 +219,10 @@ int wt_write_tracers(wt_solver* s, const float* state4, int64_t count, const flo
                      int64_t hist_len, uint32_t trail);
 
 /* ---- launch selection (extension; no counterpart in the reference) ------------------------ */
-/* Selects the stream-collide launch. kernel must be 0. `param` cells per thread along x (1, 2 or
- * 4; 2 and 4 need f16/f32 storage and nx % param == 0, otherwise the scalar kernel runs), block
- * bx x by threads (0, 0 = default). */
+/* Selects the stream-collide launch: `param` cells per thread along x (1, 2 or 4; 2 and 4 need
+ * f16/f32 storage and nx % param == 0, otherwise the scalar kernel runs), block bx x by threads
+ * (bx * by <= 256; 0, 0 = default), and `kernel` = occupancy hint of the vectorised kernel: 0 =
+ * none, 2..4 = registers capped so that many 256-thread CTAs fit on an SM. */
 int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32_t by);
 int wt_get_launch(const wt_solver* s, int32_t* out4);
 /* The project's launch tuner: times every applicable launch candidate on this handle's

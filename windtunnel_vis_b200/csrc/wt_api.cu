@@ -559,13 +559,13 @@ int wt_write_tracers(wt_solver* s, const float* state4, int64_t count, const flo
 
 int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32_t by) {
   if (!s) return WT_E_INVALID;
-  if (kernel == 0) {
-    if (!(param == 1 || param == 2 || param == 4) || bx < 0 || by < 0 || bx * by > 1024 || (bx % 32) != 0 ||
-        ((bx == 0) != (by == 0)))
-      return fail(s, WT_E_INVALID, "wt_set_launch: register-fed kernel needs v in {1,2,4}, bx % 32 == 0, bx*by <= 1024");
-  } else {
-    return fail(s, WT_E_INVALID, "wt_set_launch: kernel must be 0 (register-fed)");
-  }
+  if (!(kernel == 0 || (kernel >= 2 && kernel <= 4)))
+    return fail(s, WT_E_INVALID, "wt_set_launch: occupancy hint must be 0 or 2..4 CTAs per SM");
+  if (kernel == 4 && param == 4)
+    return fail(s, WT_E_INVALID, "wt_set_launch: 4 cells per thread supports occupancy hints 0..3");
+  if (!(param == 1 || param == 2 || param == 4) || bx < 0 || by < 0 || bx * by > 256 || (bx % 32) != 0 ||
+      ((bx == 0) != (by == 0)))
+    return fail(s, WT_E_INVALID, "wt_set_launch: need v in {1,2,4}, bx % 32 == 0, bx*by <= 256");
   s->sc_kernel = kernel;
   s->sc_param = param;
   s->sc_bx = bx;
@@ -587,11 +587,14 @@ int wt_autotune(wt_solver* s, int32_t iters, int32_t* out4) {
   for (int v : {2, 4}) {
     if (!vec || s->dims.nx % v) continue;
     const int runs = s->dims.nx / v;
-    for (int bx : {32, 64, 128, 256}) {
-      if (bx > ((runs + 31) / 32) * 32) continue;
-      for (int threads : {128, 256}) {
-        if (threads % bx) continue;
-        cands.push_back({0, v, bx, threads / bx});
+    for (int mb : {0, 2, 3, 4}) {
+      if (v == 4 && mb == 4) continue;
+      for (int bx : {32, 64, 128, 256}) {
+        if (bx > ((runs + 31) / 32) * 32) continue;
+        for (int threads : {128, 256}) {
+          if (threads % bx) continue;
+          cands.push_back({mb, v, bx, threads / bx});
+        }
       }
     }
   }

@@ -581,18 +581,24 @@ __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // relaxation time of one bulk cell: molecular tau0 + outlet sponge, Smagorinsky closure
 __device__ __forceinline__ void relax_cell(const wt_kparams& P, float fx, float pn, float irho, float& omega) {
   float t0 = P.tau0;
   if (fx > P.sponge_start) {
     const float den = (float)P.nx - P.sponge_start;
-    const float sp = fminf((fx - P.sponge_start) / (den > 1.0f ? den : 1.0f), 1.0f);
+    const float sp = fminf(__fdividef(fx - P.sponge_start, den > 1.0f ? den : 1.0f), 1.0f);
     t0 += 3.0f * P.sponge_nu * sp * sp;
   }
   float tau = t0;
   if (P.csmag2 > 0.0f) {
     const float k = (float)(18.0 * 1.4142135623730951) * P.csmag2;
-    tau = 0.5f * (t0 + sqrtf(t0 * t0 + k * sqrtf(pn) * irho));
+    tau = 0.5f * (t0 + sqrt_approx(t0 * t0 + k * sqrt_approx(pn) * irho));
   }
   omega = 1.0f - __fdividef(1.0f, tau);
 }
@@ -723,35 +729,55 @@ __device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const floa
   }
 }
 
-// two-cell loads / stores of shifted populations: elements (o, o + 1), o even
+// two-cell loads / stores of shifted populations: elements (o, o + 1), o even. Loads are split
+// into a raw fetch and a later conversion so that a thread can put all of its loads in flight
+// before it converts any of them.
 template <class S> struct PairIO;
 template <> struct PairIO<StF16> {
-  __device__ __forceinline__ static float2 ld(const __half* __restrict__ p, uint32_t o, float /*w*/) {
-    const uint32_t u = __ldg(reinterpret_cast<const unsigned int*>(p + o));
+  typedef uint32_t pair_t;
+  typedef unsigned short one_t;
+  __device__ __forceinline__ static pair_t ld(const __half* __restrict__ p, uint32_t o) {
+    return __ldg(reinterpret_cast<const unsigned int*>(p + o));
+  }
+  __device__ __forceinline__ static one_t ld1(const __half* __restrict__ p, uint32_t o) {
+    return __ldg(reinterpret_cast<const unsigned short*>(p + o));
+  }
+  __device__ __forceinline__ static float2 cvt(pair_t u, float /*w*/) {
     return __half22float2(*reinterpret_cast<const __half2*>(&u));
+  }
+  __device__ __forceinline__ static float cvt1(one_t u, float /*w*/) {
+    return __half2float(*reinterpret_cast<const __half*>(&u));
   }
   __device__ __forceinline__ static void st(__half* __restrict__ p, uint32_t o, float2 v, float /*w*/) {
     *reinterpret_cast<__half2*>(p + o) = __float22half2_rn(v);
   }
 };
 template <> struct PairIO<StF32> {
-  __device__ __forceinline__ static float2 ld(const float* __restrict__ p, uint32_t o, float w) {
-    const float2 f = __ldg(reinterpret_cast<const float2*>(p + o));
-    return make_float2(f.x - w, f.y - w);
+  typedef float2 pair_t;
+  typedef float one_t;
+  __device__ __forceinline__ static pair_t ld(const float* __restrict__ p, uint32_t o) {
+    return __ldg(reinterpret_cast<const float2*>(p + o));
   }
+  __device__ __forceinline__ static one_t ld1(const float* __restrict__ p, uint32_t o) { return __ldg(p + o); }
+  __device__ __forceinline__ static float2 cvt(pair_t f, float w) { return make_float2(f.x - w, f.y - w); }
+  __device__ __forceinline__ static float cvt1(one_t f, float w) { return f - w; }
   __device__ __forceinline__ static void st(float* __restrict__ p, uint32_t o, float2 v, float w) {
     *reinterpret_cast<float2*>(p + o) = make_float2(v.x + w, v.y + w);
   }
 };
 
-template <class L, class S, int V>
-__global__ void __launch_bounds__(256) k_stream_collide_v(const __grid_constant__ wt_kparams P,
+// MINB: CTAs of 256 threads the register allocation must leave room for (0 = no constraint)
+template <int MINB> struct Bounds { static constexpr int v = MINB; };
+
+template <class L, class S, int V, int MINB>
+__global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(const __grid_constant__ wt_kparams P,
                                                           const typename S::T* __restrict__ fin,
                                                           typename S::T* __restrict__ fout,
                                                           const uint8_t* __restrict__ cls,
                                                           const uint32_t* __restrict__ flags,
                                                           const uint32_t* __restrict__ sdf,
                                                           const __grid_constant__ Wheels W) {
+  typedef PairIO<S> IO;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
   constexpr int G = V / 2;  // groups of two cells collided together in f32x2 lanes
@@ -769,32 +795,39 @@ __global__ void __launch_bounds__(256) k_stream_collide_v(const __grid_constant_
   const bool fast = cv == 0u && iy > 0 && iy < NY - 1 && (!D3 || (iz > 0 && iz < NZ - 1));
   float2 o[G][Q];
   if (fast) {
-    float2 h[G][Q];
+    // phase 1: every load of the V cells in flight (bulk cells: y - cy, z - cz inside the domain)
+    typename IO::pair_t rp[G][Q];
+    typename IO::one_t r1[Q];
+    const bool last = x0 + V >= NX;
     static_for<Q>([&](auto I) {
       constexpr int i = I;
       constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
-      constexpr float w = (float)Wc<L, i>::v;
-      // source row of direction i (bulk cells: y - cy and z - cz are inside the domain)
       const uint32_t src = i * N + idx0 - (uint32_t)(cy * (int)sy) - (uint32_t)(cz * (int)sz);
+#pragma unroll
+      for (int g = 0; g < G; g++) rp[g][i] = IO::ld(fin, src + 2 * g);
+      if constexpr (cx > 0) r1[i] = IO::ld1(fin, x0 > 0 ? src - 1u : src);          // x - 1
+      if constexpr (cx < 0) r1[i] = IO::ld1(fin, last ? src + (V - 1) : src + V);   // x + 1, outlet clamp
+    });
+    // phase 2: convert and shift into the pulled populations of each cell
+    float2 h[G][Q];
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      constexpr int cx = L::c[i][0];
+      constexpr float w = (float)Wc<L, i>::v;
       float2 cur[G];
 #pragma unroll
-      for (int g = 0; g < G; g++) cur[g] = PairIO<S>::ld(fin, src + 2 * g, w);
+      for (int g = 0; g < G; g++) cur[g] = IO::cvt(rp[g][i], w);
       if constexpr (cx == 0) {
 #pragma unroll
         for (int g = 0; g < G; g++) h[g][i] = cur[g];
       } else if constexpr (cx > 0) {
-        // pull from x - 1: the last element of the previous run, then the run shifted by one
-        const float prev = ld_shift(fin, x0 > 0 ? src - 1u : src, w);
-        h[0][i] = make_float2(prev, cur[0].x);
+        h[0][i] = make_float2(IO::cvt1(r1[i], w), cur[0].x);
 #pragma unroll
         for (int g = 1; g < G; g++) h[g][i] = make_float2(cur[g - 1].y, cur[g].x);
       } else {
-        // pull from x + 1, clamped to the outlet column (zero gradient)
-        const bool last = x0 + V >= NX;
-        const float next = ld_shift(fin, last ? src + (V - 1) : src + V, w);
 #pragma unroll
         for (int g = 0; g < G - 1; g++) h[g][i] = make_float2(cur[g].y, cur[g + 1].x);
-        h[G - 1][i] = make_float2(cur[G - 1].y, next);
+        h[G - 1][i] = make_float2(cur[G - 1].y, IO::cvt1(r1[i], w));
       }
     });
     if (x0 == 0) {
@@ -837,7 +870,7 @@ __global__ void __launch_bounds__(256) k_stream_collide_v(const __grid_constant_
     constexpr int i = I;
     constexpr float w = (float)Wc<L, i>::v;
 #pragma unroll
-    for (int g = 0; g < G; g++) PairIO<S>::st(fout, i * N + idx0 + 2 * g, o[g][i], w);
+    for (int g = 0; g < G; g++) IO::st(fout, i * N + idx0 + 2 * g, o[g][i], w);
   });
 }
 
@@ -1109,14 +1142,21 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
       }
       const dim3 block(bx, by);
       const dim3 grid((runs + bx - 1) / bx, (s->dims.ny + by - 1) / by, s->dims.nz);
-      if (V == 2)
-        k_stream_collide_v<L, S, 2><<<grid, block, 0, s->stream>>>(s->kp, (const typename S::T*)fin,
-                                                                    (typename S::T*)fout, s->cls, s->flags, s->sdf,
-                                                                    s->wheels);
-      else
-        k_stream_collide_v<L, S, 4><<<grid, block, 0, s->stream>>>(s->kp, (const typename S::T*)fin,
-                                                                    (typename S::T*)fout, s->cls, s->flags, s->sdf,
-                                                                    s->wheels);
+#define WT_LAUNCH_V(VV, MB)                                                                                       \
+  k_stream_collide_v<L, S, VV, MB><<<grid, block, 0, s->stream>>>(s->kp, (const typename S::T*)fin,                   \
+                                                                  (typename S::T*)fout, s->cls, s->flags, s->sdf, s->wheels)
+      const int mb = s->sc_kernel;
+      if (V == 2) {
+        if (mb == 2) WT_LAUNCH_V(2, 2);
+        else if (mb == 3) WT_LAUNCH_V(2, 3);
+        else if (mb == 4) WT_LAUNCH_V(2, 4);
+        else WT_LAUNCH_V(2, 0);
+      } else {
+        if (mb == 2) WT_LAUNCH_V(4, 2);
+        else if (mb == 3) WT_LAUNCH_V(4, 3);
+        else WT_LAUNCH_V(4, 0);
+      }
+#undef WT_LAUNCH_V
       s->launches++;
       return cudaGetLastError();
     }
