@@ -9,6 +9,7 @@ without it, so single-precision results differ by a few ulp per step):
                                 the rounding of a stored half, and the force sums hundreds of
                                 wall links), 1e-10 (f64); counts exact
   EMA means .................. relative 1e-4 (f32, f64), 5e-3 (f16)
+  reference-plane density .... absolute 1e-5 (f32, f64), 5e-5 (f16)
   velocity field ............. absolute 2e-6 (f32, f64), 5e-5 (f16)
   voxelizer flags, sdf, info . bit-exact (compiled without contraction)
   tracers .................... bit-exact state and trail
@@ -72,7 +73,7 @@ def test_stream_collide_matches_oracle(gpu, oracle, dims, pset, prec, launch):
     scale = max(np.abs(so["raw"][:3]).max(), 1e-3)
     assert np.abs(sg["raw"][:3] - so["raw"][:3]).max() <= rt * scale + 1e-9, (sg["raw"], so["raw"])
     assert abs(sg["raw"][3] - so["raw"][3]) <= rt * so["raw"][3] + 1e-12
-    assert abs(sg["rhoRef"] - so["rhoRef"]) <= 1e-5
+    assert abs(sg["rhoRef"] - so["rhoRef"]) <= (5e-5 if prec == "f16" else 1e-5)
     assert sg["raw"][5:].tolist() == so["raw"][5:].tolist()
     assert sg["step"] == so["step"] == 30 and not sg["unstable"]
     vg = g.read_velocity()

@@ -605,8 +605,8 @@ __device__ __forceinline__ void relax_cell(const wt_kparams& P, float fx, float 
 
 // Regularized / BGK collision of two bulk cells at once on shifted populations (lanes .x, .y),
 // same algebra as collide_shifted.
-template <class L>
-__device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const float2 (&h)[L::Q], int x, float2 (&o)[L::Q]) {
+template <class L, bool BGK, class Emit>
+__device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const float2 (&h)[L::Q], int x, Emit&& emit) {
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
   float2 drho = h[0];
@@ -668,8 +668,28 @@ __device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const floa
   const float2 Exy = add2(Dxx, pyy), Exz = add2(Dxx, pzz), Eyz = add2(Dyy, pzz);
   const float2 ju = fma2(jx, ux, fma2(jy, uy, mul2(jz, uz)));
   const float2 base = fma2(f2(-1.5f), ju, drho);
-  const bool bgk = P.collision == 1u;
   const float2 a = sub2(f2(1.0f), omega);
+  // inlet absorbing layer: blend towards the free-stream equilibrium (wgslLbm.ts:224-237)
+  float2 keep = f2(1.0f), sIn = f2(0.0f);
+  const bool sponge_in = P.sponge_in > 0.0f && (float)x < P.sponge_in;
+  if (sponge_in) {
+    const float inv = __fdividef(1.0f, fmaxf(P.sponge_in, 1.0f));
+    const float s0 = fminf(fmaxf(1.0f - (float)x * inv, 0.0f), 1.0f);
+    const float s1 = fminf(fmaxf(1.0f - (float)(x + 1) * inv, 0.0f), 1.0f);
+    sIn = make_float2(0.08f * s0 * s0, 0.08f * s1 * s1);
+    keep = sub2(f2(1.0f), sIn);
+  }
+  auto out = [&](auto I, float2 v) {
+    constexpr int i = decltype(I)::value;
+    if (sponge_in) {
+      constexpr int cx = L::c[i][0];
+      constexpr float w = (float)Wc<L, i>::v;
+      const float U = P.uin;
+      const float eqw = w * ((float)(3 * cx) * U + (float)(4.5 * cx * cx) * U * U - 1.5f * U * U);
+      v = fma2(v, keep, mul2(f2(eqw), sIn));
+    }
+    emit(I, v);
+  };
   static_for<Q>([&](auto I) {
     constexpr int i = I;
     constexpr int io = opp<L>(i);
@@ -699,34 +719,18 @@ __device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const floa
         qp = fma2(f2((float)(2 * sa * sb)), Pab, E);
       }
       const float2 e = fma2(mul2(f2(4.5f), cj), cu, base);  // even part of (feq - w) / w
-      if (!bgk) {
+      if constexpr (!BGK) {
         const float2 wt = mul2(f2(w), fma2(k1, qp, e));
-        o[i] = fma2(f2(3.0f * w), cj, wt);
-        if constexpr (i > 0) o[io] = fma2(f2(-3.0f * w), cj, wt);
+        out(std::integral_constant<int, i>{}, fma2(f2(3.0f * w), cj, wt));
+        if constexpr (i > 0) out(std::integral_constant<int, io>{}, fma2(f2(-3.0f * w), cj, wt));
       } else {
         const float2 we = mul2(f2(w), e);
-        o[i] = fma2(a, fma2(f2(3.0f * w), cj, we), mul2(omega, h[i]));
-        if constexpr (i > 0) o[io] = fma2(a, fma2(f2(-3.0f * w), cj, we), mul2(omega, h[io]));
+        out(std::integral_constant<int, i>{}, fma2(a, fma2(f2(3.0f * w), cj, we), mul2(omega, h[i])));
+        if constexpr (i > 0)
+          out(std::integral_constant<int, io>{}, fma2(a, fma2(f2(-3.0f * w), cj, we), mul2(omega, h[io])));
       }
     }
   });
-  // inlet absorbing layer: blend towards the free-stream equilibrium (wgslLbm.ts:224-237)
-  if (P.sponge_in > 0.0f && (float)x < P.sponge_in) {
-    float2 sIn;
-    const float inv = __fdividef(1.0f, fmaxf(P.sponge_in, 1.0f));
-    const float s0 = fminf(fmaxf(1.0f - (float)x * inv, 0.0f), 1.0f);
-    const float s1 = fminf(fmaxf(1.0f - (float)(x + 1) * inv, 0.0f), 1.0f);
-    sIn = make_float2(0.08f * s0 * s0, 0.08f * s1 * s1);
-    const float2 keep = sub2(f2(1.0f), sIn);
-    const float U = P.uin;
-    static_for<Q>([&](auto I) {
-      constexpr int i = I;
-      constexpr int cx = L::c[i][0];
-      constexpr float w = (float)Wc<L, i>::v;
-      const float eqw = w * ((float)(3 * cx) * U + (float)(4.5 * cx * cx) * U * U - 1.5f * U * U);
-      o[i] = fma2(o[i], keep, mul2(f2(eqw), sIn));
-    });
-  }
 }
 
 // two-cell loads / stores of shifted populations: elements (o, o + 1), o even. Loads are split
@@ -769,7 +773,7 @@ template <> struct PairIO<StF32> {
 // MINB: CTAs of 256 threads the register allocation must leave room for (0 = no constraint)
 template <int MINB> struct Bounds { static constexpr int v = MINB; };
 
-template <class L, class S, int V, int MINB>
+template <class L, class S, int V, int MINB, bool BGK>
 __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(const __grid_constant__ wt_kparams P,
                                                           const typename S::T* __restrict__ fin,
                                                           typename S::T* __restrict__ fout,
@@ -793,7 +797,6 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
   if constexpr (V == 2) cv = __ldg(reinterpret_cast<const unsigned short*>(cls + idx0));
   else cv = __ldg(reinterpret_cast<const unsigned int*>(cls + idx0));
   const bool fast = cv == 0u && iy > 0 && iy < NY - 1 && (!D3 || (iz > 0 && iz < NZ - 1));
-  float2 o[G][Q];
   if (fast) {
     // phase 1: every load of the V cells in flight (bulk cells: y - cy, z - cz inside the domain)
     typename IO::pair_t rp[G][Q];
@@ -843,8 +846,13 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
       });
     }
 #pragma unroll
-    for (int g = 0; g < G; g++) collide_shifted2<L>(P, h[g], x0 + 2 * g, o[g]);
+    for (int g = 0; g < G; g++)
+      collide_shifted2<L, BGK>(P, h[g], x0 + 2 * g, [&](auto I, float2 v) {
+        constexpr int i = decltype(I)::value;
+        IO::st(fout, i * N + idx0 + 2 * g, v, (float)Wc<L, i>::v);
+      });
   } else {
+    float2 o[G][Q];
 #pragma unroll
     for (int v = 0; v < V; v++) {
       float ov[Q];
@@ -865,13 +873,13 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
         else o[v / 2][i].x = ov[i];
       }
     }
-  }
-  static_for<Q>([&](auto I) {
-    constexpr int i = I;
-    constexpr float w = (float)Wc<L, i>::v;
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      constexpr float w = (float)Wc<L, i>::v;
 #pragma unroll
-    for (int g = 0; g < G; g++) IO::st(fout, i * N + idx0 + 2 * g, o[g][i], w);
-  });
+      for (int g = 0; g < G; g++) IO::st(fout, i * N + idx0 + 2 * g, o[g][i], w);
+    });
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1142,9 +1150,15 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
       }
       const dim3 block(bx, by);
       const dim3 grid((runs + bx - 1) / bx, (s->dims.ny + by - 1) / by, s->dims.nz);
-#define WT_LAUNCH_V(VV, MB)                                                                                       \
-  k_stream_collide_v<L, S, VV, MB><<<grid, block, 0, s->stream>>>(s->kp, (const typename S::T*)fin,                   \
-                                                                  (typename S::T*)fout, s->cls, s->flags, s->sdf, s->wheels)
+#define WT_LAUNCH_V(VV, MB)                                                                                     \
+  do {                                                                                                             \
+    if (s->kp.collision == 1u)                                                                                     \
+      k_stream_collide_v<L, S, VV, MB, true><<<grid, block, 0, s->stream>>>(                                       \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->flags, s->sdf, s->wheels);            \
+    else                                                                                                           \
+      k_stream_collide_v<L, S, VV, MB, false><<<grid, block, 0, s->stream>>>(                                      \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->flags, s->sdf, s->wheels);            \
+  } while (0)
       const int mb = s->sc_kernel;
       if (V == 2) {
         if (mb == 2) WT_LAUNCH_V(2, 2);
