@@ -10,7 +10,7 @@ without it, so single-precision results differ by a few ulp per step):
                                 wall links), 1e-10 (f64); counts exact
   EMA means .................. relative 1e-4 (f32, f64), 5e-3 (f16)
   reference-plane density .... absolute 1e-5 (f32, f64), 5e-5 (f16)
-  velocity field ............. absolute 2e-6 (f32, f64), 5e-5 (f16)
+  velocity field ............. absolute 2e-6 (f32, f64), 1e-4 (f16)
   voxelizer flags, sdf, info . bit-exact (compiled without contraction)
   tracers .................... bit-exact state and trail
 """
@@ -27,7 +27,7 @@ pytestmark = pytest.mark.gpu
 TOL = {"f64": (1e-12, 1e-12), "f32": (1e-6, 2e-5), "f16": (2e-5, 3e-4)}
 STAT_RTOL = {"f64": 1e-10, "f32": 1e-4, "f16": 5e-3}
 MEAN_TOL = {"f64": (1e-4, 1e-7), "f32": (1e-4, 1e-7), "f16": (5e-3, 5e-5)}
-VEL_ATOL = {"f64": 2e-6, "f32": 2e-6, "f16": 5e-5}  # f16: one half ulp of ~10 populations
+VEL_ATOL = {"f64": 2e-6, "f32": 2e-6, "f16": 1e-4}  # f16: a few half ulps of ~10 populations
 
 
 def _pair(oracle, dims, params):
