@@ -224,10 +224,15 @@ __device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L
 // Reference-exact update of one fluid cell with every boundary rule of the pull (inlet
 // equilibrium, zero-gradient outlet, free-slip / no-slip / moving-belt floor with tyre contact
 // patches, specular or periodic sides, Bouzidi walls, rotating wheels with their mass fix;
-// wgslLbm.ts:138-175, 276-291). Kept out of line: it runs only for cells next to walls and
-// domain faces, and must not inflate the register budget of the bulk path.
-// `near` = the cell's class byte says some in-domain pull source is solid; without it the
-// solid checks (and their dependent loads) are skipped, which keeps the face rows cheap.
+// wgslLbm.ts:138-175, 276-291), for cells on the domain faces and next to solids.
+//
+// Organised as gather-then-apply over groups of six links: every load a link can need (its source
+// population; for a cell next to a solid also the source flags, both wall distances, the bounce
+// partner f_opp(x), the Bouzidi partner population and flags at x + c_i, and f_i(x)) has a
+// coordinate-only address, so a group's loads are all issued before any of them is used and the
+// group costs one memory round trip instead of a chain of dependent loads per link. `near` = the
+// cell's class byte says some in-domain pull source is solid; without it the solid checks are
+// skipped. Kept out of line so that it does not inflate the register budget of the bulk path.
 template <class L, class S>
 __device__ __noinline__ void cell_general(const wt_kparams& P, const typename S::T* __restrict__ fin,
                                           const uint32_t* __restrict__ flags, const uint32_t* __restrict__ sdf,
@@ -235,15 +240,18 @@ __device__ __noinline__ void cell_general(const wt_kparams& P, const typename S:
   typedef typename S::R R;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
+  constexpr int CH = 6;  // links per gather group
+  constexpr int NCH = (Q - 1 + CH - 1) / CH;
+  enum : int { K_INLET = 0, K_GROUND = 1, K_MIRROR = 2, K_INTERIOR = 3 };
   const int NX = P.nx, NY = P.ny, NZ = P.nz;
   const size_t N = P.n;
   const size_t idx = cell_id(ix, iy, iz, NX, NY);
   const R U = (R)P.uin;
   R f[Q];
   bool wall = false, gwall = false;
-  f[0] = S::ld(fin, idx, (R)Wc<L, 0>::v);
   R mvSum = 0, mvW = 0;
   uint32_t wm = 0;
+  f[0] = S::ld(fin, idx, (R)Wc<L, 0>::v);
   R belt = P.ground == 2u ? (R)1 : (R)0;
   if (belt > (R)0 && iy == 0) {
     // tyre contact patches: belt held still near non-wheel solids (wgslLbm.ts:276-287)
@@ -258,81 +266,129 @@ __device__ __noinline__ void cell_general(const wt_kparams& P, const typename S:
           }
         }
   }
-  static_for<Q>([&](auto I) {
-    constexpr int i = I;
-    if constexpr (i > 0) {
-      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
-      constexpr int io = opp<L>(i);
-      const R w = (R)Wc<L, i>::v;
-      int sx = ix - cx;
-      const int sy = iy - cy, sz = D3 ? iz - cz : 0;
-      if constexpr (cx < 0) sx = min(sx, NX - 1);
-      const bool yOut = cy > 0 ? sy < 0 : (cy < 0 ? sy >= NY : false);
-      const bool zOut = D3 ? (cz > 0 ? sz < 0 : (cz < 0 ? sz >= NZ : false)) : false;
-      R v;
-      if (cx > 0 && sx < 0) {
-        const R cu = (R)1 * U;
-        v = w * (R)P.rho_in * ((R)1 + (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * U * U);
-      } else if (cy > 0 && yOut && P.ground != 0u) {
-        wall = true;
-        gwall = true;
-        v = S::ld(fin, (size_t)io * N + idx, (R)Wc<L, io>::v);
-        if constexpr (cx != 0) v = v + belt * ((R)(6.0 * Wc<L, i>::v * cx) * (R)P.u_ground);
-      } else {
+  const R sdf_self = (near && P.interp != 0u) ? sdf_at<R>(sdf, idx) : (R)-1;
+  static_for<NCH>([&](auto C) {
+    constexpr int c0 = 1 + CH * decltype(C)::value;
+    int kind[CH], sxcv[CH], syv[CH], szv[CH];
+    bool inA[CH];
+    R gsrc[CH], gb[CH], gah[CH], gself[CH], gsd[CH];
+    uint32_t gfs[CH], gfa[CH];
+    // ---- gather ----
+    static_for<CH>([&](auto J) {
+      constexpr int j = J;
+      constexpr int i = c0 + j;
+      if constexpr (i < Q) {
+        constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+        constexpr int io = opp<L>(i);
+        int sx = ix - cx;
+        const int sy = iy - cy, sz = D3 ? iz - cz : 0;
+        if constexpr (cx < 0) sx = min(sx, NX - 1);
+        const bool yOut = cy > 0 ? sy < 0 : (cy < 0 ? sy >= NY : false);
+        const bool zOut = D3 ? (cz > 0 ? sz < 0 : (cz < 0 ? sz >= NZ : false)) : false;
         const int sxc = min(max(sx, 0), NX - 1);
-        if (D3 && yOut && zOut) {
-          constexpr int k = mirYZ<L>(i);
-          v = S::ld(fin, (size_t)k * N + cell_id(sxc, iy, iz, NX, NY), (R)Wc<L, k>::v);
+        sxcv[j] = sxc;
+        syv[j] = sy;
+        szv[j] = sz;
+        int k;
+        size_t a = 0;
+        if (cx > 0 && sx < 0) {
+          k = K_INLET;
+        } else if (cy > 0 && yOut && P.ground != 0u) {
+          k = K_GROUND;
+        } else if (D3 && yOut && zOut) {
+          k = K_MIRROR;
+          a = (size_t)mirYZ<L>(i) * N + cell_id(sxc, iy, iz, NX, NY);
         } else if (yOut) {
-          constexpr int k = mirY<L>(i);
-          const int zz = D3 ? min(max(sz, 0), NZ - 1) : 0;
-          v = S::ld(fin, (size_t)k * N + cell_id(sxc, iy, zz, NX, NY), (R)Wc<L, k>::v);
+          k = K_MIRROR;
+          a = (size_t)mirY<L>(i) * N + cell_id(sxc, iy, D3 ? min(max(sz, 0), NZ - 1) : 0, NX, NY);
         } else if (D3 && zOut) {
-          if (P.side_mode == 1u) {
-            v = S::ld(fin, (size_t)i * N + cell_id(sxc, sy, (sz + NZ) % NZ, NX, NY), w);
-          } else {
-            constexpr int k = mirZ<L>(i);
-            v = S::ld(fin, (size_t)k * N + cell_id(sxc, sy, iz, NX, NY), (R)Wc<L, k>::v);
-          }
+          k = K_MIRROR;
+          a = P.side_mode == 1u ? (size_t)i * N + cell_id(sxc, sy, (sz + NZ) % NZ, NX, NY)
+                                : (size_t)mirZ<L>(i) * N + cell_id(sxc, sy, iz, NX, NY);
         } else {
+          k = K_INTERIOR;
+          a = (size_t)i * N + cell_id(sxc, sy, sz, NX, NY);
+        }
+        kind[j] = k;
+        // the plane of `a` (i or a mirror of i) decides the shift w; every plane's w is w_i here
+        // (mirrors preserve |c| and therefore w), so w_i is the right shift for the load
+        gsrc[j] = (k >= K_MIRROR) ? S::ld(fin, a, (R)Wc<L, i>::v) : (R)0;
+        const bool nb = near && k == K_INTERIOR;
+        gb[j] = (k == K_GROUND || nb) ? S::ld(fin, (size_t)io * N + idx, (R)Wc<L, io>::v) : (R)0;
+        gfs[j] = 0u;
+        gfa[j] = 1u;
+        inA[j] = false;
+        gah[j] = (R)0;
+        gself[j] = (R)0;
+        gsd[j] = (R)-1;
+        if (nb) {
           const size_t sc = cell_id(sxc, sy, sz, NX, NY);
-          const uint32_t fs = near ? flags[sc] : 0u;
-          if (fs != 0u) {
-            // interpolated bounce-back (Bouzidi)
-            wall = true;
-            const R fb = S::ld(fin, (size_t)io * N + idx, (R)Wc<L, io>::v);
-            R q = link_q<R>(P, sdf, idx, sc);
-            v = fb;
-            if (q < (R)0.5) {
-              const int ax = ix + cx, ay = iy + cy, az = D3 ? iz + cz : 0;
-              if (ax >= 0 && ay >= 0 && az >= 0 && ax < NX && ay < NY && az < NZ &&
-                  flags[cell_id(ax, ay, az, NX, NY)] == 0u) {
-                v = (R)2 * q * fb +
-                    ((R)1 - (R)2 * q) * S::ld(fin, (size_t)io * N + cell_id(ax, ay, az, NX, NY), (R)Wc<L, io>::v);
-              } else {
-                q = (R)0.5;
-              }
-            } else if (q > (R)0.5) {
-              v = ((R)0.5 / q) * fb + ((R)1 - (R)0.5 / q) * S::ld(fin, (size_t)i * N + idx, w);
-            }
-            if ((fs >> 8u) != 0u) {
-              R ux, uy, uz;
-              wheel_vel<R>(P, W, (fs >> 8u) - 1u, (R)0.5 * (R)(ix + sxc) + (R)0.5, (R)0.5 * (R)(iy + sy) + (R)0.5,
-                           (R)0.5 * (R)(iz + sz) + (R)0.5, ux, uy, uz);
-              const R dot = (R)cx * ux + (R)cy * uy + (R)cz * uz;
-              const R mv = (R)(6.0 * Wc<L, i>::v) * dot * (q > (R)0.5 ? (R)0.5 / q : (R)1);
-              v += mv;
-              mvSum += mv;
-              mvW += w;
-              wm |= 1u << i;
-            }
-          } else {
-            v = S::ld(fin, (size_t)i * N + sc, w);
+          gfs[j] = flags[sc];
+          if (P.interp != 0u) gsd[j] = sdf_at<R>(sdf, sc);
+          const int ax = ix + cx, ay = iy + cy, az = D3 ? iz + cz : 0;
+          inA[j] = ax >= 0 && ay >= 0 && az >= 0 && ax < NX && ay < NY && az < NZ;
+          if (inA[j]) {
+            const size_t ac = cell_id(ax, ay, az, NX, NY);
+            gfa[j] = flags[ac];
+            gah[j] = S::ld(fin, (size_t)io * N + ac, (R)Wc<L, io>::v);
           }
+          gself[j] = S::ld(fin, (size_t)i * N + idx, (R)Wc<L, i>::v);
         }
       }
-      f[i] = v;
-    }
+    });
+    // ---- apply ----
+    static_for<CH>([&](auto J) {
+      constexpr int j = J;
+      constexpr int i = c0 + j;
+      if constexpr (i < Q) {
+        constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+        const R w = (R)Wc<L, i>::v;
+        R v;
+        if (kind[j] == K_INLET) {
+          const R cu = (R)1 * U;
+          v = w * (R)P.rho_in * ((R)1 + (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * U * U);
+        } else if (kind[j] == K_GROUND) {
+          wall = true;
+          gwall = true;
+          v = gb[j];
+          if constexpr (cx != 0) v = v + belt * ((R)(6.0 * Wc<L, i>::v * cx) * (R)P.u_ground);
+        } else if (kind[j] == K_MIRROR || gfs[j] == 0u) {
+          v = gsrc[j];
+        } else {
+          // interpolated bounce-back (Bouzidi) on a solid source
+          wall = true;
+          const uint32_t fs = gfs[j];
+          const R fb = gb[j];
+          R q = (R)0.5;
+          if (P.interp != 0u) {
+            const R a = sdf_self, b = gsd[j];
+            if (!(a < (R)0 || b < (R)0 || a + b < (R)1e-6f)) {
+              q = a / (a + b);
+              q = q < (R)0.01f ? (R)0.01f : (q > (R)0.99f ? (R)0.99f : q);
+            }
+          }
+          v = fb;
+          if (q < (R)0.5) {
+            if (inA[j] && gfa[j] == 0u) v = (R)2 * q * fb + ((R)1 - (R)2 * q) * gah[j];
+            else q = (R)0.5;
+          } else if (q > (R)0.5) {
+            v = ((R)0.5 / q) * fb + ((R)1 - (R)0.5 / q) * gself[j];
+          }
+          if ((fs >> 8u) != 0u) {
+            R ux, uy, uz;
+            wheel_vel<R>(P, W, (fs >> 8u) - 1u, (R)0.5 * (R)(ix + sxcv[j]) + (R)0.5,
+                         (R)0.5 * (R)(iy + syv[j]) + (R)0.5, (R)0.5 * (R)(iz + szv[j]) + (R)0.5, ux, uy, uz);
+            const R dot = (R)cx * ux + (R)cy * uy + (R)cz * uz;
+            const R mv = (R)(6.0 * Wc<L, i>::v) * dot * (q > (R)0.5 ? (R)0.5 / q : (R)1);
+            v += mv;
+            mvSum += mv;
+            mvW += w;
+            wm |= 1u << i;
+          }
+        }
+        f[i] = v;
+      }
+    });
   });
   // wheel links: remove the net mass of the moving-wall terms (wgslLbm.ts:289-291)
   if (mvW > (R)0) {
