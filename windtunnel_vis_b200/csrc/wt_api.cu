@@ -68,11 +68,12 @@ int64_t bytes_for(const wt_dims* d, int prec) {
 
 void free_all(wt_solver* s) {
   void* bufs[] = {s->f[0], s->f[1], s->flags, s->sdf, s->cls, s->vel, s->meanA, s->meanB,
-                  s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist};
+                  s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->result_host) cudaFreeHost(s->result_host);
   if (s->err_host) cudaFreeHost(s->err_host);
+  if (s->bnd_count_host) cudaFreeHost(s->bnd_count_host);
   if (s->stream) cudaStreamDestroy(s->stream);
 }
 
@@ -234,9 +235,11 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
             alloc((void**)&s->cls, s->n, "cell class") && alloc((void**)&s->vel, s->n * 8, "velocity") &&
             alloc((void**)&s->meanA, s->n * 16, "meanA") && alloc((void**)&s->meanB, s->n * 4, "meanB") &&
             alloc((void**)&s->partials, (size_t)s->partial_blocks * 64, "partials") &&
-            alloc((void**)&s->result_dev, 64, "result") && alloc((void**)&s->err_dev, 4, "error word");
+            alloc((void**)&s->result_dev, 64, "result") && alloc((void**)&s->err_dev, 4, "error word") &&
+            alloc((void**)&s->bnd_count, 4, "boundary counter");
   if (ok && (cudaMallocHost((void**)&s->result_host, 64) != cudaSuccess ||
-             cudaMallocHost((void**)&s->err_host, 4) != cudaSuccess)) {
+             cudaMallocHost((void**)&s->err_host, 4) != cudaSuccess ||
+             cudaMallocHost((void**)&s->bnd_count_host, 4) != cudaSuccess)) {
     where = "cudaMallocHost(result)";
     ok = false;
   }

@@ -28,6 +28,15 @@ struct wt_solver {
   uint32_t* sdf = nullptr;
   uint8_t* cls = nullptr;
   bool cls_dirty = true;
+  // cells the vectorised bulk kernel leaves to the boundary kernel: every cell of an aligned group
+  // of `gs` cells along x that holds a solid cell, a fluid cell next to a solid, or lies on a
+  // domain face (built by launch_classify)
+  uint32_t* bnd = nullptr;
+  uint32_t nbnd = 0;
+  size_t bnd_cap = 0;
+  int gs = 1;
+  uint32_t* bnd_count = nullptr;  // device counter used while building the list
+  uint32_t* bnd_count_host = nullptr;  // pinned
   uint2* vel = nullptr;  // half4 (ux, uy, uz, rho) per cell
   float4* meanA = nullptr;
   float* meanB = nullptr;

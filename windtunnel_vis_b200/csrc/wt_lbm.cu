@@ -833,10 +833,7 @@ template <class L, class S, int V, int MINB, bool BGK>
 __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(const __grid_constant__ wt_kparams P,
                                                           const typename S::T* __restrict__ fin,
                                                           typename S::T* __restrict__ fout,
-                                                          const uint8_t* __restrict__ cls,
-                                                          const uint32_t* __restrict__ flags,
-                                                          const uint32_t* __restrict__ sdf,
-                                                          const __grid_constant__ Wheels W) {
+                                                          const uint8_t* __restrict__ cls, int gs) {
   typedef PairIO<S> IO;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
@@ -846,95 +843,133 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
   const int iz = blockIdx.z;
   if (x0 >= NX || iy >= NY) return;
+  // rows on the domain faces and groups holding solid / near-solid cells belong to k_boundary
+  if (iy == 0 || iy == NY - 1 || (D3 && (iz == 0 || iz == NZ - 1))) return;
   const uint32_t N = P.n;
   const uint32_t sy = (uint32_t)NX, sz = (uint32_t)NX * (uint32_t)NY;
   const uint32_t idx0 = (uint32_t)x0 + sy * (uint32_t)iy + sz * (uint32_t)iz;
   uint32_t cv;
-  if constexpr (V == 2) cv = __ldg(reinterpret_cast<const unsigned short*>(cls + idx0));
-  else cv = __ldg(reinterpret_cast<const unsigned int*>(cls + idx0));
-  const bool fast = cv == 0u && iy > 0 && iy < NY - 1 && (!D3 || (iz > 0 && iz < NZ - 1));
-  if (fast) {
-    // phase 1: every load of the V cells in flight (bulk cells: y - cy, z - cz inside the domain)
-    typename IO::pair_t rp[G][Q];
-    typename IO::one_t r1[Q];
-    const bool last = x0 + V >= NX;
-    static_for<Q>([&](auto I) {
-      constexpr int i = I;
-      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
-      const uint32_t src = i * N + idx0 - (uint32_t)(cy * (int)sy) - (uint32_t)(cz * (int)sz);
+  if (gs == 4) cv = __ldg(reinterpret_cast<const unsigned int*>(cls + (idx0 & ~3u)));
+  else cv = __ldg(reinterpret_cast<const unsigned short*>(cls + idx0));
+  if (cv != 0u) return;
+  // phase 1: every load of the V cells in flight (bulk cells: y - cy, z - cz inside the domain)
+  typename IO::pair_t rp[G][Q];
+  typename IO::one_t r1[Q];
+  const bool last = x0 + V >= NX;
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+    const uint32_t src = i * N + idx0 - (uint32_t)(cy * (int)sy) - (uint32_t)(cz * (int)sz);
 #pragma unroll
-      for (int g = 0; g < G; g++) rp[g][i] = IO::ld(fin, src + 2 * g);
-      if constexpr (cx > 0) r1[i] = IO::ld1(fin, x0 > 0 ? src - 1u : src);          // x - 1
-      if constexpr (cx < 0) r1[i] = IO::ld1(fin, last ? src + (V - 1) : src + V);   // x + 1, outlet clamp
-    });
-    // phase 2: convert and shift into the pulled populations of each cell
-    float2 h[G][Q];
+    for (int g = 0; g < G; g++) rp[g][i] = IO::ld(fin, src + 2 * g);
+    if constexpr (cx > 0) r1[i] = IO::ld1(fin, x0 > 0 ? src - 1u : src);          // x - 1
+    if constexpr (cx < 0) r1[i] = IO::ld1(fin, last ? src + (V - 1) : src + V);   // x + 1, outlet clamp
+  });
+  // phase 2: convert and shift into the pulled populations of each cell
+  float2 h[G][Q];
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    constexpr int cx = L::c[i][0];
+    constexpr float w = (float)Wc<L, i>::v;
+    float2 cur[G];
+#pragma unroll
+    for (int g = 0; g < G; g++) cur[g] = IO::cvt(rp[g][i], w);
+    if constexpr (cx == 0) {
+#pragma unroll
+      for (int g = 0; g < G; g++) h[g][i] = cur[g];
+    } else if constexpr (cx > 0) {
+      h[0][i] = make_float2(IO::cvt1(r1[i], w), cur[0].x);
+#pragma unroll
+      for (int g = 1; g < G; g++) h[g][i] = make_float2(cur[g - 1].y, cur[g].x);
+    } else {
+#pragma unroll
+      for (int g = 0; g < G - 1; g++) h[g][i] = make_float2(cur[g].y, cur[g + 1].x);
+      h[G - 1][i] = make_float2(cur[G - 1].y, IO::cvt1(r1[i], w));
+    }
+  });
+  if (x0 == 0) {
+    // inlet column: populations entering from x < 0 are the free-stream equilibrium
+    const float U = P.uin;
     static_for<Q>([&](auto I) {
       constexpr int i = I;
       constexpr int cx = L::c[i][0];
-      constexpr float w = (float)Wc<L, i>::v;
-      float2 cur[G];
-#pragma unroll
-      for (int g = 0; g < G; g++) cur[g] = IO::cvt(rp[g][i], w);
-      if constexpr (cx == 0) {
-#pragma unroll
-        for (int g = 0; g < G; g++) h[g][i] = cur[g];
-      } else if constexpr (cx > 0) {
-        h[0][i] = make_float2(IO::cvt1(r1[i], w), cur[0].x);
-#pragma unroll
-        for (int g = 1; g < G; g++) h[g][i] = make_float2(cur[g - 1].y, cur[g].x);
-      } else {
-#pragma unroll
-        for (int g = 0; g < G - 1; g++) h[g][i] = make_float2(cur[g].y, cur[g + 1].x);
-        h[G - 1][i] = make_float2(cur[G - 1].y, IO::cvt1(r1[i], w));
+      if constexpr (cx > 0) {
+        constexpr float w = (float)Wc<L, i>::v;
+        h[0][i].x = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
       }
     });
-    if (x0 == 0) {
-      // inlet column: populations entering from x < 0 are the free-stream equilibrium
-      const float U = P.uin;
-      static_for<Q>([&](auto I) {
-        constexpr int i = I;
-        constexpr int cx = L::c[i][0];
-        if constexpr (cx > 0) {
-          constexpr float w = (float)Wc<L, i>::v;
-          h[0][i].x = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
-        }
-      });
-    }
+  }
 #pragma unroll
-    for (int g = 0; g < G; g++)
-      collide_shifted2<L, BGK>(P, h[g], x0 + 2 * g, [&](auto I, float2 v) {
-        constexpr int i = decltype(I)::value;
-        IO::st(fout, i * N + idx0 + 2 * g, v, (float)Wc<L, i>::v);
-      });
-  } else {
-    float2 o[G][Q];
-#pragma unroll
-    for (int v = 0; v < V; v++) {
-      float ov[Q];
-      if ((cv >> (8 * v)) & CLS_SOLID) {
-#pragma unroll
-        for (int i = 0; i < Q; i++) ov[i] = 0.0f;  // solids hold f = w
-      } else {
-        float fo[Q];
-        cell_general<L, S>(P, fin, flags, sdf, W, x0 + v, iy, iz, ((cv >> (8 * v)) & CLS_NEAR_SOLID) != 0, fo);
-        static_for<Q>([&](auto I) {
-          constexpr int i = I;
-          ov[i] = fo[i] - (float)Wc<L, i>::v;
-        });
-      }
-#pragma unroll
-      for (int i = 0; i < Q; i++) {
-        if (v & 1) o[v / 2][i].y = ov[i];
-        else o[v / 2][i].x = ov[i];
-      }
-    }
+  for (int g = 0; g < G; g++)
+    collide_shifted2<L, BGK>(P, h[g], x0 + 2 * g, [&](auto I, float2 v) {
+      constexpr int i = decltype(I)::value;
+      IO::st(fout, i * N + idx0 + 2 * g, v, (float)Wc<L, i>::v);
+    });
+}
+
+// Cells the bulk kernel leaves out (domain faces, solids and their fluid neighbours, and the rest
+// of their aligned groups): one thread per listed cell, reference-exact boundary rules.
+template <class L, class S>
+__global__ void __launch_bounds__(128) k_boundary(const __grid_constant__ wt_kparams P,
+                                                  const typename S::T* __restrict__ fin,
+                                                  typename S::T* __restrict__ fout,
+                                                  const uint8_t* __restrict__ cls,
+                                                  const uint32_t* __restrict__ flags,
+                                                  const uint32_t* __restrict__ sdf,
+                                                  const __grid_constant__ Wheels W,
+                                                  const uint32_t* __restrict__ list, uint32_t count) {
+  typedef typename S::R R;
+  constexpr int Q = L::Q;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const uint32_t c = list[t];
+  const uint32_t NX = P.nx, NY = P.ny;
+  const int ix = (int)(c % NX), iy = (int)((c / NX) % NY), iz = (int)(c / (NX * NY));
+  const size_t N = P.n;
+  const uint8_t cl = cls[c];
+  if (cl & CLS_SOLID) {
     static_for<Q>([&](auto I) {
       constexpr int i = I;
-      constexpr float w = (float)Wc<L, i>::v;
-#pragma unroll
-      for (int g = 0; g < G; g++) IO::st(fout, i * N + idx0 + 2 * g, o[g][i], w);
+      fout[(size_t)i * N + c] = S::solid((R)Wc<L, i>::v);
     });
+    return;
+  }
+  R fo[Q];
+  cell_general<L, S>(P, fin, flags, sdf, W, ix, iy, iz, (cl & CLS_NEAR_SOLID) != 0, fo);
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    S::st(fout, (size_t)i * N + c, fo[i], (R)Wc<L, i>::v);
+  });
+}
+
+// Builds the boundary list: pass 0 counts, pass 1 writes (warp-aggregated slots, in x order
+// inside each warp).
+template <class L>
+__global__ void __launch_bounds__(256) k_boundary_list(const __grid_constant__ wt_kparams P,
+                                                       const uint8_t* __restrict__ cls, int gs,
+                                                       uint32_t* __restrict__ counter, uint32_t* __restrict__ list,
+                                                       int pass) {
+  constexpr bool D3 = L::DIM == 3;
+  const uint32_t NX = P.nx, NY = P.ny, NZ = P.nz;
+  const uint32_t N = P.n;
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t base = (blockIdx.x * blockDim.x + (threadIdx.x & ~31u)); base < N; base += gridDim.x * blockDim.x) {
+    const uint32_t c = base + lane;
+    bool sel = false;
+    if (c < N) {
+      const uint32_t y = (c / NX) % NY, z = c / (NX * NY);
+      const bool face = y == 0 || y == NY - 1 || (D3 && (z == 0 || z == NZ - 1));
+      const uint32_t g0 = c - (c % NX) % (uint32_t)gs;
+      bool dirty = face;
+      for (int k = 0; k < gs; k++) dirty = dirty || cls[g0 + k] != 0;
+      sel = dirty;
+    }
+    const uint32_t ball = __ballot_sync(0xffffffffu, sel);
+    if (ball == 0u) continue;
+    uint32_t slot = 0;
+    if (lane == 0) slot = atomicAdd(counter, __popc(ball));
+    slot = __shfl_sync(0xffffffffu, slot, 0);
+    if (pass == 1 && sel) list[slot + __popc(ball & ((1u << lane) - 1u))] = c;
   }
 }
 
@@ -1174,7 +1209,44 @@ static cudaError_t classify_t(wt_solver* s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_classify(wt_solver* s) { return s->is3d ? classify_t<D3Q19>(s) : classify_t<D2Q9>(s); }
+template <class L>
+static cudaError_t boundary_list_t(wt_solver* s) {
+  cudaError_t e;
+  const unsigned blocks = (unsigned)std::min<size_t>((s->n + 255) / 256, 148 * 16);
+  if ((e = cudaMemsetAsync(s->bnd_count, 0, 4, s->stream)) != cudaSuccess) return e;
+  k_boundary_list<L><<<blocks, 256, 0, s->stream>>>(s->kp, s->cls, s->gs, s->bnd_count, nullptr, 0);
+  s->launches++;
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(s->bnd_count_host, s->bnd_count, 4, cudaMemcpyDeviceToHost, s->stream)) != cudaSuccess)
+    return e;
+  if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return e;
+  const uint32_t count = *s->bnd_count_host;
+  if ((size_t)count > s->bnd_cap) {
+    if (s->bnd) cudaFree(s->bnd);
+    s->bnd = nullptr;
+    s->bnd_cap = 0;
+    if ((e = cudaMalloc((void**)&s->bnd, (size_t)count * 4)) != cudaSuccess) return e;
+    s->bnd_cap = count;
+  }
+  s->nbnd = count;
+  if (count == 0) return cudaSuccess;
+  if ((e = cudaMemsetAsync(s->bnd_count, 0, 4, s->stream)) != cudaSuccess) return e;
+  k_boundary_list<L><<<blocks, 256, 0, s->stream>>>(s->kp, s->cls, s->gs, s->bnd_count, s->bnd, 1);
+  s->launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_classify(wt_solver* s) {
+  // group size of the bulk kernel's clean / boundary decision along x
+  s->gs = s->dims.nx % 4 == 0 ? 4 : (s->dims.nx % 2 == 0 ? 2 : 1);
+  cudaError_t e = s->is3d ? classify_t<D3Q19>(s) : classify_t<D2Q9>(s);
+  if (e != cudaSuccess) return e;
+  if (s->gs == 1) {
+    s->nbnd = 0;
+    return cudaSuccess;
+  }
+  return s->is3d ? boundary_list_t<D3Q19>(s) : boundary_list_t<D2Q9>(s);
+}
 
 template <class L, class S>
 static cudaError_t init_t(wt_solver* s) {
@@ -1197,7 +1269,7 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
   constexpr bool vec_ok = S::PREC == WT_PREC_F16 || S::PREC == WT_PREC_F32;
   if constexpr (vec_ok) {
     const int V = s->sc_param;
-    if ((V == 2 || V == 4) && s->dims.nx % V == 0 && offsets32(s)) {
+    if ((V == 2 || V == 4) && s->dims.nx % V == 0 && s->gs >= V && offsets32(s)) {
       const int runs = s->dims.nx / V;
       int bx = s->sc_bx, by = s->sc_by;
       if (bx <= 0 || by <= 0) {
@@ -1210,10 +1282,10 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
   do {                                                                                                             \
     if (s->kp.collision == 1u)                                                                                     \
       k_stream_collide_v<L, S, VV, MB, true><<<grid, block, 0, s->stream>>>(                                       \
-          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->flags, s->sdf, s->wheels);            \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs);                                  \
     else                                                                                                           \
       k_stream_collide_v<L, S, VV, MB, false><<<grid, block, 0, s->stream>>>(                                      \
-          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->flags, s->sdf, s->wheels);            \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs);                                  \
   } while (0)
       const int mb = s->sc_kernel;
       if (V == 2) {
@@ -1227,6 +1299,12 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
         else WT_LAUNCH_V(4, 0);
       }
 #undef WT_LAUNCH_V
+      s->launches++;
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess || s->nbnd == 0) return e;
+      k_boundary<L, S><<<(s->nbnd + 127) / 128, 128, 0, s->stream>>>(s->kp, (const typename S::T*)fin,
+                                                                    (typename S::T*)fout, s->cls, s->flags, s->sdf,
+                                                                    s->wheels, s->bnd, s->nbnd);
       s->launches++;
       return cudaGetLastError();
     }
