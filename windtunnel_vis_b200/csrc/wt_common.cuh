@@ -104,8 +104,10 @@ struct Wheels {
 
 // ---- cell classes (built from the flags by k_classify) --------------------------------------
 enum : uint8_t {
-  CLS_SOLID = 1,      // flags != 0
-  CLS_NEAR_SOLID = 2  // fluid with at least one in-domain pull source that is solid
+  CLS_SOLID = 1,        // flags != 0
+  CLS_NEAR_SOLID = 2,   // fluid with at least one in-domain pull source that is solid
+  CLS_BELT_STILL = 4,   // floor cell (y = 0) with a non-wheel solid within the tyre contact patch
+  CLS_BOUNDARY = CLS_SOLID | CLS_NEAR_SOLID  // bits that send a cell to the per-cell boundary path
 };
 
 __host__ __device__ __forceinline__ uint32_t pcg_hash(uint32_t v) {

@@ -74,6 +74,19 @@ __global__ void __launch_bounds__(256) k_classify(const wt_kparams P, const uint
     return;
   }
   uint8_t c = 0;
+  if (iy == 0) {
+    // tyre contact patch: a non-wheel solid within |dx|, |dz| <= contactH, dy in {0, 1}
+    const int r = (int)P.contact_h;
+    for (int dz = -r; dz <= r; dz++)
+      for (int dx = -r; dx <= r; dx++)
+        for (int dy = 0; dy <= 1 && dy < NY; dy++) {
+          const int qx = ix + dx, qz = iz + dz;
+          if (qx >= 0 && qx < NX && qz >= 0 && qz < NZ) {
+            const uint32_t fq = flags[cell_id(qx, dy, qz, NX, NY)];
+            if (fq != 0u && (fq >> 8u) == 0u) c |= CLS_BELT_STILL;
+          }
+        }
+  }
   static_for<L::Q>([&](auto I) {
     constexpr int i = I;
     if constexpr (i > 0) {
@@ -85,7 +98,7 @@ __global__ void __launch_bounds__(256) k_classify(const wt_kparams P, const uint
       const bool zOut = L::DIM == 3 && (sz < 0 || sz >= NZ);
       if (!inlet && !yOut && !zOut) {
         const int sxc = min(max(sx, 0), NX - 1);
-        if (flags[cell_id(sxc, sy, sz, NX, NY)] != 0u) c = CLS_NEAR_SOLID;
+        if (flags[cell_id(sxc, sy, sz, NX, NY)] != 0u) c |= CLS_NEAR_SOLID;
       }
     }
   });
@@ -434,7 +447,7 @@ __global__ void __launch_bounds__(256) k_stream_collide(const __grid_constant__ 
     return;
   }
   R fo[Q];
-  const bool fast = cl == 0 && iy > 0 && iy < NY - 1 && (!D3 || (iz > 0 && iz < NZ - 1));
+  const bool fast = (cl & CLS_BOUNDARY) == 0 && iy > 0 && iy < NY - 1 && (!D3 || (iz > 0 && iz < NZ - 1));
   if (fast) {
     // bulk: every pull source is an in-domain fluid cell, except the inlet / outlet columns
     const R U = (R)P.uin;
@@ -644,13 +657,15 @@ __device__ __forceinline__ float sqrt_approx(float x) {
 }
 
 // relaxation time of one bulk cell: molecular tau0 + outlet sponge, Smagorinsky closure
-__device__ __forceinline__ void relax_cell(const wt_kparams& P, float fx, float pn, float irho, float& omega) {
+__device__ __forceinline__ void relax_cell(const wt_kparams& P, float fx, float pn, float irho, float& omega,
+                                           float t_floor) {
   float t0 = P.tau0;
   if (fx > P.sponge_start) {
     const float den = (float)P.nx - P.sponge_start;
     const float sp = fminf(__fdividef(fx - P.sponge_start, den > 1.0f ? den : 1.0f), 1.0f);
     t0 += 3.0f * P.sponge_nu * sp * sp;
   }
+  t0 = fmaxf(t0, t_floor);
   float tau = t0;
   if (P.csmag2 > 0.0f) {
     const float k = (float)(18.0 * 1.4142135623730951) * P.csmag2;
@@ -662,7 +677,8 @@ __device__ __forceinline__ void relax_cell(const wt_kparams& P, float fx, float 
 // Regularized / BGK collision of two bulk cells at once on shifted populations (lanes .x, .y),
 // same algebra as collide_shifted.
 template <class L, bool BGK, class Emit>
-__device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const float2 (&h)[L::Q], int x, Emit&& emit) {
+__device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const float2 (&h)[L::Q], int x, Emit&& emit,
+                                                 float t_floor = 0.0f) {
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
   float2 drho = h[0];
@@ -708,11 +724,11 @@ __device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const floa
     pyz = fma2(jy, nuz, syz);
   }
   float2 omega, k1;
-  if (P.csmag2 > 0.0f || P.sponge_start < (float)P.nx) {
+  if (P.csmag2 > 0.0f || P.sponge_start < (float)P.nx || t_floor > P.tau0) {
     float2 pn = fma2(pxx, pxx, fma2(pyy, pyy, mul2(f2(2.f), mul2(pxy, pxy))));
     if constexpr (D3) pn = fma2(pzz, pzz, fma2(f2(2.f), fma2(pxz, pxz, mul2(pyz, pyz)), pn));
-    relax_cell(P, (float)x, pn.x, irho.x, omega.x);
-    relax_cell(P, (float)(x + 1), pn.y, irho.y, omega.y);
+    relax_cell(P, (float)x, pn.x, irho.x, omega.x, t_floor);
+    relax_cell(P, (float)(x + 1), pn.y, irho.y, omega.y, t_floor);
   } else {
     const float om = 1.0f - __fdividef(1.0f, P.tau0);
     omega = f2(om);
@@ -851,7 +867,7 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
   uint32_t cv;
   if (gs == 4) cv = __ldg(reinterpret_cast<const unsigned int*>(cls + (idx0 & ~3u)));
   else cv = __ldg(reinterpret_cast<const unsigned short*>(cls + idx0));
-  if (cv != 0u) return;
+  if ((cv & 0x03030303u) != 0u) return;
   // phase 1: every load of the V cells in flight (bulk cells: y - cy, z - cz inside the domain)
   typename IO::pair_t rp[G][Q];
   typename IO::one_t r1[Q];
@@ -907,8 +923,143 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
     });
 }
 
-// Cells the bulk kernel leaves out (domain faces, solids and their fluid neighbours, and the rest
-// of their aligned groups): one thread per listed cell, reference-exact boundary rules.
+// Rows on the domain faces (y = 0 or ny - 1, and z = 0 or nz - 1 in 3-D), vectorised like the
+// bulk. The boundary rule of a direction is the same along a whole row, so each direction's source
+// is a (population plane, row, x shift) triple chosen once per row (wgslLbm.ts:138-175): the
+// specular images mirrorY / mirrorZ / mirrorYZ or the periodic image for pulls from beyond the
+// roof and sides, bounce-back of the cell's own opposite population plus the belt term on a
+// no-slip or moving floor, and the inlet equilibrium / zero-gradient outlet as in the bulk. Floor
+// rows with bounce-back collide with BGK and the tauWall floor, like the reference's wall cells.
+// Groups holding a solid or a fluid cell next to a solid are left to k_boundary.
+template <class L, class S>
+__global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kparams P,
+                                                const typename S::T* __restrict__ fin,
+                                                typename S::T* __restrict__ fout,
+                                                const uint8_t* __restrict__ cls, int gs) {
+  typedef PairIO<S> IO;
+  constexpr int Q = L::Q;
+  constexpr bool D3 = L::DIM == 3;
+  const int NX = P.nx, NY = P.ny, NZ = P.nz;
+  const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 2;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  int iy, iz;
+  if constexpr (!D3) {
+    if (r >= 2) return;
+    iy = r == 0 ? 0 : NY - 1;
+    iz = 0;
+  } else {
+    if (r >= 2 * NY + 2 * (NZ - 2)) return;
+    if (r < NY) {
+      iy = r;
+      iz = 0;
+    } else if (r < 2 * NY) {
+      iy = r - NY;
+      iz = NZ - 1;
+    } else {
+      const int k = r - 2 * NY;
+      iz = 1 + (k >> 1);
+      iy = (k & 1) ? NY - 1 : 0;
+    }
+  }
+  if (x0 >= NX) return;
+  const uint32_t N = P.n;
+  const uint32_t sy = (uint32_t)NX, sz = (uint32_t)NX * (uint32_t)NY;
+  const uint32_t idx0 = (uint32_t)x0 + sy * (uint32_t)iy + sz * (uint32_t)iz;
+  uint32_t cv, c0, c1;
+  if (gs == 4) {
+    cv = __ldg(reinterpret_cast<const unsigned int*>(cls + (idx0 & ~3u)));
+    const int sh = 8 * (int)(idx0 & 3u);
+    c0 = (cv >> sh) & 0xffu;
+    c1 = (cv >> (sh + 8)) & 0xffu;
+  } else {
+    cv = __ldg(reinterpret_cast<const unsigned short*>(cls + idx0));
+    c0 = cv & 0xffu;
+    c1 = (cv >> 8) & 0xffu;
+  }
+  if ((cv & 0x03030303u) != 0u) return;
+  const bool gwall = iy == 0 && P.ground != 0u;
+  const float2 belt = (gwall && P.ground == 2u)
+                          ? make_float2((c0 & CLS_BELT_STILL) ? 0.0f : 1.0f, (c1 & CLS_BELT_STILL) ? 0.0f : 1.0f)
+                          : f2(0.0f);
+  const bool last = x0 + 2 >= NX;
+  typename IO::pair_t rp[Q];
+  typename IO::one_t r1[Q];
+  bool bnc[Q];
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+    const int syy = iy - cy, szz = D3 ? iz - cz : 0;
+    const bool yOut = syy < 0 || syy >= NY;
+    const bool zOut = D3 && (szz < 0 || szz >= NZ);
+    int k = i, ry = syy, rz = szz;
+    bool bounce = false;
+    if (cy > 0 && yOut && P.ground != 0u) {
+      bounce = true;
+      k = opp<L>(i);
+      ry = iy;
+      rz = iz;
+    } else if (D3 && yOut && zOut) {
+      k = mirYZ<L>(i);
+      ry = iy;
+      rz = iz;
+    } else if (yOut) {
+      k = mirY<L>(i);
+      ry = iy;
+      rz = D3 ? min(max(szz, 0), NZ - 1) : 0;
+    } else if (D3 && zOut) {
+      if (P.side_mode == 1u) {
+        rz = (szz + NZ) % NZ;
+      } else {
+        k = mirZ<L>(i);
+        rz = iz;
+      }
+    }
+    bnc[i] = bounce;
+    const uint32_t src = (uint32_t)k * N + sy * (uint32_t)ry + sz * (uint32_t)rz + (uint32_t)x0;
+    rp[i] = IO::ld(fin, src);
+    if constexpr (cx > 0) r1[i] = IO::ld1(fin, (x0 > 0 && !bounce) ? src - 1u : src);
+    if constexpr (cx < 0) r1[i] = IO::ld1(fin, (last || bounce) ? src + 1u : src + 2u);
+  });
+  float2 h[Q];
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    constexpr int cx = L::c[i][0];
+    constexpr float w = (float)Wc<L, i>::v;  // mirror and opposite planes share w_i
+    const float2 cur = IO::cvt(rp[i], w);
+    if constexpr (cx == 0) {
+      h[i] = cur;
+    } else {
+      if (bnc[i]) {
+        h[i] = fma2(belt, f2((float)(6.0 * Wc<L, i>::v * cx) * P.u_ground), cur);
+      } else if constexpr (cx > 0) {
+        h[i] = make_float2(IO::cvt1(r1[i], w), cur.x);
+      } else {
+        h[i] = make_float2(cur.y, IO::cvt1(r1[i], w));
+      }
+    }
+  });
+  if (x0 == 0) {
+    const float U = P.uin;
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      constexpr int cx = L::c[i][0];
+      if constexpr (cx > 0) {
+        constexpr float w = (float)Wc<L, i>::v;
+        h[i].x = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
+      }
+    });
+  }
+  auto emit = [&](auto I, float2 v) {
+    constexpr int i = decltype(I)::value;
+    IO::st(fout, i * N + idx0, v, (float)Wc<L, i>::v);
+  };
+  if (gwall) collide_shifted2<L, true>(P, h, x0, emit, P.tau_wall);
+  else if (P.collision == 1u) collide_shifted2<L, true>(P, h, x0, emit);
+  else collide_shifted2<L, false>(P, h, x0, emit);
+}
+
+// Groups holding a solid or a fluid cell next to a solid (listed by k_boundary_list): one thread
+// per listed cell, reference-exact boundary rules.
 template <class L, class S>
 __global__ void __launch_bounds__(128) k_boundary(const __grid_constant__ wt_kparams P,
                                                   const typename S::T* __restrict__ fin,
@@ -942,26 +1093,23 @@ __global__ void __launch_bounds__(128) k_boundary(const __grid_constant__ wt_kpa
   });
 }
 
-// Builds the boundary list: pass 0 counts, pass 1 writes (warp-aggregated slots, in x order
-// inside each warp).
+// Builds the boundary list (every cell of a group holding a solid or near-solid cell): pass 0
+// counts, pass 1 writes (warp-aggregated slots, in x order inside each warp).
 template <class L>
 __global__ void __launch_bounds__(256) k_boundary_list(const __grid_constant__ wt_kparams P,
                                                        const uint8_t* __restrict__ cls, int gs,
                                                        uint32_t* __restrict__ counter, uint32_t* __restrict__ list,
                                                        int pass) {
-  constexpr bool D3 = L::DIM == 3;
-  const uint32_t NX = P.nx, NY = P.ny, NZ = P.nz;
+  const uint32_t NX = P.nx;
   const uint32_t N = P.n;
   const uint32_t lane = threadIdx.x & 31;
   for (uint32_t base = (blockIdx.x * blockDim.x + (threadIdx.x & ~31u)); base < N; base += gridDim.x * blockDim.x) {
     const uint32_t c = base + lane;
     bool sel = false;
     if (c < N) {
-      const uint32_t y = (c / NX) % NY, z = c / (NX * NY);
-      const bool face = y == 0 || y == NY - 1 || (D3 && (z == 0 || z == NZ - 1));
       const uint32_t g0 = c - (c % NX) % (uint32_t)gs;
-      bool dirty = face;
-      for (int k = 0; k < gs; k++) dirty = dirty || cls[g0 + k] != 0;
+      bool dirty = false;
+      for (int k = 0; k < gs; k++) dirty = dirty || (cls[g0 + k] & CLS_BOUNDARY) != 0;
       sel = dirty;
     }
     const uint32_t ball = __ballot_sync(0xffffffffu, sel);
@@ -1269,7 +1417,8 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
   constexpr bool vec_ok = S::PREC == WT_PREC_F16 || S::PREC == WT_PREC_F32;
   if constexpr (vec_ok) {
     const int V = s->sc_param;
-    if ((V == 2 || V == 4) && s->dims.nx % V == 0 && s->gs >= V && offsets32(s)) {
+    const bool faces_ok = s->dims.ny >= 2 && (L::DIM == 2 || s->dims.nz >= 2);
+    if ((V == 2 || V == 4) && s->dims.nx % V == 0 && s->gs >= V && faces_ok && offsets32(s)) {
       const int runs = s->dims.nx / V;
       int bx = s->sc_bx, by = s->sc_by;
       if (bx <= 0 || by <= 0) {
@@ -1301,7 +1450,19 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
 #undef WT_LAUNCH_V
       s->launches++;
       cudaError_t e = cudaGetLastError();
-      if (e != cudaSuccess || s->nbnd == 0) return e;
+      if (e != cudaSuccess) return e;
+      {
+        const int fr = L::DIM == 3 ? 2 * s->dims.ny + 2 * (s->dims.nz - 2) : 2;
+        const int runs2 = s->dims.nx / 2;
+        const int fbx = runs2 >= 128 ? 128 : ((runs2 + 31) / 32) * 32;
+        const int fby = 256 / fbx;
+        const dim3 fgrid((runs2 + fbx - 1) / fbx, (fr + fby - 1) / fby, 1);
+        k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, s->stream>>>(s->kp, (const typename S::T*)fin,
+                                                                (typename S::T*)fout, s->cls, s->gs);
+        s->launches++;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      }
+      if (s->nbnd == 0) return cudaSuccess;
       k_boundary<L, S><<<(s->nbnd + 127) / 128, 128, 0, s->stream>>>(s->kp, (const typename S::T*)fin,
                                                                     (typename S::T*)fout, s->cls, s->flags, s->sdf,
                                                                     s->wheels, s->bnd, s->nbnd);
