@@ -75,6 +75,7 @@ struct StF32 {
   __device__ __forceinline__ static R ld(const T* __restrict__ p, size_t o, R /*w*/) { return __ldg(p + o); }
   __device__ __forceinline__ static void st(T* __restrict__ p, size_t o, R v, R /*w*/) { p[o] = v; }
   __device__ __forceinline__ static T solid(R w) { return w; }
+  __device__ __forceinline__ static R cvt(T v, R /*w*/) { return v; }
 };
 struct StF16 {
   typedef __half T;
@@ -85,6 +86,7 @@ struct StF16 {
   }
   __device__ __forceinline__ static void st(T* __restrict__ p, size_t o, R v, R w) { p[o] = __float2half_rn(v - w); }
   __device__ __forceinline__ static T solid(R /*w*/) { return __float2half_rn(0.0f); }
+  __device__ __forceinline__ static R cvt(T v, R w) { return __half2float(v) + w; }
 };
 struct StF64 {
   typedef double T;
@@ -93,6 +95,7 @@ struct StF64 {
   __device__ __forceinline__ static R ld(const T* __restrict__ p, size_t o, R /*w*/) { return __ldg(p + o); }
   __device__ __forceinline__ static void st(T* __restrict__ p, size_t o, R v, R /*w*/) { p[o] = v; }
   __device__ __forceinline__ static T solid(R w) { return w; }
+  __device__ __forceinline__ static R cvt(T v, R /*w*/) { return v; }
 };
 
 // ---- wheels (SolverGPU.setWheels packing, SolverGPU.ts:325-335) ----------------------------

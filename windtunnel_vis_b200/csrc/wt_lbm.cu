@@ -237,20 +237,23 @@ __device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L
 // Reference-exact update of one fluid cell with every boundary rule of the pull (inlet
 // equilibrium, zero-gradient outlet, free-slip / no-slip / moving-belt floor with tyre contact
 // patches, specular or periodic sides, Bouzidi walls, rotating wheels with their mass fix;
-// wgslLbm.ts:138-175, 276-291), for cells on the domain faces and next to solids.
+// wgslLbm.ts:138-175, 276-291), for cells in groups that touch a solid.
 //
-// Organised as gather-then-apply over groups of six links: every load a link can need (its source
-// population; for a cell next to a solid also the source flags, both wall distances, the bounce
-// partner f_opp(x), the Bouzidi partner population and flags at x + c_i, and f_i(x)) has a
-// coordinate-only address, so a group's loads are all issued before any of them is used and the
-// group costs one memory round trip instead of a chain of dependent loads per link. `near` = the
-// cell's class byte says some in-domain pull source is solid; without it the solid checks are
-// skipped. Kept out of line so that it does not inflate the register budget of the bulk path.
+// Organised as gather-then-apply. The cell's own 19 populations are loaded first; then, for groups
+// of six links, every value a link can need (its source population, the source flags and wall
+// distance, the Bouzidi partner population and flags at x + c_i) is fetched through a clamped,
+// always-valid address without being inspected, and only after the whole group is in flight are
+// the raw values converted and the reference's rules applied. A group therefore costs one memory
+// round trip instead of a chain of dependent loads per link. `cl` is the cell's class byte: its
+// near-solid bit enables the solid checks, its belt-still bit holds the moving belt still (the
+// tyre contact patch test of wgslLbm.ts:276-287, evaluated once by k_classify). Kept out of line
+// so that it does not inflate the register budget of the kernels that call it.
 template <class L, class S>
 __device__ __noinline__ void cell_general(const wt_kparams& P, const typename S::T* __restrict__ fin,
                                           const uint32_t* __restrict__ flags, const uint32_t* __restrict__ sdf,
-                                          const Wheels& W, int ix, int iy, int iz, bool near, typename S::R* out) {
+                                          const Wheels& W, int ix, int iy, int iz, uint32_t cl, typename S::R* out) {
   typedef typename S::R R;
+  typedef typename S::T T;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
   constexpr int CH = 6;  // links per gather group
@@ -259,34 +262,34 @@ __device__ __noinline__ void cell_general(const wt_kparams& P, const typename S:
   const int NX = P.nx, NY = P.ny, NZ = P.nz;
   const size_t N = P.n;
   const size_t idx = cell_id(ix, iy, iz, NX, NY);
+  const bool near = (cl & CLS_NEAR_SOLID) != 0;
   const R U = (R)P.uin;
+  // the cell's own populations: bounce partners f_opp(x) and the q > 1/2 Bouzidi term f_i(x)
+  T own_raw[Q];
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    own_raw[i] = __ldg(fin + (size_t)i * N + idx);
+  });
+  const uint32_t sdf_self_raw = __ldg(sdf + idx);
+  R own[Q];
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    own[i] = S::cvt(own_raw[i], (R)Wc<L, i>::v);
+  });
   R f[Q];
+  f[0] = own[0];
   bool wall = false, gwall = false;
   R mvSum = 0, mvW = 0;
   uint32_t wm = 0;
-  f[0] = S::ld(fin, idx, (R)Wc<L, 0>::v);
-  R belt = P.ground == 2u ? (R)1 : (R)0;
-  if (belt > (R)0 && iy == 0) {
-    // tyre contact patches: belt held still near non-wheel solids (wgslLbm.ts:276-287)
-    const int r = (int)P.contact_h;
-    for (int dz = -r; dz <= r; dz++)
-      for (int dx = -r; dx <= r; dx++)
-        for (int dy = 0; dy <= 1 && dy < NY; dy++) {
-          const int qx = ix + dx, qz = iz + dz;
-          if (qx >= 0 && qx < NX && qz >= 0 && qz < NZ) {
-            const uint32_t fq = flags[cell_id(qx, dy, qz, NX, NY)];
-            if (fq != 0u && (fq >> 8u) == 0u) belt = (R)0;
-          }
-        }
-  }
-  const R sdf_self = (near && P.interp != 0u) ? sdf_at<R>(sdf, idx) : (R)-1;
+  const R belt = (P.ground == 2u && !(cl & CLS_BELT_STILL)) ? (R)1 : (R)0;
+  const R sdf_self = (P.interp != 0u && sdf_self_raw != 0u) ? (R)__uint_as_float(~sdf_self_raw) : (R)-1;
   static_for<NCH>([&](auto C) {
     constexpr int c0 = 1 + CH * decltype(C)::value;
     int kind[CH], sxcv[CH], syv[CH], szv[CH];
     bool inA[CH];
-    R gsrc[CH], gb[CH], gah[CH], gself[CH], gsd[CH];
-    uint32_t gfs[CH], gfa[CH];
-    // ---- gather ----
+    T rsrc[CH], rah[CH];
+    uint32_t rfs[CH], rfa[CH], rsd[CH];
+    // ---- gather: addresses from coordinates only, every load issued before any is inspected ----
     static_for<CH>([&](auto J) {
       constexpr int j = J;
       constexpr int i = c0 + j;
@@ -299,11 +302,12 @@ __device__ __noinline__ void cell_general(const wt_kparams& P, const typename S:
         const bool yOut = cy > 0 ? sy < 0 : (cy < 0 ? sy >= NY : false);
         const bool zOut = D3 ? (cz > 0 ? sz < 0 : (cz < 0 ? sz >= NZ : false)) : false;
         const int sxc = min(max(sx, 0), NX - 1);
+        const int syc = min(max(sy, 0), NY - 1), szc = D3 ? min(max(sz, 0), NZ - 1) : 0;
         sxcv[j] = sxc;
         syv[j] = sy;
         szv[j] = sz;
         int k;
-        size_t a = 0;
+        size_t a = idx;
         if (cx > 0 && sx < 0) {
           k = K_INLET;
         } else if (cy > 0 && yOut && P.ground != 0u) {
@@ -313,7 +317,7 @@ __device__ __noinline__ void cell_general(const wt_kparams& P, const typename S:
           a = (size_t)mirYZ<L>(i) * N + cell_id(sxc, iy, iz, NX, NY);
         } else if (yOut) {
           k = K_MIRROR;
-          a = (size_t)mirY<L>(i) * N + cell_id(sxc, iy, D3 ? min(max(sz, 0), NZ - 1) : 0, NX, NY);
+          a = (size_t)mirY<L>(i) * N + cell_id(sxc, iy, szc, NX, NY);
         } else if (D3 && zOut) {
           k = K_MIRROR;
           a = P.side_mode == 1u ? (size_t)i * N + cell_id(sxc, sy, (sz + NZ) % NZ, NX, NY)
@@ -323,58 +327,45 @@ __device__ __noinline__ void cell_general(const wt_kparams& P, const typename S:
           a = (size_t)i * N + cell_id(sxc, sy, sz, NX, NY);
         }
         kind[j] = k;
-        // the plane of `a` (i or a mirror of i) decides the shift w; every plane's w is w_i here
-        // (mirrors preserve |c| and therefore w), so w_i is the right shift for the load
-        gsrc[j] = (k >= K_MIRROR) ? S::ld(fin, a, (R)Wc<L, i>::v) : (R)0;
-        const bool nb = near && k == K_INTERIOR;
-        gb[j] = (k == K_GROUND || nb) ? S::ld(fin, (size_t)io * N + idx, (R)Wc<L, io>::v) : (R)0;
-        gfs[j] = 0u;
-        gfa[j] = 1u;
-        inA[j] = false;
-        gah[j] = (R)0;
-        gself[j] = (R)0;
-        gsd[j] = (R)-1;
-        if (nb) {
-          const size_t sc = cell_id(sxc, sy, sz, NX, NY);
-          gfs[j] = flags[sc];
-          if (P.interp != 0u) gsd[j] = sdf_at<R>(sdf, sc);
-          const int ax = ix + cx, ay = iy + cy, az = D3 ? iz + cz : 0;
-          inA[j] = ax >= 0 && ay >= 0 && az >= 0 && ax < NX && ay < NY && az < NZ;
-          if (inA[j]) {
-            const size_t ac = cell_id(ax, ay, az, NX, NY);
-            gfa[j] = flags[ac];
-            gah[j] = S::ld(fin, (size_t)io * N + ac, (R)Wc<L, io>::v);
-          }
-          gself[j] = S::ld(fin, (size_t)i * N + idx, (R)Wc<L, i>::v);
-        }
+        const size_t sc = cell_id(sxc, syc, szc, NX, NY);
+        const int ax = ix + cx, ay = iy + cy, az = D3 ? iz + cz : 0;
+        inA[j] = ax >= 0 && ay >= 0 && az >= 0 && ax < NX && ay < NY && az < NZ;
+        const size_t ac = inA[j] ? cell_id(ax, ay, az, NX, NY) : idx;
+        rsrc[j] = __ldg(fin + a);
+        rfs[j] = __ldg(flags + sc);
+        rsd[j] = __ldg(sdf + sc);
+        rfa[j] = __ldg(flags + ac);
+        rah[j] = __ldg(fin + (size_t)io * N + ac);
       }
     });
-    // ---- apply ----
+    // ---- apply the reference's rules ----
     static_for<CH>([&](auto J) {
       constexpr int j = J;
       constexpr int i = c0 + j;
       if constexpr (i < Q) {
         constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+        constexpr int io = opp<L>(i);
         const R w = (R)Wc<L, i>::v;
         R v;
+        const uint32_t fs = (near && kind[j] == K_INTERIOR) ? rfs[j] : 0u;
         if (kind[j] == K_INLET) {
           const R cu = (R)1 * U;
           v = w * (R)P.rho_in * ((R)1 + (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * U * U);
         } else if (kind[j] == K_GROUND) {
           wall = true;
           gwall = true;
-          v = gb[j];
+          v = own[io];
           if constexpr (cx != 0) v = v + belt * ((R)(6.0 * Wc<L, i>::v * cx) * (R)P.u_ground);
-        } else if (kind[j] == K_MIRROR || gfs[j] == 0u) {
-          v = gsrc[j];
+        } else if (fs == 0u) {
+          // mirror / periodic image or an interior fluid source; every such plane has weight w_i
+          v = S::cvt(rsrc[j], w);
         } else {
           // interpolated bounce-back (Bouzidi) on a solid source
           wall = true;
-          const uint32_t fs = gfs[j];
-          const R fb = gb[j];
+          const R fb = own[io];
           R q = (R)0.5;
           if (P.interp != 0u) {
-            const R a = sdf_self, b = gsd[j];
+            const R a = sdf_self, b = rsd[j] != 0u ? (R)__uint_as_float(~rsd[j]) : (R)-1;
             if (!(a < (R)0 || b < (R)0 || a + b < (R)1e-6f)) {
               q = a / (a + b);
               q = q < (R)0.01f ? (R)0.01f : (q > (R)0.99f ? (R)0.99f : q);
@@ -382,10 +373,10 @@ __device__ __noinline__ void cell_general(const wt_kparams& P, const typename S:
           }
           v = fb;
           if (q < (R)0.5) {
-            if (inA[j] && gfa[j] == 0u) v = (R)2 * q * fb + ((R)1 - (R)2 * q) * gah[j];
+            if (inA[j] && rfa[j] == 0u) v = (R)2 * q * fb + ((R)1 - (R)2 * q) * S::cvt(rah[j], (R)Wc<L, io>::v);
             else q = (R)0.5;
           } else if (q > (R)0.5) {
-            v = ((R)0.5 / q) * fb + ((R)1 - (R)0.5 / q) * gself[j];
+            v = ((R)0.5 / q) * fb + ((R)1 - (R)0.5 / q) * own[i];
           }
           if ((fs >> 8u) != 0u) {
             R ux, uy, uz;
@@ -470,7 +461,7 @@ __global__ void __launch_bounds__(256) k_stream_collide(const __grid_constant__ 
     });
     collide_full<L, R>(P, f, ix, false, false, fo);
   } else {
-    cell_general<L, S>(P, fin, flags, sdf, W, ix, iy, iz, (cl & CLS_NEAR_SOLID) != 0, fo);
+    cell_general<L, S>(P, fin, flags, sdf, W, ix, iy, iz, cl, fo);
   }
   static_for<Q>([&](auto I) {
     constexpr int i = I;
@@ -1086,7 +1077,7 @@ __global__ void __launch_bounds__(128) k_boundary(const __grid_constant__ wt_kpa
     return;
   }
   R fo[Q];
-  cell_general<L, S>(P, fin, flags, sdf, W, ix, iy, iz, (cl & CLS_NEAR_SOLID) != 0, fo);
+  cell_general<L, S>(P, fin, flags, sdf, W, ix, iy, iz, cl, fo);
   static_for<Q>([&](auto I) {
     constexpr int i = I;
     S::st(fout, (size_t)i * N + c, fo[i], (R)Wc<L, i>::v);
