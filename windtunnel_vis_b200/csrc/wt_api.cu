@@ -74,7 +74,21 @@ void free_all(wt_solver* s) {
   if (s->result_host) cudaFreeHost(s->result_host);
   if (s->err_host) cudaFreeHost(s->err_host);
   if (s->bnd_count_host) cudaFreeHost(s->bnd_count_host);
+  for (auto& g : s->step_graph)
+    if (g) cudaGraphExecDestroy(g);
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  if (s->ev_join) cudaEventDestroy(s->ev_join);
+  if (s->aux) cudaStreamDestroy(s->aux);
   if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+// Drops the captured step graphs (they bake in the launch shape, the parameter block, the wheels
+// and the boundary list); the next wt_step recaptures them.
+void invalidate_graphs(wt_solver* s) {
+  for (auto& g : s->step_graph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
 }
 
 // ---- small device helpers used only by the API -----------------------------------------------
@@ -99,8 +113,29 @@ unsigned grid_for(size_t n) {
 
 int ensure_classified(wt_solver* s) {
   if (!s->cls_dirty) return WT_OK;
+  invalidate_graphs(s);
   WT_CUDA(s, wt::launch_classify(s), "classify");
   s->cls_dirty = false;
+  return WT_OK;
+}
+
+// Captures the two-step graph for starting parity p: step f[p] -> f[p^1], then f[p^1] -> f[p].
+int capture_step_graph(wt_solver* s, int p) {
+  const int64_t l0 = s->launches;
+  cudaGraph_t graph = nullptr;
+  WT_CUDA(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+  cudaError_t e = wt::launch_stream_collide(s, s->f[p], s->f[p ^ 1]);
+  if (e == cudaSuccess) e = wt::launch_stream_collide(s, s->f[p ^ 1], s->f[p]);
+  cudaError_t e2 = cudaStreamEndCapture(s->stream, &graph);
+  s->graph_launches = s->launches - l0;
+  s->launches = l0;
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&s->step_graph[p], graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    s->step_graph[p] = nullptr;
+    return cuda_fail(s, e, "graph capture");
+  }
   return WT_OK;
 }
 
@@ -230,6 +265,9 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
   const size_t fbytes = (size_t)s->q * s->n * s->pop_elem;
   s->partial_blocks = (int)std::min<size_t>((s->n + 255) / 256, 148 * 8);
   bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) == cudaSuccess &&
             alloc(&s->f[0], fbytes, "populations A") && alloc(&s->f[1], fbytes, "populations B") &&
             alloc((void**)&s->flags, s->n * 4, "flags") && alloc((void**)&s->sdf, s->n * 4, "sdf") &&
             alloc((void**)&s->cls, s->n, "cell class") && alloc((void**)&s->vel, s->n * 8, "velocity") &&
@@ -284,6 +322,7 @@ int wt_set_params(wt_solver* s, const wt_params* p) {
   if (p->precision != s->prec) return fail(s, WT_E_INVALID, "wt_set_params: precision is fixed at creation");
   s->params = *p;
   wt_pack_params(&s->dims, p, &s->kp);
+  invalidate_graphs(s);
   return WT_OK;
 }
 
@@ -341,6 +380,7 @@ int wt_upload_sdf(wt_solver* s, const float* d, int64_t n) {
 
 int wt_set_wheels(wt_solver* s, const wt_wheel* w, int32_t count) {
   if (!s || (count > 0 && !w) || count < 0) return WT_E_INVALID;
+  invalidate_graphs(s);
   std::memset(&s->wheels, 0, sizeof s->wheels);
   const int n = count < 16 ? count : 16;
   s->wheels.count = (uint32_t)n;
@@ -419,7 +459,19 @@ int wt_step(wt_solver* s, int32_t steps) {
   int rc = ensure_classified(s);
   if (!rc) rc = ensure_init(s);
   if (rc) return rc;
-  for (int32_t k = 0; k < steps; k++) {
+  int32_t k = 0;
+  if (steps >= 2) {
+    // pairs of steps replay the captured ping-pong graph of the current parity
+    if (!s->step_graph[s->parity]) {
+      rc = capture_step_graph(s, s->parity);
+      if (rc) return rc;
+    }
+    for (; k + 2 <= steps; k += 2) {
+      WT_CUDA(s, cudaGraphLaunch(s->step_graph[s->parity], s->stream), "step graph");
+      s->launches += s->graph_launches;
+    }
+  }
+  for (; k < steps; k++) {
     cudaError_t e = wt::launch_stream_collide(s, s->f[s->parity], s->f[s->parity ^ 1]);
     if (e != cudaSuccess) return cuda_fail(s, e, "stream_collide");
     s->parity ^= 1;
@@ -573,6 +625,7 @@ int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32
   s->sc_param = param;
   s->sc_bx = bx;
   s->sc_by = by;
+  invalidate_graphs(s);
   return WT_OK;
 }
 
@@ -637,6 +690,7 @@ int wt_autotune(wt_solver* s, int32_t iters, int32_t* out4) {
   s->sc_param = pick.param;
   s->sc_bx = pick.bx;
   s->sc_by = pick.by;
+  invalidate_graphs(s);
   if (out4) {
     out4[0] = pick.kernel;
     out4[1] = pick.param;

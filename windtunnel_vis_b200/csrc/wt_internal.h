@@ -12,6 +12,14 @@
 struct wt_solver {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // the face-row and per-cell boundary kernels run on `aux`, forked from and joined back into
+  // `stream` around each step, so they overlap the bulk kernel
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // two-step (one ping-pong cycle) CUDA graphs, one per starting parity; rebuilt after any change
+  // of launch shape, parameters, wheels or boundary list
+  cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
+  int64_t graph_launches = 0;  // kernel launches inside one graph replay
   wt_dims dims{};
   wt_params params{};
   wt_kparams kp{};

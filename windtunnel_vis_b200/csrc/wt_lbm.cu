@@ -1442,23 +1442,35 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
       s->launches++;
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return e;
+      // face rows and the per-cell boundary list on the auxiliary stream, overlapping the bulk
+      cudaStream_t bs = s->aux ? s->aux : s->stream;
+      if (s->aux) {
+        if ((e = cudaEventRecord(s->ev_fork, s->stream)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s->aux, s->ev_fork, 0)) != cudaSuccess) return e;
+      }
       {
         const int fr = L::DIM == 3 ? 2 * s->dims.ny + 2 * (s->dims.nz - 2) : 2;
         const int runs2 = s->dims.nx / 2;
         const int fbx = runs2 >= 128 ? 128 : ((runs2 + 31) / 32) * 32;
         const int fby = 256 / fbx;
         const dim3 fgrid((runs2 + fbx - 1) / fbx, (fr + fby - 1) / fby, 1);
-        k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, s->stream>>>(s->kp, (const typename S::T*)fin,
-                                                                (typename S::T*)fout, s->cls, s->gs);
+        k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin, (typename S::T*)fout,
+                                                         s->cls, s->gs);
         s->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
       }
-      if (s->nbnd == 0) return cudaSuccess;
-      k_boundary<L, S><<<(s->nbnd + 127) / 128, 128, 0, s->stream>>>(s->kp, (const typename S::T*)fin,
-                                                                    (typename S::T*)fout, s->cls, s->flags, s->sdf,
-                                                                    s->wheels, s->bnd, s->nbnd);
-      s->launches++;
-      return cudaGetLastError();
+      if (s->nbnd > 0) {
+        k_boundary<L, S><<<(s->nbnd + 127) / 128, 128, 0, bs>>>(s->kp, (const typename S::T*)fin,
+                                                                (typename S::T*)fout, s->cls, s->flags, s->sdf,
+                                                                s->wheels, s->bnd, s->nbnd);
+        s->launches++;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      }
+      if (s->aux) {
+        if ((e = cudaEventRecord(s->ev_join, s->aux)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s->stream, s->ev_join, 0)) != cudaSuccess) return e;
+      }
+      return cudaSuccess;
     }
   }
   const int bx = lbm_block_x(s);
