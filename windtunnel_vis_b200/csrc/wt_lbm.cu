@@ -1418,30 +1418,7 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
       }
       const dim3 block(bx, by);
       const dim3 grid((runs + bx - 1) / bx, (s->dims.ny + by - 1) / by, s->dims.nz);
-#define WT_LAUNCH_V(VV, MB)                                                                                     \
-  do {                                                                                                             \
-    if (s->kp.collision == 1u)                                                                                     \
-      k_stream_collide_v<L, S, VV, MB, true><<<grid, block, 0, s->stream>>>(                                       \
-          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs);                                  \
-    else                                                                                                           \
-      k_stream_collide_v<L, S, VV, MB, false><<<grid, block, 0, s->stream>>>(                                      \
-          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs);                                  \
-  } while (0)
-      const int mb = s->sc_kernel;
-      if (V == 2) {
-        if (mb == 2) WT_LAUNCH_V(2, 2);
-        else if (mb == 3) WT_LAUNCH_V(2, 3);
-        else if (mb == 4) WT_LAUNCH_V(2, 4);
-        else WT_LAUNCH_V(2, 0);
-      } else {
-        if (mb == 2) WT_LAUNCH_V(4, 2);
-        else if (mb == 3) WT_LAUNCH_V(4, 3);
-        else WT_LAUNCH_V(4, 0);
-      }
-#undef WT_LAUNCH_V
-      s->launches++;
-      cudaError_t e = cudaGetLastError();
-      if (e != cudaSuccess) return e;
+      cudaError_t e = cudaSuccess;
       // face rows and the per-cell boundary list on the auxiliary stream, overlapping the bulk
       cudaStream_t bs = s->aux ? s->aux : s->stream;
       if (s->aux) {
@@ -1466,6 +1443,30 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
         s->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
       }
+      // the bulk kernel on the main stream, concurrently with the auxiliary work
+#define WT_LAUNCH_V(VV, MB)                                                                                     \
+  do {                                                                                                             \
+    if (s->kp.collision == 1u)                                                                                     \
+      k_stream_collide_v<L, S, VV, MB, true><<<grid, block, 0, s->stream>>>(                                       \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs);                                  \
+    else                                                                                                           \
+      k_stream_collide_v<L, S, VV, MB, false><<<grid, block, 0, s->stream>>>(                                      \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs);                                  \
+  } while (0)
+      const int mb = s->sc_kernel;
+      if (V == 2) {
+        if (mb == 2) WT_LAUNCH_V(2, 2);
+        else if (mb == 3) WT_LAUNCH_V(2, 3);
+        else if (mb == 4) WT_LAUNCH_V(2, 4);
+        else WT_LAUNCH_V(2, 0);
+      } else {
+        if (mb == 2) WT_LAUNCH_V(4, 2);
+        else if (mb == 3) WT_LAUNCH_V(4, 3);
+        else WT_LAUNCH_V(4, 0);
+      }
+#undef WT_LAUNCH_V
+      s->launches++;
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
       if (s->aux) {
         if ((e = cudaEventRecord(s->ev_join, s->aux)) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(s->stream, s->ev_join, 0)) != cudaSuccess) return e;
