@@ -82,6 +82,15 @@ void free_all(wt_solver* s) {
   if (s->stream) cudaStreamDestroy(s->stream);
 }
 
+// The auxiliary stream gets the highest priority so that the block scheduler dispatches the
+// small, latency-bound face / boundary kernels ahead of the bulk kernel's queued blocks.
+cudaError_t create_priority_stream(cudaStream_t* st) {
+  int lo = 0, hi = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+  if (e != cudaSuccess) return e;
+  return cudaStreamCreateWithPriority(st, cudaStreamNonBlocking, hi);
+}
+
 // Drops the captured step graphs (they bake in the launch shape, the parameter block, the wheels
 // and the boundary list); the next wt_step recaptures them.
 void invalidate_graphs(wt_solver* s) {
@@ -130,7 +139,7 @@ int capture_step_graph(wt_solver* s, int p) {
   s->graph_launches = s->launches - l0;
   s->launches = l0;
   if (e == cudaSuccess) e = e2;
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&s->step_graph[p], graph, 0);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&s->step_graph[p], graph, cudaGraphInstantiateFlagUseNodePriority);
   if (graph) cudaGraphDestroy(graph);
   if (e != cudaSuccess) {
     s->step_graph[p] = nullptr;
@@ -265,7 +274,7 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
   const size_t fbytes = (size_t)s->q * s->n * s->pop_elem;
   s->partial_blocks = (int)std::min<size_t>((s->n + 255) / 256, 148 * 8);
   bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking) == cudaSuccess &&
+            create_priority_stream(&s->aux) == cudaSuccess &&
             cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
             cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) == cudaSuccess &&
             alloc(&s->f[0], fbytes, "populations A") && alloc(&s->f[1], fbytes, "populations B") &&
