@@ -47,7 +47,7 @@ def build(force: bool = False, verbose: bool = False, extra=None) -> str:
     hdr_t = max(_mtime(os.path.join(CSRC, h)) for h in HEADERS)
     hdr_t = max(hdr_t, _mtime(os.path.join(ROOT, "include", "wt.h")))
     objs = []
-    rebuilt = False
+    jobs = []
     for unit, flags in UNITS.items():
         src = os.path.join(CSRC, unit)
         obj = os.path.join(OBJ, unit.replace(".cu", ".o"))
@@ -56,8 +56,11 @@ def build(force: bool = False, verbose: bool = False, extra=None) -> str:
             cmd = [nvcc(), *ARCH, *COMMON, *flags, *(extra or []), "-c", src, "-o", obj]
             if verbose:
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
-            rebuilt = True
+            jobs.append((cmd, subprocess.Popen(cmd)))
+    for cmd, proc in jobs:
+        if proc.wait() != 0:
+            raise subprocess.CalledProcessError(proc.returncode, cmd)
+    rebuilt = bool(jobs)
     if rebuilt or not os.path.exists(LIB) or _mtime(LIB) < max(_mtime(o) for o in objs):
         cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-cudart", "static", *objs, "-o", LIB + ".tmp"]
         if verbose:

@@ -858,7 +858,10 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
   uint32_t cv;
   if (gs == 4) cv = __ldg(reinterpret_cast<const unsigned int*>(cls + (idx0 & ~3u)));
   else cv = __ldg(reinterpret_cast<const unsigned short*>(cls + idx0));
-  if ((cv & 0x03030303u) != 0u) return;
+  // groups holding solid / near-solid cells are written by k_boundary; their loads are still
+  // issued (every address is inside the domain for an interior row) so that the class byte does
+  // not add a memory round trip in front of the population loads, and only the stores are skipped
+  const bool clean = (cv & 0x03030303u) == 0u;
   // phase 1: every load of the V cells in flight (bulk cells: y - cy, z - cz inside the domain)
   typename IO::pair_t rp[G][Q];
   typename IO::one_t r1[Q];
@@ -910,7 +913,7 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
   for (int g = 0; g < G; g++)
     collide_shifted2<L, BGK>(P, h[g], x0 + 2 * g, [&](auto I, float2 v) {
       constexpr int i = decltype(I)::value;
-      IO::st(fout, i * N + idx0 + 2 * g, v, (float)Wc<L, i>::v);
+      if (clean) IO::st(fout, i * N + idx0 + 2 * g, v, (float)Wc<L, i>::v);
     });
 }
 
