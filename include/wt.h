@@ -153,8 +153,9 @@ int wt_pack_params(const wt_dims* dims, const wt_params* p, wt_kparams* out);
 int wt_create(const wt_dims* dims, const wt_params* p, wt_solver** out);
 /* LbmSolver.destroy (src/backend/types.ts:15). Accepts NULL. */
 void wt_destroy(wt_solver* s);
-/* Message of the last failing call on this handle (or of the last failing wt_create when s is
- * NULL). Valid until the next call on the handle. */
+/* Message of the last failing call on this handle; with s NULL, of the calling thread's last
+ * failing call that has no handle (wt_create, wt_fits, wt_sample_noalloc). Valid until the next
+ * such call. */
 const char* wt_last_error(const wt_solver* s);
 /* Backend.setParams (src/backend/types.ts:30) / SolverGPU.setParams (SolverGPU.ts:155-158).
  * precision must equal the creation precision. */
@@ -237,6 +238,43 @@ void* wt_stream(const wt_solver* s);
 int32_t wt_device(const wt_solver* s);
 /* Number of kernel launches this handle has issued since creation. */
 int64_t wt_launch_count(const wt_solver* s);
+
+/* ---- sampling pass on caller-owned buffers, without allocating ------------------------------
+ * No counterpart in the reference: the reference's solver always owns its buffers.
+ *
+ * For callers that may not allocate device memory: hosts whose device memory all belongs to
+ * another allocator (a framework's caching allocator, or an arena reserved at start-up). Such a
+ * host must not call cudaMalloc / cudaFree, because those calls synchronise the whole device and
+ * take memory that the owning allocator does not account for. It keeps the tunnel's buffers in
+ * its own memory and runs the sampling pass on them here: velocity field, EMA statistics,
+ * momentum-exchange force and the reductions, as wt_sample does for a handle. The call allocates
+ * nothing: no cudaMalloc, no cudaFree, no allocating library routine.
+ *
+ * The pass needs a reduction scratch of one 64-byte slot per 256 cells. It is a fixed array in
+ * the library's device memory (1 MiB per device), so grids are limited to
+ * WT_SAMPLE_NOALLOC_MAX_CELLS cells; larger grids are rejected with WT_E_INVALID.
+ *
+ * Buffers: device memory of the device current on the calling thread, laid out as a handle's:
+ *   populations  q * n values in the storage format of p->precision (f16 holds f - w)
+ *   flags        n u32 (bit 0 solid, bits 8-15 wheel tag)
+ *   sdf_encoded  n u32, ~bits(distance) and 0 where unknown (the format of wt_read_sdf)
+ *   vel_half4    n x 4 binary16 (ux, uy, uz, rho), written
+ *   mean4, meanb n x 4 and n floats of EMA state, read and rewritten (a handle starts them at
+ *                (0, 0, 0, 1) and 0)
+ *   result8      8 doubles, written: the raw reduction of wt_stats.raw
+ * wheels (host array, up to 16) and p are read during the call only. The kernels are queued on
+ * `stream` (NULL: the default stream) and the call returns without waiting for them.
+ *
+ * The first call on a device looks up the scratch array's address (cudaGetSymbolAddress), which
+ * can load the library's device code; make that first call before any stream capture. Every call
+ * shares the one array and it keeps the last call's contents; a call writes every slot it reads
+ * before reading it, so nothing has to be cleared. Calls that overlap on the GPU (streams with no
+ * ordering between them) race on the array: order them on one stream or with events.
+ * Errors: WT_E_INVALID, WT_E_NO_DEVICE, WT_E_CUDA; the message is in wt_last_error(NULL). */
+#define WT_SAMPLE_NOALLOC_MAX_CELLS 4194304
+int wt_sample_noalloc(const wt_dims* dims, const wt_params* p, const wt_wheel* wheels, int32_t nwheels,
+                      const void* populations, const uint32_t* flags, const uint32_t* sdf_encoded, void* vel_half4,
+                      float* mean4, float* meanb, double* result8, void* stream);
 
 #ifdef __cplusplus
 }

@@ -87,3 +87,17 @@ def test_errors_without_device_are_reported(wtlib):
     assert b"no CUDA device" in wtlib.wt_last_error(None)
     rc = wtlib.wt_create(C.byref(abi.Dims(0, 8, 8)), C.byref(P), C.byref(h))
     assert rc == abi.WT_E_INVALID
+
+
+def test_sample_noalloc_argument_checks_without_device(wtlib):
+    # size and argument checks come before any CUDA call, so they hold on a machine without a GPU
+    P = abi.make_params(dict(u=0.05, nu=0.01, precision="f16"))
+    dummy = C.c_void_p(4096)  # never dereferenced: every call below is rejected first
+    args = [None, 0] + [dummy] * 7 + [None]
+    rc = wtlib.wt_sample_noalloc(C.byref(abi.Dims(256, 128, 129)), C.byref(P), *args)
+    assert rc == abi.WT_E_INVALID
+    assert b"exceed the limit of 4194304 cells" in wtlib.wt_last_error(None)
+    rc = wtlib.wt_sample_noalloc(C.byref(abi.Dims(0, 8, 8)), C.byref(P), *args)
+    assert rc == abi.WT_E_INVALID
+    rc = wtlib.wt_sample_noalloc(C.byref(abi.Dims(8, 8, 8)), C.byref(P), None, 17, *args[2:])
+    assert rc == abi.WT_E_INVALID

@@ -157,6 +157,7 @@ def _sig(lib):
         "wt_stream": ([S], v),
         "wt_device": ([S], i32),
         "wt_launch_count": ([S], i64),
+        "wt_sample_noalloc": ([P(Dims), P(Params), P(Wheel), i32, v, v, v, v, v, v, v, v], C.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)

@@ -182,6 +182,10 @@ void decode(const wt_solver* s, const double* d, wt_stats* out) {
 
 }  // namespace
 
+namespace wt {
+int fail_unbound(int code, const std::string& msg) { return fail(nullptr, code, msg); }
+}  // namespace wt
+
 extern "C" {
 
 int wt_version(void) { return WT_ABI_VERSION; }

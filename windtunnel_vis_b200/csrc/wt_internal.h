@@ -91,4 +91,7 @@ cudaError_t launch_voxelize(wt_solver* s, const VoxelJob& job);
 // tracers (wt_tracer.cu)
 cudaError_t launch_tracers(wt_solver* s, const wt_tracer_params& p);
 
+// records `msg` as the calling thread's message for wt_last_error(NULL) and returns `code`
+int fail_unbound(int code, const std::string& msg);
+
 }  // namespace wt

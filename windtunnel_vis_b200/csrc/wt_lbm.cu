@@ -15,6 +15,8 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 #include "wt_internal.h"
 
@@ -1513,4 +1515,144 @@ cudaError_t launch_init(wt_solver* s) { WT_DISPATCH(init_t, s); }
 cudaError_t launch_stream_collide(wt_solver* s, const void* fin, void* fout) { WT_DISPATCH(sc_t, s, fin, fout); }
 cudaError_t launch_macro(wt_solver* s) { WT_DISPATCH(macro_t, s); }
 
+// ---------------------------------------------------------------------------------------------
+// sampling pass on caller-owned buffers, with its reduction scratch in a fixed device array
+// ---------------------------------------------------------------------------------------------
+// Some hosts may not allocate device memory at all (their memory belongs to another allocator,
+// and cudaMalloc / cudaFree would synchronise the device behind its back). For them the macro
+// pass's per-block partial sums live in this file-scope array instead of a handle's buffer: one
+// 8-double slot per block of MACRO_THREADS cells, enough for WT_SAMPLE_NOALLOC_MAX_CELLS cells.
+// k_macro writes all 8 slots of every block it runs before k_reduce_partials reads them, so what
+// an earlier call left in the array is never read and nothing is cleared. The array is shared by
+// every call on a device: calls that overlap on the GPU race on it.
+constexpr int NOALLOC_MAX_BLOCKS = WT_SAMPLE_NOALLOC_MAX_CELLS / MACRO_THREADS;
+static_assert(NOALLOC_MAX_BLOCKS * MACRO_THREADS == WT_SAMPLE_NOALLOC_MAX_CELLS, "whole blocks");
+static __device__ __align__(256) double g_sample_scratch[NOALLOC_MAX_BLOCKS * 8];
+
+namespace {
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_scratch_mu;
+double* g_scratch_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of g_sample_scratch on `dev`, which must be the current device. Looked up on the
+// first call for that device (this may load the module's device code) and cached.
+cudaError_t scratch_address(int dev, double** out) {
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_ptr[dev]) {
+    double* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_sample_scratch);
+    if (e != cudaSuccess) return e;
+    g_scratch_ptr[dev] = ptr;
+  }
+  *out = g_scratch_ptr[dev];
+  return cudaSuccess;
+}
+
+template <class L, class S>
+cudaError_t sample_noalloc_t(const wt_kparams& kp, const void* fin, const uint32_t* flags, const uint32_t* sdf,
+                             const Wheels& W, uint2* vel, float4* meanA, float* meanB, double* scratch, int nblocks,
+                             double* result, cudaStream_t st) {
+  k_macro<L, S><<<nblocks, MACRO_THREADS, 0, st>>>(kp, (const typename S::T*)fin, flags, sdf, W, vel, meanA, meanB,
+                                                    scratch);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_reduce_partials<<<1, 256, 0, st>>>(scratch, nblocks, result);
+  return cudaGetLastError();
+}
+
+// a caller's buffer must be device (or managed) memory of `dev`, aligned to `align` bytes
+const char* buffer_problem(const void* p, size_t align, int dev) {
+  if (!p) return "is NULL";
+  if ((uintptr_t)p % align != 0) return "is misaligned for its element type";
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return "is not a CUDA pointer";
+  }
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) return "is not device memory";
+  if (a.device != dev) return "is on another device than the current one";
+  return nullptr;
+}
+
+}  // namespace
 }  // namespace wt
+
+extern "C" int wt_sample_noalloc(const wt_dims* dims, const wt_params* p, const wt_wheel* wheels, int32_t nwheels,
+                                 const void* populations, const uint32_t* flags, const uint32_t* sdf_encoded,
+                                 void* vel_half4, float* mean4, float* meanb, double* result8, void* stream) {
+  using namespace wt;
+  auto invalid = [](const std::string& m) { return fail_unbound(WT_E_INVALID, "wt_sample_noalloc: " + m); };
+  if (!dims || !p) return invalid("dims and params are required");
+  if (dims->nx < 1 || dims->ny < 1 || dims->nz < 1) return invalid("dims must be >= 1");
+  const uint64_t n = (uint64_t)dims->nx * (uint64_t)dims->ny * (uint64_t)dims->nz;
+  if (n > (uint64_t)WT_SAMPLE_NOALLOC_MAX_CELLS)
+    return invalid(std::to_string(n) + " cells exceed the limit of " + std::to_string(WT_SAMPLE_NOALLOC_MAX_CELLS) +
+                   " cells set by the fixed reduction scratch (1 MiB); use a handle (wt_create) for larger grids");
+  if (p->precision < WT_PREC_F32 || p->precision > WT_PREC_F64) return invalid("bad precision");
+  if (nwheels < 0 || nwheels > 16 || (nwheels > 0 && !wheels)) return invalid("need 0..16 wheels and a wheel array");
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
+    cudaGetLastError();
+    return fail_unbound(WT_E_NO_DEVICE, "wt_sample_noalloc: no CUDA device");
+  }
+  if (dev >= NOALLOC_MAX_DEVICES) return invalid("device ordinal above 63");
+  const size_t elem = p->precision == WT_PREC_F16 ? 2 : (p->precision == WT_PREC_F64 ? 8 : 4);
+  const struct {
+    const void* ptr;
+    size_t align;
+    const char* name;
+  } bufs[] = {{populations, elem, "populations"}, {flags, 4, "flags"},  {sdf_encoded, 4, "sdf_encoded"},
+              {vel_half4, 8, "vel_half4"},      {mean4, 16, "mean4"}, {meanb, 4, "meanb"},
+              {result8, 8, "result8"}};
+  for (const auto& b : bufs)
+    if (const char* why = buffer_problem(b.ptr, b.align, dev)) return invalid(std::string(b.name) + " " + why);
+
+  double* scratch = nullptr;
+  cudaError_t e = scratch_address(dev, &scratch);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail_unbound(WT_E_CUDA, std::string("wt_sample_noalloc: cudaGetSymbolAddress(scratch): ") +
+                                       cudaGetErrorString(e));
+  }
+  wt_kparams kp;
+  wt_pack_params(dims, p, &kp);
+  Wheels W{};
+  W.count = (uint32_t)nwheels;
+  for (int k = 0; k < nwheels; k++) {
+    const double r = wheels[k].r > 1e-3 ? wheels[k].r : 1e-3;
+    W.w[2 * k] = make_float4((float)wheels[k].c[0], (float)wheels[k].c[1], (float)wheels[k].c[2], (float)(1.0 / r));
+    W.w[2 * k + 1] =
+        make_float4((float)wheels[k].axis[0], (float)wheels[k].axis[1], (float)wheels[k].axis[2], (float)wheels[k].hw);
+  }
+  const int nblocks = (int)((n + MACRO_THREADS - 1) / MACRO_THREADS);
+  const cudaStream_t st = (cudaStream_t)stream;
+  auto* vel = (uint2*)vel_half4;
+  auto* mA = (float4*)mean4;
+  if (dims->nz > 1) {
+    if (p->precision == WT_PREC_F16)
+      e = sample_noalloc_t<D3Q19, StF16>(kp, populations, flags, sdf_encoded, W, vel, mA, meanb, scratch, nblocks,
+                                         result8, st);
+    else if (p->precision == WT_PREC_F64)
+      e = sample_noalloc_t<D3Q19, StF64>(kp, populations, flags, sdf_encoded, W, vel, mA, meanb, scratch, nblocks,
+                                         result8, st);
+    else
+      e = sample_noalloc_t<D3Q19, StF32>(kp, populations, flags, sdf_encoded, W, vel, mA, meanb, scratch, nblocks,
+                                         result8, st);
+  } else {
+    if (p->precision == WT_PREC_F16)
+      e = sample_noalloc_t<D2Q9, StF16>(kp, populations, flags, sdf_encoded, W, vel, mA, meanb, scratch, nblocks,
+                                        result8, st);
+    else if (p->precision == WT_PREC_F64)
+      e = sample_noalloc_t<D2Q9, StF64>(kp, populations, flags, sdf_encoded, W, vel, mA, meanb, scratch, nblocks,
+                                        result8, st);
+    else
+      e = sample_noalloc_t<D2Q9, StF32>(kp, populations, flags, sdf_encoded, W, vel, mA, meanb, scratch, nblocks,
+                                        result8, st);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail_unbound(WT_E_CUDA, std::string("wt_sample_noalloc: launch: ") + cudaGetErrorString(e));
+  }
+  return WT_OK;
+}
