@@ -164,9 +164,11 @@ def run_ours(args, rank, world, local_rank, dist):
         if dist is not None:
             dist.barrier()
 
+    if args.launch:
+        s.set_launch(*(int(v) for v in args.launch.split(",")))
     for _ in range(max(args.warmup, 3)):
         s.step_and_sample(CHUNK)
-    shape = s.autotune(10)
+    shape = s.get_launch() if args.launch else s.autotune(10)
     torch.cuda.synchronize()
     barrier()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -198,6 +200,7 @@ def run_ours(args, rank, world, local_rank, dist):
     # end to end through the public API with host buffers
     fl_h = torch.from_numpy(flags).pin_memory()
     sd_h = torch.from_numpy(sdf).pin_memory()
+    vel_h = torch.empty((n, 4), dtype=torch.float32).pin_memory()
     vel_bytes = n * 16
     e2e_steps = max(2, min(args.steps, 10))
     s.step_and_sample(CHUNK)
@@ -208,7 +211,7 @@ def run_ours(args, rank, world, local_rank, dist):
         s.upload_flags(fl_h.numpy())
         s.upload_sdf(sd_h.numpy())
         st = s.step_and_sample(CHUNK)
-        s.read_velocity()
+        s.read_velocity(vel_h.numpy())
     e2e_s = time.perf_counter() - t0
     if dist is not None:
         t = torch.tensor([e2e_s], device="cuda")
@@ -260,6 +263,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--launch", default="", help="fixed stream-collide launch 'hint,cells,bx,by' instead of the tuner")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -67,7 +67,7 @@ int64_t bytes_for(const wt_dims* d, int prec) {
 }
 
 void free_all(wt_solver* s) {
-  void* bufs[] = {s->f[0], s->f[1], s->flags, s->sdf, s->cls, s->vel, s->meanA, s->meanB,
+  void* bufs[] = {s->f[0], s->f[1], s->flags, s->sdf, s->cls, s->vel, s->vel_f32, s->meanA, s->meanB,
                   s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count};
   for (void* b : bufs)
     if (b) cudaFree(b);
@@ -112,6 +112,15 @@ __global__ void k_clear_stats(float4* __restrict__ meanA, float* __restrict__ me
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     meanA[i] = make_float4(0.f, 0.f, 0.f, 1.f);
     meanB[i] = 0.f;
+  }
+}
+
+__global__ void k_vel_to_f32(const uint2* __restrict__ vel, float4* __restrict__ out, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint2 v = vel[i];
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&v.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&v.y));
+    out[i] = make_float4(a.x, a.y, b.x, b.y);
   }
 }
 
@@ -276,7 +285,9 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
     return true;
   };
   const size_t fbytes = (size_t)s->q * s->n * s->pop_elem;
-  s->partial_blocks = (int)std::min<size_t>((s->n + 255) / 256, 148 * 8);
+  // one macro block per 256 cells up to 4096 blocks (several cells per thread beyond: the block
+  // reductions amortise and the final reduce reads at most 256 KB), one 64-byte partial each
+  s->partial_blocks = (int)std::min<size_t>((s->n + 255) / 256, 4096);
   bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
             create_priority_stream(&s->aux) == cudaSuccess &&
             cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
@@ -498,6 +509,8 @@ int wt_sample(wt_solver* s, wt_stats* out) {
   DeviceGuard g(s->device);
   int rc = ensure_init(s);
   if (rc) return rc;
+  rc = ensure_classified(s);  // the macro pass reads the class byte
+  if (rc) return rc;
   WT_CUDA(s, wt::launch_macro(s), "macro");
   WT_CUDA(s, cudaMemcpyAsync(s->result_host, s->result_dev, 64, cudaMemcpyDeviceToHost, s->stream), "read result");
   WT_CUDA(s, cudaMemcpyAsync(s->err_host, s->err_dev, 4, cudaMemcpyDeviceToHost, s->stream), "read error word");
@@ -553,10 +566,13 @@ int wt_write_populations(wt_solver* s, const void* in, int64_t bytes) {
 int wt_read_velocity(wt_solver* s, float* out4, int64_t n) {
   if (!s || !out4 || (size_t)n != s->n) return WT_E_INVALID;
   DeviceGuard g(s->device);
-  std::vector<__half> h(4 * s->n);
-  WT_CUDA(s, cudaMemcpyAsync(h.data(), s->vel, s->n * 8, cudaMemcpyDeviceToHost, s->stream), "read velocity");
+  // widened on the device, then one copy into the caller's buffer (fastest when it is pinned)
+  if (!s->vel_f32) WT_CUDA(s, cudaMalloc((void**)&s->vel_f32, s->n * 16), "cudaMalloc(velocity readback)");
+  k_vel_to_f32<<<grid_for(s->n), 256, 0, s->stream>>>(s->vel, s->vel_f32, s->n);
+  s->launches++;
+  WT_CUDA(s, cudaGetLastError(), "read velocity");
+  WT_CUDA(s, cudaMemcpyAsync(out4, s->vel_f32, s->n * 16, cudaMemcpyDeviceToHost, s->stream), "read velocity");
   WT_CUDA(s, cudaStreamSynchronize(s->stream), "read velocity");
-  for (size_t i = 0; i < 4 * s->n; i++) out4[i] = __half2float(h[i]);
   return WT_OK;
 }
 

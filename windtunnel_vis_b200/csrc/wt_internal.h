@@ -46,6 +46,7 @@ struct wt_solver {
   uint32_t* bnd_count = nullptr;  // device counter used while building the list
   uint32_t* bnd_count_host = nullptr;  // pinned
   uint2* vel = nullptr;  // half4 (ux, uy, uz, rho) per cell
+  float4* vel_f32 = nullptr;  // f32 copy of `vel` for readback, allocated by the first wt_read_velocity
   float4* meanA = nullptr;
   float* meanB = nullptr;
   double* partials = nullptr;  // per-block partial reductions of the macro pass

@@ -1131,10 +1131,14 @@ __device__ __forceinline__ float warp_max(float v) {
   return v;
 }
 
+// Grid-stride over cells (one per thread when the grid has a block per 256 cells). `cls` (may be NULL)
+// is the class byte: a fluid cell without CLS_NEAR_SOLID has no in-domain solid neighbour, so its
+// 18 link checks are skipped; with NULL every fluid cell checks its links.
 template <class L, class S>
-__global__ void __launch_bounds__(MACRO_THREADS) k_macro(const wt_kparams P, const typename S::T* __restrict__ fin,
+__global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, const typename S::T* __restrict__ fin,
                                                          const uint32_t* __restrict__ flags,
-                                                         const uint32_t* __restrict__ sdf, const Wheels W,
+                                                         const uint32_t* __restrict__ sdf,
+                                                         const uint8_t* __restrict__ cls, const Wheels W,
                                                          uint2* __restrict__ vel, float4* __restrict__ meanA,
                                                          float* __restrict__ meanB, double* __restrict__ partials) {
   typedef typename S::R R;
@@ -1143,23 +1147,34 @@ __global__ void __launch_bounds__(MACRO_THREADS) k_macro(const wt_kparams P, con
   const int NX = P.nx, NY = P.ny, NZ = P.nz;
   const size_t N = P.n;
   const float a = P.ema_alpha;
-  double accF[3] = {0, 0, 0}, accRho = 0, accNref = 0, accNan = 0, accSolid = 0;
+  double accF[3] = {0, 0, 0}, accRho = 0;
+  uint32_t accNref = 0, accNan = 0, accSolid = 0;
   float accMax = 0.0f;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < N; idx += (size_t)gridDim.x * blockDim.x) {
-    const int ix = (int)(idx % (size_t)NX);
-    const int iy = (int)((idx / (size_t)NX) % (size_t)NY);
-    const int iz = (int)(idx / ((size_t)NX * NY));
+    const uint32_t c32 = (uint32_t)idx;  // n < 2^32
+    const int ix = (int)(c32 % (uint32_t)NX);
+    // y and z only on the paths that visit neighbours (cells next to walls, solid cells)
+    auto cell_yz = [&](int& y, int& z) {
+      const uint32_t t = c32 / (uint32_t)NX;
+      y = (int)(t % (uint32_t)NY);
+      z = (int)(t / (uint32_t)NY);
+    };
     auto safe = [&](int x, int y, int z) -> int64_t {
       if (x < 0 || y < 0 || z < 0 || x >= NX || y >= NY || z >= NZ) return -1;
       return (int64_t)cell_id(x, y, z, NX, NY);
     };
     float out[4] = {0.f, 0.f, 0.f, 1.f};
-    if (flags[idx] == 0u) {
-      R f[Q];
-      static_for<Q>([&](auto I) {
-        constexpr int i = I;
-        f[i] = S::ld(fin, (size_t)i * N + idx, (R)Wc<L, i>::v);
-      });
+    // every load of the cell is issued before the first branch: one memory round trip per cell
+    const uint32_t fl = flags[idx];
+    const bool links = cls == nullptr || (cls[idx] & CLS_NEAR_SOLID) != 0;
+    float4 m = meanA[idx];
+    const float mb = meanB[idx];
+    R f[Q];
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      f[i] = S::ld(fin, (size_t)i * N + idx, (R)Wc<L, i>::v);
+    });
+    if (fl == 0u) {
       R rho = f[0], jx = 0, jy = 0, jz = 0;
       static_for<Q>([&](auto I) {
         constexpr int i = I;
@@ -1169,9 +1184,12 @@ __global__ void __launch_bounds__(MACRO_THREADS) k_macro(const wt_kparams P, con
         if constexpr (cy != 0) jy += (R)cy * f[i];
         if constexpr (cz != 0) jz += (R)cz * f[i];
       });
-      const R ux = jx / rho, uy = jy / rho, uz = D3 ? jz / rho : (R)0;
+      const R ir = (R)1 / rho;
+      const R ux = jx * ir, uy = jy * ir, uz = D3 ? jz * ir : (R)0;
       R Fx = 0, Fy = 0, Fz = 0, mvSum = 0, mvW = 0, Cwx = 0, Cwy = 0, Cwz = 0;
-      static_for<Q>([&](auto I) {
+      int iy = 0, iz = 0;
+      if (links) cell_yz(iy, iz);
+      if (links) static_for<Q>([&](auto I) {
         constexpr int i = I;
         if constexpr (i > 0) {
           constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
@@ -1227,19 +1245,20 @@ __global__ void __launch_bounds__(MACRO_THREADS) k_macro(const wt_kparams P, con
       accMax = fmaxf(accMax, bad ? 1.0e6f : (float)uu);
       if ((uint32_t)ix == P.ref_x) {
         accRho += (double)rho;
-        accNref += 1.0;
+        accNref++;
       }
-      accNan += bad ? 1.0 : 0.0;
-      float4 m = meanA[idx];
+      accNan += bad ? 1u : 0u;
       m.x = m.x * (1.0f - a) + out[0] * a;
       m.y = m.y * (1.0f - a) + out[1] * a;
       m.z = m.z * (1.0f - a) + out[2] * a;
       m.w = m.w * (1.0f - a) + out[3] * a;
       meanA[idx] = m;
-      meanB[idx] = meanB[idx] * (1.0f - a) + (float)uu * a;
+      meanB[idx] = mb * (1.0f - a) + (float)uu * a;
     } else {
       // density extrapolated into the solid from fluid face neighbours (wgslLbm.ts:460-466)
       R rs = 0, rn = 0;
+      int iy, iz;
+      cell_yz(iy, iz);
       const int nb[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
 #pragma unroll
       for (int k = 0; k < (D3 ? 6 : 4); k++) {
@@ -1255,14 +1274,13 @@ __global__ void __launch_bounds__(MACRO_THREADS) k_macro(const wt_kparams P, con
         }
       }
       if (rn > (R)0) out[3] = (float)(rs / rn);
-      float4 m = meanA[idx];
       m.x = m.x * (1.0f - a) + out[0] * a;
       m.y = m.y * (1.0f - a) + out[1] * a;
       m.z = m.z * (1.0f - a) + out[2] * a;
       m.w = m.w * (1.0f - a) + out[3] * a;
       meanA[idx] = m;
       meanB[idx] = 0.0f;
-      accSolid += 1.0;
+      accSolid++;
     }
     __half2 h01 = __floats2half2_rn(out[0], out[1]);
     __half2 h23 = __floats2half2_rn(out[2], out[3]);
@@ -1271,17 +1289,30 @@ __global__ void __launch_bounds__(MACRO_THREADS) k_macro(const wt_kparams P, con
     pk.y = *reinterpret_cast<uint32_t*>(&h23);
     vel[idx] = pk;
   }
-  // block reduction: warp shuffles, then one warp over the per-warp values
+  // block reduction. Counts by warp votes / integer reductions; the FP64 sums are shuffled only in
+  // warps that hold a non-zero value (most warps have no wall link and no reference-plane cell).
   __shared__ double sh[MACRO_THREADS / 32][8];
-  double v[8] = {accF[0], accF[1], accF[2], 0.0, accRho, accNref, accNan, accSolid};
-  float mx = warp_max(accMax);
-#pragma unroll
-  for (int k = 0; k < 8; k++)
-    if (k != 3) v[k] = warp_sum(v[k]);
+  const unsigned full = 0xffffffffu;
+  if (__any_sync(full, accF[0] != 0.0 || accF[1] != 0.0 || accF[2] != 0.0)) {
+    accF[0] = warp_sum(accF[0]);
+    accF[1] = warp_sum(accF[1]);
+    accF[2] = warp_sum(accF[2]);
+  }
+  if (__any_sync(full, accNref != 0u)) accRho = warp_sum(accRho);
+  const float mx = warp_max(accMax);
+  const uint32_t nref = __reduce_add_sync(full, accNref);
+  const uint32_t nnan = __reduce_add_sync(full, accNan);
+  const uint32_t nsolid = __reduce_add_sync(full, accSolid);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < 8; k++) sh[wid][k] = k == 3 ? (double)mx : v[k];
+    sh[wid][0] = accF[0];
+    sh[wid][1] = accF[1];
+    sh[wid][2] = accF[2];
+    sh[wid][3] = (double)mx;
+    sh[wid][4] = accRho;
+    sh[wid][5] = (double)nref;
+    sh[wid][6] = (double)nnan;
+    sh[wid][7] = (double)nsolid;
   }
   __syncthreads();
   if (wid == 0) {
@@ -1300,17 +1331,26 @@ __global__ void __launch_bounds__(MACRO_THREADS) k_macro(const wt_kparams P, con
   }
 }
 
-// final reduction of the per-block partials (one block; fixed order, deterministic)
-__global__ void __launch_bounds__(256) k_reduce_partials(const double* __restrict__ partials, int nblocks,
-                                                        double* __restrict__ result) {
-  __shared__ double sh[8][8];
+// final reduction of the per-block partials (one block of REDUCE_THREADS; fixed order, so the
+// result is deterministic for a given number of partials)
+constexpr int REDUCE_THREADS = 1024;
+
+__global__ void __launch_bounds__(REDUCE_THREADS) k_reduce_partials(const double* __restrict__ partials,
+                                                                   int nblocks, double* __restrict__ result) {
+  __shared__ double sh[REDUCE_THREADS / 32][8];
   double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 4
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const double x = partials[(size_t)b * 8 + k];
-      v[k] = k == 3 ? fmax(v[k], x) : v[k] + x;
-    }
+    const double2* p2 = reinterpret_cast<const double2*>(partials + (size_t)b * 8);
+    const double2 a0 = p2[0], a1 = p2[1], a2 = p2[2], a3 = p2[3];
+    v[0] += a0.x;
+    v[1] += a0.y;
+    v[2] += a1.x;
+    v[3] = fmax(v[3], a1.y);
+    v[4] += a2.x;
+    v[5] += a2.y;
+    v[6] += a3.x;
+    v[7] += a3.y;
   }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
@@ -1489,12 +1529,12 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
 template <class L, class S>
 static cudaError_t macro_t(wt_solver* s) {
   k_macro<L, S><<<s->partial_blocks, MACRO_THREADS, 0, s->stream>>>(
-      s->kp, (const typename S::T*)s->f[s->parity], s->flags, s->sdf, s->wheels, s->vel, s->meanA, s->meanB,
+      s->kp, (const typename S::T*)s->f[s->parity], s->flags, s->sdf, s->cls, s->wheels, s->vel, s->meanA, s->meanB,
       s->partials);
   s->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_reduce_partials<<<1, 256, 0, s->stream>>>(s->partials, s->partial_blocks, s->result_dev);
+  k_reduce_partials<<<1, REDUCE_THREADS, 0, s->stream>>>(s->partials, s->partial_blocks, s->result_dev);
   s->launches++;
   return cudaGetLastError();
 }
@@ -1553,11 +1593,11 @@ template <class L, class S>
 cudaError_t sample_noalloc_t(const wt_kparams& kp, const void* fin, const uint32_t* flags, const uint32_t* sdf,
                              const Wheels& W, uint2* vel, float4* meanA, float* meanB, double* scratch, int nblocks,
                              double* result, cudaStream_t st) {
-  k_macro<L, S><<<nblocks, MACRO_THREADS, 0, st>>>(kp, (const typename S::T*)fin, flags, sdf, W, vel, meanA, meanB,
-                                                    scratch);
+  k_macro<L, S><<<nblocks, MACRO_THREADS, 0, st>>>(kp, (const typename S::T*)fin, flags, sdf, nullptr, W, vel, meanA,
+                                                    meanB, scratch);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_reduce_partials<<<1, 256, 0, st>>>(scratch, nblocks, result);
+  k_reduce_partials<<<1, REDUCE_THREADS, 0, st>>>(scratch, nblocks, result);
   return cudaGetLastError();
 }
 

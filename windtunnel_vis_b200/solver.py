@@ -171,8 +171,14 @@ class Solver:
         a = np.ascontiguousarray(a, POP_DTYPE[self.precision]).ravel()
         self._check(self._lib.wt_write_populations(self._h, _ptr(a), a.nbytes))
 
-    def read_velocity(self):
-        out = np.empty((self.n, 4), np.float32)
+    def read_velocity(self, out=None):
+        """(ux, uy, uz, rho) per cell as float32, shape (n, 4): the velocity texture the renderer
+        samples. `out` (optional) is a C-contiguous float32 array of that shape to fill, e.g. a
+        view of pinned host memory."""
+        if out is None:
+            out = np.empty((self.n, 4), np.float32)
+        elif out.dtype != np.float32 or out.size != 4 * self.n or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float32 array of n x 4 values")
         self._check(self._lib.wt_read_velocity(self._h, _ptr(out), self.n))
         return out
 
