@@ -148,7 +148,7 @@ def test_autotune_keeps_state(gpu):
         s.set_wheels(wheels)
         s.step(5)
     shape = a.autotune(3)
-    assert shape[0] in (0, 1)
+    assert shape[0] in (0, 2, 3, 4) and shape[1] in (1, 2, 4)  # occupancy hint, cells per thread
     a.step(5)
     b.step(5)
     np.testing.assert_allclose(a.read_populations().astype(np.float32), b.read_populations().astype(np.float32),

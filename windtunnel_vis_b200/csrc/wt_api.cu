@@ -68,7 +68,8 @@ int64_t bytes_for(const wt_dims* d, int prec) {
 
 void free_all(wt_solver* s) {
   void* bufs[] = {s->f[0], s->f[1], s->flags, s->sdf, s->cls, s->vel, s->vel_f32, s->meanA, s->meanB,
-                  s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count};
+                  s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count,
+                  s->bcell, s->brec, s->bgam};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->result_host) cudaFreeHost(s->result_host);
@@ -129,11 +130,19 @@ unsigned grid_for(size_t n) {
   return (unsigned)(b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b));
 }
 
+// Class bytes, boundary list and link records after a geometry change; link records alone after a
+// change of parameters or wheels (they hold the wall and inlet terms).
 int ensure_classified(wt_solver* s) {
-  if (!s->cls_dirty) return WT_OK;
-  invalidate_graphs(s);
-  WT_CUDA(s, wt::launch_classify(s), "classify");
-  s->cls_dirty = false;
+  if (s->cls_dirty) {
+    invalidate_graphs(s);
+    WT_CUDA(s, wt::launch_classify(s), "classify");
+    s->cls_dirty = false;
+    s->tab_dirty = false;
+  } else if (s->tab_dirty) {
+    invalidate_graphs(s);
+    WT_CUDA(s, wt::launch_boundary_table(s), "boundary links");
+    s->tab_dirty = false;
+  }
   return WT_OK;
 }
 
@@ -161,6 +170,7 @@ int ensure_init(wt_solver* s) {
   if (!s->pending_init) return WT_OK;
   WT_CUDA(s, wt::launch_init(s), "init");
   s->pending_init = false;
+  s->solid_ok[0] = s->solid_ok[1] = true;  // init writes the rest state into solid cells
   return WT_OK;
 }
 
@@ -347,6 +357,7 @@ int wt_set_params(wt_solver* s, const wt_params* p) {
   s->params = *p;
   wt_pack_params(&s->dims, p, &s->kp);
   invalidate_graphs(s);
+  s->tab_dirty = true;
   return WT_OK;
 }
 
@@ -405,6 +416,7 @@ int wt_upload_sdf(wt_solver* s, const float* d, int64_t n) {
 int wt_set_wheels(wt_solver* s, const wt_wheel* w, int32_t count) {
   if (!s || (count > 0 && !w) || count < 0) return WT_E_INVALID;
   invalidate_graphs(s);
+  s->tab_dirty = true;
   std::memset(&s->wheels, 0, sizeof s->wheels);
   const int n = count < 16 ? count : 16;
   s->wheels.count = (uint32_t)n;
@@ -484,7 +496,14 @@ int wt_step(wt_solver* s, int32_t steps) {
   if (!rc) rc = ensure_init(s);
   if (rc) return rc;
   int32_t k = 0;
-  if (steps >= 2) {
+  // single steps until both buffers hold the rest state in their solid cells (the steps that
+  // write it are not part of the captured graphs)
+  for (; k < steps && !(s->solid_ok[0] && s->solid_ok[1]); k++) {
+    cudaError_t e = wt::launch_stream_collide(s, s->f[s->parity], s->f[s->parity ^ 1]);
+    if (e != cudaSuccess) return cuda_fail(s, e, "stream_collide");
+    s->parity ^= 1;
+  }
+  if (steps - k >= 2) {
     // pairs of steps replay the captured ping-pong graph of the current parity
     if (!s->step_graph[s->parity]) {
       rc = capture_step_graph(s, s->parity);
@@ -560,6 +579,7 @@ int wt_write_populations(wt_solver* s, const void* in, int64_t bytes) {
   WT_CUDA(s, cudaMemcpyAsync(s->f[s->parity], in, (size_t)bytes, cudaMemcpyHostToDevice, s->stream), "write populations");
   WT_CUDA(s, cudaStreamSynchronize(s->stream), "write populations");
   s->pending_init = false;
+  s->solid_ok[s->parity] = false;  // the written solid cells are read as written until rewritten
   return WT_OK;
 }
 

@@ -36,6 +36,7 @@ struct wt_solver {
   uint32_t* sdf = nullptr;
   uint8_t* cls = nullptr;
   bool cls_dirty = true;
+  bool tab_dirty = false;  // link records need a rebuild (parameters or wheels changed)
   // cells the vectorised bulk kernel leaves to the boundary kernel: every cell of an aligned group
   // of `gs` cells along x that holds a solid cell, a fluid cell next to a solid, or lies on a
   // domain face (built by launch_classify)
@@ -45,6 +46,14 @@ struct wt_solver {
   int gs = 1;
   uint32_t* bnd_count = nullptr;  // device counter used while building the list
   uint32_t* bnd_count_host = nullptr;  // pinned
+  // link records of the listed cells (k_boundary_build), applied every step by k_boundary_tab
+  uint2* bcell = nullptr;  // {cell, BC_* bits} per listed cell
+  uint4* brec = nullptr;   // {a1, a2, alpha, beta} per link
+  float* bgam = nullptr;   // gamma per link
+  size_t btab_cap = 0;     // cells the record buffers hold
+  // solid cells of f[b] hold the rest state (the reference rewrites them every step; here they
+  // are written once per buffer after a classification or a raw population write)
+  bool solid_ok[2] = {false, false};
   uint2* vel = nullptr;  // half4 (ux, uy, uz, rho) per cell
   float4* vel_f32 = nullptr;  // f32 copy of `vel` for readback, allocated by the first wt_read_velocity
   float4* meanA = nullptr;
@@ -72,6 +81,7 @@ namespace wt {
 
 int lbm_block_x(const wt_solver* s);
 cudaError_t launch_classify(wt_solver* s);
+cudaError_t launch_boundary_table(wt_solver* s);
 cudaError_t launch_init(wt_solver* s);
 cudaError_t launch_stream_collide(wt_solver* s, const void* fin, void* fout);
 cudaError_t launch_macro(wt_solver* s);

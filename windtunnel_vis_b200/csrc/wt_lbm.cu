@@ -852,7 +852,8 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
   const int iz = blockIdx.z;
   if (x0 >= NX || iy >= NY) return;
-  // rows on the domain faces and groups holding solid / near-solid cells belong to k_boundary
+  // rows on the domain faces belong to k_face_v, groups holding solid / near-solid cells to
+  // k_boundary_tab (fluid cells) or to nobody (solid cells keep the rest state)
   if (iy == 0 || iy == NY - 1 || (D3 && (iz == 0 || iz == NZ - 1))) return;
   const uint32_t N = P.n;
   const uint32_t sy = (uint32_t)NX, sz = (uint32_t)NX * (uint32_t)NY;
@@ -860,7 +861,7 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
   uint32_t cv;
   if (gs == 4) cv = __ldg(reinterpret_cast<const unsigned int*>(cls + (idx0 & ~3u)));
   else cv = __ldg(reinterpret_cast<const unsigned short*>(cls + idx0));
-  // groups holding solid / near-solid cells are written by k_boundary; their loads are still
+  // groups holding solid / near-solid cells are not written here; their loads are still
   // issued (every address is inside the domain for an interior row) so that the class byte does
   // not add a memory round trip in front of the population loads, and only the stores are skipped
   const bool clean = (cv & 0x03030303u) == 0u;
@@ -926,7 +927,7 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
 // roof and sides, bounce-back of the cell's own opposite population plus the belt term on a
 // no-slip or moving floor, and the inlet equilibrium / zero-gradient outlet as in the bulk. Floor
 // rows with bounce-back collide with BGK and the tauWall floor, like the reference's wall cells.
-// Groups holding a solid or a fluid cell next to a solid are left to k_boundary.
+// Groups holding a solid or a fluid cell next to a solid are left to k_boundary_tab.
 template <class L, class S>
 __global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kparams P,
                                                 const typename S::T* __restrict__ fin,
@@ -1054,43 +1055,235 @@ __global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kpara
   else collide_shifted2<L, false>(P, h, x0, emit);
 }
 
-// Groups holding a solid or a fluid cell next to a solid (listed by k_boundary_list): one thread
-// per listed cell, reference-exact boundary rules.
-template <class L, class S>
-__global__ void __launch_bounds__(128) k_boundary(const __grid_constant__ wt_kparams P,
-                                                  const typename S::T* __restrict__ fin,
-                                                  typename S::T* __restrict__ fout,
-                                                  const uint8_t* __restrict__ cls,
-                                                  const uint32_t* __restrict__ flags,
-                                                  const uint32_t* __restrict__ sdf,
-                                                  const __grid_constant__ Wheels W,
-                                                  const uint32_t* __restrict__ list, uint32_t count) {
-  typedef typename S::R R;
-  constexpr int Q = L::Q;
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= count) return;
-  const uint32_t c = list[t];
-  const uint32_t NX = P.nx, NY = P.ny;
-  const int ix = (int)(c % NX), iy = (int)((c / NX) % NY), iz = (int)(c / (NX * NY));
-  const size_t N = P.n;
-  const uint8_t cl = cls[c];
-  if (cl & CLS_SOLID) {
-    static_for<Q>([&](auto I) {
-      constexpr int i = I;
-      fout[(size_t)i * N + c] = S::solid((R)Wc<L, i>::v);
-    });
-    return;
-  }
-  R fo[Q];
-  cell_general<L, S>(P, fin, flags, sdf, W, ix, iy, iz, cl, fo);
-  static_for<Q>([&](auto I) {
-    constexpr int i = I;
-    S::st(fout, (size_t)i * N + c, fo[i], (R)Wc<L, i>::v);
+// ---------------------------------------------------------------------------------------------
+// cells next to walls: per-link recipes built at classification, applied every step
+// ---------------------------------------------------------------------------------------------
+// Every incoming population of a fluid cell next to a wall is an affine combination of at most
+// two stored populations, v = alpha * F[a1] + beta * F[a2] + gamma: an interior, mirrored or
+// periodic pull has alpha = 1; floor bounce-back adds the belt term in gamma; a Bouzidi link mixes
+// f_opp(x) with f_opp(x + c_i) (q < 1/2) or f_i(x) (q > 1/2) and carries the wheel's moving-wall
+// term and its mass fix in gamma; an inlet link is gamma alone. Geometry, parameters and wheels
+// are fixed between classifications, so k_boundary_build evaluates the reference's rules
+// (wgslLbm.ts:138-175, 276-291; the same rules as cell_general) once per cell and link, and
+// k_boundary_tab applies them every step with one record load and two gathers per link, no
+// dependent flag or distance loads. The FP16 shift is folded into gamma: every population a link
+// of direction i reads has the weight w_i (direction i, its opposite, or a mirror image of i).
+//
+// Records are stored per block of BT<L>::CELLS cells as [block][link][cell]; thread t of a block
+// handles (link, cell) = (t / CELLS, t % CELLS), so record loads are contiguous.
+template <class L> struct BT {
+  static constexpr int CELLS = 256 / L::Q;  // 13 for D3Q19, 28 for D2Q9
+};
+enum : uint32_t { BC_WALL = 1u, BC_GWALL = 2u };
+
+template <class L>
+__device__ __forceinline__ float lattice_w(int i) {
+  float w = 0.f;
+  static_for<L::Q>([&](auto I) {
+    constexpr int j = I;
+    if (i == j) w = (float)Wc<L, j>::v;
   });
+  return w;
 }
 
-// Builds the boundary list (every cell of a group holding a solid or near-solid cell): pass 0
-// counts, pass 1 writes (warp-aggregated slots, in x order inside each warp).
+// one thread per listed fluid cell; writes its cell word {cell, BC_* bits} and its Q link records
+template <class L, class S>
+__global__ void __launch_bounds__(128) k_boundary_build(const __grid_constant__ wt_kparams P,
+                                                        const uint32_t* __restrict__ flags,
+                                                        const uint32_t* __restrict__ sdf,
+                                                        const uint8_t* __restrict__ cls,
+                                                        const __grid_constant__ Wheels W,
+                                                        const uint32_t* __restrict__ list, uint32_t count,
+                                                        uint2* __restrict__ bcell, uint4* __restrict__ rec,
+                                                        float* __restrict__ gam) {
+  constexpr int Q = L::Q;
+  constexpr bool D3 = L::DIM == 3;
+  constexpr int CB = BT<L>::CELLS;
+  constexpr bool SHIFT = S::PREC == WT_PREC_F16;
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const uint32_t c = list[k];
+  const int NX = P.nx, NY = P.ny, NZ = P.nz;
+  const uint32_t N = P.n;  // q * n < 2^32 on the vectorised path
+  const int ix = (int)(c % (uint32_t)NX);
+  const int iy = (int)((c / (uint32_t)NX) % (uint32_t)NY);
+  const int iz = (int)(c / ((uint32_t)NX * (uint32_t)NY));
+  auto cid = [&](int x, int y, int z) -> uint32_t { return (uint32_t)x + (uint32_t)NX * ((uint32_t)y + (uint32_t)NY * (uint32_t)z); };
+  const uint8_t cl = cls[c];
+  const bool near = (cl & CLS_NEAR_SOLID) != 0;
+  const float U = P.uin;
+  const float belt = (P.ground == 2u && !(cl & CLS_BELT_STILL)) ? 1.0f : 0.0f;
+  const uint32_t sdf_raw = sdf[c];
+  const float sdf_self = (P.interp != 0u && sdf_raw != 0u) ? __uint_as_float(~sdf_raw) : -1.0f;
+  const size_t rb = (size_t)(k / CB) * Q * CB + (k % CB);  // record of link i: rb + i * CB
+  float ga[Q];
+  uint32_t bits = 0, wm = 0;
+  float mvSum = 0.f, mvW = 0.f;
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+    constexpr int io = opp<L>(i);
+    const float w = (float)Wc<L, i>::v;
+    uint32_t A = (uint32_t)i * N + c, B = 0xffffffffu;
+    float alpha = 1.f, beta = 0.f, gamma = 0.f;
+    if constexpr (i > 0) {
+      int sx = ix - cx;
+      const int sy = iy - cy, sz = D3 ? iz - cz : 0;
+      if constexpr (cx < 0) sx = min(sx, NX - 1);
+      const bool yOut = cy > 0 ? sy < 0 : (cy < 0 ? sy >= NY : false);
+      const bool zOut = D3 ? (cz > 0 ? sz < 0 : (cz < 0 ? sz >= NZ : false)) : false;
+      const int sxc = min(max(sx, 0), NX - 1);
+      const int szc = D3 ? min(max(sz, 0), NZ - 1) : 0;
+      if (cx > 0 && sx < 0) {
+        // inlet: equilibrium at (rho_in, U)
+        const float cu = 1.0f * U;
+        alpha = 0.f;
+        gamma = w * P.rho_in * (1.0f + 3.0f * cu + 4.5f * cu * cu - 1.5f * U * U);
+      } else if (cy > 0 && yOut && P.ground != 0u) {
+        // no-slip / moving floor: bounce-back plus the belt term
+        bits |= BC_WALL | BC_GWALL;
+        A = (uint32_t)io * N + c;
+        if constexpr (cx != 0) gamma = belt * ((float)(6.0 * Wc<L, i>::v * cx) * P.u_ground);
+      } else if (D3 && yOut && zOut) {
+        A = (uint32_t)mirYZ<L>(i) * N + cid(sxc, iy, iz);
+      } else if (yOut) {
+        A = (uint32_t)mirY<L>(i) * N + cid(sxc, iy, szc);
+      } else if (D3 && zOut) {
+        A = P.side_mode == 1u ? (uint32_t)i * N + cid(sxc, sy, (sz + NZ) % NZ)
+                              : (uint32_t)mirZ<L>(i) * N + cid(sxc, sy, iz);
+      } else {
+        const uint32_t sc = cid(sxc, sy, sz);
+        const uint32_t fs = near ? flags[sc] : 0u;
+        if (fs == 0u) {
+          A = (uint32_t)i * N + sc;
+        } else {
+          // interpolated bounce-back (Bouzidi) on a solid source
+          bits |= BC_WALL;
+          A = (uint32_t)io * N + c;
+          float q = 0.5f;
+          if (P.interp != 0u) {
+            const uint32_t rs = sdf[sc];
+            const float a = sdf_self, b = rs != 0u ? __uint_as_float(~rs) : -1.0f;
+            if (!(a < 0.f || b < 0.f || a + b < 1e-6f)) {
+              q = a / (a + b);
+              q = q < 0.01f ? 0.01f : (q > 0.99f ? 0.99f : q);
+            }
+          }
+          if (q < 0.5f) {
+            const int ax = ix + cx, ay = iy + cy, az = D3 ? iz + cz : 0;
+            const bool inA = ax >= 0 && ay >= 0 && az >= 0 && ax < NX && ay < NY && az < NZ;
+            if (inA && flags[cid(ax, ay, az)] == 0u) {
+              alpha = 2.0f * q;
+              beta = 1.0f - 2.0f * q;
+              B = (uint32_t)io * N + cid(ax, ay, az);
+            } else {
+              q = 0.5f;
+            }
+          } else if (q > 0.5f) {
+            alpha = 0.5f / q;
+            beta = 1.0f - 0.5f / q;
+            B = (uint32_t)i * N + c;
+          }
+          if ((fs >> 8u) != 0u) {
+            float ux, uy, uz;
+            wheel_vel<float>(P, W, (fs >> 8u) - 1u, 0.5f * (float)(ix + sxc) + 0.5f, 0.5f * (float)(iy + sy) + 0.5f,
+                             0.5f * (float)(iz + sz) + 0.5f, ux, uy, uz);
+            const float dot = (float)cx * ux + (float)cy * uy + (float)cz * uz;
+            const float mv = (float)(6.0 * Wc<L, i>::v) * dot * (q > 0.5f ? 0.5f / q : 1.0f);
+            gamma += mv;
+            mvSum += mv;
+            mvW += w;
+            wm |= 1u << i;
+          }
+        }
+      }
+    }
+    if (B == 0xffffffffu) B = A;
+    ga[i] = gamma;
+    rec[rb + (size_t)i * CB] = make_uint4(A, B, __float_as_uint(alpha), __float_as_uint(SHIFT ? alpha + beta : beta));
+  });
+  // wheel links: remove the net mass of the moving-wall terms (wgslLbm.ts:289-291)
+  const float corr = mvW > 0.f ? mvSum / mvW : 0.f;
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    float g = ga[i];
+    if (wm & (1u << i)) g -= (float)Wc<L, i>::v * corr;
+    if constexpr (SHIFT) {
+      // stored h = f - w_i for both sources: alpha (h1 + w) + beta (h2 + w) + g
+      const uint4 r = rec[rb + (size_t)i * CB];
+      const float alpha = __uint_as_float(r.z), ab = __uint_as_float(r.w);
+      const float beta = ab - alpha;
+      rec[rb + (size_t)i * CB] = make_uint4(r.x, r.y, r.z, __float_as_uint(beta));
+      g += ab * (float)Wc<L, i>::v;
+    }
+    gam[rb + (size_t)i * CB] = g;
+  });
+  bcell[k] = make_uint2(c, bits);
+}
+
+// Applies the link records: phase 1 gathers every link value of the block's cells (one thread per
+// link), phase 2 collides one cell per thread on the values staged in shared memory, phase 3 stores
+// the post-collision populations (one thread per population).
+template <class L, class S>
+__global__ void __launch_bounds__(256) k_boundary_tab(const __grid_constant__ wt_kparams P,
+                                                      const typename S::T* __restrict__ fin,
+                                                      typename S::T* __restrict__ fout,
+                                                      const uint2* __restrict__ bcell, const uint4* __restrict__ rec,
+                                                      const float* __restrict__ gam, uint32_t count) {
+  constexpr int Q = L::Q;
+  constexpr int CB = BT<L>::CELLS;
+  __shared__ float sh[Q * CB];
+  __shared__ uint2 shc[CB];
+  const int t = threadIdx.x;
+  const uint32_t k0 = blockIdx.x * CB;
+  const int nc = (int)min((uint32_t)CB, count - k0);
+  const int li = t / CB, lc = t - li * CB;
+  const bool act = li < Q && lc < nc;
+  if (t < nc) shc[t] = bcell[k0 + t];
+  if (act) {
+    const size_t r = ((size_t)blockIdx.x * Q + li) * CB + lc;
+    const uint4 R4 = rec[r];
+    const float g = gam[r];
+    const float x1 = S::cvt(__ldg(fin + R4.x), 0.0f), x2 = S::cvt(__ldg(fin + R4.y), 0.0f);
+    sh[li * CB + lc] = fmaf(__uint_as_float(R4.z), x1, fmaf(__uint_as_float(R4.w), x2, g));
+  }
+  __syncthreads();
+  if (t < nc) {
+    float f[Q], fo[Q];
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      f[i] = sh[i * CB + t];
+    });
+    const uint2 hc = shc[t];
+    const int ix = (int)(hc.x % P.nx);
+    collide_full<L, float>(P, f, ix, (hc.y & BC_WALL) != 0u, (hc.y & BC_GWALL) != 0u, fo);
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      sh[i * CB + t] = fo[i];
+    });
+  }
+  __syncthreads();
+  if (act) S::st(fout, (size_t)li * P.n + shc[lc].x, sh[li * CB + lc], lattice_w<L>(li));
+}
+
+// Rest state written into the solid cells of one population buffer.
+template <class L, class S>
+__global__ void __launch_bounds__(256) k_fill_solid(const __grid_constant__ wt_kparams P,
+                                                    const uint8_t* __restrict__ cls, typename S::T* __restrict__ f) {
+  const size_t N = P.n;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < N; idx += (size_t)gridDim.x * blockDim.x) {
+    if (cls[idx] & CLS_SOLID) {
+      static_for<L::Q>([&](auto I) {
+        constexpr int i = I;
+        f[(size_t)i * N + idx] = S::solid((typename S::R)Wc<L, i>::v);
+      });
+    }
+  }
+}
+
+// Builds the boundary list (every fluid cell of a group holding a solid or near-solid cell; solid
+// cells keep the rest state and need no per-step work): pass 0 counts, pass 1 writes
+// (warp-aggregated slots, in x order inside each warp).
 template <class L>
 __global__ void __launch_bounds__(256) k_boundary_list(const __grid_constant__ wt_kparams P,
                                                        const uint8_t* __restrict__ cls, int gs,
@@ -1106,7 +1299,7 @@ __global__ void __launch_bounds__(256) k_boundary_list(const __grid_constant__ w
       const uint32_t g0 = c - (c % NX) % (uint32_t)gs;
       bool dirty = false;
       for (int k = 0; k < gs; k++) dirty = dirty || (cls[g0 + k] & CLS_BOUNDARY) != 0;
-      sel = dirty;
+      sel = dirty && (cls[c] & CLS_SOLID) == 0;
     }
     const uint32_t ball = __ballot_sync(0xffffffffu, sel);
     if (ball == 0u) continue;
@@ -1372,6 +1565,22 @@ __global__ void __launch_bounds__(REDUCE_THREADS) k_reduce_partials(const double
 // ---------------------------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------------------------
+#define WT_DISPATCH(FN, ...)                                                                  \
+  do {                                                                                        \
+    if (s->is3d) {                                                                            \
+      if (s->prec == WT_PREC_F16) return FN<D3Q19, StF16>(__VA_ARGS__);                      \
+      if (s->prec == WT_PREC_F64) return FN<D3Q19, StF64>(__VA_ARGS__);                      \
+      return FN<D3Q19, StF32>(__VA_ARGS__);                                                  \
+    }                                                                                         \
+    if (s->prec == WT_PREC_F16) return FN<D2Q9, StF16>(__VA_ARGS__);                         \
+    if (s->prec == WT_PREC_F64) return FN<D2Q9, StF64>(__VA_ARGS__);                         \
+    return FN<D2Q9, StF32>(__VA_ARGS__);                                                     \
+  } while (0)
+
+static bool offsets32(const wt_solver* s) { return (uint64_t)s->q * (uint64_t)s->n < (1ull << 32); }
+
+static unsigned grid_cells(const wt_solver* s) { return (unsigned)std::min<size_t>((s->n + 255) / 256, 148 * 16); }
+
 int lbm_block_x(const wt_solver* s) {
   if (s->block_x > 0) return s->block_x;
   const int nx = s->dims.nx;
@@ -1420,16 +1629,59 @@ static cudaError_t boundary_list_t(wt_solver* s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_classify(wt_solver* s) {
-  // group size of the bulk kernel's clean / boundary decision along x
-  s->gs = s->dims.nx % 4 == 0 ? 4 : (s->dims.nx % 2 == 0 ? 2 : 1);
-  cudaError_t e = s->is3d ? classify_t<D3Q19>(s) : classify_t<D2Q9>(s);
+// Link records of the listed cells (vectorised f16 / f32 path only; see k_boundary_build).
+template <class L, class S>
+static cudaError_t boundary_table_t(wt_solver* s) {
+  if constexpr (S::PREC == WT_PREC_F64) {
+    return cudaSuccess;
+  } else {
+    if (s->nbnd == 0 || !offsets32(s)) return cudaSuccess;
+    constexpr int CB = BT<L>::CELLS;
+    const size_t nblk = (s->nbnd + CB - 1) / CB;
+    cudaError_t e;
+    if (nblk * CB > s->btab_cap) {
+      cudaFree(s->bcell);
+      cudaFree(s->brec);
+      cudaFree(s->bgam);
+      s->bcell = nullptr;
+      s->brec = nullptr;
+      s->bgam = nullptr;
+      s->btab_cap = 0;
+      if ((e = cudaMalloc((void**)&s->bcell, nblk * CB * sizeof(uint2))) != cudaSuccess) return e;
+      if ((e = cudaMalloc((void**)&s->brec, nblk * CB * L::Q * sizeof(uint4))) != cudaSuccess) return e;
+      if ((e = cudaMalloc((void**)&s->bgam, nblk * CB * L::Q * sizeof(float))) != cudaSuccess) return e;
+      s->btab_cap = nblk * CB;
+    }
+    k_boundary_build<L, S><<<(s->nbnd + 127) / 128, 128, 0, s->stream>>>(
+        s->kp, s->flags, s->sdf, s->cls, s->wheels, s->bnd, s->nbnd, s->bcell, s->brec, s->bgam);
+    s->launches++;
+    return cudaGetLastError();
+  }
+}
+
+template <class L, class S>
+static cudaError_t classify_all_t(wt_solver* s) {
+  cudaError_t e = classify_t<L>(s);
   if (e != cudaSuccess) return e;
+  // solid cells are written with the rest state when each buffer is next a step's output
+  s->solid_ok[0] = s->solid_ok[1] = false;
   if (s->gs == 1) {
     s->nbnd = 0;
     return cudaSuccess;
   }
-  return s->is3d ? boundary_list_t<D3Q19>(s) : boundary_list_t<D2Q9>(s);
+  if ((e = boundary_list_t<L>(s)) != cudaSuccess) return e;
+  return boundary_table_t<L, S>(s);
+}
+
+cudaError_t launch_boundary_table(wt_solver* s) {
+  if (s->gs == 1) return cudaSuccess;
+  WT_DISPATCH(boundary_table_t, s);
+}
+
+cudaError_t launch_classify(wt_solver* s) {
+  // group size of the bulk kernel's clean / boundary decision along x
+  s->gs = s->dims.nx % 4 == 0 ? 4 : (s->dims.nx % 2 == 0 ? 2 : 1);
+  WT_DISPATCH(classify_all_t, s);
 }
 
 template <class L, class S>
@@ -1446,7 +1698,6 @@ static cudaError_t init_t(wt_solver* s) {
 }
 
 // the vectorised kernel indexes populations with 32-bit element offsets
-static bool offsets32(const wt_solver* s) { return (uint64_t)s->q * (uint64_t)s->n < (1ull << 32); }
 
 template <class L, class S>
 static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
@@ -1464,6 +1715,14 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
       const dim3 block(bx, by);
       const dim3 grid((runs + bx - 1) / bx, (s->dims.ny + by - 1) / by, s->dims.nz);
       cudaError_t e = cudaSuccess;
+      // no kernel of this path writes solid cells: the output buffer gets the rest state once
+      const int out = fout == s->f[0] ? 0 : 1;
+      if (!s->solid_ok[out]) {
+        k_fill_solid<L, S><<<grid_cells(s), 256, 0, s->stream>>>(s->kp, s->cls, (typename S::T*)fout);
+        s->launches++;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        s->solid_ok[out] = true;
+      }
       // face rows and the per-cell boundary list on the auxiliary stream, overlapping the bulk
       cudaStream_t bs = s->aux ? s->aux : s->stream;
       if (s->aux) {
@@ -1482,9 +1741,9 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
       }
       if (s->nbnd > 0) {
-        k_boundary<L, S><<<(s->nbnd + 127) / 128, 128, 0, bs>>>(s->kp, (const typename S::T*)fin,
-                                                                (typename S::T*)fout, s->cls, s->flags, s->sdf,
-                                                                s->wheels, s->bnd, s->nbnd);
+        constexpr int CB = BT<L>::CELLS;
+        k_boundary_tab<L, S><<<(s->nbnd + CB - 1) / CB, 256, 0, bs>>>(
+            s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd);
         s->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
       }
@@ -1523,6 +1782,7 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
   k_stream_collide<L, S><<<row_grid(s, bx), bx, 0, s->stream>>>(
       s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->flags, s->sdf, s->wheels);
   s->launches++;
+  s->solid_ok[fout == s->f[0] ? 0 : 1] = true;  // this kernel writes the solid cells itself
   return cudaGetLastError();
 }
 
@@ -1539,17 +1799,6 @@ static cudaError_t macro_t(wt_solver* s) {
   return cudaGetLastError();
 }
 
-#define WT_DISPATCH(FN, ...)                                                                  \
-  do {                                                                                        \
-    if (s->is3d) {                                                                            \
-      if (s->prec == WT_PREC_F16) return FN<D3Q19, StF16>(__VA_ARGS__);                      \
-      if (s->prec == WT_PREC_F64) return FN<D3Q19, StF64>(__VA_ARGS__);                      \
-      return FN<D3Q19, StF32>(__VA_ARGS__);                                                  \
-    }                                                                                         \
-    if (s->prec == WT_PREC_F16) return FN<D2Q9, StF16>(__VA_ARGS__);                         \
-    if (s->prec == WT_PREC_F64) return FN<D2Q9, StF64>(__VA_ARGS__);                         \
-    return FN<D2Q9, StF32>(__VA_ARGS__);                                                     \
-  } while (0)
 
 cudaError_t launch_init(wt_solver* s) { WT_DISPATCH(init_t, s); }
 cudaError_t launch_stream_collide(wt_solver* s, const void* fin, void* fout) { WT_DISPATCH(sc_t, s, fin, fout); }

@@ -190,8 +190,9 @@ class Solver:
 
     # ---- launch shape ------------------------------------------------------------------------
     def set_launch(self, kernel, param, bx=0, by=0):
-        """kernel 0: register-fed, param = cells per thread (1, 2, 4); kernel 1: TMA-staged,
-        param = pipeline stages (2..4)."""
+        """Stream-collide launch: kernel = occupancy hint (0 none, 2..4 CTAs of 256 threads per
+        SM), param = cells per thread along x (1 = the scalar kernel, 2 or 4), block bx x by
+        (0 = default)."""
         self._check(self._lib.wt_set_launch(self._h, int(kernel), int(param), int(bx), int(by)))
 
     def get_launch(self):
