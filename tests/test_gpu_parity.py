@@ -54,10 +54,14 @@ CASES = [(p, k) for p in ("f32", "f16") for k in LAUNCHES] + [("f64", "reg1")]
 @pytest.mark.parametrize("pset", list(PARAM_SETS))
 @pytest.mark.parametrize("dims", [(32, 14, 12), (48, 16, 1), (160, 12, 1)])
 def test_stream_collide_matches_oracle(gpu, oracle, dims, pset, prec, launch):
-    params = dict(PARAM_SETS[pset], precision=prec)
+    _check_against_oracle(oracle, dims, dict(PARAM_SETS[pset], precision=prec), LAUNCHES[launch])
+
+
+def _check_against_oracle(oracle, dims, params, launch):
+    prec = params["precision"]
     g, o, flags = _pair(oracle, dims, params)
-    g.set_launch(*LAUNCHES[launch])
-    assert g.get_launch() == LAUNCHES[launch]
+    g.set_launch(*launch)
+    assert g.get_launch() == launch
     t1, t30 = TOL[prec]
     g.step(1)
     o.step(1)
@@ -155,6 +159,38 @@ def test_autotune_keeps_state(gpu):
                                atol=3e-4)
 
 
+@pytest.mark.parametrize("prec", ["f32", "f16"])
+def test_raw_write_and_geometry_change_follow_oracle(gpu, oracle, prec):
+    # solid cells are read as stored (mirror images on the faces) until a step rewrites them; a
+    # raw population write and a mid-run change of the body must give the oracle's results
+    dims = (32, 14, 12)
+    params = dict(PARAM_SETS["belt_periodic_les"], precision=prec)
+    g, o, flags = _pair(oracle, dims, params)
+    g.set_launch(3, 2, 32, 4)
+    g.step(4)
+    o.step(4)
+    f = g.read_populations().reshape(19, -1).copy()
+    rng = np.random.default_rng(5)
+    solid = flags != 0
+    f[:, solid] = (rng.random((19, int(solid.sum()))) * 0.01).astype(f.dtype)
+    g.write_populations(f.ravel())
+    o.a[:] = f.ravel()
+    t1, t30 = TOL[prec]
+    for k in range(3):
+        g.step(1)
+        o.step(1)
+        d = np.abs(_as_float(g.read_populations()) - _as_float(o.current)).max()
+        assert d <= t30, f"step {k + 1} after the write: max |diff| {d:.3e}"
+    moved = np.roll(flags.reshape(dims[::-1]), 2, axis=2).ravel()
+    for s in (g, o):
+        s.upload_flags(moved)
+    g.step(5)
+    o.step(5)
+    d = np.abs(_as_float(g.read_populations()) - _as_float(o.current)).max()
+    assert d <= t30, f"after the geometry change: max |diff| {d:.3e}"
+    g.destroy()
+
+
 def test_errors_are_reported(gpu):
     s = Solver((16, 8, 4), dict(u=0.05, nu=0.02))
     with pytest.raises(WtError):
@@ -166,6 +202,9 @@ def test_errors_are_reported(gpu):
         s.set_params(dict(precision="f16"))
     with pytest.raises(WtError):
         Solver((0, 8, 8), dict(u=0.05, nu=0.02))
+    for bad in ((1, 2), (5, 2), (4, 4), (0, 2, 48, 2), (0, 2, 128, 4)):  # hint, cells, block shape
+        with pytest.raises(WtError):
+            s.set_launch(*bad)
 
 
 # ---- voxelizer -------------------------------------------------------------------------------

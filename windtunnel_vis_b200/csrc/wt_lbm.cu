@@ -811,6 +811,12 @@ template <> struct PairIO<StF16> {
   __device__ __forceinline__ static one_t ld1(const __half* __restrict__ p, uint32_t o) {
     return __ldg(reinterpret_cast<const unsigned short*>(p + o));
   }
+  // elements (o .. o + 3), o a multiple of 4: one 8-byte load
+  __device__ __forceinline__ static void ld4(const __half* __restrict__ p, uint32_t o, pair_t& a, pair_t& b) {
+    const uint2 q = __ldg(reinterpret_cast<const uint2*>(p + o));
+    a = q.x;
+    b = q.y;
+  }
   __device__ __forceinline__ static float2 cvt(pair_t u, float /*w*/) {
     return __half22float2(*reinterpret_cast<const __half2*>(&u));
   }
@@ -828,6 +834,12 @@ template <> struct PairIO<StF32> {
     return __ldg(reinterpret_cast<const float2*>(p + o));
   }
   __device__ __forceinline__ static one_t ld1(const float* __restrict__ p, uint32_t o) { return __ldg(p + o); }
+  // elements (o .. o + 3), o a multiple of 4: one 16-byte load
+  __device__ __forceinline__ static void ld4(const float* __restrict__ p, uint32_t o, pair_t& a, pair_t& b) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(p + o));
+    a = make_float2(q.x, q.y);
+    b = make_float2(q.z, q.w);
+  }
   __device__ __forceinline__ static float2 cvt(pair_t f, float w) { return make_float2(f.x - w, f.y - w); }
   __device__ __forceinline__ static float cvt1(one_t f, float w) { return f - w; }
   __device__ __forceinline__ static void st(float* __restrict__ p, uint32_t o, float2 v, float w) {
@@ -873,51 +885,50 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
     constexpr int i = I;
     constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
     const uint32_t src = i * N + idx0 - (uint32_t)(cy * (int)sy) - (uint32_t)(cz * (int)sz);
+    if constexpr (G == 2) {
+      IO::ld4(fin, src, rp[0][i], rp[1][i]);  // src is a multiple of 4 when nx % 4 == 0
+    } else {
 #pragma unroll
-    for (int g = 0; g < G; g++) rp[g][i] = IO::ld(fin, src + 2 * g);
+      for (int g = 0; g < G; g++) rp[g][i] = IO::ld(fin, src + 2 * g);
+    }
     if constexpr (cx > 0) r1[i] = IO::ld1(fin, x0 > 0 ? src - 1u : src);          // x - 1
     if constexpr (cx < 0) r1[i] = IO::ld1(fin, last ? src + (V - 1) : src + V);   // x + 1, outlet clamp
   });
-  // phase 2: convert and shift into the pulled populations of each cell
-  float2 h[G][Q];
-  static_for<Q>([&](auto I) {
-    constexpr int i = I;
-    constexpr int cx = L::c[i][0];
-    constexpr float w = (float)Wc<L, i>::v;
-    float2 cur[G];
+  // phase 2, one pair of cells at a time (the other pairs stay packed in their raw registers):
+  // convert and shift into the pulled populations, collide, store
 #pragma unroll
-    for (int g = 0; g < G; g++) cur[g] = IO::cvt(rp[g][i], w);
-    if constexpr (cx == 0) {
-#pragma unroll
-      for (int g = 0; g < G; g++) h[g][i] = cur[g];
-    } else if constexpr (cx > 0) {
-      h[0][i] = make_float2(IO::cvt1(r1[i], w), cur[0].x);
-#pragma unroll
-      for (int g = 1; g < G; g++) h[g][i] = make_float2(cur[g - 1].y, cur[g].x);
-    } else {
-#pragma unroll
-      for (int g = 0; g < G - 1; g++) h[g][i] = make_float2(cur[g].y, cur[g + 1].x);
-      h[G - 1][i] = make_float2(cur[G - 1].y, IO::cvt1(r1[i], w));
-    }
-  });
-  if (x0 == 0) {
-    // inlet column: populations entering from x < 0 are the free-stream equilibrium
-    const float U = P.uin;
+  for (int g = 0; g < G; g++) {
+    float2 h[Q];
     static_for<Q>([&](auto I) {
       constexpr int i = I;
       constexpr int cx = L::c[i][0];
-      if constexpr (cx > 0) {
-        constexpr float w = (float)Wc<L, i>::v;
-        h[0][i].x = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
+      constexpr float w = (float)Wc<L, i>::v;
+      const float2 cur = IO::cvt(rp[g][i], w);
+      if constexpr (cx == 0) {
+        h[i] = cur;
+      } else if constexpr (cx > 0) {
+        h[i] = make_float2(g == 0 ? IO::cvt1(r1[i], w) : IO::cvt(rp[g > 0 ? g - 1 : 0][i], w).y, cur.x);
+      } else {
+        h[i] = make_float2(cur.y, g == G - 1 ? IO::cvt1(r1[i], w) : IO::cvt(rp[g < G - 1 ? g + 1 : g][i], w).x);
       }
     });
-  }
-#pragma unroll
-  for (int g = 0; g < G; g++)
-    collide_shifted2<L, BGK>(P, h[g], x0 + 2 * g, [&](auto I, float2 v) {
+    if (g == 0 && x0 == 0) {
+      // inlet column: populations entering from x < 0 are the free-stream equilibrium
+      const float U = P.uin;
+      static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        constexpr int cx = L::c[i][0];
+        if constexpr (cx > 0) {
+          constexpr float w = (float)Wc<L, i>::v;
+          h[i].x = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
+        }
+      });
+    }
+    collide_shifted2<L, BGK>(P, h, x0 + 2 * g, [&](auto I, float2 v) {
       constexpr int i = decltype(I)::value;
       if (clean) IO::st(fout, i * N + idx0 + 2 * g, v, (float)Wc<L, i>::v);
     });
+  }
 }
 
 // Rows on the domain faces (y = 0 or ny - 1, and z = 0 or nz - 1 in 3-D), vectorised like the
