@@ -18,6 +18,7 @@ Multi-GPU: independent tunnel replicas, one per rank (no data-path collective).
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -45,6 +46,19 @@ def peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def measured_traffic(shape):
+    """DRAM bytes (read + write) per step of this launch shape from the committed ncu summary
+    (steady state over 30 steps), or None when that launch was not captured."""
+    p = os.path.join(ROOT, "profiles", "stream_collide_d3q19_f16_sphere256.md")
+    if not os.path.exists(p):
+        return None
+    key = ",".join(str(int(v)) for v in shape)
+    for m in re.finditer(r"^traffic_bytes_per_step\[([0-9,]+)\]:\s*(\d+)", open(p).read(), flags=re.M):
+        if m.group(1) == key:
+            return int(m.group(2))
+    return None
 
 
 def geometry():
@@ -224,10 +238,7 @@ def run_ours(args, rank, world, local_rank, dist):
         return
     peak, peak_kind = peaks()
     achieved = n * BYTES_PER_UPDATE / (sc_ms / 1e3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "stream_collide_d3q19_f16_traffic.json")
-    if os.path.exists(tp):
-        traffic = json.load(open(tp)).get("bytes_per_launch")
+    traffic = measured_traffic(shape)
     cpu = None
     if world == 1 and not args.no_cpu:
         mlups, th, done = cpu_port_mlups(args.cpu_seconds)
@@ -243,8 +254,10 @@ def run_ours(args, rank, world, local_rank, dist):
                    "launch": {"cells_per_thread": shape[1], "block": [shape[2], shape[3]]}},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "k_stream_collide_v<D3Q19,StF16>" if shape[1] > 1 else "k_stream_collide<D3Q19,StF16>", "bytes_per_launch_alg": n * BYTES_PER_UPDATE,
-                     "launch_ms": round(sc_ms, 5)},
+                     "kernel": ("one lattice update: k_stream_collide_v<D3Q19,StF16> (bulk) overlapped with "
+                                "k_face_v and k_boundary_tab" if shape[1] > 1 else "k_stream_collide<D3Q19,StF16>"),
+                     "bytes_alg_per_update": n * BYTES_PER_UPDATE, "traffic_per": "lattice update (ncu, steady state)",
+                     "update_ms": round(sc_ms, 5)},
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e, 1), "unit": "MLUPS", "h2d_bytes_per_step": n * 8,
                 "d2h_bytes_per_step": 64 + vel_bytes},
