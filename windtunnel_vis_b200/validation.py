@@ -4,6 +4,7 @@ round_flags .... src/analysis/validation.ts:35-53 (analytic circle / sphere flag
 freestream ..... src/analysis/validation.ts:61-88
 cylinder ....... src/analysis/validation.ts:89-136
 sphere ......... src/analysis/validation.ts:137-184
+sphere_les ..... the D3Q19 LES sphere tunnel of the benchmark (FP16 storage against FP64 populations)
 
 A factory is any callable make(dims, params) returning an object with the LbmSolver surface
 (upload_flags, upload_sdf, step_and_sample, destroy) — windtunnel_vis_b200.solver.SolverFactory
@@ -134,4 +135,75 @@ def sphere(make, valscale=1.0):
                         "blockage": frontal / (d[1] * d[2])}}
 
 
+def sphere_les(make, precision="f16", steps=20000, dims=(256, 128, 128), diameter=24, u=0.05, re=300.0, cs=0.1,
+               seed=1, chunk=50, measure_from=None):
+    """Sphere in a D3Q19 LES tunnel: diameter 24 at (64, 64.37, 64.21) (off-axis by fractions of a
+    cell like the reference's sphere case), inlet u = 0.05, Re = 300, Smagorinsky Cs = 0.1,
+    rest state with seeded 1e-4 velocity noise. Returns the C_D / C_L / C_S series and the mean
+    C_D with its batch-means standard error over the steps from `measure_from` (default: the
+    second half). Run it with precision "f16" (shifted FP16 storage) and "f64" (FP64 populations
+    on the GPU, the plain method's reference run) to state the storage error."""
+    from .analysis import window_stats
+
+    t0 = time.perf_counter()
+    nu = u * diameter / re
+    p = dict(u=u, nu=nu, cs=cs, ground="freeslip", sides="freeslip", spongeNu=0.03, spongeStart=0.85, emaAlpha=0,
+             precision=precision, init="rest_noise", initNoise=1e-4, initSeed=seed)
+    flags, frontal, sdf = round_flags(dims, (64.0, 64.37, 64.21), diameter / 2, False)
+    s = make(dims, p)
+    s.upload_flags(flags)
+    s.upload_sdf(sdf)
+    tt, cd, cl, cz = [], [], [], []
+    step = 0
+    unstable = False
+    while step < steps:
+        st = s.step_and_sample(chunk)
+        step += chunk
+        if st["unstable"]:
+            unstable = True
+            break
+        c = coefficients(st["fx"], st["fy"], st["fz"], u, frontal)
+        tt.append(st["step"])
+        cd.append(c["cd"])
+        cl.append(c["cl"])
+        cz.append(c["cs"])
+    s.destroy()
+    start = steps // 2 if measure_from is None else measure_from
+    sel = [k for k, t in enumerate(tt) if t >= start]
+    ws = window_stats([tt[k] for k in sel], [cd[k] for k in sel], float(steps)) if len(sel) >= 16 else None
+    amp = lambda v: (max(v[k] for k in sel) - min(v[k] for k in sel)) / 2 if sel else math.nan
+    return {"id": "sphere_les", "precision": precision, "passed": not unstable and ws is not None,
+            "seconds": time.perf_counter() - t0, "series": {"t": tt, "cd": cd, "cl": cl, "cs": cz},
+            "metrics": {"cd_mean": ws["mean"] if ws else math.nan, "cd_se": ws["se"] if ws else math.nan,
+                        "cl_amplitude": amp(cl), "cs_amplitude": amp(cz), "steps": step, "measured_from": start,
+                        "frontal": frontal, "grid": list(dims), "nu": nu, "unstable": unstable}}
+
+
 CASES = {"freestream": freestream, "cylinder": cylinder, "sphere": sphere}
+
+
+def main(argv=None):
+    """python -m windtunnel_vis_b200.validation sphere_les --precision f16 --steps 20000
+    python -m windtunnel_vis_b200.validation cylinder|sphere|freestream [--valscale 0.5]
+    Prints one JSON line (metrics, series omitted) per case on the CUDA path."""
+    import argparse
+    import json
+
+    from .solver import solver_factory
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["sphere_les", *CASES])
+    ap.add_argument("--precision", default="f16")
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--valscale", type=float, default=1.0)
+    a = ap.parse_args(argv)
+    if a.case == "sphere_les":
+        r = sphere_les(solver_factory, a.precision, a.steps)
+    else:
+        r = CASES[a.case](solver_factory, a.valscale)
+    r.pop("series", None)
+    print(json.dumps(r), flush=True)
+
+
+if __name__ == "__main__":
+    main()
