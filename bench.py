@@ -129,6 +129,109 @@ def cpu_port_mlups(seconds=12.0, threads=0, steps_cap=None):
     return n * done / dt / 1e6, th, done
 
 
+def components(s, peak, no_cpu):
+    """Timings of the other kernels on the path, rank 0 at N = 1 (each with its CPU restatement
+    timed beside it on the host cores):
+      sample ..... the macro pass (force, EMA statistics, velocity field) on the bench tunnel;
+                   91 B per cell: 19 x 2 B populations, flags, class byte, 16 + 4 B EMA read and
+                   written, 8 B velocity
+      tracers .... 150,000 particles, trail 20, 50 lattice steps per frame, 18 nozzles (the
+                   reference app's 3-D settings), advected through the bench tunnel's velocity
+                   field; 48 B per particle (state read and written, one trail point)
+      voxelize ... the vehicle body (about 200k triangles) into 512 x 256 x 256 through the public
+                   API (host mesh in, flags / wall distances / info on the device); 24 B per cell
+                   (3 i32 crossing counters, vote word, flags, wall distance)
+    """
+    import torch
+
+    from oracle import oracle as O
+    from windtunnel_vis_b200 import abi
+    from windtunnel_vis_b200.solver import Solver
+    from windtunnel_vis_b200.validation import vehicle_setup
+
+    n = DIMS[0] * DIMS[1] * DIMS[2]
+    st = torch.cuda.ExternalStream(s.stream)
+    out = {}
+
+    def timed(fn, reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        a.record(st)
+        for _ in range(reps):
+            fn()
+        b.record(st)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps, (time.perf_counter() - t0) * 1e3 / reps
+
+    # macro pass
+    ms, wall = timed(s.sample, 10)
+    alg = n * 91
+    out["sample"] = {"ms": round(ms, 4), "e2e_ms": round(wall, 4), "bytes_alg": alg,
+                     "achieved_gbs": round(alg / ms / 1e6, 1), "frac": round(alg / ms / 1e6 / peak, 4)}
+
+    # tracers
+    count, trail, steps = 150000, 20, float(CHUNK)
+    tp = abi.TracerParams(count=count, trail=trail, head=0, emitter=0, steps=steps, seed=7,
+                          max_age=min(max(1.2 * DIMS[0] / max(U * steps, 1e-3), 60.0), 6000.0), nozzles=18)
+    tp.fill, tp.advance = 1, 0
+    s.advect_tracers(tp)
+    tp.fill, tp.advance = 0, 1
+    frame = [0]
+
+    def advect():
+        frame[0] += 1
+        tp.head = frame[0] % trail
+        tp.seed = 7 + frame[0]
+        s.advect_tracers(tp)
+
+    ms, wall = timed(advect, 20)
+    out["tracers"] = {"ms": round(ms, 4), "e2e_ms": round(wall, 4), "particles": count, "trail": trail,
+                      "mparticles_per_s": round(count / ms / 1e3, 1), "bytes_alg": count * 48,
+                      "achieved_gbs": round(count * 48 / ms / 1e6, 1)}
+    if not no_cpu:
+        vel = s.read_velocity().astype(np.float16)
+        flags = np.asarray(geometry()[0], np.uint32)
+        state, hist = s.read_tracers(count, trail)
+        state, hist = state.copy(), hist.copy()
+        tp.head = (frame[0] + 1) % trail
+        t0 = time.perf_counter()
+        O.tracers(DIMS, tp, vel, flags, state, hist)
+        out["tracers"]["cpu_ref_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+        out["tracers"]["cpu_kind"] = "port"
+        out["tracers"]["cpu_threads"] = O.threads(0)
+
+    # voxelizer (vehicle config, its own 512 x 256 x 256 handle)
+    vd = (512, 256, 256)
+    p, idx, M16, wheels, _ = vehicle_setup(vd)
+    v = Solver(vd, dict(u=0.06, nu=1e-5, cs=0.14, ground="moving", precision="f16"))
+    v.voxelize(p, idx, M16, wheels)
+    vst = torch.cuda.ExternalStream(v.stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a.record(vst)
+    reps = 5
+    for _ in range(reps):
+        info = v.voxelize(p, idx, M16, wheels)
+    b.record(vst)
+    torch.cuda.synchronize()
+    vms, vwall = a.elapsed_time(b) / reps, (time.perf_counter() - t0) * 1e3 / reps
+    nv = vd[0] * vd[1] * vd[2]
+    out["voxelize"] = {"ms": round(vms, 3), "e2e_ms": round(vwall, 3), "grid": list(vd),
+                       "triangles": int(np.asarray(idx).size // 3), "solid_cells": info["solidCells"],
+                       "bytes_alg": nv * 24, "achieved_gbs": round(nv * 24 / vms / 1e6, 1),
+                       "frac": round(nv * 24 / vms / 1e6 / peak, 4)}
+    v.destroy()
+    if not no_cpu:
+        t0 = time.perf_counter()
+        O.voxelize_f64(vd, p, idx, M16)
+        out["voxelize"]["cpu_ref_s"] = round(time.perf_counter() - t0, 3)
+        out["voxelize"]["cpu_kind"] = "port (f64, the reference's CPU voxelizer)"
+        out["voxelize"]["cpu_threads"] = O.threads(0)
+    return out
+
+
 def run_reference(args, rank, world):
     """Reference arm: the reference's WGSL path cannot run here (TypeScript + WebGPU; no Node
     and no graphics stack), so its algorithm runs as the CPU restatement on the host cores."""
@@ -239,6 +342,9 @@ def run_ours(args, rank, world, local_rank, dist):
     peak, peak_kind = peaks()
     achieved = n * BYTES_PER_UPDATE / (sc_ms / 1e3) / 1e9
     traffic = measured_traffic(shape)
+    comps = None
+    if world == 1 and not args.no_components:
+        comps = components(s, peak, args.no_cpu)
     cpu = None
     if world == 1 and not args.no_cpu:
         mlups, th, done = cpu_port_mlups(args.cpu_seconds)
@@ -262,6 +368,7 @@ def run_ours(args, rank, world, local_rank, dist):
         "e2e": {"value": round(e2e, 1), "unit": "MLUPS", "h2d_bytes_per_step": n * 8,
                 "d2h_bytes_per_step": 64 + vel_bytes},
         "gpu_launches": launches,
+        "components": comps,
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -276,6 +383,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-components", action="store_true", help="skip the sample / tracer / voxelizer timings")
     ap.add_argument("--launch", default="", help="fixed stream-collide launch 'hint,cells,bx,by' instead of the tuner")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

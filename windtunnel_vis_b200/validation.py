@@ -5,6 +5,7 @@ freestream ..... src/analysis/validation.ts:61-88
 cylinder ....... src/analysis/validation.ts:89-136
 sphere ......... src/analysis/validation.ts:137-184
 sphere_les ..... the D3Q19 LES sphere tunnel of the benchmark (FP16 storage against FP64 populations)
+vehicle ........ the D3Q19 vehicle tunnel of the benchmark (GPU voxelizer, moving belt, wheels)
 
 A factory is any callable make(dims, params) returning an object with the LbmSolver surface
 (upload_flags, upload_sdf, step_and_sample, destroy) — windtunnel_vis_b200.solver.SolverFactory
@@ -179,11 +180,71 @@ def sphere_les(make, precision="f16", steps=20000, dims=(256, 128, 128), diamete
                         "frontal": frontal, "grid": list(dims), "nu": nu, "unstable": unstable}}
 
 
+def vehicle_setup(dims=(512, 256, 256), target_tris=200_000, seed=1):
+    """The vehicle-like body of the benchmark: seeded superellipsoid body (length nx / 3, aspect
+    4 : 1.5 : 1.2) on four 16-segment wheels of radius 0.12 * height, about 200k triangles,
+    placed on the floor with a ride height of 0.08 * body height (the reference app's placement,
+    mode 'ground', at x = 0.34 nx). Returns (positions, indices, column-major matrix, grid-space
+    wheels, body height in cells)."""
+    from . import mesh as Mh
+
+    p, idx, wheels, lo, hi = Mh.vehicle_body(target_tris=target_tris, seed=seed)
+    scale = dims[0] / 3.0  # lengthFrac 1/3 of a unit-length mesh
+    height = float(hi[1] - lo[1]) * scale
+    M16, _, full = Mh.placement_matrix(p, lo, hi, dims, dict(mode="ground", lengthFrac=1 / 3, diamFrac=0.3,
+                                                             xFrac=0.34, rideCells=0.08 * height))
+    return p, idx, M16, Mh.grid_wheels(wheels, full), height
+
+
+def vehicle(make, precision="f16", steps=30000, dims=(512, 256, 256), u=0.06, re_l=1e6, cs=0.14, chunk=100,
+            measure_from=None):
+    """Vehicle tunnel: the body of vehicle_setup voxelized on the GPU (solver.voxelize), moving
+    belt at the inlet speed, rotating wheels, Re_L = 1e6 on the body length with Smagorinsky LES
+    (Cs 0.14, the reference app's default), rest initial state with seeded noise. Reports mean
+    C_D / C_L (frontal area from the voxelizer) with batch-means errors over the second half."""
+    from .analysis import window_stats
+
+    t0 = time.perf_counter()
+    p, idx, M16, wheels, height = vehicle_setup(dims)
+    length = dims[0] / 3.0
+    nu = u * length / re_l
+    params = dict(u=u, nu=nu, cs=cs, ground="moving", sides="freeslip", spongeNu=0.03, spongeStart=0.85,
+                  emaAlpha=0, precision=precision, init="rest_noise", initNoise=1e-4, initSeed=1)
+    s = make(dims, params)
+    info = s.voxelize(p, idx, M16, wheels)
+    t_vox = time.perf_counter() - t0
+    tt, cd, cl = [], [], []
+    step = 0
+    unstable = False
+    while step < steps:
+        st = s.step_and_sample(chunk)
+        step += chunk
+        if st["unstable"]:
+            unstable = True
+            break
+        c = coefficients(st["fx"], st["fy"], st["fz"], u, info["frontal"])
+        tt.append(st["step"])
+        cd.append(c["cd"])
+        cl.append(c["cl"])
+    s.destroy()
+    start = steps // 2 if measure_from is None else measure_from
+    sel = [k for k, t in enumerate(tt) if t >= start]
+    wd = window_stats([tt[k] for k in sel], [cd[k] for k in sel], float(steps)) if len(sel) >= 16 else None
+    wl = window_stats([tt[k] for k in sel], [cl[k] for k in sel], float(steps)) if len(sel) >= 16 else None
+    return {"id": "vehicle", "precision": precision, "passed": not unstable and wd is not None,
+            "seconds": time.perf_counter() - t0, "series": {"t": tt, "cd": cd, "cl": cl},
+            "metrics": {"cd_mean": wd["mean"] if wd else math.nan, "cd_se": wd["se"] if wd else math.nan,
+                        "cl_mean": wl["mean"] if wl else math.nan, "cl_se": wl["se"] if wl else math.nan,
+                        "voxel": info, "triangles": int(np.asarray(idx).size // 3), "body_height_cells": height,
+                        "tau0": 3 * nu + 0.5, "steps": step, "unstable": unstable, "setup_seconds": t_vox}}
+
+
 CASES = {"freestream": freestream, "cylinder": cylinder, "sphere": sphere}
 
 
 def main(argv=None):
     """python -m windtunnel_vis_b200.validation sphere_les --precision f16 --steps 20000
+    python -m windtunnel_vis_b200.validation vehicle --precision f16 --steps 30000
     python -m windtunnel_vis_b200.validation cylinder|sphere|freestream [--valscale 0.5]
     Prints one JSON line (metrics, series omitted) per case on the CUDA path."""
     import argparse
@@ -192,13 +253,15 @@ def main(argv=None):
     from .solver import solver_factory
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["sphere_les", *CASES])
+    ap.add_argument("case", choices=["sphere_les", "vehicle", *CASES])
     ap.add_argument("--precision", default="f16")
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--valscale", type=float, default=1.0)
     a = ap.parse_args(argv)
     if a.case == "sphere_les":
         r = sphere_les(solver_factory, a.precision, a.steps)
+    elif a.case == "vehicle":
+        r = vehicle(solver_factory, a.precision, a.steps)
     else:
         r = CASES[a.case](solver_factory, a.valscale)
     r.pop("series", None)
