@@ -239,6 +239,31 @@ def test_voxelizer_bit_exact(gpu, oracle, kind, dims):
     assert info0["solidCells"] == 0 and s.read_flags().sum() == 0
 
 
+@pytest.mark.parametrize("prec", ["f16", "f32"])
+def test_steps_after_voxelize_follow_oracle(gpu, oracle, prec):
+    # the voxelizer's scratch lives in the population buffer the next step overwrites: stepping on
+    # after a voxelization must give the oracle's populations from the same state and geometry
+    dims = (64, 32, 24)
+    params = dict(PARAM_SETS["freeslip_reg"], precision=prec, init="rest_noise", initNoise=0.01)
+    s = Solver(dims, params)
+    s.step(5)
+    f0 = s.read_populations()
+    p, idx, M16, wheels = _sphere(dims)
+    s.voxelize(p, idx, M16, wheels)
+    o = oracle.OracleSolver(dims, params)
+    o.upload_flags(s.read_flags())
+    o.sdf[:] = s.read_sdf_encoded()
+    o.pending_init = False
+    o.a[:] = f0
+    t1, t30 = TOL[prec]
+    for k in (1, 2, 5):
+        s.step(k)
+        o.step(k)
+        d = np.abs(_as_float(s.read_populations()) - _as_float(o.current)).max()
+        assert d <= t30, f"max |diff| {d:.3e}"
+    s.destroy()
+
+
 # ---- tracers ---------------------------------------------------------------------------------
 @pytest.mark.parametrize("dims,emitter", [((48, 24, 16), 0), ((48, 24, 16), 1), ((64, 32, 1), 0), ((64, 32, 1), 1)])
 def test_tracers_bit_exact(gpu, oracle, dims, emitter):

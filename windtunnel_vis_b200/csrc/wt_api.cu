@@ -69,7 +69,7 @@ int64_t bytes_for(const wt_dims* d, int prec) {
 void free_all(wt_solver* s) {
   void* bufs[] = {s->f[0], s->f[1], s->flags, s->sdf, s->cls, s->vel, s->vel_f32, s->meanA, s->meanB,
                   s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count,
-                  s->bcell, s->brec, s->bgam};
+                  s->bcell, s->brec, s->bgam, s->vox_pos, s->vox_idx, s->vox_info};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->result_host) cudaFreeHost(s->result_host);
@@ -444,19 +444,30 @@ int wt_voxelize(wt_solver* s, const float* pos, int64_t nverts, const uint32_t* 
   }
   for (int64_t i = 0; i < 3 * ntri; i++)
     if ((int64_t)idx[i] >= nverts) return fail(s, WT_E_INVALID, "wt_voxelize: index out of range of the vertex array");
-  void *dpos = nullptr, *didx = nullptr, *hits = nullptr, *vote = nullptr, *dinfo = nullptr;
-  auto cleanup = [&]() {
-    for (void* b : {dpos, didx, hits, vote, dinfo})
-      if (b) cudaFree(b);
+  // mesh buffers are kept by the handle and grown when a larger mesh arrives
+  auto grow = [&](void** buf, size_t* cap, size_t bytes) -> cudaError_t {
+    if (bytes <= *cap) return cudaSuccess;
+    if (*buf) cudaFree(*buf);
+    *buf = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc(buf, bytes);
+    if (e == cudaSuccess) *cap = bytes;
+    return e;
   };
   cudaError_t e = cudaSuccess;
-  if ((e = cudaMalloc(&dpos, (size_t)nverts * 12 + 16)) != cudaSuccess ||
-      (e = cudaMalloc(&didx, (size_t)ntri * 12 + 16)) != cudaSuccess ||
-      (e = cudaMalloc(&hits, 3 * s->n * 4)) != cudaSuccess || (e = cudaMalloc(&vote, s->n * 4)) != cudaSuccess ||
-      (e = cudaMalloc(&dinfo, 32)) != cudaSuccess) {
-    cleanup();
-    return cuda_fail(s, e, "wt_voxelize: scratch allocation");
-  }
+  if ((e = grow(&s->vox_pos, &s->vox_pos_cap, (size_t)nverts * 12 + 16)) != cudaSuccess ||
+      (e = grow(&s->vox_idx, &s->vox_idx_cap, (size_t)ntri * 12 + 16)) != cudaSuccess ||
+      (!s->vox_info && (e = cudaMalloc((void**)&s->vox_info, 32)) != cudaSuccess))
+    return cuda_fail(s, e, "wt_voxelize: mesh buffers");
+  // the crossing counters (3 n i32) and vote words (n u32) live in the population buffer that the
+  // next step writes in full (16 B per cell; a buffer holds at least 18): the geometry change
+  // below makes that step rewrite the solid cells as well, and a pending initialisation rewrites
+  // both buffers
+  void* dpos = s->vox_pos;
+  void* didx = s->vox_idx;
+  void* dinfo = s->vox_info;
+  void* hits = s->f[s->parity ^ 1];
+  void* vote = (char*)hits + 3 * s->n * 4;
   const uint32_t info_init[8] = {0, 0, 0xffffffffu, 0xffffffffu, 0xffffffffu, 0, 0, 0};
   uint32_t info_h[8];
   wt::VoxelJob job;
@@ -474,10 +485,9 @@ int wt_voxelize(wt_solver* s, const float* pos, int64_t nverts, const uint32_t* 
       (e = cudaMemcpyAsync(info_h, dinfo, 32, cudaMemcpyDeviceToHost, s->stream)) != cudaSuccess ||
       (e = cudaStreamSynchronize(s->stream)) != cudaSuccess) {
     cudaStreamSynchronize(s->stream);
-    cleanup();
+    s->cls_dirty = true;
     return cuda_fail(s, e, "wt_voxelize");
   }
-  cleanup();
   s->cls_dirty = true;
   const bool ok = info_h[1] > 0;
   info->frontal = (int32_t)info_h[0];

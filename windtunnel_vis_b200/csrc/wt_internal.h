@@ -63,6 +63,11 @@ struct wt_solver {
   double* result_dev = nullptr;  // 8 doubles
   double* result_host = nullptr; // pinned
   wt::Wheels wheels{};
+  // voxelizer: device copies of the last mesh (grown as needed) and the 8-word info block
+  void* vox_pos = nullptr;
+  void* vox_idx = nullptr;
+  size_t vox_pos_cap = 0, vox_idx_cap = 0;
+  uint32_t* vox_info = nullptr;
   // tracers
   float4* tr_state = nullptr;
   float4* tr_hist = nullptr;
