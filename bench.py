@@ -135,6 +135,8 @@ def components(s, peak, no_cpu):
       sample ..... the macro pass (force, EMA statistics, velocity field) on the bench tunnel;
                    91 B per cell: 19 x 2 B populations, flags, class byte, 16 + 4 B EMA read and
                    written, 8 B velocity
+      derive ..... the derived-field pass on the bench tunnel; 56 B per cell: velocity 8 B,
+                   flags 4 B, EMA 16 + 4 B read, three binary16 x 4 fields written
       tracers .... 150,000 particles, trail 20, 50 lattice steps per frame, 18 nozzles (the
                    reference app's 3-D settings), advected through the bench tunnel's velocity
                    field; 48 B per particle (state read and written, one trail point)
@@ -169,6 +171,13 @@ def components(s, peak, no_cpu):
     alg = n * 91
     out["sample"] = {"ms": round(ms, 4), "e2e_ms": round(wall, 4), "bytes_alg": alg,
                      "achieved_gbs": round(alg / ms / 1e6, 1), "frac": round(alg / ms / 1e6 / peak, 4)}
+
+    # derived fields (vorticity, Q, turbulence intensity, binary16 mean)
+    s.derive_fields()
+    ms, wall = timed(s.derive_fields, 10)
+    alg = n * 56
+    out["derive"] = {"ms": round(ms, 4), "bytes_alg": alg, "achieved_gbs": round(alg / ms / 1e6, 1),
+                     "frac": round(alg / ms / 1e6 / peak, 4)}
 
     # tracers
     count, trail, steps = 150000, 20, float(CHUNK)

@@ -219,6 +219,23 @@ int wt_read_tracers(wt_solver* s, float* state4, int64_t count, float* hist4, in
 int wt_write_tracers(wt_solver* s, const float* state4, int64_t count, const float* hist4,
                      int64_t hist_len, uint32_t trail);
 
+/* ---- derived fields and field export ----------------------------------------------------- */
+/* Derived fields (the derived pass, src/solver/wgslLbm.ts:527-592): vorticity (wx, wy, wz) and the
+ * Q-criterion (faded out within two cells of a solid) from central differences of the velocity
+ * field, turbulence intensity sqrt(k / 3) / uRef from the EMA statistics, and the mean field, as
+ * binary16 x 4 per cell (the reference's rgba16float textures), from the velocity field and
+ * statistics of the last sample. The first call allocates 24 B per cell. */
+int wt_derive_fields(wt_solver* s);
+/* Full-resolution read of the derived fields as n x 4 floats; any pointer may be NULL:
+ * vort4 = (wx, wy, wz, Q), stat4 = (turbulence intensity, solid, 0, 0), mean4 = the mean field
+ * rounded to binary16. Needs a wt_derive_fields call first. */
+int wt_read_derived(wt_solver* s, float* vort4, float* stat4, float* mean4, int64_t n);
+/* SolverGPU.exportFields (src/solver/SolverGPU.ts:374-425): derives the fields, then reads
+ * velocity, mean and vorticity at every stride-th cell (clamped to the last cell) into
+ * points = ceil(nx/stride) * ceil(ny/stride) * ceil(nz/stride) float4 each (x fastest); any
+ * output pointer may be NULL. */
+int wt_export_fields(wt_solver* s, int32_t stride, float* vel4, float* mean4, float* vort4, int64_t points);
+
 /* ---- launch selection (extension; no counterpart in the reference) ------------------------ */
 /* Selects the stream-collide launch: `param` cells per thread along x (1, 2 or 4; 2 and 4 need
  * f16/f32 storage and nx % param == 0, otherwise the scalar kernel runs), block bx x by threads

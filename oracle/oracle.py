@@ -41,6 +41,8 @@ def lib():
         L.or_voxelize_f32.argtypes = [P(abi.Dims), v, v, C.c_int64, v, v, C.c_int, v, v, v, v, v]
         L.or_voxelize_f64.argtypes = [P(abi.Dims), v, C.c_int64, v, C.c_int64, v, v, v, v]
         L.or_tracers.argtypes = [P(abi.Dims), P(abi.TracerParams), v, v, v, v]
+        L.or_derive.argtypes = [P(abi.Dims), C.c_float, v, v, v, v, v, v, v]
+        L.or_export.argtypes = [P(abi.Dims), C.c_int, v, v, v, v, v, v]
         L.or_pcg.argtypes = [C.c_uint32]
         L.or_pcg.restype = C.c_uint32
         _lib = L
@@ -239,3 +241,24 @@ def tracers(dims, tp: abi.TracerParams, vel_half4, flags, state, hist):
 
 def pcg(v):
     return lib().or_pcg(v & 0xFFFFFFFF)
+
+
+def derive(dims, u_ref, vel_half4, flags, meanA, meanB):
+    """Derived fields: returns (vort, stat, mean) as float16 arrays of shape (n, 4)."""
+    n = dims[0] * dims[1] * dims[2]
+    vel = np.ascontiguousarray(vel_half4, np.float16).reshape(n, 4).view(np.uint16)
+    outs = [np.zeros((n, 4), np.uint16) for _ in range(3)]
+    lib().or_derive(C.byref(dims_of(dims)), float(np.float32(u_ref)), _p(vel), _p(np.ascontiguousarray(flags, np.uint32)),
+                    _p(np.ascontiguousarray(meanA, np.float32)), _p(np.ascontiguousarray(meanB, np.float32)),
+                    *(_p(o) for o in outs))
+    return tuple(o.view(np.float16) for o in outs)
+
+
+def export(dims, stride, vel_half4, mean_half4, vort_half4):
+    """Strided export of half4 fields: {dims, stride, vel, mean, vort} (float32, (points, 4))."""
+    o = [-(-d // stride) for d in dims]
+    n = o[0] * o[1] * o[2]
+    src = [np.ascontiguousarray(a, np.float16).view(np.uint16) for a in (vel_half4, mean_half4, vort_half4)]
+    out = [np.zeros((n, 4), np.float32) for _ in range(3)]
+    lib().or_export(C.byref(dims_of(dims)), int(stride), *(_p(a) for a in src), *(_p(a) for a in out))
+    return {"dims": tuple(o), "stride": stride, "vel": out[0], "mean": out[1], "vort": out[2]}

@@ -22,6 +22,7 @@
  *   GPU voxelizer (f32) ....... src/voxelize/wgslVoxel.ts:33-322, VoxelizerGPU.ts:48-151
  *   CPU voxelizer (f64) ....... src/voxelize/voxelizeCPU.ts:11-199
  *   particle tracers .......... src/render/tracers.ts:3-106, render/wgslRender.ts:22-37
+ *   derived fields, export .... src/solver/wgslLbm.ts:527-592, SolverGPU.ts:374-425
  *
  * Arithmetic follows the WGSL expression order, evaluated left to right in IEEE single precision
  * without contraction (build with -ffp-contract=off). Float literals of the generated WGSL
@@ -1386,5 +1387,123 @@ int or_tracers(const wt_dims* d, const wt_tracer_params* p, const uint16_t* vel,
 }
 
 uint32_t or_pcg(uint32_t v) { return pcg(v); }
+
+/* Derived fields (src/solver/wgslLbm.ts:527-592): inputs are the half4 velocity texture (raw
+ * binary16 bits), the flags, the EMA statistics and uRef; outputs vort / stat / mean as raw
+ * binary16 x 4 per cell (the reference's rgba16float textures). */
+int or_derive(const wt_dims* d, float u_ref, const uint16_t* vel_h, const uint32_t* flags, const float* meanA,
+              const float* meanB, uint16_t* vort_h, uint16_t* stat_h, uint16_t* mean_h) {
+  const int NX = d->nx, NY = d->ny, NZ = d->nz;
+  const int dim = NZ > 1 ? 3 : 2;
+  const size_t N = (size_t)NX * NY * NZ;
+  auto cell = [&](int x, int y, int z) { return (size_t)x + (size_t)NX * ((size_t)y + (size_t)NY * (size_t)z); };
+  auto vel = [&](int x, int y, int z, float out[3]) {
+    x = x < 0 ? 0 : (x > NX - 1 ? NX - 1 : x);
+    y = y < 0 ? 0 : (y > NY - 1 ? NY - 1 : y);
+    z = z < 0 ? 0 : (z > NZ - 1 ? NZ - 1 : z);
+    const uint16_t* v = vel_h + 4 * cell(x, y, z);
+    for (int k = 0; k < 3; k++) {
+      _Float16 h;
+      std::memcpy(&h, v + k, 2);
+      out[k] = (float)h;
+    }
+  };
+  auto solidAt = [&](int x, int y, int z) {
+    if (x < 0 || y < 0 || z < 0 || x >= NX || y >= NY || z >= NZ) return false;
+    return flags[cell(x, y, z)] != 0u;
+  };
+  auto put = [&](uint16_t* o, const float v[4]) {
+    for (int k = 0; k < 4; k++) {
+      _Float16 h = (_Float16)v[k];
+      std::memcpy(o + k, &h, 2);
+    }
+  };
+#pragma omp parallel for schedule(static)
+  for (int64_t ii = 0; ii < (int64_t)N; ii++) {
+    const size_t idx = (size_t)ii;
+    const int x = (int)(idx % NX), y = (int)((idx / NX) % NY), z = (int)(idx / ((size_t)NX * NY));
+    const bool solid = flags[idx] != 0u;
+    float vort[4] = {0.f, 0.f, 0.f, 0.f};
+    if (!solid) {
+      float xp[3], xm[3], yp[3], ym[3], zp[3] = {0, 0, 0}, zm[3] = {0, 0, 0};
+      vel(x + 1, y, z, xp);
+      vel(x - 1, y, z, xm);
+      vel(x, y + 1, z, yp);
+      vel(x, y - 1, z, ym);
+      float J[3][3];  // J[j][i] = d u_i / d x_j; columns dx, dy, dz of mat3x3(dx, dy, dz)
+      for (int i = 0; i < 3; i++) {
+        J[0][i] = 0.5f * (xp[i] - xm[i]);
+        J[1][i] = 0.5f * (yp[i] - ym[i]);
+      }
+      if (dim == 3) {
+        vel(x, y, z + 1, zp);
+        vel(x, y, z - 1, zm);
+        for (int i = 0; i < 3; i++) J[2][i] = 0.5f * (zp[i] - zm[i]);
+      } else {
+        for (int i = 0; i < 3; i++) J[2][i] = 0.0f;
+      }
+      const float wx = J[1][2] - J[2][1];
+      const float wy = J[2][0] - J[0][2];
+      const float wz = J[0][1] - J[1][0];
+      float S2 = 0.0f, W2 = 0.0f;
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+          const float sv = 0.5f * (J[j][i] + J[i][j]);
+          const float wv = 0.5f * (J[j][i] - J[i][j]);
+          S2 += sv * sv;
+          W2 += wv * wv;
+        }
+      float near = 0.0f;
+      for (int dd = 1; dd <= 2; dd++)
+        for (int a = 0; a < dim; a++) {
+          const int ex = a == 0 ? dd : 0, ey = a == 1 ? dd : 0, ez = a == 2 ? dd : 0;
+          if (solidAt(x + ex, y + ey, z + ez) || solidAt(x - ex, y - ey, z - ez)) {
+            const float v = dd == 1 ? 1.0f : 0.5f;
+            near = near > v ? near : v;
+          }
+        }
+      vort[0] = wx;
+      vort[1] = wy;
+      vort[2] = wz;
+      vort[3] = 0.5f * (W2 - S2) * (1.0f - near);
+    }
+    const float* m = meanA + 4 * idx;
+    const float dotm = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+    float k = meanB[idx] - dotm;
+    k = k > 0.0f ? k : 0.0f;
+    const float ur = u_ref > 1e-6f ? u_ref : 1e-6f;
+    const float ti = std::sqrt(k / 3.0f) / ur;
+    const float st[4] = {solid ? 0.0f : ti, solid ? 1.0f : 0.0f, 0.0f, 0.0f};
+    put(vort_h + 4 * idx, vort);
+    put(stat_h + 4 * idx, st);
+    put(mean_h + 4 * idx, m);
+  }
+  return WT_OK;
+}
+
+/* Strided export (src/solver/SolverGPU.ts:374-425): the raw half4 fields at every stride-th cell,
+ * clamped to the last cell, x fastest. */
+int or_export(const wt_dims* d, int stride, const uint16_t* vel_h, const uint16_t* mean_h, const uint16_t* vort_h,
+              float* vel4, float* mean4, float* vort4) {
+  const int NX = d->nx, NY = d->ny, NZ = d->nz;
+  const int ox = (NX + stride - 1) / stride, oy = (NY + stride - 1) / stride, oz = (NZ + stride - 1) / stride;
+  const int64_t n = (int64_t)ox * oy * oz;
+  for (int64_t i = 0; i < n; i++) {
+    const int gx = (int)(i % ox), gy = (int)((i / ox) % oy), gz = (int)(i / ((int64_t)ox * oy));
+    const int px = gx * stride < NX - 1 ? gx * stride : NX - 1;
+    const int py = gy * stride < NY - 1 ? gy * stride : NY - 1;
+    const int pz = gz * stride < NZ - 1 ? gz * stride : NZ - 1;
+    const size_t c = (size_t)px + (size_t)NX * ((size_t)py + (size_t)NY * (size_t)pz);
+    const uint16_t* src[3] = {vel_h, mean_h, vort_h};
+    float* dst[3] = {vel4, mean4, vort4};
+    for (int f = 0; f < 3; f++)
+      for (int k = 0; k < 4; k++) {
+        _Float16 h;
+        std::memcpy(&h, src[f] + 4 * c + k, 2);
+        dst[f][4 * i + k] = (float)h;
+      }
+  }
+  return WT_OK;
+}
 
 }  // extern "C"

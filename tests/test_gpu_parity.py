@@ -264,6 +264,49 @@ def test_steps_after_voxelize_follow_oracle(gpu, oracle, prec):
     s.destroy()
 
 
+# ---- derived fields and export ---------------------------------------------------------------
+@pytest.mark.parametrize("dims", [(40, 18, 14), (64, 24, 1)])
+def test_derived_fields_and_export_bit_exact(gpu, oracle, dims):
+    flags, sdf, wheels = scene(dims)
+    s = Solver(dims, dict(PARAM_SETS["belt_periodic_les"], precision="f32"))
+    s.upload_flags(flags)
+    s.upload_sdf(sdf)
+    s.set_wheels(wheels)
+    for _ in range(4):
+        s.step_and_sample(10)  # EMA statistics with alpha 0.1
+    s.derive_fields()
+    vort, stat, mean = s.read_derived()
+    vel = s.read_velocity().astype(np.float16)
+    ma, mb = s.read_means()
+    ov, os_, om = oracle.derive(dims, s.kparams().u_ref, vel, flags, ma, mb)
+    np.testing.assert_array_equal(vort, ov.astype(np.float32))
+    np.testing.assert_array_equal(stat, os_.astype(np.float32))
+    np.testing.assert_array_equal(mean, om.astype(np.float32))
+    fluid = flags == 0
+    assert np.abs(vort[fluid, :3]).max() > 0 and (stat[~fluid, 1] == 1).all() and (stat[fluid, 1] == 0).all()
+    for stride in (1, 2, 3, 7):
+        e = s.export_fields(stride)
+        r = oracle.export(dims, stride, vel, om, ov)
+        assert e["dims"] == r["dims"] and e["stride"] == stride
+        for k in ("vel", "mean", "vort"):
+            np.testing.assert_array_equal(e[k], r[k], err_msg=f"{k} stride {stride}")
+    s.destroy()
+
+
+def test_backend_export_stride(gpu):
+    from windtunnel_vis_b200.solver import Backend
+
+    b = Backend()
+    b.create_solver((64, 32, 16), dict(u=0.05, nu=0.02))
+    b.frame(4)
+    n = 64 * 32 * 16
+    for max_points, stride in ((n, 1), (n // 8, 2), (n // 8 - 1, 3), (1000, 4)):
+        e = b.export_fields(max_points)
+        assert e["stride"] == stride
+        assert e["vel"].shape[0] == np.prod(e["dims"]) and e["dims"] == tuple(-(-d // stride) for d in (64, 32, 16))
+    b.destroy()
+
+
 # ---- tracers ---------------------------------------------------------------------------------
 @pytest.mark.parametrize("dims,emitter", [((48, 24, 16), 0), ((48, 24, 16), 1), ((64, 32, 1), 0), ((64, 32, 1), 1)])
 def test_tracers_bit_exact(gpu, oracle, dims, emitter):

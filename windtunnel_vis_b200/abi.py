@@ -151,6 +151,9 @@ def _sig(lib):
         "wt_advect_tracers": ([S, P(TracerParams)], C.c_int),
         "wt_read_tracers": ([S, v, i64, v, i64], C.c_int),
         "wt_write_tracers": ([S, v, i64, v, i64, C.c_uint32], C.c_int),
+        "wt_derive_fields": ([S], C.c_int),
+        "wt_read_derived": ([S, v, v, v, i64], C.c_int),
+        "wt_export_fields": ([S, i32, v, v, v, i64], C.c_int),
         "wt_set_launch": ([S, i32, i32, i32, i32], C.c_int),
         "wt_get_launch": ([S, P(i32)], C.c_int),
         "wt_autotune": ([S, i32, P(i32)], C.c_int),

@@ -5,7 +5,7 @@
 Each .cu in csrc/ is compiled by nvcc to an object in _build/, then linked into
 windtunnel_vis_b200/libwt.so with the static CUDA runtime. The voxelizer and tracer units are
 compiled with -fmad=false (no contraction) so their f32 results are bit-identical to the CPU
-restatement; the LBM unit keeps FMA contraction (it is bandwidth-bound and checked within
+restatement, as is the derived-field unit; the LBM unit keeps FMA contraction (it is bandwidth-bound and checked within
 stated tolerances).
 """
 import os
@@ -27,6 +27,7 @@ UNITS = {
     "wt_lbm.cu": [],
     "wt_voxel.cu": ["-fmad=false"],
     "wt_tracer.cu": ["-fmad=false"],
+    "wt_fields.cu": ["-fmad=false"],
 }
 HEADERS = ["wt_common.cuh", "wt_internal.h"]
 

@@ -69,7 +69,8 @@ int64_t bytes_for(const wt_dims* d, int prec) {
 void free_all(wt_solver* s) {
   void* bufs[] = {s->f[0], s->f[1], s->flags, s->sdf, s->cls, s->vel, s->vel_f32, s->meanA, s->meanB,
                   s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count,
-                  s->bcell, s->brec, s->bgam, s->vox_pos, s->vox_idx, s->vox_info};
+                  s->bcell, s->brec, s->bgam, s->vox_pos, s->vox_idx, s->vox_info,
+                  s->dvort, s->dstat, s->dmean, s->exp_buf};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->result_host) cudaFreeHost(s->result_host);
@@ -612,6 +613,68 @@ int wt_read_means(wt_solver* s, float* mean4, float* meanb, int64_t n) {
   if (mean4) WT_CUDA(s, cudaMemcpyAsync(mean4, s->meanA, s->n * 16, cudaMemcpyDeviceToHost, s->stream), "read meanA");
   if (meanb) WT_CUDA(s, cudaMemcpyAsync(meanb, s->meanB, s->n * 4, cudaMemcpyDeviceToHost, s->stream), "read meanB");
   WT_CUDA(s, cudaStreamSynchronize(s->stream), "read means");
+  return WT_OK;
+}
+
+int wt_derive_fields(wt_solver* s) {
+  if (!s) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  for (uint2** b : {&s->dvort, &s->dstat, &s->dmean})
+    if (!*b) WT_CUDA(s, cudaMalloc((void**)b, s->n * 8), "cudaMalloc(derived fields)");
+  WT_CUDA(s, wt::launch_derive(s), "derive fields");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "derive fields");
+  return WT_OK;
+}
+
+int wt_read_derived(wt_solver* s, float* vort4, float* stat4, float* mean4, int64_t n) {
+  if (!s || (size_t)n != s->n) return WT_E_INVALID;
+  if (!s->dvort) return fail(s, WT_E_STATE, "wt_read_derived: no derived fields yet (call wt_derive_fields)");
+  DeviceGuard g(s->device);
+  // widened on the device through the export staging buffer, one field at a time
+  const size_t need = s->n;
+  if (s->exp_cap < need) {
+    if (s->exp_buf) cudaFree(s->exp_buf);
+    s->exp_buf = nullptr;
+    s->exp_cap = 0;
+    WT_CUDA(s, cudaMalloc((void**)&s->exp_buf, need * 16), "cudaMalloc(export)");
+    s->exp_cap = need;
+  }
+  const uint2* src[3] = {s->dvort, s->dstat, s->dmean};
+  float* dst[3] = {vort4, stat4, mean4};
+  for (int k = 0; k < 3; k++) {
+    if (!dst[k]) continue;
+    WT_CUDA(s, wt::launch_widen_half4(s, src[k], s->exp_buf, s->n), "read derived");
+    WT_CUDA(s, cudaMemcpyAsync(dst[k], s->exp_buf, s->n * 16, cudaMemcpyDeviceToHost, s->stream), "read derived");
+    WT_CUDA(s, cudaStreamSynchronize(s->stream), "read derived");
+  }
+  return WT_OK;
+}
+
+int wt_export_fields(wt_solver* s, int32_t stride, float* vel4, float* mean4, float* vort4, int64_t points) {
+  if (!s || stride < 1) return WT_E_INVALID;
+  const int ox = (s->dims.nx + stride - 1) / stride, oy = (s->dims.ny + stride - 1) / stride,
+            oz = (s->dims.nz + stride - 1) / stride;
+  const int64_t n = (int64_t)ox * oy * oz;
+  if (points != n)
+    return fail(s, WT_E_INVALID, "wt_export_fields: points != ceil(nx/stride) * ceil(ny/stride) * ceil(nz/stride)");
+  int rc = wt_derive_fields(s);
+  if (rc) return rc;
+  DeviceGuard g(s->device);
+  const size_t need = 3 * (size_t)n;
+  if (s->exp_cap < need) {
+    if (s->exp_buf) cudaFree(s->exp_buf);
+    s->exp_buf = nullptr;
+    s->exp_cap = 0;
+    WT_CUDA(s, cudaMalloc((void**)&s->exp_buf, need * 16), "cudaMalloc(export)");
+    s->exp_cap = need;
+  }
+  WT_CUDA(s, wt::launch_export(s, stride, ox, oy, oz, s->exp_buf), "export fields");
+  float* dst[3] = {vel4, mean4, vort4};
+  for (int k = 0; k < 3; k++)
+    if (dst[k])
+      WT_CUDA(s, cudaMemcpyAsync(dst[k], s->exp_buf + k * n, (size_t)n * 16, cudaMemcpyDeviceToHost, s->stream),
+              "export fields");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "export fields");
   return WT_OK;
 }
 

@@ -63,6 +63,13 @@ struct wt_solver {
   double* result_dev = nullptr;  // 8 doubles
   double* result_host = nullptr; // pinned
   wt::Wheels wheels{};
+  // derived fields (binary16 x 4 per cell, allocated by the first wt_derive_fields): vorticity and
+  // Q, turbulence intensity and the solid mask, the mean field; and the export staging buffer
+  uint2* dvort = nullptr;
+  uint2* dstat = nullptr;
+  uint2* dmean = nullptr;
+  float4* exp_buf = nullptr;
+  size_t exp_cap = 0;  // float4 elements
   // voxelizer: device copies of the last mesh (grown as needed) and the 8-word info block
   void* vox_pos = nullptr;
   void* vox_idx = nullptr;
@@ -103,6 +110,11 @@ struct VoxelJob {
   uint32_t* info;
 };
 cudaError_t launch_voxelize(wt_solver* s, const VoxelJob& job);
+
+// derived fields and export (wt_fields.cu)
+cudaError_t launch_derive(wt_solver* s);
+cudaError_t launch_export(wt_solver* s, int stride, int ox, int oy, int oz, float4* out);
+cudaError_t launch_widen_half4(wt_solver* s, const uint2* src, float4* dst, size_t n);
 
 // tracers (wt_tracer.cu)
 cudaError_t launch_tracers(wt_solver* s, const wt_tracer_params& p);

@@ -12,6 +12,7 @@ back as the SolverStats dict (fx, fy, fz, maxU, rhoRef, unstable, step). Errors 
 with the library's message. Every call runs on the GPU through libwt.so; there is no CPU path.
 """
 import ctypes as C
+import math
 
 import numpy as np
 
@@ -188,6 +189,27 @@ class Solver:
         self._check(self._lib.wt_read_means(self._h, _ptr(a), _ptr(b), self.n))
         return a, b
 
+    # ---- derived fields / export ---------------------------------------------------------------
+    def derive_fields(self):
+        """The derived pass: vorticity, Q-criterion, turbulence intensity, binary16 mean field."""
+        self._check(self._lib.wt_derive_fields(self._h))
+
+    def read_derived(self):
+        """(vort (n, 4) = wx, wy, wz, Q; stat (n, 4) = TI, solid, 0, 0; mean (n, 4)) as float32."""
+        out = [np.empty((self.n, 4), np.float32) for _ in range(3)]
+        self._check(self._lib.wt_read_derived(self._h, *(_ptr(a) for a in out), self.n))
+        return tuple(out)
+
+    def export_fields(self, stride: int):
+        """SolverGPU.exportFields: FieldExport dict {dims, stride, vel, mean, vort}, every field a
+        float32 array of shape (points, 4), x fastest."""
+        stride = int(stride)
+        o = [-(-d // stride) for d in self.dims]
+        n = o[0] * o[1] * o[2]
+        vel, mean, vort = (np.empty((n, 4), np.float32) for _ in range(3))
+        self._check(self._lib.wt_export_fields(self._h, stride, _ptr(vel), _ptr(mean), _ptr(vort), n))
+        return {"dims": tuple(o), "stride": stride, "vel": vel, "mean": mean, "vort": vort}
+
     # ---- launch shape ------------------------------------------------------------------------
     def set_launch(self, kernel, param, bx=0, by=0):
         """Stream-collide launch: kernel = occupancy hint (0 none, 2..4 CTAs of 256 threads per
@@ -302,6 +324,12 @@ class Backend:
         if on_stats:
             on_stats(st)
         return st
+
+    def export_fields(self, max_points: int):
+        """Backend.exportFields (src/backend/webgpu.ts:133-137): the stride that keeps the point
+        count at or below about max_points, then SolverGPU.exportFields."""
+        stride = max(1, math.ceil(float(np.cbrt(self.solver.n / max_points))))
+        return self.solver.export_fields(stride)
 
     def solver_factory(self):
         return solver_factory
