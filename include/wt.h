@@ -137,6 +137,17 @@ typedef struct wt_tracer_params {
   float rake_d[4];
 } wt_tracer_params;
 
+/* Streamline uniform SLU (src/render/tracers.ts:152-160) as packed by RendererGPU
+ * (src/render/RendererGPU.ts:544-557): seeds = seeds per line x rake lines, points per line,
+ * use_mean (0 instantaneous, 1 mean field), per_line = seeds per line; h = step length in cells. */
+typedef struct wt_streamline_params {
+  uint32_t seeds, points, use_mean, per_line;
+  float rake_a[4];
+  float rake_b[4];
+  float h, p0, p1, p2;
+  float rake_d[4];
+} wt_streamline_params;
+
 typedef struct wt_solver wt_solver;
 
 /* ---- library ---------------------------------------------------------------------------- */
@@ -235,6 +246,15 @@ int wt_read_derived(wt_solver* s, float* vort4, float* stat4, float* mean4, int6
  * points = ceil(nx/stride) * ceil(ny/stride) * ceil(nz/stride) float4 each (x fastest); any
  * output pointer may be NULL. */
 int wt_export_fields(wt_solver* s, int32_t stride, float* vel4, float* mean4, float* vort4, int64_t points);
+
+/* Streamlines (the streamline pass, src/render/tracers.ts:152-200): seeds x points float4
+ * (x, y, z, speed; speed = -1 once the line has ended), seed-major. Mean-field lines use the
+ * mean field of the derived pass, which this call runs first. */
+int wt_streamlines(wt_solver* s, const wt_streamline_params* p, float* pts4, int64_t n);
+/* Probes (the probe pass, src/render/tracers.ts:109-125; Backend.probeData): up to 8 points
+ * (pos4: x, y, z, unused) -> out8 per probe: instantaneous (ux, uy, uz, rho) then the mean. Runs
+ * the derived pass first for the mean field. */
+int wt_probes(wt_solver* s, const float* pos4, int32_t count, float* out8);
 
 /* ---- launch selection (extension; no counterpart in the reference) ------------------------ */
 /* Selects the stream-collide launch: `param` cells per thread along x (1, 2 or 4; 2 and 4 need

@@ -43,6 +43,8 @@ def lib():
         L.or_tracers.argtypes = [P(abi.Dims), P(abi.TracerParams), v, v, v, v]
         L.or_derive.argtypes = [P(abi.Dims), C.c_float, v, v, v, v, v, v, v]
         L.or_export.argtypes = [P(abi.Dims), C.c_int, v, v, v, v, v, v]
+        L.or_streamlines.argtypes = [P(abi.Dims), P(abi.StreamlineParams), C.c_float, v, v, v, v]
+        L.or_probes.argtypes = [P(abi.Dims), v, C.c_int, v, v, v]
         L.or_pcg.argtypes = [C.c_uint32]
         L.or_pcg.restype = C.c_uint32
         _lib = L
@@ -262,3 +264,24 @@ def export(dims, stride, vel_half4, mean_half4, vort_half4):
     out = [np.zeros((n, 4), np.float32) for _ in range(3)]
     lib().or_export(C.byref(dims_of(dims)), int(stride), *(_p(a) for a in src), *(_p(a) for a in out))
     return {"dims": tuple(o), "stride": stride, "vel": out[0], "mean": out[1], "vort": out[2]}
+
+
+def streamlines(dims, sp, u_lat, vel_half4, mean_half4, flags):
+    """Streamline pass: (seeds * points, 4) float32, seed-major."""
+    n = sp.seeds * sp.points
+    out = np.zeros((n, 4), np.float32)
+    vel = np.ascontiguousarray(vel_half4, np.float16).view(np.uint16)
+    mean = np.ascontiguousarray(mean_half4, np.float16).view(np.uint16)
+    lib().or_streamlines(C.byref(dims_of(dims)), C.byref(sp), float(np.float32(u_lat)), _p(vel), _p(mean),
+                         _p(np.ascontiguousarray(flags, np.uint32)), _p(out))
+    return out
+
+
+def probes(dims, pos4, vel_half4, mean_half4):
+    """Probe pass: (count, 8) float32 = instantaneous (ux, uy, uz, rho) and mean."""
+    pos = np.ascontiguousarray(pos4, np.float32).reshape(-1, 4)
+    out = np.zeros((pos.shape[0], 8), np.float32)
+    vel = np.ascontiguousarray(vel_half4, np.float16).view(np.uint16)
+    mean = np.ascontiguousarray(mean_half4, np.float16).view(np.uint16)
+    lib().or_probes(C.byref(dims_of(dims)), _p(pos), pos.shape[0], _p(vel), _p(mean), _p(out))
+    return out

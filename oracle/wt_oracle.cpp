@@ -23,6 +23,7 @@
  *   CPU voxelizer (f64) ....... src/voxelize/voxelizeCPU.ts:11-199
  *   particle tracers .......... src/render/tracers.ts:3-106, render/wgslRender.ts:22-37
  *   derived fields, export .... src/solver/wgslLbm.ts:527-592, SolverGPU.ts:374-425
+ *   streamlines, probes ....... src/render/tracers.ts:109-125, 152-200
  *
  * Arithmetic follows the WGSL expression order, evaluated left to right in IEEE single precision
  * without contraction (build with -ffp-contract=off). Float literals of the generated WGSL
@@ -805,6 +806,32 @@ struct Tr {
     }
     return v3(out[0], out[1], out[2]);
   }
+  /* the same sampling of all four channels of any half4 field */
+  void sF4(const uint16_t* f, V3 p, float out[4]) const {
+    int n[3] = {(int)dims[0], (int)dims[1], (int)dims[2]};
+    float t[3] = {p.x / dims[0], p.y / dims[1], p.z / dims[2]};
+    if (dims[3] > 0.5f) t[2] = 0.5f;
+    int i0[3], i1[3];
+    float fr[3];
+    for (int a = 0; a < 3; a++) {
+      float u = t[a] * (float)n[a] - 0.5f;
+      float fl = std::floor(u);
+      fr[a] = u - fl;
+      int k = f2i(fl);
+      i0[a] = k < 0 ? 0 : (k > n[a] - 1 ? n[a] - 1 : k);
+      i1[a] = k + 1 < 0 ? 0 : (k + 1 > n[a] - 1 ? n[a] - 1 : k + 1);
+    }
+    for (int ch = 0; ch < 4; ch++) {
+      auto at = [&](int x, int y, int z) { return h2f(f[4 * ((size_t)x + (size_t)n[0] * ((size_t)y + (size_t)n[1] * z)) + ch]); };
+      float c00 = at(i0[0], i0[1], i0[2]) * (1.0f - fr[0]) + at(i1[0], i0[1], i0[2]) * fr[0];
+      float c10 = at(i0[0], i1[1], i0[2]) * (1.0f - fr[0]) + at(i1[0], i1[1], i0[2]) * fr[0];
+      float c01 = at(i0[0], i0[1], i1[2]) * (1.0f - fr[0]) + at(i1[0], i0[1], i1[2]) * fr[0];
+      float c11 = at(i0[0], i1[1], i1[2]) * (1.0f - fr[0]) + at(i1[0], i1[1], i1[2]) * fr[0];
+      float c0 = c00 * (1.0f - fr[1]) + c10 * fr[1];
+      float c1 = c01 * (1.0f - fr[1]) + c11 * fr[1];
+      out[ch] = c0 * (1.0f - fr[2]) + c1 * fr[2];
+    }
+  }
   V3 vel3(V3 p) const {
     V3 v = sVel(p);
     if (dims[3] > 0.5f) v.z = 0.0f;
@@ -1387,6 +1414,87 @@ int or_tracers(const wt_dims* d, const wt_tracer_params* p, const uint16_t* vel,
 }
 
 uint32_t or_pcg(uint32_t v) { return pcg(v); }
+
+/* Streamlines (src/render/tracers.ts:152-200): pts seeds x points float4, seed-major. */
+int or_streamlines(const wt_dims* d, const wt_streamline_params* S, float u_lat, const uint16_t* vel,
+                   const uint16_t* mean, const uint32_t* flags, float* pts) {
+  Tr T;
+  std::memset(&T, 0, sizeof T);
+  T.dims[0] = (float)d->nx;
+  T.dims[1] = (float)d->ny;
+  T.dims[2] = (float)d->nz;
+  T.dims[3] = d->nz == 1 ? 1.0f : 0.0f;
+  T.vel = vel;
+  T.flags = flags;
+  const bool is2D = T.dims[3] > 0.5f;
+  auto velf = [&](V3 p) {
+    float v4[4];
+    T.sF4(S->use_mean ? mean : vel, p, v4);
+    V3 v = v3(v4[0], v4[1], v4[2]);
+    if (is2D) v.z = 0.0f;
+    return v;
+  };
+  auto outside = [&](V3 p) {
+    if (is2D) return p.x < 0.0f || p.y < 0.0f || p.x >= T.dims[0] || p.y >= T.dims[1];
+    return p.x < 0.0f || p.y < 0.0f || p.z < 0.0f || p.x >= T.dims[0] || p.y >= T.dims[1] || p.z >= T.dims[2];
+  };
+  const uint32_t per = S->per_line > 1u ? S->per_line : 1u;
+  for (uint32_t s = 0; s < S->seeds; s++) {
+    const float l = (float)(s / per) - 0.5f * (float)(S->seeds / per - 1u);
+    const float t = ((float)(s % per) + 0.5f) / (float)per;
+    V3 A = v3(S->rake_a[0], S->rake_a[1], S->rake_a[2]), B = v3(S->rake_b[0], S->rake_b[1], S->rake_b[2]);
+    V3 D = v3(S->rake_d[0], S->rake_d[1], S->rake_d[2]);
+    V3 p = add(add(mul(A, 1.0f - t), mul(B, t)), mul(D, l));
+    if (is2D) p.z = 0.5f;
+    bool alive = true;
+    const float U = u_lat > 1e-5f ? u_lat : 1e-5f;
+    for (uint32_t k = 0; k < S->points; k++) {
+      const V3 v = velf(p);
+      const float sp = len(v);
+      if (alive && (outside(p) || T.solidAt(p) || sp < U * 1e-3f)) alive = false;
+      float* o = pts + 4 * ((size_t)s * S->points + k);
+      o[0] = p.x;
+      o[1] = p.y;
+      o[2] = p.z;
+      o[3] = alive ? sp : -1.0f;
+      if (!alive) continue;
+      const V3 a = v3(v.x / sp, v.y / sp, v.z / sp);
+      const V3 vm = velf(add(p, mul(a, 0.5f * S->h)));
+      const float lm = len(vm);
+      if (lm < 1e-9f) {
+        alive = false;
+        continue;
+      }
+      p = add(p, mul(v3(vm.x / lm, vm.y / lm, vm.z / lm), S->h));
+    }
+  }
+  return WT_OK;
+}
+
+/* Probes (src/render/tracers.ts:109-125): out 2 float4 per probe (instantaneous, mean). */
+int or_probes(const wt_dims* d, const float* pos4, int count, const uint16_t* vel, const uint16_t* mean, float* out) {
+  Tr T;
+  std::memset(&T, 0, sizeof T);
+  T.dims[0] = (float)d->nx;
+  T.dims[1] = (float)d->ny;
+  T.dims[2] = (float)d->nz;
+  T.dims[3] = d->nz == 1 ? 1.0f : 0.0f;
+  for (int i = 0; i < count; i++) {
+    V3 p = v3(pos4[4 * i], pos4[4 * i + 1], pos4[4 * i + 2]);
+    float v[4], m[4];
+    T.sF4(vel, p, v);
+    T.sF4(mean, p, m);
+    if (T.dims[3] > 0.5f) {
+      v[2] = 0.0f;
+      m[2] = 0.0f;
+    }
+    for (int k = 0; k < 4; k++) {
+      out[8 * i + k] = v[k];
+      out[8 * i + 4 + k] = m[k];
+    }
+  }
+  return WT_OK;
+}
 
 /* Derived fields (src/solver/wgslLbm.ts:527-592): inputs are the half4 velocity texture (raw
  * binary16 bits), the flags, the EMA statistics and uRef; outputs vort / stat / mean as raw

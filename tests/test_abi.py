@@ -41,6 +41,7 @@ def test_library_exports_every_declared_symbol(wtlib):
 STRUCTS = {
     "wt_dims": abi.Dims, "wt_params": abi.Params, "wt_kparams": abi.KParams, "wt_stats": abi.Stats,
     "wt_wheel": abi.Wheel, "wt_voxel_info": abi.VoxelInfo, "wt_tracer_params": abi.TracerParams,
+    "wt_streamline_params": abi.StreamlineParams,
 }
 
 

@@ -307,6 +307,39 @@ def test_backend_export_stride(gpu):
     b.destroy()
 
 
+@pytest.mark.parametrize("dims", [(48, 24, 16), (64, 32, 1)])
+def test_streamlines_and_probes_bit_exact(gpu, oracle, dims):
+    flags, sdf, wheels = scene(dims)
+    s = Solver(dims, dict(PARAM_SETS["freeslip_reg"], init="rest_noise", initNoise=0.02))
+    s.upload_flags(flags)
+    s.upload_sdf(sdf)
+    for _ in range(3):
+        s.step_and_sample(20)
+    vel = s.read_velocity().astype(np.float16)
+    u_lat = s.kparams().uin
+    for use_mean in (0, 1):
+        sp = abi.StreamlineParams(seeds=3 * 14, points=120, use_mean=use_mean, per_line=14)
+        sp.rake_a[:] = [3.0, 2.0, 2.0, 0.0]
+        sp.rake_b[:] = [3.0, dims[1] - 2.0, max(dims[2] - 2.0, 0.5), 0.0]
+        sp.rake_d[:] = [0.0, 0.0, 2.5, 0.0]
+        sp.h = 0.7
+        pts = s.streamlines(sp)
+        mean = s.read_derived()[2].astype(np.float16) if use_mean else vel
+        ref = oracle.streamlines(dims, sp, u_lat, vel, mean, flags)
+        np.testing.assert_array_equal(pts, ref, err_msg=f"use_mean {use_mean}")
+        alive = pts[:, 3] >= 0
+        assert alive.sum() > 0 and (~alive).sum() > 0  # lines advance, and some end
+    pos = [(5.5, 7.25, 3.1), (20.0, 12.0, 8.0), (30.7, 3.3, 1.0)]
+    pr = s.probes(pos)
+    _, _, mean = s.read_derived()
+    p4 = np.zeros((3, 4), np.float32)
+    p4[:, :3] = pos
+    ref = oracle.probes(dims, p4, vel, mean.astype(np.float16))
+    got = np.array([p["inst"] + p["mean"] for p in pr], np.float32)
+    np.testing.assert_array_equal(got, ref)
+    s.destroy()
+
+
 # ---- tracers ---------------------------------------------------------------------------------
 @pytest.mark.parametrize("dims,emitter", [((48, 24, 16), 0), ((48, 24, 16), 1), ((64, 32, 1), 0), ((64, 32, 1), 1)])
 def test_tracers_bit_exact(gpu, oracle, dims, emitter):

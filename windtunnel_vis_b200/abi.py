@@ -74,6 +74,15 @@ class TracerParams(C.Structure):
     ]
 
 
+class StreamlineParams(C.Structure):
+    _fields_ = [
+        ("seeds", C.c_uint32), ("points", C.c_uint32), ("use_mean", C.c_uint32), ("per_line", C.c_uint32),
+        ("rake_a", C.c_float * 4), ("rake_b", C.c_float * 4),
+        ("h", C.c_float), ("p0", C.c_float), ("p1", C.c_float), ("p2", C.c_float),
+        ("rake_d", C.c_float * 4),
+    ]
+
+
 def make_params(p: dict) -> Params:
     """SolverParams dict (reference field names, types.ts:3-29) -> wt_params with the reference's
     defaults for the optional fields (tauWall 0.5, interp true, spongeIn 0, f32, regularized)."""
@@ -154,6 +163,8 @@ def _sig(lib):
         "wt_derive_fields": ([S], C.c_int),
         "wt_read_derived": ([S, v, v, v, i64], C.c_int),
         "wt_export_fields": ([S, i32, v, v, v, i64], C.c_int),
+        "wt_streamlines": ([S, P(StreamlineParams), v, i64], C.c_int),
+        "wt_probes": ([S, v, i32, v], C.c_int),
         "wt_set_launch": ([S, i32, i32, i32, i32], C.c_int),
         "wt_get_launch": ([S, P(i32)], C.c_int),
         "wt_autotune": ([S, i32, P(i32)], C.c_int),

@@ -70,7 +70,7 @@ void free_all(wt_solver* s) {
   void* bufs[] = {s->f[0], s->f[1], s->flags, s->sdf, s->cls, s->vel, s->vel_f32, s->meanA, s->meanB,
                   s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count,
                   s->bcell, s->brec, s->bgam, s->vox_pos, s->vox_idx, s->vox_info,
-                  s->dvort, s->dstat, s->dmean, s->exp_buf};
+                  s->dvort, s->dstat, s->dmean, s->exp_buf, s->probe_buf};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->result_host) cudaFreeHost(s->result_host);
@@ -675,6 +675,44 @@ int wt_export_fields(wt_solver* s, int32_t stride, float* vel4, float* mean4, fl
       WT_CUDA(s, cudaMemcpyAsync(dst[k], s->exp_buf + k * n, (size_t)n * 16, cudaMemcpyDeviceToHost, s->stream),
               "export fields");
   WT_CUDA(s, cudaStreamSynchronize(s->stream), "export fields");
+  return WT_OK;
+}
+
+static int ensure_export(wt_solver* s, size_t float4s) {
+  if (s->exp_cap >= float4s) return WT_OK;
+  if (s->exp_buf) cudaFree(s->exp_buf);
+  s->exp_buf = nullptr;
+  s->exp_cap = 0;
+  WT_CUDA(s, cudaMalloc((void**)&s->exp_buf, float4s * 16), "cudaMalloc(export)");
+  s->exp_cap = float4s;
+  return WT_OK;
+}
+
+int wt_streamlines(wt_solver* s, const wt_streamline_params* p, float* pts4, int64_t n) {
+  if (!s || !p || !pts4 || n != (int64_t)p->seeds * (int64_t)p->points) return WT_E_INVALID;
+  if (p->seeds == 0 || p->points == 0) return WT_OK;
+  DeviceGuard g(s->device);
+  int rc = WT_OK;
+  if (p->use_mean) rc = wt_derive_fields(s);
+  if (!rc) rc = ensure_export(s, (size_t)n);
+  if (rc) return rc;
+  WT_CUDA(s, wt::launch_streamlines(s, *p, s->exp_buf), "streamlines");
+  WT_CUDA(s, cudaMemcpyAsync(pts4, s->exp_buf, (size_t)n * 16, cudaMemcpyDeviceToHost, s->stream), "streamlines");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "streamlines");
+  return WT_OK;
+}
+
+int wt_probes(wt_solver* s, const float* pos4, int32_t count, float* out8) {
+  if (!s || count < 0 || count > 8 || (count > 0 && (!pos4 || !out8))) return WT_E_INVALID;
+  if (count == 0) return WT_OK;
+  int rc = wt_derive_fields(s);
+  if (rc) return rc;
+  DeviceGuard g(s->device);
+  if (!s->probe_buf) WT_CUDA(s, cudaMalloc((void**)&s->probe_buf, 24 * 16), "cudaMalloc(probes)");
+  WT_CUDA(s, cudaMemcpyAsync(s->probe_buf, pos4, (size_t)count * 16, cudaMemcpyHostToDevice, s->stream), "probes");
+  WT_CUDA(s, wt::launch_probes(s, s->probe_buf, count, s->probe_buf + 8), "probes");
+  WT_CUDA(s, cudaMemcpyAsync(out8, s->probe_buf + 8, (size_t)count * 32, cudaMemcpyDeviceToHost, s->stream), "probes");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "probes");
   return WT_OK;
 }
 

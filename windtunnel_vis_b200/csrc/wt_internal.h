@@ -70,6 +70,7 @@ struct wt_solver {
   uint2* dmean = nullptr;
   float4* exp_buf = nullptr;
   size_t exp_cap = 0;  // float4 elements
+  float4* probe_buf = nullptr;  // 8 positions + 16 results
   // voxelizer: device copies of the last mesh (grown as needed) and the 8-word info block
   void* vox_pos = nullptr;
   void* vox_idx = nullptr;
@@ -116,8 +117,10 @@ cudaError_t launch_derive(wt_solver* s);
 cudaError_t launch_export(wt_solver* s, int stride, int ox, int oy, int oz, float4* out);
 cudaError_t launch_widen_half4(wt_solver* s, const uint2* src, float4* dst, size_t n);
 
-// tracers (wt_tracer.cu)
+// tracers, streamlines and probes (wt_tracer.cu)
 cudaError_t launch_tracers(wt_solver* s, const wt_tracer_params& p);
+cudaError_t launch_streamlines(wt_solver* s, const wt_streamline_params& p, float4* pts);
+cudaError_t launch_probes(wt_solver* s, const float4* pos, int count, float4* out);
 
 // records `msg` as the calling thread's message for wt_last_error(NULL) and returns `code`
 int fail_unbound(int code, const std::string& msg);

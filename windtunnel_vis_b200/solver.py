@@ -210,6 +210,21 @@ class Solver:
         self._check(self._lib.wt_export_fields(self._h, stride, _ptr(vel), _ptr(mean), _ptr(vort), n))
         return {"dims": tuple(o), "stride": stride, "vel": vel, "mean": mean, "vort": vort}
 
+    def streamlines(self, sp: abi.StreamlineParams):
+        """The streamline pass: (seeds * points, 4) float32 (x, y, z, speed; -1 after the end)."""
+        out = np.empty((sp.seeds * sp.points, 4), np.float32)
+        self._check(self._lib.wt_streamlines(self._h, C.byref(sp), _ptr(out), out.shape[0]))
+        return out
+
+    def probes(self, positions):
+        """Backend.probeData: per probe {'inst': [ux, uy, uz, rho], 'mean': [...]} (at most 8)."""
+        pos = np.zeros((len(positions), 4), np.float32)
+        for k, p in enumerate(positions):
+            pos[k, :3] = p[:3]
+        out = np.empty((len(positions), 8), np.float32)
+        self._check(self._lib.wt_probes(self._h, _ptr(pos), len(positions), _ptr(out)))
+        return [{"inst": out[k, :4].tolist(), "mean": out[k, 4:].tolist()} for k in range(len(positions))]
+
     # ---- launch shape ------------------------------------------------------------------------
     def set_launch(self, kernel, param, bx=0, by=0):
         """Stream-collide launch: kernel = occupancy hint (0 none, 2..4 CTAs of 256 threads per
@@ -330,6 +345,10 @@ class Backend:
         count at or below about max_points, then SolverGPU.exportFields."""
         stride = max(1, math.ceil(float(np.cbrt(self.solver.n / max_points))))
         return self.solver.export_fields(stride)
+
+    def probe_data(self, positions):
+        """Backend.probeData: instantaneous and mean samples at up to 8 probe points."""
+        return self.solver.probes(positions)
 
     def solver_factory(self):
         return solver_factory
