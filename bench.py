@@ -129,6 +129,25 @@ def cpu_port_mlups(seconds=12.0, threads=0, steps_cap=None):
     return n * done / dt / 1e6, th, done
 
 
+def max_over_ranks(dist, v):
+    """The slowest rank's time (ms or s): an all-reduce MAX over the process group (a CUDA tensor
+    for NCCL, a CPU one for gloo); v itself with one process."""
+    if dist is None:
+        return v
+    import torch
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_mlups(world, cells, updates, ms):
+    """Whole-job lattice updates per second over `world` independent tunnels of `cells` cells,
+    each advanced `updates` steps in `ms` milliseconds (the slowest rank's time), in MLUPS."""
+    return world * cells * updates / (ms / 1e3) / 1e6
+
+
 def components(s, peak, no_cpu):
     """Timings of the other kernels on the path, rank 0 at N = 1 (each with its CPU restatement
     timed beside it on the host cores):
@@ -316,12 +335,8 @@ def run_ours(args, rank, world, local_rank, dist):
     launches = s.launches - launches0
     ms = t_start.elapsed_time(t_end)
     sc_ms = sum(a.elapsed_time(b) for a, b in ev) / (args.steps * CHUNK)
-    ms_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = world * n * CHUNK * args.steps / (ms_max / 1e3) / 1e6
+    ms_max = max_over_ranks(dist, ms)
+    value = replica_mlups(world, n, CHUNK * args.steps, ms_max)
 
     # end to end through the public API with host buffers
     fl_h = torch.from_numpy(flags).pin_memory()
@@ -339,11 +354,8 @@ def run_ours(args, rank, world, local_rank, dist):
         st = s.step_and_sample(CHUNK)
         s.read_velocity(vel_h.numpy())
     e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * n * CHUNK * e2e_steps / e2e_s / 1e6
+    e2e_s = max_over_ranks(dist, e2e_s)
+    e2e = replica_mlups(world, n, CHUNK * e2e_steps, e2e_s * 1e3)
 
     if rank != 0:
         s.destroy()
