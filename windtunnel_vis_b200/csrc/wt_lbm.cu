@@ -984,7 +984,9 @@ __global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kpara
     c0 = cv & 0xffu;
     c1 = (cv >> 8) & 0xffu;
   }
-  if ((cv & 0x03030303u) != 0u) return;
+  // groups holding solid / near-solid cells belong to k_boundary_tab: their loads are still issued
+  // (every source address is valid) so the class byte adds no round trip; only the stores are skipped
+  const bool clean = (cv & 0x03030303u) == 0u;
   const bool gwall = iy == 0 && P.ground != 0u;
   const float2 belt = (gwall && P.ground == 2u)
                           ? make_float2((c0 & CLS_BELT_STILL) ? 0.0f : 1.0f, (c1 & CLS_BELT_STILL) ? 0.0f : 1.0f)
@@ -1059,7 +1061,7 @@ __global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kpara
   }
   auto emit = [&](auto I, float2 v) {
     constexpr int i = decltype(I)::value;
-    IO::st(fout, i * N + idx0, v, (float)Wc<L, i>::v);
+    if (clean) IO::st(fout, i * N + idx0, v, (float)Wc<L, i>::v);
   };
   if (gwall) collide_shifted2<L, true>(P, h, x0, emit, P.tau_wall);
   else if (P.collision == 1u) collide_shifted2<L, true>(P, h, x0, emit);
@@ -1080,22 +1082,9 @@ __global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kpara
 // dependent flag or distance loads. The FP16 shift is folded into gamma: every population a link
 // of direction i reads has the weight w_i (direction i, its opposite, or a mirror image of i).
 //
-// Records are stored per block of BT<L>::CELLS cells as [block][link][cell]; thread t of a block
-// handles (link, cell) = (t / CELLS, t % CELLS), so record loads are contiguous.
-template <class L> struct BT {
-  static constexpr int CELLS = 256 / L::Q;  // 13 for D3Q19, 28 for D2Q9
-};
+// Records are stored link-major, record (link i, cell k) at i * cap + k (cap = capacity in
+// cells), so the record loads of a warp of consecutive cells are contiguous.
 enum : uint32_t { BC_WALL = 1u, BC_GWALL = 2u };
-
-template <class L>
-__device__ __forceinline__ float lattice_w(int i) {
-  float w = 0.f;
-  static_for<L::Q>([&](auto I) {
-    constexpr int j = I;
-    if (i == j) w = (float)Wc<L, j>::v;
-  });
-  return w;
-}
 
 // one thread per listed fluid cell; writes its cell word {cell, BC_* bits} and its Q link records
 template <class L, class S>
@@ -1105,11 +1094,10 @@ __global__ void __launch_bounds__(128) k_boundary_build(const __grid_constant__ 
                                                         const uint8_t* __restrict__ cls,
                                                         const __grid_constant__ Wheels W,
                                                         const uint32_t* __restrict__ list, uint32_t count,
-                                                        uint2* __restrict__ bcell, uint4* __restrict__ rec,
-                                                        float* __restrict__ gam) {
+                                                        uint32_t cap, uint2* __restrict__ bcell,
+                                                        uint4* __restrict__ rec, float* __restrict__ gam) {
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
-  constexpr int CB = BT<L>::CELLS;
   constexpr bool SHIFT = S::PREC == WT_PREC_F16;
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= count) return;
@@ -1126,7 +1114,7 @@ __global__ void __launch_bounds__(128) k_boundary_build(const __grid_constant__ 
   const float belt = (P.ground == 2u && !(cl & CLS_BELT_STILL)) ? 1.0f : 0.0f;
   const uint32_t sdf_raw = sdf[c];
   const float sdf_self = (P.interp != 0u && sdf_raw != 0u) ? __uint_as_float(~sdf_raw) : -1.0f;
-  const size_t rb = (size_t)(k / CB) * Q * CB + (k % CB);  // record of link i: rb + i * CB
+  const size_t rb = k;  // record of link i: rb + i * cap
   float ga[Q];
   uint32_t bits = 0, wm = 0;
   float mvSum = 0.f, mvW = 0.f;
@@ -1211,7 +1199,7 @@ __global__ void __launch_bounds__(128) k_boundary_build(const __grid_constant__ 
     }
     if (B == 0xffffffffu) B = A;
     ga[i] = gamma;
-    rec[rb + (size_t)i * CB] = make_uint4(A, B, __float_as_uint(alpha), __float_as_uint(SHIFT ? alpha + beta : beta));
+    rec[rb + (size_t)i * cap] = make_uint4(A, B, __float_as_uint(alpha), __float_as_uint(SHIFT ? alpha + beta : beta));
   });
   // wheel links: remove the net mass of the moving-wall terms (wgslLbm.ts:289-291)
   const float corr = mvW > 0.f ? mvSum / mvW : 0.f;
@@ -1221,60 +1209,53 @@ __global__ void __launch_bounds__(128) k_boundary_build(const __grid_constant__ 
     if (wm & (1u << i)) g -= (float)Wc<L, i>::v * corr;
     if constexpr (SHIFT) {
       // stored h = f - w_i for both sources: alpha (h1 + w) + beta (h2 + w) + g
-      const uint4 r = rec[rb + (size_t)i * CB];
+      const uint4 r = rec[rb + (size_t)i * cap];
       const float alpha = __uint_as_float(r.z), ab = __uint_as_float(r.w);
       const float beta = ab - alpha;
-      rec[rb + (size_t)i * CB] = make_uint4(r.x, r.y, r.z, __float_as_uint(beta));
+      rec[rb + (size_t)i * cap] = make_uint4(r.x, r.y, r.z, __float_as_uint(beta));
       g += ab * (float)Wc<L, i>::v;
     }
-    gam[rb + (size_t)i * CB] = g;
+    gam[rb + (size_t)i * cap] = g;
   });
   bcell[k] = make_uint2(c, bits);
 }
 
-// Applies the link records: phase 1 gathers every link value of the block's cells (one thread per
-// link), phase 2 collides one cell per thread on the values staged in shared memory, phase 3 stores
-// the post-collision populations (one thread per population).
+// Applies the link records, one thread per listed cell: every record load of the cell in flight
+// at once (coalesced across the warp), then every gather, then the collision and the stores.
 template <class L, class S>
-__global__ void __launch_bounds__(256) k_boundary_tab(const __grid_constant__ wt_kparams P,
-                                                      const typename S::T* __restrict__ fin,
-                                                      typename S::T* __restrict__ fout,
-                                                      const uint2* __restrict__ bcell, const uint4* __restrict__ rec,
-                                                      const float* __restrict__ gam, uint32_t count) {
+__global__ void __launch_bounds__(64) k_boundary_tab(const __grid_constant__ wt_kparams P,
+                                                     const typename S::T* __restrict__ fin,
+                                                     typename S::T* __restrict__ fout,
+                                                     const uint2* __restrict__ bcell, const uint4* __restrict__ rec,
+                                                     const float* __restrict__ gam, uint32_t count, uint32_t cap) {
   constexpr int Q = L::Q;
-  constexpr int CB = BT<L>::CELLS;
-  __shared__ float sh[Q * CB];
-  __shared__ uint2 shc[CB];
-  const int t = threadIdx.x;
-  const uint32_t k0 = blockIdx.x * CB;
-  const int nc = (int)min((uint32_t)CB, count - k0);
-  const int li = t / CB, lc = t - li * CB;
-  const bool act = li < Q && lc < nc;
-  if (t < nc) shc[t] = bcell[k0 + t];
-  if (act) {
-    const size_t r = ((size_t)blockIdx.x * Q + li) * CB + lc;
-    const uint4 R4 = rec[r];
-    const float g = gam[r];
-    const float x1 = S::cvt(__ldg(fin + R4.x), 0.0f), x2 = S::cvt(__ldg(fin + R4.y), 0.0f);
-    sh[li * CB + lc] = fmaf(__uint_as_float(R4.z), x1, fmaf(__uint_as_float(R4.w), x2, g));
-  }
-  __syncthreads();
-  if (t < nc) {
-    float f[Q], fo[Q];
-    static_for<Q>([&](auto I) {
-      constexpr int i = I;
-      f[i] = sh[i * CB + t];
-    });
-    const uint2 hc = shc[t];
-    const int ix = (int)(hc.x % P.nx);
-    collide_full<L, float>(P, f, ix, (hc.y & BC_WALL) != 0u, (hc.y & BC_GWALL) != 0u, fo);
-    static_for<Q>([&](auto I) {
-      constexpr int i = I;
-      sh[i * CB + t] = fo[i];
-    });
-  }
-  __syncthreads();
-  if (act) S::st(fout, (size_t)li * P.n + shc[lc].x, sh[li * CB + lc], lattice_w<L>(li));
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const uint2 hc = bcell[k];
+  uint4 r[Q];
+  float g[Q];
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    r[i] = __ldg(rec + (size_t)i * cap + k);
+    g[i] = __ldg(gam + (size_t)i * cap + k);
+  });
+  typename S::T x1[Q], x2[Q];
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    x1[i] = __ldg(fin + r[i].x);
+    x2[i] = __ldg(fin + r[i].y);
+  });
+  float f[Q], fo[Q];
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    f[i] = fmaf(__uint_as_float(r[i].z), S::cvt(x1[i], 0.0f), fmaf(__uint_as_float(r[i].w), S::cvt(x2[i], 0.0f), g[i]));
+  });
+  const int ix = (int)(hc.x % P.nx);
+  collide_full<L, float>(P, f, ix, (hc.y & BC_WALL) != 0u, (hc.y & BC_GWALL) != 0u, fo);
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    S::st(fout, (size_t)i * P.n + hc.x, fo[i], (float)Wc<L, i>::v);
+  });
 }
 
 // Rest state written into the solid cells of one population buffer.
@@ -1647,10 +1628,9 @@ static cudaError_t boundary_table_t(wt_solver* s) {
     return cudaSuccess;
   } else {
     if (s->nbnd == 0 || !offsets32(s)) return cudaSuccess;
-    constexpr int CB = BT<L>::CELLS;
-    const size_t nblk = (s->nbnd + CB - 1) / CB;
+    const size_t cap = ((size_t)s->nbnd + 63) / 64 * 64;
     cudaError_t e;
-    if (nblk * CB > s->btab_cap) {
+    if (cap > s->btab_cap) {
       cudaFree(s->bcell);
       cudaFree(s->brec);
       cudaFree(s->bgam);
@@ -1658,13 +1638,14 @@ static cudaError_t boundary_table_t(wt_solver* s) {
       s->brec = nullptr;
       s->bgam = nullptr;
       s->btab_cap = 0;
-      if ((e = cudaMalloc((void**)&s->bcell, nblk * CB * sizeof(uint2))) != cudaSuccess) return e;
-      if ((e = cudaMalloc((void**)&s->brec, nblk * CB * L::Q * sizeof(uint4))) != cudaSuccess) return e;
-      if ((e = cudaMalloc((void**)&s->bgam, nblk * CB * L::Q * sizeof(float))) != cudaSuccess) return e;
-      s->btab_cap = nblk * CB;
+      if ((e = cudaMalloc((void**)&s->bcell, cap * sizeof(uint2))) != cudaSuccess) return e;
+      if ((e = cudaMalloc((void**)&s->brec, cap * L::Q * sizeof(uint4))) != cudaSuccess) return e;
+      if ((e = cudaMalloc((void**)&s->bgam, cap * L::Q * sizeof(float))) != cudaSuccess) return e;
+      s->btab_cap = cap;
     }
     k_boundary_build<L, S><<<(s->nbnd + 127) / 128, 128, 0, s->stream>>>(
-        s->kp, s->flags, s->sdf, s->cls, s->wheels, s->bnd, s->nbnd, s->bcell, s->brec, s->bgam);
+        s->kp, s->flags, s->sdf, s->cls, s->wheels, s->bnd, s->nbnd, (uint32_t)s->btab_cap, s->bcell, s->brec,
+        s->bgam);
     s->launches++;
     return cudaGetLastError();
   }
@@ -1752,9 +1733,9 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
       }
       if (s->nbnd > 0) {
-        constexpr int CB = BT<L>::CELLS;
-        k_boundary_tab<L, S><<<(s->nbnd + CB - 1) / CB, 256, 0, bs>>>(
-            s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd);
+        k_boundary_tab<L, S><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
+            s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
+            (uint32_t)s->btab_cap);
         s->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
       }
