@@ -52,7 +52,7 @@ CASES = [(p, k) for p in ("f32", "f16") for k in LAUNCHES] + [("f64", "reg1")]
 
 @pytest.mark.parametrize("prec,launch", CASES)
 @pytest.mark.parametrize("pset", list(PARAM_SETS))
-@pytest.mark.parametrize("dims", [(32, 14, 12), (48, 16, 1), (160, 12, 1)])
+@pytest.mark.parametrize("dims", [(32, 14, 12), (34, 14, 10), (48, 16, 1), (160, 12, 1)])
 def test_stream_collide_matches_oracle(gpu, oracle, dims, pset, prec, launch):
     _check_against_oracle(oracle, dims, dict(PARAM_SETS[pset], precision=prec), LAUNCHES[launch])
 
