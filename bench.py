@@ -198,6 +198,43 @@ def components(s, peak, no_cpu):
     out["derive"] = {"ms": round(ms, 4), "bytes_alg": alg, "achieved_gbs": round(alg / ms / 1e6, 1),
                      "frac": round(alg / ms / 1e6 / peak, 4)}
 
+    # streamlines (the reference app's 3-D setting: 700 points per line, step 0.7, a 3 x 24 rake)
+    from windtunnel_vis_b200 import abi as A
+
+    sp = A.StreamlineParams(seeds=3 * 24, points=700, use_mean=0, per_line=24)
+    sp.rake_a[:] = [4.0, 40.0, 40.0, 0.0]
+    sp.rake_b[:] = [4.0, 88.0, 88.0, 0.0]
+    sp.rake_d[:] = [0.0, 0.0, 6.0, 0.0]
+    sp.h = 0.7
+    ms, wall = timed(lambda: s.streamlines(sp), 5)
+    out["streamlines"] = {"ms": round(ms, 4), "e2e_ms": round(wall, 4), "lines": sp.seeds, "points": sp.points}
+    probes = [(64.0 + 20 * k, 64.0, 64.0) for k in range(8)]
+    ms, wall = timed(lambda: s.probes(probes), 10)
+    out["probes"] = {"ms": round(ms, 4), "e2e_ms": round(wall, 4), "count": len(probes)}
+    if not no_cpu:
+        vel16 = s.read_velocity().astype(np.float16)
+        _, _, mean = s.read_derived()
+        flags_all = np.asarray(geometry()[0], np.uint32)
+        t0 = time.perf_counter()
+        O.streamlines(DIMS, sp, s.kparams().uin, vel16, mean.astype(np.float16), flags_all)
+        out["streamlines"]["cpu_ref_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+        ma, mb = s.read_means()
+        t0 = time.perf_counter()
+        O.derive(DIMS, s.kparams().u_ref, vel16, flags_all, ma, mb)
+        out["derive"]["cpu_ref_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+        out["derive"]["cpu_threads"] = O.threads(0)
+        # the macro pass restated on the host (one sample of the same tunnel)
+        t0 = time.perf_counter()
+        oo = O.OracleSolver(DIMS, PARAMS)
+        oo.upload_flags(flags_all)
+        oo.upload_sdf(geometry()[2])
+        oo.pending_init = False
+        oo.a[:] = s.read_populations()
+        t1 = time.perf_counter()
+        oo.sample()
+        out["sample"]["cpu_ref_ms"] = round((time.perf_counter() - t1) * 1e3, 2)
+        out["sample"]["cpu_threads"] = O.threads(0)
+
     # tracers
     count, trail, steps = 150000, 20, float(CHUNK)
     tp = abi.TracerParams(count=count, trail=trail, head=0, emitter=0, steps=steps, seed=7,
