@@ -881,18 +881,23 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
   typename IO::pair_t rp[G][Q];
   typename IO::one_t r1[Q];
   const bool last = x0 + V >= NX;
+  // one 64-bit base per thread; each direction adds an offset that is the same for every thread
+  // (plane i, shifted back by c_i along y and z)
+  const typename S::T* fb = fin + idx0;
+  typename S::T* ob = fout + idx0;
   static_for<Q>([&](auto I) {
     constexpr int i = I;
     constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
-    const uint32_t src = i * N + idx0 - (uint32_t)(cy * (int)sy) - (uint32_t)(cz * (int)sz);
+    const ptrdiff_t off = (ptrdiff_t)i * N - (ptrdiff_t)cy * sy - (ptrdiff_t)cz * sz;
+    const typename S::T* ps = fb + off;
     if constexpr (G == 2) {
-      IO::ld4(fin, src, rp[0][i], rp[1][i]);  // src is a multiple of 4 when nx % 4 == 0
+      IO::ld4(ps, 0u, rp[0][i], rp[1][i]);  // 8- or 16-byte aligned when nx % 4 == 0
     } else {
 #pragma unroll
-      for (int g = 0; g < G; g++) rp[g][i] = IO::ld(fin, src + 2 * g);
+      for (int g = 0; g < G; g++) rp[g][i] = IO::ld(ps, 2 * g);
     }
-    if constexpr (cx > 0) r1[i] = IO::ld1(fin, x0 > 0 ? src - 1u : src);          // x - 1
-    if constexpr (cx < 0) r1[i] = IO::ld1(fin, last ? src + (V - 1) : src + V);   // x + 1, outlet clamp
+    if constexpr (cx > 0) r1[i] = IO::ld1(x0 > 0 ? ps - 1 : ps, 0u);            // x - 1
+    if constexpr (cx < 0) r1[i] = IO::ld1(ps + (last ? V - 1 : V), 0u);         // x + 1, outlet clamp
   });
   // phase 2, one pair of cells at a time (the other pairs stay packed in their raw registers):
   // convert and shift into the pulled populations, collide, store
@@ -926,7 +931,7 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
     }
     collide_shifted2<L, BGK>(P, h, x0 + 2 * g, [&](auto I, float2 v) {
       constexpr int i = decltype(I)::value;
-      if (clean) IO::st(fout, i * N + idx0 + 2 * g, v, (float)Wc<L, i>::v);
+      if (clean) IO::st(ob + (ptrdiff_t)i * N, 2 * g, v, (float)Wc<L, i>::v);
     });
   }
 }
