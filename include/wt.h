@@ -259,8 +259,10 @@ int wt_probes(wt_solver* s, const float* pos4, int32_t count, float* out8);
 /* ---- launch selection (extension; no counterpart in the reference) ------------------------ */
 /* Selects the stream-collide launch: `param` cells per thread along x (1, 2 or 4; 2 and 4 need
  * f16/f32 storage and nx % param == 0, otherwise the scalar kernel runs), block bx x by threads
- * (bx * by <= 256; 0, 0 = default), and `kernel` = occupancy hint of the vectorised kernel: 0 =
- * none, 2..4 = registers capped so that many 256-thread CTAs fit on an SM. */
+ * (bx * by <= 256; 0, 0 = one row of up to 128 threads), and `kernel` = occupancy hint of the
+ * vectorised kernel: 0 = none, 2..4 = registers capped so that many 256-thread CTAs fit on an SM.
+ * Until this call or wt_autotune, a handle runs 2 cells per thread, default blocks, and hint 4 for
+ * the regularized collision (none for BGK). */
 int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32_t by);
 int wt_get_launch(const wt_solver* s, int32_t* out4);
 /* The project's launch tuner: times every applicable launch candidate on this handle's
@@ -268,6 +270,24 @@ int wt_get_launch(const wt_solver* s, int32_t* out4);
  * the state does not change) and keeps the fastest. out4 (may be NULL) receives
  * {kernel, param, bx, by}. */
 int wt_autotune(wt_solver* s, int32_t iters, int32_t* out4);
+
+/* ---- batches of tunnels ------------------------------------------------------------------- */
+/* No counterpart in the reference, whose studies panel runs one tunnel at a time
+ * (src/ui/studies.ts:223-252). A batch steps many independent tunnels (any sizes, one device)
+ * together: pairs of steps replay one CUDA graph in which every member's step kernels hang off a
+ * common fork, so small tunnels run concurrently and one launch advances all of them. Members stay
+ * ordinary handles (parameters, geometry and readback work as before; a change of a member's
+ * launch, parameters, wheels or geometry makes the batch recapture on its next step). Members must
+ * not be used from another thread while a batch call runs, and must outlive the batch. */
+typedef struct wt_batch wt_batch;
+int wt_batch_create(wt_solver* const* members, int32_t count, wt_batch** out);
+void wt_batch_destroy(wt_batch* b); /* the members stay alive */
+const char* wt_batch_last_error(const wt_batch* b);
+int32_t wt_batch_size(const wt_batch* b);
+/* `steps` lattice updates of every member */
+int wt_batch_step(wt_batch* b, int32_t steps);
+/* the sampling pass of every member (queued together, then read back): out has count entries */
+int wt_batch_sample(wt_batch* b, wt_stats* out);
 
 /* ---- device plumbing -------------------------------------------------------------------- */
 /* The handle's cudaStream_t (for event timing by the caller) and its device ordinal. */

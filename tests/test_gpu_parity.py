@@ -46,7 +46,8 @@ def _as_float(a):
 
 
 # (kernel, param, bx, by): 1 / 2 / 4 cells per thread, explicit and default block shapes
-LAUNCHES = {"reg1": (0, 1, 0, 0), "reg2": (0, 2, 32, 4), "reg4": (0, 4, 32, 4), "reg2d": (0, 2, 0, 0)}
+LAUNCHES = {"reg1": (0, 1, 0, 0), "reg2": (0, 2, 32, 4), "reg4": (0, 4, 32, 4), "reg2d": (0, 2, 0, 0),
+            "hint4": (4, 2, 0, 0)}
 CASES = [(p, k) for p in ("f32", "f16") for k in LAUNCHES] + [("f64", "reg1")]
 
 
@@ -368,3 +369,46 @@ def test_tracers_bit_exact(gpu, oracle, dims, emitter):
         gs, gh = s.read_tracers(count, trail)
         np.testing.assert_array_equal(gs, st, err_msg=f"frame {frame}")
         np.testing.assert_array_equal(gh, hi, err_msg=f"frame {frame}")
+
+
+# ---- batches of tunnels -----------------------------------------------------------------------
+def test_batch_matches_members_stepped_alone(gpu):
+    from windtunnel_vis_b200.solver import Batch
+
+    cases = [((32, 14, 12), dict(PARAM_SETS["belt_periodic_les"], precision="f16")),
+             ((48, 20, 16), dict(PARAM_SETS["freeslip_reg"], precision="f32")),
+             ((64, 16, 1), dict(PARAM_SETS["noslip_bgk_halfway"], precision="f16")),
+             ((36, 12, 10), dict(PARAM_SETS["freeslip_reg"], precision="f64"))]
+
+    def make(dims, params):
+        flags, sdf, wheels = scene(dims)
+        s = Solver(dims, params)
+        s.upload_flags(flags)
+        s.upload_sdf(sdf)
+        s.set_wheels(wheels)
+        return s
+
+    batch_members = [make(d, p) for d, p in cases]
+    alone = [make(d, p) for d, p in cases]
+    b = Batch(batch_members)
+    for steps in (7, 10, 1, 6):
+        b.step(steps)
+        for s in alone:
+            s.step(steps)
+    for s, t in zip(batch_members, alone):
+        np.testing.assert_array_equal(s.read_populations(), t.read_populations())
+        assert s.step_count == t.step_count == 24
+    got = b.sample()
+    for st, t in zip(got, alone):
+        assert st["raw"].tolist() == t.sample()["raw"].tolist()
+    # a member's parameters change mid-run: the batch recaptures and stays with its twin
+    batch_members[1].set_params(dict(u=0.07))
+    alone[1].set_params(dict(u=0.07))
+    b.step(8)
+    for s in alone:
+        s.step(8)
+    for s, t in zip(batch_members, alone):
+        np.testing.assert_array_equal(s.read_populations(), t.read_populations())
+    b.destroy()
+    for s in batch_members + alone:
+        s.destroy()

@@ -165,6 +165,12 @@ def _sig(lib):
         "wt_export_fields": ([S, i32, v, v, v, i64], C.c_int),
         "wt_streamlines": ([S, P(StreamlineParams), v, i64], C.c_int),
         "wt_probes": ([S, v, i32, v], C.c_int),
+        "wt_batch_create": ([P(S), i32, P(S)], C.c_int),
+        "wt_batch_destroy": ([S], None),
+        "wt_batch_last_error": ([S], C.c_char_p),
+        "wt_batch_size": ([S], i32),
+        "wt_batch_step": ([S, i32], C.c_int),
+        "wt_batch_sample": ([S, P(Stats)], C.c_int),
         "wt_set_launch": ([S, i32, i32, i32, i32], C.c_int),
         "wt_get_launch": ([S, P(i32)], C.c_int),
         "wt_autotune": ([S, i32, P(i32)], C.c_int),

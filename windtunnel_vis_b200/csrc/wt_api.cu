@@ -100,6 +100,7 @@ void invalidate_graphs(wt_solver* s) {
     if (g) cudaGraphExecDestroy(g);
     g = nullptr;
   }
+  s->graph_gen++;
 }
 
 // ---- small device helpers used only by the API -----------------------------------------------
@@ -285,6 +286,7 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
   s->n = (size_t)d->nx * d->ny * d->nz;
   s->pop_elem = elem_bytes(s->prec);
   wt_pack_params(d, p, &s->kp);
+  if (!s->launch_explicit) s->sc_kernel = p->collision == WT_COLL_BGK ? 0 : 4;
   std::string where;
   auto alloc = [&](void** ptr, size_t bytes, const char* name) -> bool {
     cudaError_t e = cudaMalloc(ptr, bytes);
@@ -357,6 +359,7 @@ int wt_set_params(wt_solver* s, const wt_params* p) {
   if (p->precision != s->prec) return fail(s, WT_E_INVALID, "wt_set_params: precision is fixed at creation");
   s->params = *p;
   wt_pack_params(&s->dims, p, &s->kp);
+  if (!s->launch_explicit) s->sc_kernel = p->collision == WT_COLL_BGK ? 0 : 4;
   invalidate_graphs(s);
   s->tab_dirty = true;
   return WT_OK;
@@ -785,6 +788,7 @@ int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32
   s->sc_param = param;
   s->sc_bx = bx;
   s->sc_by = by;
+  s->launch_explicit = true;
   invalidate_graphs(s);
   return WT_OK;
 }
@@ -850,6 +854,7 @@ int wt_autotune(wt_solver* s, int32_t iters, int32_t* out4) {
   s->sc_param = pick.param;
   s->sc_bx = pick.bx;
   s->sc_by = pick.by;
+  s->launch_explicit = true;
   invalidate_graphs(s);
   if (out4) {
     out4[0] = pick.kernel;
@@ -872,5 +877,219 @@ int wt_get_launch(const wt_solver* s, int32_t* out4) {
 void* wt_stream(const wt_solver* s) { return s ? (void*)s->stream : nullptr; }
 int32_t wt_device(const wt_solver* s) { return s ? s->device : -1; }
 int64_t wt_launch_count(const wt_solver* s) { return s ? s->launches : -1; }
+
+}  // extern "C"
+
+/* ---- batches of tunnels -------------------------------------------------------------------- */
+struct wt_batch {
+  int device = 0;
+  std::vector<wt_solver*> m;
+  cudaStream_t stream = nullptr;  // capture origin and replay stream
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_done;
+  cudaGraphExec_t graph = nullptr;
+  std::vector<uint64_t> gens;       // member graph generations the graph was captured at
+  std::vector<int> parities;        // member parities the graph was captured at
+  std::vector<int64_t> per_replay;  // kernel launches of each member inside one replay
+  std::string err;
+};
+
+namespace {
+
+int bfail(wt_batch* b, int code, const std::string& msg) {
+  if (b) b->err = msg;
+  else g_create_err = msg;
+  return code;
+}
+
+void batch_drop_graph(wt_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+}
+
+bool batch_graph_current(const wt_batch* b) {
+  if (!b->graph) return false;
+  for (size_t k = 0; k < b->m.size(); k++)
+    if (b->gens[k] != b->m[k]->graph_gen || b->parities[k] != b->m[k]->parity) return false;
+  return true;
+}
+
+// One graph for two steps of every member: each member's step kernels hang off a fork from the
+// batch stream, so independent tunnels run concurrently, and all join back at the end.
+int batch_capture(wt_batch* b) {
+  batch_drop_graph(b);
+  const size_t n = b->m.size();
+  std::vector<int64_t> l0(n);
+  for (size_t k = 0; k < n; k++) l0[k] = b->m[k]->launches;
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch capture: ") + cudaGetErrorString(e));
+  e = cudaEventRecord(b->ev_fork, b->stream);
+  for (size_t k = 0; k < n && e == cudaSuccess; k++) {
+    wt_solver* s = b->m[k];
+    const int p = s->parity;
+    e = cudaStreamWaitEvent(s->stream, b->ev_fork, 0);
+    if (e == cudaSuccess) e = wt::launch_stream_collide(s, s->f[p], s->f[p ^ 1]);
+    if (e == cudaSuccess) e = wt::launch_stream_collide(s, s->f[p ^ 1], s->f[p]);
+    if (e == cudaSuccess) e = cudaEventRecord(b->ev_done[k], s->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->ev_done[k], 0);
+  }
+  const cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, graph, cudaGraphInstantiateFlagUseNodePriority);
+  if (graph) cudaGraphDestroy(graph);
+  for (size_t k = 0; k < n; k++) {
+    b->per_replay[k] = b->m[k]->launches - l0[k];
+    b->m[k]->launches = l0[k];
+    b->gens[k] = b->m[k]->graph_gen;
+    b->parities[k] = b->m[k]->parity;
+  }
+  if (e != cudaSuccess) {
+    b->graph = nullptr;
+    cudaGetLastError();
+    return bfail(b, WT_E_CUDA, std::string("batch capture: ") + cudaGetErrorString(e));
+  }
+  return WT_OK;
+}
+
+int batch_single_step(wt_batch* b) {
+  for (wt_solver* s : b->m) {
+    cudaError_t e = wt::launch_stream_collide(s, s->f[s->parity], s->f[s->parity ^ 1]);
+    if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch step: ") + cudaGetErrorString(e));
+    s->parity ^= 1;
+  }
+  return WT_OK;
+}
+
+// orders the batch stream behind all work queued so far on every member's stream
+int batch_wait_members(wt_batch* b) {
+  for (wt_solver* s : b->m) {
+    cudaError_t e = cudaEventRecord(s->ev_join, s->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, s->ev_join, 0);
+    if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch step: ") + cudaGetErrorString(e));
+  }
+  return WT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wt_batch_create(wt_solver* const* members, int32_t count, wt_batch** out) {
+  if (!out) return bfail(nullptr, WT_E_INVALID, "wt_batch_create: out is NULL");
+  *out = nullptr;
+  if (!members || count < 1) return bfail(nullptr, WT_E_INVALID, "wt_batch_create: need at least one solver");
+  for (int32_t k = 0; k < count; k++) {
+    if (!members[k]) return bfail(nullptr, WT_E_INVALID, "wt_batch_create: NULL solver");
+    if (members[k]->device != members[0]->device)
+      return bfail(nullptr, WT_E_INVALID, "wt_batch_create: solvers on different devices");
+    for (int32_t j = 0; j < k; j++)
+      if (members[j] == members[k]) return bfail(nullptr, WT_E_INVALID, "wt_batch_create: a solver appears twice");
+  }
+  wt_batch* b = new (std::nothrow) wt_batch();
+  if (!b) return bfail(nullptr, WT_E_OOM, "wt_batch_create: host allocation failed");
+  b->device = members[0]->device;
+  b->m.assign(members, members + count);
+  b->gens.assign(count, 0);
+  b->parities.assign(count, 0);
+  b->per_replay.assign(count, 0);
+  b->ev_done.assign(count, nullptr);
+  DeviceGuard g(b->device);
+  bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int32_t k = 0; ok && k < count; k++)
+    ok = cudaEventCreateWithFlags(&b->ev_done[k], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    wt_batch_destroy(b);
+    return bfail(nullptr, WT_E_CUDA, "wt_batch_create: stream / event creation failed");
+  }
+  *out = b;
+  return WT_OK;
+}
+
+void wt_batch_destroy(wt_batch* b) {
+  if (!b) return;
+  DeviceGuard g(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop_graph(b);
+  for (cudaEvent_t e : b->ev_done)
+    if (e) cudaEventDestroy(e);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+const char* wt_batch_last_error(const wt_batch* b) { return b ? b->err.c_str() : g_create_err.c_str(); }
+
+int32_t wt_batch_size(const wt_batch* b) { return b ? (int32_t)b->m.size() : -1; }
+
+int wt_batch_step(wt_batch* b, int32_t steps) {
+  if (!b || steps < 0) return WT_E_INVALID;
+  DeviceGuard g(b->device);
+  for (wt_solver* s : b->m) {
+    int rc = ensure_classified(s);
+    if (!rc) rc = ensure_init(s);
+    if (rc) return bfail(b, rc, std::string("member: ") + s->err);
+  }
+  auto all_solid_ok = [&]() {
+    for (wt_solver* s : b->m)
+      if (!(s->solid_ok[0] && s->solid_ok[1])) return false;
+    return true;
+  };
+  int32_t k = 0;
+  // single steps (all members together) until the solid cells of every buffer hold the rest
+  // state: the steps that write it stay out of the graph
+  for (; k < steps && !all_solid_ok(); k++) {
+    int rc = batch_single_step(b);
+    if (rc) return rc;
+  }
+  if (steps - k >= 2) {
+    int rc = batch_wait_members(b);
+    if (rc) return rc;
+    if (!batch_graph_current(b)) {
+      rc = batch_capture(b);
+      if (rc) return rc;
+    }
+    for (; k + 2 <= steps; k += 2) {
+      cudaError_t e = cudaGraphLaunch(b->graph, b->stream);
+      if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch graph: ") + cudaGetErrorString(e));
+      for (size_t j = 0; j < b->m.size(); j++) b->m[j]->launches += b->per_replay[j];
+    }
+    // members' later work waits for the replays
+    cudaError_t e = cudaEventRecord(b->ev_fork, b->stream);
+    for (wt_solver* s : b->m)
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(s->stream, b->ev_fork, 0);
+    if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch step: ") + cudaGetErrorString(e));
+  }
+  for (; k < steps; k++) {
+    int rc = batch_single_step(b);
+    if (rc) return rc;
+  }
+  for (wt_solver* s : b->m) s->step_count += steps;
+  return WT_OK;
+}
+
+int wt_batch_sample(wt_batch* b, wt_stats* out) {
+  if (!b || !out) return WT_E_INVALID;
+  DeviceGuard g(b->device);
+  // the sampling passes of all members are queued first, then read back together
+  for (wt_solver* s : b->m) {
+    int rc = ensure_init(s);
+    if (!rc) rc = ensure_classified(s);
+    if (rc) return bfail(b, rc, std::string("member: ") + s->err);
+    cudaError_t e = wt::launch_macro(s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s->result_host, s->result_dev, 64, cudaMemcpyDeviceToHost, s->stream);
+    if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch sample: ") + cudaGetErrorString(e));
+  }
+  for (size_t k = 0; k < b->m.size(); k++) {
+    wt_solver* s = b->m[k];
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch sample: ") + cudaGetErrorString(e));
+    decode(s, s->result_host, &out[k]);
+  }
+  return WT_OK;
+}
 
 }  // extern "C"

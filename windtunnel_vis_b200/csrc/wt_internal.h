@@ -20,6 +20,7 @@ struct wt_solver {
   // of launch shape, parameters, wheels or boundary list
   cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
   int64_t graph_launches = 0;  // kernel launches inside one graph replay
+  uint64_t graph_gen = 0;      // bumped whenever the captured graphs are dropped (batches recapture)
   wt_dims dims{};
   wt_params params{};
   wt_kparams kp{};
@@ -84,6 +85,9 @@ struct wt_solver {
   // thread along x (1 = scalar kernel), block sc_bx x sc_by of the vectorised kernel (0 = default)
   int block_x = 0;
   int sc_kernel = 0, sc_param = 2, sc_bx = 0, sc_by = 0;
+  // false until wt_set_launch or wt_autotune chose a launch: the default then follows the collision
+  // operator (occupancy hint 4 for the regularized collision, which fits 64 registers; none for BGK)
+  bool launch_explicit = false;
   int* err_dev = nullptr;   // device-side error word written by kernels with bounded waits
   int* err_host = nullptr;  // pinned copy
   int64_t launches = 0;

@@ -1706,8 +1706,9 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
       const int runs = s->dims.nx / V;
       int bx = s->sc_bx, by = s->sc_by;
       if (bx <= 0 || by <= 0) {
+        // default block: one row of up to 128 threads (the tuner's usual choice on large tunnels)
         bx = runs >= 128 ? 128 : ((runs + 31) / 32) * 32;
-        by = 256 / bx;
+        by = 1;
       }
       const dim3 block(bx, by);
       const dim3 grid((runs + bx - 1) / bx, (s->dims.ny + by - 1) / by, s->dims.nz);

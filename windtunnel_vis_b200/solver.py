@@ -259,6 +259,49 @@ class Solver:
         self._check(self._lib.wt_write_tracers(self._h, _ptr(s), s.shape[0], _ptr(h), h.shape[0], int(trail)))
 
 
+class Batch:
+    """Many independent tunnels stepped together (wt_batch): pairs of steps replay one CUDA graph
+    holding every member's step kernels, so small tunnels run concurrently. Members stay ordinary
+    Solver objects for parameters, geometry and readback, and must outlive the batch."""
+
+    def __init__(self, solvers):
+        self._lib = abi.load()
+        self.members = list(solvers)
+        arr = (C.c_void_p * len(self.members))(*[s.handle.value for s in self.members])
+        h = C.c_void_p()
+        rc = self._lib.wt_batch_create(arr, len(self.members), C.byref(h))
+        if rc != 0:
+            raise WtError(rc, self._lib.wt_last_error(None).decode())
+        self._h = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise WtError(rc, self._lib.wt_batch_last_error(self._h).decode())
+
+    def step(self, steps: int):
+        self._check(self._lib.wt_batch_step(self._h, int(steps)))
+
+    def sample(self):
+        out = (abi.Stats * len(self.members))()
+        self._check(self._lib.wt_batch_sample(self._h, out))
+        return [_stats_dict(out[k]) for k in range(len(self.members))]
+
+    def step_and_sample(self, steps: int):
+        self.step(steps)
+        return self.sample()
+
+    def destroy(self):
+        if getattr(self, "_h", None):
+            self._lib.wt_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
 def solver_factory(dims, params: dict) -> Solver:
     """SolverFactory (src/backend/types.ts:18)."""
     return Solver(dims, params)

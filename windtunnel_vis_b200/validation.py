@@ -6,6 +6,7 @@ cylinder ....... src/analysis/validation.ts:89-136
 sphere ......... src/analysis/validation.ts:137-184
 sphere_les ..... the D3Q19 LES sphere tunnel of the benchmark (FP16 storage against FP64 populations)
 vehicle ........ the D3Q19 vehicle tunnel of the benchmark (GPU voxelizer, moving belt, wheels)
+batch_sweep .... 32 vehicle tunnels of uneven sizes (yaw x speed sweep) stepped as one batch
 
 A factory is any callable make(dims, params) returning an object with the LbmSolver surface
 (upload_flags, upload_sdf, step_and_sample, destroy) — windtunnel_vis_b200.solver.SolverFactory
@@ -239,6 +240,107 @@ def vehicle(make, precision="f16", steps=30000, dims=(512, 256, 256), u=0.06, re
                         "tau0": 3 * nu + 0.5, "steps": step, "unstable": unstable, "setup_seconds": t_vox}}
 
 
+def sweep_cases(count=32):
+    """The batched sweep: `count` tunnels of uneven sizes from 128 x 64 x 64 to 384 x 192 x 192
+    (nx a multiple of 4), yaw -10 to +10 degrees in 8 steps x inlet u in {0.03, 0.04, 0.05, 0.06}
+    around the vehicle body. Returns [(dims, yaw, u)]."""
+    yaws = [-10.0 + 20.0 * k / 7 for k in range(8)]
+    us = [0.03, 0.04, 0.05, 0.06]
+    out = []
+    for k in range(count):
+        sc = 1.0 + 2.0 * k / max(count - 1, 1)
+        d = (int(round(128 * sc / 4)) * 4, int(round(64 * sc)), int(round(64 * sc)))
+        out.append((d, yaws[k % 8], us[(k // 8) % 4]))
+    return out
+
+
+def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, re_l=2e4, target_tris=200_000):
+    """Runs the sweep of sweep_cases as one batch (windtunnel_vis_b200.solver.Batch): every tunnel
+    voxelizes the vehicle body at its yaw (moving belt, rotating wheels, Smagorinsky LES, FP16),
+    then all advance `steps` lattice updates together. Reports the aggregate MLUPS (device time
+    of the batch steps) and each case's mean C_D / C_L over the second half; with compare_alone,
+    the same cases stepped one tunnel at a time (each with its own CUDA graphs) for the speed-up
+    and the per-case C_D, which must agree exactly (the batch replays the same kernels)."""
+    import torch
+
+    from . import mesh as Mh
+    from .analysis import window_stats
+    from .solver import Batch, Solver
+
+    p, idx, wheels, lo, hi = Mh.vehicle_body(target_tris=target_tris)
+    cases = sweep_cases(count)
+
+    def build():
+        solvers, frontal = [], []
+        for dims, yaw, u in cases:
+            length = dims[0] / 3.0
+            s = Solver(dims, dict(u=u, nu=u * length / re_l, cs=cs, ground="moving", sides="freeslip", spongeNu=0.03,
+                                  spongeStart=0.85, emaAlpha=0, precision="f16", init="rest_noise", initNoise=1e-4,
+                                  initSeed=1))
+            body_h = float(hi[1] - lo[1]) * length
+            M16, _, full = Mh.placement_matrix(p, lo, hi, dims, dict(mode="ground", lengthFrac=1 / 3, diamFrac=0.3,
+                                                                     xFrac=0.34, yawDeg=yaw, rideCells=0.08 * body_h))
+            info = s.voxelize(p, idx, M16, Mh.grid_wheels(wheels, full))
+            frontal.append(max(info["frontal"], 1))
+            solvers.append(s)
+        return solvers, frontal
+
+    def run(step_fn, sample_fn, frontal):
+        series = [[] for _ in cases]
+        ms = 0.0
+        done = 0
+        torch.cuda.synchronize()
+        while done < steps:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            step_fn(chunk)
+            b.record()
+            torch.cuda.synchronize()
+            ms += a.elapsed_time(b)
+            done += chunk
+            for k, st in enumerate(sample_fn()):
+                series[k].append((st["step"], coefficients(st["fx"], st["fy"], st["fz"], cases[k][2], frontal[k])))
+        res = []
+        for k, ser in enumerate(series):
+            sel = [(t, c) for t, c in ser if t > steps // 2]
+            w = window_stats([t for t, _ in sel], [c["cd"] for _, c in sel], float(steps)) if len(sel) >= 16 else None
+            res.append({"dims": list(cases[k][0]), "yaw": cases[k][1], "u": cases[k][2],
+                        "cd": float(np.mean([c["cd"] for _, c in sel])) if sel else math.nan,
+                        "cd_se": w["se"] if w else math.nan,
+                        "cl": float(np.mean([c["cl"] for _, c in sel])) if sel else math.nan})
+        return ms, res
+
+    cells = sum(d[0] * d[1] * d[2] for d, _, _ in cases)
+    solvers, frontal = build()
+    batch = Batch(solvers)
+
+    def step_batch(n):
+        batch.step(n)
+        torch.cuda.synchronize()  # the batch stream is not torch's: wait before the end event
+
+    ms, res = run(step_batch, batch.sample, frontal)
+    out = {"id": "batch_sweep", "tunnels": count, "cells": cells, "steps": steps, "batch_ms": ms,
+           "batch_mlups": cells * steps / (ms * 1e-3) / 1e6, "cases": res}
+    batch.destroy()
+    for s in solvers:
+        s.destroy()
+    if compare_alone:
+        solvers, frontal = build()
+
+        def step_alone(n):
+            for s in solvers:  # one tunnel at a time
+                s.step(n)
+                torch.cuda.synchronize()
+
+        ms2, res2 = run(step_alone, lambda: [s.sample() for s in solvers], frontal)
+        out["alone_ms"] = ms2
+        out["alone_mlups"] = cells * steps / (ms2 * 1e-3) / 1e6
+        out["cd_identical"] = all(a["cd"] == b["cd"] for a, b in zip(res, res2))
+        for s in solvers:
+            s.destroy()
+    return out
+
+
 CASES = {"freestream": freestream, "cylinder": cylinder, "sphere": sphere}
 
 
@@ -253,7 +355,7 @@ def main(argv=None):
     from .solver import solver_factory
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["sphere_les", "vehicle", *CASES])
+    ap.add_argument("case", choices=["sphere_les", "vehicle", "batch_sweep", *CASES])
     ap.add_argument("--precision", default="f16")
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--valscale", type=float, default=1.0)
@@ -262,6 +364,8 @@ def main(argv=None):
         r = sphere_les(solver_factory, a.precision, a.steps)
     elif a.case == "vehicle":
         r = vehicle(solver_factory, a.precision, a.steps)
+    elif a.case == "batch_sweep":
+        r = batch_sweep(a.steps, compare_alone=True)
     else:
         r = CASES[a.case](solver_factory, a.valscale)
     r.pop("series", None)
