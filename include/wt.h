@@ -289,6 +289,90 @@ int wt_batch_step(wt_batch* b, int32_t steps);
 /* the sampling pass of every member (queued together, then read back): out has count entries */
 int wt_batch_sample(wt_batch* b, wt_stats* out);
 
+/* ---- learned LES closure (extension; no counterpart in the reference) -----------------------
+ * A per-cell network replaces the Smagorinsky eddy viscosity of the collision (the reference's
+ * closure: wgslLbm.ts:206-214) on D3Q19 handles with f16 or f32 storage. Its 10 features per
+ * cell, in the handle's lattice units, from the pre-collision populations:
+ *   0-5  non-equilibrium stress Pi_xx, Pi_yy, Pi_zz, Pi_xy, Pi_xz, Pi_yz
+ *        (Pi = sum_i c_i c_i f_i - rho (u u + I / 3))
+ *   6    |S| = 3 |Pi| / (sqrt(2) rho tau_s), tau_s = (tau0 + sqrt(tau0^2 + 18 sqrt(2) Cs^2 |Pi| / rho)) / 2
+ *        with Cs = WT_CLOSURE_FEATURE_CS and |Pi| = sqrt(Pi : Pi): the strain rate the Smagorinsky
+ *        relation assigns to the stress
+ *   7    wall distance in cells from the handle's wall-distance field, WT_CLOSURE_WALL_CAP where
+ *        unknown or larger
+ *   8    rho
+ *   9    |u|
+ * Network 10 -> 32 -> 32 -> 1: x' = bf16((x - shift) * scale); h1 = bf16(gelu(x' W1 + b1));
+ * h2 = bf16(gelu(h1 W2 + b2)); nu_t = nu_scale * softplus(h2 . w3 + b3), with W1, W2, w3 rounded
+ * to bf16, f32 accumulation and gelu(x) = x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))) / 2.
+ * The relaxation time becomes tau = tau0' + 3 nu_t, tau0' being tau0 with the outlet sponge and
+ * the floor-wall minimum exactly as for Smagorinsky. */
+#define WT_CLOSURE_IN 10
+#define WT_CLOSURE_HID 32
+#define WT_CLOSURE_FEATURE_CS 0.1f
+#define WT_CLOSURE_WALL_CAP 3.0f
+typedef struct wt_closure {
+  float shift[WT_CLOSURE_IN]; /* feature normalisation x' = (x - shift) * scale */
+  float scale[WT_CLOSURE_IN];
+  float w1[WT_CLOSURE_IN][WT_CLOSURE_HID]; /* [input][hidden] */
+  float b1[WT_CLOSURE_HID];
+  float w2[WT_CLOSURE_HID][WT_CLOSURE_HID]; /* [hidden in][hidden out] */
+  float b2[WT_CLOSURE_HID];
+  float w3[WT_CLOSURE_HID];
+  float b3;
+  float nu_scale; /* output scale (lattice viscosity units) */
+} wt_closure;
+/* Installs the network (copied) on the handle, or removes it (closure = NULL: plain Smagorinsky).
+ * WT_E_UNSUPPORTED on D2Q9 and f64 handles. */
+int wt_set_closure(wt_solver* s, const wt_closure* closure);
+/* enabled = 1 and *out = the installed network, or enabled = 0 */
+int wt_get_closure(const wt_solver* s, wt_closure* out, int32_t* enabled);
+
+/* Trainer of the closure: a device-resident pool of samples (features + target eddy viscosity),
+ * the network's f32 master weights and Adam state, and the BF16 training kernels (tcgen05 forward
+ * and input-gradient products, f32 accumulation). One trainer per device; calls on one trainer are
+ * serialized by the caller. */
+typedef struct wt_trainer wt_trainer;
+typedef struct wt_train_params {
+  int32_t steps;  /* Adam steps */
+  int32_t batch;  /* samples per step, drawn uniformly with replacement from the pool */
+  float lr, beta1, beta2, eps;
+  uint64_t seed;  /* minibatch draws */
+} wt_train_params;
+int wt_trainer_create(int32_t device, int64_t capacity, wt_trainer** out);
+void wt_trainer_destroy(wt_trainer* t);
+const char* wt_trainer_last_error(const wt_trainer* t);
+int64_t wt_trainer_count(const wt_trainer* t);
+int wt_trainer_clear(wt_trainer* t);
+/* Appends training samples from a fine run and the coarse grid it is filtered to (fine dims = 2 x
+ * coarse dims; both D3Q19, same body voxelized on each). Each coarse fluid cell whose 2 x 2 x 2
+ * fine cells are all fluid, outside both sponges and off the domain faces, is kept with
+ * probability `keep` (a hash of the cell and `seed`). Its features are those of the box-filtered
+ * fine populations (pulled, pre-collision) seen by the coarse handle (its tau0 and wall distances);
+ * its target is the eddy viscosity that best represents the unresolved stress:
+ *   T = <rho u u> / <rho> - u~ u~  +  <-2 nu_sgs S>   (filtered resolved stress plus the fine run's
+ *       own Smagorinsky stress; < > = 2 x 2 x 2 average, u~ = <rho u> / <rho>)
+ *   nu* = max(0, -sum_box dev(T) : S~ / sum_box 2 S~ : S~), S~ from central differences of u~ on the
+ *       coarse grid, sums over the 3 x 3 x 3 coarse neighbourhood (cells that are themselves kept
+ *       candidates). added (may be NULL) receives the number of samples appended. */
+int wt_trainer_add_samples(wt_trainer* t, wt_solver* fine, wt_solver* coarse, double keep, uint64_t seed,
+                           int64_t* added);
+/* host samples: x (n x 10 features), y (n targets) */
+int wt_trainer_put_samples(wt_trainer* t, const float* x, const float* y, int64_t n);
+int wt_trainer_read_samples(wt_trainer* t, int64_t offset, int64_t n, float* x, float* y);
+/* mean and standard deviation of the 10 features and the target over the pool (11 each) */
+int wt_trainer_stats(wt_trainer* t, double* mean11, double* std11);
+int wt_trainer_set_model(wt_trainer* t, const wt_closure* m); /* also resets the Adam state */
+int wt_trainer_get_model(const wt_trainer* t, wt_closure* out);
+/* Adam on L = mean(((nu_t(x) - y) / nu_scale)^2); loss (may be NULL) receives the minibatch loss of
+ * every step. */
+int wt_trainer_fit(wt_trainer* t, const wt_train_params* p, float* loss);
+/* loss and gradient (dL / d parameter, in a wt_closure whose shift, scale and nu_scale are 0) over
+ * pool samples [offset, offset + n), without an update */
+int wt_trainer_grad(wt_trainer* t, int64_t offset, int64_t n, wt_closure* grad, double* loss);
+/* nu_t of the current model for n host feature rows (the tensor-core inference path) */
+int wt_trainer_infer(wt_trainer* t, const float* x, int64_t n, float* nu);
+
 /* ---- device plumbing -------------------------------------------------------------------- */
 /* The handle's cudaStream_t (for event timing by the caller) and its device ordinal. */
 void* wt_stream(const wt_solver* s);

@@ -45,6 +45,14 @@ def lib():
         L.or_export.argtypes = [P(abi.Dims), C.c_int, v, v, v, v, v, v]
         L.or_streamlines.argtypes = [P(abi.Dims), P(abi.StreamlineParams), C.c_float, v, v, v, v]
         L.or_probes.argtypes = [P(abi.Dims), v, C.c_int, v, v, v]
+        L.or_stream_collide_lc.argtypes = [P(abi.Dims), P(abi.KParams), C.c_int, v, v, v, v, v, C.c_int, C.c_int,
+                                           P(abi.Closure)]
+        L.or_closure_features.argtypes = [v, v, C.c_int64, C.c_float, v]
+        L.or_closure_features.restype = None
+        L.or_closure_forward.argtypes = [P(abi.Closure), v, C.c_int64, v]
+        L.or_closure_forward.restype = None
+        L.or_closure_grad.argtypes = [P(abi.Closure), v, v, C.c_int64, v, v]
+        L.or_closure_grad.restype = None
         L.or_pcg.argtypes = [C.c_uint32]
         L.or_pcg.restype = C.c_uint32
         _lib = L
@@ -154,11 +162,23 @@ class OracleSolver:
             lib().or_init(C.byref(dims_of(self.dims)), C.byref(self.kp), self.prec, _p(self.flags), _p(buf), mode, seed, amp)
         self.pending_init = False
 
+    closure = None
+
+    def set_closure(self, closure):
+        """abi.Closure (the learned closure in place of Smagorinsky) or None."""
+        self.closure = closure
+
     def step(self, steps):
         if self.pending_init:
             self._init()
-        lib().or_stream_collide(C.byref(dims_of(self.dims)), C.byref(self.kp), self.prec, _p(self.a), _p(self.b),
-                                _p(self.flags), _p(self.sdf), _p(self.wheels8), self.nwheels, int(steps))
+        if self.closure is not None:
+            rc = lib().or_stream_collide_lc(C.byref(dims_of(self.dims)), C.byref(self.kp), self.prec, _p(self.a),
+                                            _p(self.b), _p(self.flags), _p(self.sdf), _p(self.wheels8), self.nwheels,
+                                            int(steps), C.byref(self.closure))
+            assert rc == 0, rc
+        else:
+            lib().or_stream_collide(C.byref(dims_of(self.dims)), C.byref(self.kp), self.prec, _p(self.a), _p(self.b),
+                                    _p(self.flags), _p(self.sdf), _p(self.wheels8), self.nwheels, int(steps))
         if steps % 2 == 1:
             self.a, self.b = self.b, self.a
         self.step_count += steps
@@ -285,3 +305,31 @@ def probes(dims, pos4, vel_half4, mean_half4):
     mean = np.ascontiguousarray(mean_half4, np.float16).view(np.uint16)
     lib().or_probes(C.byref(dims_of(dims)), _p(pos), pos.shape[0], _p(vel), _p(mean), _p(out))
     return out
+
+
+def closure_features(moments, wall, tau0):
+    """moments (n x 10: pi xx, yy, zz, xy, xz, yz, rho, ux, uy, uz), wall distances (n) -> the 10
+    closure features per row (include/wt.h, wt_closure)."""
+    m = np.ascontiguousarray(moments, np.float32).reshape(-1, 10)
+    w = np.ascontiguousarray(wall, np.float32).ravel()
+    out = np.zeros((m.shape[0], 10), np.float32)
+    lib().or_closure_features(_p(m), _p(w), m.shape[0], float(tau0), _p(out))
+    return out
+
+
+def closure_forward(closure, x):
+    """nu_t of feature rows x (n x 10) under the network `closure` (abi.Closure)."""
+    x = np.ascontiguousarray(x, np.float32).reshape(-1, 10)
+    nu = np.zeros(x.shape[0], np.float32)
+    lib().or_closure_forward(C.byref(closure), _p(x), x.shape[0], _p(nu))
+    return nu
+
+
+def closure_grad(closure, x, y):
+    """(loss, gradient of the 1441 trainable values w1, b1, w2, b2, w3, b3 in field order)."""
+    x = np.ascontiguousarray(x, np.float32).reshape(-1, 10)
+    y = np.ascontiguousarray(y, np.float32).ravel()
+    g = np.zeros(1441, np.float64)
+    loss = C.c_double()
+    lib().or_closure_grad(C.byref(closure), _p(x), _p(y), x.shape[0], _p(g), C.byref(loss))
+    return loss.value, g

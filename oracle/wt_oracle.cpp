@@ -24,6 +24,10 @@
  *   particle tracers .......... src/render/tracers.ts:3-106, render/wgslRender.ts:22-37
  *   derived fields, export .... src/solver/wgslLbm.ts:527-592, SolverGPU.ts:374-425
  *   streamlines, probes ....... src/render/tracers.ts:109-125, 152-200
+ *   learned closure ........... no counterpart in the reference: the network of include/wt.h
+ *                               (wt_closure), its features, loss gradient and the collision with
+ *                               tau = tau0' + 3 nu_t in place of the Smagorinsky closure
+ *                               (wgslLbm.ts:206-214)
  *
  * Arithmetic follows the WGSL expression order, evaluated left to right in IEEE single precision
  * without contraction (build with -ffp-contract=off). Float literals of the generated WGSL
@@ -140,6 +144,7 @@ struct Ctx {
   const uint32_t* sdf;
   uint32_t nwheels;
   float wh[32][4]; /* w[2k] = (centre, 1/R), w[2k+1] = (axis, half-width) */
+  const wt_closure* closure; /* learned closure (f32 / f16 storage), nullptr = Smagorinsky */
   size_t cellId(int x, int y, int z) const { return (size_t)x + (size_t)NX * ((size_t)y + (size_t)NY * (size_t)z); }
 };
 
@@ -198,6 +203,95 @@ template <class R, class Coef> static R signed_sum(const Lat& L, const R* f, Coe
 /* ------------------------------------------------------------------------------------------ */
 /* fused pull-stream + collide for one cell (wgslLbm.ts:134-293)                                */
 /* ------------------------------------------------------------------------------------------ */
+/* ---- learned closure: features and network (the arithmetic of include/wt.h's wt_closure) ---- */
+static float cl_bf16r(float v) {
+  uint32_t u;
+  std::memcpy(&u, &v, 4);
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  u &= 0xFFFF0000u;
+  float r;
+  std::memcpy(&r, &u, 4);
+  return r;
+}
+
+static void cl_features(float pxx, float pyy, float pzz, float pxy, float pxz, float pyz, float rho, float ux,
+                        float uy, float uz, float tau0, float wall_d, float* x) {
+  float pn = std::fma(pxx, pxx, std::fma(pyy, pyy, pzz * pzz));
+  pn = std::fma(2.0f, std::fma(pxy, pxy, std::fma(pxz, pxz, pyz * pyz)), pn);
+  const float piN = std::sqrt(pn);
+  const float k = (float)(18.0 * 1.4142135623730951) * (WT_CLOSURE_FEATURE_CS * WT_CLOSURE_FEATURE_CS);
+  const float ts = 0.5f * (tau0 + std::sqrt(std::fma(tau0, tau0, (k * piN) / rho)));
+  x[0] = pxx;
+  x[1] = pyy;
+  x[2] = pzz;
+  x[3] = pxy;
+  x[4] = pxz;
+  x[5] = pyz;
+  x[6] = (2.1213203435596424f * piN) / (rho * ts);
+  x[7] = wall_d;
+  x[8] = rho;
+  x[9] = std::sqrt(std::fma(ux, ux, std::fma(uy, uy, uz * uz)));
+}
+
+static float cl_wall_dist(uint32_t s) {
+  if (s == 0u) return WT_CLOSURE_WALL_CAP;
+  const uint32_t b = ~s;
+  float d;
+  std::memcpy(&d, &b, 4);
+  return d < WT_CLOSURE_WALL_CAP ? d : WT_CLOSURE_WALL_CAP;
+}
+
+static float cl_gelu(float x) {
+  const float inner = std::fma(0.044715f * (x * x), x, x);
+  const float t = std::tanh(0.7978845608028654f * inner);
+  const float hx = 0.5f * x;
+  return std::fma(hx, t, hx);
+}
+
+static float cl_gelu_d(float x, float& d) {
+  const float x2 = x * x;
+  const float inner = std::fma(0.044715f * x2, x, x);
+  const float t = std::tanh(0.7978845608028654f * inner);
+  const float hx = 0.5f * x;
+  const float du = 0.7978845608028654f * std::fma(0.134145f, x2, 1.0f);
+  d = std::fma(hx * std::fma(-t, t, 1.0f), du, 0.5f * (1.0f + t));
+  return std::fma(hx, t, hx);
+}
+
+static float cl_softplus(float z) { return z > 20.0f ? z : std::log1p(std::exp(z)); }
+
+/* network input k: bf16((x - shift) * scale) */
+static float cl_input(const wt_closure& C, const float* x, int k) { return cl_bf16r((x[k] - C.shift[k]) * C.scale[k]); }
+
+/* forward pass of one sample; the optional outputs keep the intermediate values for the gradient */
+static float cl_forward(const wt_closure& C, const float* xin, float* xn = nullptr, float* z1 = nullptr,
+                        float* h1 = nullptr, float* z2 = nullptr, float* h2 = nullptr, float* z3o = nullptr) {
+  float x[WT_CLOSURE_IN], a1[WT_CLOSURE_HID], b1[WT_CLOSURE_HID], a2[WT_CLOSURE_HID], b2[WT_CLOSURE_HID];
+  for (int k = 0; k < WT_CLOSURE_IN; k++) x[k] = cl_input(C, xin, k);
+  for (int j = 0; j < WT_CLOSURE_HID; j++) {
+    float a = 0.0f;
+    for (int k = 0; k < WT_CLOSURE_IN; k++) a = std::fma(x[k], cl_bf16r(C.w1[k][j]), a);
+    a1[j] = a + C.b1[j];
+    b1[j] = cl_bf16r(cl_gelu(a1[j]));
+  }
+  float z3 = 0.0f;
+  for (int j = 0; j < WT_CLOSURE_HID; j++) {
+    float a = 0.0f;
+    for (int i = 0; i < WT_CLOSURE_HID; i++) a = std::fma(b1[i], cl_bf16r(C.w2[i][j]), a);
+    a2[j] = a + C.b2[j];
+    b2[j] = cl_bf16r(cl_gelu(a2[j]));
+    z3 = std::fma(b2[j], cl_bf16r(C.w3[j]), z3);
+  }
+  z3 = z3 + C.b3;
+  if (xn) std::memcpy(xn, x, sizeof x);
+  if (z1) std::memcpy(z1, a1, sizeof a1);
+  if (h1) std::memcpy(h1, b1, sizeof b1);
+  if (z2) std::memcpy(z2, a2, sizeof a2);
+  if (h2) std::memcpy(h2, b2, sizeof b2);
+  if (z3o) *z3o = z3;
+  return C.nu_scale * cl_softplus(z3);
+}
+
 template <int PREC> static void sc_cell(const Ctx& X, const Pops<PREC>& F, size_t idx) {
   typedef typename RT<PREC>::T R;
   const Lat& L = *X.L;
@@ -333,6 +427,13 @@ template <int PREC> static void sc_cell(const Ctx& X, const Pops<PREC>& F, size_
   R t0 = (R)P.tau0 + (R)3 * (R)P.sponge_nu * sp * sp;
   if (gwall) t0 = t0 > (R)P.tau_wall ? t0 : (R)P.tau_wall;
   R tau = (R)0.5 * (t0 + std::sqrt(t0 * t0 + (R)(18.0 * std::sqrt(2.0)) * (R)P.csmag2 * piN * irho));
+  if (X.closure != nullptr && dim == 3 && PREC != WT_PREC_F64) {
+    /* pi[] is ordered xx, xy, xz, yy, yz, zz */
+    float x[WT_CLOSURE_IN];
+    cl_features((float)pi[0], (float)pi[3], (float)pi[5], (float)pi[1], (float)pi[2], (float)pi[4], (float)rho,
+                (float)u[0], (float)u[1], (float)u[2], P.tau0, cl_wall_dist(X.sdf[idx]), x);
+    tau = t0 + (R)3 * (R)cl_forward(*X.closure, x);
+  }
   R k1 = ((R)1 - (R)1 / tau) * (R)4.5;
   bool useBGK = wall || P.collision == 1u;
   R sIn_den = (R)P.sponge_in > (R)1 ? (R)P.sponge_in : (R)1;
@@ -1015,6 +1116,97 @@ int or_stream_collide(const wt_dims* d, const wt_kparams* kp, int prec, void* a,
     dst = t;
   }
   return WT_OK;
+}
+
+/* or_stream_collide with the learned closure in place of Smagorinsky (f32 / f16 storage, D3Q19) */
+int or_stream_collide_lc(const wt_dims* d, const wt_kparams* kp, int prec, void* a, void* b, const uint32_t* flags,
+                         const uint32_t* sdf, const float* wheels8, int nwheels, int steps, const wt_closure* c) {
+  if (!c || prec == WT_PREC_F64 || !d || d->nz < 2 || !sdf) return WT_E_INVALID;
+  Ctx X;
+  int rc = make_ctx(X, d, kp, flags, sdf, wheels8, nwheels);
+  if (rc) return rc;
+  X.closure = c;
+  const int64_t N = (int64_t)X.N;
+  void* src = a;
+  void* dst = b;
+  for (int s = 0; s < steps; s++) {
+    if (prec == WT_PREC_F32) {
+      Pops<WT_PREC_F32> F{src, dst, X.N, X.L};
+#pragma omp parallel for schedule(static)
+      for (int64_t cc = 0; cc < N; cc++) sc_cell<WT_PREC_F32>(X, F, (size_t)cc);
+    } else {
+      Pops<WT_PREC_F16> F{src, dst, X.N, X.L};
+#pragma omp parallel for schedule(static)
+      for (int64_t cc = 0; cc < N; cc++) sc_cell<WT_PREC_F16>(X, F, (size_t)cc);
+    }
+    void* t = src;
+    src = dst;
+    dst = t;
+  }
+  return WT_OK;
+}
+
+/* the 10 closure features of n cells from their moments: m (n x 10) = pi xx, yy, zz, xy, xz, yz,
+ * rho, ux, uy, uz; wall (n) = wall distance */
+void or_closure_features(const float* m, const float* wall, int64_t n, float tau0, float* out) {
+  for (int64_t r = 0; r < n; r++) {
+    const float* q = m + r * 10;
+    cl_features(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], q[9], tau0, wall[r], out + r * WT_CLOSURE_IN);
+  }
+}
+
+/* nu_t of n feature rows */
+void or_closure_forward(const wt_closure* c, const float* x, int64_t n, float* nu) {
+#pragma omp parallel for schedule(static)
+  for (int64_t r = 0; r < n; r++) nu[r] = cl_forward(*c, x + r * WT_CLOSURE_IN);
+}
+
+/* loss L = mean(((nu - y) / nu_scale)^2) and dL / d(w1, b1, w2, b2, w3, b3) (1441 values, in the
+ * wt_closure field order), with the rounding points of the training kernel: dz2 = bf16(dz3 w3
+ * gelu'(z2)), dz1 = bf16((dz2 W2^T) gelu'(z1)) */
+void or_closure_grad(const wt_closure* c, const float* x, const float* y, int64_t n, double* grad, double* loss) {
+  const int H = WT_CLOSURE_HID, I = WT_CLOSURE_IN;
+  const int NP = I * H + H + H * H + H + H + 1;
+  std::vector<double> g((size_t)NP, 0.0);
+  double ls = 0.0;
+  for (int64_t r = 0; r < n; r++) {
+    float xn[WT_CLOSURE_IN], z1[WT_CLOSURE_HID], h1[WT_CLOSURE_HID], z2[WT_CLOSURE_HID], h2[WT_CLOSURE_HID], z3;
+    const float nu = cl_forward(*c, x + r * I, xn, z1, h1, z2, h2, &z3);
+    const float d = (nu - y[r]) / c->nu_scale;
+    ls += (double)(d * d);
+    const float dz3 = 2.0f * d * (1.0f / (1.0f + std::exp(-z3)));
+    float dz2[WT_CLOSURE_HID], dz1[WT_CLOSURE_HID];
+    for (int j = 0; j < H; j++) {
+      float gd;
+      cl_gelu_d(z2[j], gd);
+      dz2[j] = cl_bf16r(dz3 * cl_bf16r(c->w3[j]) * gd);
+    }
+    for (int i = 0; i < H; i++) {
+      float a = 0.0f;
+      for (int j = 0; j < H; j++) a = std::fma(dz2[j], cl_bf16r(c->w2[i][j]), a);
+      float gd;
+      cl_gelu_d(z1[i], gd);
+      dz1[i] = cl_bf16r(a * gd);
+    }
+    double* gw1 = g.data();
+    double* gb1 = gw1 + I * H;
+    double* gw2 = gb1 + H;
+    double* gb2 = gw2 + H * H;
+    double* gw3 = gb2 + H;
+    double* gb3 = gw3 + H;
+    for (int k = 0; k < I; k++)
+      for (int j = 0; j < H; j++) gw1[k * H + j] += (double)xn[k] * dz1[j];
+    for (int j = 0; j < H; j++) gb1[j] += dz1[j];
+    for (int i = 0; i < H; i++)
+      for (int j = 0; j < H; j++) gw2[i * H + j] += (double)h1[i] * dz2[j];
+    for (int j = 0; j < H; j++) {
+      gb2[j] += dz2[j];
+      gw3[j] += (double)dz3 * h2[j];
+    }
+    gb3[0] += dz3;
+  }
+  for (int p = 0; p < NP; p++) grad[p] = n > 0 ? g[(size_t)p] / (double)n : 0.0;
+  if (loss) *loss = n > 0 ? ls / (double)n : 0.0;
 }
 
 /* macro pass on the current populations: vel4 (f32 view of the half4 velTex), EMA buffers

@@ -41,7 +41,7 @@ def test_library_exports_every_declared_symbol(wtlib):
 STRUCTS = {
     "wt_dims": abi.Dims, "wt_params": abi.Params, "wt_kparams": abi.KParams, "wt_stats": abi.Stats,
     "wt_wheel": abi.Wheel, "wt_voxel_info": abi.VoxelInfo, "wt_tracer_params": abi.TracerParams,
-    "wt_streamline_params": abi.StreamlineParams,
+    "wt_streamline_params": abi.StreamlineParams, "wt_closure": abi.Closure, "wt_train_params": abi.TrainParams,
 }
 
 
@@ -102,3 +102,13 @@ def test_sample_noalloc_argument_checks_without_device(wtlib):
     assert rc == abi.WT_E_INVALID
     rc = wtlib.wt_sample_noalloc(C.byref(abi.Dims(8, 8, 8)), C.byref(P), None, 17, *args[2:])
     assert rc == abi.WT_E_INVALID
+
+
+def test_trainer_without_device_is_reported(wtlib):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is visible")
+    h = C.c_void_p()
+    assert wtlib.wt_trainer_create(0, 16, C.byref(h)) == abi.WT_E_NO_DEVICE
+    assert wtlib.wt_trainer_create(0, -1, C.byref(h)) == abi.WT_E_INVALID

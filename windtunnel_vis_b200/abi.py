@@ -83,6 +83,28 @@ class StreamlineParams(C.Structure):
     ]
 
 
+CLOSURE_IN = 10
+CLOSURE_HID = 32
+
+
+class Closure(C.Structure):
+    """wt_closure: feature normalisation, the 10 -> 32 -> 32 -> 1 network, output scale."""
+    _fields_ = [
+        ("shift", C.c_float * CLOSURE_IN), ("scale", C.c_float * CLOSURE_IN),
+        ("w1", (C.c_float * CLOSURE_HID) * CLOSURE_IN), ("b1", C.c_float * CLOSURE_HID),
+        ("w2", (C.c_float * CLOSURE_HID) * CLOSURE_HID), ("b2", C.c_float * CLOSURE_HID),
+        ("w3", C.c_float * CLOSURE_HID), ("b3", C.c_float), ("nu_scale", C.c_float),
+    ]
+
+
+class TrainParams(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int32), ("batch", C.c_int32),
+        ("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+        ("seed", C.c_uint64),
+    ]
+
+
 def make_params(p: dict) -> Params:
     """SolverParams dict (reference field names, types.ts:3-29) -> wt_params with the reference's
     defaults for the optional fields (tauWall 0.5, interp true, spongeIn 0, f32, regularized)."""
@@ -178,6 +200,22 @@ def _sig(lib):
         "wt_device": ([S], i32),
         "wt_launch_count": ([S], i64),
         "wt_sample_noalloc": ([P(Dims), P(Params), P(Wheel), i32, v, v, v, v, v, v, v, v], C.c_int),
+        "wt_set_closure": ([S, P(Closure)], C.c_int),
+        "wt_get_closure": ([S, P(Closure), P(i32)], C.c_int),
+        "wt_trainer_create": ([i32, i64, P(S)], C.c_int),
+        "wt_trainer_destroy": ([S], None),
+        "wt_trainer_last_error": ([S], C.c_char_p),
+        "wt_trainer_count": ([S], i64),
+        "wt_trainer_clear": ([S], C.c_int),
+        "wt_trainer_add_samples": ([S, S, S, C.c_double, C.c_uint64, P(i64)], C.c_int),
+        "wt_trainer_put_samples": ([S, v, v, i64], C.c_int),
+        "wt_trainer_read_samples": ([S, i64, i64, v, v], C.c_int),
+        "wt_trainer_stats": ([S, v, v], C.c_int),
+        "wt_trainer_set_model": ([S, P(Closure)], C.c_int),
+        "wt_trainer_get_model": ([S, P(Closure)], C.c_int),
+        "wt_trainer_fit": ([S, P(TrainParams), v], C.c_int),
+        "wt_trainer_grad": ([S, i64, i64, P(Closure), P(C.c_double)], C.c_int),
+        "wt_trainer_infer": ([S, v, i64, v], C.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)

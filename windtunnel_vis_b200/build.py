@@ -28,8 +28,9 @@ UNITS = {
     "wt_voxel.cu": ["-fmad=false"],
     "wt_tracer.cu": ["-fmad=false"],
     "wt_fields.cu": ["-fmad=false"],
+    "wt_closure.cu": [],
 }
-HEADERS = ["wt_common.cuh", "wt_internal.h"]
+HEADERS = ["wt_common.cuh", "wt_internal.h", "wt_closure.cuh", "wt_umma.cuh"]
 
 
 def nvcc():

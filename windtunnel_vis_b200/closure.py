@@ -1,0 +1,327 @@
+"""Learned LES closure: training data generated by the solver itself, BF16 training on the GPU,
+and the comparison with plain Smagorinsky.
+
+The reference's only sub-grid model is Smagorinsky (src/solver/wgslLbm.ts:206-214); this module
+drives the extension declared in include/wt.h (wt_closure, wt_trainer):
+
+  data ....... seeded bluff bodies (spheres, boxes, ellipsoids of aspect 1-4) run at a fine grid
+               with the method itself (FP16, Smagorinsky); wt_trainer_add_samples box-filters
+               the fine populations 2 x 2 x 2 onto the coarse grid and stores, per coarse cell, the
+               features the coarse solver would see and the eddy viscosity that best represents
+               the unresolved stress (filtered resolved stress + the fine run's own Smagorinsky
+               stress, projected on the filtered strain rate over a 3 x 3 x 3 neighbourhood)
+  training ... Adam on mean(((nu_t - nu*) / nu_scale)^2) with the project's tcgen05 kernels
+  use ........ Solver.set_closure(model): the coarse run's collision takes tau = tau0' + 3 nu_t
+"""
+import ctypes as C
+import json
+import math
+import time
+
+import numpy as np
+
+from . import abi
+
+FEATURES = ("pi_xx", "pi_yy", "pi_zz", "pi_xy", "pi_xz", "pi_yz", "strain", "wall_distance", "rho", "speed")
+N_IN = abi.CLOSURE_IN
+N_HID = abi.CLOSURE_HID
+N_PARAM = N_IN * N_HID + N_HID + N_HID * N_HID + N_HID + N_HID + 1
+CS_FEATURE = 0.1  # WT_CLOSURE_FEATURE_CS
+
+
+class ClosureError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{msg} (code {code})")
+        self.code = code
+
+
+# ---- the network as numpy arrays -------------------------------------------------------------
+def init_model(seed=1, shift=None, scale=None, nu_scale=1e-3):
+    """Seeded initial network: Xavier-uniform weights, zero biases except b3 (softplus(b3) = 0.1,
+    a small initial viscosity)."""
+    rng = np.random.default_rng(seed)
+
+    def xavier(fan_in, fan_out):
+        lim = math.sqrt(6.0 / (fan_in + fan_out))
+        return rng.uniform(-lim, lim, size=(fan_in, fan_out)).astype(np.float32)
+
+    return {
+        "shift": np.zeros(N_IN, np.float32) if shift is None else np.asarray(shift, np.float32),
+        "scale": np.ones(N_IN, np.float32) if scale is None else np.asarray(scale, np.float32),
+        "w1": xavier(N_IN, N_HID), "b1": np.zeros(N_HID, np.float32),
+        "w2": xavier(N_HID, N_HID), "b2": np.zeros(N_HID, np.float32),
+        "w3": xavier(N_HID, 1)[:, 0].copy(), "b3": np.float32(math.log(math.expm1(0.1))),
+        "nu_scale": np.float32(nu_scale),
+    }
+
+
+def to_struct(m) -> abi.Closure:
+    c = abi.Closure()
+    C.memmove(c.shift, np.ascontiguousarray(m["shift"], np.float32).ctypes.data, 4 * N_IN)
+    C.memmove(c.scale, np.ascontiguousarray(m["scale"], np.float32).ctypes.data, 4 * N_IN)
+    C.memmove(c.w1, np.ascontiguousarray(m["w1"], np.float32).ctypes.data, 4 * N_IN * N_HID)
+    C.memmove(c.b1, np.ascontiguousarray(m["b1"], np.float32).ctypes.data, 4 * N_HID)
+    C.memmove(c.w2, np.ascontiguousarray(m["w2"], np.float32).ctypes.data, 4 * N_HID * N_HID)
+    C.memmove(c.b2, np.ascontiguousarray(m["b2"], np.float32).ctypes.data, 4 * N_HID)
+    C.memmove(c.w3, np.ascontiguousarray(m["w3"], np.float32).ctypes.data, 4 * N_HID)
+    c.b3 = float(m["b3"])
+    c.nu_scale = float(m["nu_scale"])
+    return c
+
+
+def from_struct(c: abi.Closure):
+    raw = np.frombuffer(bytes(c), np.float32)
+    o = 0
+
+    def take(n, shape=None):
+        nonlocal o
+        a = raw[o:o + n].copy()
+        o += n
+        return a.reshape(shape) if shape else a
+
+    m = {"shift": take(N_IN), "scale": take(N_IN), "w1": take(N_IN * N_HID, (N_IN, N_HID)), "b1": take(N_HID),
+         "w2": take(N_HID * N_HID, (N_HID, N_HID)), "b2": take(N_HID), "w3": take(N_HID)}
+    m["b3"] = np.float32(take(1)[0])
+    m["nu_scale"] = np.float32(take(1)[0])
+    return m
+
+
+def flat_params(m):
+    """The 1441 trainable values in wt_closure field order (w1, b1, w2, b2, w3, b3)."""
+    return np.concatenate([np.ravel(m["w1"]), m["b1"], np.ravel(m["w2"]), m["b2"], m["w3"], [m["b3"]]]).astype(np.float32)
+
+
+def save(m, path):
+    np.savez(path, **{k: np.asarray(v) for k, v in m.items()})
+
+
+def load(path):
+    z = np.load(path)
+    return {k: (z[k] if z[k].ndim else z[k][()]) for k in z.files}
+
+
+def smagorinsky_nu(x, cs=CS_FEATURE):
+    """Smagorinsky's eddy viscosity for feature rows (Delta = 1 cell): Cs^2 |S| (feature 6)."""
+    return (cs * cs) * np.asarray(x, np.float64)[:, 6]
+
+
+# ---- trainer ------------------------------------------------------------------------------------
+class Trainer:
+    """wt_trainer: device-resident sample pool, master weights, Adam state."""
+
+    def __init__(self, capacity, device=0):
+        self._lib = abi.load()
+        h = C.c_void_p()
+        rc = self._lib.wt_trainer_create(int(device), int(capacity), C.byref(h))
+        if rc != 0:
+            raise ClosureError(rc, self._lib.wt_last_error(None).decode())
+        self._h = h
+        self.capacity = int(capacity)
+
+    def _check(self, rc):
+        if rc != 0:
+            raise ClosureError(rc, self._lib.wt_trainer_last_error(self._h).decode())
+
+    def destroy(self):
+        if getattr(self, "_h", None):
+            self._lib.wt_trainer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    @property
+    def count(self):
+        return int(self._lib.wt_trainer_count(self._h))
+
+    def clear(self):
+        self._check(self._lib.wt_trainer_clear(self._h))
+
+    def add_samples(self, fine, coarse, keep=1.0, seed=1):
+        added = C.c_int64()
+        self._check(self._lib.wt_trainer_add_samples(self._h, fine.handle, coarse.handle, float(keep), int(seed),
+                                                     C.byref(added)))
+        return int(added.value)
+
+    def put_samples(self, x, y):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, N_IN)
+        y = np.ascontiguousarray(y, np.float32).ravel()
+        assert x.shape[0] == y.size
+        self._check(self._lib.wt_trainer_put_samples(self._h, x.ctypes.data_as(C.c_void_p),
+                                                     y.ctypes.data_as(C.c_void_p), x.shape[0]))
+
+    def read_samples(self, offset=0, n=None):
+        n = self.count - offset if n is None else n
+        x = np.zeros((n, N_IN), np.float32)
+        y = np.zeros(n, np.float32)
+        self._check(self._lib.wt_trainer_read_samples(self._h, int(offset), int(n), x.ctypes.data_as(C.c_void_p),
+                                                      y.ctypes.data_as(C.c_void_p)))
+        return x, y
+
+    def stats(self):
+        mean = np.zeros(N_IN + 1, np.float64)
+        std = np.zeros(N_IN + 1, np.float64)
+        self._check(self._lib.wt_trainer_stats(self._h, mean.ctypes.data_as(C.c_void_p), std.ctypes.data_as(C.c_void_p)))
+        return mean, std
+
+    def set_model(self, m):
+        self._check(self._lib.wt_trainer_set_model(self._h, C.byref(to_struct(m))))
+
+    def get_model(self):
+        c = abi.Closure()
+        self._check(self._lib.wt_trainer_get_model(self._h, C.byref(c)))
+        return from_struct(c)
+
+    def fit(self, steps, batch=16384, lr=2e-3, beta1=0.9, beta2=0.999, eps=1e-8, seed=1):
+        p = abi.TrainParams(int(steps), int(batch), float(lr), float(beta1), float(beta2), float(eps), int(seed))
+        loss = np.zeros(max(int(steps), 1), np.float32)
+        self._check(self._lib.wt_trainer_fit(self._h, C.byref(p), loss.ctypes.data_as(C.c_void_p)))
+        return loss[:steps]
+
+    def grad(self, offset, n):
+        g = abi.Closure()
+        loss = C.c_double()
+        self._check(self._lib.wt_trainer_grad(self._h, int(offset), int(n), C.byref(g), C.byref(loss)))
+        return loss.value, flat_params(from_struct(g)).astype(np.float64)
+
+    def infer(self, x):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, N_IN)
+        nu = np.zeros(x.shape[0], np.float32)
+        self._check(self._lib.wt_trainer_infer(self._h, x.ctypes.data_as(C.c_void_p), x.shape[0],
+                                               nu.ctypes.data_as(C.c_void_p)))
+        return nu
+
+
+def normalized_model(trainer, seed=1):
+    """Initial network whose feature normalisation and output scale come from the pool: shift =
+    mean, scale = 1 / std (features with no spread keep scale 1), nu_scale = mean target."""
+    mean, std = trainer.stats()
+    scale = np.where(std[:N_IN] > 1e-12, 1.0 / np.maximum(std[:N_IN], 1e-12), 1.0)
+    nu_scale = float(max(mean[N_IN], 1e-7))
+    return init_model(seed=seed, shift=mean[:N_IN], scale=scale, nu_scale=nu_scale)
+
+
+# ---- bodies -------------------------------------------------------------------------------------
+def seeded_bodies(count, seed=1, kinds=("sphere", "box", "ellipsoid")):
+    """Bluff bodies for training / evaluation: kind, aspect (streamwise length / height, 1-4 for
+    boxes and ellipsoids), spanwise ratio, and a small off-axis offset, all from the seed. Sizes are
+    fractions of the tunnel height so the same body maps onto the fine and the coarse grid."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        kind = kinds[k % len(kinds)]
+        aspect = 1.0 if kind == "sphere" else float(rng.uniform(1.0, 4.0))
+        span = 1.0 if kind == "sphere" else float(rng.uniform(0.7, 1.3))
+        out.append({"kind": kind, "aspect": aspect, "span": span, "height": 0.125,
+                    "offset": [float(rng.uniform(-0.01, 0.01)), float(rng.uniform(-0.01, 0.01))]})
+    return out
+
+
+def body_fields(dims, body, x_frac=0.3):
+    """Analytic flags (u32), frontal cell count and wall distances (|d| < 2.5 cells, else -1) of a
+    body on a grid, evaluated at cell centres in f64."""
+    nx, ny, nz = dims
+    h = body["height"] * ny
+    half = np.array([0.5 * h * body["aspect"], 0.5 * h, 0.5 * h * body["span"]])
+    c = np.array([x_frac * nx, (0.5 + body["offset"][0]) * ny, (0.5 + body["offset"][1]) * nz])
+    z, y, x = np.meshgrid(np.arange(nz, dtype=np.float64) + 0.5, np.arange(ny, dtype=np.float64) + 0.5,
+                          np.arange(nx, dtype=np.float64) + 0.5, indexing="ij")
+    p = [x - c[0], y - c[1], z - c[2]]
+    if body["kind"] == "box":
+        q = [np.abs(p[a]) - half[a] for a in range(3)]
+        outside = np.sqrt(sum(np.maximum(qa, 0.0) ** 2 for qa in q))
+        inside = np.minimum(np.maximum(np.maximum(q[0], q[1]), q[2]), 0.0)
+        d = outside + inside
+    else:
+        k0 = np.sqrt(sum((p[a] / half[a]) ** 2 for a in range(3)))
+        k1 = np.sqrt(sum((p[a] / half[a] ** 2) ** 2 for a in range(3)))
+        d = k0 * (k0 - 1.0) / np.maximum(k1, 1e-12)
+    solid = d < 0.0
+    dist = np.abs(d)
+    sdf = np.where(dist < 2.5, dist, -1.0).astype(np.float32).ravel()
+    flags = solid.astype(np.uint32).ravel()
+    frontal = int(solid.any(axis=2).sum())
+    return flags, frontal, sdf
+
+
+def tunnel_params(body, dims, u=0.05, re=2000.0, cs=0.1, precision="f16", seed=1):
+    """LES tunnel of a body: Re on the body height, Smagorinsky Cs, outlet sponge, rest state with
+    seeded noise. The molecular viscosity halves with the grid spacing at fixed lattice velocity."""
+    h = body["height"] * dims[1]
+    return dict(u=u, nu=u * h / re, cs=cs, ground="freeslip", sides="freeslip", spongeNu=0.03, spongeStart=0.85,
+                emaAlpha=0, precision=precision, init="rest_noise", initNoise=1e-4, initSeed=seed)
+
+
+def drag_run(make, dims, body, steps, chunk=50, closure=None, measure_from=None, **kw):
+    """One tunnel run of a body: mean C_D (batch-means error bar) over the second half, wall time."""
+    from .analysis import coefficients, window_stats
+
+    flags, frontal, sdf = body_fields(dims, body)
+    p = tunnel_params(body, dims, **kw)
+    s = make(dims, p)
+    s.upload_flags(flags)
+    s.upload_sdf(sdf)
+    if closure is not None:
+        s.set_closure(closure)
+    t0 = time.perf_counter()
+    tt, cd = [], []
+    unstable = False
+    step = 0
+    while step < steps:
+        st = s.step_and_sample(chunk)
+        step += chunk
+        if st["unstable"]:
+            unstable = True
+            break
+        tt.append(st["step"])
+        cd.append(coefficients(st["fx"], st["fy"], st["fz"], p["u"], frontal)["cd"])
+    seconds = time.perf_counter() - t0
+    s.destroy()
+    start = steps // 2 if measure_from is None else measure_from
+    sel = [k for k, t in enumerate(tt) if t >= start]
+    ws = window_stats([tt[k] for k in sel], [cd[k] for k in sel], float(steps)) if len(sel) >= 16 else None
+    return {"cd": ws["mean"] if ws else math.nan, "cd_se": ws["se"] if ws else math.nan, "seconds": seconds,
+            "unstable": unstable, "frontal": frontal, "steps": step, "cells": int(np.prod(dims))}
+
+
+def add_body_samples(trainer, make, body, fine_dims, steps, snapshots=1, every=500, keep=1.0, seed=1, **kw):
+    """Runs the fine tunnel of `body` for `steps`, then takes `snapshots` sample sets `every` steps
+    apart (filtered onto the half-resolution grid of the same body). Returns samples added."""
+    coarse_dims = tuple(d // 2 for d in fine_dims)
+    ff, _, fs = body_fields(fine_dims, body)
+    cf, _, cs_ = body_fields(coarse_dims, body)
+    fine = make(fine_dims, tunnel_params(body, fine_dims, **kw))
+    fine.upload_flags(ff)
+    fine.upload_sdf(fs)
+    pc = tunnel_params(body, fine_dims, **kw)
+    pc["nu"] = pc["nu"] / 2.0
+    coarse = make(coarse_dims, pc)
+    coarse.upload_flags(cf)
+    coarse.upload_sdf(cs_)
+    added = 0
+    fine.step(steps)
+    for k in range(snapshots):
+        if k:
+            fine.step(every)
+        added += trainer.add_samples(fine, coarse, keep=keep, seed=seed * 1000 + k + 1)
+    fine.destroy()
+    coarse.destroy()
+    return added
+
+
+def a_priori_metrics(nu, y):
+    """Error of predicted eddy viscosities against the targets: mean squared error normalised by
+    the target variance (0 = perfect, 1 = no better than the mean), and the correlation."""
+    nu = np.asarray(nu, np.float64)
+    y = np.asarray(y, np.float64)
+    var = float(np.var(y)) if y.size else 0.0
+    mse = float(np.mean((nu - y) ** 2)) if y.size else math.nan
+    corr = float(np.corrcoef(nu, y)[0, 1]) if y.size > 1 and np.std(nu) > 0 and np.std(y) > 0 else math.nan
+    return {"nmse": mse / var if var > 0 else math.nan, "mse": mse, "corr": corr}
+
+
+def summarize(d):
+    return json.dumps(d, indent=1, default=float)

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "wt_internal.h"
+#include "wt_closure.cuh"
 
 namespace {
 
@@ -70,7 +71,7 @@ void free_all(wt_solver* s) {
   void* bufs[] = {s->f[0], s->f[1], s->flags, s->sdf, s->cls, s->vel, s->vel_f32, s->meanA, s->meanB,
                   s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count,
                   s->bcell, s->brec, s->bgam, s->vox_pos, s->vox_idx, s->vox_info,
-                  s->dvort, s->dstat, s->dmean, s->exp_buf, s->probe_buf};
+                  s->dvort, s->dstat, s->dmean, s->exp_buf, s->probe_buf, s->closure_dev};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->result_host) cudaFreeHost(s->result_host);
@@ -428,6 +429,50 @@ int wt_set_wheels(wt_solver* s, const wt_wheel* w, int32_t count) {
     const double r = w[k].r > 1e-3 ? w[k].r : 1e-3;
     s->wheels.w[2 * k] = make_float4((float)w[k].c[0], (float)w[k].c[1], (float)w[k].c[2], (float)(1.0 / r));
     s->wheels.w[2 * k + 1] = make_float4((float)w[k].axis[0], (float)w[k].axis[1], (float)w[k].axis[2], (float)w[k].hw);
+  }
+  return WT_OK;
+}
+
+int wt_set_closure(wt_solver* s, const wt_closure* c) {
+  if (!s) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  if (c == nullptr) {
+    if (s->closure_dev) {
+      invalidate_graphs(s);
+      WT_CUDA(s, cudaStreamSynchronize(s->stream), "wt_set_closure");
+      cudaFree(s->closure_dev);
+      s->closure_dev = nullptr;
+    }
+    return WT_OK;
+  }
+  if (!s->is3d || s->prec == WT_PREC_F64)
+    return fail(s, WT_E_UNSUPPORTED, "wt_set_closure: the learned closure needs a D3Q19 handle with f16 or f32 storage");
+  if (s->dims.nx % 2 != 0 || s->dims.ny < 2 || s->dims.nz < 2 || (uint64_t)s->q * (uint64_t)s->n >= (1ull << 32))
+    return fail(s, WT_E_UNSUPPORTED, "wt_set_closure: the learned closure needs an even nx, ny >= 2, nz >= 2 and "
+                                     "19 n < 2^32");
+  const float* v = reinterpret_cast<const float*>(c);
+  for (size_t k = 0; k < sizeof(wt_closure) / sizeof(float); k++)
+    if (!std::isfinite(v[k])) return fail(s, WT_E_INVALID, "wt_set_closure: non-finite network value");
+  if (!(c->nu_scale >= 0.0f)) return fail(s, WT_E_INVALID, "wt_set_closure: nu_scale must be >= 0");
+  wt::ClosureDev host;
+  std::memset(&host, 0, sizeof host);
+  wt::closure_pack(*c, host);
+  if (!s->closure_dev) {
+    WT_CUDA(s, cudaMalloc((void**)&s->closure_dev, sizeof(wt::ClosureDev)), "wt_set_closure");
+    invalidate_graphs(s);
+  }
+  WT_CUDA(s, cudaMemcpyAsync(s->closure_dev, &host, sizeof host, cudaMemcpyHostToDevice, s->stream), "wt_set_closure");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "wt_set_closure");
+  s->closure_host = *c;
+  return WT_OK;
+}
+
+int wt_get_closure(const wt_solver* s, wt_closure* out, int32_t* enabled) {
+  if (!s) return WT_E_INVALID;
+  if (enabled) *enabled = s->closure_dev != nullptr ? 1 : 0;
+  if (out) {
+    if (s->closure_dev) *out = s->closure_host;
+    else std::memset(out, 0, sizeof *out);
   }
   return WT_OK;
 }

@@ -9,6 +9,10 @@
 #include "../../include/wt.h"
 #include "wt_common.cuh"
 
+namespace wt {
+struct ClosureDev;
+}
+
 struct wt_solver {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -88,6 +92,9 @@ struct wt_solver {
   // false until wt_set_launch or wt_autotune chose a launch: the default then follows the collision
   // operator (occupancy hint 4 for the regularized collision, which fits 64 registers; none for BGK)
   bool launch_explicit = false;
+  // learned closure (wt_set_closure): device copy of the network, nullptr = Smagorinsky
+  wt::ClosureDev* closure_dev = nullptr;
+  wt_closure closure_host{};
   int* err_dev = nullptr;   // device-side error word written by kernels with bounded waits
   int* err_host = nullptr;  // pinned copy
   int64_t launches = 0;
@@ -115,6 +122,10 @@ struct VoxelJob {
   uint32_t* info;
 };
 cudaError_t launch_voxelize(wt_solver* s, const VoxelJob& job);
+
+// learned closure training data (wt_lbm.cu): the fine handle's current populations box-filtered
+// onto a cnx x cny x cnz grid (fine dims = 2 x coarse dims); `out` holds 11 * cnx * cny * cnz floats
+cudaError_t launch_closure_filter(wt_solver* fine, int cnx, int cny, int cnz, float* out, cudaStream_t st);
 
 // derived fields and export (wt_fields.cu)
 cudaError_t launch_derive(wt_solver* s);

@@ -17,8 +17,10 @@
 #include <algorithm>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "wt_internal.h"
+#include "wt_closure.cuh"
 
 namespace wt {
 
@@ -165,9 +167,12 @@ __global__ void __launch_bounds__(256) k_init(const wt_kparams P, typename S::T*
 // Collision on full populations, in the reference's formulation: regularized BGK (or BGK on wall
 // cells / collision = bgk) with the Smagorinsky relaxation time and the outlet / inlet sponges
 // (wgslLbm.ts:177-240). fo receives the post-collision populations.
+//
+// With a learned closure (cw != nullptr, f32 only) the network's eddy viscosity replaces the
+// Smagorinsky term: tau = tau0' + 3 nu_t (tau0' = tau0 with the outlet sponge and the wall floor).
 template <class L, class R>
 __device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L::Q], int ix, bool wall, bool gwall,
-                                             R (&fo)[L::Q]) {
+                                             R (&fo)[L::Q], const ClosureDev* cw = nullptr, float wall_d = 0.0f) {
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
   const R U = (R)P.uin;
@@ -209,7 +214,18 @@ __device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L
   sp = sp < (R)0 ? (R)0 : (sp > (R)1 ? (R)1 : sp);
   R t0 = (R)P.tau0 + (R)3 * (R)P.sponge_nu * sp * sp;
   if (gwall) t0 = t0 > (R)P.tau_wall ? t0 : (R)P.tau_wall;
-  const R tau = (R)0.5 * (t0 + sqrt(t0 * t0 + (R)(18.0 * 1.4142135623730951) * (R)P.csmag2 * piN * irho));
+  R tau;
+  if constexpr (std::is_same<R, float>::value && L::DIM == 3) {
+    if (cw != nullptr) {
+      float x[CL_IN];
+      cl_features(pxx, pyy, pzz, pxy, pxz, pyz, rho, ux, uy, uz, P.tau0, wall_d, x);
+      tau = t0 + 3.0f * closure_nu(cw, x);
+    } else {
+      tau = (R)0.5 * (t0 + sqrt(t0 * t0 + (R)(18.0 * 1.4142135623730951) * (R)P.csmag2 * piN * irho));
+    }
+  } else {
+    tau = (R)0.5 * (t0 + sqrt(t0 * t0 + (R)(18.0 * 1.4142135623730951) * (R)P.csmag2 * piN * irho));
+  }
   const R omega = (R)1 - (R)1 / tau;
   const R k1 = omega * (R)4.5;
   const bool useBGK = wall || P.collision == 1u;
@@ -249,8 +265,9 @@ __device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L
 // round trip instead of a chain of dependent loads per link. `cl` is the cell's class byte: its
 // near-solid bit enables the solid checks, its belt-still bit holds the moving belt still (the
 // tyre contact patch test of wgslLbm.ts:276-287, evaluated once by k_classify). Kept out of line
-// so that it does not inflate the register budget of the kernels that call it.
-template <class L, class S>
+// so that it does not inflate the register budget of the kernels that call it. With PULL the
+// pulled (pre-collision) populations are returned instead of the collided ones.
+template <class L, class S, bool PULL = false>
 __device__ __noinline__ void cell_general(const wt_kparams& P, const typename S::T* __restrict__ fin,
                                           const uint32_t* __restrict__ flags, const uint32_t* __restrict__ sdf,
                                           const Wheels& W, int ix, int iy, int iz, uint32_t cl, typename S::R* out) {
@@ -405,12 +422,19 @@ __device__ __noinline__ void cell_general(const wt_kparams& P, const typename S:
         if (wm & (1u << i)) f[i] -= (R)Wc<L, i>::v * corr;
     });
   }
-  R fo[Q];
-  collide_full<L, R>(P, f, ix, wall, gwall, fo);
-  static_for<Q>([&](auto I) {
-    constexpr int i = I;
-    out[i] = fo[i];
-  });
+  if constexpr (PULL) {
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      out[i] = f[i];
+    });
+  } else {
+    R fo[Q];
+    collide_full<L, R>(P, f, ix, wall, gwall, fo);
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      out[i] = fo[i];
+    });
+  }
 }
 
 // One cell per thread; any storage. Used for f64 and for odd nx.
@@ -667,11 +691,23 @@ __device__ __forceinline__ void relax_cell(const wt_kparams& P, float fx, float 
   omega = 1.0f - __fdividef(1.0f, tau);
 }
 
+// tau0 of one cell with the outlet sponge and a floor (the part of relax_cell before the closure)
+__device__ __forceinline__ float tau0_eff(const wt_kparams& P, float fx, float t_floor) {
+  float t0 = P.tau0;
+  if (fx > P.sponge_start) {
+    const float den = (float)P.nx - P.sponge_start;
+    const float sp = fminf(__fdividef(fx - P.sponge_start, den > 1.0f ? den : 1.0f), 1.0f);
+    t0 += 3.0f * P.sponge_nu * sp * sp;
+  }
+  return fmaxf(t0, t_floor);
+}
+
 // Regularized / BGK collision of two bulk cells at once on shifted populations (lanes .x, .y),
-// same algebra as collide_shifted.
-template <class L, bool BGK, class Emit>
-__device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const float2 (&h)[L::Q], int x, Emit&& emit,
-                                                 float t_floor = 0.0f) {
+// same algebra as collide_shifted. `ofn(rho, irho, ux, uy, uz, pxx, pyy, pzz, pxy, pxz, pyz)`
+// returns the two cells' omega = 1 - 1 / tau (the closure).
+template <class L, bool BGK, class Emit, class OmegaFn>
+__device__ __forceinline__ void collide_shifted2x(const wt_kparams& P, const float2 (&h)[L::Q], int x, Emit&& emit,
+                                                  OmegaFn&& ofn) {
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
   float2 drho = h[0];
@@ -716,17 +752,8 @@ __device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const floa
     pxz = fma2(jx, nuz, sxz);
     pyz = fma2(jy, nuz, syz);
   }
-  float2 omega, k1;
-  if (P.csmag2 > 0.0f || P.sponge_start < (float)P.nx || t_floor > P.tau0) {
-    float2 pn = fma2(pxx, pxx, fma2(pyy, pyy, mul2(f2(2.f), mul2(pxy, pxy))));
-    if constexpr (D3) pn = fma2(pzz, pzz, fma2(f2(2.f), fma2(pxz, pxz, mul2(pyz, pyz)), pn));
-    relax_cell(P, (float)x, pn.x, irho.x, omega.x, t_floor);
-    relax_cell(P, (float)(x + 1), pn.y, irho.y, omega.y, t_floor);
-  } else {
-    const float om = 1.0f - __fdividef(1.0f, P.tau0);
-    omega = f2(om);
-  }
-  k1 = mul2(f2(4.5f), omega);
+  const float2 omega = ofn(rho, irho, ux, uy, uz, pxx, pyy, pzz, pxy, pxz, pyz);
+  const float2 k1 = mul2(f2(4.5f), omega);
   const float2 trP = mul2(add2(add2(pxx, pyy), pzz), f2(1.0f / 3.0f));
   // Q_i : Pi - trP for axis directions (Daa) and for two-component directions (Eab +- 2 Pab)
   const float2 Dxx = sub2(pxx, trP), Dyy = sub2(pyy, trP), Dzz = sub2(pzz, trP);
@@ -796,6 +823,46 @@ __device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const floa
       }
     }
   });
+}
+
+// collide_shifted2x with the reference's closure: molecular tau0, outlet sponge, wall floor and
+// the Smagorinsky eddy viscosity
+template <class L, bool BGK, class Emit>
+__device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const float2 (&h)[L::Q], int x, Emit&& emit,
+                                                 float t_floor = 0.0f) {
+  collide_shifted2x<L, BGK>(P, h, x, emit,
+                            [&](float2 /*rho*/, float2 irho, float2, float2, float2, float2 pxx, float2 pyy, float2 pzz,
+                                float2 pxy, float2 pxz, float2 pyz) {
+                              float2 omega;
+                              if (P.csmag2 > 0.0f || P.sponge_start < (float)P.nx || t_floor > P.tau0) {
+                                float2 pn = fma2(pxx, pxx, fma2(pyy, pyy, mul2(f2(2.f), mul2(pxy, pxy))));
+                                if constexpr (L::DIM == 3)
+                                  pn = fma2(pzz, pzz, fma2(f2(2.f), fma2(pxz, pxz, mul2(pyz, pyz)), pn));
+                                relax_cell(P, (float)x, pn.x, irho.x, omega.x, t_floor);
+                                relax_cell(P, (float)(x + 1), pn.y, irho.y, omega.y, t_floor);
+                              } else {
+                                omega = f2(1.0f - __fdividef(1.0f, P.tau0));
+                              }
+                              return omega;
+                            });
+}
+
+// the learned closure for cells collided on CUDA cores (face rows): the network per lane
+template <class L, bool BGK, class Emit>
+__device__ __forceinline__ void collide_shifted2_lc(const wt_kparams& P, const float2 (&h)[L::Q], int x, Emit&& emit,
+                                                    float t_floor, const ClosureDev* __restrict__ cw, float2 wd) {
+  collide_shifted2x<L, BGK>(P, h, x, emit,
+                            [&](float2 rho, float2, float2 ux, float2 uy, float2 uz, float2 pxx, float2 pyy,
+                                float2 pzz, float2 pxy, float2 pxz, float2 pyz) {
+                              float xa[CL_IN], xb[CL_IN];
+                              cl_features(pxx.x, pyy.x, pzz.x, pxy.x, pxz.x, pyz.x, rho.x, ux.x, uy.x, uz.x, P.tau0,
+                                          wd.x, xa);
+                              cl_features(pxx.y, pyy.y, pzz.y, pxy.y, pxz.y, pyz.y, rho.y, ux.y, uy.y, uz.y, P.tau0,
+                                          wd.y, xb);
+                              const float ta = tau0_eff(P, (float)x, t_floor) + 3.0f * closure_nu(cw, xa);
+                              const float tb = tau0_eff(P, (float)(x + 1), t_floor) + 3.0f * closure_nu(cw, xb);
+                              return make_float2(1.0f - __fdividef(1.0f, ta), 1.0f - __fdividef(1.0f, tb));
+                            });
 }
 
 // two-cell loads / stores of shifted populations: elements (o, o + 1), o even. Loads are split
@@ -944,11 +1011,14 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
 // no-slip or moving floor, and the inlet equilibrium / zero-gradient outlet as in the bulk. Floor
 // rows with bounce-back collide with BGK and the tauWall floor, like the reference's wall cells.
 // Groups holding a solid or a fluid cell next to a solid are left to k_boundary_tab.
-template <class L, class S>
+// With LC the learned closure replaces Smagorinsky (network on CUDA cores, wall distance from sdf).
+template <class L, class S, bool LC = false>
 __global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kparams P,
                                                 const typename S::T* __restrict__ fin,
                                                 typename S::T* __restrict__ fout,
-                                                const uint8_t* __restrict__ cls, int gs) {
+                                                const uint8_t* __restrict__ cls, int gs,
+                                                const uint32_t* __restrict__ sdf = nullptr,
+                                                const ClosureDev* __restrict__ cw = nullptr) {
   typedef PairIO<S> IO;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
@@ -1068,9 +1138,246 @@ __global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kpara
     constexpr int i = decltype(I)::value;
     if (clean) IO::st(fout, i * N + idx0, v, (float)Wc<L, i>::v);
   };
-  if (gwall) collide_shifted2<L, true>(P, h, x0, emit, P.tau_wall);
-  else if (P.collision == 1u) collide_shifted2<L, true>(P, h, x0, emit);
-  else collide_shifted2<L, false>(P, h, x0, emit);
+  if constexpr (LC) {
+    const uint2 sw = __ldg(reinterpret_cast<const uint2*>(sdf + idx0));
+    const float2 wd = make_float2(cl_wall_dist(sw.x), cl_wall_dist(sw.y));
+    if (gwall) collide_shifted2_lc<L, true>(P, h, x0, emit, P.tau_wall, cw, wd);
+    else if (P.collision == 1u) collide_shifted2_lc<L, true>(P, h, x0, emit, 0.0f, cw, wd);
+    else collide_shifted2_lc<L, false>(P, h, x0, emit, 0.0f, cw, wd);
+  } else {
+    if (gwall) collide_shifted2<L, true>(P, h, x0, emit, P.tau_wall);
+    else if (P.collision == 1u) collide_shifted2<L, true>(P, h, x0, emit);
+    else collide_shifted2<L, false>(P, h, x0, emit);
+  }
+}
+
+// ---- bulk kernel with the learned closure: the network on tcgen05 tensor cores -----------------
+//
+// Same pull as the vectorised kernel with two cells per thread (x0, x0 + 1), 128 threads per
+// block. Between the moments and the relaxation the block evaluates the network for its 256 cells:
+// every thread writes the bf16 inputs of its two cells as row `tid` of two 128 x 16 A tiles in
+// shared memory (tile 0: cells x0, tile 1: cells x0 + 1), one thread issues the layer-1 MMAs
+// (M = 128, N = 32, K = 16; tile t accumulates in tensor-memory columns 32 t .. 32 t + 31), every
+// thread reads its row back (tensor-memory lane = tid), adds the bias, applies gelu and writes row
+// `tid` of two 128 x 32 hidden tiles, and the layer-2 MMAs (two K = 16 steps per tile) reuse the
+// same columns. The 32 -> 1 output layer and softplus run on CUDA cores. Rows of threads outside
+// the interior rows carry the rest state and are not stored. Waits on the MMA barrier are bounded;
+// a timeout sets bit 4 of the error word and the block stores nothing.
+constexpr int LC_THREADS = 128;
+constexpr uint32_t LC_TMEM_COLS = 64;
+constexpr int LC_SMEM_A = 0;       // 2 tiles x 128 x 16 bf16
+constexpr int LC_SMEM_H = 8192;    // 2 tiles x 128 x 32 bf16
+constexpr int LC_SMEM_W1 = 24576;  // W1 image, 32 x 16 bf16 (followed by the W2 image: one 3 KB copy)
+constexpr int LC_SMEM_W2 = 25600;  // W2 image, 32 x 32 bf16
+constexpr int LC_SMEM_BAR = 27648; // mbarrier (8 B), then the tensor-memory address (4 B)
+// dynamic shared memory per block: more than 228 KB / 8, so at most 7 blocks share an SM and their
+// 7 x 64 tensor-memory columns fit in the SM's 512 (an allocation never has to wait)
+constexpr int LC_SMEM_BYTES = 29 * 1024;
+constexpr uint32_t LC_WAIT_LIMIT = 1u << 22;
+static_assert(LC_SMEM_BAR + 12 <= LC_SMEM_BYTES, "shared-memory layout");
+static_assert(offsetof(ClosureDev, w2img) == offsetof(ClosureDev, w1img) + 1024, "weight images are contiguous");
+
+// row r of a 128 x 16 A tile: the normalised, bf16-rounded features (10) and zero padding
+__device__ __forceinline__ void lc_write_inputs(uint8_t* tile, uint32_t r, const float (&x)[CL_IN],
+                                                const ClosureDev* __restrict__ cw) {
+  uint32_t w[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const int k0 = 2 * k, k1 = 2 * k + 1;
+    const uint32_t lo = k0 < CL_IN ? bf16_bits(__fmul_rn(__fsub_rn(x[k0], cw->shift[k0]), cw->scale[k0])) : 0u;
+    const uint32_t hi = k1 < CL_IN ? bf16_bits(__fmul_rn(__fsub_rn(x[k1], cw->shift[k1]), cw->scale[k1])) : 0u;
+    w[k] = lo | (hi << 16);
+  }
+  *reinterpret_cast<uint4*>(tile + umma::kmaj_off(r, 0, CL_K1)) = make_uint4(w[0], w[1], w[2], w[3]);
+  *reinterpret_cast<uint4*>(tile + umma::kmaj_off(r, 8, CL_K1)) = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+template <class S, bool BGK>
+__global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_constant__ wt_kparams P,
+                                                                   const typename S::T* __restrict__ fin,
+                                                                   typename S::T* __restrict__ fout,
+                                                                   const uint8_t* __restrict__ cls, int gs,
+                                                                   const uint32_t* __restrict__ sdf,
+                                                                   const ClosureDev* __restrict__ cw,
+                                                                   int* __restrict__ err) {
+  typedef D3Q19 L;
+  typedef PairIO<S> IO;
+  constexpr int Q = L::Q;
+  extern __shared__ __align__(128) uint8_t lc_smem[];
+  const int NX = P.nx, NY = P.ny, NZ = P.nz;
+  const uint32_t tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const uint32_t warp = tid >> 5;
+  const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 2;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z;
+  const bool inside = x0 < NX && iy > 0 && iy < NY - 1 && iz > 0 && iz < NZ - 1;
+  const uint32_t N = P.n;
+  const uint32_t sy = (uint32_t)NX, sz = (uint32_t)NX * (uint32_t)NY;
+  const uint32_t idx0 = inside ? (uint32_t)x0 + sy * (uint32_t)iy + sz * (uint32_t)iz : 0u;
+  // phase 1: the loads of the two cells in flight (as k_stream_collide_v), then the block set-up
+  uint32_t cv = 0x01010101u;
+  typename IO::pair_t rp[Q];
+  typename IO::one_t r1[Q];
+  uint2 sw = make_uint2(0u, 0u);
+  if (inside) {
+    if (gs == 4) cv = __ldg(reinterpret_cast<const unsigned int*>(cls + (idx0 & ~3u)));
+    else cv = __ldg(reinterpret_cast<const unsigned short*>(cls + idx0));
+    const bool last = x0 + 2 >= NX;
+    const typename S::T* fb = fin + idx0;
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+      const typename S::T* ps = fb + ((ptrdiff_t)i * N - (ptrdiff_t)cy * sy - (ptrdiff_t)cz * sz);
+      rp[i] = IO::ld(ps, 0u);
+      if constexpr (cx > 0) r1[i] = IO::ld1(x0 > 0 ? ps - 1 : ps, 0u);
+      if constexpr (cx < 0) r1[i] = IO::ld1(ps + (last ? 1 : 2), 0u);
+    });
+    sw = __ldg(reinterpret_cast<const uint2*>(sdf + idx0));
+  } else {
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      rp[i] = typename IO::pair_t{};
+      r1[i] = typename IO::one_t{};
+    });
+  }
+  uint8_t* const sA = lc_smem + LC_SMEM_A;
+  uint8_t* const sH = lc_smem + LC_SMEM_H;
+  uint64_t* const mbar = reinterpret_cast<uint64_t*>(lc_smem + LC_SMEM_BAR);
+  uint32_t* const tslot = reinterpret_cast<uint32_t*>(lc_smem + LC_SMEM_BAR + 8);
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(cw->w1img);
+    uint4* dst = reinterpret_cast<uint4*>(lc_smem + LC_SMEM_W1);
+    for (uint32_t k = tid; k < 192u; k += LC_THREADS) dst[k] = __ldg(src + k);
+  }
+  if (tid == 0) umma::mbar_init(mbar, 1);
+  if (warp == 0) umma::tmem_alloc(tslot, LC_TMEM_COLS);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *tslot;
+  // phase 2: pulled populations (rest state outside), the network, collision, stores
+  float2 h[Q];
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    constexpr int cx = L::c[i][0];
+    constexpr float w = (float)Wc<L, i>::v;
+    const float2 cur = IO::cvt(rp[i], w);
+    float2 v;
+    if constexpr (cx == 0) v = cur;
+    else if constexpr (cx > 0) v = make_float2(IO::cvt1(r1[i], w), cur.x);
+    else v = make_float2(cur.y, IO::cvt1(r1[i], w));
+    h[i] = inside ? v : f2(0.0f);
+  });
+  if (inside && x0 == 0) {
+    const float U = P.uin;
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      constexpr int cx = L::c[i][0];
+      if constexpr (cx > 0) {
+        constexpr float w = (float)Wc<L, i>::v;
+        h[i].x = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
+      }
+    });
+  }
+  const float2 wd = make_float2(cl_wall_dist(sw.x), cl_wall_dist(sw.y));
+  const bool store = inside && (cv & 0x03030303u) == 0u;
+  bool ok = true;
+  typename S::T* ob = fout + idx0;
+  collide_shifted2x<L, BGK>(
+      P, h, x0,
+      [&](auto I, float2 v) {
+        constexpr int i = decltype(I)::value;
+        if (store && ok) IO::st(ob + (ptrdiff_t)i * N, 0u, v, (float)Wc<L, i>::v);
+      },
+      [&](float2 rho, float2, float2 ux, float2 uy, float2 uz, float2 pxx, float2 pyy, float2 pzz, float2 pxy,
+          float2 pxz, float2 pyz) {
+        {
+          float xa[CL_IN], xb[CL_IN];
+          cl_features(pxx.x, pyy.x, pzz.x, pxy.x, pxz.x, pyz.x, rho.x, ux.x, uy.x, uz.x, P.tau0, wd.x, xa);
+          cl_features(pxx.y, pyy.y, pzz.y, pxy.y, pxz.y, pyz.y, rho.y, ux.y, uy.y, uz.y, P.tau0, wd.y, xb);
+          lc_write_inputs(sA, tid, xa, cw);
+          lc_write_inputs(sA + 4096, tid, xb, cw);
+        }
+        constexpr uint32_t ID = umma::idesc_bf16<128, CL_H>();
+        umma::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+          umma::fence_after_sync();
+          const uint64_t bw1 = umma::sdesc(umma::smem_u32(lc_smem + LC_SMEM_W1), 128, 256);
+          umma::mma_bf16(tmem, umma::sdesc(umma::smem_u32(sA), 128, 256), bw1, ID, false);
+          umma::mma_bf16(tmem + 32, umma::sdesc(umma::smem_u32(sA + 4096), 128, 256), bw1, ID, false);
+          umma::commit(mbar);
+        }
+        ok = umma::mbar_wait(mbar, 0, LC_WAIT_LIMIT);
+        umma::fence_after_sync();
+        // hidden layer 1: bias, gelu, bf16 -> row tid of the hidden tiles
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+          float v[4][8];
+#pragma unroll
+          for (int c = 0; c < 4; c++) umma::tmem_ld8(umma::tmem_lane_addr(tmem, warp, 32 * t + 8 * c), v[c]);
+          umma::tmem_wait_ld();
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            uint32_t pk[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+              const int j = 8 * c + 2 * e;
+              const uint32_t lo = bf16_bits(cl_gelu(__fadd_rn(v[c][2 * e], cw->b1[j])));
+              const uint32_t hi = bf16_bits(cl_gelu(__fadd_rn(v[c][2 * e + 1], cw->b1[j + 1])));
+              pk[e] = lo | (hi << 16);
+            }
+            *reinterpret_cast<uint4*>(sH + 8192 * t + umma::kmaj_off(tid, 8 * c, CL_H)) =
+                make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          }
+        }
+        umma::fence_before_sync();
+        umma::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+          umma::fence_after_sync();
+          const uint32_t w2 = umma::smem_u32(lc_smem + LC_SMEM_W2);
+#pragma unroll
+          for (int t = 0; t < 2; t++) {
+            const uint32_t a = umma::smem_u32(sH + 8192 * t);
+            umma::mma_bf16(tmem + 32 * t, umma::sdesc(a, 128, 512), umma::sdesc(w2, 128, 512), ID, false);
+            umma::mma_bf16(tmem + 32 * t, umma::sdesc(a + 256, 128, 512), umma::sdesc(w2 + 256, 128, 512), ID,
+                           true);
+          }
+          umma::commit(mbar);
+        }
+        ok = umma::mbar_wait(mbar, 1, LC_WAIT_LIMIT) && ok;
+        umma::fence_after_sync();
+        // hidden layer 2 and the output layer
+        float z3[2];
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+          float v[4][8];
+#pragma unroll
+          for (int c = 0; c < 4; c++) umma::tmem_ld8(umma::tmem_lane_addr(tmem, warp, 32 * t + 8 * c), v[c]);
+          umma::tmem_wait_ld();
+          float z = 0.0f;
+#pragma unroll
+          for (int c = 0; c < 4; c++)
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+              const int j = 8 * c + e;
+              z = __fmaf_rn(bf16r(cl_gelu(__fadd_rn(v[c][e], cw->b2[j]))), cw->w3[j], z);
+            }
+          z3[t] = __fmul_rn(cw->nu_scale, cl_softplus(__fadd_rn(z, cw->b3)));
+        }
+        const float ta = tau0_eff(P, (float)x0, 0.0f) + 3.0f * z3[0];
+        const float tb = tau0_eff(P, (float)(x0 + 1), 0.0f) + 3.0f * z3[1];
+        return make_float2(1.0f - __fdividef(1.0f, ta), 1.0f - __fdividef(1.0f, tb));
+      });
+  // release the tensor memory once every thread's reads have completed
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_free(tmem, LC_TMEM_COLS);
+  }
+  if (!ok) atomicOr(err, 4);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1227,12 +1534,15 @@ __global__ void __launch_bounds__(128) k_boundary_build(const __grid_constant__ 
 
 // Applies the link records, one thread per listed cell: every record load of the cell in flight
 // at once (coalesced across the warp), then every gather, then the collision and the stores.
-template <class L, class S>
+// With LC the learned closure replaces Smagorinsky (network on CUDA cores, wall distance from sdf).
+template <class L, class S, bool LC = false>
 __global__ void __launch_bounds__(64) k_boundary_tab(const __grid_constant__ wt_kparams P,
                                                      const typename S::T* __restrict__ fin,
                                                      typename S::T* __restrict__ fout,
                                                      const uint2* __restrict__ bcell, const uint4* __restrict__ rec,
-                                                     const float* __restrict__ gam, uint32_t count, uint32_t cap) {
+                                                     const float* __restrict__ gam, uint32_t count, uint32_t cap,
+                                                     const uint32_t* __restrict__ sdf = nullptr,
+                                                     const ClosureDev* __restrict__ cw = nullptr) {
   constexpr int Q = L::Q;
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= count) return;
@@ -1256,7 +1566,11 @@ __global__ void __launch_bounds__(64) k_boundary_tab(const __grid_constant__ wt_
     f[i] = fmaf(__uint_as_float(r[i].z), S::cvt(x1[i], 0.0f), fmaf(__uint_as_float(r[i].w), S::cvt(x2[i], 0.0f), g[i]));
   });
   const int ix = (int)(hc.x % P.nx);
-  collide_full<L, float>(P, f, ix, (hc.y & BC_WALL) != 0u, (hc.y & BC_GWALL) != 0u, fo);
+  if constexpr (LC)
+    collide_full<L, float>(P, f, ix, (hc.y & BC_WALL) != 0u, (hc.y & BC_GWALL) != 0u, fo, cw,
+                           cl_wall_dist(__ldg(sdf + hc.x)));
+  else
+    collide_full<L, float>(P, f, ix, (hc.y & BC_WALL) != 0u, (hc.y & BC_GWALL) != 0u, fo);
   static_for<Q>([&](auto I) {
     constexpr int i = I;
     S::st(fout, (size_t)i * P.n + hc.x, fo[i], (float)Wc<L, i>::v);
@@ -1560,6 +1874,93 @@ __global__ void __launch_bounds__(REDUCE_THREADS) k_reduce_partials(const double
 }
 
 // ---------------------------------------------------------------------------------------------
+// learned closure: box filter of a fine run onto the coarse grid (training data)
+// ---------------------------------------------------------------------------------------------
+// One thread per coarse cell (cx, cy, cz) over the fine cells (2 cx + a, 2 cy + b, 2 cz + c). Each
+// fine cell's pulled, pre-collision populations (every boundary rule, cell_general) give rho, j and
+// the non-equilibrium stress Pi; the fine run's own Smagorinsky stress is
+//   sigma = -2 nu_sgs S = 3 nu_sgs Pi / (rho tau_s),  tau_s = (t0 + sqrt(t0^2 + 18 sqrt(2) Cs^2 |Pi| / rho)) / 2,
+//   nu_sgs = (tau_s - t0) / 3 (t0 = the fine tau0),
+// and the filtered quantities are
+//   rho~ = <rho>,  u~ = <j> / <rho>,  T = <rho u u> / <rho> - u~ u~ + <sigma>
+// (< > = mean over the 8 fine cells; stresses are invariant between the two lattices under the
+// same lattice velocity). out (11 floats per coarse cell, structure of arrays [k * nc + cell]):
+// rho~, u~ (3), T (xx, yy, zz, xy, xz, yz), valid (1 if all 8 fine cells are fluid, else 0).
+template <class S>
+__global__ void __launch_bounds__(128) k_closure_filter(const __grid_constant__ wt_kparams P,
+                                                        const typename S::T* __restrict__ fin,
+                                                        const uint32_t* __restrict__ flags,
+                                                        const uint32_t* __restrict__ sdf,
+                                                        const uint8_t* __restrict__ cls,
+                                                        const __grid_constant__ Wheels W, int cnx, int cny, int cnz,
+                                                        float* __restrict__ out) {
+  typedef D3Q19 L;
+  typedef typename S::R R;
+  constexpr int Q = L::Q;
+  const int cx = blockIdx.x * blockDim.x + threadIdx.x, cy = blockIdx.y, cz = blockIdx.z;
+  if (cx >= cnx) return;
+  const size_t nc = (size_t)cnx * cny * cnz;
+  const size_t cidx = (size_t)cx + (size_t)cnx * ((size_t)cy + (size_t)cny * (size_t)cz);
+  double srho = 0, sj[3] = {0, 0, 0}, suu[6] = {0, 0, 0, 0, 0, 0}, ssg[6] = {0, 0, 0, 0, 0, 0};
+  bool valid = true;
+  const double t0 = P.tau0;
+  const double k = 18.0 * 1.4142135623730951 * (double)P.csmag2;
+  for (int c = 0; c < 8 && valid; c++) {
+    const int ix = 2 * cx + (c & 1), iy = 2 * cy + ((c >> 1) & 1), iz = 2 * cz + (c >> 2);
+    const size_t idx = cell_id(ix, iy, iz, P.nx, P.ny);
+    const uint8_t cl = cls[idx];
+    if (cl & CLS_SOLID) {
+      valid = false;
+      break;
+    }
+    R f[Q];
+    cell_general<L, S, true>(P, fin, flags, sdf, W, ix, iy, iz, cl, f);
+    double rho = 0, j[3] = {0, 0, 0}, m[6] = {0, 0, 0, 0, 0, 0};
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      constexpr int ex = L::c[i][0], ey = L::c[i][1], ez = L::c[i][2];
+      const double v = (double)f[i];
+      rho += v;
+      j[0] += ex * v;
+      j[1] += ey * v;
+      j[2] += ez * v;
+      m[0] += ex * ex * v;
+      m[1] += ey * ey * v;
+      m[2] += ez * ez * v;
+      m[3] += ex * ey * v;
+      m[4] += ex * ez * v;
+      m[5] += ey * ez * v;
+    });
+    const double u[3] = {j[0] / rho, j[1] / rho, j[2] / rho};
+    const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+    double pi[6], pn = 0;
+    for (int q = 0; q < 6; q++) {
+      pi[q] = m[q] - rho * (u[pa[q]] * u[pb[q]] + (q < 3 ? 1.0 / 3.0 : 0.0));
+      pn += (q < 3 ? 1.0 : 2.0) * pi[q] * pi[q];
+    }
+    const double ts = 0.5 * (t0 + sqrt(t0 * t0 + k * sqrt(pn) / rho));
+    const double nus = (ts - t0) / 3.0;
+    srho += rho;
+    for (int a = 0; a < 3; a++) sj[a] += j[a];
+    for (int q = 0; q < 6; q++) {
+      suu[q] += j[pa[q]] * j[pb[q]] / rho;
+      ssg[q] += 3.0 * nus * pi[q] / (rho * ts);
+    }
+  }
+  if (!valid) {
+    for (int q = 0; q < 11; q++) out[(size_t)q * nc + cidx] = 0.0f;
+    return;
+  }
+  const double u[3] = {sj[0] / srho, sj[1] / srho, sj[2] / srho};
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+  out[cidx] = (float)(srho / 8.0);
+  for (int a = 0; a < 3; a++) out[(size_t)(1 + a) * nc + cidx] = (float)u[a];
+  for (int q = 0; q < 6; q++)
+    out[(size_t)(4 + q) * nc + cidx] = (float)(suu[q] / srho - u[pa[q]] * u[pb[q]] + ssg[q] / 8.0);
+  out[(size_t)10 * nc + cidx] = 1.0f;
+}
+
+// ---------------------------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------------------------
 #define WT_DISPATCH(FN, ...)                                                                  \
@@ -1702,7 +2103,11 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
   if constexpr (vec_ok) {
     const int V = s->sc_param;
     const bool faces_ok = s->dims.ny >= 2 && (L::DIM == 2 || s->dims.nz >= 2);
-    if ((V == 2 || V == 4) && s->dims.nx % V == 0 && s->gs >= V && faces_ok && offsets32(s)) {
+    // the learned closure runs on this path only (bulk kernel k_stream_collide_lc)
+    const ClosureDev* cw = L::DIM == 3 ? s->closure_dev : nullptr;
+    if (cw != nullptr && !(s->dims.nx % 2 == 0 && s->gs >= 2 && faces_ok && offsets32(s)))
+      return cudaErrorNotSupported;
+    if (cw != nullptr || ((V == 2 || V == 4) && s->dims.nx % V == 0 && s->gs >= V && faces_ok && offsets32(s))) {
       const int runs = s->dims.nx / V;
       int bx = s->sc_bx, by = s->sc_by;
       if (bx <= 0 || by <= 0) {
@@ -1733,15 +2138,29 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
         const int fbx = runs2 >= 128 ? 128 : ((runs2 + 31) / 32) * 32;
         const int fby = 256 / fbx;
         const dim3 fgrid((runs2 + fbx - 1) / fbx, (fr + fby - 1) / fby, 1);
-        k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin, (typename S::T*)fout,
-                                                         s->cls, s->gs);
+        if constexpr (L::DIM == 3) {
+          if (cw != nullptr)
+            k_face_v<L, S, true><<<fgrid, dim3(fbx, fby), 0, bs>>>(
+                s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, cw);
+          else
+            k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin,
+                                                             (typename S::T*)fout, s->cls, s->gs);
+        } else {
+          k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin, (typename S::T*)fout,
+                                                           s->cls, s->gs);
+        }
         s->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
       }
       if (s->nbnd > 0) {
-        k_boundary_tab<L, S><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
-            s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
-            (uint32_t)s->btab_cap);
+        if (cw != nullptr)
+          k_boundary_tab<L, S, L::DIM == 3><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
+              s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
+              (uint32_t)s->btab_cap, s->sdf, cw);
+        else
+          k_boundary_tab<L, S><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
+              s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
+              (uint32_t)s->btab_cap);
         s->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
       }
@@ -1756,6 +2175,28 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
           s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs);                                  \
   } while (0)
       const int mb = s->sc_kernel;
+      if constexpr (L::DIM == 3) {
+        if (cw != nullptr) {
+          // learned closure: 128-thread blocks of (tpr, 128 / tpr) over the rows
+          const int runs2 = s->dims.nx / 2;
+          const int tpr = runs2 > 64 ? 128 : (runs2 > 32 ? 64 : 32);
+          const dim3 lblock(tpr, LC_THREADS / tpr);
+          const dim3 lgrid((runs2 + tpr - 1) / tpr, (s->dims.ny + lblock.y - 1) / lblock.y, s->dims.nz);
+          if (s->kp.collision == 1u)
+            k_stream_collide_lc<S, true><<<lgrid, lblock, LC_SMEM_BYTES, s->stream>>>(
+                s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, cw, s->err_dev);
+          else
+            k_stream_collide_lc<S, false><<<lgrid, lblock, LC_SMEM_BYTES, s->stream>>>(
+                s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, cw, s->err_dev);
+          s->launches++;
+          if ((e = cudaGetLastError()) != cudaSuccess) return e;
+          if (s->aux) {
+            if ((e = cudaEventRecord(s->ev_join, s->aux)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(s->stream, s->ev_join, 0)) != cudaSuccess) return e;
+          }
+          return cudaSuccess;
+        }
+      }
       if (V == 2) {
         if (mb == 2) WT_LAUNCH_V(2, 2);
         else if (mb == 3) WT_LAUNCH_V(2, 3);
@@ -1801,6 +2242,22 @@ static cudaError_t macro_t(wt_solver* s) {
 cudaError_t launch_init(wt_solver* s) { WT_DISPATCH(init_t, s); }
 cudaError_t launch_stream_collide(wt_solver* s, const void* fin, void* fout) { WT_DISPATCH(sc_t, s, fin, fout); }
 cudaError_t launch_macro(wt_solver* s) { WT_DISPATCH(macro_t, s); }
+
+cudaError_t launch_closure_filter(wt_solver* fine, int cnx, int cny, int cnz, float* out, cudaStream_t st) {
+  const wt_solver* s = fine;
+  if (!s->is3d) return cudaErrorNotSupported;
+  const int bx = cnx >= 128 ? 128 : ((cnx + 31) / 32) * 32;
+  const dim3 grid((unsigned)((cnx + bx - 1) / bx), (unsigned)cny, (unsigned)cnz);
+#define WT_FILTER(SS)                                                                                         \
+  k_closure_filter<SS><<<grid, bx, 0, st>>>(s->kp, (const typename SS::T*)s->f[s->parity], s->flags, s->sdf, \
+                                            s->cls, s->wheels, cnx, cny, cnz, out)
+  if (s->prec == WT_PREC_F16) WT_FILTER(StF16);
+  else if (s->prec == WT_PREC_F64) WT_FILTER(StF64);
+  else WT_FILTER(StF32);
+#undef WT_FILTER
+  fine->launches++;
+  return cudaGetLastError();
+}
 
 // ---------------------------------------------------------------------------------------------
 // sampling pass on caller-owned buffers, with its reduction scratch in a fixed device array

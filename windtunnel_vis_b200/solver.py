@@ -110,6 +110,28 @@ class Solver:
     def clear_stats(self):
         self._check(self._lib.wt_clear_stats(self._h))
 
+    # ---- learned closure (wt_set_closure) -----------------------------------------------------
+    def set_closure(self, model):
+        """Installs the learned closure (a dict of arrays, see windtunnel_vis_b200.closure, or an
+        abi.Closure) in place of Smagorinsky; None restores Smagorinsky."""
+        if model is None:
+            self._check(self._lib.wt_set_closure(self._h, None))
+            return
+        from .closure import to_struct
+
+        c = model if isinstance(model, abi.Closure) else to_struct(model)
+        self._check(self._lib.wt_set_closure(self._h, C.byref(c)))
+
+    def get_closure(self):
+        c = abi.Closure()
+        on = C.c_int32()
+        self._check(self._lib.wt_get_closure(self._h, C.byref(c), C.byref(on)))
+        if not on.value:
+            return None
+        from .closure import from_struct
+
+        return from_struct(c)
+
     # ---- geometry ----------------------------------------------------------------------------
     def upload_flags(self, flags):
         f = np.ascontiguousarray(np.asarray(flags).ravel(), np.uint32)
