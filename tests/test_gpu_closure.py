@@ -116,7 +116,7 @@ def test_stream_collide_with_network_matches_oracle(gpu, oracle, dims, pset):
     p.upload_sdf(sdf)
     p.set_wheels(wheels)
     p.step(10)
-    assert np.abs(p.current.astype(np.float64) - o.current.astype(np.float64)).max() > 50 * 1e-5
+    assert np.abs(p.current.astype(np.float64) - o.current.astype(np.float64)).max() > 10 * 1e-5
     assert g.get_closure() is not None
     g.destroy()
 
