@@ -48,17 +48,27 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def measured_traffic(shape):
+def measured_traffic(shape, closure=False):
     """DRAM bytes (read + write) per step of this launch shape from the committed ncu summary
     (steady state over 30 steps), or None when that launch was not captured."""
-    p = os.path.join(ROOT, "profiles", "stream_collide_d3q19_f16_sphere256.md")
+    name = "stream_collide_d3q19_f16_sphere256_learned_closure.md" if closure else "stream_collide_d3q19_f16_sphere256.md"
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
-    key = ",".join(str(int(v)) for v in shape)
+    key = "lc" if closure else ",".join(str(int(v)) for v in shape)
     for m in re.finditer(r"^traffic_bytes_per_step\[([0-9,]+)\]:\s*(\d+)", open(p).read(), flags=re.M):
         if m.group(1) == key:
             return int(m.group(2))
     return None
+
+
+def bench_closure():
+    """A seeded network for timing the learned-closure step, its input normalisation set to the
+    bench tunnel's feature ranges (timing does not depend on the weights' values)."""
+    from windtunnel_vis_b200 import closure as CL
+
+    scale = 1.0 / np.array([2e-4, 2e-4, 2e-4, 1e-4, 1e-4, 1e-4, 2e-3, 1.0, 2e-3, 0.02])
+    return CL.init_model(seed=1, shift=[0, 0, 0, 0, 0, 0, 1e-3, 2.5, 1.0, 0.05], scale=scale, nu_scale=2e-4)
 
 
 def geometry():
@@ -162,6 +172,9 @@ def components(s, peak, no_cpu):
       voxelize ... the vehicle body (about 200k triangles) into 512 x 256 x 256 through the public
                    API (host mesh in, flags / wall distances / info on the device); 24 B per cell
                    (3 i32 crossing counters, vote word, flags, wall distance)
+      closure_step the bench tunnel's stream-collide step with the learned closure in place of
+                   Smagorinsky; 76 B per update as the headline, plus 3072 tensor-core flops per
+                   cell (x' W1 with K padded to 16, then h1 W2)
     """
     import torch
 
@@ -266,6 +279,43 @@ def components(s, peak, no_cpu):
         out["tracers"]["cpu_kind"] = "port"
         out["tracers"]["cpu_threads"] = O.threads(0)
 
+    # learned closure: the stream-collide step of the bench tunnel with the network in place of
+    # Smagorinsky (bulk kernel with the two 32-wide layers on tcgen05), its own handle
+    from windtunnel_vis_b200 import closure as CL
+
+    flags_c, _, sdf_c = geometry()
+    c = Solver(DIMS, PARAMS)
+    c.upload_flags(flags_c)
+    c.upload_sdf(sdf_c)
+    c.set_closure(bench_closure())
+    c.step(20)
+    cst = torch.cuda.ExternalStream(c.stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 40
+    torch.cuda.synchronize()
+    a.record(cst)
+    for _ in range(reps):
+        c.step(2)
+    b.record(cst)
+    torch.cuda.synchronize()
+    cms = a.elapsed_time(b) / (2 * reps)
+    out["closure_step"] = {"ms_per_update": round(cms, 4), "mlups": round(n / cms / 1e3, 1),
+                           "bytes_alg": n * 76, "achieved_gbs": round(n * 76 / cms / 1e6, 1),
+                           "frac": round(n * 76 / cms / 1e6 / peak, 4),
+                           "tensor_flop_per_cell": 2 * (16 * 32 + 32 * 32),
+                           "tensor_tflops": round(2 * (16 * 32 + 32 * 32) * n / cms / 1e9, 2)}
+    c.destroy()
+    if not no_cpu:
+        oc = O.OracleSolver(DIMS, PARAMS)
+        oc.upload_flags(flags_c)
+        oc.upload_sdf(sdf_c)
+        oc.set_closure(CL.to_struct(CL.init_model(seed=1, nu_scale=2e-4)))
+        oc._init()
+        t0 = time.perf_counter()
+        oc.step(1)
+        out["closure_step"]["cpu_ref_ms"] = round((time.perf_counter() - t0) * 1e3, 1)
+        out["closure_step"]["cpu_threads"] = O.threads(0)
+
     # voxelizer (vehicle config, its own 512 x 256 x 256 handle)
     vd = (512, 256, 256)
     p, idx, M16, wheels, _ = vehicle_setup(vd)
@@ -348,9 +398,12 @@ def run_ours(args, rank, world, local_rank, dist):
 
     if args.launch:
         s.set_launch(*(int(v) for v in args.launch.split(",")))
+    if args.closure:
+        s.set_closure(bench_closure())
     for _ in range(max(args.warmup, 3)):
         s.step_and_sample(CHUNK)
-    shape = s.get_launch() if args.launch else s.autotune(10)
+    # the tuner times the Smagorinsky kernel's launches; the closure kernel has one launch shape
+    shape = s.get_launch() if (args.launch or args.closure) else s.autotune(10)
     torch.cuda.synchronize()
     barrier()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -399,9 +452,9 @@ def run_ours(args, rank, world, local_rank, dist):
         return
     peak, peak_kind = peaks()
     achieved = n * BYTES_PER_UPDATE / (sc_ms / 1e3) / 1e9
-    traffic = measured_traffic(shape)
+    traffic = measured_traffic(shape, args.closure)
     comps = None
-    if world == 1 and not args.no_components:
+    if world == 1 and not args.no_components and not args.closure:
         comps = components(s, peak, args.no_cpu)
     cpu = None
     if world == 1 and not args.no_cpu:
@@ -412,13 +465,16 @@ def run_ours(args, rank, world, local_rank, dist):
         "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": list(DIMS), "storage": "f16 shifted (f - w)",
+        "config": {"workload": WORKLOAD + (", learned closure in place of Smagorinsky" if args.closure else ""),
+                   "grid": list(DIMS), "storage": "f16 shifted (f - w)",
                    "bench_step": f"{CHUNK} lattice updates + macro/force pass + stats readback",
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2: 2 x 159 MB population buffers",
                    "launch": {"cells_per_thread": shape[1], "block": [shape[2], shape[3]]}},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": ("one lattice update: k_stream_collide_v<D3Q19,StF16> (bulk) overlapped with "
+                     "kernel": ("one lattice update: k_stream_collide_lc<StF16> (bulk, network on tcgen05) overlapped "
+                                "with k_face_v and k_boundary_tab (network on CUDA cores)" if args.closure else
+                                "one lattice update: k_stream_collide_v<D3Q19,StF16> (bulk) overlapped with "
                                 "k_face_v and k_boundary_tab" if shape[1] > 1 else "k_stream_collide<D3Q19,StF16>"),
                      "bytes_alg_per_update": n * BYTES_PER_UPDATE, "traffic_per": "lattice update (ncu, steady state)",
                      "update_ms": round(sc_ms, 5)},
@@ -443,6 +499,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-components", action="store_true", help="skip the sample / tracer / voxelizer timings")
     ap.add_argument("--launch", default="", help="fixed stream-collide launch 'hint,cells,bx,by' instead of the tuner")
+    ap.add_argument("--closure", action="store_true", help="time the step with the learned closure in place of "
+                    "Smagorinsky (a seeded network; no component timings)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

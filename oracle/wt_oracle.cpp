@@ -241,27 +241,30 @@ static float cl_wall_dist(uint32_t s) {
   return d < WT_CLOSURE_WALL_CAP ? d : WT_CLOSURE_WALL_CAP;
 }
 
+/* gelu(x) = x (1/2 + tanh(u) / 2), u = x (C0 + C1 x^2), C0 = sqrt(2/pi), C1 = 0.044715 C0 */
+static const float GELU_C0 = 0.7978845608028654f, GELU_C1 = 0.035677408136300125f,
+                   GELU_C1x3 = 0.10703222440890037f;
+
 static float cl_gelu(float x) {
-  const float inner = std::fma(0.044715f * (x * x), x, x);
-  const float t = std::tanh(0.7978845608028654f * inner);
-  const float hx = 0.5f * x;
-  return std::fma(hx, t, hx);
+  const float t = std::tanh(x * std::fma(GELU_C1, x * x, GELU_C0));
+  return x * std::fma(0.5f, t, 0.5f);
 }
 
 static float cl_gelu_d(float x, float& d) {
   const float x2 = x * x;
-  const float inner = std::fma(0.044715f * x2, x, x);
-  const float t = std::tanh(0.7978845608028654f * inner);
-  const float hx = 0.5f * x;
-  const float du = 0.7978845608028654f * std::fma(0.134145f, x2, 1.0f);
-  d = std::fma(hx * std::fma(-t, t, 1.0f), du, 0.5f * (1.0f + t));
-  return std::fma(hx, t, hx);
+  const float t = std::tanh(x * std::fma(GELU_C1, x2, GELU_C0));
+  const float q = std::fma(0.5f, t, 0.5f);
+  const float du = std::fma(GELU_C1x3, x2, GELU_C0);
+  d = std::fma((0.5f * x) * std::fma(-t, t, 1.0f), du, q);
+  return x * q;
 }
 
 static float cl_softplus(float z) { return z > 20.0f ? z : std::log1p(std::exp(z)); }
 
-/* network input k: bf16((x - shift) * scale) */
-static float cl_input(const wt_closure& C, const float* x, int k) { return cl_bf16r((x[k] - C.shift[k]) * C.scale[k]); }
+/* network input k: bf16(fma(x, scale, nshift)), nshift = -(shift * scale) */
+static float cl_input(const wt_closure& C, const float* x, int k) {
+  return cl_bf16r(std::fma(x[k], C.scale[k], -(C.shift[k] * C.scale[k])));
+}
 
 /* forward pass of one sample; the optional outputs keep the intermediate values for the gradient */
 static float cl_forward(const wt_closure& C, const float* xin, float* xn = nullptr, float* z1 = nullptr,
@@ -274,15 +277,16 @@ static float cl_forward(const wt_closure& C, const float* xin, float* xn = nullp
     a1[j] = a + C.b1[j];
     b1[j] = cl_bf16r(cl_gelu(a1[j]));
   }
-  float z3 = 0.0f;
+  float ze = 0.0f, zo = 0.0f; /* even and odd hidden units summed separately */
   for (int j = 0; j < WT_CLOSURE_HID; j++) {
     float a = 0.0f;
     for (int i = 0; i < WT_CLOSURE_HID; i++) a = std::fma(b1[i], cl_bf16r(C.w2[i][j]), a);
     a2[j] = a + C.b2[j];
-    b2[j] = cl_bf16r(cl_gelu(a2[j]));
-    z3 = std::fma(b2[j], cl_bf16r(C.w3[j]), z3);
+    b2[j] = cl_gelu(a2[j]); /* h2 stays f32 */
+    if (j & 1) zo = std::fma(b2[j], cl_bf16r(C.w3[j]), zo);
+    else ze = std::fma(b2[j], cl_bf16r(C.w3[j]), ze);
   }
-  z3 = z3 + C.b3;
+  const float z3 = (ze + zo) + C.b3;
   if (xn) std::memcpy(xn, x, sizeof x);
   if (z1) std::memcpy(z1, a1, sizeof a1);
   if (h1) std::memcpy(h1, b1, sizeof b1);

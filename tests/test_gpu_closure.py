@@ -170,3 +170,156 @@ def test_closure_rejects_unsupported_handles(gpu):
     with pytest.raises(WtError):
         s.set_closure(m)
     s.destroy()
+
+
+def _np_samples(oracle, fpop, fflags, fdims, fkp, cdims, ctau0, cflags, csdf, x_lo, x_hi):
+    """numpy restatement of wt_trainer_add_samples (keep = 1) on the interior: pulled populations
+    by shifting (exact away from walls and faces), 2 x 2 x 2 filter, strain, 3 x 3 x 3 projection,
+    features. Returns (cell indices, features, targets) in cell order."""
+    lat = oracle.lattice(3)
+    fx, fy, fz = fdims
+    cx, cy, cz = cdims
+    F = fpop.astype(np.float64).reshape(19, fz, fy, fx)
+    pulled = np.stack([np.roll(F[i], shift=(lat["c"][i][2], lat["c"][i][1], lat["c"][i][0]), axis=(0, 1, 2))
+                       for i in range(19)])
+    c = lat["c"].astype(np.float64)
+    rho = pulled.sum(0)
+    j = np.einsum("ia,izyx->azyx", c, pulled)
+    pa, pb = [0, 1, 2, 0, 0, 1], [0, 1, 2, 1, 2, 2]
+    m = np.stack([np.einsum("i,izyx->zyx", c[:, a] * c[:, b], pulled) for a, b in zip(pa, pb)])
+    u = j / rho
+    pi = np.stack([m[q] - rho * (u[pa[q]] * u[pb[q]] + (1 / 3 if q < 3 else 0)) for q in range(6)])
+    pn = sum((1.0 if q < 3 else 2.0) * pi[q] ** 2 for q in range(6))
+    t0 = float(np.float32(fkp.tau0))
+    k = 18 * np.sqrt(2.0) * float(np.float32(fkp.csmag2))
+    ts = 0.5 * (t0 + np.sqrt(t0 * t0 + k * np.sqrt(pn) / rho))
+    nus = (ts - t0) / 3
+    box = lambda a: a.reshape(cz, 2, cy, 2, cx, 2).sum(axis=(1, 3, 5))
+    srho = box(rho)
+    sj = [box(j[a]) for a in range(3)]
+    uc = [sj[a] / srho for a in range(3)]
+    T = [(box(j[pa[q]] * j[pb[q]] / rho) / srho - uc[pa[q]] * uc[pb[q]] + box(3 * nus * pi[q] / (rho * ts)) / 8)
+         .astype(np.float32) for q in range(6)]
+    rho_c = (srho / 8).astype(np.float32)
+    u32 = [a.astype(np.float32).astype(np.float64) for a in uc]
+    # strain: central differences of u~, then the projection terms
+    g = [[0.5 * (np.roll(u32[a], -1, axis=2 - b) - np.roll(u32[a], 1, axis=2 - b)) for b in range(3)] for a in range(3)]
+    S = [0.5 * (g[pa[q]][pb[q]] + g[pb[q]][pa[q]]) for q in range(6)]
+    Td = [T[q].astype(np.float64) for q in range(6)]
+    tr = (Td[0] + Td[1] + Td[2]) / 3
+    num = -sum((1.0 if q < 3 else 2.0) * (Td[q] - (tr if q < 3 else 0.0)) * S[q] for q in range(6))
+    den = sum(2.0 * (1.0 if q < 3 else 2.0) * S[q] ** 2 for q in range(6))
+    num, den = num.astype(np.float32).astype(np.float64), den.astype(np.float32).astype(np.float64)
+    # stencil validity: the coarse cell and its six neighbours hold no solid fine cell, off the faces
+    fsolid = (fflags.reshape(fz, fy, fx) != 0).reshape(cz, 2, cy, 2, cx, 2).any(axis=(1, 3, 5))
+    okc = ~fsolid
+    for ax in range(3):
+        okc = okc & np.roll(~fsolid, 1, ax) & np.roll(~fsolid, -1, ax)
+    okc[[0, -1], :, :] = okc[:, [0, -1], :] = okc[:, :, [0, -1]] = False
+    num = np.where(okc, num, 0.0)
+    den = np.where(okc, den, -1.0)
+    S32 = [a.astype(np.float32) for a in S]
+    out_idx, out_x, out_y, out_b = [], [], [], []
+    cf = cflags.reshape(cz, cy, cx)
+    sdf = csdf.reshape(cz, cy, cx)
+    for zz in range(2, cz - 2):
+        for yy in range(2, cy - 2):
+            for xx in range(2, cx - 2):
+                if xx < x_lo or xx >= x_hi or cf[zz, yy, xx] or den[zz, yy, xx] < 0:
+                    continue
+                sl = (slice(zz - 1, zz + 2), slice(yy - 1, yy + 2), slice(xx - 1, xx + 2))
+                dm = den[sl] >= 0
+                sn, sd = num[sl][dm].sum(), den[sl][dm].sum()
+                nu = max(sn / sd, 0.0) if sd > 1e-30 else 0.0
+                out_b.append(np.abs(num[sl][dm]).sum() / sd if sd > 1e-30 else 0.0)
+                kk = np.float32(-(2.0 / 3.0) * float(rho_c[zz, yy, xx]) * (float(np.float32(ctau0)) + 3.0 * nu))
+                mom = np.array([kk * S32[q][zz, yy, xx] for q in range(6)] +
+                               [rho_c[zz, yy, xx]] + [np.float32(a[zz, yy, xx]) for a in uc], np.float32)
+                d = sdf[zz, yy, xx]
+                wall = min(float(d), 3.0) if d >= 0 else 3.0
+                out_idx.append(xx + cx * (yy + cy * zz))
+                out_x.append(oracle.closure_features(mom[None, :], np.array([wall], np.float32), ctau0)[0])
+                out_y.append(nu)
+    return np.array(out_idx), np.array(out_x), np.array(out_y), np.array(out_b)
+
+
+def test_training_samples_match_numpy_restatement(gpu, oracle):
+    fdims, cdims = (96, 48, 48), (48, 24, 24)
+    body = CL.seeded_bodies(1, seed=4)[0]
+    ff, _, fs = CL.body_fields(fdims, body)
+    cf, _, cs = CL.body_fields(cdims, body)
+    pf = CL.tunnel_params(body, fdims, precision="f32", re=500.0)
+    pf["init"] = "freestream"
+    pc = dict(pf, nu=pf["nu"] / 2)
+    fine, coarse = Solver(fdims, pf), Solver(cdims, pc)
+    fine.upload_flags(ff)
+    fine.upload_sdf(fs)
+    coarse.upload_flags(cf)
+    coarse.upload_sdf(cs)
+    fine.step(60)
+    t = CL.Trainer(1 << 16)
+    added = t.add_samples(fine, coarse, keep=1.0, seed=9)
+    assert added > 1000
+    xg, yg = t.read_samples()
+    assert np.all(np.isfinite(xg)) and np.all(yg >= 0)
+    ckp = coarse.kparams()
+    idx, xn, yn, bound = _np_samples(oracle, fine.read_populations(), ff, fdims, fine.kparams(), cdims, ckp.tau0, cf, cs,
+                              ckp.sponge_in, min(cdims[0], ckp.sponge_start))
+    assert len(idx) == added  # the same cells are kept, in cell order
+    # compare where the shifted pull is exact: every fine cell of the 5 x 5 x 5 coarse neighbourhood is
+    # at least one cell away from any solid and from the domain faces
+    solid = ff.reshape(fdims[2], fdims[1], fdims[0]).astype(bool)
+    near = solid.copy()
+    for ax in range(3):
+        near |= np.roll(solid, 1, ax) | np.roll(solid, -1, ax)
+    near[[0, -1], :, :] = near[:, [0, -1], :] = near[:, :, [0, -1]] = True
+    cbad = near.reshape(cdims[2], 2, cdims[1], 2, cdims[0], 2).any(axis=(1, 3, 5))
+    bad5 = cbad.copy()
+    for ax in range(3):
+        for s in (1, 2):
+            bad5 |= np.roll(cbad, s, ax) | np.roll(cbad, -s, ax)
+    zz, rem = np.divmod(idx, cdims[0] * cdims[1])
+    yy, xx = np.divmod(rem, cdims[0])
+    ok = ~bad5[zz, yy, xx]
+    assert ok.sum() > 0.5 * len(idx)
+    # the target is a ratio of sums over 27 cells that can cancel: one-ulp f32 differences of the
+    # summands move it by about 1e-7 (sum |num|) / (sum den), the bound used here with a margin
+    err = np.abs(yg[ok] - yn[ok])
+    assert np.all(err <= 1e-5 * bound[ok] + 1e-7 * np.max(np.abs(yn[ok]))), np.max(err / (bound[ok] + 1e-30))
+    assert np.median(err / (np.abs(yn[ok]) + 1e-30)) < 1e-5
+    scale = np.maximum(np.abs(xn[ok]).mean(axis=0), 1e-30)
+    assert np.max(np.abs(xg[ok] - xn[ok]) / scale) < 1e-2
+    # argument checks
+    with pytest.raises(CL.ClosureError):
+        t.add_samples(coarse, fine)
+    t.destroy()
+    fine.destroy()
+    coarse.destroy()
+
+
+def test_trained_network_beats_smagorinsky_a_priori(gpu):
+    """What the trained network gains over the method without it, on a held-out body: the error of
+    its eddy viscosity against the filtered fine run's, next to Smagorinsky's (Cs = 0.1)."""
+    from windtunnel_vis_b200.solver import solver_factory
+
+    fd = (128, 64, 64)
+    tr = CL.Trainer(1 << 21)
+    for b, body in enumerate(CL.seeded_bodies(3, seed=2)):
+        CL.add_body_samples(tr, solver_factory, body, fd, steps=1200, snapshots=2, every=200, keep=1.0, seed=b + 1,
+                            re=400.0)
+    assert tr.count > 50000
+    tr.set_model(CL.normalized_model(tr, seed=1))
+    hist = tr.fit(800, batch=8192, lr=3e-3, seed=3)
+    assert np.mean(hist[-50:]) < np.mean(hist[:50])
+    model = tr.get_model()
+    tr.destroy()
+    ev = CL.Trainer(1 << 20)
+    CL.add_body_samples(ev, solver_factory, CL.seeded_bodies(2, seed=99)[1], fd, steps=1200, keep=1.0, seed=50,
+                        re=400.0)
+    x, y = ev.read_samples()
+    ev.set_model(model)
+    learned = CL.a_priori_metrics(ev.infer(x), y)
+    smag = CL.a_priori_metrics(CL.smagorinsky_nu(x), y)
+    ev.destroy()
+    assert learned["nmse"] < smag["nmse"], (learned, smag)
+    assert learned["nmse"] < 1.0, learned

@@ -255,52 +255,10 @@ def tunnel_params(body, dims, u=0.05, re=2000.0, cs=0.1, precision="f16", seed=1
                 emaAlpha=0, precision=precision, init="rest_noise", initNoise=1e-4, initSeed=seed)
 
 
-def drag_run(make, dims, body, steps, chunk=50, closure=None, measure_from=None, **kw):
-    """One tunnel run of a body: mean C_D (batch-means error bar) over the second half, wall time."""
-    from .analysis import coefficients, window_stats
-
-    flags, frontal, sdf = body_fields(dims, body)
-    p = tunnel_params(body, dims, **kw)
-    s = make(dims, p)
-    s.upload_flags(flags)
-    s.upload_sdf(sdf)
-    if closure is not None:
-        s.set_closure(closure)
-    t0 = time.perf_counter()
-    tt, cd = [], []
-    unstable = False
-    step = 0
-    while step < steps:
-        st = s.step_and_sample(chunk)
-        step += chunk
-        if st["unstable"]:
-            unstable = True
-            break
-        tt.append(st["step"])
-        cd.append(coefficients(st["fx"], st["fy"], st["fz"], p["u"], frontal)["cd"])
-    seconds = time.perf_counter() - t0
-    s.destroy()
-    start = steps // 2 if measure_from is None else measure_from
-    sel = [k for k, t in enumerate(tt) if t >= start]
-    ws = window_stats([tt[k] for k in sel], [cd[k] for k in sel], float(steps)) if len(sel) >= 16 else None
-    return {"cd": ws["mean"] if ws else math.nan, "cd_se": ws["se"] if ws else math.nan, "seconds": seconds,
-            "unstable": unstable, "frontal": frontal, "steps": step, "cells": int(np.prod(dims))}
-
-
 def add_body_samples(trainer, make, body, fine_dims, steps, snapshots=1, every=500, keep=1.0, seed=1, **kw):
     """Runs the fine tunnel of `body` for `steps`, then takes `snapshots` sample sets `every` steps
     apart (filtered onto the half-resolution grid of the same body). Returns samples added."""
-    coarse_dims = tuple(d // 2 for d in fine_dims)
-    ff, _, fs = body_fields(fine_dims, body)
-    cf, _, cs_ = body_fields(coarse_dims, body)
-    fine = make(fine_dims, tunnel_params(body, fine_dims, **kw))
-    fine.upload_flags(ff)
-    fine.upload_sdf(fs)
-    pc = tunnel_params(body, fine_dims, **kw)
-    pc["nu"] = pc["nu"] / 2.0
-    coarse = make(coarse_dims, pc)
-    coarse.upload_flags(cf)
-    coarse.upload_sdf(cs_)
+    fine, coarse, _, _ = _fine_coarse(make, body, fine_dims, seed=seed, **kw)
     added = 0
     fine.step(steps)
     for k in range(snapshots):
@@ -321,6 +279,133 @@ def a_priori_metrics(nu, y):
     mse = float(np.mean((nu - y) ** 2)) if y.size else math.nan
     corr = float(np.corrcoef(nu, y)[0, 1]) if y.size > 1 and np.std(nu) > 0 and np.std(y) > 0 else math.nan
     return {"nmse": mse / var if var > 0 else math.nan, "mse": mse, "corr": corr}
+
+
+def _fine_coarse(make, body, fine_dims, **kw):
+    coarse_dims = tuple(d // 2 for d in fine_dims)
+    ff, f_front, fs = body_fields(fine_dims, body)
+    cf, c_front, cs_ = body_fields(coarse_dims, body)
+    pf = tunnel_params(body, fine_dims, **kw)
+    pc = dict(pf, nu=pf["nu"] / 2.0)
+    fine = make(fine_dims, pf)
+    fine.upload_flags(ff)
+    fine.upload_sdf(fs)
+    coarse = make(coarse_dims, pc)
+    coarse.upload_flags(cf)
+    coarse.upload_sdf(cs_)
+    return fine, coarse, pf, f_front
+
+
+def _cd_series(s, steps, chunk, u, frontal):
+    from .analysis import coefficients
+
+    tt, cd = [], []
+    unstable = False
+    step = 0
+    while step < steps:
+        st = s.step_and_sample(chunk)
+        step += chunk
+        if st["unstable"]:
+            unstable = True
+            break
+        tt.append(st["step"])
+        cd.append(coefficients(st["fx"], st["fy"], st["fz"], u, frontal)["cd"])
+    return tt, cd, unstable
+
+
+def _mean_se(tt, cd, start, horizon):
+    from .analysis import window_stats
+
+    sel = [k for k, t in enumerate(tt) if t >= start]
+    ws = window_stats([tt[k] for k in sel], [cd[k] for k in sel], float(horizon)) if len(sel) >= 16 else None
+    return (ws["mean"], ws["se"]) if ws else (math.nan, math.nan)
+
+
+def study(make=None, fine_dims=(512, 256, 256), train_bodies=8, eval_bodies=2, seed=1, re=1000.0, u=0.05,
+          warm=6000, snapshots=2, every=1000, samples=1 << 24, keep=0.4, train_steps=3000, batch=16384, lr=2e-3,
+          eval_steps=16000, chunk=100, log=print):
+    """The learned-closure experiment. Training data: `train_bodies` seeded bodies run at
+    fine_dims (FP16, Smagorinsky Cs = 0.1, Re on the body height), `snapshots` filtered sample sets
+    each (cells kept with probability `keep`, up to `samples`). Training: Adam on the GPU. Evaluation
+    on `eval_bodies` held-out bodies (other seeds): the fine run's mean C_D over its second half
+    (eval_steps fine steps) against coarse runs over the same physical time (eval_steps / 2 coarse
+    steps) with plain Smagorinsky and with the network, wall times of all three, and the a-priori
+    error of the network and of Smagorinsky against the held-out targets."""
+    from .solver import solver_factory
+
+    make = make or solver_factory
+    out = {"fine_dims": list(fine_dims), "re": re, "u": u, "train_bodies": train_bodies, "eval_bodies": eval_bodies}
+    t_start = time.perf_counter()
+    tr = Trainer(samples)
+    gen_s = 0.0
+    for b, body in enumerate(seeded_bodies(train_bodies, seed=seed)):
+        t0 = time.perf_counter()
+        fine, coarse, _, _ = _fine_coarse(make, body, fine_dims, u=u, re=re, seed=seed + b)
+        fine.step(warm)
+        for k in range(snapshots):
+            if k:
+                fine.step(every)
+            tr.add_samples(fine, coarse, keep=keep, seed=1000 * (seed + b) + k + 1)
+        fine.destroy()
+        coarse.destroy()
+        gen_s += time.perf_counter() - t0
+        log(f"train body {b} ({body['kind']}, aspect {body['aspect']:.2f}): pool {tr.count}")
+    out["samples"] = tr.count
+    out["data_seconds"] = gen_s
+    m0 = normalized_model(tr, seed=seed)
+    tr.set_model(m0)
+    t0 = time.perf_counter()
+    hist = tr.fit(train_steps, batch=batch, lr=lr, seed=seed)
+    out["train_seconds"] = time.perf_counter() - t0
+    out["loss_first"] = float(np.mean(hist[:50]))
+    out["loss_last"] = float(np.mean(hist[-50:]))
+    model = tr.get_model()
+    tr.destroy()
+    log(f"trained: loss {out['loss_first']:.4g} -> {out['loss_last']:.4g} in {out['train_seconds']:.1f} s")
+    ev = Trainer(1 << 22)
+    cases = []
+    for b, body in enumerate(seeded_bodies(eval_bodies, seed=seed + 7919)):
+        fine, coarse, pf, f_front = _fine_coarse(make, body, fine_dims, u=u, re=re, seed=seed + 100 + b)
+        t0 = time.perf_counter()
+        tt, cd, unst = _cd_series(fine, eval_steps, chunk, u, f_front)
+        f_sec = time.perf_counter() - t0
+        f_mean, f_se = _mean_se(tt, cd, eval_steps // 2, eval_steps)
+        n0 = ev.count
+        if not unst:
+            ev.add_samples(fine, coarse, keep=0.25, seed=777 + b)
+        fine.destroy()
+        coarse.destroy()
+        case = {"body": body, "fine": {"cd": f_mean, "cd_se": f_se, "seconds": f_sec, "unstable": unst}}
+        cdims = tuple(d // 2 for d in fine_dims)
+        for name, cl in (("smagorinsky", None), ("learned", model)):
+            cf, c_front, cs_ = body_fields(cdims, body)
+            pc = dict(pf, nu=pf["nu"] / 2.0)
+            s = make(cdims, pc)
+            s.upload_flags(cf)
+            s.upload_sdf(cs_)
+            if cl is not None:
+                s.set_closure(cl)
+            t0 = time.perf_counter()
+            tt, cd, unst_c = _cd_series(s, eval_steps // 2, chunk // 2, u, c_front)
+            sec = time.perf_counter() - t0
+            s.destroy()
+            mean, se = _mean_se(tt, cd, eval_steps // 4, eval_steps // 2)
+            case[name] = {"cd": mean, "cd_se": se, "seconds": sec, "unstable": unst_c,
+                          "cd_err_vs_fine": (mean - f_mean) / f_mean if f_mean == f_mean and f_mean else math.nan,
+                          "speedup_vs_fine": f_sec / sec if sec > 0 else math.nan}
+        if ev.count > n0:
+            x, y = ev.read_samples(n0, ev.count - n0)
+            ev.set_model(model)
+            case["a_priori"] = {"learned": a_priori_metrics(ev.infer(x), y),
+                                "smagorinsky": a_priori_metrics(smagorinsky_nu(x), y), "samples": int(y.size)}
+        cases.append(case)
+        log(f"eval body {b}: fine C_D {f_mean:.4f} ({f_sec:.1f} s), smagorinsky {case['smagorinsky']['cd']:.4f}, "
+            f"learned {case['learned']['cd']:.4f} ({case['learned']['seconds']:.1f} s)")
+    ev.destroy()
+    out["cases"] = cases
+    out["model"] = {k: np.asarray(v).tolist() for k, v in model.items()}
+    out["seconds"] = time.perf_counter() - t_start
+    return out
 
 
 def summarize(d):

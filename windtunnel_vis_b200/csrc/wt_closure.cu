@@ -50,15 +50,15 @@ constexpr int TS_A = 0;          // inputs x', 128 x 16 bf16, K-major (A of laye
 constexpr int TS_H1 = 4096;      // h1, 128 x 32 bf16, K-major (A of layer 2)
 constexpr int TS_DZ2 = 12288;    // dz2, 128 x 32 bf16, K-major (A of the dH1 product)
 constexpr int TS_DZ1 = 20480;    // dz1, [128][32] bf16
-constexpr int TS_H2 = 28672;     // h2, [128][32] bf16
-constexpr int TS_W1 = 36864;     // W1 image (N = 32 hidden, K = 16 inputs)
-constexpr int TS_W2 = 37888;     // W2 image (N = out, K = in)
-constexpr int TS_W2T = 39936;    // W2 transposed image (N = in, K = out)
-constexpr int TS_DZ3 = 41984;    // dz3 [128] f32
-constexpr int TS_LOSS = 42496;   // per-row loss [128] f32
-constexpr int TS_BAR = 43008;    // mbarrier, then the tensor-memory address
-// 48 KB of dynamic shared memory: at most 4 blocks per SM, whose 4 x 128 tensor-memory columns fit
-constexpr int TS_BYTES = 48 * 1024;
+constexpr int TS_H2 = 28672;     // h2, [128][32] f32
+constexpr int TS_W1 = 45056;     // W1 image (N = 32 hidden, K = 16 inputs)
+constexpr int TS_W2 = 46080;     // W2 image (N = out, K = in)
+constexpr int TS_W2T = 48128;    // W2 transposed image (N = in, K = out)
+constexpr int TS_DZ3 = 50176;    // dz3 [128] f32
+constexpr int TS_LOSS = 50688;   // per-row loss [128] f32
+constexpr int TS_BAR = 51200;    // mbarrier, then the tensor-memory address
+// 53 KB of dynamic shared memory: at most 4 blocks per SM, whose 4 x 128 tensor-memory columns fit
+constexpr int TS_BYTES = 53 * 1024;
 static_assert(TS_BAR + 12 <= TS_BYTES, "layout");
 
 // parameter offsets in the master vector
@@ -74,7 +74,7 @@ struct TrainArgs {
   uint64_t seed;      // random mode when nonzero
   uint64_t draw;      // index of this minibatch
   const float* P;
-  float shift[CL_IN], scale[CL_IN], nu_scale;
+  float scale[CL_IN], nshift[CL_IN], nu_scale;  // x' = bf16(fma(x, scale, nshift))
   float* nu_out;      // inference
   float* partials;    // training: [block][TR_NOUT]
 };
@@ -133,8 +133,8 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
 #pragma unroll
     for (int k = 0; k < 8; k++) {
       const int k0 = 2 * k, k1 = 2 * k + 1;
-      const uint32_t lo = (valid && k0 < CL_IN) ? bf16_bits(__fmul_rn(__fsub_rn(x[k0], A.shift[k0]), A.scale[k0])) : 0u;
-      const uint32_t hi = (valid && k1 < CL_IN) ? bf16_bits(__fmul_rn(__fsub_rn(x[k1], A.shift[k1]), A.scale[k1])) : 0u;
+      const uint32_t lo = (valid && k0 < CL_IN) ? bf16_bits(__fmaf_rn(x[k0], A.scale[k0], A.nshift[k0])) : 0u;
+      const uint32_t hi = (valid && k1 < CL_IN) ? bf16_bits(__fmaf_rn(x[k1], A.scale[k1], A.nshift[k1])) : 0u;
       w[k] = lo | (hi << 16);
     }
     *reinterpret_cast<uint4*>(sm + TS_A + umma::kmaj_off(tid, 0, CL_K1)) = make_uint4(w[0], w[1], w[2], w[3]);
@@ -196,14 +196,15 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
 #pragma unroll
     for (int e = 0; e < 8; e++) z2[8 * c + e] = __fadd_rn(v[e], A.P[PO_B2 + 8 * c + e]);
   }
-  float z3 = 0.0f;
+  float ze = 0.0f, zo = 0.0f;
   float h2[CL_H];
 #pragma unroll
   for (int j = 0; j < CL_H; j++) {
-    h2[j] = bf16r(cl_gelu(z2[j]));
-    z3 = __fmaf_rn(h2[j], bf16r(A.P[PO_W3 + j]), z3);
+    h2[j] = cl_gelu(z2[j]);
+    if (j & 1) zo = __fmaf_rn(h2[j], bf16r(A.P[PO_W3 + j]), zo);
+    else ze = __fmaf_rn(h2[j], bf16r(A.P[PO_W3 + j]), ze);
   }
-  z3 = __fadd_rn(z3, A.P[PO_B3]);
+  const float z3 = __fadd_rn(__fadd_rn(ze, zo), A.P[PO_B3]);
   const float nu = __fmul_rn(A.nu_scale, cl_softplus(z3));
   if constexpr (!TRAIN) {
     if (valid) A.nu_out[row] = ok ? nu : __int_as_float(0x7fc00000);
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
     reinterpret_cast<float*>(sm + TS_LOSS)[tid] = d * d;
 #pragma unroll
     for (int c = 0; c < 4; c++) {
-      uint32_t pk[4], ph[4];
+      uint32_t pk[4];
 #pragma unroll
       for (int e = 0; e < 4; e++) {
         const int j = 8 * c + 2 * e;
@@ -224,10 +225,11 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
         const uint32_t lo = bf16_bits(dz3 * bf16r(A.P[PO_W3 + j]) * g0);
         const uint32_t hi = bf16_bits(dz3 * bf16r(A.P[PO_W3 + j + 1]) * g1);
         pk[e] = lo | (hi << 16);
-        ph[e] = (uint32_t)bf16_bits(h2[j]) | ((uint32_t)bf16_bits(h2[j + 1]) << 16);
       }
       *reinterpret_cast<uint4*>(sm + TS_DZ2 + umma::kmaj_off(tid, 8 * c, CL_H)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-      *reinterpret_cast<uint4*>(sm + TS_H2 + (tid * CL_H + 8 * c) * 2) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+      float4* hrow = reinterpret_cast<float4*>(sm + TS_H2 + (tid * CL_H + 8 * c) * 4);
+      hrow[0] = make_float4(h2[8 * c], h2[8 * c + 1], h2[8 * c + 2], h2[8 * c + 3]);
+      hrow[1] = make_float4(h2[8 * c + 4], h2[8 * c + 5], h2[8 * c + 6], h2[8 * c + 7]);
     }
     umma::fence_before_sync();
     umma::fence_async_smem();
@@ -283,7 +285,8 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
       } else if (p < PO_B3) {
         const int j = p - PO_W3;
         const float* dz = reinterpret_cast<const float*>(sm + TS_DZ3);
-        for (int r = 0; r < TR_THREADS; r++) acc = __fmaf_rn(dz[r], sm_bf16(sm + TS_H2, (r * CL_H + j) * 2), acc);
+        const float* h2s = reinterpret_cast<const float*>(sm + TS_H2);
+        for (int r = 0; r < TR_THREADS; r++) acc = __fmaf_rn(dz[r], h2s[r * CL_H + j], acc);
       } else if (p == PO_B3) {
         const float* dz = reinterpret_cast<const float*>(sm + TS_DZ3);
         for (int r = 0; r < TR_THREADS; r++) acc = __fadd_rn(acc, dz[r]);
@@ -523,6 +526,13 @@ int ensure_partials(wt_trainer* t, int64_t blocks) {
   return WT_OK;
 }
 
+// k_train's dynamic shared memory exceeds the 48 KB default: opt in (on the current device)
+cudaError_t train_smem_optin() {
+  cudaError_t r = cudaFuncSetAttribute(k_train<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TS_BYTES);
+  if (r == cudaSuccess) r = cudaFuncSetAttribute(k_train<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TS_BYTES);
+  return r;
+}
+
 TrainArgs make_args(const wt_trainer* t) {
   TrainArgs A;
   std::memset(&A, 0, sizeof A);
@@ -531,8 +541,8 @@ TrainArgs make_args(const wt_trainer* t) {
   A.count = t->count;
   A.P = t->P;
   for (int k = 0; k < CL_IN; k++) {
-    A.shift[k] = t->shift[k];
     A.scale[k] = t->scale[k];
+    A.nshift[k] = -(t->shift[k] * t->scale[k]);
   }
   A.nu_scale = t->nu_scale;
   return A;
@@ -557,6 +567,7 @@ int wt_trainer_create(int32_t device, int64_t capacity, wt_trainer** out) {
   t->cap = capacity;
   TrDevice g(device);
   bool okk = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking) == cudaSuccess;
+  okk = okk && train_smem_optin() == cudaSuccess;
   okk = okk && cudaMalloc((void**)&t->P, CL_NPARAM * sizeof(float)) == cudaSuccess;
   okk = okk && cudaMalloc((void**)&t->m, CL_NPARAM * sizeof(float)) == cudaSuccess;
   okk = okk && cudaMalloc((void**)&t->v, CL_NPARAM * sizeof(float)) == cudaSuccess;

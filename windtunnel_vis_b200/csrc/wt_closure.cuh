@@ -3,14 +3,16 @@
 // copy of a network.
 //
 // The network (10 -> 32 -> 32 -> 1) and its numerics:
-//   x'  = bf16((x - shift) * scale)                     features, padded to 16 with zeros
-//   z1  = x' W1 + b1,  h1 = bf16(gelu(z1))              W1 rounded to bf16, f32 accumulation
-//   z2  = h1 W2 + b2,  h2 = bf16(gelu(z2))
-//   z3  = h2 . w3 + b3,  nu_t = nu_scale * softplus(z3)
-//   gelu(x) = x/2 (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))   (tanh form; tanh.approx.f32)
+//   x'  = bf16(fma(x, scale, nshift)),  nshift = -shift * scale (f32)      inputs, padded to 16
+//   z1  = x' W1 + b1,  h1 = bf16(gelu(z1))                                 W1 rounded to bf16
+//   z2  = h1 W2 + b2,  h2 = gelu(z2) (f32: it feeds only the CUDA-core      f32 accumulation
+//                                     output layer)
+//   z3  = (sum_even h2_j w3_j + sum_odd h2_j w3_j) + b3,  nu_t = nu_scale * softplus(z3)
+//   gelu(x) = x * (1/2 + tanh(u) / 2),  u = x (C0 + C1 x^2),  C0 = sqrt(2/pi), C1 = 0.044715 C0
+//             (the tanh form of gelu; tanh.approx.f32)
 // The two 32-wide layers run on tcgen05 tensor cores in the bulk kernel and the trainer; face and
 // wall cells evaluate the same network on CUDA cores (closure_nu). Both use the identical gelu,
-// bias and rounding steps; they differ only in the order of the f32 accumulations.
+// bias and rounding steps; they differ only in the order of the f32 accumulations of z1 and z2.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -26,6 +28,20 @@ constexpr int CL_IN = WT_CLOSURE_IN;    // 10 features
 constexpr int CL_K1 = 16;               // layer-1 K, padded for the K = 16 MMA step
 constexpr int CL_H = WT_CLOSURE_HID;    // 32 hidden units
 constexpr int CL_NPARAM = CL_IN * CL_H + CL_H + CL_H * CL_H + CL_H + CL_H + 1;  // 1441 trainable values
+constexpr float GELU_C0 = 0.7978845608028654f;
+constexpr float GELU_C1 = 0.035677408136300125f;
+constexpr float GELU_C1x3 = 0.10703222440890037f;
+
+// The small per-network values: biases, the bf16-rounded output weights, the input normalisation
+// as fma(x, scale, nshift). The bulk kernel takes them by value (constant bank).
+struct ClosureParams {
+  float b1[CL_H];
+  float b2[CL_H];
+  float w3[CL_H];
+  float b3, nu_scale;
+  float scale[CL_IN];
+  float nshift[CL_IN];
+};
 
 // Device copy of a network. Images are the tcgen05 B operands (N x K, K-major, no swizzle):
 // w1img[n = hidden j][k = input], w2img[n = out j][k = in i] (forward), w2timg[n = in i][k = out j]
@@ -37,13 +53,7 @@ struct __align__(128) ClosureDev {
   uint16_t w2timg[CL_H * CL_H];
   float w1[CL_IN][CL_H];
   float w2[CL_H][CL_H];
-  float w3[CL_H];
-  float b1[CL_H];
-  float b2[CL_H];
-  float b3;
-  float nu_scale;
-  float shift[CL_IN];
-  float scale[CL_IN];
+  ClosureParams p;  // the by-value part, for the CUDA-core path
 };
 
 // bf16 round to nearest even (finite inputs), as a float and as raw bits
@@ -69,6 +79,15 @@ __host__ __device__ __forceinline__ float bf16_val(uint16_t b) {
 }
 __host__ __device__ __forceinline__ float bf16r(float v) { return bf16_val(bf16_bits(v)); }
 
+// two floats -> bf16x2 bits (lo = a), one cvt.rn.bf16x2.f32
+__device__ __forceinline__ uint32_t bf16x2_bits(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+__device__ __forceinline__ float2 bf16x2_vals(uint32_t w) {
+  return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xFFFF0000u));
+}
+
 __device__ __forceinline__ float tanh_fast(float x) {
   float r;
   asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
@@ -77,23 +96,33 @@ __device__ __forceinline__ float tanh_fast(float x) {
 
 // gelu, tanh form; explicit roundings so every kernel evaluates it identically
 __device__ __forceinline__ float cl_gelu(float x) {
-  const float inner = __fmaf_rn(__fmul_rn(0.044715f, __fmul_rn(x, x)), x, x);
-  const float t = tanh_fast(__fmul_rn(0.7978845608028654f, inner));
-  const float hx = __fmul_rn(0.5f, x);
-  return __fmaf_rn(hx, t, hx);
+  const float u = __fmul_rn(x, __fmaf_rn(GELU_C1, __fmul_rn(x, x), GELU_C0));
+  return __fmul_rn(x, __fmaf_rn(0.5f, tanh_fast(u), 0.5f));
 }
-// gelu and its derivative
+// the same on two lanes with f32x2 instructions (identical per-lane roundings)
+__device__ __forceinline__ float2 cl_gelu2(float2 x) {
+  const float2 u = __fmul2_rn(x, __ffma2_rn(make_float2(GELU_C1, GELU_C1), __fmul2_rn(x, x),
+                                            make_float2(GELU_C0, GELU_C0)));
+  const float2 t = make_float2(tanh_fast(u.x), tanh_fast(u.y));
+  return __fmul2_rn(x, __ffma2_rn(make_float2(0.5f, 0.5f), t, make_float2(0.5f, 0.5f)));
+}
+// gelu and its derivative d = q + (x/2)(1 - t^2)(C0 + 3 C1 x^2), q = 1/2 + t/2
 __device__ __forceinline__ float cl_gelu_d(float x, float& d) {
   const float x2 = __fmul_rn(x, x);
-  const float inner = __fmaf_rn(__fmul_rn(0.044715f, x2), x, x);
-  const float t = tanh_fast(__fmul_rn(0.7978845608028654f, inner));
-  const float hx = __fmul_rn(0.5f, x);
-  const float du = __fmul_rn(0.7978845608028654f, __fmaf_rn(0.134145f, x2, 1.0f));
-  d = __fmaf_rn(__fmul_rn(hx, __fmaf_rn(-t, t, 1.0f)), du, __fmul_rn(0.5f, __fadd_rn(1.0f, t)));
-  return __fmaf_rn(hx, t, hx);
+  const float t = tanh_fast(__fmul_rn(x, __fmaf_rn(GELU_C1, x2, GELU_C0)));
+  const float q = __fmaf_rn(0.5f, t, 0.5f);
+  const float du = __fmaf_rn(GELU_C1x3, x2, GELU_C0);
+  d = __fmaf_rn(__fmul_rn(__fmul_rn(0.5f, x), __fmaf_rn(-t, t, 1.0f)), du, q);
+  return __fmul_rn(x, q);
 }
 __device__ __forceinline__ float cl_softplus(float z) { return z > 20.0f ? z : log1pf(expf(z)); }
 __device__ __forceinline__ float cl_sigmoid(float z) { return 1.0f / (1.0f + expf(-z)); }
+
+__device__ __forceinline__ float cl_sqrt(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 
 // wall-distance feature from the sdf word of a cell (~bits(d), 0 = unknown)
 __device__ __forceinline__ float cl_wall_dist(uint32_t s) {
@@ -104,55 +133,71 @@ __device__ __forceinline__ float cl_wall_dist(uint32_t s) {
 // velocity, the handle's molecular tau0 and the wall distance. |S| is the strain rate the
 // Smagorinsky relation assigns to |Pi| at Cs = WT_CLOSURE_FEATURE_CS:
 //   tau_s = (tau0 + sqrt(tau0^2 + 18 sqrt(2) Cs^2 |Pi| / rho)) / 2,  |S| = 3 |Pi| / (sqrt(2) rho tau_s)
+// (approximate square roots and quotients: the features are network inputs, not conserved
+// quantities)
 __device__ __forceinline__ void cl_features(float pxx, float pyy, float pzz, float pxy, float pxz, float pyz,
                                             float rho, float ux, float uy, float uz, float tau0, float wall_d,
                                             float (&x)[CL_IN]) {
   float pn = __fmaf_rn(pxx, pxx, __fmaf_rn(pyy, pyy, __fmul_rn(pzz, pzz)));
   pn = __fmaf_rn(2.0f, __fmaf_rn(pxy, pxy, __fmaf_rn(pxz, pxz, __fmul_rn(pyz, pyz))), pn);
-  const float piN = __fsqrt_rn(pn);
+  const float piN = cl_sqrt(pn);
   const float k = (float)(18.0 * 1.4142135623730951) * (WT_CLOSURE_FEATURE_CS * WT_CLOSURE_FEATURE_CS);
-  const float ts = __fmul_rn(0.5f, __fadd_rn(tau0, __fsqrt_rn(__fmaf_rn(tau0, tau0, __fdiv_rn(__fmul_rn(k, piN), rho)))));
+  const float ts = 0.5f * (tau0 + cl_sqrt(__fmaf_rn(tau0, tau0, __fdividef(k * piN, rho))));
   x[0] = pxx;
   x[1] = pyy;
   x[2] = pzz;
   x[3] = pxy;
   x[4] = pxz;
   x[5] = pyz;
-  x[6] = __fdiv_rn(__fmul_rn(2.1213203435596424f, piN), __fmul_rn(rho, ts));
+  x[6] = __fdividef(2.1213203435596424f * piN, rho * ts);
   x[7] = wall_d;
   x[8] = rho;
-  x[9] = __fsqrt_rn(__fmaf_rn(ux, ux, __fmaf_rn(uy, uy, __fmul_rn(uz, uz))));
-}
-
-// normalised, bf16-rounded network input k
-__device__ __forceinline__ float cl_input(const ClosureDev& C, const float (&x)[CL_IN], int k) {
-  return bf16r(__fmul_rn(__fsub_rn(x[k], C.shift[k]), C.scale[k]));
+  x[9] = cl_sqrt(__fmaf_rn(ux, ux, __fmaf_rn(uy, uy, __fmul_rn(uz, uz))));
 }
 
 // the whole network on CUDA cores (face and wall cells): nu_t of one cell
-static __device__ __noinline__ float closure_nu(const ClosureDev* __restrict__ C, const float* __restrict__ xin) {
+static __device__ __noinline__ float closure_nu(const ClosureDev* __restrict__ C, const ClosureParams& P,
+                                               const float* __restrict__ xin) {
   float x[CL_IN];
 #pragma unroll
-  for (int k = 0; k < CL_IN; k++) x[k] = bf16r(__fmul_rn(__fsub_rn(xin[k], C->shift[k]), C->scale[k]));
+  for (int k = 0; k < CL_IN; k++) x[k] = bf16r(__fmaf_rn(xin[k], P.scale[k], P.nshift[k]));
   float h1[CL_H];
 #pragma unroll 4
   for (int j = 0; j < CL_H; j++) {
     float a = 0.0f;
 #pragma unroll
     for (int k = 0; k < CL_IN; k++) a = __fmaf_rn(x[k], C->w1[k][j], a);
-    h1[j] = bf16r(cl_gelu(__fadd_rn(a, C->b1[j])));
+    h1[j] = bf16r(cl_gelu(__fadd_rn(a, P.b1[j])));
   }
-  float z3 = 0.0f;
+  float ze = 0.0f, zo = 0.0f;
 #pragma unroll 2
   for (int j = 0; j < CL_H; j++) {
     float a = 0.0f;
 #pragma unroll
     for (int i = 0; i < CL_H; i++) a = __fmaf_rn(h1[i], C->w2[i][j], a);
-    z3 = __fmaf_rn(bf16r(cl_gelu(__fadd_rn(a, C->b2[j]))), C->w3[j], z3);
+    const float h2 = cl_gelu(__fadd_rn(a, P.b2[j]));
+    if (j & 1) zo = __fmaf_rn(h2, P.w3[j], zo);
+    else ze = __fmaf_rn(h2, P.w3[j], ze);
   }
-  return __fmul_rn(C->nu_scale, cl_softplus(__fadd_rn(z3, C->b3)));
+  return __fmul_rn(P.nu_scale, cl_softplus(__fadd_rn(__fadd_rn(ze, zo), P.b3)));
 }
 
+// the by-value part of a network
+__host__ __device__ inline ClosureParams closure_params(const wt_closure& c) {
+  ClosureParams p;
+  for (int j = 0; j < CL_H; j++) {
+    p.b1[j] = c.b1[j];
+    p.b2[j] = c.b2[j];
+    p.w3[j] = bf16r(c.w3[j]);
+  }
+  p.b3 = c.b3;
+  p.nu_scale = c.nu_scale;
+  for (int k = 0; k < CL_IN; k++) {
+    p.scale[k] = c.scale[k];
+    p.nshift[k] = -(c.shift[k] * c.scale[k]);
+  }
+  return p;
+}
 
 // fills the bf16 images and rounded f32 copies of `c` into `d` (host or device)
 __host__ __device__ inline void closure_pack(const wt_closure& c, ClosureDev& d) {
@@ -170,17 +215,7 @@ __host__ __device__ inline void closure_pack(const wt_closure& c, ClosureDev& d)
     }
   for (int k = 0; k < CL_IN; k++)
     for (int j = 0; j < CL_H; j++) d.w1[k][j] = bf16r(c.w1[k][j]);
-  for (int j = 0; j < CL_H; j++) {
-    d.w3[j] = bf16r(c.w3[j]);
-    d.b1[j] = c.b1[j];
-    d.b2[j] = c.b2[j];
-  }
-  d.b3 = c.b3;
-  d.nu_scale = c.nu_scale;
-  for (int k = 0; k < CL_IN; k++) {
-    d.shift[k] = c.shift[k];
-    d.scale[k] = c.scale[k];
-  }
+  d.p = closure_params(c);
 }
 
 }  // namespace wt

@@ -7,11 +7,8 @@
 #include <string>
 
 #include "../../include/wt.h"
+#include "wt_closure.cuh"
 #include "wt_common.cuh"
-
-namespace wt {
-struct ClosureDev;
-}
 
 struct wt_solver {
   int device = 0;
@@ -94,6 +91,8 @@ struct wt_solver {
   bool launch_explicit = false;
   // learned closure (wt_set_closure): device copy of the network, nullptr = Smagorinsky
   wt::ClosureDev* closure_dev = nullptr;
+  wt::ClosureParams closure_params{};  // by-value part, baked into the bulk kernel's launches
+  uint32_t* lc_tiles = nullptr;        // tile counter of the persistent closure kernel
   wt_closure closure_host{};
   int* err_dev = nullptr;   // device-side error word written by kernels with bounded waits
   int* err_host = nullptr;  // pinned copy

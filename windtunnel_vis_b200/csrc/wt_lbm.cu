@@ -219,7 +219,7 @@ __device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L
     if (cw != nullptr) {
       float x[CL_IN];
       cl_features(pxx, pyy, pzz, pxy, pxz, pyz, rho, ux, uy, uz, P.tau0, wall_d, x);
-      tau = t0 + 3.0f * closure_nu(cw, x);
+      tau = t0 + 3.0f * closure_nu(cw, cw->p, x);
     } else {
       tau = (R)0.5 * (t0 + sqrt(t0 * t0 + (R)(18.0 * 1.4142135623730951) * (R)P.csmag2 * piN * irho));
     }
@@ -859,8 +859,8 @@ __device__ __forceinline__ void collide_shifted2_lc(const wt_kparams& P, const f
                                           wd.x, xa);
                               cl_features(pxx.y, pyy.y, pzz.y, pxy.y, pxz.y, pyz.y, rho.y, ux.y, uy.y, uz.y, P.tau0,
                                           wd.y, xb);
-                              const float ta = tau0_eff(P, (float)x, t_floor) + 3.0f * closure_nu(cw, xa);
-                              const float tb = tau0_eff(P, (float)(x + 1), t_floor) + 3.0f * closure_nu(cw, xb);
+                              const float ta = tau0_eff(P, (float)x, t_floor) + 3.0f * closure_nu(cw, cw->p, xa);
+                              const float tb = tau0_eff(P, (float)(x + 1), t_floor) + 3.0f * closure_nu(cw, cw->p, xb);
                               return make_float2(1.0f - __fdividef(1.0f, ta), 1.0f - __fdividef(1.0f, tb));
                             });
 }
@@ -1169,29 +1169,28 @@ constexpr int LC_SMEM_A = 0;       // 2 tiles x 128 x 16 bf16
 constexpr int LC_SMEM_H = 8192;    // 2 tiles x 128 x 32 bf16
 constexpr int LC_SMEM_W1 = 24576;  // W1 image, 32 x 16 bf16 (followed by the W2 image: one 3 KB copy)
 constexpr int LC_SMEM_W2 = 25600;  // W2 image, 32 x 32 bf16
-constexpr int LC_SMEM_BAR = 27648; // mbarrier (8 B), then the tensor-memory address (4 B)
+constexpr int LC_SMEM_BAR = 27648; // mbarrier (8 B), tensor-memory address (4 B), current tile (4 B)
 // dynamic shared memory per block: more than 228 KB / 8, so at most 7 blocks share an SM and their
 // 7 x 64 tensor-memory columns fit in the SM's 512 (an allocation never has to wait)
 constexpr int LC_SMEM_BYTES = 29 * 1024;
 constexpr uint32_t LC_WAIT_LIMIT = 1u << 22;
-static_assert(LC_SMEM_BAR + 12 <= LC_SMEM_BYTES, "shared-memory layout");
+static_assert(LC_SMEM_BAR + 16 <= LC_SMEM_BYTES, "shared-memory layout");
 static_assert(offsetof(ClosureDev, w2img) == offsetof(ClosureDev, w1img) + 1024, "weight images are contiguous");
 
 // row r of a 128 x 16 A tile: the normalised, bf16-rounded features (10) and zero padding
 __device__ __forceinline__ void lc_write_inputs(uint8_t* tile, uint32_t r, const float (&x)[CL_IN],
-                                                const ClosureDev* __restrict__ cw) {
-  uint32_t w[8];
+                                                const ClosureParams& CP) {
+  uint32_t w[5];
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    const int k0 = 2 * k, k1 = 2 * k + 1;
-    const uint32_t lo = k0 < CL_IN ? bf16_bits(__fmul_rn(__fsub_rn(x[k0], cw->shift[k0]), cw->scale[k0])) : 0u;
-    const uint32_t hi = k1 < CL_IN ? bf16_bits(__fmul_rn(__fsub_rn(x[k1], cw->shift[k1]), cw->scale[k1])) : 0u;
-    w[k] = lo | (hi << 16);
-  }
+  for (int k = 0; k < 5; k++)
+    w[k] = bf16x2_bits(__fmaf_rn(x[2 * k], CP.scale[2 * k], CP.nshift[2 * k]),
+                       __fmaf_rn(x[2 * k + 1], CP.scale[2 * k + 1], CP.nshift[2 * k + 1]));
   *reinterpret_cast<uint4*>(tile + umma::kmaj_off(r, 0, CL_K1)) = make_uint4(w[0], w[1], w[2], w[3]);
-  *reinterpret_cast<uint4*>(tile + umma::kmaj_off(r, 8, CL_K1)) = make_uint4(w[4], w[5], w[6], w[7]);
+  *reinterpret_cast<uint4*>(tile + umma::kmaj_off(r, 8, CL_K1)) = make_uint4(w[4], 0u, 0u, 0u);
 }
 
+// Persistent: each block allocates its tensor memory and stages the weight images once, then takes
+// tiles (tpr cells pairs x 128 / tpr rows) from `tiles_next` until `ntiles` are done.
 template <class S, bool BGK>
 __global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_constant__ wt_kparams P,
                                                                    const typename S::T* __restrict__ fin,
@@ -1199,51 +1198,27 @@ __global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_c
                                                                    const uint8_t* __restrict__ cls, int gs,
                                                                    const uint32_t* __restrict__ sdf,
                                                                    const ClosureDev* __restrict__ cw,
+                                                                   const __grid_constant__ ClosureParams CP,
+                                                                   uint32_t* __restrict__ tiles_next, int tpr,
                                                                    int* __restrict__ err) {
   typedef D3Q19 L;
   typedef PairIO<S> IO;
   constexpr int Q = L::Q;
   extern __shared__ __align__(128) uint8_t lc_smem[];
   const int NX = P.nx, NY = P.ny, NZ = P.nz;
-  const uint32_t tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const uint32_t tid = threadIdx.x;
   const uint32_t warp = tid >> 5;
-  const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 2;
-  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
-  const int iz = blockIdx.z;
-  const bool inside = x0 < NX && iy > 0 && iy < NY - 1 && iz > 0 && iz < NZ - 1;
+  const int rpb = LC_THREADS / tpr;
+  const int tx = (int)tid % tpr, ty = (int)tid / tpr;
+  const int tiles_x = (NX / 2 + tpr - 1) / tpr, tiles_y = (NY + rpb - 1) / rpb;
+  const uint32_t ntiles = (uint32_t)tiles_x * (uint32_t)tiles_y * (uint32_t)NZ;
   const uint32_t N = P.n;
   const uint32_t sy = (uint32_t)NX, sz = (uint32_t)NX * (uint32_t)NY;
-  const uint32_t idx0 = inside ? (uint32_t)x0 + sy * (uint32_t)iy + sz * (uint32_t)iz : 0u;
-  // phase 1: the loads of the two cells in flight (as k_stream_collide_v), then the block set-up
-  uint32_t cv = 0x01010101u;
-  typename IO::pair_t rp[Q];
-  typename IO::one_t r1[Q];
-  uint2 sw = make_uint2(0u, 0u);
-  if (inside) {
-    if (gs == 4) cv = __ldg(reinterpret_cast<const unsigned int*>(cls + (idx0 & ~3u)));
-    else cv = __ldg(reinterpret_cast<const unsigned short*>(cls + idx0));
-    const bool last = x0 + 2 >= NX;
-    const typename S::T* fb = fin + idx0;
-    static_for<Q>([&](auto I) {
-      constexpr int i = I;
-      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
-      const typename S::T* ps = fb + ((ptrdiff_t)i * N - (ptrdiff_t)cy * sy - (ptrdiff_t)cz * sz);
-      rp[i] = IO::ld(ps, 0u);
-      if constexpr (cx > 0) r1[i] = IO::ld1(x0 > 0 ? ps - 1 : ps, 0u);
-      if constexpr (cx < 0) r1[i] = IO::ld1(ps + (last ? 1 : 2), 0u);
-    });
-    sw = __ldg(reinterpret_cast<const uint2*>(sdf + idx0));
-  } else {
-    static_for<Q>([&](auto I) {
-      constexpr int i = I;
-      rp[i] = typename IO::pair_t{};
-      r1[i] = typename IO::one_t{};
-    });
-  }
   uint8_t* const sA = lc_smem + LC_SMEM_A;
   uint8_t* const sH = lc_smem + LC_SMEM_H;
   uint64_t* const mbar = reinterpret_cast<uint64_t*>(lc_smem + LC_SMEM_BAR);
   uint32_t* const tslot = reinterpret_cast<uint32_t*>(lc_smem + LC_SMEM_BAR + 8);
+  uint32_t* const stile = reinterpret_cast<uint32_t*>(lc_smem + LC_SMEM_BAR + 12);
   {
     const uint4* src = reinterpret_cast<const uint4*>(cw->w1img);
     uint4* dst = reinterpret_cast<uint4*>(lc_smem + LC_SMEM_W1);
@@ -1255,124 +1230,165 @@ __global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_c
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tmem = *tslot;
-  // phase 2: pulled populations (rest state outside), the network, collision, stores
-  float2 h[Q];
-  static_for<Q>([&](auto I) {
-    constexpr int i = I;
-    constexpr int cx = L::c[i][0];
-    constexpr float w = (float)Wc<L, i>::v;
-    const float2 cur = IO::cvt(rp[i], w);
-    float2 v;
-    if constexpr (cx == 0) v = cur;
-    else if constexpr (cx > 0) v = make_float2(IO::cvt1(r1[i], w), cur.x);
-    else v = make_float2(cur.y, IO::cvt1(r1[i], w));
-    h[i] = inside ? v : f2(0.0f);
-  });
-  if (inside && x0 == 0) {
-    const float U = P.uin;
+  bool ok = true;
+  for (;;) {
+    // next tile; the barrier also closes the previous tile (its tensor-memory reads are fenced)
+    if (tid == 0) *stile = atomicAdd(tiles_next, 1u);
+    umma::fence_before_sync();
+    __syncthreads();
+    const uint32_t tile = *stile;
+    if (tile >= ntiles) break;
+    const int bx = (int)(tile % (uint32_t)tiles_x);
+    const int by = (int)((tile / (uint32_t)tiles_x) % (uint32_t)tiles_y);
+    const int iz = (int)(tile / ((uint32_t)tiles_x * (uint32_t)tiles_y));
+    const int x0 = (bx * tpr + tx) * 2;
+    const int iy = by * rpb + ty;
+    const bool inside = x0 < NX && iy > 0 && iy < NY - 1 && iz > 0 && iz < NZ - 1;
+    const uint32_t idx0 = inside ? (uint32_t)x0 + sy * (uint32_t)iy + sz * (uint32_t)iz : 0u;
+    // the loads of the two cells in flight (as k_stream_collide_v)
+    uint32_t cv = 0x01010101u;
+    typename IO::pair_t rp[Q];
+    typename IO::one_t r1[Q];
+    uint2 sw = make_uint2(0u, 0u);
+    if (inside) {
+      if (gs == 4) cv = __ldg(reinterpret_cast<const unsigned int*>(cls + (idx0 & ~3u)));
+      else cv = __ldg(reinterpret_cast<const unsigned short*>(cls + idx0));
+      const bool last = x0 + 2 >= NX;
+      const typename S::T* fb = fin + idx0;
+      static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+        const typename S::T* ps = fb + ((ptrdiff_t)i * N - (ptrdiff_t)cy * sy - (ptrdiff_t)cz * sz);
+        rp[i] = IO::ld(ps, 0u);
+        if constexpr (cx > 0) r1[i] = IO::ld1(x0 > 0 ? ps - 1 : ps, 0u);
+        if constexpr (cx < 0) r1[i] = IO::ld1(ps + (last ? 1 : 2), 0u);
+      });
+      sw = __ldg(reinterpret_cast<const uint2*>(sdf + idx0));
+    } else {
+      static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        rp[i] = typename IO::pair_t{};
+        r1[i] = typename IO::one_t{};
+      });
+    }
+    // pulled populations (rest state outside), the network, collision, stores
+    float2 h[Q];
     static_for<Q>([&](auto I) {
       constexpr int i = I;
       constexpr int cx = L::c[i][0];
-      if constexpr (cx > 0) {
-        constexpr float w = (float)Wc<L, i>::v;
-        h[i].x = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
-      }
+      constexpr float w = (float)Wc<L, i>::v;
+      const float2 cur = IO::cvt(rp[i], w);
+      float2 v;
+      if constexpr (cx == 0) v = cur;
+      else if constexpr (cx > 0) v = make_float2(IO::cvt1(r1[i], w), cur.x);
+      else v = make_float2(cur.y, IO::cvt1(r1[i], w));
+      h[i] = inside ? v : f2(0.0f);
     });
-  }
-  const float2 wd = make_float2(cl_wall_dist(sw.x), cl_wall_dist(sw.y));
-  const bool store = inside && (cv & 0x03030303u) == 0u;
-  bool ok = true;
-  typename S::T* ob = fout + idx0;
-  collide_shifted2x<L, BGK>(
-      P, h, x0,
-      [&](auto I, float2 v) {
-        constexpr int i = decltype(I)::value;
-        if (store && ok) IO::st(ob + (ptrdiff_t)i * N, 0u, v, (float)Wc<L, i>::v);
-      },
-      [&](float2 rho, float2, float2 ux, float2 uy, float2 uz, float2 pxx, float2 pyy, float2 pzz, float2 pxy,
-          float2 pxz, float2 pyz) {
-        {
-          float xa[CL_IN], xb[CL_IN];
-          cl_features(pxx.x, pyy.x, pzz.x, pxy.x, pxz.x, pyz.x, rho.x, ux.x, uy.x, uz.x, P.tau0, wd.x, xa);
-          cl_features(pxx.y, pyy.y, pzz.y, pxy.y, pxz.y, pyz.y, rho.y, ux.y, uy.y, uz.y, P.tau0, wd.y, xb);
-          lc_write_inputs(sA, tid, xa, cw);
-          lc_write_inputs(sA + 4096, tid, xb, cw);
+    if (inside && x0 == 0) {
+      const float U = P.uin;
+      static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        constexpr int cx = L::c[i][0];
+        if constexpr (cx > 0) {
+          constexpr float w = (float)Wc<L, i>::v;
+          h[i].x = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
         }
-        constexpr uint32_t ID = umma::idesc_bf16<128, CL_H>();
-        umma::fence_async_smem();
-        __syncthreads();
-        if (tid == 0) {
-          umma::fence_after_sync();
-          const uint64_t bw1 = umma::sdesc(umma::smem_u32(lc_smem + LC_SMEM_W1), 128, 256);
-          umma::mma_bf16(tmem, umma::sdesc(umma::smem_u32(sA), 128, 256), bw1, ID, false);
-          umma::mma_bf16(tmem + 32, umma::sdesc(umma::smem_u32(sA + 4096), 128, 256), bw1, ID, false);
-          umma::commit(mbar);
-        }
-        ok = umma::mbar_wait(mbar, 0, LC_WAIT_LIMIT);
-        umma::fence_after_sync();
-        // hidden layer 1: bias, gelu, bf16 -> row tid of the hidden tiles
-#pragma unroll
-        for (int t = 0; t < 2; t++) {
-          float v[4][8];
-#pragma unroll
-          for (int c = 0; c < 4; c++) umma::tmem_ld8(umma::tmem_lane_addr(tmem, warp, 32 * t + 8 * c), v[c]);
-          umma::tmem_wait_ld();
-#pragma unroll
-          for (int c = 0; c < 4; c++) {
-            uint32_t pk[4];
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-              const int j = 8 * c + 2 * e;
-              const uint32_t lo = bf16_bits(cl_gelu(__fadd_rn(v[c][2 * e], cw->b1[j])));
-              const uint32_t hi = bf16_bits(cl_gelu(__fadd_rn(v[c][2 * e + 1], cw->b1[j + 1])));
-              pk[e] = lo | (hi << 16);
-            }
-            *reinterpret_cast<uint4*>(sH + 8192 * t + umma::kmaj_off(tid, 8 * c, CL_H)) =
-                make_uint4(pk[0], pk[1], pk[2], pk[3]);
+      });
+    }
+    const float2 wd = make_float2(cl_wall_dist(sw.x), cl_wall_dist(sw.y));
+    const bool store = inside && (cv & 0x03030303u) == 0u;
+    typename S::T* ob = fout + idx0;
+    collide_shifted2x<L, BGK>(
+        P, h, x0,
+        [&](auto I, float2 v) {
+          constexpr int i = decltype(I)::value;
+          if (store && ok) IO::st(ob + (ptrdiff_t)i * N, 0u, v, (float)Wc<L, i>::v);
+        },
+        [&](float2 rho, float2, float2 ux, float2 uy, float2 uz, float2 pxx, float2 pyy, float2 pzz, float2 pxy,
+            float2 pxz, float2 pyz) {
+          {
+            float xa[CL_IN], xb[CL_IN];
+            cl_features(pxx.x, pyy.x, pzz.x, pxy.x, pxz.x, pyz.x, rho.x, ux.x, uy.x, uz.x, P.tau0, wd.x, xa);
+            cl_features(pxx.y, pyy.y, pzz.y, pxy.y, pxz.y, pyz.y, rho.y, ux.y, uy.y, uz.y, P.tau0, wd.y, xb);
+            lc_write_inputs(sA, tid, xa, CP);
+            lc_write_inputs(sA + 4096, tid, xb, CP);
           }
-        }
-        umma::fence_before_sync();
-        umma::fence_async_smem();
-        __syncthreads();
-        if (tid == 0) {
+          constexpr uint32_t ID = umma::idesc_bf16<128, CL_H>();
+          umma::fence_async_smem();
+          __syncthreads();
+          if (tid == 0) {
+            umma::fence_after_sync();
+            const uint64_t bw1 = umma::sdesc(umma::smem_u32(lc_smem + LC_SMEM_W1), 128, 256);
+            umma::mma_bf16(tmem, umma::sdesc(umma::smem_u32(sA), 128, 256), bw1, ID, false);
+            umma::mma_bf16(tmem + 32, umma::sdesc(umma::smem_u32(sA + 4096), 128, 256), bw1, ID, false);
+            umma::commit(mbar);
+          }
+          ok = umma::mbar_wait(mbar, 0, LC_WAIT_LIMIT) && ok;
           umma::fence_after_sync();
-          const uint32_t w2 = umma::smem_u32(lc_smem + LC_SMEM_W2);
+          // hidden layer 1: bias, gelu (two units per f32x2 lane pair), bf16x2 -> row tid of the hidden tiles
 #pragma unroll
           for (int t = 0; t < 2; t++) {
-            const uint32_t a = umma::smem_u32(sH + 8192 * t);
-            umma::mma_bf16(tmem + 32 * t, umma::sdesc(a, 128, 512), umma::sdesc(w2, 128, 512), ID, false);
-            umma::mma_bf16(tmem + 32 * t, umma::sdesc(a + 256, 128, 512), umma::sdesc(w2 + 256, 128, 512), ID,
-                           true);
-          }
-          umma::commit(mbar);
-        }
-        ok = umma::mbar_wait(mbar, 1, LC_WAIT_LIMIT) && ok;
-        umma::fence_after_sync();
-        // hidden layer 2 and the output layer
-        float z3[2];
+            float v[4][8];
 #pragma unroll
-        for (int t = 0; t < 2; t++) {
-          float v[4][8];
+            for (int c = 0; c < 4; c++) umma::tmem_ld8(umma::tmem_lane_addr(tmem, warp, 32 * t + 8 * c), v[c]);
+            umma::tmem_wait_ld();
 #pragma unroll
-          for (int c = 0; c < 4; c++) umma::tmem_ld8(umma::tmem_lane_addr(tmem, warp, 32 * t + 8 * c), v[c]);
-          umma::tmem_wait_ld();
-          float z = 0.0f;
+            for (int c = 0; c < 4; c++) {
+              uint32_t pk[4];
 #pragma unroll
-          for (int c = 0; c < 4; c++)
-#pragma unroll
-            for (int e = 0; e < 8; e++) {
-              const int j = 8 * c + e;
-              z = __fmaf_rn(bf16r(cl_gelu(__fadd_rn(v[c][e], cw->b2[j]))), cw->w3[j], z);
+              for (int e = 0; e < 4; e++) {
+                const int j = 8 * c + 2 * e;
+                const float2 g = cl_gelu2(__fadd2_rn(make_float2(v[c][2 * e], v[c][2 * e + 1]),
+                                                     make_float2(CP.b1[j], CP.b1[j + 1])));
+                pk[e] = bf16x2_bits(g.x, g.y);
+              }
+              *reinterpret_cast<uint4*>(sH + 8192 * t + umma::kmaj_off(tid, 8 * c, CL_H)) =
+                  make_uint4(pk[0], pk[1], pk[2], pk[3]);
             }
-          z3[t] = __fmul_rn(cw->nu_scale, cl_softplus(__fadd_rn(z, cw->b3)));
-        }
-        const float ta = tau0_eff(P, (float)x0, 0.0f) + 3.0f * z3[0];
-        const float tb = tau0_eff(P, (float)(x0 + 1), 0.0f) + 3.0f * z3[1];
-        return make_float2(1.0f - __fdividef(1.0f, ta), 1.0f - __fdividef(1.0f, tb));
-      });
+          }
+          umma::fence_before_sync();
+          umma::fence_async_smem();
+          __syncthreads();
+          if (tid == 0) {
+            umma::fence_after_sync();
+            const uint32_t w2 = umma::smem_u32(lc_smem + LC_SMEM_W2);
+#pragma unroll
+            for (int t = 0; t < 2; t++) {
+              const uint32_t a = umma::smem_u32(sH + 8192 * t);
+              umma::mma_bf16(tmem + 32 * t, umma::sdesc(a, 128, 512), umma::sdesc(w2, 128, 512), ID, false);
+              umma::mma_bf16(tmem + 32 * t, umma::sdesc(a + 256, 128, 512), umma::sdesc(w2 + 256, 128, 512), ID,
+                             true);
+            }
+            umma::commit(mbar);
+          }
+          ok = umma::mbar_wait(mbar, 1, LC_WAIT_LIMIT) && ok;
+          umma::fence_after_sync();
+          // hidden layer 2 (f32) and the output layer: even units in lane .x, odd units in lane .y
+          float z3[2];
+#pragma unroll
+          for (int t = 0; t < 2; t++) {
+            float v[4][8];
+#pragma unroll
+            for (int c = 0; c < 4; c++) umma::tmem_ld8(umma::tmem_lane_addr(tmem, warp, 32 * t + 8 * c), v[c]);
+            umma::tmem_wait_ld();
+            float2 z = f2(0.0f);
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+#pragma unroll
+              for (int e = 0; e < 4; e++) {
+                const int j = 8 * c + 2 * e;
+                const float2 g = cl_gelu2(__fadd2_rn(make_float2(v[c][2 * e], v[c][2 * e + 1]),
+                                                     make_float2(CP.b2[j], CP.b2[j + 1])));
+                z = __ffma2_rn(g, make_float2(CP.w3[j], CP.w3[j + 1]), z);
+              }
+            z3[t] = __fmul_rn(CP.nu_scale, cl_softplus(__fadd_rn(__fadd_rn(z.x, z.y), CP.b3)));
+          }
+          const float ta = tau0_eff(P, (float)x0, 0.0f) + 3.0f * z3[0];
+          const float tb = tau0_eff(P, (float)(x0 + 1), 0.0f) + 3.0f * z3[1];
+          return make_float2(1.0f - __fdividef(1.0f, ta), 1.0f - __fdividef(1.0f, tb));
+        });
+  }
   // release the tensor memory once every thread's reads have completed
-  umma::fence_before_sync();
-  __syncthreads();
   if (warp == 0) {
     umma::fence_after_sync();
     umma::tmem_free(tmem, LC_TMEM_COLS);
@@ -2177,17 +2193,23 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
       const int mb = s->sc_kernel;
       if constexpr (L::DIM == 3) {
         if (cw != nullptr) {
-          // learned closure: 128-thread blocks of (tpr, 128 / tpr) over the rows
+          // learned closure: persistent 128-thread blocks, as many as fit on the device, taking tiles of
+          // tpr cell pairs x 128 / tpr rows from a counter reset before the launch
           const int runs2 = s->dims.nx / 2;
           const int tpr = runs2 > 64 ? 128 : (runs2 > 32 ? 64 : 32);
-          const dim3 lblock(tpr, LC_THREADS / tpr);
-          const dim3 lgrid((runs2 + tpr - 1) / tpr, (s->dims.ny + lblock.y - 1) / lblock.y, s->dims.nz);
-          if (s->kp.collision == 1u)
-            k_stream_collide_lc<S, true><<<lgrid, lblock, LC_SMEM_BYTES, s->stream>>>(
-                s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, cw, s->err_dev);
-          else
-            k_stream_collide_lc<S, false><<<lgrid, lblock, LC_SMEM_BYTES, s->stream>>>(
-                s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, cw, s->err_dev);
+          const int rpb = LC_THREADS / tpr;
+          const int64_t ntiles = (int64_t)((runs2 + tpr - 1) / tpr) * ((s->dims.ny + rpb - 1) / rpb) * s->dims.nz;
+          if ((e = cudaMemsetAsync(s->lc_tiles, 0, 4, s->stream)) != cudaSuccess) return e;
+          auto kern = s->kp.collision == 1u ? k_stream_collide_lc<S, true> : k_stream_collide_lc<S, false>;
+          int per_sm = 0, sms = 0;
+          if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, LC_THREADS, LC_SMEM_BYTES)) !=
+              cudaSuccess)
+            return e;
+          if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device)) != cudaSuccess) return e;
+          const int64_t blocks = std::min<int64_t>(ntiles, (int64_t)std::max(per_sm, 1) * sms);
+          kern<<<(unsigned)blocks, LC_THREADS, LC_SMEM_BYTES, s->stream>>>(
+              s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, cw, s->closure_params,
+              s->lc_tiles, tpr, s->err_dev);
           s->launches++;
           if ((e = cudaGetLastError()) != cudaSuccess) return e;
           if (s->aux) {

@@ -7,6 +7,8 @@ sphere ......... src/analysis/validation.ts:137-184
 sphere_les ..... the D3Q19 LES sphere tunnel of the benchmark (FP16 storage against FP64 populations)
 vehicle ........ the D3Q19 vehicle tunnel of the benchmark (GPU voxelizer, moving belt, wheels)
 batch_sweep .... 32 vehicle tunnels of uneven sizes (yaw x speed sweep) stepped as one batch
+learned_closure  training data from filtered fine runs, GPU training, coarse runs with the network
+                 against the fine run and plain Smagorinsky (windtunnel_vis_b200.closure.study)
 
 A factory is any callable make(dims, params) returning an object with the LbmSolver surface
 (upload_flags, upload_sdf, step_and_sample, destroy) — windtunnel_vis_b200.solver.SolverFactory
@@ -355,11 +357,31 @@ def main(argv=None):
     from .solver import solver_factory
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["sphere_les", "vehicle", "batch_sweep", *CASES])
+    ap.add_argument("case", choices=["sphere_les", "vehicle", "batch_sweep", "learned_closure", *CASES])
     ap.add_argument("--precision", default="f16")
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--valscale", type=float, default=1.0)
+    ap.add_argument("--fine", default="512,256,256", help="learned_closure: fine grid nx,ny,nz")
+    ap.add_argument("--train-bodies", type=int, default=8)
+    ap.add_argument("--eval-bodies", type=int, default=2)
+    ap.add_argument("--warm", type=int, default=6000)
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--keep", type=float, default=0.4)
+    ap.add_argument("--re", type=float, default=1000.0)
+    ap.add_argument("--save", default=None, help="learned_closure: write the trained network (.npz)")
     a = ap.parse_args(argv)
+    if a.case == "learned_closure":
+        from . import closure as CL
+
+        fine = tuple(int(v) for v in a.fine.split(","))
+        r = CL.study(solver_factory, fine_dims=fine, train_bodies=a.train_bodies, eval_bodies=a.eval_bodies,
+                     warm=a.warm, train_steps=a.train_steps, keep=a.keep, re=a.re, eval_steps=a.steps,
+                     log=lambda m: print(m, flush=True))
+        if a.save:
+            CL.save({k: np.asarray(v, np.float32) for k, v in r["model"].items()}, a.save)
+        r.pop("model", None)
+        print(json.dumps(r, default=float), flush=True)
+        return
     if a.case == "sphere_les":
         r = sphere_les(solver_factory, a.precision, a.steps)
     elif a.case == "vehicle":
