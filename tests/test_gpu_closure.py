@@ -266,18 +266,21 @@ def test_training_samples_match_numpy_restatement(gpu, oracle):
     idx, xn, yn, bound = _np_samples(oracle, fine.read_populations(), ff, fdims, fine.kparams(), cdims, ckp.tau0, cf, cs,
                               ckp.sponge_in, min(cdims[0], ckp.sponge_start))
     assert len(idx) == added  # the same cells are kept, in cell order
-    # compare where the shifted pull is exact: every fine cell of the 5 x 5 x 5 coarse neighbourhood is
-    # at least one cell away from any solid and from the domain faces
+    # compare where the shifted pull is exact: no fine cell of the 5 x 5 x 5 coarse neighbourhood has a
+    # solid among its 26 neighbours (D3Q19 pulls along faces and edges) or lies on a domain face
     solid = ff.reshape(fdims[2], fdims[1], fdims[0]).astype(bool)
     near = solid.copy()
-    for ax in range(3):
-        near |= np.roll(solid, 1, ax) | np.roll(solid, -1, ax)
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                near |= np.roll(solid, (dz, dy, dx), axis=(0, 1, 2))
     near[[0, -1], :, :] = near[:, [0, -1], :] = near[:, :, [0, -1]] = True
     cbad = near.reshape(cdims[2], 2, cdims[1], 2, cdims[0], 2).any(axis=(1, 3, 5))
     bad5 = cbad.copy()
-    for ax in range(3):
-        for s in (1, 2):
-            bad5 |= np.roll(cbad, s, ax) | np.roll(cbad, -s, ax)
+    for dz in range(-2, 3):
+        for dy in range(-2, 3):
+            for dx in range(-2, 3):
+                bad5 |= np.roll(cbad, (dz, dy, dx), axis=(0, 1, 2))
     zz, rem = np.divmod(idx, cdims[0] * cdims[1])
     yy, xx = np.divmod(rem, cdims[0])
     ok = ~bad5[zz, yy, xx]

@@ -71,7 +71,7 @@ void free_all(wt_solver* s) {
   void* bufs[] = {s->f[0], s->f[1], s->flags, s->sdf, s->cls, s->vel, s->vel_f32, s->meanA, s->meanB,
                   s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count,
                   s->bcell, s->brec, s->bgam, s->vox_pos, s->vox_idx, s->vox_info,
-                  s->dvort, s->dstat, s->dmean, s->exp_buf, s->probe_buf, s->closure_dev, s->lc_tiles};
+                  s->dvort, s->dstat, s->dmean, s->exp_buf, s->probe_buf, s->closure_dev};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->result_host) cudaFreeHost(s->result_host);
@@ -442,8 +442,6 @@ int wt_set_closure(wt_solver* s, const wt_closure* c) {
       WT_CUDA(s, cudaStreamSynchronize(s->stream), "wt_set_closure");
       cudaFree(s->closure_dev);
       s->closure_dev = nullptr;
-      cudaFree(s->lc_tiles);
-      s->lc_tiles = nullptr;
     }
     return WT_OK;
   }
@@ -462,7 +460,6 @@ int wt_set_closure(wt_solver* s, const wt_closure* c) {
   // the captured step graphs carry the network's by-value part: rebuild them
   invalidate_graphs(s);
   if (!s->closure_dev) WT_CUDA(s, cudaMalloc((void**)&s->closure_dev, sizeof(wt::ClosureDev)), "wt_set_closure");
-  if (!s->lc_tiles) WT_CUDA(s, cudaMalloc((void**)&s->lc_tiles, 4), "wt_set_closure");
   WT_CUDA(s, cudaMemcpyAsync(s->closure_dev, &host, sizeof host, cudaMemcpyHostToDevice, s->stream), "wt_set_closure");
   WT_CUDA(s, cudaStreamSynchronize(s->stream), "wt_set_closure");
   s->closure_host = *c;

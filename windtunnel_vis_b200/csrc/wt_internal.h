@@ -92,7 +92,6 @@ struct wt_solver {
   // learned closure (wt_set_closure): device copy of the network, nullptr = Smagorinsky
   wt::ClosureDev* closure_dev = nullptr;
   wt::ClosureParams closure_params{};  // by-value part, baked into the bulk kernel's launches
-  uint32_t* lc_tiles = nullptr;        // tile counter of the persistent closure kernel
   wt_closure closure_host{};
   int* err_dev = nullptr;   // device-side error word written by kernels with bounded waits
   int* err_host = nullptr;  // pinned copy

@@ -1169,7 +1169,7 @@ constexpr int LC_SMEM_A = 0;       // 2 tiles x 128 x 16 bf16
 constexpr int LC_SMEM_H = 8192;    // 2 tiles x 128 x 32 bf16
 constexpr int LC_SMEM_W1 = 24576;  // W1 image, 32 x 16 bf16 (followed by the W2 image: one 3 KB copy)
 constexpr int LC_SMEM_W2 = 25600;  // W2 image, 32 x 32 bf16
-constexpr int LC_SMEM_BAR = 27648; // mbarrier (8 B), tensor-memory address (4 B), current tile (4 B)
+constexpr int LC_SMEM_BAR = 27648; // mbarrier (8 B), then the tensor-memory address (4 B)
 // dynamic shared memory per block: more than 228 KB / 8, so at most 7 blocks share an SM and their
 // 7 x 64 tensor-memory columns fit in the SM's 512 (an allocation never has to wait)
 constexpr int LC_SMEM_BYTES = 29 * 1024;
@@ -1189,8 +1189,7 @@ __device__ __forceinline__ void lc_write_inputs(uint8_t* tile, uint32_t r, const
   *reinterpret_cast<uint4*>(tile + umma::kmaj_off(r, 8, CL_K1)) = make_uint4(w[4], 0u, 0u, 0u);
 }
 
-// Persistent: each block allocates its tensor memory and stages the weight images once, then takes
-// tiles (tpr cells pairs x 128 / tpr rows) from `tiles_next` until `ntiles` are done.
+// One tile (tpr cell pairs x 128 / tpr rows) per block, 1-D grid over the tiles.
 template <class S, bool BGK>
 __global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_constant__ wt_kparams P,
                                                                    const typename S::T* __restrict__ fin,
@@ -1199,8 +1198,7 @@ __global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_c
                                                                    const uint32_t* __restrict__ sdf,
                                                                    const ClosureDev* __restrict__ cw,
                                                                    const __grid_constant__ ClosureParams CP,
-                                                                   uint32_t* __restrict__ tiles_next, int tpr,
-                                                                   int* __restrict__ err) {
+                                                                   int tpr, int* __restrict__ err) {
   typedef D3Q19 L;
   typedef PairIO<S> IO;
   constexpr int Q = L::Q;
@@ -1211,14 +1209,12 @@ __global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_c
   const int rpb = LC_THREADS / tpr;
   const int tx = (int)tid % tpr, ty = (int)tid / tpr;
   const int tiles_x = (NX / 2 + tpr - 1) / tpr, tiles_y = (NY + rpb - 1) / rpb;
-  const uint32_t ntiles = (uint32_t)tiles_x * (uint32_t)tiles_y * (uint32_t)NZ;
   const uint32_t N = P.n;
   const uint32_t sy = (uint32_t)NX, sz = (uint32_t)NX * (uint32_t)NY;
   uint8_t* const sA = lc_smem + LC_SMEM_A;
   uint8_t* const sH = lc_smem + LC_SMEM_H;
   uint64_t* const mbar = reinterpret_cast<uint64_t*>(lc_smem + LC_SMEM_BAR);
   uint32_t* const tslot = reinterpret_cast<uint32_t*>(lc_smem + LC_SMEM_BAR + 8);
-  uint32_t* const stile = reinterpret_cast<uint32_t*>(lc_smem + LC_SMEM_BAR + 12);
   {
     const uint4* src = reinterpret_cast<const uint4*>(cw->w1img);
     uint4* dst = reinterpret_cast<uint4*>(lc_smem + LC_SMEM_W1);
@@ -1231,13 +1227,8 @@ __global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_c
   umma::fence_after_sync();
   const uint32_t tmem = *tslot;
   bool ok = true;
-  for (;;) {
-    // next tile; the barrier also closes the previous tile (its tensor-memory reads are fenced)
-    if (tid == 0) *stile = atomicAdd(tiles_next, 1u);
-    umma::fence_before_sync();
-    __syncthreads();
-    const uint32_t tile = *stile;
-    if (tile >= ntiles) break;
+  {
+    const uint32_t tile = blockIdx.x;
     const int bx = (int)(tile % (uint32_t)tiles_x);
     const int by = (int)((tile / (uint32_t)tiles_x) % (uint32_t)tiles_y);
     const int iz = (int)(tile / ((uint32_t)tiles_x * (uint32_t)tiles_y));
@@ -1389,6 +1380,8 @@ __global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_c
         });
   }
   // release the tensor memory once every thread's reads have completed
+  umma::fence_before_sync();
+  __syncthreads();
   if (warp == 0) {
     umma::fence_after_sync();
     umma::tmem_free(tmem, LC_TMEM_COLS);
@@ -2193,23 +2186,15 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
       const int mb = s->sc_kernel;
       if constexpr (L::DIM == 3) {
         if (cw != nullptr) {
-          // learned closure: persistent 128-thread blocks, as many as fit on the device, taking tiles of
-          // tpr cell pairs x 128 / tpr rows from a counter reset before the launch
+          // learned closure: 128-thread blocks, one tile of tpr cell pairs x 128 / tpr rows each
           const int runs2 = s->dims.nx / 2;
           const int tpr = runs2 > 64 ? 128 : (runs2 > 32 ? 64 : 32);
           const int rpb = LC_THREADS / tpr;
           const int64_t ntiles = (int64_t)((runs2 + tpr - 1) / tpr) * ((s->dims.ny + rpb - 1) / rpb) * s->dims.nz;
-          if ((e = cudaMemsetAsync(s->lc_tiles, 0, 4, s->stream)) != cudaSuccess) return e;
           auto kern = s->kp.collision == 1u ? k_stream_collide_lc<S, true> : k_stream_collide_lc<S, false>;
-          int per_sm = 0, sms = 0;
-          if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, LC_THREADS, LC_SMEM_BYTES)) !=
-              cudaSuccess)
-            return e;
-          if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device)) != cudaSuccess) return e;
-          const int64_t blocks = std::min<int64_t>(ntiles, (int64_t)std::max(per_sm, 1) * sms);
-          kern<<<(unsigned)blocks, LC_THREADS, LC_SMEM_BYTES, s->stream>>>(
+          kern<<<(unsigned)ntiles, LC_THREADS, LC_SMEM_BYTES, s->stream>>>(
               s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, cw, s->closure_params,
-              s->lc_tiles, tpr, s->err_dev);
+              tpr, s->err_dev);
           s->launches++;
           if ((e = cudaGetLastError()) != cudaSuccess) return e;
           if (s->aux) {
