@@ -456,14 +456,15 @@ int wt_set_closure(wt_solver* s, const wt_closure* c) {
   if (!(c->nu_scale >= 0.0f)) return fail(s, WT_E_INVALID, "wt_set_closure: nu_scale must be >= 0");
   wt::ClosureDev host;
   std::memset(&host, 0, sizeof host);
-  wt::closure_pack(*c, host);
+  wt::ClosureWeights cwt;
+  wt::closure_pack(*c, host, cwt);
   // the captured step graphs carry the network's by-value part: rebuild them
   invalidate_graphs(s);
   if (!s->closure_dev) WT_CUDA(s, cudaMalloc((void**)&s->closure_dev, sizeof(wt::ClosureDev)), "wt_set_closure");
   WT_CUDA(s, cudaMemcpyAsync(s->closure_dev, &host, sizeof host, cudaMemcpyHostToDevice, s->stream), "wt_set_closure");
   WT_CUDA(s, cudaStreamSynchronize(s->stream), "wt_set_closure");
   s->closure_host = *c;
-  s->closure_params = wt::closure_params(*c);
+  s->closure_w = cwt;
   return WT_OK;
 }
 

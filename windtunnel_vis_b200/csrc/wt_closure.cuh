@@ -43,17 +43,25 @@ struct ClosureParams {
   float nshift[CL_IN];
 };
 
-// Device copy of a network. Images are the tcgen05 B operands (N x K, K-major, no swizzle):
+// Device copy of a network's weight images, the tcgen05 B operands (N x K, K-major, no swizzle):
 // w1img[n = hidden j][k = input], w2img[n = out j][k = in i] (forward), w2timg[n = in i][k = out j]
-// (the dH1 = dZ2 W2^T product of the backward pass). The f32 arrays hold the same bf16-rounded
-// weights for the CUDA-core path.
+// (the dH1 = dZ2 W2^T product of the backward pass).
 struct __align__(128) ClosureDev {
   uint16_t w1img[CL_H * CL_K1];
   uint16_t w2img[CL_H * CL_H];
   uint16_t w2timg[CL_H * CL_H];
+};
+
+// The whole network for the CUDA-core path (face rows and wall cells), passed by value so that
+// every weight is a constant-bank operand: the bf16-rounded W1 and W2 as f32, and the small values.
+struct ClosureWeights {
   float w1[CL_IN][CL_H];
   float w2[CL_H][CL_H];
-  ClosureParams p;  // the by-value part, for the CUDA-core path
+  ClosureParams p;
+};
+// placeholder parameter of the kernels' Smagorinsky instantiations
+struct NoClosure {
+  int unused;
 };
 
 // bf16 round to nearest even (finite inputs), as a float and as raw bits
@@ -156,25 +164,25 @@ __device__ __forceinline__ void cl_features(float pxx, float pyy, float pzz, flo
 }
 
 // the whole network on CUDA cores (face and wall cells): nu_t of one cell
-static __device__ __noinline__ float closure_nu(const ClosureDev* __restrict__ C, const ClosureParams& P,
-                                               const float* __restrict__ xin) {
+static __device__ __noinline__ float closure_nu(const ClosureWeights& W, const float* __restrict__ xin) {
+  const ClosureParams& P = W.p;
   float x[CL_IN];
 #pragma unroll
   for (int k = 0; k < CL_IN; k++) x[k] = bf16r(__fmaf_rn(xin[k], P.scale[k], P.nshift[k]));
   float h1[CL_H];
-#pragma unroll 4
+#pragma unroll
   for (int j = 0; j < CL_H; j++) {
     float a = 0.0f;
 #pragma unroll
-    for (int k = 0; k < CL_IN; k++) a = __fmaf_rn(x[k], C->w1[k][j], a);
+    for (int k = 0; k < CL_IN; k++) a = __fmaf_rn(x[k], W.w1[k][j], a);
     h1[j] = bf16r(cl_gelu(__fadd_rn(a, P.b1[j])));
   }
   float ze = 0.0f, zo = 0.0f;
-#pragma unroll 2
+#pragma unroll
   for (int j = 0; j < CL_H; j++) {
     float a = 0.0f;
 #pragma unroll
-    for (int i = 0; i < CL_H; i++) a = __fmaf_rn(h1[i], C->w2[i][j], a);
+    for (int i = 0; i < CL_H; i++) a = __fmaf_rn(h1[i], W.w2[i][j], a);
     const float h2 = cl_gelu(__fadd_rn(a, P.b2[j]));
     if (j & 1) zo = __fmaf_rn(h2, P.w3[j], zo);
     else ze = __fmaf_rn(h2, P.w3[j], ze);
@@ -199,8 +207,8 @@ __host__ __device__ inline ClosureParams closure_params(const wt_closure& c) {
   return p;
 }
 
-// fills the bf16 images and rounded f32 copies of `c` into `d` (host or device)
-__host__ __device__ inline void closure_pack(const wt_closure& c, ClosureDev& d) {
+// fills the bf16 images of `c` into `d` and the CUDA-core copy into `w` (host or device)
+__host__ __device__ inline void closure_pack(const wt_closure& c, ClosureDev& d, ClosureWeights& w) {
   for (int j = 0; j < CL_H; j++)
     for (int k = 0; k < CL_K1; k++) {
       const float v = k < CL_IN ? c.w1[k][j] : 0.0f;
@@ -211,11 +219,11 @@ __host__ __device__ inline void closure_pack(const wt_closure& c, ClosureDev& d)
       const uint16_t b = bf16_bits(c.w2[i][j]);
       d.w2img[umma::kmaj_off(j, i, CL_H) / 2] = b;
       d.w2timg[umma::kmaj_off(i, j, CL_H) / 2] = b;
-      d.w2[i][j] = bf16_val(b);
+      w.w2[i][j] = bf16_val(b);
     }
   for (int k = 0; k < CL_IN; k++)
-    for (int j = 0; j < CL_H; j++) d.w1[k][j] = bf16r(c.w1[k][j]);
-  d.p = closure_params(c);
+    for (int j = 0; j < CL_H; j++) w.w1[k][j] = bf16r(c.w1[k][j]);
+  w.p = closure_params(c);
 }
 
 }  // namespace wt

@@ -91,7 +91,7 @@ struct wt_solver {
   bool launch_explicit = false;
   // learned closure (wt_set_closure): device copy of the network, nullptr = Smagorinsky
   wt::ClosureDev* closure_dev = nullptr;
-  wt::ClosureParams closure_params{};  // by-value part, baked into the bulk kernel's launches
+  wt::ClosureWeights closure_w{};  // the network by value (CUDA-core path; .p for the bulk kernel)
   wt_closure closure_host{};
   int* err_dev = nullptr;   // device-side error word written by kernels with bounded waits
   int* err_host = nullptr;  // pinned copy

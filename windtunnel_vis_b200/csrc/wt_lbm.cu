@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(256) k_init(const wt_kparams P, typename S::T*
 // Smagorinsky term: tau = tau0' + 3 nu_t (tau0' = tau0 with the outlet sponge and the wall floor).
 template <class L, class R>
 __device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L::Q], int ix, bool wall, bool gwall,
-                                             R (&fo)[L::Q], const ClosureDev* cw = nullptr, float wall_d = 0.0f) {
+                                             R (&fo)[L::Q], const ClosureWeights* cw = nullptr, float wall_d = 0.0f) {
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
   const R U = (R)P.uin;
@@ -219,7 +219,7 @@ __device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L
     if (cw != nullptr) {
       float x[CL_IN];
       cl_features(pxx, pyy, pzz, pxy, pxz, pyz, rho, ux, uy, uz, P.tau0, wall_d, x);
-      tau = t0 + 3.0f * closure_nu(cw, cw->p, x);
+      tau = t0 + 3.0f * closure_nu(*cw, x);
     } else {
       tau = (R)0.5 * (t0 + sqrt(t0 * t0 + (R)(18.0 * 1.4142135623730951) * (R)P.csmag2 * piN * irho));
     }
@@ -850,7 +850,7 @@ __device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const floa
 // the learned closure for cells collided on CUDA cores (face rows): the network per lane
 template <class L, bool BGK, class Emit>
 __device__ __forceinline__ void collide_shifted2_lc(const wt_kparams& P, const float2 (&h)[L::Q], int x, Emit&& emit,
-                                                    float t_floor, const ClosureDev* __restrict__ cw, float2 wd) {
+                                                    float t_floor, const ClosureWeights& cw, float2 wd) {
   collide_shifted2x<L, BGK>(P, h, x, emit,
                             [&](float2 rho, float2, float2 ux, float2 uy, float2 uz, float2 pxx, float2 pyy,
                                 float2 pzz, float2 pxy, float2 pxz, float2 pyz) {
@@ -859,8 +859,8 @@ __device__ __forceinline__ void collide_shifted2_lc(const wt_kparams& P, const f
                                           wd.x, xa);
                               cl_features(pxx.y, pyy.y, pzz.y, pxy.y, pxz.y, pyz.y, rho.y, ux.y, uy.y, uz.y, P.tau0,
                                           wd.y, xb);
-                              const float ta = tau0_eff(P, (float)x, t_floor) + 3.0f * closure_nu(cw, cw->p, xa);
-                              const float tb = tau0_eff(P, (float)(x + 1), t_floor) + 3.0f * closure_nu(cw, cw->p, xb);
+                              const float ta = tau0_eff(P, (float)x, t_floor) + 3.0f * closure_nu(cw, xa);
+                              const float tb = tau0_eff(P, (float)(x + 1), t_floor) + 3.0f * closure_nu(cw, xb);
                               return make_float2(1.0f - __fdividef(1.0f, ta), 1.0f - __fdividef(1.0f, tb));
                             });
 }
@@ -1012,13 +1012,16 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
 // rows with bounce-back collide with BGK and the tauWall floor, like the reference's wall cells.
 // Groups holding a solid or a fluid cell next to a solid are left to k_boundary_tab.
 // With LC the learned closure replaces Smagorinsky (network on CUDA cores, wall distance from sdf).
+template <bool LC> struct LCW { typedef NoClosure type; };
+template <> struct LCW<true> { typedef ClosureWeights type; };
+
 template <class L, class S, bool LC = false>
 __global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kparams P,
                                                 const typename S::T* __restrict__ fin,
                                                 typename S::T* __restrict__ fout,
                                                 const uint8_t* __restrict__ cls, int gs,
-                                                const uint32_t* __restrict__ sdf = nullptr,
-                                                const ClosureDev* __restrict__ cw = nullptr) {
+                                                const uint32_t* __restrict__ sdf,
+                                                const __grid_constant__ typename LCW<LC>::type CW) {
   typedef PairIO<S> IO;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
@@ -1141,9 +1144,9 @@ __global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kpara
   if constexpr (LC) {
     const uint2 sw = __ldg(reinterpret_cast<const uint2*>(sdf + idx0));
     const float2 wd = make_float2(cl_wall_dist(sw.x), cl_wall_dist(sw.y));
-    if (gwall) collide_shifted2_lc<L, true>(P, h, x0, emit, P.tau_wall, cw, wd);
-    else if (P.collision == 1u) collide_shifted2_lc<L, true>(P, h, x0, emit, 0.0f, cw, wd);
-    else collide_shifted2_lc<L, false>(P, h, x0, emit, 0.0f, cw, wd);
+    if (gwall) collide_shifted2_lc<L, true>(P, h, x0, emit, P.tau_wall, CW, wd);
+    else if (P.collision == 1u) collide_shifted2_lc<L, true>(P, h, x0, emit, 0.0f, CW, wd);
+    else collide_shifted2_lc<L, false>(P, h, x0, emit, 0.0f, CW, wd);
   } else {
     if (gwall) collide_shifted2<L, true>(P, h, x0, emit, P.tau_wall);
     else if (P.collision == 1u) collide_shifted2<L, true>(P, h, x0, emit);
@@ -1550,8 +1553,8 @@ __global__ void __launch_bounds__(64) k_boundary_tab(const __grid_constant__ wt_
                                                      typename S::T* __restrict__ fout,
                                                      const uint2* __restrict__ bcell, const uint4* __restrict__ rec,
                                                      const float* __restrict__ gam, uint32_t count, uint32_t cap,
-                                                     const uint32_t* __restrict__ sdf = nullptr,
-                                                     const ClosureDev* __restrict__ cw = nullptr) {
+                                                     const uint32_t* __restrict__ sdf,
+                                                     const __grid_constant__ typename LCW<LC>::type CW) {
   constexpr int Q = L::Q;
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= count) return;
@@ -1576,7 +1579,7 @@ __global__ void __launch_bounds__(64) k_boundary_tab(const __grid_constant__ wt_
   });
   const int ix = (int)(hc.x % P.nx);
   if constexpr (LC)
-    collide_full<L, float>(P, f, ix, (hc.y & BC_WALL) != 0u, (hc.y & BC_GWALL) != 0u, fo, cw,
+    collide_full<L, float>(P, f, ix, (hc.y & BC_WALL) != 0u, (hc.y & BC_GWALL) != 0u, fo, &CW,
                            cl_wall_dist(__ldg(sdf + hc.x)));
   else
     collide_full<L, float>(P, f, ix, (hc.y & BC_WALL) != 0u, (hc.y & BC_GWALL) != 0u, fo);
@@ -2150,26 +2153,29 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
         if constexpr (L::DIM == 3) {
           if (cw != nullptr)
             k_face_v<L, S, true><<<fgrid, dim3(fbx, fby), 0, bs>>>(
-                s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, cw);
+                s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, s->closure_w);
           else
             k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin,
-                                                             (typename S::T*)fout, s->cls, s->gs);
+                                                             (typename S::T*)fout, s->cls, s->gs, s->sdf,
+                                                             NoClosure{0});
         } else {
           k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin, (typename S::T*)fout,
-                                                           s->cls, s->gs);
+                                                           s->cls, s->gs, s->sdf, NoClosure{0});
         }
         s->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
       }
       if (s->nbnd > 0) {
-        if (cw != nullptr)
-          k_boundary_tab<L, S, L::DIM == 3><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
-              s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
-              (uint32_t)s->btab_cap, s->sdf, cw);
-        else
+        if (cw != nullptr) {
+          if constexpr (L::DIM == 3)
+            k_boundary_tab<L, S, true><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
+                s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
+                (uint32_t)s->btab_cap, s->sdf, s->closure_w);
+        } else {
           k_boundary_tab<L, S><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
               s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
-              (uint32_t)s->btab_cap);
+              (uint32_t)s->btab_cap, s->sdf, NoClosure{0});
+        }
         s->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
       }
@@ -2193,7 +2199,7 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
           const int64_t ntiles = (int64_t)((runs2 + tpr - 1) / tpr) * ((s->dims.ny + rpb - 1) / rpb) * s->dims.nz;
           auto kern = s->kp.collision == 1u ? k_stream_collide_lc<S, true> : k_stream_collide_lc<S, false>;
           kern<<<(unsigned)ntiles, LC_THREADS, LC_SMEM_BYTES, s->stream>>>(
-              s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, cw, s->closure_params,
+              s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, cw, s->closure_w.p,
               tpr, s->err_dev);
           s->launches++;
           if ((e = cudaGetLastError()) != cudaSuccess) return e;
