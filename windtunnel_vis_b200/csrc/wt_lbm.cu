@@ -1015,13 +1015,10 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
 template <bool LC> struct LCW { typedef NoClosure type; };
 template <> struct LCW<true> { typedef ClosureWeights type; };
 
-template <class L, class S, bool LC = false>
-__global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kparams P,
-                                                const typename S::T* __restrict__ fin,
-                                                typename S::T* __restrict__ fout,
-                                                const uint8_t* __restrict__ cls, int gs,
-                                                const uint32_t* __restrict__ sdf,
-                                                const __grid_constant__ typename LCW<LC>::type CW) {
+template <class L, class S, bool LC>
+__device__ __forceinline__ void face_rows(const wt_kparams& P, const typename S::T* __restrict__ fin,
+                                          typename S::T* __restrict__ fout, const uint8_t* __restrict__ cls, int gs,
+                                          const uint32_t* __restrict__ sdf, const typename LCW<LC>::type& CW) {
   typedef PairIO<S> IO;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
@@ -1152,6 +1149,25 @@ __global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kpara
     else if (P.collision == 1u) collide_shifted2<L, true>(P, h, x0, emit);
     else collide_shifted2<L, false>(P, h, x0, emit);
   }
+}
+
+template <class L, class S>
+__global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kparams P,
+                                                const typename S::T* __restrict__ fin,
+                                                typename S::T* __restrict__ fout,
+                                                const uint8_t* __restrict__ cls, int gs) {
+  face_rows<L, S, false>(P, fin, fout, cls, gs, nullptr, NoClosure{0});
+}
+
+// face rows with the learned closure (network on CUDA cores, registers capped for two blocks per SM)
+template <class L, class S>
+__global__ void __launch_bounds__(256, 2) k_face_lc(const __grid_constant__ wt_kparams P,
+                                                    const typename S::T* __restrict__ fin,
+                                                    typename S::T* __restrict__ fout,
+                                                    const uint8_t* __restrict__ cls, int gs,
+                                                    const uint32_t* __restrict__ sdf,
+                                                    const __grid_constant__ ClosureWeights CW) {
+  face_rows<L, S, true>(P, fin, fout, cls, gs, sdf, CW);
 }
 
 // ---- bulk kernel with the learned closure: the network on tcgen05 tensor cores -----------------
@@ -2152,15 +2168,14 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
         const dim3 fgrid((runs2 + fbx - 1) / fbx, (fr + fby - 1) / fby, 1);
         if constexpr (L::DIM == 3) {
           if (cw != nullptr)
-            k_face_v<L, S, true><<<fgrid, dim3(fbx, fby), 0, bs>>>(
+            k_face_lc<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(
                 s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, s->closure_w);
           else
             k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin,
-                                                             (typename S::T*)fout, s->cls, s->gs, s->sdf,
-                                                             NoClosure{0});
+                                                             (typename S::T*)fout, s->cls, s->gs);
         } else {
           k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin, (typename S::T*)fout,
-                                                           s->cls, s->gs, s->sdf, NoClosure{0});
+                                                           s->cls, s->gs);
         }
         s->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
