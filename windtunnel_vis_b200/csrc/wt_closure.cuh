@@ -170,7 +170,7 @@ static __device__ __noinline__ float closure_nu(const ClosureWeights& W, const f
 #pragma unroll
   for (int k = 0; k < CL_IN; k++) x[k] = bf16r(__fmaf_rn(xin[k], P.scale[k], P.nshift[k]));
   float h1[CL_H];
-#pragma unroll
+#pragma unroll 8
   for (int j = 0; j < CL_H; j++) {
     float a = 0.0f;
 #pragma unroll
@@ -178,7 +178,7 @@ static __device__ __noinline__ float closure_nu(const ClosureWeights& W, const f
     h1[j] = bf16r(cl_gelu(__fadd_rn(a, P.b1[j])));
   }
   float ze = 0.0f, zo = 0.0f;
-#pragma unroll
+#pragma unroll 2
   for (int j = 0; j < CL_H; j++) {
     float a = 0.0f;
 #pragma unroll
