@@ -56,7 +56,7 @@ def measured_traffic(shape, closure=False):
     if not os.path.exists(p):
         return None
     key = "lc" if closure else ",".join(str(int(v)) for v in shape)
-    for m in re.finditer(r"^traffic_bytes_per_step\[([0-9,]+)\]:\s*(\d+)", open(p).read(), flags=re.M):
+    for m in re.finditer(r"^traffic_bytes_per_step\[([0-9a-z,]+)\]:\s*(\d+)", open(p).read(), flags=re.M):
         if m.group(1) == key:
             return int(m.group(2))
     return None

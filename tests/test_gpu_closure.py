@@ -326,3 +326,44 @@ def test_trained_network_beats_smagorinsky_a_priori(gpu):
     ev.destroy()
     assert learned["nmse"] < smag["nmse"], (learned, smag)
     assert learned["nmse"] < 1.0, learned
+
+
+def test_batch_with_networks_matches_members_stepped_alone(gpu):
+    """A batch of tunnels whose members carry learned closures (and one plain member) advances each
+    member exactly as it advances alone; installing a network mid-run makes the batch recapture."""
+    from windtunnel_vis_b200.solver import Batch
+
+    cases = [((32, 14, 12), dict(PARAM_SETS["belt_periodic_les"], precision="f16"), _scene_model(seed=31)),
+             ((48, 20, 16), dict(PARAM_SETS["freeslip_reg"], precision="f32"), _scene_model(seed=32)),
+             ((40, 16, 12), dict(PARAM_SETS["noslip_bgk_halfway"], precision="f16"), None)]
+
+    def make(dims, params, model):
+        flags, sdf, wheels = scene(dims)
+        s = Solver(dims, params)
+        s.upload_flags(flags)
+        s.upload_sdf(sdf)
+        s.set_wheels(wheels)
+        if model is not None:
+            s.set_closure(model)
+        return s
+
+    members = [make(*c) for c in cases]
+    alone = [make(*c) for c in cases]
+    b = Batch(members)
+    for steps in (7, 4):
+        b.step(steps)
+        for s in alone:
+            s.step(steps)
+    for s, t in zip(members, alone):
+        np.testing.assert_array_equal(s.read_populations(), t.read_populations())
+    m = _scene_model(seed=33)
+    members[2].set_closure(m)
+    alone[2].set_closure(m)
+    b.step(6)
+    for s in alone:
+        s.step(6)
+    for s, t in zip(members, alone):
+        np.testing.assert_array_equal(s.read_populations(), t.read_populations())
+    b.destroy()
+    for s in members + alone:
+        s.destroy()
