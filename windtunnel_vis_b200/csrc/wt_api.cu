@@ -79,6 +79,8 @@ void free_all(wt_solver* s) {
   if (s->bnd_count_host) cudaFreeHost(s->bnd_count_host);
   for (auto& g : s->step_graph)
     if (g) cudaGraphExecDestroy(g);
+  for (auto& g : s->long_graph)
+    if (g) cudaGraphExecDestroy(g);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
   if (s->aux) cudaStreamDestroy(s->aux);
@@ -98,6 +100,10 @@ cudaError_t create_priority_stream(cudaStream_t* st) {
 // and the boundary list); the next wt_step recaptures them.
 void invalidate_graphs(wt_solver* s) {
   for (auto& g : s->step_graph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+  for (auto& g : s->long_graph) {
     if (g) cudaGraphExecDestroy(g);
     g = nullptr;
   }
@@ -149,25 +155,32 @@ int ensure_classified(wt_solver* s) {
   return WT_OK;
 }
 
-// Captures the two-step graph for starting parity p: step f[p] -> f[p^1], then f[p^1] -> f[p].
-int capture_step_graph(wt_solver* s, int p) {
+// Captures `pairs` ping-pong step pairs for starting parity p (f[p] -> f[p^1] -> f[p], repeated)
+// into *out; *launches receives the kernel launches of one replay.
+int capture_steps(wt_solver* s, int p, int pairs, cudaGraphExec_t* out, int64_t* launches) {
   const int64_t l0 = s->launches;
   cudaGraph_t graph = nullptr;
   WT_CUDA(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
-  cudaError_t e = wt::launch_stream_collide(s, s->f[p], s->f[p ^ 1]);
-  if (e == cudaSuccess) e = wt::launch_stream_collide(s, s->f[p ^ 1], s->f[p]);
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < pairs && e == cudaSuccess; k++) {
+    e = wt::launch_stream_collide(s, s->f[p], s->f[p ^ 1]);
+    if (e == cudaSuccess) e = wt::launch_stream_collide(s, s->f[p ^ 1], s->f[p]);
+  }
   cudaError_t e2 = cudaStreamEndCapture(s->stream, &graph);
-  s->graph_launches = s->launches - l0;
+  *launches = s->launches - l0;
   s->launches = l0;
   if (e == cudaSuccess) e = e2;
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&s->step_graph[p], graph, cudaGraphInstantiateFlagUseNodePriority);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(out, graph, cudaGraphInstantiateFlagUseNodePriority);
   if (graph) cudaGraphDestroy(graph);
   if (e != cudaSuccess) {
-    s->step_graph[p] = nullptr;
+    *out = nullptr;
     return cuda_fail(s, e, "graph capture");
   }
   return WT_OK;
 }
+
+// the two-step graph for starting parity p: step f[p] -> f[p^1], then f[p^1] -> f[p]
+int capture_step_graph(wt_solver* s, int p) { return capture_steps(s, p, 1, &s->step_graph[p], &s->graph_launches); }
 
 int ensure_init(wt_solver* s) {
   if (!s->pending_init) return WT_OK;
@@ -562,6 +575,17 @@ int wt_step(wt_solver* s, int32_t steps) {
     cudaError_t e = wt::launch_stream_collide(s, s->f[s->parity], s->f[s->parity ^ 1]);
     if (e != cudaSuccess) return cuda_fail(s, e, "stream_collide");
     s->parity ^= 1;
+  }
+  if (steps - k >= 2 * WT_LONG_PAIRS) {
+    // runs of WT_LONG_PAIRS step pairs replay one long graph (fewer graph launches)
+    if (!s->long_graph[s->parity]) {
+      rc = capture_steps(s, s->parity, WT_LONG_PAIRS, &s->long_graph[s->parity], &s->long_graph_launches);
+      if (rc) return rc;
+    }
+    for (; k + 2 * WT_LONG_PAIRS <= steps; k += 2 * WT_LONG_PAIRS) {
+      WT_CUDA(s, cudaGraphLaunch(s->long_graph[s->parity], s->stream), "step graph");
+      s->launches += s->long_graph_launches;
+    }
   }
   if (steps - k >= 2) {
     // pairs of steps replay the captured ping-pong graph of the current parity

@@ -10,6 +10,9 @@
 #include "wt_closure.cuh"
 #include "wt_common.cuh"
 
+// step pairs captured in one long step graph
+constexpr int WT_LONG_PAIRS = 5;
+
 struct wt_solver {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -21,6 +24,9 @@ struct wt_solver {
   // of launch shape, parameters, wheels or boundary list
   cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
   int64_t graph_launches = 0;  // kernel launches inside one graph replay
+  // the same for 2 x WT_LONG_PAIRS steps: fewer graph launches per reference sample chunk
+  cudaGraphExec_t long_graph[2] = {nullptr, nullptr};
+  int64_t long_graph_launches = 0;
   uint64_t graph_gen = 0;      // bumped whenever the captured graphs are dropped (batches recapture)
   wt_dims dims{};
   wt_params params{};
