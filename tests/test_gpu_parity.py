@@ -412,3 +412,48 @@ def test_batch_matches_members_stepped_alone(gpu):
     b.destroy()
     for s in batch_members + alone:
         s.destroy()
+
+
+def test_reuploading_unchanged_geometry_keeps_the_classification(gpu):
+    """Uploads land in a staging buffer and replace the geometry only when it differs: re-uploading
+    the same flags and wall distances adds only the compare (and sdf encode) launches, and the run
+    stays bit-identical to one without the re-upload."""
+    dims = (48, 20, 16)
+    params = dict(PARAM_SETS["freeslip_reg"], precision="f16")
+    flags, sdf, wheels = scene(dims)
+    a, b = Solver(dims, params), Solver(dims, params)
+    for s in (a, b):
+        s.upload_flags(flags)
+        s.upload_sdf(sdf)
+        s.set_wheels(wheels)
+        s.step(12)
+    la, lb = a.launches, b.launches
+    a.upload_flags(flags)
+    a.upload_sdf(sdf)
+    a.step(12)
+    b.step(12)
+    assert a.launches - la == b.launches - lb + 3  # diff (flags), encode + diff (sdf)
+    np.testing.assert_array_equal(a.read_populations(), b.read_populations())
+    a.destroy()
+    b.destroy()
+
+
+def test_sdf_only_upload_refreshes_the_wall_links(gpu, oracle):
+    """New wall distances alone (same flags) change the Bouzidi fractions of the link records: a run
+    that switches distances mid-way matches the oracle doing the same."""
+    dims = (32, 14, 12)
+    params = dict(PARAM_SETS["freeslip_reg"], precision="f32")
+    flags, sdf, wheels = scene(dims)
+    sdf2 = np.where(sdf >= 0, np.clip(sdf * 0.6 + 0.2, 0.0, 2.4), sdf).astype(np.float32)
+    g = Solver(dims, params)
+    o = oracle.OracleSolver(dims, params)
+    for s in (g, o):
+        s.upload_flags(flags)
+        s.upload_sdf(sdf)
+        s.set_wheels(wheels)
+        s.step(5)
+        s.upload_sdf(sdf2)
+        s.step(5)
+    d = np.abs(g.read_populations().astype(np.float64) - o.current.astype(np.float64))
+    assert d.max() <= 2e-5, d.max()
+    g.destroy()

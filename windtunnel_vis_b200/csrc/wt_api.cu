@@ -11,6 +11,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "wt_internal.h"
@@ -63,20 +64,22 @@ bool dims_ok(const wt_dims* d) {
 int64_t bytes_for(const wt_dims* d, int prec) {
   const int64_t n = (int64_t)d->nx * d->ny * d->nz;
   const int64_t q = d->nz > 1 ? 19 : 9;
-  // 2 population buffers + flags + sdf + class byte + half4 velocity + meanA + meanB
-  return n * (2 * q * (int64_t)elem_bytes(prec) + 4 + 4 + 1 + 8 + 16 + 4);
+  // 2 population buffers + flags + sdf + upload stage + class byte + half4 velocity + meanA + meanB
+  return n * (2 * q * (int64_t)elem_bytes(prec) + 4 + 4 + 4 + 1 + 8 + 16 + 4);
 }
 
 void free_all(wt_solver* s) {
   void* bufs[] = {s->f[0], s->f[1], s->flags, s->sdf, s->cls, s->vel, s->vel_f32, s->meanA, s->meanB,
                   s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count,
                   s->bcell, s->brec, s->bgam, s->vox_pos, s->vox_idx, s->vox_info,
-                  s->dvort, s->dstat, s->dmean, s->exp_buf, s->probe_buf, s->closure_dev};
+                  s->dvort, s->dstat, s->dmean, s->exp_buf, s->probe_buf, s->closure_dev, s->stage,
+                  s->diff_dev};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->result_host) cudaFreeHost(s->result_host);
   if (s->err_host) cudaFreeHost(s->err_host);
   if (s->bnd_count_host) cudaFreeHost(s->bnd_count_host);
+  if (s->diff_host) cudaFreeHost(s->diff_host);
   for (auto& g : s->step_graph)
     if (g) cudaGraphExecDestroy(g);
   for (auto& g : s->long_graph)
@@ -116,6 +119,15 @@ __global__ void k_encode_sdf(uint32_t* __restrict__ buf, size_t n) {
     const float v = __uint_as_float(buf[i]);
     buf[i] = v >= 0.0f ? ~__float_as_uint(v) : 0u;  // negative or NaN -> unknown
   }
+}
+
+// *out |= 1 if a and b differ anywhere
+__global__ void k_diff_words(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b, size_t n,
+                             uint32_t* __restrict__ out) {
+  bool d = false;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    d = d || a[i] != b[i];
+  if (__syncthreads_or(d) && threadIdx.x == 0) atomicOr(out, 1u);
 }
 
 __global__ void k_clear_stats(float4* __restrict__ meanA, float* __restrict__ meanB, size_t n) {
@@ -409,13 +421,41 @@ int wt_clear_stats(wt_solver* s) {
 
 int64_t wt_step_count(const wt_solver* s) { return s ? s->step_count : -1; }
 
+// Compares the staged upload with *cur on the device; when they differ the stage becomes the
+// current buffer (the old one becomes the stage) and `changed` is set.
+int commit_stage(wt_solver* s, uint32_t** cur, bool* changed, const char* what) {
+  WT_CUDA(s, cudaMemsetAsync(s->diff_dev, 0, 4, s->stream), what);
+  k_diff_words<<<grid_for(s->n), 256, 0, s->stream>>>(s->stage, *cur, s->n, s->diff_dev);
+  s->launches++;
+  WT_CUDA(s, cudaGetLastError(), what);
+  WT_CUDA(s, cudaMemcpyAsync(s->diff_host, s->diff_dev, 4, cudaMemcpyDeviceToHost, s->stream), what);
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), what);
+  *changed = *s->diff_host != 0u;
+  if (*changed) std::swap(*cur, s->stage);
+  return WT_OK;
+}
+
+int ensure_stage(wt_solver* s) {
+  if (s->stage) return WT_OK;
+  if (cudaMalloc((void**)&s->stage, s->n * 4) != cudaSuccess || cudaMalloc((void**)&s->diff_dev, 4) != cudaSuccess ||
+      cudaMallocHost((void**)&s->diff_host, 4) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(s, WT_E_OOM, "upload staging buffer");
+  }
+  return WT_OK;
+}
+
 int wt_upload_flags(wt_solver* s, const uint32_t* flags, int64_t n) {
   if (!s || !flags) return WT_E_INVALID;
   if ((size_t)n != s->n) return fail(s, WT_E_INVALID, "wt_upload_flags: n != nx*ny*nz");
   DeviceGuard g(s->device);
-  WT_CUDA(s, cudaMemcpyAsync(s->flags, flags, s->n * 4, cudaMemcpyHostToDevice, s->stream), "upload flags");
-  WT_CUDA(s, cudaStreamSynchronize(s->stream), "upload flags");
-  s->cls_dirty = true;
+  int rc = ensure_stage(s);
+  if (rc) return rc;
+  WT_CUDA(s, cudaMemcpyAsync(s->stage, flags, s->n * 4, cudaMemcpyHostToDevice, s->stream), "upload flags");
+  bool changed = false;
+  rc = commit_stage(s, &s->flags, &changed, "upload flags");
+  if (rc) return rc;
+  if (changed) s->cls_dirty = true;
   return WT_OK;
 }
 
@@ -423,11 +463,18 @@ int wt_upload_sdf(wt_solver* s, const float* d, int64_t n) {
   if (!s || !d) return WT_E_INVALID;
   if ((size_t)n != s->n) return fail(s, WT_E_INVALID, "wt_upload_sdf: n != nx*ny*nz");
   DeviceGuard g(s->device);
-  WT_CUDA(s, cudaMemcpyAsync(s->sdf, d, s->n * 4, cudaMemcpyHostToDevice, s->stream), "upload sdf");
-  k_encode_sdf<<<grid_for(s->n), 256, 0, s->stream>>>(s->sdf, s->n);
+  int rc = ensure_stage(s);
+  if (rc) return rc;
+  WT_CUDA(s, cudaMemcpyAsync(s->stage, d, s->n * 4, cudaMemcpyHostToDevice, s->stream), "upload sdf");
+  k_encode_sdf<<<grid_for(s->n), 256, 0, s->stream>>>(s->stage, s->n);
   s->launches++;
   WT_CUDA(s, cudaGetLastError(), "encode sdf");
-  WT_CUDA(s, cudaStreamSynchronize(s->stream), "upload sdf");
+  bool changed = false;
+  rc = commit_stage(s, &s->sdf, &changed, "upload sdf");
+  if (rc) return rc;
+  // the wall distances set the Bouzidi fractions of the link records, and the graphs hold the
+  // buffer's address
+  if (changed) s->tab_dirty = true;
   return WT_OK;
 }
 

@@ -42,6 +42,11 @@ struct wt_solver {
   bool pending_init = true;
   uint32_t* flags = nullptr;
   uint32_t* sdf = nullptr;
+  // uploads land here first and replace flags / sdf only when their content differs, so that
+  // re-uploading unchanged geometry keeps the classification and the captured graphs
+  uint32_t* stage = nullptr;
+  uint32_t* diff_dev = nullptr;   // device word: the staged words differ from the current ones
+  uint32_t* diff_host = nullptr;  // pinned copy
   uint8_t* cls = nullptr;
   bool cls_dirty = true;
   bool tab_dirty = false;  // link records need a rebuild (parameters or wheels changed)
