@@ -16,11 +16,18 @@ drives the extension declared in include/wt.h (wt_closure, wt_trainer):
 import ctypes as C
 import json
 import math
+import os
 import time
 
 import numpy as np
 
 from . import abi
+
+# A network trained by `python -m windtunnel_vis_b200.validation learned_closure --steps 16000
+# --keep 0.3 --save closure_bluff_bodies.npz` on a B200: 8 seeded bluff bodies at 512 x 256 x 256,
+# Re = 1000 on the body height, FP16 storage, Smagorinsky Cs = 0.1 in the fine runs, 15.9 M
+# samples, 3000 Adam steps of 16384 samples.
+PRETRAINED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "closure_bluff_bodies.npz")
 
 FEATURES = ("pi_xx", "pi_yy", "pi_zz", "pi_xy", "pi_xz", "pi_yz", "strain", "wall_distance", "rho", "speed")
 N_IN = abi.CLOSURE_IN

@@ -256,13 +256,15 @@ def sweep_cases(count=32):
     return out
 
 
-def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, re_l=2e4, target_tris=200_000):
+def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, re_l=2e4, target_tris=200_000,
+                closure=None):
     """Runs the sweep of sweep_cases as one batch (windtunnel_vis_b200.solver.Batch): every tunnel
     voxelizes the vehicle body at its yaw (moving belt, rotating wheels, Smagorinsky LES, FP16),
     then all advance `steps` lattice updates together. Reports the aggregate MLUPS (device time
     of the batch steps) and each case's mean C_D / C_L over the second half; with compare_alone,
     the same cases stepped one tunnel at a time (each with its own CUDA graphs) for the speed-up
-    and the per-case C_D, which must agree exactly (the batch replays the same kernels)."""
+    and the per-case C_D, which must agree exactly (the batch replays the same kernels). `closure`
+    (a network, see windtunnel_vis_b200.closure) replaces Smagorinsky in every tunnel."""
     import torch
 
     from . import mesh as Mh
@@ -283,6 +285,8 @@ def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, 
             M16, _, full = Mh.placement_matrix(p, lo, hi, dims, dict(mode="ground", lengthFrac=1 / 3, diamFrac=0.3,
                                                                      xFrac=0.34, yawDeg=yaw, rideCells=0.08 * body_h))
             info = s.voxelize(p, idx, M16, Mh.grid_wheels(wheels, full))
+            if closure is not None:
+                s.set_closure(closure)
             frontal.append(max(info["frontal"], 1))
             solvers.append(s)
         return solvers, frontal
@@ -321,7 +325,8 @@ def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, 
         torch.cuda.synchronize()  # the batch stream is not torch's: wait before the end event
 
     ms, res = run(step_batch, batch.sample, frontal)
-    out = {"id": "batch_sweep", "tunnels": count, "cells": cells, "steps": steps, "batch_ms": ms,
+    out = {"id": "batch_sweep", "tunnels": count, "cells": cells, "steps": steps, "closure": closure is not None,
+           "batch_ms": ms,
            "batch_mlups": cells * steps / (ms * 1e-3) / 1e6, "cases": res}
     batch.destroy()
     for s in solvers:
@@ -369,6 +374,8 @@ def main(argv=None):
     ap.add_argument("--keep", type=float, default=0.4)
     ap.add_argument("--re", type=float, default=1000.0)
     ap.add_argument("--save", default=None, help="learned_closure: write the trained network (.npz)")
+    ap.add_argument("--closure", default=None,
+                    help="batch_sweep: a network (.npz) or 'pretrained' in place of Smagorinsky in every tunnel")
     a = ap.parse_args(argv)
     if a.case == "learned_closure":
         from . import closure as CL
@@ -387,7 +394,12 @@ def main(argv=None):
     elif a.case == "vehicle":
         r = vehicle(solver_factory, a.precision, a.steps)
     elif a.case == "batch_sweep":
-        r = batch_sweep(a.steps, compare_alone=True)
+        model = None
+        if a.closure:
+            from . import closure as CL
+
+            model = CL.load(CL.PRETRAINED if a.closure == "pretrained" else a.closure)
+        r = batch_sweep(a.steps, compare_alone=True, closure=model)
     else:
         r = CASES[a.case](solver_factory, a.valscale)
     r.pop("series", None)
