@@ -14,6 +14,8 @@
 //
 // This translation unit is compiled with -fmad=false: every f32 expression is evaluated
 // operation by operation, so the flags are bit-identical to the f32 CPU restatement.
+#include <climits>
+
 #include "wt_internal.h"
 
 namespace wt {
@@ -219,13 +221,47 @@ __device__ __forceinline__ float3 closest_pt(float3 p, float3 a, float3 b, float
   return add3(add3(a, mul3(ab, vb * den)), mul3(ac, vc * den));
 }
 
-// 5. wall distances of cell centres within 2.5 cells (wgslVoxel.ts:205-265). Lanes of a warp
-// take different surface samples of one triangle; each sample scans its 5x5x5 neighbourhood.
+// 5. wall distances of cell centres within 2.5 cells (wgslVoxel.ts:205-265). The reference's set:
+// each surface sample p of a triangle (a (steps+1) x (steps+2) / 2 barycentric grid) scans the
+// 5 x 5 x 5 cells around floor(p), and every scanned cell whose centre lies within 2.5 of the
+// triangle gets that exact distance (min over triangles via atomicMax of ~bits). The distance
+// does not depend on which sample reached the cell, so the result is the union of the boxes,
+// each cell evaluated once:
+//   - one warp per triangle; the floor cells of its samples are marked in a bitmap of 32-bit rows
+//     (x in bits, one row per (y, z)) over their bounding box widened by 2, which is then dilated
+//     by +-2 along x (shifts), y and z (row ORs), and every set cell is evaluated once;
+//   - triangles whose widened box exceeds 32 cells along x or 256 rows, and 2-D grids, scan every
+//     sample's box as the reference does (atomicMax makes repeated cells harmless).
+constexpr int SDF_ROWS = 256;  // bitmap rows per warp
+
+__device__ __forceinline__ void tri_sample(uint32_t s, uint32_t steps, float3 a, float3 e1, float3 e2, float fs,
+                                           float3& p) {
+  // decode the sample index into (i, j), j <= steps - i, rows of length steps + 1 - i
+  uint32_t i = 0, rem = s;
+  while (rem >= steps + 1 - i) {
+    rem -= steps + 1 - i;
+    i++;
+  }
+  p = add3(add3(a, mul3(e1, (float)i / fs)), mul3(e2, (float)rem / fs));
+}
+
+__device__ __forceinline__ void sdf_cell(const VP& V, int qx, int qy, int qz, float3 a, float3 b, float3 c,
+                                         uint32_t* __restrict__ sdf) {
+  if (qx < 0 || qy < 0 || qz < 0 || qx >= V.nx || qy >= V.ny || qz >= V.nz) return;
+  const float3 ctr = make_float3((float)qx + 0.5f, (float)qy + 0.5f, (float)qz + 0.5f);
+  const float d = len3(sub3(ctr, closest_pt(ctr, a, b, c)));
+  if (d > 2.5f) return;
+  atomicMax(&sdf[V.cell(qx, qy, qz)], ~__float_as_uint(d));
+}
+
 __global__ void __launch_bounds__(WARPS * 32) k_sdf(const VP V, const float* __restrict__ pos,
                                                     const uint32_t* __restrict__ idx, int64_t ntri,
                                                     uint32_t* __restrict__ sdf) {
-  const int lane = threadIdx.x & 31;
-  for (int64_t t = (int64_t)blockIdx.x * WARPS + (threadIdx.x >> 5); t < ntri; t += (int64_t)gridDim.x * WARPS) {
+  __shared__ uint32_t bm[WARPS][2][SDF_ROWS];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t* rows = bm[w][0];
+  uint32_t* tmp = bm[w][1];
+  for (int64_t t = (int64_t)blockIdx.x * WARPS + w; t < ntri; t += (int64_t)gridDim.x * WARPS) {
     const float3 a = vtx(V, pos, idx, 3 * t), b = vtx(V, pos, idx, 3 * t + 1), c = vtx(V, pos, idx, 3 * t + 2);
     const float3 e1 = sub3(b, a), e2 = sub3(c, a);
     if (len3(cross3(e1, e2)) < 1e-12f) continue;
@@ -234,30 +270,84 @@ __global__ void __launch_bounds__(WARPS * 32) k_sdf(const VP V, const float* __r
     const float fs = (float)steps;
     const bool is2D = V.nz == 1;
     const uint32_t total = (steps + 1) * (steps + 2) / 2;
+    // bounding box of the samples' floor cells
+    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
     for (uint32_t s = lane; s < total; s += 32) {
-      // decode the sample index into (i, j), j <= steps - i, rows of length steps + 1 - i
-      uint32_t i = 0, rem = s;
-      while (rem >= steps + 1 - i) {
-        rem -= steps + 1 - i;
-        i++;
-      }
-      const uint32_t j = rem;
-      const float3 p = add3(add3(a, mul3(e1, (float)i / fs)), mul3(e2, (float)j / fs));
-      if (is2D && fabsf(p.z - 0.5f) > 2.5f) continue;
-      const int bx = (int)floorf(p.x), by = (int)floorf(p.y), bz = (int)floorf(p.z);
-      for (int dz = -2; dz <= 2; dz++) {
-        if (is2D && dz != 0) continue;
-        for (int dy = -2; dy <= 2; dy++)
-          for (int dx = -2; dx <= 2; dx++) {
-            const int qx = bx + dx, qy = by + dy, qz = is2D ? 0 : bz + dz;
-            if (qx < 0 || qy < 0 || qz < 0 || qx >= V.nx || qy >= V.ny || qz >= V.nz) continue;
-            const float3 ctr = make_float3((float)qx + 0.5f, (float)qy + 0.5f, (float)qz + 0.5f);
-            const float d = len3(sub3(ctr, closest_pt(ctr, a, b, c)));
-            if (d > 2.5f) continue;
-            atomicMax(&sdf[V.cell(qx, qy, qz)], ~__float_as_uint(d));
-          }
+      float3 p;
+      tri_sample(s, steps, a, e1, e2, fs, p);
+      const int f[3] = {(int)floorf(p.x), (int)floorf(p.y), (int)floorf(p.z)};
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        lo[k] = min(lo[k], f[k]);
+        hi[k] = max(hi[k], f[k]);
       }
     }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      lo[k] = __reduce_min_sync(0xffffffffu, lo[k]);
+      hi[k] = __reduce_max_sync(0xffffffffu, hi[k]);
+    }
+    const int ox = lo[0] - 2, oy = lo[1] - 2, oz = lo[2] - 2;
+    const int lx = hi[0] - lo[0] + 5, ly = hi[1] - lo[1] + 5, lz = hi[2] - lo[2] + 5;
+    if (is2D || lx > 32 || ly * lz > SDF_ROWS) {
+      // the reference's scan: every sample's 5 x 5 x 5 (2-D: 5 x 5) box
+      for (uint32_t s = lane; s < total; s += 32) {
+        float3 p;
+        tri_sample(s, steps, a, e1, e2, fs, p);
+        if (is2D && fabsf(p.z - 0.5f) > 2.5f) continue;
+        const int bx = (int)floorf(p.x), by = (int)floorf(p.y), bz = (int)floorf(p.z);
+        for (int dz = -2; dz <= 2; dz++) {
+          if (is2D && dz != 0) continue;
+          for (int dy = -2; dy <= 2; dy++)
+            for (int dx = -2; dx <= 2; dx++) sdf_cell(V, bx + dx, by + dy, is2D ? 0 : bz + dz, a, b, c, sdf);
+        }
+      }
+      continue;
+    }
+    const int nrow = ly * lz;
+    for (int r = lane; r < nrow; r += 32) rows[r] = 0u;
+    __syncwarp();
+    for (uint32_t s = lane; s < total; s += 32) {
+      float3 p;
+      tri_sample(s, steps, a, e1, e2, fs, p);
+      const int fx = (int)floorf(p.x) - ox, fy = (int)floorf(p.y) - oy, fz = (int)floorf(p.z) - oz;
+      atomicOr(&rows[fy + ly * fz], 1u << fx);
+    }
+    __syncwarp();
+    // dilate by +-2: x within each row, then y, then z (through the second buffer)
+    const uint32_t xmask = lx == 32 ? 0xffffffffu : ((1u << lx) - 1u);
+    for (int r = lane; r < nrow; r += 32) {
+      const uint32_t v = rows[r];
+      tmp[r] = (v | (v << 1) | (v << 2) | (v >> 1) | (v >> 2)) & xmask;
+    }
+    __syncwarp();
+    for (int r = lane; r < nrow; r += 32) {
+      const int y = r % ly, z = r / ly;
+      uint32_t v = 0u;
+      for (int d = -2; d <= 2; d++)
+        if (y + d >= 0 && y + d < ly) v |= tmp[(y + d) + ly * z];
+      rows[r] = v;
+    }
+    __syncwarp();
+    for (int r = lane; r < nrow; r += 32) {
+      const int y = r % ly, z = r / ly;
+      uint32_t v = 0u;
+      for (int d = -2; d <= 2; d++)
+        if (z + d >= 0 && z + d < lz) v |= rows[y + ly * (z + d)];
+      tmp[r] = v;
+    }
+    __syncwarp();
+    // every cell of the union once
+    for (int r = lane; r < nrow; r += 32) {
+      uint32_t v = tmp[r];
+      const int qy = oy + r % ly, qz = oz + r / ly;
+      while (v) {
+        const int bit = __ffs(v) - 1;
+        v &= v - 1u;
+        sdf_cell(V, ox + bit, qy, qz, a, b, c, sdf);
+      }
+    }
+    __syncwarp();
   }
 }
 
