@@ -457,3 +457,34 @@ def test_sdf_only_upload_refreshes_the_wall_links(gpu, oracle):
     d = np.abs(g.read_populations().astype(np.float64) - o.current.astype(np.float64))
     assert d.max() <= 2e-5, d.max()
     g.destroy()
+
+
+@pytest.mark.parametrize("prec", ["f32", "f16"])
+def test_zero_weight_means_follow_the_oracle_with_non_finite_cells(gpu, oracle, prec):
+    """With emaAlpha = 0 the sampling pass leaves the means of finite cells untouched and writes
+    them only where the sample is not finite (0 x NaN = NaN), as the reference's mix() does: means
+    after a sample of populations holding NaN and Inf cells match the oracle's."""
+    dims = (32, 14, 12)
+    params = dict(PARAM_SETS["freeslip_reg"], precision=prec, emaAlpha=0.0)
+    g, o, flags = _pair(oracle, dims, params)
+    g.step(4)
+    o.step(4)
+    pops = g.read_populations().copy()
+    n = dims[0] * dims[1] * dims[2]
+    fluid = np.flatnonzero(flags == 0)
+    bad = fluid[[7, 300, 999]]
+    pops[1 * n + bad[0]] = np.nan
+    pops[2 * n + bad[1]] = np.inf
+    pops[5 * n + bad[2]] = -np.inf
+    g.write_populations(pops)
+    o.a[:] = pops
+    g.sample()
+    o.sample()
+    ma, mb = g.read_means()
+    ma, mb = ma.reshape(-1, 4), np.asarray(mb).ravel()
+    oa, ob = o.meanA.reshape(-1, 4), o.meanB
+    assert np.array_equal(np.isnan(ma), np.isnan(oa)) and np.array_equal(np.isnan(mb), np.isnan(ob))
+    assert np.isnan(ma[bad]).any(axis=1).all()
+    ok = ~np.isnan(oa)
+    assert np.array_equal(ma[ok], oa[ok])
+    g.destroy()

@@ -1696,17 +1696,25 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
       return (int64_t)cell_id(x, y, z, NX, NY);
     };
     float out[4] = {0.f, 0.f, 0.f, 1.f};
-    // every load of the cell is issued before the first branch: one memory round trip per cell
-    const uint32_t fl = flags[idx];
-    const bool links = cls == nullptr || (cls[idx] & CLS_NEAR_SOLID) != 0;
-    float4 m = meanA[idx];
-    const float mb = meanB[idx];
+    // every load of the cell is issued before the first branch: one memory round trip per cell.
+    // With the class byte, the cell's own solid test reads it (1 B) instead of the flags (4 B).
+    const uint8_t cl = cls != nullptr ? cls[idx] : (uint8_t)0;
+    const bool solid = cls != nullptr ? (cl & CLS_SOLID) != 0 : flags[idx] != 0u;
+    const bool links = cls == nullptr || (cl & CLS_NEAR_SOLID) != 0;
+    // EMA: with a = 0, m (1 - a) + v a leaves a fluid cell's means unchanged unless v or |u|^2 is
+    // not finite (0 x NaN = NaN); they are then read and written only in that case
+    float4 m = make_float4(0.f, 0.f, 0.f, 0.f);
+    float mb = 0.0f;
+    if (a != 0.0f || solid) {
+      m = meanA[idx];
+      mb = meanB[idx];
+    }
     R f[Q];
     static_for<Q>([&](auto I) {
       constexpr int i = I;
       f[i] = S::ld(fin, (size_t)i * N + idx, (R)Wc<L, i>::v);
     });
-    if (fl == 0u) {
+    if (!solid) {
       R rho = f[0], jx = 0, jy = 0, jz = 0;
       static_for<Q>([&](auto I) {
         constexpr int i = I;
@@ -1780,12 +1788,20 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
         accNref++;
       }
       accNan += bad ? 1u : 0u;
-      m.x = m.x * (1.0f - a) + out[0] * a;
-      m.y = m.y * (1.0f - a) + out[1] * a;
-      m.z = m.z * (1.0f - a) + out[2] * a;
-      m.w = m.w * (1.0f - a) + out[3] * a;
-      meanA[idx] = m;
-      meanB[idx] = mb * (1.0f - a) + (float)uu * a;
+      const bool finite = isfinite(out[0]) && isfinite(out[1]) && isfinite(out[2]) && isfinite(out[3]) &&
+                          isfinite((float)uu);
+      if (a != 0.0f || !finite) {
+        if (a == 0.0f) {
+          m = meanA[idx];
+          mb = meanB[idx];
+        }
+        m.x = m.x * (1.0f - a) + out[0] * a;
+        m.y = m.y * (1.0f - a) + out[1] * a;
+        m.z = m.z * (1.0f - a) + out[2] * a;
+        m.w = m.w * (1.0f - a) + out[3] * a;
+        meanA[idx] = m;
+        meanB[idx] = mb * (1.0f - a) + (float)uu * a;
+      }
     } else {
       // density extrapolated into the solid from fluid face neighbours (wgslLbm.ts:460-466)
       R rs = 0, rn = 0;
