@@ -326,7 +326,7 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
   const size_t fbytes = (size_t)s->q * s->n * s->pop_elem;
   // one macro block per 256 cells up to 4096 blocks (several cells per thread beyond: the block
   // reductions amortise and the final reduce reads at most 256 KB), one 64-byte partial each
-  s->partial_blocks = (int)std::min<size_t>((s->n + 255) / 256, 65536);  // one cell per thread up to 16.8 M cells
+  s->partial_blocks = (int)std::min<size_t>((s->n + 255) / 256, 4096);
   bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
             create_priority_stream(&s->aux) == cudaSuccess &&
             cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
