@@ -1031,7 +1031,48 @@ bool batch_graph_current(const wt_batch* b) {
   return true;
 }
 
-// One graph for two steps of every member: each member's step kernels hang off a fork from the
+// Whether the batch's steps fuse: every member takes the batch kernel with the same storage and
+// collision, and the table holds them all.
+bool batch_fused(const wt_batch* b) {
+  if (b->m.size() > (size_t)wt::BATCH_MAX_FUSED) return false;
+  for (const wt_solver* s : b->m)
+    if (!wt::batch_fusable(s) || s->prec != b->m[0]->prec || s->kp.collision != b->m[0]->kp.collision) return false;
+  return true;
+}
+
+// One step of every member with the bulk rows of all of them in one launch of the batch kernel on
+// the batch stream; each member's face rows and wall cells run on its auxiliary stream alongside,
+// and join back before the next step.
+cudaError_t batch_fused_step(wt_batch* b, int half) {
+  wt::BatchTable tab;
+  std::memset(&tab, 0, sizeof tab);
+  tab.count = (uint32_t)b->m.size();
+  uint32_t tiles = 0;
+  cudaError_t e = cudaSuccess;
+  for (size_t k = 0; k < b->m.size() && e == cudaSuccess; k++) {
+    wt_solver* s = b->m[k];
+    const int p = s->parity ^ half;
+    e = wt::launch_aux_kernels(s, s->f[p], s->f[p ^ 1], b->stream);
+    wt::BatchTunnel& t = tab.t[k];
+    t.P = s->kp;
+    t.fin = s->f[p];
+    t.fout = s->f[p ^ 1];
+    t.cls = s->cls;
+    t.gs = s->gs;
+    t.tiles_x = (uint32_t)((s->dims.nx / 2 + wt::BATCH_BX - 1) / wt::BATCH_BX);
+    t.tiles_y = (uint32_t)((s->dims.ny + wt::BATCH_BY - 1) / wt::BATCH_BY);
+    tab.tile0[k] = tiles;
+    tiles += t.tiles_x * t.tiles_y * (uint32_t)s->dims.nz;
+  }
+  tab.tile0[b->m.size()] = tiles;
+  if (e == cudaSuccess) e = wt::launch_batch_bulk(b->m[0]->prec, b->m[0]->kp.collision == 1u, tab, tiles, b->stream);
+  if (e == cudaSuccess) b->m[0]->launches++;
+  for (size_t k = 0; k < b->m.size() && e == cudaSuccess; k++) e = cudaStreamWaitEvent(b->stream, b->m[k]->ev_join, 0);
+  return e;
+}
+
+// One graph for two steps of every member. Fused batches: two steps of the batch kernel plus the
+// members' face and wall kernels. Otherwise each member's step kernels hang off a fork from the
 // batch stream, so independent tunnels run concurrently, and all join back at the end.
 int batch_capture(wt_batch* b) {
   batch_drop_graph(b);
@@ -1041,15 +1082,20 @@ int batch_capture(wt_batch* b) {
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch capture: ") + cudaGetErrorString(e));
-  e = cudaEventRecord(b->ev_fork, b->stream);
-  for (size_t k = 0; k < n && e == cudaSuccess; k++) {
-    wt_solver* s = b->m[k];
-    const int p = s->parity;
-    e = cudaStreamWaitEvent(s->stream, b->ev_fork, 0);
-    if (e == cudaSuccess) e = wt::launch_stream_collide(s, s->f[p], s->f[p ^ 1]);
-    if (e == cudaSuccess) e = wt::launch_stream_collide(s, s->f[p ^ 1], s->f[p]);
-    if (e == cudaSuccess) e = cudaEventRecord(b->ev_done[k], s->stream);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->ev_done[k], 0);
+  if (batch_fused(b)) {
+    e = batch_fused_step(b, 0);
+    if (e == cudaSuccess) e = batch_fused_step(b, 1);
+  } else {
+    e = cudaEventRecord(b->ev_fork, b->stream);
+    for (size_t k = 0; k < n && e == cudaSuccess; k++) {
+      wt_solver* s = b->m[k];
+      const int p = s->parity;
+      e = cudaStreamWaitEvent(s->stream, b->ev_fork, 0);
+      if (e == cudaSuccess) e = wt::launch_stream_collide(s, s->f[p], s->f[p ^ 1]);
+      if (e == cudaSuccess) e = wt::launch_stream_collide(s, s->f[p ^ 1], s->f[p]);
+      if (e == cudaSuccess) e = cudaEventRecord(b->ev_done[k], s->stream);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->ev_done[k], 0);
+    }
   }
   const cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
   if (e == cudaSuccess) e = e2;

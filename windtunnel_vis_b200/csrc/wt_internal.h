@@ -132,6 +132,32 @@ struct VoxelJob {
 };
 cudaError_t launch_voxelize(wt_solver* s, const VoxelJob& job);
 
+// Batches (wt_lbm.cu): the bulk rows of every tunnel of a batch in one launch. A tunnel's blocks
+// are tiles of BATCH_BX x BATCH_BY threads (two cells per thread along x); tile0 is the prefix of
+// the tile counts. The table travels by value (constant bank).
+constexpr int BATCH_MAX_FUSED = 64;
+constexpr int BATCH_BX = 64, BATCH_BY = 2;
+struct BatchTunnel {
+  wt_kparams P;
+  const void* fin;
+  void* fout;
+  const uint8_t* cls;
+  int gs;
+  uint32_t tiles_x, tiles_y, pad;
+};
+struct BatchTable {
+  uint32_t count;
+  uint32_t tile0[BATCH_MAX_FUSED + 1];
+  BatchTunnel t[BATCH_MAX_FUSED];
+};
+// whether a handle's step can join the batch kernel: D3Q19, f16 / f32, vectorised path, no closure
+bool batch_fusable(const wt_solver* s);
+// the face-row and wall-cell kernels of one step of `s` on its auxiliary stream, forked from
+// `origin`; s->ev_join is recorded at their end (the caller joins it into `origin`)
+cudaError_t launch_aux_kernels(wt_solver* s, const void* fin, void* fout, cudaStream_t origin);
+// the batch kernel over `tab` (all members: precision `prec`, collision `bgk`)
+cudaError_t launch_batch_bulk(int prec, bool bgk, const BatchTable& tab, uint32_t tiles, cudaStream_t st);
+
 // learned closure training data (wt_lbm.cu): the fine handle's current populations box-filtered
 // onto a cnx x cny x cnz grid (fine dims = 2 x coarse dims); `out` holds 11 * cnx * cny * cnz floats
 cudaError_t launch_closure_filter(wt_solver* fine, int cnx, int cny, int cnz, float* out, cudaStream_t st);

@@ -917,19 +917,17 @@ template <> struct PairIO<StF32> {
 // MINB: CTAs of 256 threads the register allocation must leave room for (0 = no constraint)
 template <int MINB> struct Bounds { static constexpr int v = MINB; };
 
-template <class L, class S, int V, int MINB, bool BGK>
-__global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(const __grid_constant__ wt_kparams P,
-                                                          const typename S::T* __restrict__ fin,
-                                                          typename S::T* __restrict__ fout,
-                                                          const uint8_t* __restrict__ cls, int gs) {
+// The V cells x0 .. x0 + V - 1 of row (iy, iz) (bulk rows only); shared by the single-tunnel
+// kernel and the batch kernel.
+template <class L, class S, int V, bool BGK>
+__device__ __forceinline__ void bulk_cells(const wt_kparams& P, const typename S::T* __restrict__ fin,
+                                           typename S::T* __restrict__ fout, const uint8_t* __restrict__ cls,
+                                           int gs, int x0, int iy, int iz) {
   typedef PairIO<S> IO;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
   constexpr int G = V / 2;  // groups of two cells collided together in f32x2 lanes
   const int NX = P.nx, NY = P.ny, NZ = P.nz;
-  const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
-  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
-  const int iz = blockIdx.z;
   if (x0 >= NX || iy >= NY) return;
   // rows on the domain faces belong to k_face_v, groups holding solid / near-solid cells to
   // k_boundary_tab (fluid cells) or to nobody (solid cells keep the rest state)
@@ -1001,6 +999,38 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
       if (clean) IO::st(ob + (ptrdiff_t)i * N, 2 * g, v, (float)Wc<L, i>::v);
     });
   }
+}
+
+template <class L, class S, int V, int MINB, bool BGK>
+__global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(const __grid_constant__ wt_kparams P,
+                                                          const typename S::T* __restrict__ fin,
+                                                          typename S::T* __restrict__ fout,
+                                                          const uint8_t* __restrict__ cls, int gs) {
+  bulk_cells<L, S, V, BGK>(P, fin, fout, cls, gs, (blockIdx.x * blockDim.x + threadIdx.x) * V,
+                           blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z);
+}
+
+// The bulk rows of every tunnel of a batch (D3Q19, two cells per thread): block b belongs to the
+// tunnel m with tile0[m] <= b < tile0[m + 1], and covers tile b - tile0[m] of its grid.
+template <class S, int MINB, bool BGK>
+__global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_batch_bulk(const __grid_constant__ BatchTable T) {
+  __shared__ uint32_t member;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    uint32_t lo = 0, hi = T.count;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (T.tile0[mid] <= blockIdx.x) lo = mid;
+      else hi = mid;
+    }
+    member = lo;
+  }
+  __syncthreads();
+  const BatchTunnel& t = T.t[member];
+  const uint32_t tile = blockIdx.x - T.tile0[member];
+  const uint32_t bx = tile % t.tiles_x, by = (tile / t.tiles_x) % t.tiles_y, bz = tile / (t.tiles_x * t.tiles_y);
+  bulk_cells<D3Q19, S, 2, BGK>(t.P, (const typename S::T*)t.fin, (typename S::T*)t.fout, t.cls, t.gs,
+                               (int)(bx * blockDim.x + threadIdx.x) * 2, (int)(by * blockDim.y + threadIdx.y),
+                               (int)bz);
 }
 
 // Rows on the domain faces (y = 0 or ny - 1, and z = 0 or nz - 1 in 3-D), vectorised like the
@@ -2286,6 +2316,56 @@ static cudaError_t macro_t(wt_solver* s) {
 cudaError_t launch_init(wt_solver* s) { WT_DISPATCH(init_t, s); }
 cudaError_t launch_stream_collide(wt_solver* s, const void* fin, void* fout) { WT_DISPATCH(sc_t, s, fin, fout); }
 cudaError_t launch_macro(wt_solver* s) { WT_DISPATCH(macro_t, s); }
+
+bool batch_fusable(const wt_solver* s) {
+  return s->is3d && (s->prec == WT_PREC_F16 || s->prec == WT_PREC_F32) && s->closure_dev == nullptr &&
+         s->dims.nx % 2 == 0 && s->gs >= 2 && s->dims.ny >= 2 && s->dims.nz >= 2 && offsets32(s) &&
+         s->solid_ok[0] && s->solid_ok[1];
+}
+
+template <class L, class S>
+static cudaError_t aux_t(wt_solver* s, const void* fin, void* fout, cudaStream_t origin) {
+  if constexpr (L::DIM == 3 && (S::PREC == WT_PREC_F16 || S::PREC == WT_PREC_F32)) {
+    cudaError_t e;
+    if ((e = cudaEventRecord(s->ev_fork, origin)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(s->aux, s->ev_fork, 0)) != cudaSuccess) return e;
+    const int fr = 2 * s->dims.ny + 2 * (s->dims.nz - 2);
+    const int runs2 = s->dims.nx / 2;
+    const int fbx = runs2 >= 128 ? 128 : ((runs2 + 31) / 32) * 32;
+    const int fby = 256 / fbx;
+    const dim3 fgrid((runs2 + fbx - 1) / fbx, (fr + fby - 1) / fby, 1);
+    k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, s->aux>>>(s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls,
+                                                         s->gs);
+    s->launches++;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (s->nbnd > 0) {
+      k_boundary_tab<L, S><<<(s->nbnd + 63) / 64, 64, 0, s->aux>>>(
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
+          (uint32_t)s->btab_cap, s->sdf, NoClosure{0});
+      s->launches++;
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaEventRecord(s->ev_join, s->aux);
+  } else {
+    return cudaErrorNotSupported;
+  }
+}
+
+cudaError_t launch_aux_kernels(wt_solver* s, const void* fin, void* fout, cudaStream_t origin) {
+  WT_DISPATCH(aux_t, s, fin, fout, origin);
+}
+
+cudaError_t launch_batch_bulk(int prec, bool bgk, const BatchTable& tab, uint32_t tiles, cudaStream_t st) {
+  const dim3 block(BATCH_BX, BATCH_BY);
+  if (prec == WT_PREC_F16) {
+    if (bgk) k_batch_bulk<StF16, 0, true><<<tiles, block, 0, st>>>(tab);
+    else k_batch_bulk<StF16, 4, false><<<tiles, block, 0, st>>>(tab);
+  } else {
+    if (bgk) k_batch_bulk<StF32, 0, true><<<tiles, block, 0, st>>>(tab);
+    else k_batch_bulk<StF32, 4, false><<<tiles, block, 0, st>>>(tab);
+  }
+  return cudaGetLastError();
+}
 
 cudaError_t launch_closure_filter(wt_solver* fine, int cnx, int cny, int cnz, float* out, cudaStream_t st) {
   const wt_solver* s = fine;
