@@ -288,6 +288,11 @@ int32_t wt_batch_size(const wt_batch* b);
 int wt_batch_step(wt_batch* b, int32_t steps);
 /* the sampling pass of every member (queued together, then read back): out has count entries */
 int wt_batch_sample(wt_batch* b, wt_stats* out);
+/* on != 0: when every member is D3Q19 with the same f16 / f32 storage and collision, no learned
+ * closure and the vectorised launch, the bulk rows of all members step in one launch of a batch
+ * kernel over a table of per-tunnel descriptors (face rows and wall cells stay per member).
+ * Default off: on a B200 the members' own kernels under one graph measured faster. */
+int wt_batch_set_fused(wt_batch* b, int32_t on);
 
 /* ---- learned LES closure (extension; no counterpart in the reference) -----------------------
  * A per-cell network replaces the Smagorinsky eddy viscosity of the collision (the reference's

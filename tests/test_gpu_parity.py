@@ -511,7 +511,7 @@ def test_fused_batch_matches_members_stepped_alone(gpu, prec):
 
     members = [make(d, p) for d, p in cases]
     alone = [make(d, p) for d, p in cases]
-    b = Batch(members)
+    b = Batch(members, fused=True)
     l0, la0 = sum(s.launches for s in members), sum(t.launches for t in alone)
     for steps in (7, 10, 1, 6):
         b.step(steps)

@@ -193,6 +193,7 @@ def _sig(lib):
         "wt_batch_size": ([S], i32),
         "wt_batch_step": ([S, i32], C.c_int),
         "wt_batch_sample": ([S, P(Stats)], C.c_int),
+        "wt_batch_set_fused": ([S, i32], C.c_int),
         "wt_set_launch": ([S, i32, i32, i32, i32], C.c_int),
         "wt_get_launch": ([S, P(i32)], C.c_int),
         "wt_autotune": ([S, i32, P(i32)], C.c_int),

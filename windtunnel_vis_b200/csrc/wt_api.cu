@@ -1004,10 +1004,13 @@ struct wt_batch {
   cudaStream_t stream = nullptr;  // capture origin and replay stream
   cudaEvent_t ev_fork = nullptr;
   std::vector<cudaEvent_t> ev_done;
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph = nullptr;       // one step pair of every member
+  cudaGraphExec_t long_graph = nullptr;  // WT_LONG_PAIRS step pairs
   std::vector<uint64_t> gens;       // member graph generations the graph was captured at
   std::vector<int> parities;        // member parities the graph was captured at
   std::vector<int64_t> per_replay;  // kernel launches of each member inside one replay
+  std::vector<int64_t> long_per_replay;
+  bool fused = false;  // wt_batch_set_fused
   std::string err;
 };
 
@@ -1021,7 +1024,9 @@ int bfail(wt_batch* b, int code, const std::string& msg) {
 
 void batch_drop_graph(wt_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->long_graph) cudaGraphExecDestroy(b->long_graph);
   b->graph = nullptr;
+  b->long_graph = nullptr;
 }
 
 bool batch_graph_current(const wt_batch* b) {
@@ -1034,7 +1039,7 @@ bool batch_graph_current(const wt_batch* b) {
 // Whether the batch's steps fuse: every member takes the batch kernel with the same storage and
 // collision, and the table holds them all.
 bool batch_fused(const wt_batch* b) {
-  if (b->m.size() > (size_t)wt::BATCH_MAX_FUSED) return false;
+  if (!b->fused || b->m.size() > (size_t)wt::BATCH_MAX_FUSED) return false;
   for (const wt_solver* s : b->m)
     if (!wt::batch_fusable(s) || s->prec != b->m[0]->prec || s->kp.collision != b->m[0]->kp.collision) return false;
   return true;
@@ -1074,8 +1079,7 @@ cudaError_t batch_fused_step(wt_batch* b, int half) {
 // One graph for two steps of every member. Fused batches: two steps of the batch kernel plus the
 // members' face and wall kernels. Otherwise each member's step kernels hang off a fork from the
 // batch stream, so independent tunnels run concurrently, and all join back at the end.
-int batch_capture(wt_batch* b) {
-  batch_drop_graph(b);
+int batch_capture_pairs(wt_batch* b, int pairs, cudaGraphExec_t* out, std::vector<int64_t>* per_replay) {
   const size_t n = b->m.size();
   std::vector<int64_t> l0(n);
   for (size_t k = 0; k < n; k++) l0[k] = b->m[k]->launches;
@@ -1083,34 +1087,52 @@ int batch_capture(wt_batch* b) {
   cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch capture: ") + cudaGetErrorString(e));
   if (batch_fused(b)) {
-    e = batch_fused_step(b, 0);
-    if (e == cudaSuccess) e = batch_fused_step(b, 1);
+    for (int k = 0; k < pairs && e == cudaSuccess; k++) {
+      e = batch_fused_step(b, 0);
+      if (e == cudaSuccess) e = batch_fused_step(b, 1);
+    }
   } else {
     e = cudaEventRecord(b->ev_fork, b->stream);
     for (size_t k = 0; k < n && e == cudaSuccess; k++) {
       wt_solver* s = b->m[k];
       const int p = s->parity;
       e = cudaStreamWaitEvent(s->stream, b->ev_fork, 0);
-      if (e == cudaSuccess) e = wt::launch_stream_collide(s, s->f[p], s->f[p ^ 1]);
-      if (e == cudaSuccess) e = wt::launch_stream_collide(s, s->f[p ^ 1], s->f[p]);
+      for (int j = 0; j < pairs && e == cudaSuccess; j++) {
+        e = wt::launch_stream_collide(s, s->f[p], s->f[p ^ 1]);
+        if (e == cudaSuccess) e = wt::launch_stream_collide(s, s->f[p ^ 1], s->f[p]);
+      }
       if (e == cudaSuccess) e = cudaEventRecord(b->ev_done[k], s->stream);
       if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->ev_done[k], 0);
     }
   }
   const cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
   if (e == cudaSuccess) e = e2;
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, graph, cudaGraphInstantiateFlagUseNodePriority);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(out, graph, cudaGraphInstantiateFlagUseNodePriority);
   if (graph) cudaGraphDestroy(graph);
   for (size_t k = 0; k < n; k++) {
-    b->per_replay[k] = b->m[k]->launches - l0[k];
+    (*per_replay)[k] = b->m[k]->launches - l0[k];
     b->m[k]->launches = l0[k];
-    b->gens[k] = b->m[k]->graph_gen;
-    b->parities[k] = b->m[k]->parity;
   }
   if (e != cudaSuccess) {
-    b->graph = nullptr;
+    *out = nullptr;
     cudaGetLastError();
     return bfail(b, WT_E_CUDA, std::string("batch capture: ") + cudaGetErrorString(e));
+  }
+  return WT_OK;
+}
+
+// the step-pair graph and the long graph, at the members' current generations and parities
+int batch_capture(wt_batch* b) {
+  batch_drop_graph(b);
+  int rc = batch_capture_pairs(b, 1, &b->graph, &b->per_replay);
+  if (!rc) rc = batch_capture_pairs(b, WT_LONG_PAIRS, &b->long_graph, &b->long_per_replay);
+  if (rc) {
+    batch_drop_graph(b);
+    return rc;
+  }
+  for (size_t k = 0; k < b->m.size(); k++) {
+    b->gens[k] = b->m[k]->graph_gen;
+    b->parities[k] = b->m[k]->parity;
   }
   return WT_OK;
 }
@@ -1156,6 +1178,7 @@ int wt_batch_create(wt_solver* const* members, int32_t count, wt_batch** out) {
   b->gens.assign(count, 0);
   b->parities.assign(count, 0);
   b->per_replay.assign(count, 0);
+  b->long_per_replay.assign(count, 0);
   b->ev_done.assign(count, nullptr);
   DeviceGuard g(b->device);
   bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
@@ -1187,6 +1210,15 @@ const char* wt_batch_last_error(const wt_batch* b) { return b ? b->err.c_str() :
 
 int32_t wt_batch_size(const wt_batch* b) { return b ? (int32_t)b->m.size() : -1; }
 
+int wt_batch_set_fused(wt_batch* b, int32_t on) {
+  if (!b) return WT_E_INVALID;
+  DeviceGuard g(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop_graph(b);
+  b->fused = on != 0;
+  return WT_OK;
+}
+
 int wt_batch_step(wt_batch* b, int32_t steps) {
   if (!b || steps < 0) return WT_E_INVALID;
   DeviceGuard g(b->device);
@@ -1213,6 +1245,11 @@ int wt_batch_step(wt_batch* b, int32_t steps) {
     if (!batch_graph_current(b)) {
       rc = batch_capture(b);
       if (rc) return rc;
+    }
+    for (; k + 2 * WT_LONG_PAIRS <= steps; k += 2 * WT_LONG_PAIRS) {
+      cudaError_t e = cudaGraphLaunch(b->long_graph, b->stream);
+      if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch graph: ") + cudaGetErrorString(e));
+      for (size_t j = 0; j < b->m.size(); j++) b->m[j]->launches += b->long_per_replay[j];
     }
     for (; k + 2 <= steps; k += 2) {
       cudaError_t e = cudaGraphLaunch(b->graph, b->stream);

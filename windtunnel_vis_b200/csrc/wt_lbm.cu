@@ -1012,10 +1012,14 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
 
 // The bulk rows of every tunnel of a batch (D3Q19, two cells per thread): block b belongs to the
 // tunnel m with tile0[m] <= b < tile0[m + 1], and covers tile b - tile0[m] of its grid.
+// The block's tunnel parameters are copied to shared memory once, so the body reads them with
+// uniform shared loads instead of indexed constant-bank loads.
 template <class S, int MINB, bool BGK>
 __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_batch_bulk(const __grid_constant__ BatchTable T) {
   __shared__ uint32_t member;
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
+  __shared__ wt_kparams sp;
+  const uint32_t tid = threadIdx.x + blockDim.x * threadIdx.y;
+  if (tid == 0) {
     uint32_t lo = 0, hi = T.count;
     while (hi - lo > 1) {
       const uint32_t mid = (lo + hi) >> 1;
@@ -1025,10 +1029,15 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_batch_bulk(const _
     member = lo;
   }
   __syncthreads();
-  const BatchTunnel& t = T.t[member];
-  const uint32_t tile = blockIdx.x - T.tile0[member];
+  const uint32_t m = member;
+  static_assert(sizeof(wt_kparams) % 4 == 0 && sizeof(wt_kparams) / 4 <= 32, "parameter block copy");
+  if (tid < sizeof(wt_kparams) / 4)
+    reinterpret_cast<uint32_t*>(&sp)[tid] = reinterpret_cast<const uint32_t*>(&T.t[m].P)[tid];
+  __syncthreads();
+  const BatchTunnel& t = T.t[m];
+  const uint32_t tile = blockIdx.x - T.tile0[m];
   const uint32_t bx = tile % t.tiles_x, by = (tile / t.tiles_x) % t.tiles_y, bz = tile / (t.tiles_x * t.tiles_y);
-  bulk_cells<D3Q19, S, 2, BGK>(t.P, (const typename S::T*)t.fin, (typename S::T*)t.fout, t.cls, t.gs,
+  bulk_cells<D3Q19, S, 2, BGK>(sp, (const typename S::T*)t.fin, (typename S::T*)t.fout, t.cls, t.gs,
                                (int)(bx * blockDim.x + threadIdx.x) * 2, (int)(by * blockDim.y + threadIdx.y),
                                (int)bz);
 }

@@ -286,7 +286,7 @@ class Batch:
     holding every member's step kernels, so small tunnels run concurrently. Members stay ordinary
     Solver objects for parameters, geometry and readback, and must outlive the batch."""
 
-    def __init__(self, solvers):
+    def __init__(self, solvers, fused=False):
         self._lib = abi.load()
         self.members = list(solvers)
         arr = (C.c_void_p * len(self.members))(*[s.handle.value for s in self.members])
@@ -295,6 +295,12 @@ class Batch:
         if rc != 0:
             raise WtError(rc, self._lib.wt_last_error(None).decode())
         self._h = h
+        if fused:
+            self.set_fused(True)
+
+    def set_fused(self, on: bool):
+        """Bulk rows of all members in one batch-kernel launch (wt_batch_set_fused)."""
+        self._check(self._lib.wt_batch_set_fused(self._h, 1 if on else 0))
 
     def _check(self, rc):
         if rc != 0:

@@ -257,7 +257,7 @@ def sweep_cases(count=32):
 
 
 def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, re_l=2e4, target_tris=200_000,
-                closure=None):
+                closure=None, fused=False):
     """Runs the sweep of sweep_cases as one batch (windtunnel_vis_b200.solver.Batch): every tunnel
     voxelizes the vehicle body at its yaw (moving belt, rotating wheels, Smagorinsky LES, FP16),
     then all advance `steps` lattice updates together. Reports the aggregate MLUPS (device time
@@ -318,7 +318,7 @@ def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, 
 
     cells = sum(d[0] * d[1] * d[2] for d, _, _ in cases)
     solvers, frontal = build()
-    batch = Batch(solvers)
+    batch = Batch(solvers, fused=fused)
 
     def step_batch(n):
         batch.step(n)
@@ -326,6 +326,7 @@ def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, 
 
     ms, res = run(step_batch, batch.sample, frontal)
     out = {"id": "batch_sweep", "tunnels": count, "cells": cells, "steps": steps, "closure": closure is not None,
+           "fused": fused,
            "batch_ms": ms,
            "batch_mlups": cells * steps / (ms * 1e-3) / 1e6, "cases": res}
     batch.destroy()
@@ -374,6 +375,7 @@ def main(argv=None):
     ap.add_argument("--keep", type=float, default=0.4)
     ap.add_argument("--re", type=float, default=1000.0)
     ap.add_argument("--save", default=None, help="learned_closure: write the trained network (.npz)")
+    ap.add_argument("--fused", action="store_true", help="batch_sweep: bulk rows of all tunnels in one kernel")
     ap.add_argument("--closure", default=None,
                     help="batch_sweep: a network (.npz) or 'pretrained' in place of Smagorinsky in every tunnel")
     a = ap.parse_args(argv)
@@ -399,7 +401,7 @@ def main(argv=None):
             from . import closure as CL
 
             model = CL.load(CL.PRETRAINED if a.closure == "pretrained" else a.closure)
-        r = batch_sweep(a.steps, compare_alone=True, closure=model)
+        r = batch_sweep(a.steps, compare_alone=True, closure=model, fused=a.fused)
     else:
         r = CASES[a.case](solver_factory, a.valscale)
     r.pop("series", None)
