@@ -257,14 +257,15 @@ def sweep_cases(count=32):
 
 
 def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, re_l=2e4, target_tris=200_000,
-                closure=None, fused=False):
+                closure=None, fused=False, autotune=True):
     """Runs the sweep of sweep_cases as one batch (windtunnel_vis_b200.solver.Batch): every tunnel
     voxelizes the vehicle body at its yaw (moving belt, rotating wheels, Smagorinsky LES, FP16),
     then all advance `steps` lattice updates together. Reports the aggregate MLUPS (device time
     of the batch steps) and each case's mean C_D / C_L over the second half; with compare_alone,
     the same cases stepped one tunnel at a time (each with its own CUDA graphs) for the speed-up
     and the per-case C_D, which must agree exactly (the batch replays the same kernels). `closure`
-    (a network, see windtunnel_vis_b200.closure) replaces Smagorinsky in every tunnel."""
+    (a network, see windtunnel_vis_b200.closure) replaces Smagorinsky in every tunnel; with
+    `autotune` the project's launch tuner picks each tunnel's block shape and cells per thread."""
     import torch
 
     from . import mesh as Mh
@@ -287,6 +288,8 @@ def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, 
             info = s.voxelize(p, idx, M16, Mh.grid_wheels(wheels, full))
             if closure is not None:
                 s.set_closure(closure)
+            elif autotune:
+                s.autotune(6)
             frontal.append(max(info["frontal"], 1))
             solvers.append(s)
         return solvers, frontal
@@ -326,7 +329,7 @@ def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, 
 
     ms, res = run(step_batch, batch.sample, frontal)
     out = {"id": "batch_sweep", "tunnels": count, "cells": cells, "steps": steps, "closure": closure is not None,
-           "fused": fused,
+           "fused": fused, "autotune": autotune and closure is None,
            "batch_ms": ms,
            "batch_mlups": cells * steps / (ms * 1e-3) / 1e6, "cases": res}
     batch.destroy()
