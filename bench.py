@@ -11,7 +11,7 @@ the macro pass (momentum-exchange force, FP64 sums) and the 64-byte statistics r
 `value` = lattice updates (all ranks) / device time of the timed steps (CUDA events, max over
 ranks). `e2e` = the same metric through the public API with host buffers: every step uploads the
 body's flags and wall distances from pinned host memory, runs stepAndSample(50) and reads the
-velocity field back. `roofline` = algorithmic bytes of one stream-collide launch
+velocity field back in its storage format (rgba16float, 8 B per cell) into pinned memory. `roofline` = algorithmic bytes of one stream-collide launch
 (19 x (2 + 2) B per cell) over its mean duration, timed with events on the solver's stream.
 Multi-GPU: independent tunnel replicas, one per rank (no data-path collective).
 """
@@ -431,8 +431,8 @@ def run_ours(args, rank, world, local_rank, dist):
     # end to end through the public API with host buffers
     fl_h = torch.from_numpy(flags).pin_memory()
     sd_h = torch.from_numpy(sdf).pin_memory()
-    vel_h = torch.empty((n, 4), dtype=torch.float32).pin_memory()
-    vel_bytes = n * 16
+    vel_h = torch.empty((n, 4), dtype=torch.float16).pin_memory()
+    vel_bytes = n * 8
     e2e_steps = max(2, min(args.steps, 10))
     s.step_and_sample(CHUNK)
     torch.cuda.synchronize()
@@ -442,7 +442,7 @@ def run_ours(args, rank, world, local_rank, dist):
         s.upload_flags(fl_h.numpy())
         s.upload_sdf(sd_h.numpy())
         st = s.step_and_sample(CHUNK)
-        s.read_velocity(vel_h.numpy())
+        s.read_velocity_half(vel_h.numpy())
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(dist, e2e_s)
     e2e = replica_mlups(world, n, CHUNK * e2e_steps, e2e_s * 1e3)

@@ -217,6 +217,9 @@ int wt_write_populations(wt_solver* s, const void* in, int64_t bytes);
 /* velTex of the last sample (wgslLbm.ts:439-468): (ux, uy, uz, rho) per cell, stored as FP16 like
  * the reference's rgba16float texture, returned as f32. */
 int wt_read_velocity(wt_solver* s, float* out4, int64_t n);
+/* The same field in its storage format, the reference texture's rgba16float: 4 IEEE binary16 per
+ * cell (8 bytes), copied without widening. */
+int wt_read_velocity_half4(wt_solver* s, void* out_half4, int64_t n);
 /* meanA (ux, uy, uz, rho EMA, 4 f32 per cell) and meanB (<u.u> EMA, 1 f32 per cell). */
 int wt_read_means(wt_solver* s, float* mean4, float* meanb, int64_t n);
 

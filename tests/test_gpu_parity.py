@@ -527,3 +527,18 @@ def test_fused_batch_matches_members_stepped_alone(gpu, prec):
     b.destroy()
     for s in members + alone:
         s.destroy()
+
+
+def test_half4_velocity_readback_is_the_storage_format(gpu):
+    """wt_read_velocity_half4 returns the stored binary16 field; wt_read_velocity widens it."""
+    dims = (32, 14, 12)
+    g = Solver(dims, dict(PARAM_SETS["freeslip_reg"], precision="f16"))
+    flags, sdf, wheels = scene(dims)
+    g.upload_flags(flags)
+    g.upload_sdf(sdf)
+    g.step_and_sample(6)
+    h = g.read_velocity_half()
+    f = g.read_velocity()
+    assert h.dtype == np.float16 and h.shape == f.shape
+    np.testing.assert_array_equal(h.astype(np.float32), f)
+    g.destroy()

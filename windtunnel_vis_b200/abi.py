@@ -178,6 +178,7 @@ def _sig(lib):
         "wt_read_populations": ([S, v, i64], C.c_int),
         "wt_write_populations": ([S, v, i64], C.c_int),
         "wt_read_velocity": ([S, v, i64], C.c_int),
+        "wt_read_velocity_half4": ([S, v, i64], C.c_int),
         "wt_read_means": ([S, v, v, i64], C.c_int),
         "wt_advect_tracers": ([S, P(TracerParams)], C.c_int),
         "wt_read_tracers": ([S, v, i64, v, i64], C.c_int),

@@ -727,6 +727,14 @@ int wt_read_velocity(wt_solver* s, float* out4, int64_t n) {
   return WT_OK;
 }
 
+int wt_read_velocity_half4(wt_solver* s, void* out_half4, int64_t n) {
+  if (!s || !out_half4 || (size_t)n != s->n) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  WT_CUDA(s, cudaMemcpyAsync(out_half4, s->vel, s->n * 8, cudaMemcpyDeviceToHost, s->stream), "read velocity");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "read velocity");
+  return WT_OK;
+}
+
 int wt_read_means(wt_solver* s, float* mean4, float* meanb, int64_t n) {
   if (!s || (size_t)n != s->n) return WT_E_INVALID;
   DeviceGuard g(s->device);

@@ -205,6 +205,16 @@ class Solver:
         self._check(self._lib.wt_read_velocity(self._h, _ptr(out), self.n))
         return out
 
+    def read_velocity_half(self, out=None):
+        """The velocity field in its storage format: (n, 4) float16 (ux, uy, uz, rho), the
+        reference's rgba16float texture. `out` (optional): a C-contiguous float16 array of that
+        shape, e.g. a view of pinned host memory."""
+        if out is None:
+            out = np.empty((self.n, 4), np.float16)
+        assert out.dtype == np.float16 and out.shape == (self.n, 4) and out.flags["C_CONTIGUOUS"]
+        self._check(self._lib.wt_read_velocity_half4(self._h, _ptr(out), self.n))
+        return out
+
     def read_means(self):
         a = np.empty((self.n, 4), np.float32)
         b = np.empty(self.n, np.float32)
