@@ -1001,16 +1001,11 @@ __device__ __forceinline__ void bulk_cells(const wt_kparams& P, const typename S
   }
 }
 
-// Launched with programmatic stream serialization: every block lets the next launch in the stream
-// be scheduled (launch_dependents) and waits for the previous one to complete and flush before
-// its first load (griddepcontrol.wait is a no-op for an ordinary launch).
 template <class L, class S, int V, int MINB, bool BGK>
 __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(const __grid_constant__ wt_kparams P,
                                                           const typename S::T* __restrict__ fin,
                                                           typename S::T* __restrict__ fout,
                                                           const uint8_t* __restrict__ cls, int gs) {
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  asm volatile("griddepcontrol.wait;" ::: "memory");
   bulk_cells<L, S, V, BGK>(P, fin, fout, cls, gs, (blockIdx.x * blockDim.x + threadIdx.x) * V,
                            blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z);
 }
@@ -2255,25 +2250,14 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
       }
       // the bulk kernel on the main stream, concurrently with the auxiliary work
-      cudaLaunchAttribute pdl[1];
-      pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-      pdl[0].val.programmaticStreamSerializationAllowed = 1;
-      cudaLaunchConfig_t lc = {};
-      lc.gridDim = grid;
-      lc.blockDim = block;
-      lc.stream = s->stream;
-      lc.attrs = pdl;
-      lc.numAttrs = 1;
-      const typename S::T* fin_t = (const typename S::T*)fin;
-      typename S::T* fout_t = (typename S::T*)fout;
 #define WT_LAUNCH_V(VV, MB)                                                                                     \
   do {                                                                                                             \
     if (s->kp.collision == 1u)                                                                                     \
-      e = cudaLaunchKernelEx(&lc, k_stream_collide_v<L, S, VV, MB, true>, s->kp, fin_t, fout_t,                    \
-                             (const uint8_t*)s->cls, s->gs);                                                       \
+      k_stream_collide_v<L, S, VV, MB, true><<<grid, block, 0, s->stream>>>(                                       \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs);                                  \
     else                                                                                                           \
-      e = cudaLaunchKernelEx(&lc, k_stream_collide_v<L, S, VV, MB, false>, s->kp, fin_t, fout_t,                   \
-                             (const uint8_t*)s->cls, s->gs);                                                       \
+      k_stream_collide_v<L, S, VV, MB, false><<<grid, block, 0, s->stream>>>(                                      \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs);                                  \
   } while (0)
       const int mb = s->sc_kernel;
       if constexpr (L::DIM == 3) {
@@ -2308,7 +2292,6 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
       }
 #undef WT_LAUNCH_V
       s->launches++;
-      if (e != cudaSuccess) return e;
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       if (s->aux) {
         if ((e = cudaEventRecord(s->ev_join, s->aux)) != cudaSuccess) return e;
