@@ -361,10 +361,14 @@ int wt_trainer_clear(wt_trainer* t);
  *   T = <rho u u> / <rho> - u~ u~  +  <-2 nu_sgs S>   (filtered resolved stress plus the fine run's
  *       own Smagorinsky stress; < > = 2 x 2 x 2 average, u~ = <rho u> / <rho>)
  *   nu* = max(0, -sum_box dev(T) : S~ / sum_box 2 S~ : S~), S~ from central differences of u~ on the
- *       coarse grid, sums over the 3 x 3 x 3 coarse neighbourhood (cells that are themselves kept
- *       candidates). added (may be NULL) receives the number of samples appended. */
+ *       coarse grid, sums over the 3 x 3 x 3 coarse neighbourhood (see
+ *       wt_trainer_set_projection_radius) of cells with a full stencil. added (may be NULL) receives the number of samples appended. */
 int wt_trainer_add_samples(wt_trainer* t, wt_solver* fine, wt_solver* coarse, double keep, uint64_t seed,
                            int64_t* added);
+/* half-width of the projection box of later wt_trainer_add_samples calls: the sums run over
+ * (2 radius + 1)^3 coarse cells (1, the default, to 3); kept cells lie radius + 1 cells off the
+ * faces */
+int wt_trainer_set_projection_radius(wt_trainer* t, int32_t radius);
 /* host samples: x (n x 10 features), y (n targets) */
 int wt_trainer_put_samples(wt_trainer* t, const float* x, const float* y, int64_t n);
 int wt_trainer_read_samples(wt_trainer* t, int64_t offset, int64_t n, float* x, float* y);

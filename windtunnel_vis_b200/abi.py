@@ -211,6 +211,7 @@ def _sig(lib):
         "wt_trainer_clear": ([S], C.c_int),
         "wt_trainer_add_samples": ([S, S, S, C.c_double, C.c_uint64, P(i64)], C.c_int),
         "wt_trainer_put_samples": ([S, v, v, i64], C.c_int),
+        "wt_trainer_set_projection_radius": ([S, i32], C.c_int),
         "wt_trainer_read_samples": ([S, i64, i64, v, v], C.c_int),
         "wt_trainer_stats": ([S, v, v], C.c_int),
         "wt_trainer_set_model": ([S, P(Closure)], C.c_int),

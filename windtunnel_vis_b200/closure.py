@@ -147,6 +147,10 @@ class Trainer:
     def clear(self):
         self._check(self._lib.wt_trainer_clear(self._h))
 
+    def set_projection_radius(self, radius):
+        """Projection sums over (2 radius + 1)^3 coarse cells for later add_samples calls."""
+        self._check(self._lib.wt_trainer_set_projection_radius(self._h, int(radius)))
+
     def add_samples(self, fine, coarse, keep=1.0, seed=1):
         added = C.c_int64()
         self._check(self._lib.wt_trainer_add_samples(self._h, fine.handle, coarse.handle, float(keep), int(seed),
@@ -330,7 +334,7 @@ def _mean_se(tt, cd, start, horizon):
 
 def study(make=None, fine_dims=(512, 256, 256), train_bodies=8, eval_bodies=2, seed=1, re=1000.0, u=0.05,
           warm=6000, snapshots=2, every=1000, samples=1 << 24, keep=0.4, train_steps=3000, batch=16384, lr=2e-3,
-          eval_steps=16000, chunk=100, log=print):
+          eval_steps=16000, chunk=100, radius=1, log=print):
     """The learned-closure experiment. Training data: `train_bodies` seeded bodies run at
     fine_dims (FP16, Smagorinsky Cs = 0.1, Re on the body height), `snapshots` filtered sample sets
     each (cells kept with probability `keep`, up to `samples`). Training: Adam on the GPU. Evaluation
@@ -341,9 +345,11 @@ def study(make=None, fine_dims=(512, 256, 256), train_bodies=8, eval_bodies=2, s
     from .solver import solver_factory
 
     make = make or solver_factory
-    out = {"fine_dims": list(fine_dims), "re": re, "u": u, "train_bodies": train_bodies, "eval_bodies": eval_bodies}
+    out = {"fine_dims": list(fine_dims), "re": re, "u": u, "train_bodies": train_bodies, "eval_bodies": eval_bodies,
+           "projection_radius": radius}
     t_start = time.perf_counter()
     tr = Trainer(samples)
+    tr.set_projection_radius(radius)
     gen_s = 0.0
     for b, body in enumerate(seeded_bodies(train_bodies, seed=seed)):
         t0 = time.perf_counter()
@@ -370,6 +376,7 @@ def study(make=None, fine_dims=(512, 256, 256), train_bodies=8, eval_bodies=2, s
     tr.destroy()
     log(f"trained: loss {out['loss_first']:.4g} -> {out['loss_last']:.4g} in {out['train_seconds']:.1f} s")
     ev = Trainer(1 << 22)
+    ev.set_projection_radius(radius)
     cases = []
     for b, body in enumerate(seeded_bodies(eval_bodies, seed=seed + 7919)):
         fine, coarse, pf, f_front = _fine_coarse(make, body, fine_dims, u=u, re=re, seed=seed + 100 + b)

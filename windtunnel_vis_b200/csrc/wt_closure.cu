@@ -36,6 +36,7 @@ struct wt_trainer {
   size_t scratch_floats = 0;
   float* io = nullptr;         // staging for host rows
   size_t io_floats = 0;
+  int radius = 1;              // projection sums over (2 radius + 1)^3 coarse cells
   std::string err;
 };
 
@@ -384,12 +385,14 @@ struct SelectArgs {
   float x_lo, x_hi; // kept x range (outside the sponges)
   uint32_t keep;    // keep threshold on a 32-bit hash
   uint64_t seed;
+  int radius;       // projection box half-width
 };
 
-// the sample of coarse cell c: nu* from the 3 x 3 x 3 sums of num and den over stencil cells;
+// the sample of coarse cell c: nu* from the (2 radius + 1)^3 sums of num and den over stencil cells;
 // features of the stress the coarse handle sees at that viscosity, Pi = -(2/3) rho~ (tau0 + 3 nu*) S~
 __device__ bool closure_sample(const SelectArgs& A, int x, int y, int z, float (&xf)[CL_IN], float& yt) {
-  if (x < 2 || y < 2 || z < 2 || x > A.nx - 3 || y > A.ny - 3 || z > A.nz - 3) return false;
+  const int R = A.radius;
+  if (x < R + 1 || y < R + 1 || z < R + 1 || x > A.nx - R - 2 || y > A.ny - R - 2 || z > A.nz - R - 2) return false;
   if ((float)x < A.x_lo || (float)x >= A.x_hi) return false;
   const size_t n = (size_t)A.nx * A.ny * A.nz;
   const size_t c = (size_t)x + (size_t)A.nx * ((size_t)y + (size_t)A.ny * (size_t)z);
@@ -397,9 +400,9 @@ __device__ bool closure_sample(const SelectArgs& A, int x, int y, int z, float (
   const uint32_t h = (uint32_t)(mix64(A.seed ^ (uint64_t)c) >> 32);
   if (h >= A.keep) return false;
   double sn = 0, sd = 0;
-  for (int dz = -1; dz <= 1; dz++)
-    for (int dy = -1; dy <= 1; dy++)
-      for (int dx = -1; dx <= 1; dx++) {
+  for (int dz = -R; dz <= R; dz++)
+    for (int dy = -R; dy <= R; dy++)
+      for (int dx = -R; dx <= R; dx++) {
         const size_t q = c + (size_t)((ptrdiff_t)dx + (ptrdiff_t)A.nx * ((ptrdiff_t)dy + (ptrdiff_t)A.ny * dz));
         const float d = A.tgt[n + q];
         if (d >= 0.0f) {
@@ -609,6 +612,12 @@ int wt_trainer_clear(wt_trainer* t) {
   return WT_OK;
 }
 
+int wt_trainer_set_projection_radius(wt_trainer* t, int32_t radius) {
+  if (!t || radius < 1 || radius > 3) return WT_E_INVALID;
+  t->radius = radius;
+  return WT_OK;
+}
+
 int wt_trainer_put_samples(wt_trainer* t, const float* x, const float* y, int64_t n) {
   if (!t || n < 0 || (n > 0 && (!x || !y))) return WT_E_INVALID;
   if (t->count + n > t->cap) return tfail(t, WT_E_INVALID, "wt_trainer_put_samples: pool capacity exceeded");
@@ -678,6 +687,7 @@ int wt_trainer_add_samples(wt_trainer* t, wt_solver* fine, wt_solver* coarse, do
   A.x_hi = std::min((float)nx, coarse->kp.sponge_start);
   A.keep = keep >= 1.0 ? 0xFFFFFFFFu : (uint32_t)(keep * 4294967296.0);
   A.seed = seed;
+  A.radius = t->radius;
   const int64_t blocks = (int64_t)((n + 255) / 256);
   uint32_t* counts = nullptr;
   int64_t* base = nullptr;

@@ -377,6 +377,7 @@ def main(argv=None):
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--keep", type=float, default=0.4)
     ap.add_argument("--re", type=float, default=1000.0)
+    ap.add_argument("--radius", type=int, default=1, help="learned_closure: projection box half-width")
     ap.add_argument("--save", default=None, help="learned_closure: write the trained network (.npz)")
     ap.add_argument("--fused", action="store_true", help="batch_sweep: bulk rows of all tunnels in one kernel")
     ap.add_argument("--closure", default=None,
@@ -387,7 +388,7 @@ def main(argv=None):
 
         fine = tuple(int(v) for v in a.fine.split(","))
         r = CL.study(solver_factory, fine_dims=fine, train_bodies=a.train_bodies, eval_bodies=a.eval_bodies,
-                     warm=a.warm, train_steps=a.train_steps, keep=a.keep, re=a.re, eval_steps=a.steps,
+                     warm=a.warm, train_steps=a.train_steps, keep=a.keep, re=a.re, eval_steps=a.steps, radius=a.radius,
                      log=lambda m: print(m, flush=True))
         if a.save:
             CL.save({k: np.asarray(v, np.float32) for k, v in r["model"].items()}, a.save)
