@@ -73,7 +73,7 @@ void free_all(wt_solver* s) {
                   s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count,
                   s->bcell, s->brec, s->bgam, s->vox_pos, s->vox_idx, s->vox_info,
                   s->dvort, s->dstat, s->dmean, s->exp_buf, s->probe_buf, s->closure_dev, s->stage,
-                  s->diff_dev};
+                  s->diff_dev, s->lc_rows};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->result_host) cudaFreeHost(s->result_host);
@@ -163,6 +163,11 @@ int ensure_classified(wt_solver* s) {
     invalidate_graphs(s);
     WT_CUDA(s, wt::launch_boundary_table(s), "boundary links");
     s->tab_dirty = false;
+  }
+  if (s->closure_dev) {
+    bool grown = false;
+    WT_CUDA(s, wt::closure_rows_reserve(s, &grown), "closure rows");
+    if (grown) invalidate_graphs(s);
   }
   return WT_OK;
 }
@@ -324,6 +329,11 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
     return true;
   };
   const size_t fbytes = (size_t)s->q * s->n * s->pop_elem;
+  if (cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess ||
+      s->num_sms <= 0) {
+    cudaGetLastError();
+    s->num_sms = 148;
+  }
   // one macro block per 256 cells up to 4096 blocks (several cells per thread beyond: the block
   // reductions amortise and the final reduce reads at most 256 KB), one 64-byte partial each
   s->partial_blocks = (int)std::min<size_t>((s->n + 255) / 256, 4096);
@@ -516,15 +526,14 @@ int wt_set_closure(wt_solver* s, const wt_closure* c) {
   if (!(c->nu_scale >= 0.0f)) return fail(s, WT_E_INVALID, "wt_set_closure: nu_scale must be >= 0");
   wt::ClosureDev host;
   std::memset(&host, 0, sizeof host);
-  wt::ClosureWeights cwt;
-  wt::closure_pack(*c, host, cwt);
+  wt::closure_pack(*c, host);
   // the captured step graphs carry the network's by-value part: rebuild them
   invalidate_graphs(s);
   if (!s->closure_dev) WT_CUDA(s, cudaMalloc((void**)&s->closure_dev, sizeof(wt::ClosureDev)), "wt_set_closure");
   WT_CUDA(s, cudaMemcpyAsync(s->closure_dev, &host, sizeof host, cudaMemcpyHostToDevice, s->stream), "wt_set_closure");
   WT_CUDA(s, cudaStreamSynchronize(s->stream), "wt_set_closure");
   s->closure_host = *c;
-  s->closure_w = cwt;
+  s->closure_p = wt::closure_params(*c);
   return WT_OK;
 }
 

@@ -10,9 +10,8 @@
 //   z3  = (sum_even h2_j w3_j + sum_odd h2_j w3_j) + b3,  nu_t = nu_scale * softplus(z3)
 //   gelu(x) = x * (1/2 + tanh(u) / 2),  u = x (C0 + C1 x^2),  C0 = sqrt(2/pi), C1 = 0.044715 C0
 //             (the tanh form of gelu; tanh.approx.f32)
-// The two 32-wide layers run on tcgen05 tensor cores in the bulk kernel and the trainer; face and
-// wall cells evaluate the same network on CUDA cores (closure_nu). Both use the identical gelu,
-// bias and rounding steps; they differ only in the order of the f32 accumulations of z1 and z2.
+// The two 32-wide layers run on tcgen05 tensor cores in the bulk kernel, in the row pass that
+// serves the face rows and wall cells, and in the trainer.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -50,18 +49,6 @@ struct __align__(128) ClosureDev {
   uint16_t w1img[CL_H * CL_K1];
   uint16_t w2img[CL_H * CL_H];
   uint16_t w2timg[CL_H * CL_H];
-};
-
-// The whole network for the CUDA-core path (face rows and wall cells), passed by value so that
-// every weight is a constant-bank operand: the bf16-rounded W1 and W2 as f32, and the small values.
-struct ClosureWeights {
-  float w1[CL_IN][CL_H];
-  float w2[CL_H][CL_H];
-  ClosureParams p;
-};
-// placeholder parameter of the kernels' Smagorinsky instantiations
-struct NoClosure {
-  int unused;
 };
 
 // bf16 round to nearest even (finite inputs), as a float and as raw bits
@@ -163,33 +150,6 @@ __device__ __forceinline__ void cl_features(float pxx, float pyy, float pzz, flo
   x[9] = cl_sqrt(__fmaf_rn(ux, ux, __fmaf_rn(uy, uy, __fmul_rn(uz, uz))));
 }
 
-// the whole network on CUDA cores (face and wall cells): nu_t of one cell
-static __device__ __noinline__ float closure_nu(const ClosureWeights& W, const float* __restrict__ xin) {
-  const ClosureParams& P = W.p;
-  float x[CL_IN];
-#pragma unroll
-  for (int k = 0; k < CL_IN; k++) x[k] = bf16r(__fmaf_rn(xin[k], P.scale[k], P.nshift[k]));
-  float h1[CL_H];
-#pragma unroll 8
-  for (int j = 0; j < CL_H; j++) {
-    float a = 0.0f;
-#pragma unroll
-    for (int k = 0; k < CL_IN; k++) a = __fmaf_rn(x[k], W.w1[k][j], a);
-    h1[j] = bf16r(cl_gelu(__fadd_rn(a, P.b1[j])));
-  }
-  float ze = 0.0f, zo = 0.0f;
-#pragma unroll 2
-  for (int j = 0; j < CL_H; j++) {
-    float a = 0.0f;
-#pragma unroll
-    for (int i = 0; i < CL_H; i++) a = __fmaf_rn(h1[i], W.w2[i][j], a);
-    const float h2 = cl_gelu(__fadd_rn(a, P.b2[j]));
-    if (j & 1) zo = __fmaf_rn(h2, P.w3[j], zo);
-    else ze = __fmaf_rn(h2, P.w3[j], ze);
-  }
-  return __fmul_rn(P.nu_scale, cl_softplus(__fadd_rn(__fadd_rn(ze, zo), P.b3)));
-}
-
 // the by-value part of a network
 __host__ __device__ inline ClosureParams closure_params(const wt_closure& c) {
   ClosureParams p;
@@ -207,8 +167,8 @@ __host__ __device__ inline ClosureParams closure_params(const wt_closure& c) {
   return p;
 }
 
-// fills the bf16 images of `c` into `d` and the CUDA-core copy into `w` (host or device)
-__host__ __device__ inline void closure_pack(const wt_closure& c, ClosureDev& d, ClosureWeights& w) {
+// fills the bf16 images of `c` into `d` (host or device)
+__host__ __device__ inline void closure_pack(const wt_closure& c, ClosureDev& d) {
   for (int j = 0; j < CL_H; j++)
     for (int k = 0; k < CL_K1; k++) {
       const float v = k < CL_IN ? c.w1[k][j] : 0.0f;
@@ -219,11 +179,7 @@ __host__ __device__ inline void closure_pack(const wt_closure& c, ClosureDev& d,
       const uint16_t b = bf16_bits(c.w2[i][j]);
       d.w2img[umma::kmaj_off(j, i, CL_H) / 2] = b;
       d.w2timg[umma::kmaj_off(i, j, CL_H) / 2] = b;
-      w.w2[i][j] = bf16_val(b);
     }
-  for (int k = 0; k < CL_IN; k++)
-    for (int j = 0; j < CL_H; j++) w.w1[k][j] = bf16r(c.w1[k][j]);
-  w.p = closure_params(c);
 }
 
 }  // namespace wt

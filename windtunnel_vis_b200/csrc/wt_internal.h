@@ -15,6 +15,7 @@ constexpr int WT_LONG_PAIRS = 5;
 
 struct wt_solver {
   int device = 0;
+  int num_sms = 148;  // streaming multiprocessors of `device` (persistent grids)
   cudaStream_t stream = nullptr;
   // the face-row and per-cell boundary kernels run on `aux`, forked from and joined back into
   // `stream` around each step, so they overlap the bulk kernel
@@ -102,8 +103,12 @@ struct wt_solver {
   bool launch_explicit = false;
   // learned closure (wt_set_closure): device copy of the network, nullptr = Smagorinsky
   wt::ClosureDev* closure_dev = nullptr;
-  wt::ClosureWeights closure_w{};  // the network by value (CUDA-core path; .p for the bulk kernel)
+  wt::ClosureParams closure_p{};  // the network's small values, passed by value to the kernels
   wt_closure closure_host{};
+  // the learned closure's face rows and wall cells: their features ([rows][10]) followed by their
+  // eddy viscosities ([rows]), rows = face cells + boundary-table capacity
+  float* lc_rows = nullptr;
+  size_t lc_rows_cap = 0;
   int* err_dev = nullptr;   // device-side error word written by kernels with bounded waits
   int* err_host = nullptr;  // pinned copy
   int64_t launches = 0;
@@ -113,6 +118,9 @@ struct wt_solver {
 namespace wt {
 
 int lbm_block_x(const wt_solver* s);
+// sizes the learned closure's row buffer for the current lattice and boundary table (outside
+// graph capture); true in *grown when it was reallocated
+cudaError_t closure_rows_reserve(wt_solver* s, bool* grown);
 cudaError_t launch_classify(wt_solver* s);
 cudaError_t launch_boundary_table(wt_solver* s);
 cudaError_t launch_init(wt_solver* s);

@@ -168,11 +168,13 @@ __global__ void __launch_bounds__(256) k_init(const wt_kparams P, typename S::T*
 // cells / collision = bgk) with the Smagorinsky relaxation time and the outlet / inlet sponges
 // (wgslLbm.ts:177-240). fo receives the post-collision populations.
 //
-// With a learned closure (cw != nullptr, f32 only) the network's eddy viscosity replaces the
-// Smagorinsky term: tau = tau0' + 3 nu_t (tau0' = tau0 with the outlet sponge and the wall floor).
+// With nu_in >= 0 (the learned closure's eddy viscosity of the cell) it replaces the Smagorinsky
+// term: tau = tau0' + 3 nu_in (tau0' = tau0 with the outlet sponge and the wall floor). With xout
+// (f32 D3Q19 only) the closure's 10 features of the cell go to xout and nothing is collided.
 template <class L, class R>
 __device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L::Q], int ix, bool wall, bool gwall,
-                                             R (&fo)[L::Q], const ClosureWeights* cw = nullptr, float wall_d = 0.0f) {
+                                             R (&fo)[L::Q], float nu_in = -1.0f, float* xout = nullptr,
+                                             float wall_d = 0.0f) {
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
   const R U = (R)P.uin;
@@ -205,6 +207,13 @@ __device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L
     pxz = sxz - rho * ux * uz;
     pyz = syz - rho * uy * uz;
   }
+  if constexpr (std::is_same<R, float>::value && D3) {
+    if (xout != nullptr) {
+      cl_features(pxx, pyy, pzz, pxy, pxz, pyz, rho, ux, uy, uz, P.tau0, wall_d,
+                  *reinterpret_cast<float(*)[CL_IN]>(xout));
+      return;
+    }
+  }
   R pn = pxx * pxx + (R)2 * pxy * pxy + pyy * pyy;
   if constexpr (D3) pn = pxx * pxx + (R)2 * pxy * pxy + (R)2 * pxz * pxz + pyy * pyy + (R)2 * pyz * pyz + pzz * pzz;
   const R piN = sqrt(pn);
@@ -214,18 +223,9 @@ __device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L
   sp = sp < (R)0 ? (R)0 : (sp > (R)1 ? (R)1 : sp);
   R t0 = (R)P.tau0 + (R)3 * (R)P.sponge_nu * sp * sp;
   if (gwall) t0 = t0 > (R)P.tau_wall ? t0 : (R)P.tau_wall;
-  R tau;
-  if constexpr (std::is_same<R, float>::value && L::DIM == 3) {
-    if (cw != nullptr) {
-      float x[CL_IN];
-      cl_features(pxx, pyy, pzz, pxy, pxz, pyz, rho, ux, uy, uz, P.tau0, wall_d, x);
-      tau = t0 + 3.0f * closure_nu(*cw, x);
-    } else {
-      tau = (R)0.5 * (t0 + sqrt(t0 * t0 + (R)(18.0 * 1.4142135623730951) * (R)P.csmag2 * piN * irho));
-    }
-  } else {
-    tau = (R)0.5 * (t0 + sqrt(t0 * t0 + (R)(18.0 * 1.4142135623730951) * (R)P.csmag2 * piN * irho));
-  }
+  const R tau = nu_in >= 0.0f
+                    ? t0 + (R)3 * (R)nu_in
+                    : (R)0.5 * (t0 + sqrt(t0 * t0 + (R)(18.0 * 1.4142135623730951) * (R)P.csmag2 * piN * irho));
   const R omega = (R)1 - (R)1 / tau;
   const R k1 = omega * (R)4.5;
   const bool useBGK = wall || P.collision == 1u;
@@ -847,22 +847,38 @@ __device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const floa
                             });
 }
 
-// the learned closure for cells collided on CUDA cores (face rows): the network per lane
+// the learned closure with the two cells' eddy viscosities given (face rows)
 template <class L, bool BGK, class Emit>
-__device__ __forceinline__ void collide_shifted2_lc(const wt_kparams& P, const float2 (&h)[L::Q], int x, Emit&& emit,
-                                                    float t_floor, const ClosureWeights& cw, float2 wd) {
-  collide_shifted2x<L, BGK>(P, h, x, emit,
-                            [&](float2 rho, float2, float2 ux, float2 uy, float2 uz, float2 pxx, float2 pyy,
-                                float2 pzz, float2 pxy, float2 pxz, float2 pyz) {
-                              float xa[CL_IN], xb[CL_IN];
-                              cl_features(pxx.x, pyy.x, pzz.x, pxy.x, pxz.x, pyz.x, rho.x, ux.x, uy.x, uz.x, P.tau0,
-                                          wd.x, xa);
-                              cl_features(pxx.y, pyy.y, pzz.y, pxy.y, pxz.y, pyz.y, rho.y, ux.y, uy.y, uz.y, P.tau0,
-                                          wd.y, xb);
-                              const float ta = tau0_eff(P, (float)x, t_floor) + 3.0f * closure_nu(cw, xa);
-                              const float tb = tau0_eff(P, (float)(x + 1), t_floor) + 3.0f * closure_nu(cw, xb);
-                              return make_float2(1.0f - __fdividef(1.0f, ta), 1.0f - __fdividef(1.0f, tb));
-                            });
+__device__ __forceinline__ void collide_shifted2_nu(const wt_kparams& P, const float2 (&h)[L::Q], int x, Emit&& emit,
+                                                    float t_floor, float2 nu) {
+  collide_shifted2x<L, BGK>(P, h, x, emit, [&](float2, float2, float2, float2, float2, float2, float2, float2,
+                                               float2, float2, float2) {
+    const float ta = tau0_eff(P, (float)x, t_floor) + 3.0f * nu.x;
+    const float tb = tau0_eff(P, (float)(x + 1), t_floor) + 3.0f * nu.y;
+    return make_float2(1.0f - __fdividef(1.0f, ta), 1.0f - __fdividef(1.0f, tb));
+  });
+}
+
+// the closure features of two cells (the moments of the pulled populations) into rows
+// xrow, xrow + 1 of x (10 floats each)
+template <class L>
+__device__ __forceinline__ void features2(const wt_kparams& P, const float2 (&h)[L::Q], float2 wd,
+                                          float* __restrict__ x, size_t row) {
+  collide_shifted2x<L, true>(P, h, 0, [&](auto, float2) {},
+                             [&](float2 rho, float2, float2 ux, float2 uy, float2 uz, float2 pxx, float2 pyy,
+                                 float2 pzz, float2 pxy, float2 pxz, float2 pyz) {
+                               float xa[CL_IN], xb[CL_IN];
+                               cl_features(pxx.x, pyy.x, pzz.x, pxy.x, pxz.x, pyz.x, rho.x, ux.x, uy.x, uz.x,
+                                           P.tau0, wd.x, xa);
+                               cl_features(pxx.y, pyy.y, pzz.y, pxy.y, pxz.y, pyz.y, rho.y, ux.y, uy.y, uz.y,
+                                           P.tau0, wd.y, xb);
+#pragma unroll
+                               for (int k = 0; k < CL_IN; k++) {
+                                 x[row * CL_IN + k] = xa[k];
+                                 x[(row + 1) * CL_IN + k] = xb[k];
+                               }
+                               return f2(0.0f);
+                             });
 }
 
 // two-cell loads / stores of shifted populations: elements (o, o + 1), o even. Loads are split
@@ -1050,14 +1066,15 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_batch_bulk(const _
 // no-slip or moving floor, and the inlet equilibrium / zero-gradient outlet as in the bulk. Floor
 // rows with bounce-back collide with BGK and the tauWall floor, like the reference's wall cells.
 // Groups holding a solid or a fluid cell next to a solid are left to k_boundary_tab.
-// With LC the learned closure replaces Smagorinsky (network on CUDA cores, wall distance from sdf).
-template <bool LC> struct LCW { typedef NoClosure type; };
-template <> struct LCW<true> { typedef ClosureWeights type; };
+// MODE 0: Smagorinsky. With the learned closure, MODE 1 writes the features of every face cell
+// (row r * nx + x of `xb`) and stores nothing; MODE 2 collides with the eddy viscosities nub[row].
+enum : int { FM_SMAG = 0, FM_FEATURES = 1, FM_NU = 2 };
 
-template <class L, class S, bool LC>
+template <class L, class S, int MODE>
 __device__ __forceinline__ void face_rows(const wt_kparams& P, const typename S::T* __restrict__ fin,
                                           typename S::T* __restrict__ fout, const uint8_t* __restrict__ cls, int gs,
-                                          const uint32_t* __restrict__ sdf, const typename LCW<LC>::type& CW) {
+                                          const uint32_t* __restrict__ sdf, float* __restrict__ xb,
+                                          const float* __restrict__ nub) {
   typedef PairIO<S> IO;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
@@ -1177,12 +1194,15 @@ __device__ __forceinline__ void face_rows(const wt_kparams& P, const typename S:
     constexpr int i = decltype(I)::value;
     if (clean) IO::st(fout, i * N + idx0, v, (float)Wc<L, i>::v);
   };
-  if constexpr (LC) {
+  const size_t slot = (size_t)r * (size_t)NX + (size_t)x0;
+  if constexpr (MODE == FM_FEATURES) {
     const uint2 sw = __ldg(reinterpret_cast<const uint2*>(sdf + idx0));
-    const float2 wd = make_float2(cl_wall_dist(sw.x), cl_wall_dist(sw.y));
-    if (gwall) collide_shifted2_lc<L, true>(P, h, x0, emit, P.tau_wall, CW, wd);
-    else if (P.collision == 1u) collide_shifted2_lc<L, true>(P, h, x0, emit, 0.0f, CW, wd);
-    else collide_shifted2_lc<L, false>(P, h, x0, emit, 0.0f, CW, wd);
+    features2<L>(P, h, make_float2(cl_wall_dist(sw.x), cl_wall_dist(sw.y)), xb, slot);
+  } else if constexpr (MODE == FM_NU) {
+    const float2 nu = make_float2(__ldg(nub + slot), __ldg(nub + slot + 1));
+    if (gwall) collide_shifted2_nu<L, true>(P, h, x0, emit, P.tau_wall, nu);
+    else if (P.collision == 1u) collide_shifted2_nu<L, true>(P, h, x0, emit, 0.0f, nu);
+    else collide_shifted2_nu<L, false>(P, h, x0, emit, 0.0f, nu);
   } else {
     if (gwall) collide_shifted2<L, true>(P, h, x0, emit, P.tau_wall);
     else if (P.collision == 1u) collide_shifted2<L, true>(P, h, x0, emit);
@@ -1195,18 +1215,19 @@ __global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kpara
                                                 const typename S::T* __restrict__ fin,
                                                 typename S::T* __restrict__ fout,
                                                 const uint8_t* __restrict__ cls, int gs) {
-  face_rows<L, S, false>(P, fin, fout, cls, gs, nullptr, NoClosure{0});
+  face_rows<L, S, FM_SMAG>(P, fin, fout, cls, gs, nullptr, nullptr, nullptr);
 }
 
-// face rows with the learned closure (network on CUDA cores, registers capped for two blocks per SM)
-template <class L, class S>
-__global__ void __launch_bounds__(256, 2) k_face_lc(const __grid_constant__ wt_kparams P,
-                                                    const typename S::T* __restrict__ fin,
-                                                    typename S::T* __restrict__ fout,
-                                                    const uint8_t* __restrict__ cls, int gs,
-                                                    const uint32_t* __restrict__ sdf,
-                                                    const __grid_constant__ ClosureWeights CW) {
-  face_rows<L, S, true>(P, fin, fout, cls, gs, sdf, CW);
+// face rows with the learned closure: MODE FM_FEATURES (inputs of the network) or FM_NU (collision
+// with the network's eddy viscosities)
+template <class L, class S, int MODE>
+__global__ void __launch_bounds__(256) k_face_lc(const __grid_constant__ wt_kparams P,
+                                                 const typename S::T* __restrict__ fin,
+                                                 typename S::T* __restrict__ fout,
+                                                 const uint8_t* __restrict__ cls, int gs,
+                                                 const uint32_t* __restrict__ sdf, float* __restrict__ xb,
+                                                 const float* __restrict__ nub) {
+  face_rows<L, S, MODE>(P, fin, fout, cls, gs, sdf, xb, nub);
 }
 
 // ---- bulk kernel with the learned closure: the network on tcgen05 tensor cores -----------------
@@ -1247,7 +1268,143 @@ __device__ __forceinline__ void lc_write_inputs(uint8_t* tile, uint32_t r, const
   *reinterpret_cast<uint4*>(tile + umma::kmaj_off(r, 8, CL_K1)) = make_uint4(w[4], 0u, 0u, 0u);
 }
 
-// One tile (tpr cell pairs x 128 / tpr rows) per block, 1-D grid over the tiles.
+// The network for two 128-row tiles, called by all LC_THREADS threads of the block with the
+// weight images at LC_SMEM_W1 / LC_SMEM_W2, the barrier at LC_SMEM_BAR (phases 0 and 1 are used)
+// and 64 tensor-memory columns at tmem. Thread tid's features xa / xb are row tid of tiles 0 / 1;
+// the result holds their eddy viscosities nu_scale softplus(z3). A wait that times out clears ok.
+__device__ __forceinline__ float2 lc_network2(uint8_t* smem, uint32_t tmem, uint64_t* mbar, uint32_t tid,
+                                              const float (&xa)[CL_IN], const float (&xb)[CL_IN],
+                                              const ClosureParams& CP, bool& ok) {
+  uint8_t* const sA = smem + LC_SMEM_A;
+  uint8_t* const sH = smem + LC_SMEM_H;
+  const uint32_t warp = tid >> 5;
+  lc_write_inputs(sA, tid, xa, CP);
+  lc_write_inputs(sA + 4096, tid, xb, CP);
+  constexpr uint32_t ID = umma::idesc_bf16<128, CL_H>();
+  umma::fence_async_smem();
+  umma::fence_before_sync();  // tensor-memory reads of a previous call come before these MMAs
+  __syncthreads();
+  if (tid == 0) {
+    umma::fence_after_sync();
+    const uint64_t bw1 = umma::sdesc(umma::smem_u32(smem + LC_SMEM_W1), 128, 256);
+    umma::mma_bf16(tmem, umma::sdesc(umma::smem_u32(sA), 128, 256), bw1, ID, false);
+    umma::mma_bf16(tmem + 32, umma::sdesc(umma::smem_u32(sA + 4096), 128, 256), bw1, ID, false);
+    umma::commit(mbar);
+  }
+  ok = umma::mbar_wait(mbar, 0, LC_WAIT_LIMIT) && ok;
+  umma::fence_after_sync();
+  // hidden layer 1: bias, gelu (two units per f32x2 lane pair), bf16x2 -> row tid of the hidden tiles
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    float v[4][8];
+#pragma unroll
+    for (int c = 0; c < 4; c++) umma::tmem_ld8(umma::tmem_lane_addr(tmem, warp, 32 * t + 8 * c), v[c]);
+    umma::tmem_wait_ld();
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      uint32_t pk[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int j = 8 * c + 2 * e;
+        const float2 g = cl_gelu2(__fadd2_rn(make_float2(v[c][2 * e], v[c][2 * e + 1]),
+                                             make_float2(CP.b1[j], CP.b1[j + 1])));
+        pk[e] = bf16x2_bits(g.x, g.y);
+      }
+      *reinterpret_cast<uint4*>(sH + 8192 * t + umma::kmaj_off(tid, 8 * c, CL_H)) =
+          make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    }
+  }
+  umma::fence_before_sync();
+  umma::fence_async_smem();
+  __syncthreads();
+  if (tid == 0) {
+    umma::fence_after_sync();
+    const uint32_t w2 = umma::smem_u32(smem + LC_SMEM_W2);
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const uint32_t a = umma::smem_u32(sH + 8192 * t);
+      umma::mma_bf16(tmem + 32 * t, umma::sdesc(a, 128, 512), umma::sdesc(w2, 128, 512), ID, false);
+      umma::mma_bf16(tmem + 32 * t, umma::sdesc(a + 256, 128, 512), umma::sdesc(w2 + 256, 128, 512), ID, true);
+    }
+    umma::commit(mbar);
+  }
+  ok = umma::mbar_wait(mbar, 1, LC_WAIT_LIMIT) && ok;
+  umma::fence_after_sync();
+  // hidden layer 2 (f32) and the output layer: even units in lane .x, odd units in lane .y
+  float z3[2];
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    float v[4][8];
+#pragma unroll
+    for (int c = 0; c < 4; c++) umma::tmem_ld8(umma::tmem_lane_addr(tmem, warp, 32 * t + 8 * c), v[c]);
+    umma::tmem_wait_ld();
+    float2 z = f2(0.0f);
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int j = 8 * c + 2 * e;
+        const float2 g = cl_gelu2(__fadd2_rn(make_float2(v[c][2 * e], v[c][2 * e + 1]),
+                                             make_float2(CP.b2[j], CP.b2[j + 1])));
+        z = __ffma2_rn(g, make_float2(CP.w3[j], CP.w3[j + 1]), z);
+      }
+    z3[t] = __fmul_rn(CP.nu_scale, cl_softplus(__fadd_rn(__fadd_rn(z.x, z.y), CP.b3)));
+  }
+  return make_float2(z3[0], z3[1]);
+}
+
+// The eddy viscosities of `rows` feature rows (xb: [rows][10], the face rows' and wall cells'
+// features) into nub[rows], on the tensor cores with the bulk kernel's arithmetic: 256 rows per
+// block, row b * 256 + tid in tile 0 and b * 256 + 128 + tid in tile 1. A timed-out wait sets
+// bit 4 of the error word and the block stores nothing.
+__global__ void __launch_bounds__(LC_THREADS) k_closure_rows(const float* __restrict__ xb, uint32_t rows,
+                                                              float* __restrict__ nub,
+                                                              const ClosureDev* __restrict__ cw,
+                                                              const __grid_constant__ ClosureParams CP,
+                                                              int* __restrict__ err) {
+  extern __shared__ __align__(128) uint8_t lc_smem[];
+  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  uint64_t* const mbar = reinterpret_cast<uint64_t*>(lc_smem + LC_SMEM_BAR);
+  uint32_t* const tslot = reinterpret_cast<uint32_t*>(lc_smem + LC_SMEM_BAR + 8);
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(cw->w1img);
+    uint4* dst = reinterpret_cast<uint4*>(lc_smem + LC_SMEM_W1);
+    for (uint32_t k = tid; k < 192u; k += LC_THREADS) dst[k] = __ldg(src + k);
+  }
+  if (tid == 0) umma::mbar_init(mbar, 1);
+  if (warp == 0) umma::tmem_alloc(tslot, LC_TMEM_COLS);
+  const uint32_t r0 = blockIdx.x * (2u * LC_THREADS) + tid, r1 = r0 + LC_THREADS;
+  float xa[CL_IN], xc[CL_IN];
+#pragma unroll
+  for (int k = 0; k < CL_IN; k++) {
+    xa[k] = r0 < rows ? __ldg(xb + (size_t)r0 * CL_IN + k) : 0.0f;
+    xc[k] = r1 < rows ? __ldg(xb + (size_t)r1 * CL_IN + k) : 0.0f;
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *tslot;
+  bool ok = true;
+  const float2 nu = lc_network2(lc_smem, tmem, mbar, tid, xa, xc, CP, ok);
+  if (ok) {
+    if (r0 < rows) nub[r0] = nu.x;
+    if (r1 < rows) nub[r1] = nu.y;
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_free(tmem, LC_TMEM_COLS);
+  }
+  if (!ok) atomicOr(err, 4);
+}
+
+// Tiles of tpr cell pairs x 128 / tpr rows; block b takes tiles b, b + grid, ... (LC_TILES_PER_BLOCK
+// of them) and keeps its weight images, barrier and tensor memory for all of them. 29 KB of shared
+// memory per block: at most 7 blocks share an SM, and their 7 x 64 tensor-memory columns fit in
+// its 512. After each tile the block agrees on `ok`; a timed-out wait ends the loop for the whole
+// block.
+constexpr int LC_TILES_PER_BLOCK = 4;
 template <class S, bool BGK>
 __global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_constant__ wt_kparams P,
                                                                    const typename S::T* __restrict__ fin,
@@ -1256,7 +1413,8 @@ __global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_c
                                                                    const uint32_t* __restrict__ sdf,
                                                                    const ClosureDev* __restrict__ cw,
                                                                    const __grid_constant__ ClosureParams CP,
-                                                                   int tpr, int* __restrict__ err) {
+                                                                   int tpr, uint32_t ntiles,
+                                                                   int* __restrict__ err) {
   typedef D3Q19 L;
   typedef PairIO<S> IO;
   constexpr int Q = L::Q;
@@ -1269,8 +1427,6 @@ __global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_c
   const int tiles_x = (NX / 2 + tpr - 1) / tpr, tiles_y = (NY + rpb - 1) / rpb;
   const uint32_t N = P.n;
   const uint32_t sy = (uint32_t)NX, sz = (uint32_t)NX * (uint32_t)NY;
-  uint8_t* const sA = lc_smem + LC_SMEM_A;
-  uint8_t* const sH = lc_smem + LC_SMEM_H;
   uint64_t* const mbar = reinterpret_cast<uint64_t*>(lc_smem + LC_SMEM_BAR);
   uint32_t* const tslot = reinterpret_cast<uint32_t*>(lc_smem + LC_SMEM_BAR + 8);
   {
@@ -1285,8 +1441,7 @@ __global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_c
   umma::fence_after_sync();
   const uint32_t tmem = *tslot;
   bool ok = true;
-  {
-    const uint32_t tile = blockIdx.x;
+  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int bx = (int)(tile % (uint32_t)tiles_x);
     const int by = (int)((tile / (uint32_t)tiles_x) % (uint32_t)tiles_y);
     const int iz = (int)(tile / ((uint32_t)tiles_x * (uint32_t)tiles_y));
@@ -1359,83 +1514,16 @@ __global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_c
             float xa[CL_IN], xb[CL_IN];
             cl_features(pxx.x, pyy.x, pzz.x, pxy.x, pxz.x, pyz.x, rho.x, ux.x, uy.x, uz.x, P.tau0, wd.x, xa);
             cl_features(pxx.y, pyy.y, pzz.y, pxy.y, pxz.y, pyz.y, rho.y, ux.y, uy.y, uz.y, P.tau0, wd.y, xb);
-            lc_write_inputs(sA, tid, xa, CP);
-            lc_write_inputs(sA + 4096, tid, xb, CP);
+            const float2 nu = lc_network2(lc_smem, tmem, mbar, tid, xa, xb, CP, ok);
+            const float ta = tau0_eff(P, (float)x0, 0.0f) + 3.0f * nu.x;
+            const float tb = tau0_eff(P, (float)(x0 + 1), 0.0f) + 3.0f * nu.y;
+            return make_float2(1.0f - __fdividef(1.0f, ta), 1.0f - __fdividef(1.0f, tb));
           }
-          constexpr uint32_t ID = umma::idesc_bf16<128, CL_H>();
-          umma::fence_async_smem();
-          __syncthreads();
-          if (tid == 0) {
-            umma::fence_after_sync();
-            const uint64_t bw1 = umma::sdesc(umma::smem_u32(lc_smem + LC_SMEM_W1), 128, 256);
-            umma::mma_bf16(tmem, umma::sdesc(umma::smem_u32(sA), 128, 256), bw1, ID, false);
-            umma::mma_bf16(tmem + 32, umma::sdesc(umma::smem_u32(sA + 4096), 128, 256), bw1, ID, false);
-            umma::commit(mbar);
-          }
-          ok = umma::mbar_wait(mbar, 0, LC_WAIT_LIMIT) && ok;
-          umma::fence_after_sync();
-          // hidden layer 1: bias, gelu (two units per f32x2 lane pair), bf16x2 -> row tid of the hidden tiles
-#pragma unroll
-          for (int t = 0; t < 2; t++) {
-            float v[4][8];
-#pragma unroll
-            for (int c = 0; c < 4; c++) umma::tmem_ld8(umma::tmem_lane_addr(tmem, warp, 32 * t + 8 * c), v[c]);
-            umma::tmem_wait_ld();
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-              uint32_t pk[4];
-#pragma unroll
-              for (int e = 0; e < 4; e++) {
-                const int j = 8 * c + 2 * e;
-                const float2 g = cl_gelu2(__fadd2_rn(make_float2(v[c][2 * e], v[c][2 * e + 1]),
-                                                     make_float2(CP.b1[j], CP.b1[j + 1])));
-                pk[e] = bf16x2_bits(g.x, g.y);
-              }
-              *reinterpret_cast<uint4*>(sH + 8192 * t + umma::kmaj_off(tid, 8 * c, CL_H)) =
-                  make_uint4(pk[0], pk[1], pk[2], pk[3]);
-            }
-          }
-          umma::fence_before_sync();
-          umma::fence_async_smem();
-          __syncthreads();
-          if (tid == 0) {
-            umma::fence_after_sync();
-            const uint32_t w2 = umma::smem_u32(lc_smem + LC_SMEM_W2);
-#pragma unroll
-            for (int t = 0; t < 2; t++) {
-              const uint32_t a = umma::smem_u32(sH + 8192 * t);
-              umma::mma_bf16(tmem + 32 * t, umma::sdesc(a, 128, 512), umma::sdesc(w2, 128, 512), ID, false);
-              umma::mma_bf16(tmem + 32 * t, umma::sdesc(a + 256, 128, 512), umma::sdesc(w2 + 256, 128, 512), ID,
-                             true);
-            }
-            umma::commit(mbar);
-          }
-          ok = umma::mbar_wait(mbar, 1, LC_WAIT_LIMIT) && ok;
-          umma::fence_after_sync();
-          // hidden layer 2 (f32) and the output layer: even units in lane .x, odd units in lane .y
-          float z3[2];
-#pragma unroll
-          for (int t = 0; t < 2; t++) {
-            float v[4][8];
-#pragma unroll
-            for (int c = 0; c < 4; c++) umma::tmem_ld8(umma::tmem_lane_addr(tmem, warp, 32 * t + 8 * c), v[c]);
-            umma::tmem_wait_ld();
-            float2 z = f2(0.0f);
-#pragma unroll
-            for (int c = 0; c < 4; c++)
-#pragma unroll
-              for (int e = 0; e < 4; e++) {
-                const int j = 8 * c + 2 * e;
-                const float2 g = cl_gelu2(__fadd2_rn(make_float2(v[c][2 * e], v[c][2 * e + 1]),
-                                                     make_float2(CP.b2[j], CP.b2[j + 1])));
-                z = __ffma2_rn(g, make_float2(CP.w3[j], CP.w3[j + 1]), z);
-              }
-            z3[t] = __fmul_rn(CP.nu_scale, cl_softplus(__fadd_rn(__fadd_rn(z.x, z.y), CP.b3)));
-          }
-          const float ta = tau0_eff(P, (float)x0, 0.0f) + 3.0f * z3[0];
-          const float tb = tau0_eff(P, (float)(x0 + 1), 0.0f) + 3.0f * z3[1];
-          return make_float2(1.0f - __fdividef(1.0f, ta), 1.0f - __fdividef(1.0f, tb));
         });
+    if (!__syncthreads_and(ok)) {
+      ok = false;
+      break;
+    }
   }
   // release the tensor memory once every thread's reads have completed
   umma::fence_before_sync();
@@ -1601,15 +1689,16 @@ __global__ void __launch_bounds__(128) k_boundary_build(const __grid_constant__ 
 
 // Applies the link records, one thread per listed cell: every record load of the cell in flight
 // at once (coalesced across the warp), then every gather, then the collision and the stores.
-// With LC the learned closure replaces Smagorinsky (network on CUDA cores, wall distance from sdf).
-template <class L, class S, bool LC = false>
+// MODE as for the face rows: FM_SMAG, FM_FEATURES (the listed cell's features into row k of xb,
+// nothing stored) or FM_NU (collision with the eddy viscosity nub[k]).
+template <class L, class S, int MODE = FM_SMAG>
 __global__ void __launch_bounds__(64) k_boundary_tab(const __grid_constant__ wt_kparams P,
                                                      const typename S::T* __restrict__ fin,
                                                      typename S::T* __restrict__ fout,
                                                      const uint2* __restrict__ bcell, const uint4* __restrict__ rec,
                                                      const float* __restrict__ gam, uint32_t count, uint32_t cap,
-                                                     const uint32_t* __restrict__ sdf,
-                                                     const __grid_constant__ typename LCW<LC>::type CW) {
+                                                     const uint32_t* __restrict__ sdf, float* __restrict__ xb,
+                                                     const float* __restrict__ nub) {
   constexpr int Q = L::Q;
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= count) return;
@@ -1633,11 +1722,17 @@ __global__ void __launch_bounds__(64) k_boundary_tab(const __grid_constant__ wt_
     f[i] = fmaf(__uint_as_float(r[i].z), S::cvt(x1[i], 0.0f), fmaf(__uint_as_float(r[i].w), S::cvt(x2[i], 0.0f), g[i]));
   });
   const int ix = (int)(hc.x % P.nx);
-  if constexpr (LC)
-    collide_full<L, float>(P, f, ix, (hc.y & BC_WALL) != 0u, (hc.y & BC_GWALL) != 0u, fo, &CW,
-                           cl_wall_dist(__ldg(sdf + hc.x)));
-  else
+  if constexpr (MODE == FM_FEATURES) {
+    float x[CL_IN];
+    collide_full<L, float>(P, f, ix, false, false, fo, -1.0f, x, cl_wall_dist(__ldg(sdf + hc.x)));
+#pragma unroll
+    for (int q = 0; q < CL_IN; q++) xb[(size_t)k * CL_IN + q] = x[q];
+    return;
+  } else if constexpr (MODE == FM_NU) {
+    collide_full<L, float>(P, f, ix, (hc.y & BC_WALL) != 0u, (hc.y & BC_GWALL) != 0u, fo, __ldg(nub + k));
+  } else {
     collide_full<L, float>(P, f, ix, (hc.y & BC_WALL) != 0u, (hc.y & BC_GWALL) != 0u, fo);
+  }
   static_for<Q>([&](auto I) {
     constexpr int i = I;
     S::st(fout, (size_t)i * P.n + hc.x, fo[i], (float)Wc<L, i>::v);
@@ -2178,6 +2273,27 @@ static cudaError_t init_t(wt_solver* s) {
   return cudaGetLastError();
 }
 
+// face cells of the learned closure's row buffer: every cell of the 2 ny + 2 (nz - 2) face rows
+static size_t closure_face_cells(const wt_solver* s) {
+  return (size_t)(2 * s->dims.ny + 2 * (s->dims.nz - 2)) * (size_t)s->dims.nx;
+}
+
+cudaError_t closure_rows_reserve(wt_solver* s, bool* grown) {
+  *grown = false;
+  if (!s->is3d) return cudaSuccess;
+  const size_t rows = closure_face_cells(s) + s->btab_cap;
+  if (rows <= s->lc_rows_cap && s->lc_rows) return cudaSuccess;
+  cudaError_t e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return e;
+  cudaFree(s->lc_rows);
+  s->lc_rows = nullptr;
+  s->lc_rows_cap = 0;
+  if ((e = cudaMalloc((void**)&s->lc_rows, rows * (CL_IN + 1) * sizeof(float))) != cudaSuccess) return e;
+  s->lc_rows_cap = rows;
+  *grown = true;
+  return cudaSuccess;
+}
+
 // the vectorised kernel indexes populations with 32-bit element offsets
 
 template <class L, class S>
@@ -2222,12 +2338,35 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
         const int fby = 256 / fbx;
         const dim3 fgrid((runs2 + fbx - 1) / fbx, (fr + fby - 1) / fby, 1);
         if constexpr (L::DIM == 3) {
-          if (cw != nullptr)
-            k_face_lc<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(
-                s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, s->closure_w);
-          else
+          if (cw != nullptr) {
+            // learned closure: features of the face rows and wall cells, one tensor-core pass for
+            // their eddy viscosities, then their collisions
+            const size_t fc = closure_face_cells(s);
+            const size_t rows = fc + (size_t)s->nbnd;
+            if (s->lc_rows == nullptr || rows > s->lc_rows_cap) return cudaErrorInvalidValue;
+            float* xb = s->lc_rows;
+            float* nub = s->lc_rows + s->lc_rows_cap * CL_IN;
+            k_face_lc<L, S, FM_FEATURES><<<fgrid, dim3(fbx, fby), 0, bs>>>(
+                s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, xb, nub);
+            s->launches++;
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            if (s->nbnd > 0) {
+              k_boundary_tab<L, S, FM_FEATURES><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
+                  s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
+                  (uint32_t)s->btab_cap, s->sdf, xb + fc * CL_IN, nub + fc);
+              s->launches++;
+              if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            }
+            k_closure_rows<<<(unsigned)((rows + 2 * LC_THREADS - 1) / (2 * LC_THREADS)), LC_THREADS, LC_SMEM_BYTES,
+                             bs>>>(xb, (uint32_t)rows, nub, cw, s->closure_p, s->err_dev);
+            s->launches++;
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            k_face_lc<L, S, FM_NU><<<fgrid, dim3(fbx, fby), 0, bs>>>(
+                s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, xb, nub);
+          } else {
             k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin,
                                                              (typename S::T*)fout, s->cls, s->gs);
+          }
         } else {
           k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin, (typename S::T*)fout,
                                                            s->cls, s->gs);
@@ -2237,14 +2376,16 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
       }
       if (s->nbnd > 0) {
         if (cw != nullptr) {
-          if constexpr (L::DIM == 3)
-            k_boundary_tab<L, S, true><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
+          if constexpr (L::DIM == 3) {
+            const size_t fc = closure_face_cells(s);
+            k_boundary_tab<L, S, FM_NU><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
                 s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
-                (uint32_t)s->btab_cap, s->sdf, s->closure_w);
+                (uint32_t)s->btab_cap, s->sdf, nullptr, s->lc_rows + s->lc_rows_cap * CL_IN + fc);
+          }
         } else {
           k_boundary_tab<L, S><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
               s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
-              (uint32_t)s->btab_cap, s->sdf, NoClosure{0});
+              (uint32_t)s->btab_cap, s->sdf, nullptr, nullptr);
         }
         s->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -2268,9 +2409,10 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
           const int rpb = LC_THREADS / tpr;
           const int64_t ntiles = (int64_t)((runs2 + tpr - 1) / tpr) * ((s->dims.ny + rpb - 1) / rpb) * s->dims.nz;
           auto kern = s->kp.collision == 1u ? k_stream_collide_lc<S, true> : k_stream_collide_lc<S, false>;
-          kern<<<(unsigned)ntiles, LC_THREADS, LC_SMEM_BYTES, s->stream>>>(
-              s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, cw, s->closure_w.p,
-              tpr, s->err_dev);
+          const int64_t grid_lc = (ntiles + LC_TILES_PER_BLOCK - 1) / LC_TILES_PER_BLOCK;
+          kern<<<(unsigned)grid_lc, LC_THREADS, LC_SMEM_BYTES, s->stream>>>(
+              s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, cw, s->closure_p,
+              tpr, (uint32_t)ntiles, s->err_dev);
           s->launches++;
           if ((e = cudaGetLastError()) != cudaSuccess) return e;
           if (s->aux) {
@@ -2350,7 +2492,7 @@ static cudaError_t aux_t(wt_solver* s, const void* fin, void* fout, cudaStream_t
     if (s->nbnd > 0) {
       k_boundary_tab<L, S><<<(s->nbnd + 63) / 64, 64, 0, s->aux>>>(
           s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
-          (uint32_t)s->btab_cap, s->sdf, NoClosure{0});
+          (uint32_t)s->btab_cap, s->sdf, nullptr, nullptr);
       s->launches++;
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
