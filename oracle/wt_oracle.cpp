@@ -241,13 +241,14 @@ static float cl_wall_dist(uint32_t s) {
   return d < WT_CLOSURE_WALL_CAP ? d : WT_CLOSURE_WALL_CAP;
 }
 
-/* gelu(x) = x (1/2 + tanh(u) / 2), u = x (C0 + C1 x^2), C0 = sqrt(2/pi), C1 = 0.044715 C0 */
+/* gelu(x) = (x + x tanh(u)) / 2, u = x (C0 + C1 x^2), C0 = sqrt(2/pi), C1 = 0.044715 C0; x + x tanh(u)
+ * is one fma, halved exactly */
 static const float GELU_C0 = 0.7978845608028654f, GELU_C1 = 0.035677408136300125f,
                    GELU_C1x3 = 0.10703222440890037f;
 
 static float cl_gelu(float x) {
   const float t = std::tanh(x * std::fma(GELU_C1, x * x, GELU_C0));
-  return x * std::fma(0.5f, t, 0.5f);
+  return 0.5f * std::fma(x, t, x);
 }
 
 static float cl_gelu_d(float x, float& d) {
@@ -256,7 +257,7 @@ static float cl_gelu_d(float x, float& d) {
   const float q = std::fma(0.5f, t, 0.5f);
   const float du = std::fma(GELU_C1x3, x2, GELU_C0);
   d = std::fma((0.5f * x) * std::fma(-t, t, 1.0f), du, q);
-  return x * q;
+  return 0.5f * std::fma(x, t, x);
 }
 
 static float cl_softplus(float z) { return z > 20.0f ? z : std::log1p(std::exp(z)); }

@@ -89,17 +89,20 @@ __device__ __forceinline__ float tanh_fast(float x) {
   return r;
 }
 
-// gelu, tanh form; explicit roundings so every kernel evaluates it identically
+// gelu, tanh form, as (x + x tanh(u)) / 2 with one fma; explicit roundings so every kernel
+// evaluates it identically
 __device__ __forceinline__ float cl_gelu(float x) {
   const float u = __fmul_rn(x, __fmaf_rn(GELU_C1, __fmul_rn(x, x), GELU_C0));
-  return __fmul_rn(x, __fmaf_rn(0.5f, tanh_fast(u), 0.5f));
+  return __fmul_rn(0.5f, __fmaf_rn(x, tanh_fast(u), x));
 }
-// the same on two lanes with f32x2 instructions (identical per-lane roundings)
-__device__ __forceinline__ float2 cl_gelu2(float2 x) {
+// twice gelu on two lanes with f32x2 instructions: x + x tanh(u), the same per-lane roundings as
+// cl_gelu without its exact halving. The inference kernels fold the 1/2 into the next layer's
+// weights (the bf16 W2 image and w3 are stored halved), which leaves every product unchanged.
+__device__ __forceinline__ float2 cl_gelu2x(float2 x) {
   const float2 u = __fmul2_rn(x, __ffma2_rn(make_float2(GELU_C1, GELU_C1), __fmul2_rn(x, x),
                                             make_float2(GELU_C0, GELU_C0)));
   const float2 t = make_float2(tanh_fast(u.x), tanh_fast(u.y));
-  return __fmul2_rn(x, __ffma2_rn(make_float2(0.5f, 0.5f), t, make_float2(0.5f, 0.5f)));
+  return __ffma2_rn(x, t, x);
 }
 // gelu and its derivative d = q + (x/2)(1 - t^2)(C0 + 3 C1 x^2), q = 1/2 + t/2
 __device__ __forceinline__ float cl_gelu_d(float x, float& d) {
@@ -108,9 +111,18 @@ __device__ __forceinline__ float cl_gelu_d(float x, float& d) {
   const float q = __fmaf_rn(0.5f, t, 0.5f);
   const float du = __fmaf_rn(GELU_C1x3, x2, GELU_C0);
   d = __fmaf_rn(__fmul_rn(__fmul_rn(0.5f, x), __fmaf_rn(-t, t, 1.0f)), du, q);
-  return __fmul_rn(x, q);
+  return __fmul_rn(0.5f, __fmaf_rn(x, t, x));
 }
-__device__ __forceinline__ float cl_softplus(float z) { return z > 20.0f ? z : log1pf(expf(z)); }
+// softplus(z) = max(z, 0) + log1p(e), e = exp(-|z|) in (0, 1], from the fast exponential; log1p
+// from its Taylor series e - e^2/2 + e^3/3 - e^4/4 below e = 1/32 (truncation under 2e-7 of the
+// result), else the fast logarithm of 1 + e (absolute error near 4e-7 on a result of at least 0.03)
+__device__ __forceinline__ float cl_softplus(float z) {
+  const float e = __expf(-fabsf(z));
+  const float l = e < 0.03125f
+                      ? e * __fmaf_rn(e, __fmaf_rn(e, __fmaf_rn(e, -0.25f, 0.333333343f), -0.5f), 1.0f)
+                      : __logf(1.0f + e);
+  return fmaxf(z, 0.0f) + l;
+}
 __device__ __forceinline__ float cl_sigmoid(float z) { return 1.0f / (1.0f + expf(-z)); }
 
 __device__ __forceinline__ float cl_sqrt(float x) {
@@ -156,7 +168,7 @@ __host__ __device__ inline ClosureParams closure_params(const wt_closure& c) {
   for (int j = 0; j < CL_H; j++) {
     p.b1[j] = c.b1[j];
     p.b2[j] = c.b2[j];
-    p.w3[j] = bf16r(c.w3[j]);
+    p.w3[j] = 0.5f * bf16r(c.w3[j]);  // halved: the kernels' hidden layers hold twice gelu
   }
   p.b3 = c.b3;
   p.nu_scale = c.nu_scale;
@@ -176,9 +188,9 @@ __host__ __device__ inline void closure_pack(const wt_closure& c, ClosureDev& d)
     }
   for (int i = 0; i < CL_H; i++)
     for (int j = 0; j < CL_H; j++) {
-      const uint16_t b = bf16_bits(c.w2[i][j]);
-      d.w2img[umma::kmaj_off(j, i, CL_H) / 2] = b;
-      d.w2timg[umma::kmaj_off(i, j, CL_H) / 2] = b;
+      // bf16(w / 2) = bf16(w) / 2: the forward image is halved like w3
+      d.w2img[umma::kmaj_off(j, i, CL_H) / 2] = bf16_bits(0.5f * c.w2[i][j]);
+      d.w2timg[umma::kmaj_off(i, j, CL_H) / 2] = bf16_bits(c.w2[i][j]);
     }
 }
 

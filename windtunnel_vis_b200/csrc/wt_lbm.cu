@@ -1306,7 +1306,7 @@ __device__ __forceinline__ float2 lc_network2(uint8_t* smem, uint32_t tmem, uint
 #pragma unroll
       for (int e = 0; e < 4; e++) {
         const int j = 8 * c + 2 * e;
-        const float2 g = cl_gelu2(__fadd2_rn(make_float2(v[c][2 * e], v[c][2 * e + 1]),
+        const float2 g = cl_gelu2x(__fadd2_rn(make_float2(v[c][2 * e], v[c][2 * e + 1]),
                                              make_float2(CP.b1[j], CP.b1[j + 1])));
         pk[e] = bf16x2_bits(g.x, g.y);
       }
@@ -1344,7 +1344,7 @@ __device__ __forceinline__ float2 lc_network2(uint8_t* smem, uint32_t tmem, uint
 #pragma unroll
       for (int e = 0; e < 4; e++) {
         const int j = 8 * c + 2 * e;
-        const float2 g = cl_gelu2(__fadd2_rn(make_float2(v[c][2 * e], v[c][2 * e + 1]),
+        const float2 g = cl_gelu2x(__fadd2_rn(make_float2(v[c][2 * e], v[c][2 * e + 1]),
                                              make_float2(CP.b2[j], CP.b2[j + 1])));
         z = __ffma2_rn(g, make_float2(CP.w3[j], CP.w3[j + 1]), z);
       }
@@ -1405,8 +1405,9 @@ __global__ void __launch_bounds__(LC_THREADS) k_closure_rows(const float* __rest
 // its 512. After each tile the block agrees on `ok`; a timed-out wait ends the loop for the whole
 // block.
 constexpr int LC_TILES_PER_BLOCK = 4;
+constexpr int LC_BLOCKS_PER_SM = 7;  // the shared-memory limit; registers are capped to match
 template <class S, bool BGK>
-__global__ void __launch_bounds__(LC_THREADS) k_stream_collide_lc(const __grid_constant__ wt_kparams P,
+__global__ void __launch_bounds__(LC_THREADS, LC_BLOCKS_PER_SM) k_stream_collide_lc(const __grid_constant__ wt_kparams P,
                                                                    const typename S::T* __restrict__ fin,
                                                                    typename S::T* __restrict__ fout,
                                                                    const uint8_t* __restrict__ cls, int gs,
