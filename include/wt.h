@@ -265,7 +265,13 @@ int wt_probes(wt_solver* s, const float* pos4, int32_t count, float* out8);
  * (bx * by <= 256; 0, 0 = one row of up to 128 threads), and `kernel` = occupancy hint of the
  * vectorised kernel: 0 = none, 2..4 = registers capped so that many 256-thread CTAs fit on an SM.
  * Until this call or wt_autotune, a handle runs 2 cells per thread, default blocks, and hint 4 for
- * the regularized collision (none for BGK). */
+ * the regularized collision (none for BGK).
+ * kernel = WT_LAUNCH_ROW_PIPELINE (param 2, bx 0) selects the row pipeline for D3Q19 with f16 / f32
+ * storage: a producer warp streams whole interior rows into shared memory with bulk copies while
+ * four consumer warps collide the previous rows; `by` = interior rows per block (0 = 4, at most 16).
+ * It needs nx % 8 == 0 (f16) or nx % 4 == 0 (f32) and 3 x 19 x nx populations within 48 KB of
+ * shared memory; elsewhere the vectorised kernel runs. */
+#define WT_LAUNCH_ROW_PIPELINE 8
 int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32_t by);
 int wt_get_launch(const wt_solver* s, int32_t* out4);
 /* The project's launch tuner: times every applicable launch candidate on this handle's

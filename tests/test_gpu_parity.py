@@ -46,8 +46,9 @@ def _as_float(a):
 
 
 # (kernel, param, bx, by): 1 / 2 / 4 cells per thread, explicit and default block shapes
+# (8, 2, 0, rows): the row pipeline (3-D tunnels with nx % 8 == 0; the others run the vectorised kernel)
 LAUNCHES = {"reg1": (0, 1, 0, 0), "reg2": (0, 2, 32, 4), "reg4": (0, 4, 32, 4), "reg2d": (0, 2, 0, 0),
-            "hint4": (4, 2, 0, 0)}
+            "hint4": (4, 2, 0, 0), "rows2": (8, 2, 0, 2)}
 CASES = [(p, k) for p in ("f32", "f16") for k in LAUNCHES] + [("f64", "reg1")]
 
 
@@ -203,9 +204,37 @@ def test_errors_are_reported(gpu):
         s.set_params(dict(precision="f16"))
     with pytest.raises(WtError):
         Solver((0, 8, 8), dict(u=0.05, nu=0.02))
-    for bad in ((1, 2), (5, 2), (4, 4), (0, 2, 48, 2), (0, 2, 128, 4)):  # hint, cells, block shape
+    for bad in ((1, 2), (5, 2), (4, 4), (0, 2, 48, 2), (0, 2, 128, 4),  # hint, cells, block shape
+                (8, 4), (8, 2, 32, 1), (8, 2, 0, 17)):  # row pipeline: cells, block, rows per block
         with pytest.raises(WtError):
             s.set_launch(*bad)
+
+
+@pytest.mark.parametrize("prec", ["f16", "f32"])
+@pytest.mark.parametrize("pset", ["belt_periodic_les", "noslip_bgk_halfway"])
+@pytest.mark.parametrize("rows", [1, 3, 8, 16])
+def test_row_pipeline_matches_vectorised_kernel(gpu, prec, pset, rows):
+    """The row pipeline (rows streamed through shared memory by bulk copies) applies the vectorised
+    kernel's arithmetic to the same pulled populations: 20 steps of both agree to f32 rounding
+    (FMA contraction may differ between the two kernels). 22 x 18 interior rows do not divide by
+    3, 8 or 16, so the last block is partial."""
+    dims = (64, 24, 20)
+    params = dict(PARAM_SETS[pset], precision=prec)
+    flags, sdf, wheels = scene(dims)
+    runs = []
+    for launch in ((0, 2, 0, 0), (8, 2, 0, rows)):
+        g = Solver(dims, params)
+        g.upload_flags(flags)
+        g.upload_sdf(sdf)
+        g.set_wheels(wheels)
+        g.set_launch(*launch)
+        g.step(20)
+        runs.append(_as_float(g.read_populations()))
+        assert not g.sample()["unstable"]
+        g.destroy()
+    tol = 2e-6 if prec == "f32" else 2e-5
+    d = np.abs(runs[0] - runs[1]).max()
+    assert d <= tol, f"max |diff| {d:.3e}"
 
 
 # ---- voxelizer -------------------------------------------------------------------------------

@@ -911,13 +911,17 @@ int wt_write_tracers(wt_solver* s, const float* state4, int64_t count, const flo
 
 int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32_t by) {
   if (!s) return WT_E_INVALID;
-  if (!(kernel == 0 || (kernel >= 2 && kernel <= 4)))
+  if (kernel == WT_LAUNCH_ROW_PIPELINE) {
+    if (param != 2 || bx != 0 || by < 0 || by > 16)
+      return fail(s, WT_E_INVALID, "wt_set_launch: the row pipeline takes param 2, bx 0 and 0..16 rows per block");
+  } else if (!(kernel == 0 || (kernel >= 2 && kernel <= 4))) {
     return fail(s, WT_E_INVALID, "wt_set_launch: occupancy hint must be 0 or 2..4 CTAs per SM");
+  } else if (!(param == 1 || param == 2 || param == 4) || bx < 0 || by < 0 || bx * by > 256 || (bx % 32) != 0 ||
+             ((bx == 0) != (by == 0))) {
+    return fail(s, WT_E_INVALID, "wt_set_launch: need v in {1,2,4}, bx % 32 == 0, bx*by <= 256");
+  }
   if (kernel == 4 && param == 4)
     return fail(s, WT_E_INVALID, "wt_set_launch: 4 cells per thread supports occupancy hints 0..3");
-  if (!(param == 1 || param == 2 || param == 4) || bx < 0 || by < 0 || bx * by > 256 || (bx % 32) != 0 ||
-      ((bx == 0) != (by == 0)))
-    return fail(s, WT_E_INVALID, "wt_set_launch: need v in {1,2,4}, bx % 32 == 0, bx*by <= 256");
   s->sc_kernel = kernel;
   s->sc_param = param;
   s->sc_bx = bx;

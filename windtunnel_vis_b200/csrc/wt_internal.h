@@ -121,6 +121,8 @@ int lbm_block_x(const wt_solver* s);
 // sizes the learned closure's row buffer for the current lattice and boundary table (outside
 // graph capture); true in *grown when it was reallocated
 cudaError_t closure_rows_reserve(wt_solver* s, bool* grown);
+// dynamic shared memory of the row-pipeline bulk kernel on this handle, 0 where it does not apply
+size_t rows_pipeline_smem(const wt_solver* s);
 cudaError_t launch_classify(wt_solver* s);
 cudaError_t launch_boundary_table(wt_solver* s);
 cudaError_t launch_init(wt_solver* s);

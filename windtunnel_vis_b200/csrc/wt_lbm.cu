@@ -1026,6 +1026,166 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
                            blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z);
 }
 
+// ---- row pipeline: interior rows streamed through shared memory by bulk copies ---------------
+//
+// In k_stream_collide_v every thread's loads sit in front of its own collision, so memory latency
+// is hidden only by other warps. Here the loads of a block's next rows are in flight while its
+// current row collides: a producer warp streams whole interior rows into a ring of RP_STAGES
+// shared-memory stages with 1-D bulk copies (cp.async.bulk, completion counted in bytes on the
+// stage's mbarrier), and four consumer warps collide two cells per thread from shared memory and
+// store to global memory directly. For direction i the source row (y - c_iy, z - c_iz) of plane i
+// is one contiguous copy of nx populations; whole rows need no x halo, since x - 1 at the inlet is
+// replaced by the inlet equilibrium and x + 1 at the outlet is clamped, as in the vectorised
+// kernel. Block b takes `rows` consecutive interior rows (row r: y = 1 + r % (ny - 2),
+// z = 1 + r / (ny - 2)). Rows of plane i start 16-byte aligned when nx % 8 == 0 (f16) or
+// nx % 4 == 0 (f32); the ring must fit the default 48 KB of shared memory. Every wait is bounded: a
+// timeout sets bit 8 of the error word and the block stores nothing more. Consumers release a stage
+// after reading it; the producer reuses it only after all four consumer warps have.
+constexpr int RP_CONSUMERS = 128;              // four consumer warps, two cells per thread
+constexpr int RP_THREADS = RP_CONSUMERS + 32;  // and one producer warp
+constexpr int RP_STAGES = 3;
+constexpr int RP_MINB = 6;                     // blocks per SM the registers are capped for
+constexpr uint32_t RP_WAIT_LIMIT = 1u << 22;
+
+__device__ __forceinline__ void rp_copy_row(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+__device__ __forceinline__ void rp_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(mbar),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void rp_arrive(uint32_t mbar) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(mbar) : "memory");
+}
+
+template <class S, bool BGK>
+__global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_stream_collide_rows(const __grid_constant__ wt_kparams P,
+                                                                          const typename S::T* __restrict__ fin,
+                                                                          typename S::T* __restrict__ fout,
+                                                                          const uint8_t* __restrict__ cls, int gs,
+                                                                          uint32_t nrows, uint32_t rows,
+                                                                          int* __restrict__ err) {
+  typedef D3Q19 L;
+  typedef PairIO<S> IO;
+  typedef typename S::T T;
+  constexpr int Q = L::Q;
+  extern __shared__ __align__(128) uint8_t rp_smem[];
+  const int NX = P.nx, NY = P.ny;
+  const uint32_t N = P.n;
+  const uint32_t sy = (uint32_t)NX, sz = (uint32_t)NX * (uint32_t)NY;
+  const uint32_t stage_elems = (uint32_t)Q * (uint32_t)NX;
+  T* const ring = reinterpret_cast<T*>(rp_smem);
+  uint64_t* const full = reinterpret_cast<uint64_t*>(rp_smem + (size_t)RP_STAGES * stage_elems * sizeof(T));
+  uint64_t* const empty = full + RP_STAGES;
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+  const uint32_t row0 = blockIdx.x * rows;
+  const uint32_t nblk = min(rows, nrows - row0);
+  const uint32_t iny = (uint32_t)(NY - 2);
+  if (tid == 0) {
+#pragma unroll
+    for (int k = 0; k < RP_STAGES; k++) {
+      umma::mbar_init(full + k, 1);
+      umma::mbar_init(empty + k, RP_CONSUMERS / 32);
+    }
+  }
+  __syncthreads();
+  bool ok = true;
+  if (warp == RP_CONSUMERS / 32) {
+    // producer: lane 0 announces the stage's bytes, lanes 0 .. 18 copy one direction's row each
+    ptrdiff_t off = 0;  // plane i, shifted back by c_i along y and z
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      constexpr int cy = L::c[i][1], cz = L::c[i][2];
+      if (lane == (uint32_t)i) off = (ptrdiff_t)i * N - (ptrdiff_t)cy * sy - (ptrdiff_t)cz * sz;
+    });
+    for (uint32_t j = 0; j < nblk && ok; j++) {
+      const uint32_t st = j % RP_STAGES;
+      if (j >= RP_STAGES) ok = umma::mbar_wait(empty + st, ((j / RP_STAGES) - 1u) & 1u, RP_WAIT_LIMIT);
+      if (!ok) break;
+      const uint32_t r = row0 + j;
+      const uint32_t iy = 1u + r % iny, iz = 1u + r / iny;
+      const uint32_t fb = umma::smem_u32(full + st);
+      if (lane == 0) rp_expect_tx(fb, stage_elems * (uint32_t)sizeof(T));
+      __syncwarp();
+      if (lane < (uint32_t)Q)
+        rp_copy_row(umma::smem_u32(ring + (size_t)st * stage_elems + (size_t)lane * NX),
+                    fin + ((ptrdiff_t)(sy * iy + sz * iz) + off), (uint32_t)NX * (uint32_t)sizeof(T), fb);
+    }
+  } else {
+    for (uint32_t j = 0; j < nblk; j++) {
+      const uint32_t st = j % RP_STAGES;
+      const uint32_t r = row0 + j;
+      const uint32_t iy = 1u + r % iny, iz = 1u + r / iny;
+      const uint32_t rowbase = sy * iy + sz * iz;
+      int x0 = 2 * (int)tid;
+      auto cls_of = [&](int x) -> uint32_t {
+        const uint32_t idx = rowbase + (uint32_t)x;
+        return gs == 4 ? __ldg(reinterpret_cast<const unsigned int*>(cls + (idx & ~3u)))
+                       : (uint32_t)__ldg(reinterpret_cast<const unsigned short*>(cls + idx));
+      };
+      uint32_t cv = x0 < NX ? cls_of(x0) : 0u;  // in flight during the wait
+      ok = umma::mbar_wait(full + st, (j / RP_STAGES) & 1u, RP_WAIT_LIMIT) && ok;
+      const T* const sp0 = ring + (size_t)st * stage_elems;
+      for (; x0 < NX; x0 += 2 * RP_CONSUMERS) {
+        if (x0 != 2 * (int)tid) cv = cls_of(x0);
+        const bool clean = (cv & 0x03030303u) == 0u && ok;
+        const bool last = x0 + 2 >= NX;
+        float2 h[Q];
+        static_for<Q>([&](auto I) {
+          constexpr int i = I;
+          constexpr int cx = L::c[i][0];
+          constexpr float w = (float)Wc<L, i>::v;
+          const T* sp = sp0 + i * NX;
+          const float2 cur = IO::cvt(*reinterpret_cast<const typename IO::pair_t*>(sp + x0), w);
+          if constexpr (cx == 0) {
+            h[i] = cur;
+          } else if constexpr (cx > 0) {
+            h[i] = make_float2(IO::cvt1(*reinterpret_cast<const typename IO::one_t*>(sp + (x0 > 0 ? x0 - 1 : x0)), w),
+                               cur.x);
+          } else {
+            h[i] = make_float2(cur.y,
+                               IO::cvt1(*reinterpret_cast<const typename IO::one_t*>(sp + (last ? x0 + 1 : x0 + 2)), w));
+          }
+        });
+        if (x0 == 0) {
+          // inlet column: populations entering from x < 0 are the free-stream equilibrium
+          const float U = P.uin;
+          static_for<Q>([&](auto I) {
+            constexpr int i = I;
+            constexpr int cx = L::c[i][0];
+            if constexpr (cx > 0) {
+              constexpr float w = (float)Wc<L, i>::v;
+              h[i].x = w * P.rho_in * (1.0f + 3.0f * U + 4.5f * U * U - 1.5f * U * U) - w;
+            }
+          });
+        }
+        T* const ob = fout + rowbase + (uint32_t)x0;
+        collide_shifted2<L, BGK>(P, h, x0, [&](auto I, float2 v) {
+          constexpr int i = decltype(I)::value;
+          if (clean) IO::st(ob + (ptrdiff_t)i * N, 0u, v, (float)Wc<L, i>::v);
+        });
+      }
+      // this warp has read the stage: release it to the producer
+      __syncwarp();
+      if (lane == 0) rp_arrive(umma::smem_u32(empty + st));
+    }
+  }
+  if (!ok) atomicOr(err, 8);
+}
+
+// dynamic shared memory of the row pipeline (stages and barriers), 0 where it does not apply
+template <class S>
+static size_t rows_smem_bytes(const wt_solver* s) {
+  const int nx = s->dims.nx;
+  const int align = 16 / (int)sizeof(typename S::T);
+  if (!s->is3d || nx % align != 0 || nx < 8 || s->dims.ny < 3 || s->dims.nz < 3) return 0;
+  const size_t b = (size_t)RP_STAGES * 19 * (size_t)nx * sizeof(typename S::T) + 2 * RP_STAGES * sizeof(uint64_t);
+  return b <= 48 * 1024 ? b : 0;
+}
+
 // The bulk rows of every tunnel of a batch (D3Q19, two cells per thread): block b belongs to the
 // tunnel m with tile0[m] <= b < tile0[m + 1], and covers tile b - tile0[m] of its grid.
 // The block's tunnel parameters are copied to shared memory once, so the body reads them with
@@ -2250,6 +2410,12 @@ static cudaError_t classify_all_t(wt_solver* s) {
   return boundary_table_t<L, S>(s);
 }
 
+size_t rows_pipeline_smem(const wt_solver* s) {
+  if (s->prec == WT_PREC_F16) return rows_smem_bytes<StF16>(s);
+  if (s->prec == WT_PREC_F32) return rows_smem_bytes<StF32>(s);
+  return 0;
+}
+
 cudaError_t launch_boundary_table(wt_solver* s) {
   if (s->gs == 1) return cudaSuccess;
   WT_DISPATCH(boundary_table_t, s);
@@ -2414,6 +2580,24 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
           kern<<<(unsigned)grid_lc, LC_THREADS, LC_SMEM_BYTES, s->stream>>>(
               s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, cw, s->closure_p,
               tpr, (uint32_t)ntiles, s->err_dev);
+          s->launches++;
+          if ((e = cudaGetLastError()) != cudaSuccess) return e;
+          if (s->aux) {
+            if ((e = cudaEventRecord(s->ev_join, s->aux)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(s->stream, s->ev_join, 0)) != cudaSuccess) return e;
+          }
+          return cudaSuccess;
+        }
+      }
+      if constexpr (L::DIM == 3) {
+        const size_t rp_smem = rows_smem_bytes<S>(s);
+        if (mb == WT_LAUNCH_ROW_PIPELINE && V == 2 && rp_smem > 0) {
+          // row pipeline: `by` interior rows per block (default 4)
+          const uint32_t nrows = (uint32_t)(s->dims.ny - 2) * (uint32_t)(s->dims.nz - 2);
+          const uint32_t rows = s->sc_by > 0 ? (uint32_t)s->sc_by : 4u;
+          auto kern = s->kp.collision == 1u ? k_stream_collide_rows<S, true> : k_stream_collide_rows<S, false>;
+          kern<<<(nrows + rows - 1) / rows, RP_THREADS, rp_smem, s->stream>>>(
+              s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, nrows, rows, s->err_dev);
           s->launches++;
           if ((e = cudaGetLastError()) != cudaSuccess) return e;
           if (s->aux) {

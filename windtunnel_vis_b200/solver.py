@@ -261,7 +261,8 @@ class Solver:
     def set_launch(self, kernel, param, bx=0, by=0):
         """Stream-collide launch: kernel = occupancy hint (0 none, 2..4 CTAs of 256 threads per
         SM), param = cells per thread along x (1 = the scalar kernel, 2 or 4), block bx x by
-        (0 = default)."""
+        (0 = default). kernel = 8 (param 2, bx 0) selects the row pipeline with `by` interior rows
+        per block (0 = 4)."""
         self._check(self._lib.wt_set_launch(self._h, int(kernel), int(param), int(bx), int(by)))
 
     def get_launch(self):
