@@ -956,6 +956,8 @@ int wt_autotune(wt_solver* s, int32_t iters, int32_t* out4) {
       }
     }
   }
+  if (wt::rows_pipeline_smem(s) > 0 && s->dims.nx % 2 == 0)
+    for (int rows : {2, 4, 8}) cands.push_back({WT_LAUNCH_ROW_PIPELINE, 2, 0, rows});
   cands.push_back({0, 1, 0, 0});
   cudaEvent_t e0, e1;
   WT_CUDA(s, cudaEventCreate(&e0), "autotune");
