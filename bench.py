@@ -475,6 +475,8 @@ def run_ours(args, rank, world, local_rank, dist):
                      "kernel": ("one lattice update: k_stream_collide_lc<StF16> (bulk, network on tcgen05) overlapped "
                                 "with the face rows and wall cells (features, k_closure_rows on tcgen05, collision)"
                                 if args.closure else
+                                "one lattice update: k_stream_collide_rows<StF16> (bulk, row pipeline) overlapped "
+                                "with k_face_v and k_boundary_tab" if shape[0] == 8 else
                                 "one lattice update: k_stream_collide_v<D3Q19,StF16> (bulk) overlapped with "
                                 "k_face_v and k_boundary_tab" if shape[1] > 1 else "k_stream_collide<D3Q19,StF16>"),
                      "bytes_alg_per_update": n * BYTES_PER_UPDATE, "traffic_per": "lattice update (ncu, steady state)",

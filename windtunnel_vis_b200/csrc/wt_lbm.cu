@@ -1017,13 +1017,18 @@ __device__ __forceinline__ void bulk_cells(const wt_kparams& P, const typename S
   }
 }
 
+// zrev != 0 sweeps the z-planes in descending order (block z index nz - 1 - blockIdx.z). Steps
+// alternate the direction, so each step starts on the planes the previous step wrote last, which
+// are still in L2 (the two population buffers are larger than L2; a fixed order would always
+// start on the planes evicted first). Every cell's result is the same in either order.
 template <class L, class S, int V, int MINB, bool BGK>
 __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(const __grid_constant__ wt_kparams P,
                                                           const typename S::T* __restrict__ fin,
                                                           typename S::T* __restrict__ fout,
-                                                          const uint8_t* __restrict__ cls, int gs) {
+                                                          const uint8_t* __restrict__ cls, int gs, int zrev) {
   bulk_cells<L, S, V, BGK>(P, fin, fout, cls, gs, (blockIdx.x * blockDim.x + threadIdx.x) * V,
-                           blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z);
+                           blockIdx.y * blockDim.y + threadIdx.y,
+                           zrev ? (int)(gridDim.z - 1u - blockIdx.z) : (int)blockIdx.z);
 }
 
 // ---- row pipeline: interior rows streamed through shared memory by bulk copies ---------------
@@ -2557,15 +2562,17 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
         s->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
       }
-      // the bulk kernel on the main stream, concurrently with the auxiliary work
+      // the bulk kernel on the main stream, concurrently with the auxiliary work; steps writing
+      // buffer 1 sweep z upwards, steps writing buffer 0 downwards
+      const int zrev = fout == s->f[0] ? 1 : 0;
 #define WT_LAUNCH_V(VV, MB)                                                                                     \
   do {                                                                                                             \
     if (s->kp.collision == 1u)                                                                                     \
       k_stream_collide_v<L, S, VV, MB, true><<<grid, block, 0, s->stream>>>(                                       \
-          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs);                                  \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev);                            \
     else                                                                                                           \
       k_stream_collide_v<L, S, VV, MB, false><<<grid, block, 0, s->stream>>>(                                      \
-          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs);                                  \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev);                            \
   } while (0)
       const int mb = s->sc_kernel;
       if constexpr (L::DIM == 3) {
