@@ -22,6 +22,7 @@ import re
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -87,7 +88,7 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"wt_bench_clocks_rank{index}_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
@@ -108,7 +109,9 @@ class Clocks:
     def summary(self):
         if not self.proc:
             return None
-        rows = [r.split(", ") for r in open(self.path).read().strip().split("\n")[1:] if r.strip()]
+        with open(self.path) as fh:
+            rows = [r.split(", ") for r in fh.read().strip().split("\n")[1:] if r.strip()]
+        os.remove(self.path)
         if not rows:
             return None
         sm = [float(r[1].split()[0]) for r in rows]

@@ -1,20 +1,20 @@
 """Generate tests/golden/lattice.json from the reference's own lattice definition.
 
-Reads src/solver/lattice.ts of the reference checkout (path given by REFERENCE_ROOT, default
-/root/reference), extracts the D2Q9 and D3Q19 velocity sets and weights from the `build(...)`
+Reads src/solver/lattice.ts of the reference checkout (its root given by the REFERENCE_ROOT
+environment variable, which is required), extracts the D2Q9 and D3Q19 velocity sets and weights from the `build(...)`
 calls (lattice.ts:39-60), and derives opp / mirrorY / mirrorZ / mirrorYZ exactly as the
 reference's `build` does (lattice.ts:20-37): index of the reflected velocity in the same list.
 
 The JSON is committed; the tests read only the JSON, never the reference tree.
-Run:  python tests/golden/make_lattice_golden.py
+Run:  REFERENCE_ROOT=<reference checkout> python tests/golden/make_lattice_golden.py
 """
 import json
 import os
 import re
 from fractions import Fraction
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
-SRC = os.path.join(REF, "src", "solver", "lattice.ts")
+REF = os.environ.get("REFERENCE_ROOT", "")
+SRC = os.path.join(REF, "src", "solver", "lattice.ts") if REF else ""
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lattice.json")
 
 
@@ -63,6 +63,8 @@ def parse(text: str, name: str):
 
 
 def main():
+    if not REF:
+        raise SystemExit("set REFERENCE_ROOT to the root of the reference checkout")
     with open(SRC, encoding="utf-8") as fh:
         text = fh.read()
     data = {"source": "src/solver/lattice.ts:39-60", "D2Q9": parse(text, "D2Q9"), "D3Q19": parse(text, "D3Q19")}
