@@ -319,6 +319,8 @@ def components(s, peak, no_cpu):
         out["closure_step"]["cpu_ref_ms"] = round((time.perf_counter() - t0) * 1e3, 1)
         out["closure_step"]["cpu_threads"] = O.threads(0)
 
+    out["d2q9_cylinder"] = d2q9_cylinder(peak, no_cpu)
+
     # voxelizer (vehicle config, its own 512 x 256 x 256 handle)
     vd = (512, 256, 256)
     p, idx, M16, wheels, _ = vehicle_setup(vd)
@@ -347,6 +349,68 @@ def components(s, peak, no_cpu):
         out["voxelize"]["cpu_ref_s"] = round(time.perf_counter() - t0, 3)
         out["voxelize"]["cpu_kind"] = "port (f64, the reference's CPU voxelizer)"
         out["voxelize"]["cpu_threads"] = O.threads(0)
+    return out
+
+
+def d2q9_cylinder(peak, no_cpu, updates=4000, chunks=20):
+    """The D2Q9 cylinder channel (512 x 128, FP32 populations, BGK, D = 20 at (96, 65), u = 0.05,
+    Re = 100, rest state with seeded noise): lattice updates per second of the step alone (CUDA
+    events around `updates` steps on the solver's stream) and of the reference's sample chunk
+    (stepAndSample(50) with its statistics readback, host clock). The two 2.4 MB population
+    buffers stay in L2, so the step is bound by launch and synchronisation latency, not by HBM;
+    72 B per update (9 populations read and written in FP32) is reported for comparison."""
+    import torch
+
+    from windtunnel_vis_b200.solver import Solver
+    from windtunnel_vis_b200.validation import CHANNEL_DIMS, channel_geometry, channel_params
+
+    dims = CHANNEL_DIMS
+    n = dims[0] * dims[1]
+    flags, _, sdf = channel_geometry()
+    params = channel_params("f32")
+    s = Solver(dims, params)
+    s.upload_flags(flags)
+    s.upload_sdf(sdf)
+    for _ in range(3):
+        s.step_and_sample(CHUNK)
+    st = torch.cuda.ExternalStream(s.stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(st)
+    s.step(updates)
+    b.record(st)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / updates
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(chunks):
+        s.step_and_sample(CHUNK)
+    chunk_s = (time.perf_counter() - t0) / chunks
+    launch = s.get_launch()
+    s.destroy()
+    out = {"grid": list(dims), "storage": "f32", "collision": "bgk", "us_per_update": round(ms * 1e3, 3),
+           "mlups": round(n / ms / 1e3, 1), "steps_per_s": round(1e3 / ms, 1),
+           "chunk_mlups": round(n * CHUNK / chunk_s / 1e6, 1),
+           "chunk": f"stepAndSample({CHUNK}) incl. the sampling pass and the statistics readback (host clock)",
+           "launch": {"form": "10-step CUDA graphs: bulk kernel, face rows and wall cells per step",
+                      "cells_per_thread": launch[1], "block": [launch[2], launch[3]]},
+           "bytes_alg_per_update": n * 72, "l2_resident": True,
+           "achieved_gbs_equiv": round(n * 72 / ms / 1e6, 1)}
+    if not no_cpu:
+        from oracle import oracle as O
+
+        o = O.OracleSolver(dims, params)
+        o.upload_flags(flags)
+        o.upload_sdf(sdf)
+        o.step(1)
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < 3.0:
+            o.step(20)
+            done += 20
+        dt = time.perf_counter() - t0
+        out["cpu_ref_mlups"] = round(n * done / dt / 1e6, 2)
+        out["cpu_threads"] = O.threads(0)
+        out["cpu_kind"] = "port"
     return out
 
 

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define WT_ABI_VERSION 1
+#define WT_ABI_VERSION 2
 
 enum {
   WT_OK = 0,
@@ -96,7 +96,10 @@ typedef struct wt_kparams {
 /* SolverStats (src/solver/types.ts:31-42), decoded as SolverGPU.stepAndSample does
  * (src/solver/SolverGPU.ts:302-308). raw[] is the 8-slot reduction result:
  * [ΣFx, ΣFy, ΣFz, max|u|², Σρ on x = refX, n_ref, nan count, solid count]. The force sum is
- * accumulated in FP64. */
+ * accumulated in FP64.
+ * Extension (no counterpart in the reference): mass = Σρ over every fluid cell, each cell's density
+ * summed in FP64 in a fixed order (the global mass-conservation check), and fluid_cells = the
+ * number of cells in that sum. */
 typedef struct wt_stats {
   double fx, fy, fz;
   double max_u;
@@ -105,6 +108,8 @@ typedef struct wt_stats {
   int32_t unstable;
   int32_t reserved;
   double raw[8];
+  double mass;
+  int64_t fluid_cells;
 } wt_stats;
 
 /* WheelDef (src/voxelize/mesh.ts:54-60), grid space. */
@@ -279,6 +284,12 @@ int wt_get_launch(const wt_solver* s, int32_t* out4);
  * the state does not change) and keeps the fastest. out4 (may be NULL) receives
  * {kernel, param, bx, by}. */
 int wt_autotune(wt_solver* s, int32_t iters, int32_t* out4);
+/* Test hook (extension; no counterpart in the reference): the number of polls each consumer warp of
+ * the row pipeline (WT_LAUNCH_ROW_PIPELINE) makes on a stage's barrier before it gives up; polls < 0
+ * restores the default (4,194,304). With a small limit the consumers give up while the producer's
+ * copies are still in flight: the block stops storing, waits for its copies to land, and sets bit 8
+ * of the device error word, which the next sample turns into WT_E_CUDA. Only for tests of that path. */
+int wt_set_wait_limit(wt_solver* s, int64_t polls);
 
 /* ---- batches of tunnels ------------------------------------------------------------------- */
 /* No counterpart in the reference, whose studies panel runs one tunnel at a time
@@ -409,8 +420,8 @@ int64_t wt_launch_count(const wt_solver* s);
  * momentum-exchange force and the reductions, as wt_sample does for a handle. The call allocates
  * nothing: no cudaMalloc, no cudaFree, no allocating library routine.
  *
- * The pass needs a reduction scratch of one 64-byte slot per 256 cells. It is a fixed array in
- * the library's device memory (1 MiB per device), so grids are limited to
+ * The pass needs a reduction scratch of one 80-byte slot per 256 cells. It is a fixed array in
+ * the library's device memory (1.25 MiB per device), so grids are limited to
  * WT_SAMPLE_NOALLOC_MAX_CELLS cells; larger grids are rejected with WT_E_INVALID.
  *
  * Buffers: device memory of the device current on the calling thread, laid out as a handle's:

@@ -190,7 +190,7 @@ class OracleSolver:
     def sample(self):
         if self.pending_init:
             self._init()
-        res = np.zeros(8, np.float64)
+        res = np.zeros(10, np.float64)
         lib().or_macro(C.byref(dims_of(self.dims)), C.byref(self.kp), self.prec, _p(self.a), _p(self.flags),
                        _p(self.sdf), _p(self.wheels8), self.nwheels, _p(self.vel), _p(self.meanA), _p(self.meanB),
                        _p(res))
@@ -212,7 +212,9 @@ def decode_stats(d, step):
         "rhoRef": float(d[4] / d[5]) if d[5] > 0 else 1.0,
         "unstable": bool(d[6] > 0 or not np.isfinite(d[0]) or d[3] > 0.25),
         "step": int(step),
-        "raw": np.array(d, np.float64),
+        "raw": np.array(d[:8], np.float64),
+        "mass": float(d[8]) if len(d) > 8 else float("nan"),
+        "fluidCells": int(d[9]) if len(d) > 9 else -1,
     }
 
 

@@ -552,6 +552,7 @@ struct MacroAcc {
   double F[3];
   float maxuu;
   double rho_ref, n_ref, nan, solid;
+  double mass, fluid; /* global mass-conservation check (extension): FP64 sum of fluid densities */
 };
 
 template <int PREC> static void macro_cell(const Ctx& X, const Pops<PREC>& Fp, size_t idx, float* vel4,
@@ -632,6 +633,8 @@ template <int PREC> static void macro_cell(const Ctx& X, const Pops<PREC>& Fp, s
     for (int d = 0; d < 4; d++) meanA[4 * idx + d] = meanA[4 * idx + d] * (1.0f - a) + out[d] * a;
     meanB[idx] = meanB[idx] * (1.0f - a) + (float)uu * a;
     acc.rho_ref += (uint32_t)ix == P.ref_x ? (double)rho : 0.0;
+    acc.mass += (double)rho;
+    acc.fluid += 1.0;
   } else {
     /* density extrapolated into the solid from fluid face neighbours */
     static const int nb[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
@@ -1215,7 +1218,8 @@ void or_closure_grad(const wt_closure* c, const float* x, const float* y, int64_
 }
 
 /* macro pass on the current populations: vel4 (f32 view of the half4 velTex), EMA buffers
- * updated in place, result[8] = [ΣFx, ΣFy, ΣFz, max|u|², Σρ_ref, n_ref, nan, solid]. */
+ * updated in place, result[10] = [ΣFx, ΣFy, ΣFz, max|u|², Σρ_ref, n_ref, nan, solid] (the
+ * reference's reduction) followed by [Σρ over fluid cells in FP64, fluid cell count]. */
 int or_macro(const wt_dims* d, const wt_kparams* kp, int prec, const void* fin, const uint32_t* flags,
              const uint32_t* sdf, const float* wheels8, int nwheels, float* vel4, float* meanA, float* meanB,
              double* result) {
@@ -1237,6 +1241,8 @@ int or_macro(const wt_dims* d, const wt_kparams* kp, int prec, const void* fin, 
   result[5] = acc.n_ref;
   result[6] = acc.nan;
   result[7] = acc.solid;
+  result[8] = acc.mass;
+  result[9] = acc.fluid;
   return WT_OK;
 }
 

@@ -35,7 +35,7 @@ def test_library_exports_every_declared_symbol(wtlib):
     lib = C.CDLL(abi.LIB_PATH)
     missing = [n for n in declared_functions() if not hasattr(lib, n)]
     assert not missing, missing
-    assert lib.wt_version() == 1
+    assert lib.wt_version() == 2
 
 
 STRUCTS = {

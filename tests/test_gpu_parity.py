@@ -10,6 +10,7 @@ without it, so single-precision results differ by a few ulp per step):
                                 wall links), 1e-10 (f64); counts exact
   EMA means .................. relative 1e-4 (f32, f64), 5e-3 (f16)
   reference-plane density .... absolute 1e-5 (f32, f64), 5e-5 (f16)
+  fluid mass (FP64 sum) ...... relative 1e-12 (f64), 1e-6 (f32), 2e-5 (f16); fluid count exact
   velocity field ............. absolute 2e-6 (f32, f64), 1e-4 (f16)
   voxelizer flags, sdf, info . bit-exact (compiled without contraction)
   tracers .................... bit-exact state and trail
@@ -28,6 +29,7 @@ TOL = {"f64": (1e-12, 1e-12), "f32": (1e-6, 2e-5), "f16": (2e-5, 3e-4)}
 STAT_RTOL = {"f64": 1e-10, "f32": 1e-4, "f16": 5e-3}
 MEAN_TOL = {"f64": (1e-4, 1e-7), "f32": (1e-4, 1e-7), "f16": (5e-3, 5e-5)}
 VEL_ATOL = {"f64": 2e-6, "f32": 2e-6, "f16": 1e-4}  # f16: a few half ulps of ~10 populations
+MASS_RTOL = {"f64": 1e-12, "f32": 1e-6, "f16": 2e-5}  # FP64 sum of the fluid densities
 
 
 def _pair(oracle, dims, params):
@@ -82,6 +84,9 @@ def _check_against_oracle(oracle, dims, params, launch):
     assert abs(sg["rhoRef"] - so["rhoRef"]) <= (5e-5 if prec == "f16" else 1e-5)
     assert sg["raw"][5:].tolist() == so["raw"][5:].tolist()
     assert sg["step"] == so["step"] == 30 and not sg["unstable"]
+    # global mass-conservation check (extension): FP64 sum of the fluid cells' densities
+    assert sg["fluidCells"] == so["fluidCells"] == int((flags == 0).sum())
+    assert abs(sg["mass"] - so["mass"]) <= MASS_RTOL[prec] * so["mass"], (sg["mass"], so["mass"])
     vg = g.read_velocity()
     vo = o.vel.reshape(-1, 4)
     np.testing.assert_allclose(vg, vo, rtol=2e-3, atol=VEL_ATOL[prec])
@@ -238,6 +243,63 @@ def test_row_pipeline_matches_vectorised_kernel(gpu, prec, pset, rows):
     tol = 2e-6 if prec == "f32" else 2e-5
     d = np.abs(runs[0] - runs[1]).max()
     assert d <= tol, f"max |diff| {d:.3e}"
+
+
+@pytest.mark.parametrize("rows", [1, 4])
+def test_row_pipeline_second_x_pass(gpu, oracle, rows):
+    """nx = 320 with FP16 storage: each consumer thread takes x0 = 2 tid and x0 + 256, so the
+    second pass of the consumer loop (class byte reloaded, stage read at x0 + 256) runs; checked
+    against the oracle and against the vectorised kernel."""
+    dims = (320, 12, 10)
+    params = dict(PARAM_SETS["belt_periodic_les"], precision="f16")
+    flags, sdf, wheels = scene(dims)
+    o = oracle.OracleSolver(dims, params)
+    for s_ in (o,):
+        s_.upload_flags(flags)
+        s_.upload_sdf(sdf)
+        s_.set_wheels(wheels)
+    o.step(10)
+    runs = []
+    for launch in ((0, 2, 0, 0), (8, 2, 0, rows)):
+        g = Solver(dims, params)
+        g.upload_flags(flags)
+        g.upload_sdf(sdf)
+        g.set_wheels(wheels)
+        g.set_launch(*launch)
+        assert g.get_launch() == launch
+        g.step(10)
+        runs.append(_as_float(g.read_populations()))
+        g.destroy()
+    assert np.abs(runs[0] - runs[1]).max() <= 2e-5
+    assert np.abs(runs[1] - _as_float(o.current)).max() <= TOL["f16"][1]
+
+
+def test_row_pipeline_consumer_timeout_is_reported(gpu):
+    """Consumer waits that give up at once (a poll limit of 0) while the producer's copies are in
+    flight: the blocks store nothing, drain their copies and set bit 8 of the error word, which the
+    next sample reports as WT_E_CUDA; with the default limit restored the handle steps cleanly."""
+    dims = (64, 24, 20)
+    params = dict(PARAM_SETS["freeslip_reg"], precision="f16")
+    flags, sdf, wheels = scene(dims)
+    g = Solver(dims, params)
+    g.upload_flags(flags)
+    g.upload_sdf(sdf)
+    g.set_wheels(wheels)
+    g.set_launch(8, 2, 0, 4)
+    g.step(4)
+    saved = g.read_populations().copy()
+    ref = g.step_and_sample(4)
+    g.write_populations(saved)
+    g.set_wait_limit(0)
+    g.step(2)
+    with pytest.raises(WtError) as e:
+        g.sample()
+    assert e.value.code == abi.WT_E_CUDA and "error word 8" in str(e.value)
+    g.set_wait_limit(-1)
+    g.write_populations(saved)
+    st = g.step_and_sample(4)
+    assert not st["unstable"] and st["raw"].tolist() == ref["raw"].tolist()
+    g.destroy()
 
 
 # ---- voxelizer -------------------------------------------------------------------------------

@@ -17,7 +17,7 @@ def test_freestream(gpu):
 
 @pytest.mark.parametrize("prec", ["f32", "f16"])
 def test_cylinder_strouhal(gpu, prec):
-    # valscale 0.5 (D = 12): the oracle gives St = 0.1726, C_D = 1.501; published St 0.173
+    # valscale 0.5 (D = 12), Bouzidi walls: the oracle gives St = 0.1726, C_D = 1.501
     r = V.cylinder(lambda d, p: solver_factory(d, dict(p, precision=prec)), 0.5)
     m = r["metrics"]
     assert r["passed"], m
@@ -25,12 +25,64 @@ def test_cylinder_strouhal(gpu, prec):
     assert abs(m["cd_mean"] - 1.501) < 0.02, m
 
 
-def test_sphere_drag(gpu):
-    # D = 10 (valscale 0.5): within 20 % of Schiller-Naumann (validation.ts:137-184)
-    r = V.sphere(solver_factory, 0.5)
+def test_cylinder_published_run(gpu):
+    # the reference's published cylinder result (README.md:175): St = 0.173 from its D = 18 run
+    # (valscale 0.75), C_D about 1.5. The published table predates the reference's Bouzidi walls
+    # (README.md:262-264: they moved its D = 10 sphere from +23 % to +15 %), so the pin is the
+    # halfway bounce-back run; the Bouzidi run lands within the same margin.
+    for interp in (False, True):
+        m = V.cylinder(solver_factory, 0.75, interp=interp)["metrics"]
+        assert abs(m["St"] - 0.173) <= 0.003, (interp, m)
+        assert abs(m["cd_mean"] - 1.5) <= 0.05, (interp, m)
+
+
+@pytest.mark.parametrize("valscale,interp,cd_pub", [(0.5, False, 1.342), (0.7, False, 1.250),
+                                                    (0.5, True, 1.09173 * 1.15)])
+def test_sphere_published_runs(gpu, valscale, interp, cd_pub):
+    # the reference's published sphere drag (README.md:176): 1.342 at D = 10 (+23 %) and 1.250 at
+    # D = 14 (+14.5 %) with halfway bounce-back, and +15 % at D = 10 with Bouzidi walls
+    # (README.md:262-264), against Schiller-Naumann 1.0917 (validation.ts:137-184)
+    r = V.sphere(solver_factory, valscale, interp=interp)
     m = r["metrics"]
-    assert r["passed"], m
-    assert 1.15 < m["cd"] < 1.40, m
+    assert abs(m["cd"] / cd_pub - 1) <= 0.01, m
+
+
+def test_channel_cylinder_fp32_against_fp64_populations(gpu):
+    # the D2Q9 cylinder in a 512 x 128 channel (D = 20 at (96, 65), u = 0.05, Re = 100, BGK, rest
+    # state with seeded noise, 40,000 steps sampled every 50): FP32 populations against the FP64
+    # run of the same method on the GPU, St within 1 % and mean C_D within 0.5 %
+    r32 = V.cylinder_channel(solver_factory, "f32")
+    r64 = V.cylinder_channel(solver_factory, "f64")
+    m32, m64 = r32["metrics"], r64["metrics"]
+    assert r32["passed"] and r64["passed"], (m32, m64)
+    assert abs(m32["St"] / m64["St"] - 1) <= 1e-2, (m32, m64)
+    assert abs(m32["cd_mean"] / m64["cd_mean"] - 1) <= 5e-3, (m32, m64)
+    # from rest, the reference's equilibrium inlet (incoming populations at rho = 1, u = U) and the
+    # zero-gradient outlet settle where 3 rho* u* = 1 + 3 U - rho*: rho* about 1.039, u* about
+    # 0.74 U; on that inflow the shedding frequency is the unconfined cylinder's (St about 0.167)
+    assert abs(m64["rho_ref_end"] - 1.0388) < 2e-3 and abs(m64["u_inflow_end"] / 0.05 - 0.735) < 0.02, m64
+    assert abs(m64["St_inflow"] - 0.167) < 0.005, m64
+
+
+def test_channel_cylinder_matches_oracle_full_size(gpu, oracle):
+    # the same channel at full size, 300 steps from rest on both paths, then the sampling pass
+    dims = V.CHANNEL_DIMS
+    params = V.channel_params("f32")
+    flags, _, sdf = V.channel_geometry()
+    g = Solver(dims, params)
+    o = oracle.OracleSolver(dims, params)
+    for s in (g, o):
+        s.upload_flags(flags)
+        s.upload_sdf(sdf)
+    g.step(300)
+    o.step(300)
+    d = np.abs(g.read_populations().astype(np.float64) - o.current.astype(np.float64)).max()
+    assert d <= 1e-5, d
+    sg, so = g.sample(), o.sample()
+    assert np.abs(sg["raw"][:3] - so["raw"][:3]).max() <= 1e-4 * max(np.abs(so["raw"][:3]).max(), 1e-3)
+    assert sg["raw"][5:].tolist() == so["raw"][5:].tolist()
+    assert sg["fluidCells"] == so["fluidCells"] and abs(sg["mass"] / so["mass"] - 1) <= 1e-6
+    g.destroy()
 
 
 def test_full_size_fp16_against_fp32(gpu):

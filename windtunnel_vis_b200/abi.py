@@ -53,6 +53,7 @@ class Stats(C.Structure):
         ("fx", C.c_double), ("fy", C.c_double), ("fz", C.c_double),
         ("max_u", C.c_double), ("rho_ref", C.c_double), ("step", C.c_int64),
         ("unstable", C.c_int32), ("reserved", C.c_int32), ("raw", C.c_double * 8),
+        ("mass", C.c_double), ("fluid_cells", C.c_int64),
     ]
 
 
@@ -198,6 +199,7 @@ def _sig(lib):
         "wt_set_launch": ([S, i32, i32, i32, i32], C.c_int),
         "wt_get_launch": ([S, P(i32)], C.c_int),
         "wt_autotune": ([S, i32, P(i32)], C.c_int),
+        "wt_set_wait_limit": ([S, i64], C.c_int),
         "wt_stream": ([S], v),
         "wt_device": ([S], i32),
         "wt_launch_count": ([S], i64),

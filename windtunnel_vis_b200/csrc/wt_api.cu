@@ -223,6 +223,8 @@ int check_err_flag(wt_solver* s) {
 void decode(const wt_solver* s, const double* d, wt_stats* out) {
   std::memset(out, 0, sizeof *out);
   for (int k = 0; k < 8; k++) out->raw[k] = d[k];
+  out->mass = d[8];
+  out->fluid_cells = (int64_t)d[9];
   out->fx = d[0];
   out->fy = d[1];
   out->fz = d[2];
@@ -335,7 +337,7 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
     s->num_sms = 148;
   }
   // one macro block per 256 cells up to 4096 blocks (several cells per thread beyond: the block
-  // reductions amortise and the final reduce reads at most 256 KB), one 64-byte partial each
+  // reductions amortise and the final reduce reads at most 320 KB), one MACRO_SLOTS-double partial each
   s->partial_blocks = (int)std::min<size_t>((s->n + 255) / 256, 4096);
   bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
             create_priority_stream(&s->aux) == cudaSuccess &&
@@ -345,10 +347,10 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
             alloc((void**)&s->flags, s->n * 4, "flags") && alloc((void**)&s->sdf, s->n * 4, "sdf") &&
             alloc((void**)&s->cls, s->n, "cell class") && alloc((void**)&s->vel, s->n * 8, "velocity") &&
             alloc((void**)&s->meanA, s->n * 16, "meanA") && alloc((void**)&s->meanB, s->n * 4, "meanB") &&
-            alloc((void**)&s->partials, (size_t)s->partial_blocks * 64, "partials") &&
-            alloc((void**)&s->result_dev, 64, "result") && alloc((void**)&s->err_dev, 4, "error word") &&
+            alloc((void**)&s->partials, (size_t)s->partial_blocks * RESULT_BYTES, "partials") &&
+            alloc((void**)&s->result_dev, RESULT_BYTES, "result") && alloc((void**)&s->err_dev, 4, "error word") &&
             alloc((void**)&s->bnd_count, 4, "boundary counter");
-  if (ok && (cudaMallocHost((void**)&s->result_host, 64) != cudaSuccess ||
+  if (ok && (cudaMallocHost((void**)&s->result_host, RESULT_BYTES) != cudaSuccess ||
              cudaMallocHost((void**)&s->err_host, 4) != cudaSuccess ||
              cudaMallocHost((void**)&s->bnd_count_host, 4) != cudaSuccess)) {
     where = "cudaMallocHost(result)";
@@ -671,7 +673,7 @@ int wt_sample(wt_solver* s, wt_stats* out) {
   rc = ensure_classified(s);  // the macro pass reads the class byte
   if (rc) return rc;
   WT_CUDA(s, wt::launch_macro(s), "macro");
-  WT_CUDA(s, cudaMemcpyAsync(s->result_host, s->result_dev, 64, cudaMemcpyDeviceToHost, s->stream), "read result");
+  WT_CUDA(s, cudaMemcpyAsync(s->result_host, s->result_dev, RESULT_BYTES, cudaMemcpyDeviceToHost, s->stream), "read result");
   WT_CUDA(s, cudaMemcpyAsync(s->err_host, s->err_dev, 4, cudaMemcpyDeviceToHost, s->stream), "read error word");
   WT_CUDA(s, cudaStreamSynchronize(s->stream), "sample");
   if (*s->err_host != 0) return check_err_flag(s);
@@ -928,6 +930,13 @@ int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32
   s->sc_by = by;
   s->launch_explicit = true;
   invalidate_graphs(s);
+  return WT_OK;
+}
+
+int wt_set_wait_limit(wt_solver* s, int64_t polls) {
+  if (!s) return WT_E_INVALID;
+  s->rp_wait_limit = polls < 0 ? (1u << 22) : (uint32_t)std::min<int64_t>(polls, 0xffffffffll);
+  invalidate_graphs(s);  // the limit is a kernel argument captured in the step graphs
   return WT_OK;
 }
 
@@ -1303,7 +1312,7 @@ int wt_batch_sample(wt_batch* b, wt_stats* out) {
     if (rc) return bfail(b, rc, std::string("member: ") + s->err);
     cudaError_t e = wt::launch_macro(s);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(s->result_host, s->result_dev, 64, cudaMemcpyDeviceToHost, s->stream);
+      e = cudaMemcpyAsync(s->result_host, s->result_dev, RESULT_BYTES, cudaMemcpyDeviceToHost, s->stream);
     if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch sample: ") + cudaGetErrorString(e));
   }
   for (size_t k = 0; k < b->m.size(); k++) {

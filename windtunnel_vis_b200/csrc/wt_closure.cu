@@ -57,10 +57,11 @@ constexpr int TS_W2 = 46080;     // W2 image (N = out, K = in)
 constexpr int TS_W2T = 48128;    // W2 transposed image (N = in, K = out)
 constexpr int TS_DZ3 = 50176;    // dz3 [128] f32
 constexpr int TS_LOSS = 50688;   // per-row loss [128] f32
-constexpr int TS_BAR = 51200;    // mbarrier, then the tensor-memory address
+constexpr int TS_BAR = 51200;    // mbarrier, the tensor-memory address, pad, drain barrier
 // 53 KB of dynamic shared memory: at most 4 blocks per SM, whose 4 x 128 tensor-memory columns fit
 constexpr int TS_BYTES = 53 * 1024;
-static_assert(TS_BAR + 12 <= TS_BYTES, "layout");
+constexpr int TS_DRAIN = TS_BAR + 16;
+static_assert(TS_DRAIN + 8 <= TS_BYTES, "layout");
 
 // parameter offsets in the master vector
 constexpr int PO_W1 = 0, PO_B1 = 320, PO_W2 = 352, PO_B2 = 1376, PO_W3 = 1408, PO_B3 = 1440;
@@ -114,6 +115,7 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
   if (TRAIN && valid) y = __ldg(A.ys + si);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + TS_BAR);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + TS_BAR + 8);
+  uint64_t* dbar = reinterpret_cast<uint64_t*>(sm + TS_DRAIN);
   // weight images from the f32 master weights
   for (uint32_t e = tid; e < (uint32_t)(CL_H * CL_K1); e += TR_THREADS) {
     const uint32_t n = e / CL_K1, k = e % CL_K1;
@@ -126,7 +128,10 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
     *reinterpret_cast<uint16_t*>(sm + TS_W2 + umma::kmaj_off(j, i, CL_H)) = b;
     *reinterpret_cast<uint16_t*>(sm + TS_W2T + umma::kmaj_off(i, j, CL_H)) = b;
   }
-  if (tid == 0) umma::mbar_init(mbar, 1);
+  if (tid == 0) {
+    umma::mbar_init(mbar, 1);
+    umma::mbar_init(dbar, 1);
+  }
   if (warp == 0) umma::tmem_alloc(tslot, TR_TMEM_COLS);
   // x' row (zeros for padding rows)
   {
@@ -298,13 +303,11 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
       out[p] = acc;
     }
   }
-  umma::fence_before_sync();
+  // after a timed-out wait, the MMAs finish before their tensor memory is released
+  const bool drained = umma::drain_before_free(dbar, !ok, TR_WAIT_LIMIT);
   __syncthreads();
-  if (warp == 0) {
-    umma::fence_after_sync();
-    umma::tmem_free(tmem, TR_TMEM_COLS);
-  }
-  if (!ok) atomicOr(err, 4);
+  if (warp == 0) umma::tmem_free(tmem, TR_TMEM_COLS);
+  if (!ok || !drained) atomicOr(err, 4);
 }
 
 // sums of the block partials in f64, blocks in order

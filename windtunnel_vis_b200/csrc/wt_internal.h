@@ -12,6 +12,10 @@
 
 // step pairs captured in one long step graph
 constexpr int WT_LONG_PAIRS = 5;
+// doubles per block in the macro pass's partial reductions, and in its result: the reference's
+// 8-slot result followed by the FP64 fluid mass and the fluid cell count
+constexpr int MACRO_SLOTS = 10;
+constexpr size_t RESULT_BYTES = MACRO_SLOTS * sizeof(double);
 
 struct wt_solver {
   int device = 0;
@@ -74,7 +78,7 @@ struct wt_solver {
   float* meanB = nullptr;
   double* partials = nullptr;  // per-block partial reductions of the macro pass
   int partial_blocks = 0;
-  double* result_dev = nullptr;  // 8 doubles
+  double* result_dev = nullptr;  // MACRO_SLOTS doubles
   double* result_host = nullptr; // pinned
   wt::Wheels wheels{};
   // derived fields (binary16 x 4 per cell, allocated by the first wt_derive_fields): vorticity and
@@ -98,6 +102,8 @@ struct wt_solver {
   // thread along x (1 = scalar kernel), block sc_bx x sc_by of the vectorised kernel (0 = default)
   int block_x = 0;
   int sc_kernel = 0, sc_param = 2, sc_bx = 0, sc_by = 0;
+  // polls of each row-pipeline consumer wait before it gives up (wt_set_wait_limit)
+  uint32_t rp_wait_limit = 1u << 22;
   // false until wt_set_launch or wt_autotune chose a launch: the default then follows the collision
   // operator (occupancy hint 4 for the regularized collision, which fits 64 registers; none for BGK)
   bool launch_explicit = false;

@@ -1046,11 +1046,17 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
 // nx % 4 == 0 (f32); the ring must fit the default 48 KB of shared memory. Every wait is bounded: a
 // timeout sets bit 8 of the error word and the block stores nothing more. Consumers release a stage
 // after reading it; the producer reuses it only after all four consumer warps have.
+// Teardown: no block may exit while a bulk copy it issued can still write its shared memory. A
+// consumer warp whose wait on a stage gives up raises a shared abort flag before it releases the
+// stage, so the producer, which reads the flag after each wait on a released stage, never issues a
+// copy into a stage whose previous copy may still be landing. Every copy but the last one issued
+// into each stage was therefore waited for by the consumers; before exiting, the producer waits
+// (bounded) for those last ones.
 constexpr int RP_CONSUMERS = 128;              // four consumer warps, two cells per thread
 constexpr int RP_THREADS = RP_CONSUMERS + 32;  // and one producer warp
 constexpr int RP_STAGES = 3;
 constexpr int RP_MINB = 6;                     // blocks per SM the registers are capped for
-constexpr uint32_t RP_WAIT_LIMIT = 1u << 22;
+constexpr uint32_t RP_WAIT_LIMIT = 1u << 22;  // polls per wait (the consumers' limit is a parameter)
 
 __device__ __forceinline__ void rp_copy_row(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
@@ -1072,7 +1078,7 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_stream_collide_rows(con
                                                                           typename S::T* __restrict__ fout,
                                                                           const uint8_t* __restrict__ cls, int gs,
                                                                           uint32_t nrows, uint32_t rows,
-                                                                          int* __restrict__ err) {
+                                                                          uint32_t cwait, int* __restrict__ err) {
   typedef D3Q19 L;
   typedef PairIO<S> IO;
   typedef typename S::T T;
@@ -1085,6 +1091,7 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_stream_collide_rows(con
   T* const ring = reinterpret_cast<T*>(rp_smem);
   uint64_t* const full = reinterpret_cast<uint64_t*>(rp_smem + (size_t)RP_STAGES * stage_elems * sizeof(T));
   uint64_t* const empty = full + RP_STAGES;
+  volatile uint32_t* const abort_flag = reinterpret_cast<volatile uint32_t*>(empty + RP_STAGES);
   const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
   const uint32_t row0 = blockIdx.x * rows;
   const uint32_t nblk = min(rows, nrows - row0);
@@ -1095,6 +1102,7 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_stream_collide_rows(con
       umma::mbar_init(full + k, 1);
       umma::mbar_init(empty + k, RP_CONSUMERS / 32);
     }
+    *abort_flag = 0u;
   }
   __syncthreads();
   bool ok = true;
@@ -1106,9 +1114,14 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_stream_collide_rows(con
       constexpr int cy = L::c[i][1], cz = L::c[i][2];
       if (lane == (uint32_t)i) off = (ptrdiff_t)i * N - (ptrdiff_t)cy * sy - (ptrdiff_t)cz * sz;
     });
+    uint32_t issued = 0;
     for (uint32_t j = 0; j < nblk && ok; j++) {
       const uint32_t st = j % RP_STAGES;
-      if (j >= RP_STAGES) ok = umma::mbar_wait(empty + st, ((j / RP_STAGES) - 1u) & 1u, RP_WAIT_LIMIT);
+      if (j >= RP_STAGES) {
+        ok = umma::mbar_wait(empty + st, ((j / RP_STAGES) - 1u) & 1u, RP_WAIT_LIMIT);
+        // a consumer that gave up on this stage's previous copy raised the flag before releasing it
+        if (ok && *abort_flag != 0u) break;
+      }
       if (!ok) break;
       const uint32_t r = row0 + j;
       const uint32_t iy = 1u + r % iny, iz = 1u + r / iny;
@@ -1118,7 +1131,12 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_stream_collide_rows(con
       if (lane < (uint32_t)Q)
         rp_copy_row(umma::smem_u32(ring + (size_t)st * stage_elems + (size_t)lane * NX),
                     fin + ((ptrdiff_t)(sy * iy + sz * iz) + off), (uint32_t)NX * (uint32_t)sizeof(T), fb);
+      issued = j + 1;
     }
+    // drain: the last copy issued into each stage has landed before the block may exit
+    const uint32_t first = issued > (uint32_t)RP_STAGES ? issued - (uint32_t)RP_STAGES : 0u;
+    for (uint32_t j = first; j < issued; j++)
+      ok = umma::mbar_wait(full + j % RP_STAGES, (j / RP_STAGES) & 1u, RP_WAIT_LIMIT) && ok;
   } else {
     for (uint32_t j = 0; j < nblk; j++) {
       const uint32_t st = j % RP_STAGES;
@@ -1132,7 +1150,9 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_stream_collide_rows(con
                        : (uint32_t)__ldg(reinterpret_cast<const unsigned short*>(cls + idx));
       };
       uint32_t cv = x0 < NX ? cls_of(x0) : 0u;  // in flight during the wait
-      ok = umma::mbar_wait(full + st, (j / RP_STAGES) & 1u, RP_WAIT_LIMIT) && ok;
+      const bool landed = umma::mbar_wait(full + st, (j / RP_STAGES) & 1u, cwait);
+      if (!landed && lane == 0) *abort_flag = 1u;  // before this warp releases the stage below
+      ok = landed && ok;
       const T* const sp0 = ring + (size_t)st * stage_elems;
       for (; x0 < NX; x0 += 2 * RP_CONSUMERS) {
         if (x0 != 2 * (int)tid) cv = cls_of(x0);
@@ -1187,7 +1207,8 @@ static size_t rows_smem_bytes(const wt_solver* s) {
   const int nx = s->dims.nx;
   const int align = 16 / (int)sizeof(typename S::T);
   if (!s->is3d || nx % align != 0 || nx < 8 || s->dims.ny < 3 || s->dims.nz < 3) return 0;
-  const size_t b = (size_t)RP_STAGES * 19 * (size_t)nx * sizeof(typename S::T) + 2 * RP_STAGES * sizeof(uint64_t);
+  // the ring, full and empty barriers per stage, the abort flag (padded to 8 bytes)
+  const size_t b = (size_t)RP_STAGES * 19 * (size_t)nx * sizeof(typename S::T) + 2 * RP_STAGES * sizeof(uint64_t) + 8;
   return b <= 48 * 1024 ? b : 0;
 }
 
@@ -1413,12 +1434,13 @@ constexpr int LC_SMEM_A = 0;       // 2 tiles x 128 x 16 bf16
 constexpr int LC_SMEM_H = 8192;    // 2 tiles x 128 x 32 bf16
 constexpr int LC_SMEM_W1 = 24576;  // W1 image, 32 x 16 bf16 (followed by the W2 image: one 3 KB copy)
 constexpr int LC_SMEM_W2 = 25600;  // W2 image, 32 x 32 bf16
-constexpr int LC_SMEM_BAR = 27648; // mbarrier (8 B), then the tensor-memory address (4 B)
+constexpr int LC_SMEM_BAR = 27648; // mbarrier (8 B), the tensor-memory address (4 B), pad, drain barrier (8 B)
 // dynamic shared memory per block: more than 228 KB / 8, so at most 7 blocks share an SM and their
 // 7 x 64 tensor-memory columns fit in the SM's 512 (an allocation never has to wait)
 constexpr int LC_SMEM_BYTES = 29 * 1024;
 constexpr uint32_t LC_WAIT_LIMIT = 1u << 22;
-static_assert(LC_SMEM_BAR + 16 <= LC_SMEM_BYTES, "shared-memory layout");
+constexpr int LC_SMEM_DRAIN = LC_SMEM_BAR + 16;
+static_assert(LC_SMEM_DRAIN + 8 <= LC_SMEM_BYTES, "shared-memory layout");
 static_assert(offsetof(ClosureDev, w2img) == offsetof(ClosureDev, w1img) + 1024, "weight images are contiguous");
 
 // row r of a 128 x 16 A tile: the normalised, bf16-rounded features (10) and zero padding
@@ -1536,7 +1558,11 @@ __global__ void __launch_bounds__(LC_THREADS) k_closure_rows(const float* __rest
     uint4* dst = reinterpret_cast<uint4*>(lc_smem + LC_SMEM_W1);
     for (uint32_t k = tid; k < 192u; k += LC_THREADS) dst[k] = __ldg(src + k);
   }
-  if (tid == 0) umma::mbar_init(mbar, 1);
+  uint64_t* const dbar = reinterpret_cast<uint64_t*>(lc_smem + LC_SMEM_DRAIN);
+  if (tid == 0) {
+    umma::mbar_init(mbar, 1);
+    umma::mbar_init(dbar, 1);
+  }
   if (warp == 0) umma::tmem_alloc(tslot, LC_TMEM_COLS);
   const uint32_t r0 = blockIdx.x * (2u * LC_THREADS) + tid, r1 = r0 + LC_THREADS;
   float xa[CL_IN], xc[CL_IN];
@@ -1555,13 +1581,11 @@ __global__ void __launch_bounds__(LC_THREADS) k_closure_rows(const float* __rest
     if (r0 < rows) nub[r0] = nu.x;
     if (r1 < rows) nub[r1] = nu.y;
   }
-  umma::fence_before_sync();
+  // after a timed-out wait, the MMAs finish before their tensor memory is released
+  const bool drained = umma::drain_before_free(dbar, !ok, LC_WAIT_LIMIT);
   __syncthreads();
-  if (warp == 0) {
-    umma::fence_after_sync();
-    umma::tmem_free(tmem, LC_TMEM_COLS);
-  }
-  if (!ok) atomicOr(err, 4);
+  if (warp == 0) umma::tmem_free(tmem, LC_TMEM_COLS);
+  if (!ok || !drained) atomicOr(err, 4);
 }
 
 // Tiles of tpr cell pairs x 128 / tpr rows; block b takes tiles b, b + grid, ... (LC_TILES_PER_BLOCK
@@ -1595,12 +1619,16 @@ __global__ void __launch_bounds__(LC_THREADS, LC_BLOCKS_PER_SM) k_stream_collide
   const uint32_t sy = (uint32_t)NX, sz = (uint32_t)NX * (uint32_t)NY;
   uint64_t* const mbar = reinterpret_cast<uint64_t*>(lc_smem + LC_SMEM_BAR);
   uint32_t* const tslot = reinterpret_cast<uint32_t*>(lc_smem + LC_SMEM_BAR + 8);
+  uint64_t* const dbar = reinterpret_cast<uint64_t*>(lc_smem + LC_SMEM_DRAIN);
   {
     const uint4* src = reinterpret_cast<const uint4*>(cw->w1img);
     uint4* dst = reinterpret_cast<uint4*>(lc_smem + LC_SMEM_W1);
     for (uint32_t k = tid; k < 192u; k += LC_THREADS) dst[k] = __ldg(src + k);
   }
-  if (tid == 0) umma::mbar_init(mbar, 1);
+  if (tid == 0) {
+    umma::mbar_init(mbar, 1);
+    umma::mbar_init(dbar, 1);
+  }
   if (warp == 0) umma::tmem_alloc(tslot, LC_TMEM_COLS);
   umma::fence_before_sync();
   __syncthreads();
@@ -1691,14 +1719,12 @@ __global__ void __launch_bounds__(LC_THREADS, LC_BLOCKS_PER_SM) k_stream_collide
       break;
     }
   }
-  // release the tensor memory once every thread's reads have completed
-  umma::fence_before_sync();
+  // release the tensor memory once every thread's reads have completed and, after a timed-out
+  // wait, once the MMAs issued before it have completed
+  const bool drained = umma::drain_before_free(dbar, !ok, LC_WAIT_LIMIT);
   __syncthreads();
-  if (warp == 0) {
-    umma::fence_after_sync();
-    umma::tmem_free(tmem, LC_TMEM_COLS);
-  }
-  if (!ok) atomicOr(err, 4);
+  if (warp == 0) umma::tmem_free(tmem, LC_TMEM_COLS);
+  if (!ok || !drained) atomicOr(err, 4);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1953,6 +1979,9 @@ __global__ void __launch_bounds__(256) k_boundary_list(const __grid_constant__ w
 // macro pass: velocity field, EMA statistics, momentum-exchange force, partial reductions
 // ---------------------------------------------------------------------------------------------
 constexpr int MACRO_THREADS = 256;
+// per-block partial slots: the reference's 8 ([sum F (3), max |u|^2, sum rho on x = refX, n_ref,
+// nan count, solid count]) and the mass-conservation pair [sum rho over fluid cells (FP64), fluid count]
+static_assert(MACRO_SLOTS == 10, "partial slot layout");
 
 __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -1979,8 +2008,8 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
   const int NX = P.nx, NY = P.ny, NZ = P.nz;
   const size_t N = P.n;
   const float a = P.ema_alpha;
-  double accF[3] = {0, 0, 0}, accRho = 0;
-  uint32_t accNref = 0, accNan = 0, accSolid = 0;
+  double accF[3] = {0, 0, 0}, accRho = 0, accMass = 0;
+  uint32_t accNref = 0, accNan = 0, accSolid = 0, accFluid = 0;
   float accMax = 0.0f;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < N; idx += (size_t)gridDim.x * blockDim.x) {
     const uint32_t c32 = (uint32_t)idx;  // n < 2^32
@@ -2088,6 +2117,9 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
         accNref++;
       }
       accNan += bad ? 1u : 0u;
+      // global mass-conservation check: FP64 sum of the fluid cells' densities
+      accMass += (double)rho;
+      accFluid++;
       const bool finite = isfinite(out[0]) && isfinite(out[1]) && isfinite(out[2]) && isfinite(out[3]) &&
                           isfinite((float)uu);
       if (a != 0.0f || !finite) {
@@ -2139,7 +2171,7 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
   }
   // block reduction. Counts by warp votes / integer reductions; the FP64 sums are shuffled only in
   // warps that hold a non-zero value (most warps have no wall link and no reference-plane cell).
-  __shared__ double sh[MACRO_THREADS / 32][8];
+  __shared__ double sh[MACRO_THREADS / 32][MACRO_SLOTS];
   const unsigned full = 0xffffffffu;
   if (__any_sync(full, accF[0] != 0.0 || accF[1] != 0.0 || accF[2] != 0.0)) {
     accF[0] = warp_sum(accF[0]);
@@ -2147,10 +2179,12 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
     accF[2] = warp_sum(accF[2]);
   }
   if (__any_sync(full, accNref != 0u)) accRho = warp_sum(accRho);
+  accMass = warp_sum(accMass);
   const float mx = warp_max(accMax);
   const uint32_t nref = __reduce_add_sync(full, accNref);
   const uint32_t nnan = __reduce_add_sync(full, accNan);
   const uint32_t nsolid = __reduce_add_sync(full, accSolid);
+  const uint32_t nfluid = __reduce_add_sync(full, accFluid);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (lane == 0) {
     sh[wid][0] = accF[0];
@@ -2161,12 +2195,14 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
     sh[wid][5] = (double)nref;
     sh[wid][6] = (double)nnan;
     sh[wid][7] = (double)nsolid;
+    sh[wid][8] = accMass;
+    sh[wid][9] = (double)nfluid;
   }
   __syncthreads();
   if (wid == 0) {
     constexpr int NW = MACRO_THREADS / 32;
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
+    for (int k = 0; k < MACRO_SLOTS; k++) {
       double x = lane < NW ? sh[lane][k] : 0.0;
       if (k == 3) {
         float m = warp_max((float)x);
@@ -2174,7 +2210,7 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
       } else {
         x = warp_sum(x);
       }
-      if (lane == 0) partials[(size_t)blockIdx.x * 8 + k] = x;
+      if (lane == 0) partials[(size_t)blockIdx.x * MACRO_SLOTS + k] = x;
     }
   }
 }
@@ -2184,13 +2220,14 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
 constexpr int REDUCE_THREADS = 1024;
 
 __global__ void __launch_bounds__(REDUCE_THREADS) k_reduce_partials(const double* __restrict__ partials,
-                                                                   int nblocks, double* __restrict__ result) {
-  __shared__ double sh[REDUCE_THREADS / 32][8];
-  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                                                                   int nblocks, double* __restrict__ result,
+                                                                   int nres) {
+  __shared__ double sh[REDUCE_THREADS / 32][MACRO_SLOTS];
+  double v[MACRO_SLOTS] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll 4
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
-    const double2* p2 = reinterpret_cast<const double2*>(partials + (size_t)b * 8);
-    const double2 a0 = p2[0], a1 = p2[1], a2 = p2[2], a3 = p2[3];
+    const double2* p2 = reinterpret_cast<const double2*>(partials + (size_t)b * MACRO_SLOTS);
+    const double2 a0 = p2[0], a1 = p2[1], a2 = p2[2], a3 = p2[3], a4 = p2[4];
     v[0] += a0.x;
     v[1] += a0.y;
     v[2] += a1.x;
@@ -2199,17 +2236,19 @@ __global__ void __launch_bounds__(REDUCE_THREADS) k_reduce_partials(const double
     v[5] += a2.y;
     v[6] += a3.x;
     v[7] += a3.y;
+    v[8] += a4.x;
+    v[9] += a4.y;
   }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
+  for (int k = 0; k < MACRO_SLOTS; k++) {
     if (k == 3) v[k] = (double)warp_max((float)v[k]);
     else v[k] = warp_sum(v[k]);
   }
   if (lane == 0)
-    for (int k = 0; k < 8; k++) sh[wid][k] = v[k];
+    for (int k = 0; k < MACRO_SLOTS; k++) sh[wid][k] = v[k];
   __syncthreads();
-  if (threadIdx.x < 8) {
+  if (threadIdx.x < nres && threadIdx.x < MACRO_SLOTS) {
     const int k = threadIdx.x;
     double x = 0;
     for (int w = 0; w < (int)(blockDim.x >> 5); w++) x = k == 3 ? fmax(x, sh[w][k]) : x + sh[w][k];
@@ -2604,7 +2643,8 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
           const uint32_t rows = s->sc_by > 0 ? (uint32_t)s->sc_by : 4u;
           auto kern = s->kp.collision == 1u ? k_stream_collide_rows<S, true> : k_stream_collide_rows<S, false>;
           kern<<<(nrows + rows - 1) / rows, RP_THREADS, rp_smem, s->stream>>>(
-              s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, nrows, rows, s->err_dev);
+              s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, nrows, rows, s->rp_wait_limit,
+              s->err_dev);
           s->launches++;
           if ((e = cudaGetLastError()) != cudaSuccess) return e;
           if (s->aux) {
@@ -2650,7 +2690,7 @@ static cudaError_t macro_t(wt_solver* s) {
   s->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_reduce_partials<<<1, REDUCE_THREADS, 0, s->stream>>>(s->partials, s->partial_blocks, s->result_dev);
+  k_reduce_partials<<<1, REDUCE_THREADS, 0, s->stream>>>(s->partials, s->partial_blocks, s->result_dev, MACRO_SLOTS);
   s->launches++;
   return cudaGetLastError();
 }
@@ -2732,13 +2772,13 @@ cudaError_t launch_closure_filter(wt_solver* fine, int cnx, int cny, int cnz, fl
 // Some hosts may not allocate device memory at all (their memory belongs to another allocator,
 // and cudaMalloc / cudaFree would synchronise the device behind its back). For them the macro
 // pass's per-block partial sums live in this file-scope array instead of a handle's buffer: one
-// 8-double slot per block of MACRO_THREADS cells, enough for WT_SAMPLE_NOALLOC_MAX_CELLS cells.
-// k_macro writes all 8 slots of every block it runs before k_reduce_partials reads them, so what
+// MACRO_SLOTS-double record per block of MACRO_THREADS cells, enough for WT_SAMPLE_NOALLOC_MAX_CELLS
+// cells (1.25 MiB). k_macro writes all slots of every block it runs before k_reduce_partials reads them, so what
 // an earlier call left in the array is never read and nothing is cleared. The array is shared by
 // every call on a device: calls that overlap on the GPU race on it.
 constexpr int NOALLOC_MAX_BLOCKS = WT_SAMPLE_NOALLOC_MAX_CELLS / MACRO_THREADS;
 static_assert(NOALLOC_MAX_BLOCKS * MACRO_THREADS == WT_SAMPLE_NOALLOC_MAX_CELLS, "whole blocks");
-static __device__ __align__(256) double g_sample_scratch[NOALLOC_MAX_BLOCKS * 8];
+static __device__ __align__(256) double g_sample_scratch[NOALLOC_MAX_BLOCKS * MACRO_SLOTS];
 
 namespace {
 
@@ -2768,7 +2808,7 @@ cudaError_t sample_noalloc_t(const wt_kparams& kp, const void* fin, const uint32
                                                     meanB, scratch);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_reduce_partials<<<1, REDUCE_THREADS, 0, st>>>(scratch, nblocks, result);
+  k_reduce_partials<<<1, REDUCE_THREADS, 0, st>>>(scratch, nblocks, result, 8);
   return cudaGetLastError();
 }
 
@@ -2799,7 +2839,7 @@ extern "C" int wt_sample_noalloc(const wt_dims* dims, const wt_params* p, const 
   const uint64_t n = (uint64_t)dims->nx * (uint64_t)dims->ny * (uint64_t)dims->nz;
   if (n > (uint64_t)WT_SAMPLE_NOALLOC_MAX_CELLS)
     return invalid(std::to_string(n) + " cells exceed the limit of " + std::to_string(WT_SAMPLE_NOALLOC_MAX_CELLS) +
-                   " cells set by the fixed reduction scratch (1 MiB); use a handle (wt_create) for larger grids");
+                   " cells set by the fixed reduction scratch (1.25 MiB); use a handle (wt_create) for larger grids");
   if (p->precision < WT_PREC_F32 || p->precision > WT_PREC_F64) return invalid("bad precision");
   if (nwheels < 0 || nwheels > 16 || (nwheels > 0 && !wheels)) return invalid("need 0..16 wheels and a wheel array");
   int dev = -1;

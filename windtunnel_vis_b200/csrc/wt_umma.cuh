@@ -109,6 +109,27 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// Called by every thread of the block, with `dbar` initialised (count 1) at the start of the kernel
+// and otherwise unused. Where `pending` is set for some thread (a wait on an MMA's commit timed
+// out, so MMAs may still be writing tensor memory), thread 0 (the only thread that issues MMAs)
+// commits once more, to `dbar`: its phase 0 completes once every tcgen05 operation thread 0 issued
+// has completed. The block waits for that phase (bounded by `limit` polls) so that the tensor
+// memory is released only after the MMAs are done with it. Returns false if that wait gave up too.
+__device__ __forceinline__ bool drain_before_free(uint64_t* dbar, bool pending, uint32_t limit) {
+  fence_before_sync();
+  if (!__syncthreads_or(pending)) {
+    fence_after_sync();
+    return true;
+  }
+  if (threadIdx.x == 0) {
+    fence_after_sync();
+    commit(dbar);
+  }
+  const bool done = mbar_wait(dbar, 0, limit);
+  fence_after_sync();
+  return done;
+}
+
 // tensor-memory address of (lane base of this warp, column)
 __device__ __forceinline__ uint32_t tmem_lane_addr(uint32_t base, uint32_t warp, uint32_t col) {
   return base + (((warp & 3u) * 32u) << 16) + col;

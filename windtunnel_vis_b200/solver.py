@@ -35,6 +35,7 @@ def _stats_dict(st: abi.Stats):
     return {
         "fx": st.fx, "fy": st.fy, "fz": st.fz, "maxU": st.max_u, "rhoRef": st.rho_ref,
         "unstable": bool(st.unstable), "step": int(st.step), "raw": np.array(st.raw[:], np.float64),
+        "mass": float(st.mass), "fluidCells": int(st.fluid_cells),
     }
 
 
@@ -269,6 +270,11 @@ class Solver:
         out = (C.c_int32 * 4)()
         self._check(self._lib.wt_get_launch(self._h, out))
         return tuple(out)
+
+    def set_wait_limit(self, polls):
+        """Test hook: polls of each row-pipeline consumer wait before it gives up (negative: the
+        default)."""
+        self._check(self._lib.wt_set_wait_limit(self._h, int(polls)))
 
     def autotune(self, iters=20):
         """The launch tuner: returns the chosen (kernel, param, bx, by)."""

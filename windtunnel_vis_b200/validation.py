@@ -4,6 +4,8 @@ round_flags .... src/analysis/validation.ts:35-53 (analytic circle / sphere flag
 freestream ..... src/analysis/validation.ts:61-88
 cylinder ....... src/analysis/validation.ts:89-136
 sphere ......... src/analysis/validation.ts:137-184
+cylinder_channel the D2Q9 cylinder in a 512 x 128 channel of the benchmark (FP32 against FP64
+                 populations)
 sphere_les ..... the D3Q19 LES sphere tunnel of the benchmark (FP16 storage against FP64 populations)
 vehicle ........ the D3Q19 vehicle tunnel of the benchmark (GPU voxelizer, moving belt, wheels)
 batch_sweep .... 32 vehicle tunnels of uneven sizes (yaw x speed sweep) stepped as one batch
@@ -63,7 +65,8 @@ def freestream(make, valscale=1.0):
             "metrics": {"maxU_over_U": st["maxU"] / U, "rhoRef": st["rhoRef"]}}
 
 
-def cylinder(make, valscale=1.0):
+def cylinder(make, valscale=1.0, interp=True):
+    """interp=False: plain halfway bounce-back instead of Bouzidi walls (SolverParams.interp)."""
     t0 = time.perf_counter()
     D = js_round(24 * valscale)
     d = (js_round(25 * D), 10 * D, 1)
@@ -71,7 +74,7 @@ def cylinder(make, valscale=1.0):
     Re = 100
     nu = U * D / Re
     s = make(d, dict(u=U, nu=nu, cs=0, ground="freeslip", sides="freeslip", spongeNu=0.03, spongeStart=0.85,
-                     emaAlpha=0.0))
+                     emaAlpha=0.0, interp=interp))
     flags, _, sdf = round_flags(d, (6 * D, d[1] / 2 + 0.37, 0), D / 2, True)
     s.upload_flags(flags)
     s.upload_sdf(sdf)
@@ -102,7 +105,8 @@ def cylinder(make, valscale=1.0):
                         "cycles": fr["cycles"], "grid": d, "tau": 3 * nu + 0.5}}
 
 
-def sphere(make, valscale=1.0):
+def sphere(make, valscale=1.0, interp=True):
+    """interp=False: plain halfway bounce-back instead of Bouzidi walls (SolverParams.interp)."""
     t0 = time.perf_counter()
     D = js_round(20 * valscale)
     d = (js_round(9.6 * D), js_round(4.8 * D), js_round(4.8 * D))
@@ -110,7 +114,7 @@ def sphere(make, valscale=1.0):
     Re = 100
     nu = U * D / Re
     s = make(d, dict(u=U, nu=nu, cs=0, ground="freeslip", sides="freeslip", spongeNu=0.03, spongeStart=0.85,
-                     emaAlpha=0))
+                     emaAlpha=0, interp=interp))
     flags, frontal, sdf = round_flags(d, (2.8 * D, d[1] / 2 + 0.37, d[2] / 2 + 0.21), D / 2, False)
     s.upload_flags(flags)
     s.upload_sdf(sdf)
@@ -137,6 +141,77 @@ def sphere(make, valscale=1.0):
             "series": {"t": tt, "v": cds},
             "metrics": {"cd": cd, "cd_ref": ref, "deviation": err, "grid": d, "frontal": frontal,
                         "blockage": frontal / (d[1] * d[2])}}
+
+
+CHANNEL_DIMS = (512, 128, 1)
+
+
+def channel_params(precision="f32", u=0.05, re=100.0, diameter=20, sponge_nu=0.0, seed=1):
+    """The D2Q9 cylinder-in-a-channel parameters: plain BGK (cs = 0), nu = u D / Re (0.01 at the
+    defaults, tau = 0.53), free-slip floor and roof, zero-gradient outlet (with an outlet sponge
+    only when sponge_nu > 0; the reference's own cylinder case uses 0.03 from 0.85 nx), rest state
+    with seeded uniform +-1e-4 velocity noise."""
+    return dict(u=u, nu=u * diameter / re, cs=0.0, ground="freeslip", sides="freeslip", spongeNu=sponge_nu,
+                spongeStart=0.85, collision="bgk", emaAlpha=0.0, precision=precision, init="rest_noise",
+                initNoise=1e-4, initSeed=seed)
+
+
+def channel_geometry(dims=CHANNEL_DIMS, center=(96.0, 65.0), diameter=20):
+    """Circle of diameter D centred at `center` in cell-centre coordinates (cell k spans [k, k+1],
+    its centre at k + 1/2, as the reference's roundFlags), one cell above the channel axis; wall
+    distances from the exact circle."""
+    return round_flags(dims, (center[0], center[1], 0.0), diameter / 2, True)
+
+
+def cylinder_channel(make, precision="f32", steps=40000, dims=CHANNEL_DIMS, center=(96.0, 65.0), diameter=20,
+                     u=0.05, re=100.0, chunk=50, sponge_nu=0.0, seed=1, measure_from=None, init="rest_noise"):
+    """The D2Q9 cylinder in a channel: 512 x 128, D = 20 at (96, 65) (one cell off the axis, which
+    triggers shedding), uniform inlet u = 0.05, Re = 100, channel_params, 40,000 steps sampled every
+    50. Reports the Strouhal number from upward mean crossings of C_L (the reference's estimator,
+    src/analysis/strouhal.ts:5-30), mean C_D and the C_L amplitude over the steps from
+    `measure_from` (default: the second half), with C = F / (1/2 rho U^2 D) as the reference's 2-D
+    coefficients (src/analysis/aero.ts:4-7)."""
+    t0 = time.perf_counter()
+    flags, _, sdf = channel_geometry(dims, center, diameter)
+    s = make(dims, dict(channel_params(precision, u, re, diameter, sponge_nu, seed), init=init))
+    s.upload_flags(flags)
+    s.upload_sdf(sdf)
+    tt, cl, cd, mass, rho_ref = [], [], [], [], []
+    step = 0
+    unstable = False
+    while step < steps:
+        st = s.step_and_sample(chunk)
+        step += chunk
+        if st["unstable"]:
+            unstable = True
+            break
+        c = coefficients(st["fx"], st["fy"], 0, u, diameter)
+        tt.append(st["step"])
+        cl.append(c["cl"])
+        cd.append(c["cd"])
+        mass.append(st.get("mass", math.nan))
+        rho_ref.append(st["rhoRef"])
+    # the inflow the body actually sees: mean x velocity over the reference plane x = refX (4)
+    u_in = math.nan
+    if hasattr(s, "read_velocity"):
+        v = np.asarray(s.read_velocity(), np.float64).reshape(dims[1], dims[0], 4)
+        u_in = float(v[:, min(4, dims[0] - 1), 0].mean())
+    s.destroy()
+    start = steps // 2 if measure_from is None else measure_from
+    sel = [k for k, t in enumerate(tt) if t >= start]
+    fr = crossing_frequency([tt[k] for k in sel], [cl[k] for k in sel])
+    St = fr["f"] * diameter / u
+    cd_mean = sum(cd[k] for k in sel) / max(len(sel), 1)
+    return {"id": "cylinder_channel", "precision": precision,
+            "passed": bool(not unstable and fr["cycles"] >= 4),
+            "seconds": time.perf_counter() - t0,
+            "series": {"t": tt, "cl": cl, "cd": cd, "mass": mass, "rhoRef": rho_ref},
+            "metrics": {"St": St, "St_ref": cylinder_st_ref(re), "cd_mean": cd_mean, "cl_amplitude": fr["amplitude"],
+                        "cycles": fr["cycles"], "steps": step, "measured_from": start, "grid": list(dims),
+                        "tau": 3 * u * diameter / re + 0.5, "sponge_nu": sponge_nu, "unstable": unstable,
+                        "rho_ref_end": rho_ref[-1] if rho_ref else math.nan, "u_inflow_end": u_in,
+                        "St_inflow": fr["f"] * diameter / u_in if u_in == u_in and u_in > 0 else math.nan,
+                        "mass_end": mass[-1] if mass else math.nan}}
 
 
 def sphere_les(make, precision="f16", steps=20000, dims=(256, 128, 128), diameter=24, u=0.05, re=300.0, cs=0.1,
@@ -357,6 +432,7 @@ CASES = {"freestream": freestream, "cylinder": cylinder, "sphere": sphere}
 
 def main(argv=None):
     """python -m windtunnel_vis_b200.validation sphere_les --precision f16 --steps 20000
+    python -m windtunnel_vis_b200.validation cylinder_channel --precision f32 --steps 40000
     python -m windtunnel_vis_b200.validation vehicle --precision f16 --steps 30000
     python -m windtunnel_vis_b200.validation cylinder|sphere|freestream [--valscale 0.5]
     Prints one JSON line (metrics, series omitted) per case on the CUDA path."""
@@ -366,9 +442,11 @@ def main(argv=None):
     from .solver import solver_factory
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["sphere_les", "vehicle", "batch_sweep", "learned_closure", *CASES])
+    ap.add_argument("case", choices=["sphere_les", "vehicle", "batch_sweep", "learned_closure", "cylinder_channel",
+                                     *CASES])
     ap.add_argument("--precision", default="f16")
     ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--sponge", type=float, default=0.0, help="cylinder_channel: outlet sponge viscosity")
     ap.add_argument("--valscale", type=float, default=1.0)
     ap.add_argument("--fine", default="512,256,256", help="learned_closure: fine grid nx,ny,nz")
     ap.add_argument("--train-bodies", type=int, default=8)
@@ -397,6 +475,8 @@ def main(argv=None):
         return
     if a.case == "sphere_les":
         r = sphere_les(solver_factory, a.precision, a.steps)
+    elif a.case == "cylinder_channel":
+        r = cylinder_channel(solver_factory, a.precision, a.steps, sponge_nu=a.sponge)
     elif a.case == "vehicle":
         r = vehicle(solver_factory, a.precision, a.steps)
     elif a.case == "batch_sweep":
