@@ -408,6 +408,14 @@ void* wt_stream(const wt_solver* s);
 int32_t wt_device(const wt_solver* s);
 /* Number of kernel launches this handle has issued since creation. */
 int64_t wt_launch_count(const wt_solver* s);
+/* Number of wt_step_and_sample calls whose last step ran the sampling pass fused (extension). With
+ * f16 / f32 storage, the vectorised kernels and the reference's closure, the last step of a
+ * stepAndSample chunk writes the velocity texels, the EMA statistics and the sums of the sampling
+ * pass from the values it stores, and a short pass over the wall-adjacent and solid cells adds the
+ * momentum-exchange force: the populations are not read a second time. The statistics, the
+ * velocity field and the means are bit-identical to wt_step followed by wt_sample (the force sums
+ * to FP64 rounding, summed in another order). Other configurations run the separate pass. */
+int64_t wt_fused_sample_count(const wt_solver* s);
 
 /* ---- sampling pass on caller-owned buffers, without allocating ------------------------------
  * No counterpart in the reference: the reference's solver always owns its buffers.

@@ -81,7 +81,10 @@ def test_channel_cylinder_matches_oracle_full_size(gpu, oracle):
     sg, so = g.sample(), o.sample()
     assert np.abs(sg["raw"][:3] - so["raw"][:3]).max() <= 1e-4 * max(np.abs(so["raw"][:3]).max(), 1e-3)
     assert sg["raw"][5:].tolist() == so["raw"][5:].tolist()
-    assert sg["fluidCells"] == so["fluidCells"] and abs(sg["mass"] / so["mass"] - 1) <= 1e-6
+    # the two runs' f32 roundings differ (FMA contraction on the GPU, none in the oracle) and the
+    # collision's rounding moves mass a little every step: the mass sums agree to the drift of
+    # 300 rounded steps (the sum itself is checked on identical populations in test_gpu_mass)
+    assert sg["fluidCells"] == so["fluidCells"] and abs(sg["mass"] / so["mass"] - 1) <= 2e-5
     g.destroy()
 
 

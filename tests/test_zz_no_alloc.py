@@ -82,6 +82,44 @@ def test_sample_noalloc_matches_sample_twice(gpu):
     _check_one(torch, lib, (48, 16, 1), dict(PARAM_SETS["freeslip_reg"], precision="f32"), 15)
 
 
+def test_sample_noalloc_allocates_no_device_memory(gpu):
+    # after a first call (which may load the library's device code), further calls leave the
+    # device's free memory unchanged
+    import torch
+
+    lib = gpu
+    dims = (32, 14, 12)
+    params = dict(PARAM_SETS["freeslip_reg"], precision="f16")
+    flags, sdf, wheels = scene(dims)
+    n = dims[0] * dims[1] * dims[2]
+    s = Solver(dims, params)
+    s.upload_flags(flags)
+    s.upload_sdf(sdf)
+    s.step(5)
+    pops = _device_copy(torch, s.read_populations())
+    dflags = _device_copy(torch, s.read_flags().view(np.int32))
+    dsdf = _device_copy(torch, s.read_sdf_encoded().view(np.int32))
+    m4, mb = s.read_means()
+    dm4, dmb = _device_copy(torch, m4), _device_copy(torch, mb)
+    vel = torch.zeros((n, 4), dtype=torch.float16, device="cuda")
+    result = torch.zeros((8,), dtype=torch.float64, device="cuda")
+    s.destroy()
+    w, nw = abi.make_wheels(wheels)
+
+    def call():
+        rc = lib.wt_sample_noalloc(C.byref(abi.Dims(*dims)), C.byref(abi.make_params(params)), w, nw,
+                                   pops.data_ptr(), dflags.data_ptr(), dsdf.data_ptr(), vel.data_ptr(),
+                                   dm4.data_ptr(), dmb.data_ptr(), result.data_ptr(), None)
+        assert rc == 0, lib.wt_last_error(None).decode()
+        torch.cuda.synchronize()
+
+    call()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        call()
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_sample_noalloc_rejects_grids_above_the_limit(gpu):
     import torch
 

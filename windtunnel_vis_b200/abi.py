@@ -203,6 +203,7 @@ def _sig(lib):
         "wt_stream": ([S], v),
         "wt_device": ([S], i32),
         "wt_launch_count": ([S], i64),
+        "wt_fused_sample_count": ([S], i64),
         "wt_sample_noalloc": ([P(Dims), P(Params), P(Wheel), i32, v, v, v, v, v, v, v, v], C.c_int),
         "wt_set_closure": ([S, P(Closure)], C.c_int),
         "wt_get_closure": ([S, P(Closure), P(i32)], C.c_int),

@@ -73,7 +73,7 @@ void free_all(wt_solver* s) {
                   s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count,
                   s->bcell, s->brec, s->bgam, s->vox_pos, s->vox_idx, s->vox_info,
                   s->dvort, s->dstat, s->dmean, s->exp_buf, s->probe_buf, s->closure_dev, s->stage,
-                  s->diff_dev, s->lc_rows};
+                  s->diff_dev, s->lc_rows, s->solids, s->smp_sets};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->result_host) cudaFreeHost(s->result_host);
@@ -83,6 +83,8 @@ void free_all(wt_solver* s) {
   for (auto& g : s->step_graph)
     if (g) cudaGraphExecDestroy(g);
   for (auto& g : s->long_graph)
+    if (g) cudaGraphExecDestroy(g);
+  for (auto& g : s->sample_graph)
     if (g) cudaGraphExecDestroy(g);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
@@ -107,6 +109,10 @@ void invalidate_graphs(wt_solver* s) {
     g = nullptr;
   }
   for (auto& g : s->long_graph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+  for (auto& g : s->sample_graph) {
     if (g) cudaGraphExecDestroy(g);
     g = nullptr;
   }
@@ -198,6 +204,30 @@ int capture_steps(wt_solver* s, int p, int pairs, cudaGraphExec_t* out, int64_t*
 
 // the two-step graph for starting parity p: step f[p] -> f[p^1], then f[p^1] -> f[p]
 int capture_step_graph(wt_solver* s, int p) { return capture_steps(s, p, 1, &s->step_graph[p], &s->graph_launches); }
+
+// the tail of a stepAndSample chunk for starting parity p: WT_SAMPLE_TAIL - 1 steps, then the fused
+// sampling step (ending on f[p]: the tail has an even number of steps)
+int capture_sample_graph(wt_solver* s, int p) {
+  const int64_t l0 = s->launches;
+  cudaGraph_t graph = nullptr;
+  WT_CUDA(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+  cudaError_t e = cudaSuccess;
+  int q = p;
+  for (int k = 0; k < WT_SAMPLE_TAIL - 1 && e == cudaSuccess; k++, q ^= 1)
+    e = wt::launch_stream_collide(s, s->f[q], s->f[q ^ 1]);
+  if (e == cudaSuccess) e = wt::launch_sample_step(s, s->f[q], s->f[q ^ 1]);
+  cudaError_t e2 = cudaStreamEndCapture(s->stream, &graph);
+  s->sample_graph_launches = s->launches - l0;
+  s->launches = l0;
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&s->sample_graph[p], graph, cudaGraphInstantiateFlagUseNodePriority);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    s->sample_graph[p] = nullptr;
+    return cuda_fail(s, e, "graph capture");
+  }
+  return WT_OK;
+}
 
 int ensure_init(wt_solver* s) {
   if (!s->pending_init) return WT_OK;
@@ -349,7 +379,8 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
             alloc((void**)&s->meanA, s->n * 16, "meanA") && alloc((void**)&s->meanB, s->n * 4, "meanB") &&
             alloc((void**)&s->partials, (size_t)s->partial_blocks * RESULT_BYTES, "partials") &&
             alloc((void**)&s->result_dev, RESULT_BYTES, "result") && alloc((void**)&s->err_dev, 4, "error word") &&
-            alloc((void**)&s->bnd_count, 4, "boundary counter");
+            alloc((void**)&s->bnd_count, 4, "boundary counter") &&
+            alloc((void**)&s->smp_sets, wt::SMP_SETS_BYTES, "sampling accumulators");
   if (ok && (cudaMallocHost((void**)&s->result_host, RESULT_BYTES) != cudaSuccess ||
              cudaMallocHost((void**)&s->err_host, 4) != cudaSuccess ||
              cudaMallocHost((void**)&s->bnd_count_host, 4) != cudaSuccess)) {
@@ -682,9 +713,46 @@ int wt_sample(wt_solver* s, wt_stats* out) {
 }
 
 int wt_step_and_sample(wt_solver* s, int32_t steps, wt_stats* out) {
-  int rc = wt_step(s, steps);
+  if (!s || !out || steps < 0) return WT_E_INVALID;
+  if (steps == 0) return wt_sample(s, out);
+  DeviceGuard g(s->device);
+  int rc = wt_step(s, 0);  // classification and initialisation
   if (rc) return rc;
-  return wt_sample(s, out);
+  if (!wt::sample_step_ok(s)) {
+    rc = wt_step(s, steps);
+    return rc ? rc : wt_sample(s, out);
+  }
+  // The last step runs the sampling pass's per-cell work on what it stores (no second read of the
+  // populations), then the wall force and the solid cells, then the final reduction. With solid
+  // cells in place in both buffers, the chunk's last WT_SAMPLE_TAIL steps replay one graph.
+  const bool tail = steps >= WT_SAMPLE_TAIL;
+  rc = wt_step(s, steps - (tail ? WT_SAMPLE_TAIL : 1));
+  if (rc) return rc;
+  if (tail && s->solid_ok[0] && s->solid_ok[1]) {
+    if (!s->sample_graph[s->parity]) {
+      rc = capture_sample_graph(s, s->parity);
+      if (rc) return rc;
+    }
+    WT_CUDA(s, cudaGraphLaunch(s->sample_graph[s->parity], s->stream), "sample graph");
+    s->launches += s->sample_graph_launches;
+    s->step_count += WT_SAMPLE_TAIL;
+  } else {
+    if (tail) {
+      rc = wt_step(s, WT_SAMPLE_TAIL - 1);
+      if (rc) return rc;
+    }
+    WT_CUDA(s, wt::launch_sample_step(s, s->f[s->parity], s->f[s->parity ^ 1]), "sampling step");
+    s->parity ^= 1;
+    s->step_count += 1;
+  }
+  s->fused_samples++;
+  WT_CUDA(s, cudaMemcpyAsync(s->result_host, s->result_dev, RESULT_BYTES, cudaMemcpyDeviceToHost, s->stream),
+          "read result");
+  WT_CUDA(s, cudaMemcpyAsync(s->err_host, s->err_dev, 4, cudaMemcpyDeviceToHost, s->stream), "read error word");
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "sample");
+  if (*s->err_host != 0) return check_err_flag(s);
+  decode(s, s->result_host, out);
+  return WT_OK;
 }
 
 int wt_read_flags(wt_solver* s, uint32_t* out, int64_t n) {
@@ -1026,6 +1094,7 @@ int wt_get_launch(const wt_solver* s, int32_t* out4) {
 void* wt_stream(const wt_solver* s) { return s ? (void*)s->stream : nullptr; }
 int32_t wt_device(const wt_solver* s) { return s ? s->device : -1; }
 int64_t wt_launch_count(const wt_solver* s) { return s ? s->launches : -1; }
+int64_t wt_fused_sample_count(const wt_solver* s) { return s ? s->fused_samples : -1; }
 
 }  // extern "C"
 

@@ -77,16 +77,21 @@ struct StF32 {
   __device__ __forceinline__ static T solid(R w) { return w; }
   __device__ __forceinline__ static R cvt(T v, R /*w*/) { return v; }
 };
+// float(h) + w with one rounding (the widening is exact), in one mixed-precision add of sm_100
+__device__ __forceinline__ float h2f_add(__half h, float w) {
+  float r;
+  asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(r) : "h"(__half_as_ushort(h)), "f"(w));
+  return r;
+}
+
 struct StF16 {
   typedef __half T;
   typedef float R;
   static constexpr int PREC = WT_PREC_F16;
-  __device__ __forceinline__ static R ld(const T* __restrict__ p, size_t o, R w) {
-    return __half2float(__ldg(p + o)) + w;
-  }
-  __device__ __forceinline__ static void st(T* __restrict__ p, size_t o, R v, R w) { p[o] = __float2half_rn(v - w); }
+  __device__ __forceinline__ static R ld(const T* __restrict__ p, size_t o, R w) { return h2f_add(__ldg(p + o), w); }
+  __device__ __forceinline__ static void st(T* __restrict__ p, size_t o, R v, R w) { p[o] = __float2half_rn(__fsub_rn(v, w)); }
   __device__ __forceinline__ static T solid(R /*w*/) { return __float2half_rn(0.0f); }
-  __device__ __forceinline__ static R cvt(T v, R w) { return __half2float(v) + w; }
+  __device__ __forceinline__ static R cvt(T v, R w) { return h2f_add(v, w); }
 };
 struct StF64 {
   typedef double T;

@@ -12,6 +12,8 @@
 
 // step pairs captured in one long step graph
 constexpr int WT_LONG_PAIRS = 5;
+// steps in the captured tail of a stepAndSample chunk (even: the graph keeps the parity)
+constexpr int WT_SAMPLE_TAIL = 10;
 // doubles per block in the macro pass's partial reductions, and in its result: the reference's
 // 8-slot result followed by the FP64 fluid mass and the fluid cell count
 constexpr int MACRO_SLOTS = 10;
@@ -32,6 +34,10 @@ struct wt_solver {
   // the same for 2 x WT_LONG_PAIRS steps: fewer graph launches per reference sample chunk
   cudaGraphExec_t long_graph[2] = {nullptr, nullptr};
   int64_t long_graph_launches = 0;
+  // the tail of a stepAndSample chunk: WT_SAMPLE_TAIL - 1 steps, then the fused sampling step (with
+  // its wall-force pass and final reduction), per starting parity
+  cudaGraphExec_t sample_graph[2] = {nullptr, nullptr};
+  int64_t sample_graph_launches = 0;
   uint64_t graph_gen = 0;      // bumped whenever the captured graphs are dropped (batches recapture)
   wt_dims dims{};
   wt_params params{};
@@ -62,6 +68,14 @@ struct wt_solver {
   uint32_t nbnd = 0;
   size_t bnd_cap = 0;
   int gs = 1;
+  // every solid cell (built with the boundary list): the fused sampling pass visits them after the
+  // sampling step (density extrapolation, velocity texel, EMA statistics)
+  uint32_t* solids = nullptr;
+  uint32_t nsolid = 0;
+  size_t solid_cap = 0;
+  // accumulator sets of the fused sampling pass (zeroed before each sampling step)
+  unsigned long long* smp_sets = nullptr;
+  int64_t fused_samples = 0;  // stepAndSample calls that ran the fused sampling step
   uint32_t* bnd_count = nullptr;  // device counter used while building the list
   uint32_t* bnd_count_host = nullptr;  // pinned
   // link records of the listed cells (k_boundary_build), applied every step by k_boundary_tab
@@ -134,6 +148,13 @@ cudaError_t launch_boundary_table(wt_solver* s);
 cudaError_t launch_init(wt_solver* s);
 cudaError_t launch_stream_collide(wt_solver* s, const void* fin, void* fout);
 cudaError_t launch_macro(wt_solver* s);
+// The fused sampling step (the last step of a stepAndSample chunk runs the sampling pass's per-cell
+// work on what it stores, then the wall-force / solid-cell pass and the final reduction into
+// result_dev). sample_step_ok: whether the handle's step takes that form (vectorised kernels, f16 /
+// f32 storage, the reference's closure, not the row pipeline); needs a classified handle.
+bool sample_step_ok(const wt_solver* s);
+cudaError_t launch_sample_step(wt_solver* s, const void* fin, void* fout);
+constexpr size_t SMP_SETS_BYTES = 64 * 16 * sizeof(unsigned long long);
 
 // voxelizer (wt_voxel.cu). Scratch buffers hits (3n i32), vote (n u32), info (8 u32) are
 // allocated by the caller.

@@ -884,6 +884,206 @@ __device__ __forceinline__ void features2(const wt_kparams& P, const float2 (&h)
 // two-cell loads / stores of shifted populations: elements (o, o + 1), o even. Loads are split
 // into a raw fetch and a later conversion so that a thread can put all of its loads in flight
 // before it converts any of them.
+// ---- per-cell arithmetic of the sampling pass, shared by k_macro and the fused sampling step ----
+// The sampling pass (wgslLbm.ts:347-489) can run on its own (k_macro, re-reading every stored
+// population) or inside the last step of a stepAndSample chunk, on the values that step stores.
+// Both give the same bits: a cell's density and momentum are summed from its populations exactly
+// as stored, in the order the step kernels emit them (direction 0, then each direction followed by
+// its opposite), and the rest uses correctly rounded operations only.
+template <class L> struct EmitOrder {
+  int d[L::Q];
+  constexpr EmitOrder() : d() {
+    int k = 0;
+    for (int i = 0; i < L::Q; i++) {
+      const int io = opp<L>(i);
+      if (i == 0) {
+        d[k++] = 0;
+      } else if (i < io) {
+        d[k++] = i;
+        d[k++] = io;
+      }
+    }
+  }
+};
+template <class L> constexpr int emit_dir(int k) { return EmitOrder<L>().d[k]; }
+
+template <class R> __device__ __forceinline__ R add_rn(R a, R b);
+template <> __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+template <> __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+template <class R> __device__ __forceinline__ R mul_rn(R a, R b);
+template <> __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+template <> __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+template <class R> __device__ __forceinline__ R div_rn(R a, R b);
+template <> __device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+template <> __device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+
+// velocity from the summed density and momentum, and |u|^2 (no contraction)
+template <class R>
+__device__ __forceinline__ void cell_velocity(R rho, R jx, R jy, R jz, R& ux, R& uy, R& uz, R& uu) {
+  const R ir = div_rn((R)1, rho);
+  ux = mul_rn(jx, ir);
+  uy = mul_rn(jy, ir);
+  uz = mul_rn(jz, ir);
+  uu = add_rn(add_rn(mul_rn(ux, ux), mul_rn(uy, uy)), mul_rn(uz, uz));
+}
+
+// Accumulators of one thread. k_macro sums the densities in FP64 (MacroSums). The fused sampling
+// step (SampleSums) sums a thread's densities in FP64, then each warp's sum goes into 2^-30 fixed
+// point: an f32 density in [1/128, 16) is an integer multiple of 2^-30, so every partial sum is
+// exact and the totals do not depend on the order of the atomics; they equal the FP64 sums of the
+// same densities, which are exact too for densities in [0.5, 2) on grids below 2^28 cells. A
+// density outside [1/128, 16) (an unstable run) is counted in `nbig` and makes the fused sums NaN.
+struct MacroSums {
+  double rho_ref = 0.0, mass = 0.0;
+  float maxuu = 0.0f;
+  uint32_t nref = 0, nan = 0, nfluid = 0, nbig = 0;
+  template <class R> __device__ __forceinline__ void density(R rho, bool ref) {
+    if (ref) {
+      rho_ref += (double)rho;
+      nref++;
+    }
+    mass += (double)rho;
+    nfluid++;
+  }
+};
+struct SampleSums {
+  double rho_ref = 0.0, mass = 0.0;
+  float maxuu = 0.0f;
+  uint32_t nref = 0, nan = 0, nfluid = 0, nbig = 0;
+  __device__ __forceinline__ void density(float rho, bool ref) {
+    nfluid++;
+    if (ref) nref++;
+    if (!(rho >= 0.0078125f && rho < 16.0f)) {
+      nbig++;
+      return;
+    }
+    mass += (double)rho;
+    if (ref) rho_ref += (double)rho;
+  }
+};
+constexpr double SMP_FIXED = 1073741824.0;  // 2^30
+
+// Everything the sampling pass does with one fluid cell after its moments: the instability test,
+// the velocity texel (half4, returned), the EMA statistics and the accumulators. `m` / `mb` are the
+// cell's EMA state when `loaded`, else they are read here if needed (ema_alpha != 0, or a
+// non-finite value with ema_alpha == 0, where 0 x NaN must still poison the means).
+template <class R, class Sums>
+__device__ __forceinline__ uint2 fluid_sample(const wt_kparams& P, size_t idx, int ix, R rho, R ux, R uy, R uz, R uu,
+                                              float4* __restrict__ meanA, float* __restrict__ meanB, float4 m,
+                                              float mb, bool loaded, Sums& acc) {
+  const float a = P.ema_alpha;
+  const bool bad = !(uu < (R)1.0e6) || !(rho > (R)0);
+  const float o0 = (float)ux, o1 = (float)uy, o2 = (float)uz, o3 = (float)rho;
+  acc.maxuu = fmaxf(acc.maxuu, bad ? 1.0e6f : (float)uu);
+  acc.nan += bad ? 1u : 0u;
+  acc.density(rho, (uint32_t)ix == P.ref_x);
+  const bool finite = isfinite(o0) && isfinite(o1) && isfinite(o2) && isfinite(o3) && isfinite((float)uu);
+  if (a != 0.0f || !finite) {
+    if (!loaded) {
+      m = meanA[idx];
+      mb = meanB[idx];
+    }
+    m.x = m.x * (1.0f - a) + o0 * a;
+    m.y = m.y * (1.0f - a) + o1 * a;
+    m.z = m.z * (1.0f - a) + o2 * a;
+    m.w = m.w * (1.0f - a) + o3 * a;
+    meanA[idx] = m;
+    meanB[idx] = mb * (1.0f - a) + (float)uu * a;
+  }
+  __half2 h01 = __floats2half2_rn(o0, o1);
+  __half2 h23 = __floats2half2_rn(o2, o3);
+  return make_uint2(*reinterpret_cast<uint32_t*>(&h01), *reinterpret_cast<uint32_t*>(&h23));
+}
+
+// The sampling pass fused into a step: where the step's last kernels put the per-cell results.
+// `sets` holds SMP_SETS sets of accumulators, one 128-byte line each (SS_* slots), zeroed before
+// the step; warps add into set (warp index % SMP_SETS), so the atomics spread over 64 lines.
+constexpr int SMP_SETS = 64;
+constexpr int SMP_SET_U64 = 16;
+enum { SS_MAX = 0, SS_NAN, SS_NREF, SS_NFLUID, SS_NBIG, SS_RHOREF, SS_MASS, SS_COUNT };
+constexpr int SS_DONE = SMP_SET_U64 - 1;  // set 0: blocks of k_sample_post that have finished
+static_assert(SMP_SETS * SMP_SET_U64 * sizeof(unsigned long long) == SMP_SETS_BYTES, "accumulator sets");
+struct SampleOut {
+  uint2* vel;
+  float4* meanA;
+  float* meanB;
+  unsigned long long* sets;
+};
+
+// warp-wide: adds the lanes' accumulators into one set (every lane of the warp calls it)
+__device__ __forceinline__ void smp_flush(const SampleSums& acc, unsigned long long* __restrict__ sets,
+                                          uint32_t warp_id) {
+  const unsigned full = 0xffffffffu;
+  const uint32_t nfluid = __reduce_add_sync(full, acc.nfluid);
+  if (nfluid == 0u) return;  // uniform across the warp
+  const uint32_t mx = __reduce_max_sync(full, __float_as_uint(acc.maxuu));  // values >= 0
+  const uint32_t nan = __reduce_add_sync(full, acc.nan);
+  const uint32_t nref = __reduce_add_sync(full, acc.nref);
+  const uint32_t nbig = __reduce_add_sync(full, acc.nbig);
+  double rr = acc.rho_ref, ms = acc.mass;  // exact warp sums (see SampleSums)
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    rr += __shfl_xor_sync(full, rr, o);
+    ms += __shfl_xor_sync(full, ms, o);
+  }
+  const uint32_t lane = threadIdx.x & 31u;
+  unsigned long long* set = sets + (size_t)(warp_id % SMP_SETS) * SMP_SET_U64;
+  if (lane == SS_MAX) {
+    atomicMax(set + SS_MAX, (unsigned long long)mx);
+  } else if (lane < SS_COUNT) {
+    const unsigned long long v =
+        lane == SS_NAN ? nan : lane == SS_NREF ? nref : lane == SS_NFLUID ? nfluid : lane == SS_NBIG ? nbig
+        : lane == SS_RHOREF ? (unsigned long long)__double2ll_rn(rr * SMP_FIXED)
+                            : (unsigned long long)__double2ll_rn(ms * SMP_FIXED);
+    atomicAdd(set + lane, v);
+  }
+}
+
+__device__ __forceinline__ uint32_t global_warp_id() {
+  const uint32_t b = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  const uint32_t t = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+  return b * ((blockDim.x * blockDim.y * blockDim.z + 31u) / 32u) + t / 32u;
+}
+
+// Sampling state of two cells (f32x2 lanes) while a pair kernel emits them: their density and
+// momentum summed from the stored values in emission order (lane-wise IEEE adds, as the scalar
+// sums of k_macro).
+struct PairMoments {
+  float2 rho, jx, jy, jz;
+  // called with the directions in emission order, which starts with direction 0
+  template <class L, int I>
+  __device__ __forceinline__ void add(float2 f) {
+    constexpr int cx = L::c[I][0], cy = L::c[I][1], cz = L::c[I][2];
+    if constexpr (I == 0) {
+      rho = f;
+      jx = jy = jz = make_float2(0.0f, 0.0f);
+    } else {
+      rho = __fadd2_rn(rho, f);
+    }
+    if constexpr (cx > 0) jx = __fadd2_rn(jx, f);
+    if constexpr (cx < 0) jx = __fadd2_rn(jx, make_float2(-f.x, -f.y));
+    if constexpr (cy > 0) jy = __fadd2_rn(jy, f);
+    if constexpr (cy < 0) jy = __fadd2_rn(jy, make_float2(-f.x, -f.y));
+    if constexpr (cz > 0) jz = __fadd2_rn(jz, f);
+    if constexpr (cz < 0) jz = __fadd2_rn(jz, make_float2(-f.x, -f.y));
+  }
+};
+
+// The two cells of a pair kernel (x0, x0 + 1; x0 even) once their outputs were emitted into `pm`:
+// velocity texels (one 16-byte store), EMA statistics, accumulators.
+template <class L>
+__device__ __forceinline__ void pair_sample(const wt_kparams& P, uint32_t idx0, int x0, const PairMoments& pm,
+                                            const SampleOut& O, SampleSums& acc) {
+  float ux, uy, uz, uu;
+  cell_velocity<float>(pm.rho.x, pm.jx.x, pm.jy.x, pm.jz.x, ux, uy, uz, uu);
+  const uint2 ta = fluid_sample<float>(P, idx0, x0, pm.rho.x, ux, uy, uz, uu, O.meanA, O.meanB,
+                                       make_float4(0.f, 0.f, 0.f, 0.f), 0.0f, false, acc);
+  cell_velocity<float>(pm.rho.y, pm.jx.y, pm.jy.y, pm.jz.y, ux, uy, uz, uu);
+  const uint2 tb = fluid_sample<float>(P, idx0 + 1u, x0 + 1, pm.rho.y, ux, uy, uz, uu, O.meanA, O.meanB,
+                                       make_float4(0.f, 0.f, 0.f, 0.f), 0.0f, false, acc);
+  *reinterpret_cast<uint4*>(O.vel + idx0) = make_uint4(ta.x, ta.y, tb.x, tb.y);
+}
+
 template <class S> struct PairIO;
 template <> struct PairIO<StF16> {
   typedef uint32_t pair_t;
@@ -909,6 +1109,11 @@ template <> struct PairIO<StF16> {
   __device__ __forceinline__ static void st(__half* __restrict__ p, uint32_t o, float2 v, float /*w*/) {
     *reinterpret_cast<__half2*>(p + o) = __float22half2_rn(v);
   }
+  // the populations st stores for v, as a later pass reads them back (f = stored + w)
+  __device__ __forceinline__ static float2 readback(float2 v, float w) {
+    const __half2 h = __float22half2_rn(v);
+    return make_float2(h2f_add(__low2half(h), w), h2f_add(__high2half(h), w));
+  }
 };
 template <> struct PairIO<StF32> {
   typedef float2 pair_t;
@@ -926,7 +1131,10 @@ template <> struct PairIO<StF32> {
   __device__ __forceinline__ static float2 cvt(pair_t f, float w) { return make_float2(f.x - w, f.y - w); }
   __device__ __forceinline__ static float cvt1(one_t f, float w) { return f - w; }
   __device__ __forceinline__ static void st(float* __restrict__ p, uint32_t o, float2 v, float w) {
-    *reinterpret_cast<float2*>(p + o) = make_float2(v.x + w, v.y + w);
+    *reinterpret_cast<float2*>(p + o) = make_float2(__fadd_rn(v.x, w), __fadd_rn(v.y, w));
+  }
+  __device__ __forceinline__ static float2 readback(float2 v, float w) {
+    return make_float2(__fadd_rn(v.x, w), __fadd_rn(v.y, w));
   }
 };
 
@@ -935,10 +1143,12 @@ template <int MINB> struct Bounds { static constexpr int v = MINB; };
 
 // The V cells x0 .. x0 + V - 1 of row (iy, iz) (bulk rows only); shared by the single-tunnel
 // kernel and the batch kernel.
-template <class L, class S, int V, bool BGK>
+// With SMP the cells also run the per-cell part of the sampling pass on what they store.
+template <class L, class S, int V, bool BGK, bool SMP = false>
 __device__ __forceinline__ void bulk_cells(const wt_kparams& P, const typename S::T* __restrict__ fin,
                                            typename S::T* __restrict__ fout, const uint8_t* __restrict__ cls,
-                                           int gs, int x0, int iy, int iz) {
+                                           int gs, int x0, int iy, int iz, const SampleOut* O = nullptr,
+                                           SampleSums* acc = nullptr) {
   typedef PairIO<S> IO;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
@@ -1010,10 +1220,15 @@ __device__ __forceinline__ void bulk_cells(const wt_kparams& P, const typename S
         }
       });
     }
+    PairMoments pm;
     collide_shifted2<L, BGK>(P, h, x0 + 2 * g, [&](auto I, float2 v) {
       constexpr int i = decltype(I)::value;
       if (clean) IO::st(ob + (ptrdiff_t)i * N, 2 * g, v, (float)Wc<L, i>::v);
+      if constexpr (SMP) pm.template add<L, i>(IO::readback(v, (float)Wc<L, i>::v));
     });
+    if constexpr (SMP) {
+      if (clean) pair_sample<L>(P, idx0 + 2u * (uint32_t)g, x0 + 2 * g, pm, *O, *acc);
+    }
   }
 }
 
@@ -1021,14 +1236,19 @@ __device__ __forceinline__ void bulk_cells(const wt_kparams& P, const typename S
 // alternate the direction, so each step starts on the planes the previous step wrote last, which
 // are still in L2 (the two population buffers are larger than L2; a fixed order would always
 // start on the planes evicted first). Every cell's result is the same in either order.
-template <class L, class S, int V, int MINB, bool BGK>
+// SMP: the last step of a stepAndSample chunk, which also runs the sampling pass's per-cell work
+// on its bulk cells (accumulators flushed per warp into O.sets).
+template <class L, class S, int V, int MINB, bool BGK, bool SMP = false>
 __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(const __grid_constant__ wt_kparams P,
                                                           const typename S::T* __restrict__ fin,
                                                           typename S::T* __restrict__ fout,
-                                                          const uint8_t* __restrict__ cls, int gs, int zrev) {
-  bulk_cells<L, S, V, BGK>(P, fin, fout, cls, gs, (blockIdx.x * blockDim.x + threadIdx.x) * V,
-                           blockIdx.y * blockDim.y + threadIdx.y,
-                           zrev ? (int)(gridDim.z - 1u - blockIdx.z) : (int)blockIdx.z);
+                                                          const uint8_t* __restrict__ cls, int gs, int zrev,
+                                                          const __grid_constant__ SampleOut O) {
+  SampleSums acc;
+  bulk_cells<L, S, V, BGK, SMP>(P, fin, fout, cls, gs, (blockIdx.x * blockDim.x + threadIdx.x) * V,
+                                blockIdx.y * blockDim.y + threadIdx.y,
+                                zrev ? (int)(gridDim.z - 1u - blockIdx.z) : (int)blockIdx.z, &O, &acc);
+  if constexpr (SMP) smp_flush(acc, O.sets, global_warp_id());
 }
 
 // ---- row pipeline: interior rows streamed through shared memory by bulk copies ---------------
@@ -1256,11 +1476,12 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_batch_bulk(const _
 // (row r * nx + x of `xb`) and stores nothing; MODE 2 collides with the eddy viscosities nub[row].
 enum : int { FM_SMAG = 0, FM_FEATURES = 1, FM_NU = 2 };
 
-template <class L, class S, int MODE>
+template <class L, class S, int MODE, bool SMP = false>
 __device__ __forceinline__ void face_rows(const wt_kparams& P, const typename S::T* __restrict__ fin,
                                           typename S::T* __restrict__ fout, const uint8_t* __restrict__ cls, int gs,
                                           const uint32_t* __restrict__ sdf, float* __restrict__ xb,
-                                          const float* __restrict__ nub) {
+                                          const float* __restrict__ nub, const SampleOut* O = nullptr,
+                                          SampleSums* acc = nullptr) {
   typedef PairIO<S> IO;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
@@ -1376,9 +1597,11 @@ __device__ __forceinline__ void face_rows(const wt_kparams& P, const typename S:
       }
     });
   }
+  PairMoments pm;
   auto emit = [&](auto I, float2 v) {
     constexpr int i = decltype(I)::value;
     if (clean) IO::st(fout, i * N + idx0, v, (float)Wc<L, i>::v);
+    if constexpr (SMP) pm.template add<L, i>(IO::readback(v, (float)Wc<L, i>::v));
   };
   const size_t slot = (size_t)r * (size_t)NX + (size_t)x0;
   if constexpr (MODE == FM_FEATURES) {
@@ -1393,15 +1616,21 @@ __device__ __forceinline__ void face_rows(const wt_kparams& P, const typename S:
     if (gwall) collide_shifted2<L, true>(P, h, x0, emit, P.tau_wall);
     else if (P.collision == 1u) collide_shifted2<L, true>(P, h, x0, emit);
     else collide_shifted2<L, false>(P, h, x0, emit);
+    if constexpr (SMP) {
+      if (clean) pair_sample<L>(P, idx0, x0, pm, *O, *acc);
+    }
   }
 }
 
-template <class L, class S>
+template <class L, class S, bool SMP = false>
 __global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kparams P,
                                                 const typename S::T* __restrict__ fin,
                                                 typename S::T* __restrict__ fout,
-                                                const uint8_t* __restrict__ cls, int gs) {
-  face_rows<L, S, FM_SMAG>(P, fin, fout, cls, gs, nullptr, nullptr, nullptr);
+                                                const uint8_t* __restrict__ cls, int gs,
+                                                const __grid_constant__ SampleOut O) {
+  SampleSums acc;
+  face_rows<L, S, FM_SMAG, SMP>(P, fin, fout, cls, gs, nullptr, nullptr, nullptr, &O, &acc);
+  if constexpr (SMP) smp_flush(acc, O.sets, global_warp_id());
 }
 
 // face rows with the learned closure: MODE FM_FEATURES (inputs of the network) or FM_NU (collision
@@ -1883,17 +2112,14 @@ __global__ void __launch_bounds__(128) k_boundary_build(const __grid_constant__ 
 // at once (coalesced across the warp), then every gather, then the collision and the stores.
 // MODE as for the face rows: FM_SMAG, FM_FEATURES (the listed cell's features into row k of xb,
 // nothing stored) or FM_NU (collision with the eddy viscosity nub[k]).
-template <class L, class S, int MODE = FM_SMAG>
-__global__ void __launch_bounds__(64) k_boundary_tab(const __grid_constant__ wt_kparams P,
-                                                     const typename S::T* __restrict__ fin,
-                                                     typename S::T* __restrict__ fout,
-                                                     const uint2* __restrict__ bcell, const uint4* __restrict__ rec,
-                                                     const float* __restrict__ gam, uint32_t count, uint32_t cap,
-                                                     const uint32_t* __restrict__ sdf, float* __restrict__ xb,
-                                                     const float* __restrict__ nub) {
+template <class L, class S, int MODE = FM_SMAG, bool SMP = false>
+__device__ __forceinline__ void boundary_cell(const wt_kparams& P, const typename S::T* __restrict__ fin,
+                                              typename S::T* __restrict__ fout, const uint2* __restrict__ bcell,
+                                              const uint4* __restrict__ rec, const float* __restrict__ gam,
+                                              uint32_t k, uint32_t cap, const uint32_t* __restrict__ sdf,
+                                              float* __restrict__ xb, const float* __restrict__ nub,
+                                              const SampleOut* O, SampleSums* acc) {
   constexpr int Q = L::Q;
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= count) return;
   const uint2 hc = bcell[k];
   uint4 r[Q];
   float g[Q];
@@ -1929,6 +2155,48 @@ __global__ void __launch_bounds__(64) k_boundary_tab(const __grid_constant__ wt_
     constexpr int i = I;
     S::st(fout, (size_t)i * P.n + hc.x, fo[i], (float)Wc<L, i>::v);
   });
+  if constexpr (SMP) {
+    // the sampling pass on the stored values, summed in the pair kernels' emission order
+    float rho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+    static_for<Q>([&](auto K) {
+      constexpr int i = emit_dir<L>(K);
+      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+      float f;
+      if constexpr (S::PREC == WT_PREC_F16) {
+        constexpr float w = (float)Wc<L, i>::v;
+        f = h2f_add(__float2half_rn(__fsub_rn(fo[i], w)), w);
+      } else {
+        f = fo[i];
+      }
+      if constexpr (K == 0) rho = f;
+      else rho = __fadd_rn(rho, f);
+      if constexpr (cx > 0) jx = __fadd_rn(jx, f);
+      if constexpr (cx < 0) jx = __fadd_rn(jx, -f);
+      if constexpr (cy > 0) jy = __fadd_rn(jy, f);
+      if constexpr (cy < 0) jy = __fadd_rn(jy, -f);
+      if constexpr (cz > 0) jz = __fadd_rn(jz, f);
+      if constexpr (cz < 0) jz = __fadd_rn(jz, -f);
+    });
+    float ux, uy, uz, uu;
+    cell_velocity<float>(rho, jx, jy, jz, ux, uy, uz, uu);
+    O->vel[hc.x] = fluid_sample<float>(P, hc.x, ix, rho, ux, uy, uz, uu, O->meanA, O->meanB,
+                                       make_float4(0.f, 0.f, 0.f, 0.f), 0.0f, false, *acc);
+  }
+}
+
+template <class L, class S, int MODE = FM_SMAG, bool SMP = false>
+__global__ void __launch_bounds__(64) k_boundary_tab(const __grid_constant__ wt_kparams P,
+                                                     const typename S::T* __restrict__ fin,
+                                                     typename S::T* __restrict__ fout,
+                                                     const uint2* __restrict__ bcell, const uint4* __restrict__ rec,
+                                                     const float* __restrict__ gam, uint32_t count, uint32_t cap,
+                                                     const uint32_t* __restrict__ sdf, float* __restrict__ xb,
+                                                     const float* __restrict__ nub,
+                                                     const __grid_constant__ SampleOut O) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  SampleSums acc;
+  if (k < count) boundary_cell<L, S, MODE, SMP>(P, fin, fout, bcell, rec, gam, k, cap, sdf, xb, nub, &O, &acc);
+  if constexpr (SMP) smp_flush(acc, O.sets, global_warp_id());
 }
 
 // Rest state written into the solid cells of one population buffer.
@@ -1946,21 +2214,24 @@ __global__ void __launch_bounds__(256) k_fill_solid(const __grid_constant__ wt_k
   }
 }
 
-// Builds the boundary list (every fluid cell of a group holding a solid or near-solid cell; solid
-// cells keep the rest state and need no per-step work): pass 0 counts, pass 1 writes
-// (warp-aggregated slots, in x order inside each warp).
+// Builds the boundary list (which = 0: every fluid cell of a group holding a solid or near-solid
+// cell; solid cells keep the rest state and need no per-step work) or the solid list (which = 1:
+// every solid cell, for the fused sampling pass): pass 0 counts, pass 1 writes (warp-aggregated
+// slots, in x order inside each warp).
 template <class L>
 __global__ void __launch_bounds__(256) k_boundary_list(const __grid_constant__ wt_kparams P,
                                                        const uint8_t* __restrict__ cls, int gs,
                                                        uint32_t* __restrict__ counter, uint32_t* __restrict__ list,
-                                                       int pass) {
+                                                       int pass, int which) {
   const uint32_t NX = P.nx;
   const uint32_t N = P.n;
   const uint32_t lane = threadIdx.x & 31;
   for (uint32_t base = (blockIdx.x * blockDim.x + (threadIdx.x & ~31u)); base < N; base += gridDim.x * blockDim.x) {
     const uint32_t c = base + lane;
     bool sel = false;
-    if (c < N) {
+    if (c < N && which == 1) {
+      sel = (cls[c] & CLS_SOLID) != 0;
+    } else if (c < N) {
       const uint32_t g0 = c - (c % NX) % (uint32_t)gs;
       bool dirty = false;
       for (int k = 0; k < gs; k++) dirty = dirty || (cls[g0 + k] & CLS_BOUNDARY) != 0;
@@ -1992,6 +2263,214 @@ __device__ __forceinline__ float warp_max(float v) {
   return v;
 }
 
+// Momentum exchange of one fluid cell (wgslLbm.ts:370-392, 446-453): for every link into a solid,
+// the value streaming would build there (Bouzidi with its q branches, the wheel's moving-wall term)
+// plus the outgoing population, minus the mass fix of the wheel links. f[] are the cell's stored
+// populations (shift undone); Bouzidi partners at x - c_i are read from `fin`.
+// GATHER issues the loads in two rounds (every neighbour's flags; then, for the solid links, the
+// wall distances and the partner's flags and population) instead of one chain per link: for a
+// kernel whose few threads all take this path (k_sample_post). Without it the loads sit at each
+// link and hold no registers, for k_macro, where most cells skip the path and occupancy hides the
+// latency. Both give the same bits.
+template <class L, class S, bool GATHER>
+__device__ __forceinline__ void cell_force(const wt_kparams& P, const typename S::T* __restrict__ fin,
+                                           const uint32_t* __restrict__ flags, const uint32_t* __restrict__ sdf,
+                                           const Wheels& W, size_t idx, int ix, int iy, int iz,
+                                           const typename S::R (&f)[L::Q], typename S::R& Fx, typename S::R& Fy,
+                                           typename S::R& Fz) {
+  typedef typename S::R R;
+  constexpr int Q = L::Q;
+  const int NX = P.nx, NY = P.ny, NZ = P.nz;
+  const size_t N = P.n;
+  auto safe = [&](int x, int y, int z) -> int64_t {
+    if (x < 0 || y < 0 || z < 0 || x >= NX || y >= NY || z >= NZ) return -1;
+    return (int64_t)cell_id(x, y, z, NX, NY);
+  };
+  const bool interp = P.interp != 0u;
+  const uint32_t sd_self = interp ? __ldg(sdf + idx) : 0u;
+  // link i's words: the solid neighbour's flags, its wall distance, the partner's (x - c_i) flags
+  // (1 outside the domain) and population
+  auto link_words = [&](auto I, uint32_t& fli, uint32_t& sdi, uint32_t& flbi, R& fbi) {
+    constexpr int i = decltype(I)::value;
+    constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+    const int64_t sn = safe(ix + cx, iy + cy, iz + cz);
+    fli = sn >= 0 ? __ldg(flags + sn) : 0u;
+    sdi = 0u;
+    flbi = 1u;
+    fbi = (R)0;
+    if (fli != 0u) {
+      if (interp) sdi = __ldg(sdf + sn);
+      const int64_t bk = safe(ix - cx, iy - cy, iz - cz);
+      if (bk >= 0) {
+        flbi = __ldg(flags + bk);
+        fbi = S::ld(fin, (size_t)i * N + (size_t)bk, (R)Wc<L, i>::v);
+      }
+    }
+  };
+  uint32_t gfl[GATHER ? Q : 1], gsd[GATHER ? Q : 1], gflb[GATHER ? Q : 1];
+  R gfb[GATHER ? Q : 1];
+  if constexpr (GATHER) {
+    // round 1: every neighbour's flags
+    gfl[0] = 0u;
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      if constexpr (i > 0) {
+        constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+        const int64_t sn = safe(ix + cx, iy + cy, iz + cz);
+        gfl[i] = sn >= 0 ? __ldg(flags + sn) : 0u;
+      }
+    });
+    // round 2: the solid links' distances and partners
+    static_for<Q>([&](auto I) {
+      constexpr int i = I;
+      gsd[i] = 0u;
+      gflb[i] = 1u;
+      gfb[i] = (R)0;
+      if constexpr (i > 0) {
+        if (gfl[i] != 0u) {
+          constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+          if (interp) gsd[i] = __ldg(sdf + safe(ix + cx, iy + cy, iz + cz));
+          const int64_t bk = safe(ix - cx, iy - cy, iz - cz);
+          if (bk >= 0) {
+            gflb[i] = __ldg(flags + bk);
+            gfb[i] = S::ld(fin, (size_t)i * N + (size_t)bk, (R)Wc<L, i>::v);
+          }
+        }
+      }
+    });
+  }
+  R mvSum = 0, mvW = 0, Cwx = 0, Cwy = 0, Cwz = 0;
+  Fx = 0;
+  Fy = 0;
+  Fz = 0;
+  static_for<Q>([&](auto I) {
+    constexpr int i = I;
+    if constexpr (i > 0) {
+      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+      constexpr R w = (R)Wc<L, i>::v;
+      uint32_t fli, sdi, flbi;
+      R fbi;
+      if constexpr (GATHER) {
+        fli = gfl[i];
+        sdi = gsd[i];
+        flbi = gflb[i];
+        fbi = gfb[i];
+      } else {
+        link_words(I, fli, sdi, flbi, fbi);
+      }
+      if (fli != 0u) {
+        // linkQ (wgslLbm.ts:37-43)
+        R q = (R)0.5;
+        if (interp) {
+          const R a = sd_self == 0u ? (R)-1 : (R)__uint_as_float(~sd_self);
+          const R b = sdi == 0u ? (R)-1 : (R)__uint_as_float(~sdi);
+          if (!(a < (R)0 || b < (R)0 || a + b < (R)1e-6f)) {
+            q = a / (a + b);
+            q = q < (R)0.01f ? (R)0.01f : (q > (R)0.99f ? (R)0.99f : q);
+          }
+        }
+        R fr = f[i];
+        if (q < (R)0.5) {
+          if (flbi == 0u) fr = (R)2 * q * f[i] + ((R)1 - (R)2 * q) * fbi;
+          else q = (R)0.5;
+        } else if (q > (R)0.5) {
+          constexpr int oi = opp<L>(i);
+          fr = ((R)0.5 / q) * f[i] + ((R)1 - (R)0.5 / q) * f[oi];
+        }
+        const uint32_t tg = fli >> 8u;
+        if (tg != 0u) {
+          R wx, wy, wz;
+          wheel_vel<R>(P, W, tg - 1u, (R)ix + (R)(0.5 + cx / 2.0), (R)iy + (R)(0.5 + cy / 2.0),
+                       (R)iz + (R)(0.5 + cz / 2.0), wx, wy, wz);
+          const R dot = (R)cx * wx + (R)cy * wy + (R)cz * wz;
+          const R mv = -(R)(6.0 * Wc<L, i>::v) * (q > (R)0.5 ? (R)0.5 / q : (R)1) * dot;
+          fr += mv;
+          mvSum += mv;
+          mvW += w;
+          Cwx += (R)cx * w;
+          Cwy += (R)cy * w;
+          Cwz += (R)cz * w;
+        }
+        const R t = f[i] + fr - (R)(2.0 * Wc<L, i>::v);
+        Fx += (R)cx * t;
+        Fy += (R)cy * t;
+        Fz += (R)cz * t;
+      }
+    }
+  });
+  if (mvW > (R)0) {
+    const R k = mvSum / mvW;
+    Fx -= Cwx * k;
+    Fy -= Cwy * k;
+    Fz -= Cwz * k;
+  }
+}
+
+// A solid cell of the sampling pass: density extrapolated from its fluid face neighbours
+// (wgslLbm.ts:460-466), zero velocity, EMA towards that state (meanB cleared). Returns the texel.
+// GATHER (for k_sample_post) loads every neighbour's flags, then every population it needs, in two
+// rounds; without it (k_macro) the loads sit at each neighbour. Both give the same bits.
+template <class L, class S, bool GATHER>
+__device__ __forceinline__ uint2 solid_sample(const wt_kparams& P, const typename S::T* __restrict__ fin,
+                                              const uint32_t* __restrict__ flags, size_t idx, int ix, int iy, int iz,
+                                              float4* __restrict__ meanA, float* __restrict__ meanB, float4 m) {
+  typedef typename S::R R;
+  constexpr int NB = L::DIM == 3 ? 6 : 4;
+  const int NX = P.nx, NY = P.ny, NZ = P.nz;
+  const size_t N = P.n;
+  const float a = P.ema_alpha;
+  const int nb[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+  int64_t sn[NB];
+  bool fluid[NB];
+#pragma unroll
+  for (int k = 0; k < NB; k++) {
+    const int x = ix + nb[k][0], y = iy + nb[k][1], z = iz + nb[k][2];
+    const bool in = !(x < 0 || y < 0 || z < 0 || x >= NX || y >= NY || z >= NZ);
+    sn[k] = in ? (int64_t)cell_id(x, y, z, NX, NY) : -1;
+    if constexpr (GATHER) fluid[k] = in && __ldg(flags + sn[k]) == 0u;
+  }
+  R rs = 0, rn = 0;
+#pragma unroll
+  for (int k = 0; k < NB; k++) {
+    R r = 0;
+    if constexpr (GATHER) {
+      // the fluid neighbours' populations, as predicated loads that are all in flight together
+      // (a solid cell inside the body has no fluid neighbour and reads nothing)
+      R v[L::Q];
+      static_for<L::Q>([&](auto I) {
+        constexpr int j = I;
+        v[j] = fluid[k] ? S::ld(fin, (size_t)j * N + (size_t)sn[k], (R)Wc<L, j>::v) : (R)0;
+      });
+      static_for<L::Q>([&](auto I) {
+        constexpr int j = I;
+        r += v[j];
+      });
+    } else {
+      fluid[k] = sn[k] >= 0 && flags[sn[k]] == 0u;
+      if (fluid[k]) {
+        static_for<L::Q>([&](auto I) {
+          constexpr int j = I;
+          r += S::ld(fin, (size_t)j * N + (size_t)sn[k], (R)Wc<L, j>::v);
+        });
+      }
+    }
+    if (fluid[k]) {
+      rs += r;
+      rn += (R)1;
+    }
+  }
+  const float o3 = rn > (R)0 ? (float)(rs / rn) : 1.0f;
+  m.x = m.x * (1.0f - a) + 0.0f * a;
+  m.y = m.y * (1.0f - a) + 0.0f * a;
+  m.z = m.z * (1.0f - a) + 0.0f * a;
+  m.w = m.w * (1.0f - a) + o3 * a;
+  meanA[idx] = m;
+  meanB[idx] = 0.0f;
+  __half2 h01 = __floats2half2_rn(0.0f, 0.0f);
+  __half2 h23 = __floats2half2_rn(0.0f, o3);
+  return make_uint2(*reinterpret_cast<uint32_t*>(&h01), *reinterpret_cast<uint32_t*>(&h23));
+}
+
 // Grid-stride over cells (one per thread when the grid has a block per 256 cells). `cls` (may be NULL)
 // is the class byte: a fluid cell without CLS_NEAR_SOLID has no in-domain solid neighbour, so its
 // 18 link checks are skipped; with NULL every fluid cell checks its links.
@@ -2004,13 +2483,12 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
                                                          float* __restrict__ meanB, double* __restrict__ partials) {
   typedef typename S::R R;
   constexpr int Q = L::Q;
-  constexpr bool D3 = L::DIM == 3;
-  const int NX = P.nx, NY = P.ny, NZ = P.nz;
+  const int NX = P.nx, NY = P.ny;
   const size_t N = P.n;
   const float a = P.ema_alpha;
-  double accF[3] = {0, 0, 0}, accRho = 0, accMass = 0;
-  uint32_t accNref = 0, accNan = 0, accSolid = 0, accFluid = 0;
-  float accMax = 0.0f;
+  double accF[3] = {0, 0, 0};
+  MacroSums acc;
+  uint32_t accSolid = 0;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < N; idx += (size_t)gridDim.x * blockDim.x) {
     const uint32_t c32 = (uint32_t)idx;  // n < 2^32
     const int ix = (int)(c32 % (uint32_t)NX);
@@ -2020,11 +2498,6 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
       y = (int)(t % (uint32_t)NY);
       z = (int)(t / (uint32_t)NY);
     };
-    auto safe = [&](int x, int y, int z) -> int64_t {
-      if (x < 0 || y < 0 || z < 0 || x >= NX || y >= NY || z >= NZ) return -1;
-      return (int64_t)cell_id(x, y, z, NX, NY);
-    };
-    float out[4] = {0.f, 0.f, 0.f, 1.f};
     // every load of the cell is issued before the first branch: one memory round trip per cell.
     // With the class byte, the cell's own solid test reads it (1 B) instead of the flags (4 B).
     const uint8_t cl = cls != nullptr ? cls[idx] : (uint8_t)0;
@@ -2034,7 +2507,8 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
     // not finite (0 x NaN = NaN); they are then read and written only in that case
     float4 m = make_float4(0.f, 0.f, 0.f, 0.f);
     float mb = 0.0f;
-    if (a != 0.0f || solid) {
+    const bool loaded = a != 0.0f || solid;
+    if (loaded) {
       m = meanA[idx];
       mb = meanB[idx];
     }
@@ -2043,131 +2517,41 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
       constexpr int i = I;
       f[i] = S::ld(fin, (size_t)i * N + idx, (R)Wc<L, i>::v);
     });
+    uint2 texel;
     if (!solid) {
-      R rho = f[0], jx = 0, jy = 0, jz = 0;
-      static_for<Q>([&](auto I) {
-        constexpr int i = I;
+      // density and momentum in the step kernels' emission order (the fused sampling pass's sums)
+      R rho = 0, jx = 0, jy = 0, jz = 0;
+      static_for<Q>([&](auto K) {
+        constexpr int i = emit_dir<L>(K);
         constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
-        if constexpr (i > 0) rho += f[i];
-        if constexpr (cx != 0) jx += (R)cx * f[i];
-        if constexpr (cy != 0) jy += (R)cy * f[i];
-        if constexpr (cz != 0) jz += (R)cz * f[i];
+        if constexpr (K == 0) rho = f[i];
+        else rho = add_rn(rho, f[i]);
+        if constexpr (cx > 0) jx = add_rn(jx, f[i]);
+        if constexpr (cx < 0) jx = add_rn(jx, -f[i]);
+        if constexpr (cy > 0) jy = add_rn(jy, f[i]);
+        if constexpr (cy < 0) jy = add_rn(jy, -f[i]);
+        if constexpr (cz > 0) jz = add_rn(jz, f[i]);
+        if constexpr (cz < 0) jz = add_rn(jz, -f[i]);
       });
-      const R ir = (R)1 / rho;
-      const R ux = jx * ir, uy = jy * ir, uz = D3 ? jz * ir : (R)0;
-      R Fx = 0, Fy = 0, Fz = 0, mvSum = 0, mvW = 0, Cwx = 0, Cwy = 0, Cwz = 0;
-      int iy = 0, iz = 0;
-      if (links) cell_yz(iy, iz);
-      if (links) static_for<Q>([&](auto I) {
-        constexpr int i = I;
-        if constexpr (i > 0) {
-          constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
-          constexpr R w = (R)Wc<L, i>::v;
-          const int64_t s = safe(ix + cx, iy + cy, iz + cz);
-          if (s >= 0 && flags[s] != 0u) {
-            R q = link_q<R>(P, sdf, idx, (size_t)s);
-            R fr = f[i];
-            if (q < (R)0.5) {
-              const int64_t bk = safe(ix - cx, iy - cy, iz - cz);
-              if (bk >= 0 && flags[bk] == 0u) fr = (R)2 * q * f[i] + ((R)1 - (R)2 * q) * S::ld(fin, (size_t)i * N + (size_t)bk, w);
-              else q = (R)0.5;
-            } else if (q > (R)0.5) {
-              constexpr int oi = opp<L>(i);
-              fr = ((R)0.5 / q) * f[i] + ((R)1 - (R)0.5 / q) * f[oi];
-            }
-            const uint32_t tg = flags[s] >> 8u;
-            if (tg != 0u) {
-              R wx, wy, wz;
-              wheel_vel<R>(P, W, tg - 1u, (R)ix + (R)(0.5 + cx / 2.0), (R)iy + (R)(0.5 + cy / 2.0),
-                           (R)iz + (R)(0.5 + cz / 2.0), wx, wy, wz);
-              const R dot = (R)cx * wx + (R)cy * wy + (R)cz * wz;
-              const R mv = -(R)(6.0 * Wc<L, i>::v) * (q > (R)0.5 ? (R)0.5 / q : (R)1) * dot;
-              fr += mv;
-              mvSum += mv;
-              mvW += w;
-              Cwx += (R)cx * w;
-              Cwy += (R)cy * w;
-              Cwz += (R)cz * w;
-            }
-            const R t = f[i] + fr - (R)(2.0 * Wc<L, i>::v);
-            Fx += (R)cx * t;
-            Fy += (R)cy * t;
-            Fz += (R)cz * t;
-          }
-        }
-      });
-      if (mvW > (R)0) {
-        const R k = mvSum / mvW;
-        Fx -= Cwx * k;
-        Fy -= Cwy * k;
-        Fz -= Cwz * k;
+      R ux, uy, uz, uu;
+      cell_velocity<R>(rho, jx, jy, jz, ux, uy, uz, uu);
+      if (links) {
+        int iy, iz;
+        cell_yz(iy, iz);
+        R Fx, Fy, Fz;
+        cell_force<L, S, false>(P, fin, flags, sdf, W, idx, ix, iy, iz, f, Fx, Fy, Fz);
+        accF[0] += (double)Fx;
+        accF[1] += (double)Fy;
+        accF[2] += (double)Fz;
       }
-      const R uu = ux * ux + uy * uy + uz * uz;
-      const bool bad = !(uu < (R)1.0e6) || !(rho > (R)0);
-      out[0] = (float)ux;
-      out[1] = (float)uy;
-      out[2] = (float)uz;
-      out[3] = (float)rho;
-      accF[0] += (double)Fx;
-      accF[1] += (double)Fy;
-      accF[2] += (double)Fz;
-      accMax = fmaxf(accMax, bad ? 1.0e6f : (float)uu);
-      if ((uint32_t)ix == P.ref_x) {
-        accRho += (double)rho;
-        accNref++;
-      }
-      accNan += bad ? 1u : 0u;
-      // global mass-conservation check: FP64 sum of the fluid cells' densities
-      accMass += (double)rho;
-      accFluid++;
-      const bool finite = isfinite(out[0]) && isfinite(out[1]) && isfinite(out[2]) && isfinite(out[3]) &&
-                          isfinite((float)uu);
-      if (a != 0.0f || !finite) {
-        if (a == 0.0f) {
-          m = meanA[idx];
-          mb = meanB[idx];
-        }
-        m.x = m.x * (1.0f - a) + out[0] * a;
-        m.y = m.y * (1.0f - a) + out[1] * a;
-        m.z = m.z * (1.0f - a) + out[2] * a;
-        m.w = m.w * (1.0f - a) + out[3] * a;
-        meanA[idx] = m;
-        meanB[idx] = mb * (1.0f - a) + (float)uu * a;
-      }
+      texel = fluid_sample<R>(P, idx, ix, rho, ux, uy, uz, uu, meanA, meanB, m, mb, loaded, acc);
     } else {
-      // density extrapolated into the solid from fluid face neighbours (wgslLbm.ts:460-466)
-      R rs = 0, rn = 0;
       int iy, iz;
       cell_yz(iy, iz);
-      const int nb[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
-#pragma unroll
-      for (int k = 0; k < (D3 ? 6 : 4); k++) {
-        const int64_t s = safe(ix + nb[k][0], iy + nb[k][1], iz + nb[k][2]);
-        if (s >= 0 && flags[s] == 0u) {
-          R r = 0;
-          static_for<Q>([&](auto I) {
-            constexpr int j = I;
-            r += S::ld(fin, (size_t)j * N + (size_t)s, (R)Wc<L, j>::v);
-          });
-          rs += r;
-          rn += (R)1;
-        }
-      }
-      if (rn > (R)0) out[3] = (float)(rs / rn);
-      m.x = m.x * (1.0f - a) + out[0] * a;
-      m.y = m.y * (1.0f - a) + out[1] * a;
-      m.z = m.z * (1.0f - a) + out[2] * a;
-      m.w = m.w * (1.0f - a) + out[3] * a;
-      meanA[idx] = m;
-      meanB[idx] = 0.0f;
+      texel = solid_sample<L, S, false>(P, fin, flags, idx, ix, iy, iz, meanA, meanB, m);
       accSolid++;
     }
-    __half2 h01 = __floats2half2_rn(out[0], out[1]);
-    __half2 h23 = __floats2half2_rn(out[2], out[3]);
-    uint2 pk;
-    pk.x = *reinterpret_cast<uint32_t*>(&h01);
-    pk.y = *reinterpret_cast<uint32_t*>(&h23);
-    vel[idx] = pk;
+    vel[idx] = texel;
   }
   // block reduction. Counts by warp votes / integer reductions; the FP64 sums are shuffled only in
   // warps that hold a non-zero value (most warps have no wall link and no reference-plane cell).
@@ -2178,13 +2562,14 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
     accF[1] = warp_sum(accF[1]);
     accF[2] = warp_sum(accF[2]);
   }
-  if (__any_sync(full, accNref != 0u)) accRho = warp_sum(accRho);
-  accMass = warp_sum(accMass);
-  const float mx = warp_max(accMax);
-  const uint32_t nref = __reduce_add_sync(full, accNref);
-  const uint32_t nnan = __reduce_add_sync(full, accNan);
+  double accRho = acc.rho_ref;
+  if (__any_sync(full, acc.nref != 0u)) accRho = warp_sum(accRho);
+  const double accMass = warp_sum(acc.mass);
+  const float mx = warp_max(acc.maxuu);
+  const uint32_t nref = __reduce_add_sync(full, acc.nref);
+  const uint32_t nnan = __reduce_add_sync(full, acc.nan);
   const uint32_t nsolid = __reduce_add_sync(full, accSolid);
-  const uint32_t nfluid = __reduce_add_sync(full, accFluid);
+  const uint32_t nfluid = __reduce_add_sync(full, acc.nfluid);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (lane == 0) {
     sh[wid][0] = accF[0];
@@ -2212,6 +2597,128 @@ __global__ void __launch_bounds__(MACRO_THREADS, 3) k_macro(const wt_kparams P, 
       }
       if (lane == 0) partials[(size_t)blockIdx.x * MACRO_SLOTS + k] = x;
     }
+  }
+}
+
+// The part of the fused sampling pass that needs the whole step done (runs right after the
+// sampling step): the momentum-exchange force of the listed fluid cells (the boundary list holds
+// every fluid cell next to a solid) and every solid cell (density extrapolated from its fluid face
+// neighbours, velocity texel, EMA statistics, count). Each block writes [sum Fx, Fy, Fz (FP64),
+// solid count] to partials[4 b ..]; the block that finishes last (a counter in set 0, no waiting)
+// reduces the accumulator sets and the partials, in a fixed order, into the MACRO_SLOTS result.
+// Densities come back from fixed point; any density outside its range makes both density sums NaN.
+constexpr int POST_SLOTS = 4;
+template <class L, class S>
+__global__ void __launch_bounds__(MACRO_THREADS) k_sample_post(const __grid_constant__ wt_kparams P,
+                                                              const typename S::T* __restrict__ fin,
+                                                              const uint32_t* __restrict__ flags,
+                                                              const uint32_t* __restrict__ sdf,
+                                                              const uint8_t* __restrict__ cls,
+                                                              const __grid_constant__ Wheels W,
+                                                              const uint32_t* __restrict__ bnd, uint32_t nbnd,
+                                                              const uint32_t* __restrict__ solids, uint32_t nsolid,
+                                                              uint2* __restrict__ vel, float4* __restrict__ meanA,
+                                                              float* __restrict__ meanB, double* __restrict__ partials,
+                                                              unsigned long long* __restrict__ sets,
+                                                              double* __restrict__ result) {
+  typedef typename S::R R;
+  constexpr int Q = L::Q;
+  constexpr int NW = MACRO_THREADS / 32;
+  const int NX = P.nx, NY = P.ny;
+  const size_t N = P.n;
+  double accF[3] = {0, 0, 0};
+  uint32_t accSolid = 0;
+  const uint32_t items = nbnd + nsolid;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < items; k += gridDim.x * blockDim.x) {
+    const bool is_solid = k >= nbnd;
+    const uint32_t c = is_solid ? solids[k - nbnd] : bnd[k];
+    const int ix = (int)(c % (uint32_t)NX);
+    const uint32_t t = c / (uint32_t)NX;
+    const int iy = (int)(t % (uint32_t)NY), iz = (int)(t / (uint32_t)NY);
+    if (is_solid) {
+      vel[c] = solid_sample<L, S, true>(P, fin, flags, c, ix, iy, iz, meanA, meanB, meanA[c]);
+      accSolid++;
+    } else if (cls[c] & CLS_NEAR_SOLID) {
+      R f[Q];
+      static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        f[i] = S::ld(fin, (size_t)i * N + c, (R)Wc<L, i>::v);
+      });
+      R Fx, Fy, Fz;
+      cell_force<L, S, true>(P, fin, flags, sdf, W, c, ix, iy, iz, f, Fx, Fy, Fz);
+      accF[0] += (double)Fx;
+      accF[1] += (double)Fy;
+      accF[2] += (double)Fz;
+    }
+  }
+  __shared__ double sh[NW][POST_SLOTS];
+  __shared__ bool last;
+  const unsigned full = 0xffffffffu;
+  accF[0] = warp_sum(accF[0]);
+  accF[1] = warp_sum(accF[1]);
+  accF[2] = warp_sum(accF[2]);
+  const uint32_t nsol = __reduce_add_sync(full, accSolid);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    sh[wid][0] = accF[0];
+    sh[wid][1] = accF[1];
+    sh[wid][2] = accF[2];
+    sh[wid][3] = (double)nsol;
+  }
+  __syncthreads();
+  if (threadIdx.x < POST_SLOTS) {
+    double x = 0.0;
+    for (int w = 0; w < NW; w++) x += sh[w][threadIdx.x];
+    partials[(size_t)blockIdx.x * POST_SLOTS + threadIdx.x] = x;
+  }
+  // the last block to get here reduces everything (its partials are visible after the fence)
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(sets + SS_DONE, 1ull) == (unsigned long long)(gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // accumulator sets: warp w < SS_COUNT takes slot w of the 64 sets (two per lane)
+  __shared__ unsigned long long shS[SS_COUNT];
+  if (wid < SS_COUNT) {
+    unsigned long long v0 = sets[(size_t)lane * SMP_SET_U64 + wid];
+    unsigned long long v1 = sets[(size_t)(lane + 32) * SMP_SET_U64 + wid];
+    unsigned long long v = wid == SS_MAX ? (v0 > v1 ? v0 : v1) : v0 + v1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long u = __shfl_xor_sync(full, v, o);
+      v = wid == SS_MAX ? (u > v ? u : v) : v + u;
+    }
+    if (lane == 0) shS[wid] = v;
+  }
+  // the blocks' partials in a fixed order
+  double v[POST_SLOTS] = {0, 0, 0, 0};
+  for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < POST_SLOTS; k++) v[k] += partials[(size_t)b * POST_SLOTS + k];
+#pragma unroll
+  for (int k = 0; k < POST_SLOTS; k++) v[k] = warp_sum(v[k]);
+  __syncthreads();  // sh is reused
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < POST_SLOTS; k++) sh[wid][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double F[POST_SLOTS] = {0, 0, 0, 0};
+    for (int w = 0; w < NW; w++)
+      for (int k = 0; k < POST_SLOTS; k++) F[k] += sh[w][k];
+    const bool big = shS[SS_NBIG] != 0ull;
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    result[0] = F[0];
+    result[1] = F[1];
+    result[2] = F[2];
+    result[3] = (double)__uint_as_float((uint32_t)shS[SS_MAX]);
+    result[4] = big ? nan : (double)(long long)shS[SS_RHOREF] / SMP_FIXED;
+    result[5] = (double)shS[SS_NREF];
+    result[6] = (double)shS[SS_NAN];
+    result[7] = F[3];
+    result[8] = big ? nan : (double)(long long)shS[SS_MASS] / SMP_FIXED;
+    result[9] = (double)shS[SS_NFLUID];
   }
 }
 
@@ -2383,31 +2890,41 @@ static cudaError_t classify_t(wt_solver* s) {
   return cudaGetLastError();
 }
 
+// Counts, then writes, the cells k_boundary_list selects (which: 0 boundary list, 1 solid list)
+// into *list (grown to the count; *cap its capacity), *count the number of cells.
 template <class L>
-static cudaError_t boundary_list_t(wt_solver* s) {
+static cudaError_t cell_list_t(wt_solver* s, int which, uint32_t** list, size_t* cap, uint32_t* count) {
   cudaError_t e;
   const unsigned blocks = (unsigned)std::min<size_t>((s->n + 255) / 256, 148 * 16);
   if ((e = cudaMemsetAsync(s->bnd_count, 0, 4, s->stream)) != cudaSuccess) return e;
-  k_boundary_list<L><<<blocks, 256, 0, s->stream>>>(s->kp, s->cls, s->gs, s->bnd_count, nullptr, 0);
+  k_boundary_list<L><<<blocks, 256, 0, s->stream>>>(s->kp, s->cls, s->gs, s->bnd_count, nullptr, 0, which);
   s->launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = cudaMemcpyAsync(s->bnd_count_host, s->bnd_count, 4, cudaMemcpyDeviceToHost, s->stream)) != cudaSuccess)
     return e;
   if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return e;
-  const uint32_t count = *s->bnd_count_host;
-  if ((size_t)count > s->bnd_cap) {
-    if (s->bnd) cudaFree(s->bnd);
-    s->bnd = nullptr;
-    s->bnd_cap = 0;
-    if ((e = cudaMalloc((void**)&s->bnd, (size_t)count * 4)) != cudaSuccess) return e;
-    s->bnd_cap = count;
+  const uint32_t n = *s->bnd_count_host;
+  if ((size_t)n > *cap) {
+    if (*list) cudaFree(*list);
+    *list = nullptr;
+    *cap = 0;
+    if ((e = cudaMalloc((void**)list, (size_t)n * 4)) != cudaSuccess) return e;
+    *cap = n;
   }
-  s->nbnd = count;
-  if (count == 0) return cudaSuccess;
+  *count = n;
+  if (n == 0) return cudaSuccess;
   if ((e = cudaMemsetAsync(s->bnd_count, 0, 4, s->stream)) != cudaSuccess) return e;
-  k_boundary_list<L><<<blocks, 256, 0, s->stream>>>(s->kp, s->cls, s->gs, s->bnd_count, s->bnd, 1);
+  k_boundary_list<L><<<blocks, 256, 0, s->stream>>>(s->kp, s->cls, s->gs, s->bnd_count, *list, 1, which);
   s->launches++;
   return cudaGetLastError();
+}
+
+template <class L>
+static cudaError_t boundary_list_t(wt_solver* s) {
+  cudaError_t e = cell_list_t<L>(s, 0, &s->bnd, &s->bnd_cap, &s->nbnd);
+  if (e != cudaSuccess) return e;
+  // the solid cells, for the fused sampling pass
+  return cell_list_t<L>(s, 1, &s->solids, &s->solid_cap, &s->nsolid);
 }
 
 // Link records of the listed cells (vectorised f16 / f32 path only; see k_boundary_build).
@@ -2507,9 +3024,12 @@ cudaError_t closure_rows_reserve(wt_solver* s, bool* grown) {
 
 // the vectorised kernel indexes populations with 32-bit element offsets
 
+// One step, fin -> fout. With smp (the fused sampling step, see sample_step_ok) the face, wall-cell
+// and bulk kernels also run the sampling pass's per-cell work on what they store.
 template <class L, class S>
-static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
+static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout, const SampleOut* smp) {
   constexpr bool vec_ok = S::PREC == WT_PREC_F16 || S::PREC == WT_PREC_F32;
+  const SampleOut none{};
   if constexpr (vec_ok) {
     const int V = s->sc_param;
     const bool faces_ok = s->dims.ny >= 2 && (L::DIM == 2 || s->dims.nz >= 2);
@@ -2564,7 +3084,7 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
             if (s->nbnd > 0) {
               k_boundary_tab<L, S, FM_FEATURES><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
                   s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
-                  (uint32_t)s->btab_cap, s->sdf, xb + fc * CL_IN, nub + fc);
+                  (uint32_t)s->btab_cap, s->sdf, xb + fc * CL_IN, nub + fc, none);
               s->launches++;
               if ((e = cudaGetLastError()) != cudaSuccess) return e;
             }
@@ -2574,13 +3094,19 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
             k_face_lc<L, S, FM_NU><<<fgrid, dim3(fbx, fby), 0, bs>>>(
                 s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, s->sdf, xb, nub);
+          } else if (smp) {
+            k_face_v<L, S, true><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin,
+                                                                   (typename S::T*)fout, s->cls, s->gs, *smp);
           } else {
             k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin,
-                                                             (typename S::T*)fout, s->cls, s->gs);
+                                                             (typename S::T*)fout, s->cls, s->gs, none);
           }
+        } else if (smp) {
+          k_face_v<L, S, true><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin,
+                                                                 (typename S::T*)fout, s->cls, s->gs, *smp);
         } else {
           k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, bs>>>(s->kp, (const typename S::T*)fin, (typename S::T*)fout,
-                                                           s->cls, s->gs);
+                                                           s->cls, s->gs, none);
         }
         s->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -2591,12 +3117,16 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
             const size_t fc = closure_face_cells(s);
             k_boundary_tab<L, S, FM_NU><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
                 s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
-                (uint32_t)s->btab_cap, s->sdf, nullptr, s->lc_rows + s->lc_rows_cap * CL_IN + fc);
+                (uint32_t)s->btab_cap, s->sdf, nullptr, s->lc_rows + s->lc_rows_cap * CL_IN + fc, none);
           }
+        } else if (smp) {
+          k_boundary_tab<L, S, FM_SMAG, true><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
+              s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
+              (uint32_t)s->btab_cap, s->sdf, nullptr, nullptr, *smp);
         } else {
           k_boundary_tab<L, S><<<(s->nbnd + 63) / 64, 64, 0, bs>>>(
               s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
-              (uint32_t)s->btab_cap, s->sdf, nullptr, nullptr);
+              (uint32_t)s->btab_cap, s->sdf, nullptr, nullptr, none);
         }
         s->launches++;
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -2608,10 +3138,10 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
   do {                                                                                                             \
     if (s->kp.collision == 1u)                                                                                     \
       k_stream_collide_v<L, S, VV, MB, true><<<grid, block, 0, s->stream>>>(                                       \
-          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev);                            \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, none);                      \
     else                                                                                                           \
       k_stream_collide_v<L, S, VV, MB, false><<<grid, block, 0, s->stream>>>(                                      \
-          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev);                            \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, none);                      \
   } while (0)
       const int mb = s->sc_kernel;
       if constexpr (L::DIM == 3) {
@@ -2637,7 +3167,7 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
       }
       if constexpr (L::DIM == 3) {
         const size_t rp_smem = rows_smem_bytes<S>(s);
-        if (mb == WT_LAUNCH_ROW_PIPELINE && V == 2 && rp_smem > 0) {
+        if (mb == WT_LAUNCH_ROW_PIPELINE && V == 2 && rp_smem > 0 && !smp) {
           // row pipeline: `by` interior rows per block (default 4)
           const uint32_t nrows = (uint32_t)(s->dims.ny - 2) * (uint32_t)(s->dims.nz - 2);
           const uint32_t rows = s->sc_by > 0 ? (uint32_t)s->sc_by : 4u;
@@ -2654,7 +3184,23 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
           return cudaSuccess;
         }
       }
-      if (V == 2) {
+      if (smp) {
+        // the sampling step: the regularized collision keeps the bulk kernel's occupancy hint of 4
+        // (64 registers, no spills with the sampling state); BGK and four cells per thread run
+        // without a register cap (they would spill under it)
+        const bool bgk = s->kp.collision == 1u;
+        if (V == 2) {
+          if (bgk) k_stream_collide_v<L, S, 2, 0, true, true><<<grid, block, 0, s->stream>>>(
+                       s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, *smp);
+          else k_stream_collide_v<L, S, 2, 4, false, true><<<grid, block, 0, s->stream>>>(
+                   s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, *smp);
+        } else {
+          if (bgk) k_stream_collide_v<L, S, 4, 0, true, true><<<grid, block, 0, s->stream>>>(
+                       s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, *smp);
+          else k_stream_collide_v<L, S, 4, 0, false, true><<<grid, block, 0, s->stream>>>(
+                   s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, *smp);
+        }
+      } else if (V == 2) {
         if (mb == 2) WT_LAUNCH_V(2, 2);
         else if (mb == 3) WT_LAUNCH_V(2, 3);
         else if (mb == 4) WT_LAUNCH_V(2, 4);
@@ -2674,6 +3220,7 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout) {
       return cudaSuccess;
     }
   }
+  if (smp) return cudaErrorNotSupported;  // sample_step_ok excludes the scalar kernel
   const int bx = lbm_block_x(s);
   k_stream_collide<L, S><<<row_grid(s, bx), bx, 0, s->stream>>>(
       s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->flags, s->sdf, s->wheels);
@@ -2697,7 +3244,44 @@ static cudaError_t macro_t(wt_solver* s) {
 
 
 cudaError_t launch_init(wt_solver* s) { WT_DISPATCH(init_t, s); }
-cudaError_t launch_stream_collide(wt_solver* s, const void* fin, void* fout) { WT_DISPATCH(sc_t, s, fin, fout); }
+
+bool sample_step_ok(const wt_solver* s) {
+  if (!(s->prec == WT_PREC_F16 || s->prec == WT_PREC_F32) || s->closure_dev != nullptr || s->cls_dirty) return false;
+  const int V = s->sc_param;
+  const bool faces_ok = s->dims.ny >= 2 && (!s->is3d || s->dims.nz >= 2);
+  if (!((V == 2 || V == 4) && s->dims.nx % V == 0 && s->gs >= V && faces_ok && offsets32(s))) return false;
+  // the row pipeline has no sampling form (its steps stay unfused)
+  return !(s->is3d && s->sc_kernel == WT_LAUNCH_ROW_PIPELINE && V == 2 && rows_pipeline_smem(s) > 0);
+}
+
+template <class L, class S>
+static cudaError_t sample_step_t(wt_solver* s, const void* fin, void* fout) {
+  if constexpr (S::PREC == WT_PREC_F64) {
+    return cudaErrorNotSupported;
+  } else {
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(s->smp_sets, 0, SMP_SETS * SMP_SET_U64 * sizeof(unsigned long long), s->stream)) !=
+        cudaSuccess)
+      return e;
+    const SampleOut O{s->vel, s->meanA, s->meanB, s->smp_sets};
+    if ((e = sc_t<L, S>(s, fin, fout, &O)) != cudaSuccess) return e;
+    // after the whole step: the wall force of the listed cells and the solid cells, on what it stored
+    const uint32_t items = s->nbnd + s->nsolid;
+    const int blocks = (int)std::max<size_t>(1, std::min<size_t>(((size_t)items + MACRO_THREADS - 1) / MACRO_THREADS,
+                                                                  (size_t)s->partial_blocks));
+    k_sample_post<L, S><<<blocks, MACRO_THREADS, 0, s->stream>>>(
+        s->kp, (const typename S::T*)fout, s->flags, s->sdf, s->cls, s->wheels, s->bnd, s->nbnd, s->solids,
+        s->nsolid, s->vel, s->meanA, s->meanB, s->partials, s->smp_sets, s->result_dev);
+    s->launches++;
+    return cudaGetLastError();
+  }
+}
+
+cudaError_t launch_sample_step(wt_solver* s, const void* fin, void* fout) { WT_DISPATCH(sample_step_t, s, fin, fout); }
+cudaError_t launch_stream_collide(wt_solver* s, const void* fin, void* fout) {
+  const SampleOut* none = nullptr;
+  WT_DISPATCH(sc_t, s, fin, fout, none);
+}
 cudaError_t launch_macro(wt_solver* s) { WT_DISPATCH(macro_t, s); }
 
 bool batch_fusable(const wt_solver* s) {
@@ -2718,13 +3302,13 @@ static cudaError_t aux_t(wt_solver* s, const void* fin, void* fout, cudaStream_t
     const int fby = 256 / fbx;
     const dim3 fgrid((runs2 + fbx - 1) / fbx, (fr + fby - 1) / fby, 1);
     k_face_v<L, S><<<fgrid, dim3(fbx, fby), 0, s->aux>>>(s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls,
-                                                         s->gs);
+                                                         s->gs, SampleOut{});
     s->launches++;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (s->nbnd > 0) {
       k_boundary_tab<L, S><<<(s->nbnd + 63) / 64, 64, 0, s->aux>>>(
           s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->bcell, s->brec, s->bgam, s->nbnd,
-          (uint32_t)s->btab_cap, s->sdf, nullptr, nullptr);
+          (uint32_t)s->btab_cap, s->sdf, nullptr, nullptr, SampleOut{});
       s->launches++;
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
@@ -2788,8 +3372,19 @@ double* g_scratch_ptr[NOALLOC_MAX_DEVICES] = {};
 
 // Device address of g_sample_scratch on `dev`, which must be the current device. Looked up on the
 // first call for that device (this may load the module's device code) and cached.
+// A cached address is checked against the current context first: after cudaDeviceReset (a new
+// primary context, the module loaded again) the old address no longer names device memory of
+// `dev`, and the symbol is looked up again.
 cudaError_t scratch_address(int dev, double** out) {
   std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (g_scratch_ptr[dev]) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, g_scratch_ptr[dev]) != cudaSuccess || a.type != cudaMemoryTypeDevice ||
+        a.device != dev) {
+      cudaGetLastError();
+      g_scratch_ptr[dev] = nullptr;
+    }
+  }
   if (!g_scratch_ptr[dev]) {
     double* ptr = nullptr;
     const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_sample_scratch);

@@ -81,6 +81,11 @@ class Solver:
         return int(self._lib.wt_launch_count(self._h))
 
     @property
+    def fused_samples(self) -> int:
+        """stepAndSample calls whose last step ran the sampling pass fused (wt_fused_sample_count)."""
+        return int(self._lib.wt_fused_sample_count(self._h))
+
+    @property
     def step_count(self) -> int:
         return int(self._lib.wt_step_count(self._h))
 
