@@ -277,6 +277,13 @@ int wt_probes(wt_solver* s, const float* pos4, int32_t count, float* out8);
  * It needs nx % 8 == 0 (f16) or nx % 4 == 0 (f32) and 3 x 19 x nx populations within 48 KB of
  * shared memory; elsewhere the vectorised kernel runs. */
 #define WT_LAUNCH_ROW_PIPELINE 8
+/* kernel = WT_LAUNCH_PERSISTENT (param 2, bx 0, by 0): every wt_step call of two or more steps runs
+ * as one cooperative launch of a persistent kernel that takes all its steps, the tiles of each step
+ * dealt to the resident blocks and a grid-wide barrier between steps (the same arithmetic as the
+ * per-step kernels: bit-identical results). For small grids, where launching a step's kernels costs
+ * as much as running them. Needs f16 / f32 storage, nx even and the reference's closure; elsewhere
+ * the vectorised kernel runs. */
+#define WT_LAUNCH_PERSISTENT 9
 int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32_t by);
 int wt_get_launch(const wt_solver* s, int32_t* out4);
 /* The project's launch tuner: times every applicable launch candidate on this handle's
@@ -308,10 +315,16 @@ int32_t wt_batch_size(const wt_batch* b);
 int wt_batch_step(wt_batch* b, int32_t steps);
 /* the sampling pass of every member (queued together, then read back): out has count entries */
 int wt_batch_sample(wt_batch* b, wt_stats* out);
-/* on != 0: when every member is D3Q19 with the same f16 / f32 storage and collision, no learned
+/* on = 1: when every member is D3Q19 with the same f16 / f32 storage and collision, no learned
  * closure and the vectorised launch, the bulk rows of all members step in one launch of a batch
  * kernel over a table of per-tunnel descriptors (face rows and wall cells stay per member).
- * Default off: on a B200 the members' own kernels under one graph measured faster. */
+ * on = WT_BATCH_PERSISTENT: when every member has the same lattice, f16 / f32 storage and collision,
+ * no learned closure and an even nx (at most 48 members), each wt_batch_step call of two or more
+ * steps is one cooperative launch of the persistent kernel over all members: per step the bulk
+ * tiles, face-row tiles and wall cells of every member are dealt to the resident blocks, with a
+ * grid-wide barrier between steps. Members stay bit-identical to the same handles stepped alone.
+ * on = 0 (default): the members' own kernels under one graph. */
+#define WT_BATCH_PERSISTENT 2
 int wt_batch_set_fused(wt_batch* b, int32_t on);
 
 /* ---- learned LES closure (extension; no counterpart in the reference) -----------------------

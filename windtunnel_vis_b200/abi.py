@@ -14,6 +14,9 @@ WT_E_OOM = -3
 WT_E_STATE = -4
 WT_E_UNSUPPORTED = -5
 WT_E_NO_DEVICE = -6
+WT_LAUNCH_ROW_PIPELINE = 8
+WT_LAUNCH_PERSISTENT = 9
+WT_BATCH_PERSISTENT = 2
 
 GROUND = {"freeslip": 0, "noslip": 1, "moving": 2}
 SIDES = {"freeslip": 0, "periodic": 1}

@@ -3,10 +3,13 @@
     python -m windtunnel_vis_b200.build [--force]
 
 Each .cu in csrc/ is compiled by nvcc to an object in _build/, then linked into
-windtunnel_vis_b200/libwt.so with the static CUDA runtime. The voxelizer and tracer units are
-compiled with -fmad=false (no contraction) so their f32 results are bit-identical to the CPU
-restatement, as is the derived-field unit; the LBM unit keeps FMA contraction (it is bandwidth-bound and checked within
-stated tolerances).
+windtunnel_vis_b200/libwt.so with the static CUDA runtime. The voxelizer, tracer and
+derived-field units are compiled with -fmad=false (no contraction) so their f32 results are
+bit-identical to the CPU restatement. So is the LBM unit, for another reason: without contraction
+every rounding in it is the one written in the source (fused multiply-adds only where the code
+asks for them), so a cell's update gives the same bits in every kernel that inlines it (the
+per-step kernels, the batched kernels and the persistent multi-step kernel), whatever the
+compiler's register budget or code placement there.
 """
 import os
 import shutil
@@ -24,7 +27,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompi
           "-Xptxas", "-warn-spills", "-I", os.path.join(ROOT, "include")]
 UNITS = {
     "wt_api.cu": [],
-    "wt_lbm.cu": [],
+    "wt_lbm.cu": ["-fmad=false"],
     "wt_voxel.cu": ["-fmad=false"],
     "wt_tracer.cu": ["-fmad=false"],
     "wt_fields.cu": ["-fmad=false"],
@@ -47,7 +50,7 @@ def _mtime(p):
 def build(force: bool = False, verbose: bool = False, extra=None) -> str:
     os.makedirs(OBJ, exist_ok=True)
     hdr_t = max(_mtime(os.path.join(CSRC, h)) for h in HEADERS)
-    hdr_t = max(hdr_t, _mtime(os.path.join(ROOT, "include", "wt.h")))
+    hdr_t = max(hdr_t, _mtime(os.path.join(ROOT, "include", "wt.h")), _mtime(os.path.abspath(__file__)))
     objs = []
     jobs = []
     for unit, flags in UNITS.items():

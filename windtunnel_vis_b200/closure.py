@@ -332,6 +332,50 @@ def _mean_se(tt, cd, start, horizon):
     return (ws["mean"], ws["se"]) if ws else (math.nan, math.nan)
 
 
+def a_posteriori(make, model, body, fine_dims, u=0.05, re=1000.0, seed=1, eval_steps=16000, chunk=100, trainer=None,
+                 sample_seed=777):
+    """One held-out body: its fine run's mean C_D over the second half of `eval_steps` steps against
+    coarse runs (half the resolution, the same physical time: eval_steps / 2 steps) with no sub-grid
+    model (Cs = 0), plain Smagorinsky and the network `model`; each with its wall time and error
+    against the fine run. With `trainer`, the fine run's filtered samples are added to it and the
+    a-priori errors of the network and of Smagorinsky on them are reported."""
+    fine, coarse, pf, f_front = _fine_coarse(make, body, fine_dims, u=u, re=re, seed=seed)
+    t0 = time.perf_counter()
+    tt, cd, unst = _cd_series(fine, eval_steps, chunk, u, f_front)
+    f_sec = time.perf_counter() - t0
+    f_mean, f_se = _mean_se(tt, cd, eval_steps // 2, eval_steps)
+    n0 = trainer.count if trainer is not None else 0
+    if trainer is not None and not unst:
+        trainer.add_samples(fine, coarse, keep=0.25, seed=sample_seed)
+    fine.destroy()
+    coarse.destroy()
+    case = {"body": body, "fine": {"cd": f_mean, "cd_se": f_se, "seconds": f_sec, "unstable": unst}}
+    cdims = tuple(d // 2 for d in fine_dims)
+    # coarse runs: no sub-grid model at all (cs = 0), plain Smagorinsky, the network
+    for name, cl in (("no_model", None), ("smagorinsky", None), ("learned", model)):
+        cf, c_front, cs_ = body_fields(cdims, body)
+        pc = dict(pf, nu=pf["nu"] / 2.0, cs=0.0 if name == "no_model" else pf["cs"])
+        c = make(cdims, pc)
+        c.upload_flags(cf)
+        c.upload_sdf(cs_)
+        if cl is not None:
+            c.set_closure(cl)
+        t0 = time.perf_counter()
+        tt, cd, unst_c = _cd_series(c, eval_steps // 2, chunk // 2, u, c_front)
+        sec = time.perf_counter() - t0
+        c.destroy()
+        mean, se = _mean_se(tt, cd, eval_steps // 4, eval_steps // 2)
+        case[name] = {"cd": mean, "cd_se": se, "seconds": sec, "unstable": unst_c,
+                      "cd_err_vs_fine": (mean - f_mean) / f_mean if f_mean == f_mean and f_mean else math.nan,
+                      "speedup_vs_fine": f_sec / sec if sec > 0 else math.nan}
+    if trainer is not None and trainer.count > n0:
+        x, y = trainer.read_samples(n0, trainer.count - n0)
+        trainer.set_model(model)
+        case["a_priori"] = {"learned": a_priori_metrics(trainer.infer(x), y),
+                            "smagorinsky": a_priori_metrics(smagorinsky_nu(x), y), "samples": int(y.size)}
+    return case
+
+
 def study(make=None, fine_dims=(512, 256, 256), train_bodies=8, eval_bodies=2, seed=1, re=1000.0, u=0.05,
           warm=6000, snapshots=2, every=1000, samples=1 << 24, keep=0.4, train_steps=3000, batch=16384, lr=2e-3,
           eval_steps=16000, chunk=100, radius=1, log=print):
@@ -340,8 +384,10 @@ def study(make=None, fine_dims=(512, 256, 256), train_bodies=8, eval_bodies=2, s
     each (cells kept with probability `keep`, up to `samples`). Training: Adam on the GPU. Evaluation
     on `eval_bodies` held-out bodies (other seeds): the fine run's mean C_D over its second half
     (eval_steps fine steps) against coarse runs over the same physical time (eval_steps / 2 coarse
-    steps) with plain Smagorinsky and with the network, wall times of all three, and the a-priori
-    error of the network and of Smagorinsky against the held-out targets."""
+    steps) with no sub-grid model (Cs = 0), with plain Smagorinsky and with the network, wall times
+    of all of them, and the a-priori error of the network and of Smagorinsky against the held-out
+    targets. The no-model run separates the sub-grid model's share of the coarse error from the
+    share of the wall resolution, which no eddy-viscosity closure changes."""
     from .solver import solver_factory
 
     make = make or solver_factory
@@ -379,42 +425,12 @@ def study(make=None, fine_dims=(512, 256, 256), train_bodies=8, eval_bodies=2, s
     ev.set_projection_radius(radius)
     cases = []
     for b, body in enumerate(seeded_bodies(eval_bodies, seed=seed + 7919)):
-        fine, coarse, pf, f_front = _fine_coarse(make, body, fine_dims, u=u, re=re, seed=seed + 100 + b)
-        t0 = time.perf_counter()
-        tt, cd, unst = _cd_series(fine, eval_steps, chunk, u, f_front)
-        f_sec = time.perf_counter() - t0
-        f_mean, f_se = _mean_se(tt, cd, eval_steps // 2, eval_steps)
-        n0 = ev.count
-        if not unst:
-            ev.add_samples(fine, coarse, keep=0.25, seed=777 + b)
-        fine.destroy()
-        coarse.destroy()
-        case = {"body": body, "fine": {"cd": f_mean, "cd_se": f_se, "seconds": f_sec, "unstable": unst}}
-        cdims = tuple(d // 2 for d in fine_dims)
-        for name, cl in (("smagorinsky", None), ("learned", model)):
-            cf, c_front, cs_ = body_fields(cdims, body)
-            pc = dict(pf, nu=pf["nu"] / 2.0)
-            s = make(cdims, pc)
-            s.upload_flags(cf)
-            s.upload_sdf(cs_)
-            if cl is not None:
-                s.set_closure(cl)
-            t0 = time.perf_counter()
-            tt, cd, unst_c = _cd_series(s, eval_steps // 2, chunk // 2, u, c_front)
-            sec = time.perf_counter() - t0
-            s.destroy()
-            mean, se = _mean_se(tt, cd, eval_steps // 4, eval_steps // 2)
-            case[name] = {"cd": mean, "cd_se": se, "seconds": sec, "unstable": unst_c,
-                          "cd_err_vs_fine": (mean - f_mean) / f_mean if f_mean == f_mean and f_mean else math.nan,
-                          "speedup_vs_fine": f_sec / sec if sec > 0 else math.nan}
-        if ev.count > n0:
-            x, y = ev.read_samples(n0, ev.count - n0)
-            ev.set_model(model)
-            case["a_priori"] = {"learned": a_priori_metrics(ev.infer(x), y),
-                                "smagorinsky": a_priori_metrics(smagorinsky_nu(x), y), "samples": int(y.size)}
+        case = a_posteriori(make, model, body, fine_dims, u=u, re=re, seed=seed + 100 + b, eval_steps=eval_steps,
+                            chunk=chunk, trainer=ev, sample_seed=777 + b)
         cases.append(case)
-        log(f"eval body {b}: fine C_D {f_mean:.4f} ({f_sec:.1f} s), smagorinsky {case['smagorinsky']['cd']:.4f}, "
-            f"learned {case['learned']['cd']:.4f} ({case['learned']['seconds']:.1f} s)")
+        log(f"eval body {b}: fine C_D {case['fine']['cd']:.4f} ({case['fine']['seconds']:.1f} s), no model "
+            f"{case['no_model']['cd']:.4f}, smagorinsky {case['smagorinsky']['cd']:.4f}, learned "
+            f"{case['learned']['cd']:.4f} ({case['learned']['seconds']:.1f} s)")
     ev.destroy()
     out["cases"] = cases
     out["model"] = {k: np.asarray(v).tolist() for k, v in model.items()}

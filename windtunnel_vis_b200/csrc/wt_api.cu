@@ -73,7 +73,7 @@ void free_all(wt_solver* s) {
                   s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count,
                   s->bcell, s->brec, s->bgam, s->vox_pos, s->vox_idx, s->vox_info,
                   s->dvort, s->dstat, s->dmean, s->exp_buf, s->probe_buf, s->closure_dev, s->stage,
-                  s->diff_dev, s->lc_rows, s->solids, s->smp_sets};
+                  s->diff_dev, s->lc_rows, s->solids, s->smp_sets, s->ps_bar};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->result_host) cudaFreeHost(s->result_host);
@@ -380,7 +380,8 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
             alloc((void**)&s->partials, (size_t)s->partial_blocks * RESULT_BYTES, "partials") &&
             alloc((void**)&s->result_dev, RESULT_BYTES, "result") && alloc((void**)&s->err_dev, 4, "error word") &&
             alloc((void**)&s->bnd_count, 4, "boundary counter") &&
-            alloc((void**)&s->smp_sets, wt::SMP_SETS_BYTES, "sampling accumulators");
+            alloc((void**)&s->smp_sets, wt::SMP_SETS_BYTES, "sampling accumulators") &&
+            alloc((void**)&s->ps_bar, 2 * sizeof(unsigned), "barrier words");
   if (ok && (cudaMallocHost((void**)&s->result_host, RESULT_BYTES) != cudaSuccess ||
              cudaMallocHost((void**)&s->err_host, 4) != cudaSuccess ||
              cudaMallocHost((void**)&s->bnd_count_host, 4) != cudaSuccess)) {
@@ -665,6 +666,14 @@ int wt_step(wt_solver* s, int32_t steps) {
     if (e != cudaSuccess) return cuda_fail(s, e, "stream_collide");
     s->parity ^= 1;
   }
+  if (steps - k >= 2 && s->sc_kernel == WT_LAUNCH_PERSISTENT && wt::persistent_ok(s)) {
+    // every remaining step in one cooperative launch of the persistent kernel
+    wt_solver* one[1] = {s};
+    WT_CUDA(s, wt::launch_persistent(one, 1, steps - k, s->ps_bar, s->err_dev, s->stream), "persistent steps");
+    s->launches++;
+    if ((steps - k) & 1) s->parity ^= 1;
+    k = steps;
+  }
   if (steps - k >= 2 * WT_LONG_PAIRS) {
     // runs of WT_LONG_PAIRS step pairs replay one long graph (fewer graph launches)
     if (!s->long_graph[s->parity]) {
@@ -725,7 +734,8 @@ int wt_step_and_sample(wt_solver* s, int32_t steps, wt_stats* out) {
   // The last step runs the sampling pass's per-cell work on what it stores (no second read of the
   // populations), then the wall force and the solid cells, then the final reduction. With solid
   // cells in place in both buffers, the chunk's last WT_SAMPLE_TAIL steps replay one graph.
-  const bool tail = steps >= WT_SAMPLE_TAIL;
+  // (the persistent launch takes all steps but the last in one launch instead)
+  const bool tail = steps >= WT_SAMPLE_TAIL && s->sc_kernel != WT_LAUNCH_PERSISTENT;
   rc = wt_step(s, steps - (tail ? WT_SAMPLE_TAIL : 1));
   if (rc) return rc;
   if (tail && s->solid_ok[0] && s->solid_ok[1]) {
@@ -984,6 +994,9 @@ int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32
   if (kernel == WT_LAUNCH_ROW_PIPELINE) {
     if (param != 2 || bx != 0 || by < 0 || by > 16)
       return fail(s, WT_E_INVALID, "wt_set_launch: the row pipeline takes param 2, bx 0 and 0..16 rows per block");
+  } else if (kernel == WT_LAUNCH_PERSISTENT) {
+    if (param != 2 || bx != 0 || by != 0)
+      return fail(s, WT_E_INVALID, "wt_set_launch: the persistent kernel takes param 2, bx 0, by 0");
   } else if (!(kernel == 0 || (kernel >= 2 && kernel <= 4))) {
     return fail(s, WT_E_INVALID, "wt_set_launch: occupancy hint must be 0 or 2..4 CTAs per SM");
   } else if (!(param == 1 || param == 2 || param == 4) || bx < 0 || by < 0 || bx * by > 256 || (bx % 32) != 0 ||
@@ -1111,7 +1124,9 @@ struct wt_batch {
   std::vector<int> parities;        // member parities the graph was captured at
   std::vector<int64_t> per_replay;  // kernel launches of each member inside one replay
   std::vector<int64_t> long_per_replay;
-  bool fused = false;  // wt_batch_set_fused
+  bool fused = false;  // wt_batch_set_fused(b, 1)
+  bool persistent = false;  // wt_batch_set_fused(b, WT_BATCH_PERSISTENT)
+  unsigned* ps_bar = nullptr;  // the persistent kernel's barrier words
   std::string err;
 };
 
@@ -1143,6 +1158,17 @@ bool batch_fused(const wt_batch* b) {
   if (!b->fused || b->m.size() > (size_t)wt::BATCH_MAX_FUSED) return false;
   for (const wt_solver* s : b->m)
     if (!wt::batch_fusable(s) || s->prec != b->m[0]->prec || s->kp.collision != b->m[0]->kp.collision) return false;
+  return true;
+}
+
+// Whether the batch's steps run in the persistent kernel: same lattice, storage and collision for
+// every member, each able to take it, and the table holds them all.
+bool batch_persistent(const wt_batch* b) {
+  if (!b->persistent || b->m.size() > 48) return false;
+  const wt_solver* s0 = b->m[0];
+  for (const wt_solver* s : b->m)
+    if (!wt::persistent_ok(s) || s->is3d != s0->is3d || s->prec != s0->prec || s->kp.collision != s0->kp.collision)
+      return false;
   return true;
 }
 
@@ -1283,7 +1309,8 @@ int wt_batch_create(wt_solver* const* members, int32_t count, wt_batch** out) {
   b->ev_done.assign(count, nullptr);
   DeviceGuard g(b->device);
   bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+            cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
+            cudaMalloc((void**)&b->ps_bar, 2 * sizeof(unsigned)) == cudaSuccess;
   for (int32_t k = 0; ok && k < count; k++)
     ok = cudaEventCreateWithFlags(&b->ev_done[k], cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {
@@ -1300,6 +1327,7 @@ void wt_batch_destroy(wt_batch* b) {
   DeviceGuard g(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   batch_drop_graph(b);
+  if (b->ps_bar) cudaFree(b->ps_bar);
   for (cudaEvent_t e : b->ev_done)
     if (e) cudaEventDestroy(e);
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
@@ -1316,7 +1344,8 @@ int wt_batch_set_fused(wt_batch* b, int32_t on) {
   DeviceGuard g(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   batch_drop_graph(b);
-  b->fused = on != 0;
+  b->fused = on == 1;
+  b->persistent = on == WT_BATCH_PERSISTENT;
   return WT_OK;
 }
 
@@ -1339,6 +1368,21 @@ int wt_batch_step(wt_batch* b, int32_t steps) {
   for (; k < steps && !all_solid_ok(); k++) {
     int rc = batch_single_step(b);
     if (rc) return rc;
+  }
+  if (steps - k >= 2 && batch_persistent(b)) {
+    // every remaining step of every member in one cooperative launch of the persistent kernel
+    int rc = batch_wait_members(b);
+    if (rc) return rc;
+    cudaError_t e = wt::launch_persistent(b->m.data(), (int)b->m.size(), steps - k, b->ps_bar, b->m[0]->err_dev,
+                                          b->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(b->ev_fork, b->stream);
+    for (wt_solver* s : b->m)
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(s->stream, b->ev_fork, 0);
+    if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch persistent steps: ") + cudaGetErrorString(e));
+    b->m[0]->launches++;
+    if ((steps - k) & 1)
+      for (wt_solver* s : b->m) s->parity ^= 1;
+    k = steps;
   }
   if (steps - k >= 2) {
     int rc = batch_wait_members(b);

@@ -76,6 +76,7 @@ struct wt_solver {
   // accumulator sets of the fused sampling pass (zeroed before each sampling step)
   unsigned long long* smp_sets = nullptr;
   int64_t fused_samples = 0;  // stepAndSample calls that ran the fused sampling step
+  unsigned* ps_bar = nullptr;  // grid barrier words of the persistent kernel (WT_LAUNCH_PERSISTENT)
   uint32_t* bnd_count = nullptr;  // device counter used while building the list
   uint32_t* bnd_count_host = nullptr;  // pinned
   // link records of the listed cells (k_boundary_build), applied every step by k_boundary_tab
@@ -189,6 +190,12 @@ struct BatchTable {
 };
 // whether a handle's step can join the batch kernel: D3Q19, f16 / f32, vectorised path, no closure
 bool batch_fusable(const wt_solver* s);
+// The persistent kernel: `steps` updates of the tunnels ms[0 .. count) (same lattice, storage and
+// collision; each persistent_ok) in one cooperative launch on `st`; bar = two device words (zeroed
+// here), err = the device error word for a barrier timeout (bit 16). The members' parities are
+// not changed here.
+bool persistent_ok(const wt_solver* s);
+cudaError_t launch_persistent(wt_solver* const* ms, int count, int steps, unsigned* bar, int* err, cudaStream_t st);
 // the face-row and wall-cell kernels of one step of `s` on its auxiliary stream, forked from
 // `origin`; s->ev_join is recorded at their end (the caller joins it into `origin`)
 cudaError_t launch_aux_kernels(wt_solver* s, const void* fin, void* fout, cudaStream_t origin);

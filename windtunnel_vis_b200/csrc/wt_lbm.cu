@@ -15,6 +15,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 #include <string>
 #include <type_traits>
@@ -1084,19 +1085,31 @@ __device__ __forceinline__ void pair_sample(const wt_kparams& P, uint32_t idx0, 
   *reinterpret_cast<uint4*>(O.vel + idx0) = make_uint4(ta.x, ta.y, tb.x, tb.y);
 }
 
+// Population loads. The step kernels read their input buffer through the read-only cache (ld.nc):
+// nothing writes it while they run. COH selects loads cached in L2 only (ld.cg) instead, for the
+// persistent kernel, whose blocks read in one step what other SMs wrote in the step before.
+template <bool COH, class T>
+__device__ __forceinline__ T ldp(const T* p) {
+  if constexpr (COH) return __ldcg(p);
+  else return __ldg(p);
+}
+
 template <class S> struct PairIO;
 template <> struct PairIO<StF16> {
   typedef uint32_t pair_t;
   typedef unsigned short one_t;
+  template <bool COH = false>
   __device__ __forceinline__ static pair_t ld(const __half* __restrict__ p, uint32_t o) {
-    return __ldg(reinterpret_cast<const unsigned int*>(p + o));
+    return ldp<COH>(reinterpret_cast<const unsigned int*>(p + o));
   }
+  template <bool COH = false>
   __device__ __forceinline__ static one_t ld1(const __half* __restrict__ p, uint32_t o) {
-    return __ldg(reinterpret_cast<const unsigned short*>(p + o));
+    return ldp<COH>(reinterpret_cast<const unsigned short*>(p + o));
   }
   // elements (o .. o + 3), o a multiple of 4: one 8-byte load
+  template <bool COH = false>
   __device__ __forceinline__ static void ld4(const __half* __restrict__ p, uint32_t o, pair_t& a, pair_t& b) {
-    const uint2 q = __ldg(reinterpret_cast<const uint2*>(p + o));
+    const uint2 q = ldp<COH>(reinterpret_cast<const uint2*>(p + o));
     a = q.x;
     b = q.y;
   }
@@ -1118,13 +1131,16 @@ template <> struct PairIO<StF16> {
 template <> struct PairIO<StF32> {
   typedef float2 pair_t;
   typedef float one_t;
+  template <bool COH = false>
   __device__ __forceinline__ static pair_t ld(const float* __restrict__ p, uint32_t o) {
-    return __ldg(reinterpret_cast<const float2*>(p + o));
+    return ldp<COH>(reinterpret_cast<const float2*>(p + o));
   }
-  __device__ __forceinline__ static one_t ld1(const float* __restrict__ p, uint32_t o) { return __ldg(p + o); }
+  template <bool COH = false>
+  __device__ __forceinline__ static one_t ld1(const float* __restrict__ p, uint32_t o) { return ldp<COH>(p + o); }
   // elements (o .. o + 3), o a multiple of 4: one 16-byte load
+  template <bool COH = false>
   __device__ __forceinline__ static void ld4(const float* __restrict__ p, uint32_t o, pair_t& a, pair_t& b) {
-    const float4 q = __ldg(reinterpret_cast<const float4*>(p + o));
+    const float4 q = ldp<COH>(reinterpret_cast<const float4*>(p + o));
     a = make_float2(q.x, q.y);
     b = make_float2(q.z, q.w);
   }
@@ -1144,7 +1160,7 @@ template <int MINB> struct Bounds { static constexpr int v = MINB; };
 // The V cells x0 .. x0 + V - 1 of row (iy, iz) (bulk rows only); shared by the single-tunnel
 // kernel and the batch kernel.
 // With SMP the cells also run the per-cell part of the sampling pass on what they store.
-template <class L, class S, int V, bool BGK, bool SMP = false>
+template <class L, class S, int V, bool BGK, bool SMP = false, bool COH = false>
 __device__ __forceinline__ void bulk_cells(const wt_kparams& P, const typename S::T* __restrict__ fin,
                                            typename S::T* __restrict__ fout, const uint8_t* __restrict__ cls,
                                            int gs, int x0, int iy, int iz, const SampleOut* O = nullptr,
@@ -1182,13 +1198,13 @@ __device__ __forceinline__ void bulk_cells(const wt_kparams& P, const typename S
     const ptrdiff_t off = (ptrdiff_t)i * N - (ptrdiff_t)cy * sy - (ptrdiff_t)cz * sz;
     const typename S::T* ps = fb + off;
     if constexpr (G == 2) {
-      IO::ld4(ps, 0u, rp[0][i], rp[1][i]);  // 8- or 16-byte aligned when nx % 4 == 0
+      IO::template ld4<COH>(ps, 0u, rp[0][i], rp[1][i]);  // 8- or 16-byte aligned when nx % 4 == 0
     } else {
 #pragma unroll
-      for (int g = 0; g < G; g++) rp[g][i] = IO::ld(ps, 2 * g);
+      for (int g = 0; g < G; g++) rp[g][i] = IO::template ld<COH>(ps, 2 * g);
     }
-    if constexpr (cx > 0) r1[i] = IO::ld1(x0 > 0 ? ps - 1 : ps, 0u);            // x - 1
-    if constexpr (cx < 0) r1[i] = IO::ld1(ps + (last ? V - 1 : V), 0u);         // x + 1, outlet clamp
+    if constexpr (cx > 0) r1[i] = IO::template ld1<COH>(x0 > 0 ? ps - 1 : ps, 0u);     // x - 1
+    if constexpr (cx < 0) r1[i] = IO::template ld1<COH>(ps + (last ? V - 1 : V), 0u);  // x + 1, outlet clamp
   });
   // phase 2, one pair of cells at a time (the other pairs stay packed in their raw registers):
   // convert and shift into the pulled populations, collide, store
@@ -1476,18 +1492,16 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_batch_bulk(const _
 // (row r * nx + x of `xb`) and stores nothing; MODE 2 collides with the eddy viscosities nub[row].
 enum : int { FM_SMAG = 0, FM_FEATURES = 1, FM_NU = 2 };
 
-template <class L, class S, int MODE, bool SMP = false>
+template <class L, class S, int MODE, bool SMP = false, bool COH = false>
 __device__ __forceinline__ void face_rows(const wt_kparams& P, const typename S::T* __restrict__ fin,
                                           typename S::T* __restrict__ fout, const uint8_t* __restrict__ cls, int gs,
                                           const uint32_t* __restrict__ sdf, float* __restrict__ xb,
-                                          const float* __restrict__ nub, const SampleOut* O = nullptr,
-                                          SampleSums* acc = nullptr) {
+                                          const float* __restrict__ nub, const SampleOut* O, SampleSums* acc,
+                                          int x0, int r) {
   typedef PairIO<S> IO;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
   const int NX = P.nx, NY = P.ny, NZ = P.nz;
-  const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 2;
-  const int r = blockIdx.y * blockDim.y + threadIdx.y;
   int iy, iz;
   if constexpr (!D3) {
     if (r >= 2) return;
@@ -1564,9 +1578,9 @@ __device__ __forceinline__ void face_rows(const wt_kparams& P, const typename S:
     }
     bnc[i] = bounce;
     const uint32_t src = (uint32_t)k * N + sy * (uint32_t)ry + sz * (uint32_t)rz + (uint32_t)x0;
-    rp[i] = IO::ld(fin, src);
-    if constexpr (cx > 0) r1[i] = IO::ld1(fin, (x0 > 0 && !bounce) ? src - 1u : src);
-    if constexpr (cx < 0) r1[i] = IO::ld1(fin, (last || bounce) ? src + 1u : src + 2u);
+    rp[i] = IO::template ld<COH>(fin, src);
+    if constexpr (cx > 0) r1[i] = IO::template ld1<COH>(fin, (x0 > 0 && !bounce) ? src - 1u : src);
+    if constexpr (cx < 0) r1[i] = IO::template ld1<COH>(fin, (last || bounce) ? src + 1u : src + 2u);
   });
   float2 h[Q];
   static_for<Q>([&](auto I) {
@@ -1629,7 +1643,8 @@ __global__ void __launch_bounds__(256) k_face_v(const __grid_constant__ wt_kpara
                                                 const uint8_t* __restrict__ cls, int gs,
                                                 const __grid_constant__ SampleOut O) {
   SampleSums acc;
-  face_rows<L, S, FM_SMAG, SMP>(P, fin, fout, cls, gs, nullptr, nullptr, nullptr, &O, &acc);
+  face_rows<L, S, FM_SMAG, SMP>(P, fin, fout, cls, gs, nullptr, nullptr, nullptr, &O, &acc,
+                                (blockIdx.x * blockDim.x + threadIdx.x) * 2, blockIdx.y * blockDim.y + threadIdx.y);
   if constexpr (SMP) smp_flush(acc, O.sets, global_warp_id());
 }
 
@@ -1642,7 +1657,8 @@ __global__ void __launch_bounds__(256) k_face_lc(const __grid_constant__ wt_kpar
                                                  const uint8_t* __restrict__ cls, int gs,
                                                  const uint32_t* __restrict__ sdf, float* __restrict__ xb,
                                                  const float* __restrict__ nub) {
-  face_rows<L, S, MODE>(P, fin, fout, cls, gs, sdf, xb, nub);
+  face_rows<L, S, MODE>(P, fin, fout, cls, gs, sdf, xb, nub, nullptr, nullptr,
+                        (blockIdx.x * blockDim.x + threadIdx.x) * 2, blockIdx.y * blockDim.y + threadIdx.y);
 }
 
 // ---- bulk kernel with the learned closure: the network on tcgen05 tensor cores -----------------
@@ -2112,7 +2128,7 @@ __global__ void __launch_bounds__(128) k_boundary_build(const __grid_constant__ 
 // at once (coalesced across the warp), then every gather, then the collision and the stores.
 // MODE as for the face rows: FM_SMAG, FM_FEATURES (the listed cell's features into row k of xb,
 // nothing stored) or FM_NU (collision with the eddy viscosity nub[k]).
-template <class L, class S, int MODE = FM_SMAG, bool SMP = false>
+template <class L, class S, int MODE = FM_SMAG, bool SMP = false, bool COH = false>
 __device__ __forceinline__ void boundary_cell(const wt_kparams& P, const typename S::T* __restrict__ fin,
                                               typename S::T* __restrict__ fout, const uint2* __restrict__ bcell,
                                               const uint4* __restrict__ rec, const float* __restrict__ gam,
@@ -2131,8 +2147,8 @@ __device__ __forceinline__ void boundary_cell(const wt_kparams& P, const typenam
   typename S::T x1[Q], x2[Q];
   static_for<Q>([&](auto I) {
     constexpr int i = I;
-    x1[i] = __ldg(fin + r[i].x);
-    x2[i] = __ldg(fin + r[i].y);
+    x1[i] = ldp<COH>(fin + r[i].x);
+    x2[i] = ldp<COH>(fin + r[i].y);
   });
   float f[Q], fo[Q];
   static_for<Q>([&](auto I) {
@@ -2197,6 +2213,111 @@ __global__ void __launch_bounds__(64) k_boundary_tab(const __grid_constant__ wt_
   SampleSums acc;
   if (k < count) boundary_cell<L, S, MODE, SMP>(P, fin, fout, bcell, rec, gam, k, cap, sdf, xb, nub, &O, &acc);
   if constexpr (SMP) smp_flush(acc, O.sets, global_warp_id());
+}
+
+// ---- persistent steps: many lattice updates of one or more tunnels in one launch ---------------
+// On small grids a step's kernels finish faster than they can be launched (the D2Q9 channel of
+// 65,536 cells: about 5.5 us per step in captured graphs, most of it launch and dependency
+// latency). Here one cooperative launch runs `steps` updates of every tunnel in its table: per step
+// the work items of all tunnels (tiles of the vectorised bulk kernel, tiles of face-row cell pairs,
+// chunks of wall cells) are dealt round-robin to the resident blocks, and a grid-wide barrier
+// separates the steps. Each cell goes through the same device code as in the per-step kernels
+// (bulk_cells, face_rows, boundary_cell), so the results are bit-identical to stepping alone; its
+// population loads are cached in L2 only (ld.cg), since the input of one step is what other SMs
+// wrote in the step before.
+// The barrier's waits are bounded: a block that gives up sets bit 16 of the error word and
+// returns, and every other block then gives up too.
+constexpr int PS_THREADS = 256;
+constexpr int PS_MAX_TUNNELS = 48;
+constexpr uint32_t PS_BARRIER_POLLS = 1u << 22;
+
+struct PersistTunnel {
+  wt_kparams P;
+  void* f[2];             // step k reads f[(p0 + k) & 1] and writes the other
+  const uint8_t* cls;
+  const uint2* bcell;     // link records of the wall cells (k_boundary_tab's tables)
+  const uint4* brec;
+  const float* bgam;
+  uint32_t nbnd, btab_cap;
+  int32_t gs, p0;
+  uint32_t tbx, tby;      // bulk tile: tbx cell pairs along x by tby rows (tbx * tby = PS_THREADS)
+  uint32_t ttx, tty;      // bulk tiles per z-plane along x and y
+  uint32_t nbulk, nface;  // bulk tiles and face tiles per step
+  uint32_t item0;         // first work item of this tunnel
+  uint32_t pad;
+};
+struct PersistTable {
+  uint32_t count, items;  // tunnels, work items per step
+  uint32_t pad[2];
+  PersistTunnel t[PS_MAX_TUNNELS];
+};
+
+// grid-wide barrier over bar[0] (arrivals) and bar[1] (generation), both zero before the launch;
+// false if this block gave up waiting
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned nblocks) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = bar + 1;
+    const unsigned g = *gen;  // read before arriving: the generation cannot move until this block has
+    __threadfence();
+    int done = 1;
+    if (atomicAdd(bar, 1u) == nblocks - 1u) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      uint32_t it = 0;
+      while (*gen == g) {
+        if (++it > PS_BARRIER_POLLS) {
+          done = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    ok = done;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+template <class L, class S, bool BGK>
+__global__ void __launch_bounds__(PS_THREADS, 3) k_steps_persistent(const __grid_constant__ PersistTable T, int steps,
+                                                                  unsigned* __restrict__ bar, int* __restrict__ err) {
+  typedef typename S::T ST;
+  const uint32_t tid = threadIdx.x;
+  for (int k = 0; k < steps; k++) {
+    for (uint32_t item = blockIdx.x; item < T.items; item += gridDim.x) {
+      uint32_t m = 0;
+      while (m + 1 < T.count && T.t[m + 1].item0 <= item) m++;
+      const PersistTunnel& t = T.t[m];
+      const int par = (t.p0 + k) & 1;
+      const ST* fin = (const ST*)t.f[par];
+      ST* fout = (ST*)t.f[par ^ 1];
+      uint32_t j = item - t.item0;
+      if (j < t.nbulk) {
+        const uint32_t bx = j % t.ttx, by = (j / t.ttx) % t.tty, bz = j / (t.ttx * t.tty);
+        const uint32_t tx = tid % t.tbx, ty = tid / t.tbx;
+        bulk_cells<L, S, 2, BGK, false, true>(t.P, fin, fout, t.cls, t.gs, (int)(bx * t.tbx + tx) * 2,
+                                              (int)(by * t.tby + ty), (int)bz);
+      } else if ((j -= t.nbulk) < t.nface) {
+        const uint32_t g = j * PS_THREADS + tid, half = t.P.nx / 2u;
+        face_rows<L, S, FM_SMAG, false, true>(t.P, fin, fout, t.cls, t.gs, nullptr, nullptr, nullptr, nullptr,
+                                              nullptr, (int)(g % half) * 2, (int)(g / half));
+      } else {
+        const uint32_t c = (j - t.nface) * PS_THREADS + tid;
+        if (c < t.nbnd)
+          boundary_cell<L, S, FM_SMAG, false, true>(t.P, fin, fout, t.bcell, t.brec, t.bgam, c, t.btab_cap, nullptr,
+                                                    nullptr, nullptr, nullptr, nullptr);
+      }
+    }
+    if (k + 1 < steps && !grid_barrier(bar, gridDim.x)) {
+      if (tid == 0) atomicOr(err, 16);
+      return;
+    }
+  }
 }
 
 // Rest state written into the solid cells of one population buffer.
@@ -3283,6 +3404,70 @@ cudaError_t launch_stream_collide(wt_solver* s, const void* fin, void* fout) {
   WT_DISPATCH(sc_t, s, fin, fout, none);
 }
 cudaError_t launch_macro(wt_solver* s) { WT_DISPATCH(macro_t, s); }
+
+bool persistent_ok(const wt_solver* s) {
+  if (!(s->prec == WT_PREC_F16 || s->prec == WT_PREC_F32) || s->closure_dev != nullptr || s->cls_dirty) return false;
+  const bool faces_ok = s->dims.ny >= 2 && (!s->is3d || s->dims.nz >= 2);
+  return s->dims.nx % 2 == 0 && s->gs >= 2 && faces_ok && offsets32(s) && s->solid_ok[0] && s->solid_ok[1] &&
+         (s->nbnd == 0 || s->btab_cap >= s->nbnd);
+}
+
+template <class L, class S>
+static cudaError_t persistent_t(wt_solver* const* ms, int count, int steps, unsigned* bar, int* err,
+                                cudaStream_t st) {
+  if constexpr (S::PREC == WT_PREC_F64) {
+    return cudaErrorNotSupported;
+  } else {
+    if (count < 1 || count > PS_MAX_TUNNELS || steps < 1) return cudaErrorInvalidValue;
+    PersistTable tab;
+    std::memset(&tab, 0, sizeof tab);
+    uint32_t items = 0;
+    for (int k = 0; k < count; k++) {
+      const wt_solver* s = ms[k];
+      PersistTunnel& t = tab.t[k];
+      t.P = s->kp;
+      t.f[0] = s->f[0];
+      t.f[1] = s->f[1];
+      t.cls = s->cls;
+      t.bcell = s->bcell;
+      t.brec = s->brec;
+      t.bgam = s->bgam;
+      t.nbnd = s->nbnd;
+      t.btab_cap = (uint32_t)s->btab_cap;
+      t.gs = s->gs;
+      t.p0 = s->parity;
+      const uint32_t half = (uint32_t)s->dims.nx / 2u;
+      t.tbx = half >= 256 ? 256u : (half >= 128 ? 128u : (half >= 64 ? 64u : 32u));
+      t.tby = (uint32_t)PS_THREADS / t.tbx;
+      t.ttx = (half + t.tbx - 1) / t.tbx;
+      t.tty = ((uint32_t)s->dims.ny + t.tby - 1) / t.tby;
+      t.nbulk = t.ttx * t.tty * (uint32_t)s->dims.nz;
+      const uint32_t fr = s->is3d ? 2u * (uint32_t)s->dims.ny + 2u * (uint32_t)(s->dims.nz - 2) : 2u;
+      t.nface = (fr * half + PS_THREADS - 1) / PS_THREADS;
+      t.item0 = items;
+      items += t.nbulk + t.nface + (s->nbnd + PS_THREADS - 1) / PS_THREADS;
+    }
+    tab.count = (uint32_t)count;
+    tab.items = items;
+    auto kern = ms[0]->kp.collision == 1u ? k_steps_persistent<L, S, true> : k_steps_persistent<L, S, false>;
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PS_THREADS, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const unsigned grid = (unsigned)std::min<size_t>(items, (size_t)per_sm * (size_t)ms[0]->num_sms);
+    if ((e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st)) != cudaSuccess) return e;
+    void* args[] = {(void*)&tab, (void*)&steps, (void*)&bar, (void*)&err};
+    return cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(PS_THREADS), args, 0, st);
+  }
+}
+
+cudaError_t launch_persistent(wt_solver* const* ms, int count, int steps, unsigned* bar, int* err, cudaStream_t st) {
+  const wt_solver* s = ms[0];
+  for (int k = 1; k < count; k++)
+    if (ms[k]->is3d != s->is3d || ms[k]->prec != s->prec || ms[k]->kp.collision != s->kp.collision)
+      return cudaErrorInvalidValue;
+  WT_DISPATCH(persistent_t, ms, count, steps, bar, err, st);
+}
 
 bool batch_fusable(const wt_solver* s) {
   return s->is3d && (s->prec == WT_PREC_F16 || s->prec == WT_PREC_F32) && s->closure_dev == nullptr &&

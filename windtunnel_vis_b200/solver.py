@@ -268,7 +268,8 @@ class Solver:
         """Stream-collide launch: kernel = occupancy hint (0 none, 2..4 CTAs of 256 threads per
         SM), param = cells per thread along x (1 = the scalar kernel, 2 or 4), block bx x by
         (0 = default). kernel = 8 (param 2, bx 0) selects the row pipeline with `by` interior rows
-        per block (0 = 4)."""
+        per block (0 = 4); kernel = 9 (param 2, bx 0, by 0) the persistent kernel, which takes all
+        the steps of a call in one launch."""
         self._check(self._lib.wt_set_launch(self._h, int(kernel), int(param), int(bx), int(by)))
 
     def get_launch(self):
@@ -308,7 +309,7 @@ class Batch:
     holding every member's step kernels, so small tunnels run concurrently. Members stay ordinary
     Solver objects for parameters, geometry and readback, and must outlive the batch."""
 
-    def __init__(self, solvers, fused=False):
+    def __init__(self, solvers, fused=False, persistent=False):
         self._lib = abi.load()
         self.members = list(solvers)
         arr = (C.c_void_p * len(self.members))(*[s.handle.value for s in self.members])
@@ -319,10 +320,17 @@ class Batch:
         self._h = h
         if fused:
             self.set_fused(True)
+        if persistent:
+            self.set_persistent(True)
 
     def set_fused(self, on: bool):
-        """Bulk rows of all members in one batch-kernel launch (wt_batch_set_fused)."""
+        """Bulk rows of all members in one batch-kernel launch per step (wt_batch_set_fused(b, 1))."""
         self._check(self._lib.wt_batch_set_fused(self._h, 1 if on else 0))
+
+    def set_persistent(self, on: bool):
+        """Every wt_batch_step call of two or more steps as one cooperative launch of the
+        persistent kernel over all members (wt_batch_set_fused(b, WT_BATCH_PERSISTENT))."""
+        self._check(self._lib.wt_batch_set_fused(self._h, abi.WT_BATCH_PERSISTENT if on else 0))
 
     def _check(self, rc):
         if rc != 0:

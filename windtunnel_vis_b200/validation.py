@@ -332,7 +332,7 @@ def sweep_cases(count=32):
 
 
 def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, re_l=2e4, target_tris=200_000,
-                closure=None, fused=False, autotune=True):
+                closure=None, fused=False, autotune=True, persistent=False):
     """Runs the sweep of sweep_cases as one batch (windtunnel_vis_b200.solver.Batch): every tunnel
     voxelizes the vehicle body at its yaw (moving belt, rotating wheels, Smagorinsky LES, FP16),
     then all advance `steps` lattice updates together. Reports the aggregate MLUPS (device time
@@ -340,7 +340,8 @@ def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, 
     the same cases stepped one tunnel at a time (each with its own CUDA graphs) for the speed-up
     and the per-case C_D, which must agree exactly (the batch replays the same kernels). `closure`
     (a network, see windtunnel_vis_b200.closure) replaces Smagorinsky in every tunnel; with
-    `autotune` the project's launch tuner picks each tunnel's block shape and cells per thread."""
+    `autotune` the project's launch tuner picks each tunnel's block shape and cells per thread;
+    `persistent` runs each batch step call as one launch of the persistent kernel over all tunnels."""
     import torch
 
     from . import mesh as Mh
@@ -396,7 +397,7 @@ def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, 
 
     cells = sum(d[0] * d[1] * d[2] for d, _, _ in cases)
     solvers, frontal = build()
-    batch = Batch(solvers, fused=fused)
+    batch = Batch(solvers, fused=fused, persistent=persistent)
 
     def step_batch(n):
         batch.step(n)
@@ -404,7 +405,7 @@ def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, 
 
     ms, res = run(step_batch, batch.sample, frontal)
     out = {"id": "batch_sweep", "tunnels": count, "cells": cells, "steps": steps, "closure": closure is not None,
-           "fused": fused, "autotune": autotune and closure is None,
+           "fused": fused, "persistent": persistent, "autotune": autotune and closure is None,
            "batch_ms": ms,
            "batch_mlups": cells * steps / (ms * 1e-3) / 1e6, "cases": res}
     batch.destroy()
@@ -458,6 +459,7 @@ def main(argv=None):
     ap.add_argument("--radius", type=int, default=1, help="learned_closure: projection box half-width")
     ap.add_argument("--save", default=None, help="learned_closure: write the trained network (.npz)")
     ap.add_argument("--fused", action="store_true", help="batch_sweep: bulk rows of all tunnels in one kernel")
+    ap.add_argument("--persistent", action="store_true", help="batch_sweep: all tunnels' steps in one persistent launch")
     ap.add_argument("--closure", default=None,
                     help="batch_sweep: a network (.npz) or 'pretrained' in place of Smagorinsky in every tunnel")
     a = ap.parse_args(argv)
@@ -485,7 +487,7 @@ def main(argv=None):
             from . import closure as CL
 
             model = CL.load(CL.PRETRAINED if a.closure == "pretrained" else a.closure)
-        r = batch_sweep(a.steps, compare_alone=True, closure=model, fused=a.fused)
+        r = batch_sweep(a.steps, compare_alone=True, closure=model, fused=a.fused, persistent=a.persistent)
     else:
         r = CASES[a.case](solver_factory, a.valscale)
     r.pop("series", None)
