@@ -323,6 +323,10 @@ def components(s, peak, no_cpu):
         out["closure_step"]["cpu_threads"] = O.threads(0)
 
     out["d2q9_cylinder"] = d2q9_cylinder(peak, no_cpu)
+    # the same channel through the persistent multi-step kernel (one cooperative launch per call)
+    from windtunnel_vis_b200 import abi as A
+
+    out["d2q9_cylinder_persistent"] = d2q9_cylinder(peak, True, launch=(A.WT_LAUNCH_PERSISTENT, 2, 0, 0))
 
     # voxelizer (vehicle config, its own 512 x 256 x 256 handle)
     vd = (512, 256, 256)
@@ -355,15 +359,17 @@ def components(s, peak, no_cpu):
     return out
 
 
-def d2q9_cylinder(peak, no_cpu, updates=4000, chunks=20):
+def d2q9_cylinder(peak, no_cpu, updates=4000, chunks=20, launch=None):
     """The D2Q9 cylinder channel (512 x 128, FP32 populations, BGK, D = 20 at (96, 65), u = 0.05,
     Re = 100, rest state with seeded noise): lattice updates per second of the step alone (CUDA
     events around `updates` steps on the solver's stream) and of the reference's sample chunk
     (stepAndSample(50) with its statistics readback, host clock). The two 2.4 MB population
     buffers stay in L2, so the step is bound by launch and synchronisation latency, not by HBM;
-    72 B per update (9 populations read and written in FP32) is reported for comparison."""
+    72 B per update (9 populations read and written in FP32) is reported for comparison. `launch`
+    (kernel, param, bx, by) replaces the default launch (the persistent kernel, for instance)."""
     import torch
 
+    from windtunnel_vis_b200 import abi as A
     from windtunnel_vis_b200.solver import Solver
     from windtunnel_vis_b200.validation import CHANNEL_DIMS, channel_geometry, channel_params
 
@@ -374,6 +380,8 @@ def d2q9_cylinder(peak, no_cpu, updates=4000, chunks=20):
     s = Solver(dims, params)
     s.upload_flags(flags)
     s.upload_sdf(sdf)
+    if launch is not None:
+        s.set_launch(*launch)
     for _ in range(3):
         s.step_and_sample(CHUNK)
     st = torch.cuda.ExternalStream(s.stream)
@@ -389,14 +397,17 @@ def d2q9_cylinder(peak, no_cpu, updates=4000, chunks=20):
     for _ in range(chunks):
         s.step_and_sample(CHUNK)
     chunk_s = (time.perf_counter() - t0) / chunks
-    launch = s.get_launch()
+    used = s.get_launch()
     s.destroy()
     out = {"grid": list(dims), "storage": "f32", "collision": "bgk", "us_per_update": round(ms * 1e3, 3),
            "mlups": round(n / ms / 1e3, 1), "steps_per_s": round(1e3 / ms, 1),
            "chunk_mlups": round(n * CHUNK / chunk_s / 1e6, 1),
            "chunk": f"stepAndSample({CHUNK}) incl. the sampling pass and the statistics readback (host clock)",
            "launch": {"form": "10-step CUDA graphs: bulk kernel, face rows and wall cells per step",
-                      "cells_per_thread": launch[1], "block": [launch[2], launch[3]]},
+                      "cells_per_thread": used[1], "block": [used[2], used[3]]}
+           if used[0] != A.WT_LAUNCH_PERSISTENT else
+           {"form": "persistent kernel: one cooperative launch per call, work items from an atomic counter, "
+                    "grid barrier between steps"},
            "bytes_alg_per_update": n * 72, "l2_resident": True,
            "achieved_gbs_equiv": round(n * 72 / ms / 1e6, 1)}
     if not no_cpu:

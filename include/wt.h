@@ -278,11 +278,12 @@ int wt_probes(wt_solver* s, const float* pos4, int32_t count, float* out8);
  * shared memory; elsewhere the vectorised kernel runs. */
 #define WT_LAUNCH_ROW_PIPELINE 8
 /* kernel = WT_LAUNCH_PERSISTENT (param 2, bx 0, by 0): every wt_step call of two or more steps runs
- * as one cooperative launch of a persistent kernel that takes all its steps, the tiles of each step
- * dealt to the resident blocks and a grid-wide barrier between steps (the same arithmetic as the
- * per-step kernels: bit-identical results). For small grids, where launching a step's kernels costs
- * as much as running them. Needs f16 / f32 storage, nx even and the reference's closure; elsewhere
- * the vectorised kernel runs. */
+ * as one cooperative launch of a persistent kernel that takes all its steps: per step the resident
+ * blocks take the step's work items (wall-cell chunks, face-row tiles, bulk tiles) from an atomic
+ * counter, and a grid-wide barrier separates the steps (the same arithmetic as the per-step
+ * kernels: bit-identical results). For small grids, where launching a step's kernels costs as much
+ * as running them. Needs f16 / f32 storage, nx even and the reference's closure; elsewhere the
+ * vectorised kernel runs. */
 #define WT_LAUNCH_PERSISTENT 9
 int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32_t by);
 int wt_get_launch(const wt_solver* s, int32_t* out4);
@@ -320,9 +321,10 @@ int wt_batch_sample(wt_batch* b, wt_stats* out);
  * kernel over a table of per-tunnel descriptors (face rows and wall cells stay per member).
  * on = WT_BATCH_PERSISTENT: when every member has the same lattice, f16 / f32 storage and collision,
  * no learned closure and an even nx (at most 48 members), each wt_batch_step call of two or more
- * steps is one cooperative launch of the persistent kernel over all members: per step the bulk
- * tiles, face-row tiles and wall cells of every member are dealt to the resident blocks, with a
- * grid-wide barrier between steps. Members stay bit-identical to the same handles stepped alone.
+ * steps is one cooperative launch of the persistent kernel over all members: per step the resident
+ * blocks take the wall-cell chunks, face-row tiles and bulk tiles of every member from an atomic
+ * counter, with a grid-wide barrier between steps. Members stay bit-identical to the same handles
+ * stepped alone.
  * on = 0 (default): the members' own kernels under one graph. */
 #define WT_BATCH_PERSISTENT 2
 int wt_batch_set_fused(wt_batch* b, int32_t on);

@@ -210,3 +210,23 @@ def test_a_priori_metrics():
     y = np.linspace(0, 1, 100)
     assert CL.a_priori_metrics(y, y)["nmse"] == 0.0
     assert abs(CL.a_priori_metrics(np.full(100, y.mean()), y)["nmse"] - 1.0) < 1e-12
+
+
+def test_pretrained_network_is_gated_to_its_regime(tmp_path):
+    # the shipped network carries the Reynolds-number range it was trained and checked in
+    m = CL.load_pretrained(1000.0)
+    lo, hi = (float(v) for v in m["regime_re"])
+    assert lo <= 1000.0 <= hi and hi < 3000.0
+    CL.to_struct(m)  # the regime entry does not disturb the network's layout
+    for re in (lo / 2.0, 3000.0, 1e4, 2e4 * 0.336):
+        with pytest.raises(CL.ClosureRegimeError):
+            CL.load_pretrained(re)
+    assert float(CL.load_pretrained(1e4, allow_outside=True)["b3"]) == float(m["b3"])
+    # a network saved with a regime round-trips it; one saved without has none and is never refused
+    path = tmp_path / "net.npz"
+    CL.save(CL.init_model(seed=3), path, regime={"re": (100.0, 400.0)})
+    CL.load_pretrained(200.0, path=str(path))
+    with pytest.raises(CL.ClosureRegimeError):
+        CL.load_pretrained(800.0, path=str(path))
+    CL.save(CL.init_model(seed=3), path)
+    CL.load_pretrained(1e6, path=str(path))

@@ -79,9 +79,14 @@ def test_channel_cylinder_matches_oracle_full_size(gpu, oracle):
     d = np.abs(g.read_populations().astype(np.float64) - o.current.astype(np.float64)).max()
     assert d <= 1e-5, d
     sg, so = g.sample(), o.sample()
-    assert np.abs(sg["raw"][:3] - so["raw"][:3]).max() <= 1e-4 * max(np.abs(so["raw"][:3]).max(), 1e-3)
+    # the force is a sum over the cylinder's ~400 wall links of about 2 f each; after 300 steps the
+    # two runs' populations differ by ~1e-7 typically (1e-5 at most), so the sums may differ by a
+    # few 1e-6 in every component. The drag is 1.5e-2; the lift cancels to ~5e-5 this early, so the
+    # bound is absolute: 5e-6, 3e-4 of the drag
+    assert np.abs(sg["raw"][:3] - so["raw"][:3]).max() <= 5e-6, (sg["raw"][:3], so["raw"][:3])
+    assert abs(sg["raw"][0] / so["raw"][0] - 1) <= 2e-4
     assert sg["raw"][5:].tolist() == so["raw"][5:].tolist()
-    # the two runs' f32 roundings differ (FMA contraction on the GPU, none in the oracle) and the
+    # the two runs' f32 roundings differ (the GPU's rearranged algebra against the WGSL order) and the
     # collision's rounding moves mass a little every step: the mass sums agree to the drift of
     # 300 rounded steps (the sum itself is checked on identical populations in test_gpu_mass)
     assert sg["fluidCells"] == so["fluidCells"] and abs(sg["mass"] / so["mass"] - 1) <= 2e-5
@@ -140,7 +145,7 @@ def test_sphere_les_f16_tracks_f64_populations(gpu):
 def test_benchmark_tunnel_matches_oracle(gpu, oracle):
     # the bench workload itself (256 x 128 x 128, FP16, sphere D = 24, LES) against the oracle's
     # restatement of the reference's FP16 path: 60 steps (populations within the FP16 step
-    # tolerance: FMA contraction flips the rounding of a stored half now and then), then the macro
+    # tolerance: a one-ulp f32 difference flips the rounding of a stored half now and then), then the macro
     # pass on identical populations
     import bench
 
@@ -159,7 +164,7 @@ def test_benchmark_tunnel_matches_oracle(gpu, oracle):
     g.write_populations(o.current)
     sg, so = g.sample(), o.sample()
     # the force is a sum of ~1e4 wall-link terms of size ~0.05 that cancel to ~5e-4 this early; one
-    # f32 ulp per term (3.7e-9, FMA contraction on the GPU, none in the oracle) bounds the
+    # f32 ulp per term (3.7e-9, the GPU's summation order against the oracle's) bounds the
     # difference at ~1e-6, far below the terms themselves
     assert np.abs(sg["raw"][:3] - so["raw"][:3]).max() <= 1e-6
     assert sg["raw"][5:].tolist() == so["raw"][5:].tolist()

@@ -381,7 +381,7 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
             alloc((void**)&s->result_dev, RESULT_BYTES, "result") && alloc((void**)&s->err_dev, 4, "error word") &&
             alloc((void**)&s->bnd_count, 4, "boundary counter") &&
             alloc((void**)&s->smp_sets, wt::SMP_SETS_BYTES, "sampling accumulators") &&
-            alloc((void**)&s->ps_bar, 2 * sizeof(unsigned), "barrier words");
+            alloc((void**)&s->ps_bar, wt::PS_BAR_WORDS * sizeof(unsigned), "barrier words");
   if (ok && (cudaMallocHost((void**)&s->result_host, RESULT_BYTES) != cudaSuccess ||
              cudaMallocHost((void**)&s->err_host, 4) != cudaSuccess ||
              cudaMallocHost((void**)&s->bnd_count_host, 4) != cudaSuccess)) {
@@ -1310,7 +1310,7 @@ int wt_batch_create(wt_solver* const* members, int32_t count, wt_batch** out) {
   DeviceGuard g(b->device);
   bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
-            cudaMalloc((void**)&b->ps_bar, 2 * sizeof(unsigned)) == cudaSuccess;
+            cudaMalloc((void**)&b->ps_bar, wt::PS_BAR_WORDS * sizeof(unsigned)) == cudaSuccess;
   for (int32_t k = 0; ok && k < count; k++)
     ok = cudaEventCreateWithFlags(&b->ev_done[k], cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {

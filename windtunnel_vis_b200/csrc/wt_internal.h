@@ -191,9 +191,10 @@ struct BatchTable {
 // whether a handle's step can join the batch kernel: D3Q19, f16 / f32, vectorised path, no closure
 bool batch_fusable(const wt_solver* s);
 // The persistent kernel: `steps` updates of the tunnels ms[0 .. count) (same lattice, storage and
-// collision; each persistent_ok) in one cooperative launch on `st`; bar = two device words (zeroed
-// here), err = the device error word for a barrier timeout (bit 16). The members' parities are
-// not changed here.
+// collision; each persistent_ok) in one cooperative launch on `st`; bar = PS_BAR_WORDS device words
+// (zeroed here: the grid barrier's two and the work counters of two consecutive steps), err = the
+// device error word for a barrier timeout (bit 16). The members' parities are not changed here.
+constexpr int PS_BAR_WORDS = 4;
 bool persistent_ok(const wt_solver* s);
 cudaError_t launch_persistent(wt_solver* const* ms, int count, int steps, unsigned* bar, int* err, cudaStream_t st);
 // the face-row and wall-cell kernels of one step of `s` on its auxiliary stream, forked from

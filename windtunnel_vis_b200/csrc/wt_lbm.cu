@@ -2218,16 +2218,19 @@ __global__ void __launch_bounds__(64) k_boundary_tab(const __grid_constant__ wt_
 // ---- persistent steps: many lattice updates of one or more tunnels in one launch ---------------
 // On small grids a step's kernels finish faster than they can be launched (the D2Q9 channel of
 // 65,536 cells: about 5.5 us per step in captured graphs, most of it launch and dependency
-// latency). Here one cooperative launch runs `steps` updates of every tunnel in its table: per step
-// the work items of all tunnels (tiles of the vectorised bulk kernel, tiles of face-row cell pairs,
-// chunks of wall cells) are dealt round-robin to the resident blocks, and a grid-wide barrier
-// separates the steps. Each cell goes through the same device code as in the per-step kernels
-// (bulk_cells, face_rows, boundary_cell), so the results are bit-identical to stepping alone; its
-// population loads are cached in L2 only (ld.cg), since the input of one step is what other SMs
-// wrote in the step before.
+// latency). Here one cooperative launch runs `steps` updates of every tunnel in its table. A step's
+// work items are, in this order, the wall-cell chunks of every tunnel, then their face-row tiles,
+// then their bulk tiles (the slow items first, so that the step ends on short ones); blocks take
+// the next item from a per-step atomic counter, and a grid-wide barrier separates the steps. Each
+// cell goes through the same device code as in the per-step kernels (bulk_cells, face_rows,
+// boundary_cell), so the results are bit-identical to stepping alone; its population loads are
+// cached in L2 only (ld.cg), since the input of one step is what other SMs wrote in the step
+// before. In D3Q19 the face and wall items run out of line, so that their register demand does not
+// set the bulk tiles' occupancy.
 // The barrier's waits are bounded: a block that gives up sets bit 16 of the error word and
 // returns, and every other block then gives up too.
 constexpr int PS_THREADS = 256;
+constexpr int PS_MIN_BLOCKS = 4;  // resident blocks per SM the register budget is set for
 constexpr int PS_MAX_TUNNELS = 48;
 constexpr uint32_t PS_BARRIER_POLLS = 1u << 22;
 
@@ -2242,13 +2245,13 @@ struct PersistTunnel {
   int32_t gs, p0;
   uint32_t tbx, tby;      // bulk tile: tbx cell pairs along x by tby rows (tbx * tby = PS_THREADS)
   uint32_t ttx, tty;      // bulk tiles per z-plane along x and y
-  uint32_t nbulk, nface;  // bulk tiles and face tiles per step
-  uint32_t item0;         // first work item of this tunnel
+  uint32_t wi0, fi0, bi0; // first wall chunk, face tile and bulk tile of this tunnel in the step's items
   uint32_t pad;
 };
 struct PersistTable {
-  uint32_t count, items;  // tunnels, work items per step
-  uint32_t pad[2];
+  uint32_t count;         // tunnels
+  uint32_t fseg, bseg;    // first face item and first bulk item of a step (the wall items come first)
+  uint32_t items;         // work items per step
   PersistTunnel t[PS_MAX_TUNNELS];
 };
 
@@ -2283,35 +2286,90 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned nblocks) {
   return ok != 0;
 }
 
+// last tunnel m of the table with first(t[m]) <= item (first is nondecreasing in m; tunnels with no
+// items of the segment share their successor's start and are passed over)
+template <class F>
+__device__ __forceinline__ uint32_t ps_find(const PersistTable& T, uint32_t item, F first) {
+  uint32_t lo = 0, hi = T.count;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (first(T.t[mid]) <= item) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// wall cells c of one chunk (one per thread)
+template <class L, class S>
+__device__ __forceinline__ void ps_wall_cells(const PersistTunnel& t, const typename S::T* fin, typename S::T* fout,
+                                              uint32_t c) {
+  if (c < t.nbnd)
+    boundary_cell<L, S, FM_SMAG, false, true>(t.P, fin, fout, t.bcell, t.brec, t.bgam, c, t.btab_cap, nullptr,
+                                              nullptr, nullptr, nullptr, nullptr);
+}
+
+// face-row cell pair g (row g / (nx / 2), pair g % (nx / 2))
+template <class L, class S>
+__device__ __forceinline__ void ps_face_cells(const PersistTunnel& t, const typename S::T* fin, typename S::T* fout,
+                                              uint32_t g) {
+  const uint32_t half = t.P.nx / 2u;
+  face_rows<L, S, FM_SMAG, false, true>(t.P, fin, fout, t.cls, t.gs, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                        (int)(g % half) * 2, (int)(g / half));
+}
+
+// the same, out of line: in D3Q19 their register demand is above the bulk tiles' budget
+template <class L, class S>
+__device__ __noinline__ void ps_wall(const PersistTunnel& t, const typename S::T* fin, typename S::T* fout, uint32_t c) {
+  ps_wall_cells<L, S>(t, fin, fout, c);
+}
+template <class L, class S>
+__device__ __noinline__ void ps_face(const PersistTunnel& t, const typename S::T* fin, typename S::T* fout, uint32_t g) {
+  ps_face_cells<L, S>(t, fin, fout, g);
+}
+
 template <class L, class S, bool BGK>
-__global__ void __launch_bounds__(PS_THREADS, 3) k_steps_persistent(const __grid_constant__ PersistTable T, int steps,
-                                                                  unsigned* __restrict__ bar, int* __restrict__ err) {
+__global__ void __launch_bounds__(PS_THREADS, PS_MIN_BLOCKS)
+    k_steps_persistent(const __grid_constant__ PersistTable T, int steps, unsigned* __restrict__ bar,
+                       int* __restrict__ err) {
   typedef typename S::T ST;
+  // A block's first item of a step is its block index; thread 0 takes each further item from the
+  // step's counter (item = grid size + counter) while the block works on the current one, and
+  // passes it on through shared memory, double-buffered so that one barrier per item suffices.
+  __shared__ uint32_t s_item[2];
   const uint32_t tid = threadIdx.x;
+  uint32_t sl = 0;
   for (int k = 0; k < steps; k++) {
-    for (uint32_t item = blockIdx.x; item < T.items; item += gridDim.x) {
-      uint32_t m = 0;
-      while (m + 1 < T.count && T.t[m + 1].item0 <= item) m++;
+    unsigned* const ctr = bar + 2 + (k & 1);
+    // the next step's counter was last used by step k - 1, which every block has left
+    if (blockIdx.x == 0 && tid == 0) atomicExch(bar + 2 + ((k + 1) & 1), 0u);
+    for (uint32_t item = blockIdx.x; item < T.items; sl ^= 1u) {
+      uint32_t nxt = 0;
+      if (tid == 0) nxt = atomicAdd(ctr, 1u);  // consumed after this item's cells
+      uint32_t m;
+      if (item < T.fseg) m = ps_find(T, item, [](const PersistTunnel& q) { return q.wi0; });
+      else if (item < T.bseg) m = ps_find(T, item, [](const PersistTunnel& q) { return q.fi0; });
+      else m = ps_find(T, item, [](const PersistTunnel& q) { return q.bi0; });
       const PersistTunnel& t = T.t[m];
       const int par = (t.p0 + k) & 1;
       const ST* fin = (const ST*)t.f[par];
       ST* fout = (ST*)t.f[par ^ 1];
-      uint32_t j = item - t.item0;
-      if (j < t.nbulk) {
-        const uint32_t bx = j % t.ttx, by = (j / t.ttx) % t.tty, bz = j / (t.ttx * t.tty);
-        const uint32_t tx = tid % t.tbx, ty = tid / t.tbx;
-        bulk_cells<L, S, 2, BGK, false, true>(t.P, fin, fout, t.cls, t.gs, (int)(bx * t.tbx + tx) * 2,
-                                              (int)(by * t.tby + ty), (int)bz);
-      } else if ((j -= t.nbulk) < t.nface) {
-        const uint32_t g = j * PS_THREADS + tid, half = t.P.nx / 2u;
-        face_rows<L, S, FM_SMAG, false, true>(t.P, fin, fout, t.cls, t.gs, nullptr, nullptr, nullptr, nullptr,
-                                              nullptr, (int)(g % half) * 2, (int)(g / half));
+      if (item >= T.bseg) {
+        const uint32_t j = item - t.bi0;
+        const uint32_t bx = j % t.ttx, by = (j / t.ttx) % t.tty;
+        uint32_t bz = j / (t.ttx * t.tty);
+        if (par == 1) bz = (uint32_t)t.P.nz - 1u - bz;  // writing buffer 0: z downwards, as the step kernels
+        bulk_cells<L, S, 2, BGK, false, true>(t.P, fin, fout, t.cls, t.gs, (int)(bx * t.tbx + tid % t.tbx) * 2,
+                                              (int)(by * t.tby + tid / t.tbx), (int)bz);
+      } else if (item >= T.fseg) {
+        if constexpr (L::DIM == 3) ps_face<L, S>(t, fin, fout, (item - t.fi0) * PS_THREADS + tid);
+        else ps_face_cells<L, S>(t, fin, fout, (item - t.fi0) * PS_THREADS + tid);
       } else {
-        const uint32_t c = (j - t.nface) * PS_THREADS + tid;
-        if (c < t.nbnd)
-          boundary_cell<L, S, FM_SMAG, false, true>(t.P, fin, fout, t.bcell, t.brec, t.bgam, c, t.btab_cap, nullptr,
-                                                    nullptr, nullptr, nullptr, nullptr);
+        if constexpr (L::DIM == 3) ps_wall<L, S>(t, fin, fout, (item - t.wi0) * PS_THREADS + tid);
+        else ps_wall_cells<L, S>(t, fin, fout, (item - t.wi0) * PS_THREADS + tid);
       }
+      if (tid == 0) s_item[sl] = gridDim.x + nxt;
+      __syncthreads();
+      item = s_item[sl];
     }
     if (k + 1 < steps && !grid_barrier(bar, gridDim.x)) {
       if (tid == 0) atomicOr(err, 16);
@@ -3421,7 +3479,8 @@ static cudaError_t persistent_t(wt_solver* const* ms, int count, int steps, unsi
     if (count < 1 || count > PS_MAX_TUNNELS || steps < 1) return cudaErrorInvalidValue;
     PersistTable tab;
     std::memset(&tab, 0, sizeof tab);
-    uint32_t items = 0;
+    // items of a step: every tunnel's wall chunks, then every tunnel's face tiles, then the bulk tiles
+    uint32_t nwall[PS_MAX_TUNNELS], nface[PS_MAX_TUNNELS], nbulk[PS_MAX_TUNNELS];
     for (int k = 0; k < count; k++) {
       const wt_solver* s = ms[k];
       PersistTunnel& t = tab.t[k];
@@ -3441,12 +3500,17 @@ static cudaError_t persistent_t(wt_solver* const* ms, int count, int steps, unsi
       t.tby = (uint32_t)PS_THREADS / t.tbx;
       t.ttx = (half + t.tbx - 1) / t.tbx;
       t.tty = ((uint32_t)s->dims.ny + t.tby - 1) / t.tby;
-      t.nbulk = t.ttx * t.tty * (uint32_t)s->dims.nz;
+      nbulk[k] = t.ttx * t.tty * (uint32_t)s->dims.nz;
       const uint32_t fr = s->is3d ? 2u * (uint32_t)s->dims.ny + 2u * (uint32_t)(s->dims.nz - 2) : 2u;
-      t.nface = (fr * half + PS_THREADS - 1) / PS_THREADS;
-      t.item0 = items;
-      items += t.nbulk + t.nface + (s->nbnd + PS_THREADS - 1) / PS_THREADS;
+      nface[k] = (fr * half + PS_THREADS - 1) / PS_THREADS;
+      nwall[k] = (s->nbnd + PS_THREADS - 1) / PS_THREADS;
     }
+    uint32_t items = 0;
+    for (int k = 0; k < count; k++) tab.t[k].wi0 = items, items += nwall[k];
+    tab.fseg = items;
+    for (int k = 0; k < count; k++) tab.t[k].fi0 = items, items += nface[k];
+    tab.bseg = items;
+    for (int k = 0; k < count; k++) tab.t[k].bi0 = items, items += nbulk[k];
     tab.count = (uint32_t)count;
     tab.items = items;
     auto kern = ms[0]->kp.collision == 1u ? k_steps_persistent<L, S, true> : k_steps_persistent<L, S, false>;
@@ -3455,7 +3519,7 @@ static cudaError_t persistent_t(wt_solver* const* ms, int count, int steps, unsi
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const unsigned grid = (unsigned)std::min<size_t>(items, (size_t)per_sm * (size_t)ms[0]->num_sms);
-    if ((e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(bar, 0, PS_BAR_WORDS * sizeof(unsigned), st)) != cudaSuccess) return e;
     void* args[] = {(void*)&tab, (void*)&steps, (void*)&bar, (void*)&err};
     return cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(PS_THREADS), args, 0, st);
   }

@@ -457,9 +457,12 @@ def main(argv=None):
     ap.add_argument("--keep", type=float, default=0.4)
     ap.add_argument("--re", type=float, default=1000.0)
     ap.add_argument("--radius", type=int, default=1, help="learned_closure: projection box half-width")
+    ap.add_argument("--height", type=float, default=0.125, help="learned_closure: body height / tunnel height")
     ap.add_argument("--save", default=None, help="learned_closure: write the trained network (.npz)")
     ap.add_argument("--fused", action="store_true", help="batch_sweep: bulk rows of all tunnels in one kernel")
     ap.add_argument("--persistent", action="store_true", help="batch_sweep: all tunnels' steps in one persistent launch")
+    ap.add_argument("--outside-regime", action="store_true",
+                    help="batch_sweep: apply --closure outside its stored Reynolds-number regime (throughput only)")
     ap.add_argument("--closure", default=None,
                     help="batch_sweep: a network (.npz) or 'pretrained' in place of Smagorinsky in every tunnel")
     a = ap.parse_args(argv)
@@ -469,9 +472,11 @@ def main(argv=None):
         fine = tuple(int(v) for v in a.fine.split(","))
         r = CL.study(solver_factory, fine_dims=fine, train_bodies=a.train_bodies, eval_bodies=a.eval_bodies,
                      warm=a.warm, train_steps=a.train_steps, keep=a.keep, re=a.re, eval_steps=a.steps, radius=a.radius,
-                     log=lambda m: print(m, flush=True))
+                     height=a.height, log=lambda m: print(m, flush=True))
         if a.save:
-            CL.save({k: np.asarray(v, np.float32) for k, v in r["model"].items()}, a.save)
+            # gated to a factor of two around the Reynolds number it was trained and checked at
+            CL.save({k: np.asarray(v, np.float32) for k, v in r["model"].items()}, a.save,
+                    regime={"re": (a.re / 2.0, a.re * 2.0)})
         r.pop("model", None)
         print(json.dumps(r, default=float), flush=True)
         return
@@ -486,7 +491,10 @@ def main(argv=None):
         if a.closure:
             from . import closure as CL
 
-            model = CL.load(CL.PRETRAINED if a.closure == "pretrained" else a.closure)
+            # the vehicle tunnels run at Re_L = 2e4 on the body length, 6720 on its height (0.336 of
+            # the length): outside the shipped network's regime, allowed only for throughput runs
+            model = CL.load_pretrained(2e4 * 0.336, allow_outside=a.outside_regime,
+                                       path=CL.PRETRAINED if a.closure == "pretrained" else a.closure)
         r = batch_sweep(a.steps, compare_alone=True, closure=model, fused=a.fused, persistent=a.persistent)
     else:
         r = CASES[a.case](solver_factory, a.valscale)
