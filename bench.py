@@ -82,47 +82,89 @@ def geometry():
 
 
 class Clocks:
-    """nvidia-smi sampler for the timed region."""
+    """SM clock and clock-event reasons of this rank's GPU, sampled every 10 ms by a host thread
+    through NVML for as long as the `with` block runs (the timed region): the same counters as
+    `nvidia-smi --query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.*`, without a process
+    start-up that can outlast a short timed region. Falls back to an nvidia-smi sampler."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.thread = None
+        self.rows = []
+        self.mx = None
         self.path = os.path.join(tempfile.gettempdir(), f"wt_bench_clocks_rank{index}_{os.getpid()}.csv")
+
+    def _nvml_start(self):
+        import threading
+
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+        h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        self.mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        bits = (pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap)
+        self.stop = threading.Event()
+
+        def run():
+            while not self.stop.is_set():
+                sm = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                r = int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))
+                self.rows.append((sm, tuple(bool(r & b) for b in bits)))
+                self.stop.wait(0.01)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.fh = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv",
-                                          "-lms", "50"], stdout=self.fh, stderr=subprocess.DEVNULL)
-        except (OSError, FileNotFoundError):
-            self.proc = None
+            self._nvml_start()
+        except Exception:
+            self.thread = None
+            try:
+                self.fh = open(self.path, "w")
+                self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                              "--format=csv", "-lms", "50"], stdout=self.fh, stderr=subprocess.DEVNULL)
+            except (OSError, FileNotFoundError):
+                self.proc = None
         return self
 
     def __exit__(self, *a):
+        if self.thread:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             self.proc.wait(timeout=10)
             self.fh.close()
 
     def summary(self):
-        if not self.proc:
+        if self.thread:
+            rows, mx, source = self.rows, self.mx, "nvml, 10 ms"
+        elif self.proc:
+            with open(self.path) as fh:
+                raw = [r.split(", ") for r in fh.read().strip().split("\n")[1:] if r.strip()]
+            os.remove(self.path)
+            rows = [(float(r[1].split()[0]), tuple(r[5 + k].strip() == "Active" for k in range(4))) for r in raw]
+            mx = float(raw[0][2].split()[0]) if raw else None
+            source = "nvidia-smi, 50 ms"
+        else:
             return None
-        with open(self.path) as fh:
-            rows = [r.split(", ") for r in fh.read().strip().split("\n")[1:] if r.strip()]
-        os.remove(self.path)
         if not rows:
             return None
-        sm = [float(r[1].split()[0]) for r in rows]
-        mx = float(rows[0][2].split()[0])
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        sm = [v for v, _ in rows]
+        reasons = sorted({self.NAMES[k] for _, r in rows for k in range(4) if r[k]})
         loaded = [v for v in sm if v > 0.5 * mx] or sm
-        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows),
+                "source": source}
 
 
 def cpu_port_mlups(seconds=12.0, threads=0, steps_cap=None):
@@ -564,6 +606,8 @@ def run_ours(args, rank, world, local_rank, dist):
                                 if args.closure else
                                 "one lattice update: k_stream_collide_rows<StF16> (bulk, row pipeline) overlapped "
                                 "with k_face_v and k_boundary_tab" if shape[0] == 8 else
+                                "k_steps_persistent<D3Q19,StF16>: the chunk's updates in one cooperative launch "
+                                "(wall, face and bulk items per step, grid barrier between steps)" if shape[0] == 9 else
                                 "one lattice update: k_stream_collide_v<D3Q19,StF16> (bulk) overlapped with "
                                 "k_face_v and k_boundary_tab" if shape[1] > 1 else "k_stream_collide<D3Q19,StF16>"),
                      "bytes_alg_per_update": n * BYTES_PER_UPDATE, "traffic_per": "lattice update (ncu, steady state)",
