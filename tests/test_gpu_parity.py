@@ -1,9 +1,12 @@
 """CUDA path (through libwt.so) against the CPU oracle on the same seeded inputs.
 
-Tolerances (the oracle evaluates the WGSL expression order; the LBM kernels, compiled without FMA
-contraction, compute the same algebra rearranged (shifted populations f - w, pairwise moment sums,
-fused multiply-adds where the source writes them), so single-precision results differ by a few ulp
-per step):
+The scalar kernel (one cell per thread: every pull rule in cell_general, the collision in
+collide_full) evaluates the reference's expressions in the WGSL order, one rounding per operation
+(the LBM unit is compiled without FMA contraction), as the oracle does: its populations are
+bit-identical to the oracle's in every precision. Tolerances for the vectorised kernels, which
+compute the same algebra rearranged (shifted populations f - w, pairwise moment sums, fused
+multiply-adds where the source writes them), so single-precision results differ by a few ulp per
+step:
   f64 populations ............ |Δ| <= 1e-12 after 1 and 30 steps
   f32 populations ............ |Δ| <= 1e-6 after 1 step, <= 2e-5 after 30 steps
   f16 (f - w) populations .... |Δ| <= 2e-5 after 1 step (about 2 half ulps), <= 3e-4 after 30
@@ -69,12 +72,19 @@ def _check_against_oracle(oracle, dims, params, launch):
     g.set_launch(*launch)
     assert g.get_launch() == launch
     t1, t30 = TOL[prec]
+    # the scalar kernel (one cell per thread, collide_full) evaluates the reference's expressions in
+    # the reference's order, operation by operation, like the oracle: the same bits
+    exact = launch == LAUNCHES["reg1"]
     g.step(1)
     o.step(1)
+    if exact:
+        np.testing.assert_array_equal(g.read_populations(), o.current)
     d1 = np.abs(_as_float(g.read_populations()) - _as_float(o.current)).max()
     assert d1 <= t1, f"1 step: max |diff| {d1:.3e}"
     g.step(29)
     o.step(29)
+    if exact:
+        np.testing.assert_array_equal(g.read_populations(), o.current)
     d30 = np.abs(_as_float(g.read_populations()) - _as_float(o.current)).max()
     assert d30 <= t30, f"30 steps: max |diff| {d30:.3e}"
     # macro pass: stats, velocity field, EMA statistics

@@ -235,15 +235,32 @@ __device__ __forceinline__ void collide_full(const wt_kparams& P, const R (&f)[L
   si = si < (R)0 ? (R)0 : (si > (R)1 ? (R)1 : si);
   const R sIn = (R)P.sponge_in > (R)0 ? (R)0.08 * si * si : (R)0;
   const R trP = (pxx + pyy + pzz) * third;
-  const R base = (R)1 - (R)1.5 * usq;
   static_for<Q>([&](auto I) {
     constexpr int i = I;
     constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
     const R w = (R)Wc<L, i>::v;
     const R cu = (R)cx * ux + (R)cy * uy + (R)cz * uz;
-    const R feq = w * rho * (base + cu * ((R)3 + (R)4.5 * cu));
-    const R qpi = (R)(cx * cx) * pxx + (R)(cy * cy) * pyy + (R)(cz * cz) * pzz + (R)(2 * cx * cy) * pxy +
-                  (R)(2 * cx * cz) * pxz + (R)(2 * cy * cz) * pyz - trP;
+    // the reference's evaluation order (wgslLbm.ts:221-236): feq from 1 + 3 cu + 4.5 cu^2 - 1.5 u^2,
+    // and Q_i : Pi summed over the stress components in the order xx, xy, xz, yy, yz, zz with the
+    // zero terms left out
+    const R feq = w * rho * ((R)1 + (R)3 * cu + (R)4.5 * cu * cu - (R)1.5 * usq);
+    R qp = (R)0;
+    bool qf = true;
+    auto addq = [&](int coef, R p) {
+      if (coef == 0) return;
+      const R t = (R)coef * p;
+      qp = qf ? t : qp + t;
+      qf = false;
+    };
+    addq(cx * cx, pxx);
+    addq(2 * cx * cy, pxy);
+    if constexpr (D3) addq(2 * cx * cz, pxz);
+    addq(cy * cy, pyy);
+    if constexpr (D3) {
+      addq(2 * cy * cz, pyz);
+      addq(cz * cz, pzz);
+    }
+    const R qpi = qp - trP;
     R v = feq + (useBGK ? omega * (f[i] - feq) : w * k1 * qpi);
     if (sIn > (R)0) {
       const R eq = w * ((R)1 + (R)(3 * cx) * U + (R)(4.5 * cx * cx) * U * U - (R)1.5 * U * U);
