@@ -53,13 +53,15 @@ def peaks():
 
 
 def measured_traffic(shape, closure=False):
-    """DRAM bytes (read + write) per step of this launch shape from the committed ncu summary
-    (steady state over 30 steps), or None when that launch was not captured."""
+    """DRAM bytes (read + write) per step of this launch shape (cells per thread, block) from the
+    committed ncu summary (steady state: three consecutive launches of each step kernel), or None
+    when that shape was not captured. The occupancy hint changes the register allocation, not the
+    loads and stores, so it is not part of the key."""
     name = "stream_collide_d3q19_f16_sphere256_learned_closure.md" if closure else "stream_collide_d3q19_f16_sphere256.md"
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
-    key = "lc" if closure else ",".join(str(int(v)) for v in shape)
+    key = "lc" if closure else ",".join(str(int(v)) for v in shape[1:])
     for m in re.finditer(r"^traffic_bytes_per_step\[([0-9a-z,]+)\]:\s*(\d+)", open(p).read(), flags=re.M):
         if m.group(1) == key:
             return int(m.group(2))
@@ -598,7 +600,7 @@ def run_ours(args, rank, world, local_rank, dist):
                                  "pass fused (velocity field, EMA, sums), the wall force, the 80-byte stats readback",
                    "fused_samples": s.fused_samples,
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2: 2 x 159 MB population buffers",
-                   "launch": {"cells_per_thread": shape[1], "block": [shape[2], shape[3]]}},
+                   "launch": {"hint": shape[0], "cells_per_thread": shape[1], "block": [shape[2], shape[3]]}},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": ("one lattice update: k_stream_collide_lc<StF16> (bulk, network on tcgen05) overlapped "

@@ -93,6 +93,31 @@ def test_channel_cylinder_matches_oracle_full_size(gpu, oracle):
     g.destroy()
 
 
+@pytest.mark.parametrize("case", ["channel_f32", "sphere_tunnel_f16"])
+def test_scalar_kernel_bit_identical_to_oracle_full_size(gpu, oracle, case):
+    # the scalar kernel evaluates the reference's expressions in the reference's order: at full size
+    # its populations equal the oracle's bit for bit (the D2Q9 channel, FP32, 300 steps from rest;
+    # the benchmark's sphere tunnel, FP16 shifted storage, Smagorinsky, 10 steps)
+    import bench
+
+    if case == "channel_f32":
+        dims, params, steps = V.CHANNEL_DIMS, V.channel_params("f32"), 300
+        flags, _, sdf = V.channel_geometry()
+    else:
+        dims, params, steps = bench.DIMS, bench.PARAMS, 10
+        flags, _, sdf = bench.geometry()
+    g = Solver(dims, params)
+    o = oracle.OracleSolver(dims, params)
+    for s in (g, o):
+        s.upload_flags(flags)
+        s.upload_sdf(sdf)
+    g.set_launch(0, 1, 0, 0)
+    g.step(steps)
+    o.step(steps)
+    np.testing.assert_array_equal(g.read_populations(), o.current)
+    g.destroy()
+
+
 def test_full_size_fp16_against_fp32(gpu):
     # 256 x 128 x 128 sphere D = 24 (the benchmark workload): FP16 shifted storage tracks FP32
     dims = (256, 128, 128)

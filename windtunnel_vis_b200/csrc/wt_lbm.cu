@@ -722,8 +722,12 @@ __device__ __forceinline__ float tau0_eff(const wt_kparams& P, float fx, float t
 
 // Regularized / BGK collision of two bulk cells at once on shifted populations (lanes .x, .y),
 // same algebra as collide_shifted. `ofn(rho, irho, ux, uy, uz, pxx, pyy, pzz, pxy, pxz, pyz)`
-// returns the two cells' omega = 1 - 1 / tau (the closure).
-template <class L, bool BGK, class Emit, class OmegaFn>
+// returns the two cells' omega = 1 - 1 / tau (the closure). SP: whether the cells lie in the inlet
+// absorbing layer: SP_ON / SP_OFF when the caller has branched on it once per cell pair (no test
+// per direction), SP_TEST to test it here (for callers whose ofn holds block-wide barriers, which
+// every thread must reach through the same call).
+enum : int { SP_OFF = 0, SP_ON = 1, SP_TEST = 2 };
+template <class L, bool BGK, int SP = SP_TEST, class Emit, class OmegaFn>
 __device__ __forceinline__ void collide_shifted2x(const wt_kparams& P, const float2 (&h)[L::Q], int x, Emit&& emit,
                                                   OmegaFn&& ofn) {
   constexpr int Q = L::Q;
@@ -781,7 +785,7 @@ __device__ __forceinline__ void collide_shifted2x(const wt_kparams& P, const flo
   const float2 a = sub2(f2(1.0f), omega);
   // inlet absorbing layer: blend towards the free-stream equilibrium (wgslLbm.ts:224-237)
   float2 keep = f2(1.0f), sIn = f2(0.0f);
-  const bool sponge_in = P.sponge_in > 0.0f && (float)x < P.sponge_in;
+  const bool sponge_in = SP == SP_TEST ? P.sponge_in > 0.0f && (float)x < P.sponge_in : SP == SP_ON;
   if (sponge_in) {
     const float inv = __fdividef(1.0f, fmaxf(P.sponge_in, 1.0f));
     const float s0 = fminf(fmaxf(1.0f - (float)x * inv, 0.0f), 1.0f);
@@ -790,8 +794,8 @@ __device__ __forceinline__ void collide_shifted2x(const wt_kparams& P, const flo
     keep = sub2(f2(1.0f), sIn);
   }
   auto out = [&](auto I, float2 v) {
-    constexpr int i = decltype(I)::value;
     if (sponge_in) {
+      constexpr int i = decltype(I)::value;
       constexpr int cx = L::c[i][0];
       constexpr float w = (float)Wc<L, i>::v;
       const float U = P.uin;
@@ -848,33 +852,34 @@ __device__ __forceinline__ void collide_shifted2x(const wt_kparams& P, const flo
 template <class L, bool BGK, class Emit>
 __device__ __forceinline__ void collide_shifted2(const wt_kparams& P, const float2 (&h)[L::Q], int x, Emit&& emit,
                                                  float t_floor = 0.0f) {
-  collide_shifted2x<L, BGK>(P, h, x, emit,
-                            [&](float2 /*rho*/, float2 irho, float2, float2, float2, float2 pxx, float2 pyy, float2 pzz,
-                                float2 pxy, float2 pxz, float2 pyz) {
-                              float2 omega;
-                              if (P.csmag2 > 0.0f || P.sponge_start < (float)P.nx || t_floor > P.tau0) {
-                                float2 pn = fma2(pxx, pxx, fma2(pyy, pyy, mul2(f2(2.f), mul2(pxy, pxy))));
-                                if constexpr (L::DIM == 3)
-                                  pn = fma2(pzz, pzz, fma2(f2(2.f), fma2(pxz, pxz, mul2(pyz, pyz)), pn));
-                                relax_cell(P, (float)x, pn.x, irho.x, omega.x, t_floor);
-                                relax_cell(P, (float)(x + 1), pn.y, irho.y, omega.y, t_floor);
-                              } else {
-                                omega = f2(1.0f - __fdividef(1.0f, P.tau0));
-                              }
-                              return omega;
-                            });
+  auto ofn = [&](float2 /*rho*/, float2 irho, float2, float2, float2, float2 pxx, float2 pyy, float2 pzz,
+                 float2 pxy, float2 pxz, float2 pyz) {
+    float2 omega;
+    if (P.csmag2 > 0.0f || P.sponge_start < (float)P.nx || t_floor > P.tau0) {
+      float2 pn = fma2(pxx, pxx, fma2(pyy, pyy, mul2(f2(2.f), mul2(pxy, pxy))));
+      if constexpr (L::DIM == 3) pn = fma2(pzz, pzz, fma2(f2(2.f), fma2(pxz, pxz, mul2(pyz, pyz)), pn));
+      relax_cell(P, (float)x, pn.x, irho.x, omega.x, t_floor);
+      relax_cell(P, (float)(x + 1), pn.y, irho.y, omega.y, t_floor);
+    } else {
+      omega = f2(1.0f - __fdividef(1.0f, P.tau0));
+    }
+    return omega;
+  };
+  if (P.sponge_in > 0.0f && (float)x < P.sponge_in) collide_shifted2x<L, BGK, SP_ON>(P, h, x, emit, ofn);
+  else collide_shifted2x<L, BGK, SP_OFF>(P, h, x, emit, ofn);
 }
 
 // the learned closure with the two cells' eddy viscosities given (face rows)
 template <class L, bool BGK, class Emit>
 __device__ __forceinline__ void collide_shifted2_nu(const wt_kparams& P, const float2 (&h)[L::Q], int x, Emit&& emit,
                                                     float t_floor, float2 nu) {
-  collide_shifted2x<L, BGK>(P, h, x, emit, [&](float2, float2, float2, float2, float2, float2, float2, float2,
-                                               float2, float2, float2) {
+  auto ofn = [&](float2, float2, float2, float2, float2, float2, float2, float2, float2, float2, float2) {
     const float ta = tau0_eff(P, (float)x, t_floor) + 3.0f * nu.x;
     const float tb = tau0_eff(P, (float)(x + 1), t_floor) + 3.0f * nu.y;
     return make_float2(1.0f - __fdividef(1.0f, ta), 1.0f - __fdividef(1.0f, tb));
-  });
+  };
+  if (P.sponge_in > 0.0f && (float)x < P.sponge_in) collide_shifted2x<L, BGK, SP_ON>(P, h, x, emit, ofn);
+  else collide_shifted2x<L, BGK, SP_OFF>(P, h, x, emit, ofn);
 }
 
 // the closure features of two cells (the moments of the pulled populations) into rows
@@ -882,7 +887,7 @@ __device__ __forceinline__ void collide_shifted2_nu(const wt_kparams& P, const f
 template <class L>
 __device__ __forceinline__ void features2(const wt_kparams& P, const float2 (&h)[L::Q], float2 wd,
                                           float* __restrict__ x, size_t row) {
-  collide_shifted2x<L, true>(P, h, 0, [&](auto, float2) {},
+  collide_shifted2x<L, true, SP_OFF>(P, h, 0, [&](auto, float2) {},
                              [&](float2 rho, float2, float2 ux, float2 uy, float2 uz, float2 pxx, float2 pyy,
                                  float2 pzz, float2 pxy, float2 pxz, float2 pyz) {
                                float xa[CL_IN], xb[CL_IN];
@@ -1111,6 +1116,14 @@ __device__ __forceinline__ T ldp(const T* p) {
   else return __ldg(p);
 }
 
+// Per-direction population plane bases of a step, computed on the host and passed by value, so a
+// thread reaches direction i's source or destination with one multiply-add from the constant
+// bank: in[i] = fin + i N - c_iy nx - c_iz nx ny (the plane of direction i shifted back by c_i
+// along y and z; a bulk cell's index lands inside the buffer), out[i] = fout + i N.
+template <class T> struct DirPtrs {
+  const T* in[19];
+  T* out[19];
+};
 template <class S> struct PairIO;
 template <> struct PairIO<StF16> {
   typedef uint32_t pair_t;
@@ -1139,6 +1152,13 @@ template <> struct PairIO<StF16> {
   __device__ __forceinline__ static void st(__half* __restrict__ p, uint32_t o, float2 v, float /*w*/) {
     *reinterpret_cast<__half2*>(p + o) = __float22half2_rn(v);
   }
+  // st as one predicated store (no branch around it): nothing is written unless c
+  __device__ __forceinline__ static void st_if(__half* __restrict__ p, uint32_t o, float2 v, float, bool c) {
+    const __half2 h = __float22half2_rn(v);
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.global.b32 [%0], %1;\n\t}" ::"l"(p + o),
+                 "r"(*reinterpret_cast<const uint32_t*>(&h)), "r"((uint32_t)c)
+                 : "memory");
+  }
   // the populations st stores for v, as a later pass reads them back (f = stored + w)
   __device__ __forceinline__ static float2 readback(float2 v, float w) {
     const __half2 h = __float22half2_rn(v);
@@ -1166,6 +1186,11 @@ template <> struct PairIO<StF32> {
   __device__ __forceinline__ static void st(float* __restrict__ p, uint32_t o, float2 v, float w) {
     *reinterpret_cast<float2*>(p + o) = make_float2(__fadd_rn(v.x, w), __fadd_rn(v.y, w));
   }
+  __device__ __forceinline__ static void st_if(float* __restrict__ p, uint32_t o, float2 v, float w, bool c) {
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %3, 0;\n\t@q st.global.v2.f32 [%0], {%1, %2};\n\t}" ::"l"(p + o),
+                 "f"(__fadd_rn(v.x, w)), "f"(__fadd_rn(v.y, w)), "r"((uint32_t)c)
+                 : "memory");
+  }
   __device__ __forceinline__ static float2 readback(float2 v, float w) {
     return make_float2(__fadd_rn(v.x, w), __fadd_rn(v.y, w));
   }
@@ -1177,11 +1202,11 @@ template <int MINB> struct Bounds { static constexpr int v = MINB; };
 // The V cells x0 .. x0 + V - 1 of row (iy, iz) (bulk rows only); shared by the single-tunnel
 // kernel and the batch kernel.
 // With SMP the cells also run the per-cell part of the sampling pass on what they store.
-template <class L, class S, int V, bool BGK, bool SMP = false, bool COH = false>
+template <class L, class S, int V, bool BGK, bool SMP = false, bool COH = false, bool TAB = false>
 __device__ __forceinline__ void bulk_cells(const wt_kparams& P, const typename S::T* __restrict__ fin,
                                            typename S::T* __restrict__ fout, const uint8_t* __restrict__ cls,
                                            int gs, int x0, int iy, int iz, const SampleOut* O = nullptr,
-                                           SampleSums* acc = nullptr) {
+                                           SampleSums* acc = nullptr, const DirPtrs<typename S::T>* D = nullptr) {
   typedef PairIO<S> IO;
   constexpr int Q = L::Q;
   constexpr bool D3 = L::DIM == 3;
@@ -1205,23 +1230,35 @@ __device__ __forceinline__ void bulk_cells(const wt_kparams& P, const typename S
   typename IO::pair_t rp[G][Q];
   typename IO::one_t r1[Q];
   const bool last = x0 + V >= NX;
-  // one 64-bit base per thread; each direction adds an offset that is the same for every thread
-  // (plane i, shifted back by c_i along y and z)
+  // TAB: direction i's source is D->in[i] + idx0 (one multiply-add from the constant bank);
+  // otherwise one 64-bit base per thread, and each direction adds an offset that is the same for
+  // every thread (plane i, shifted back by c_i along y and z)
   const typename S::T* fb = fin + idx0;
   typename S::T* ob = fout + idx0;
+  const uint32_t idxm = x0 > 0 ? idx0 - 1u : idx0, idxp = idx0 + (uint32_t)(last ? V - 1 : V);
   static_for<Q>([&](auto I) {
     constexpr int i = I;
-    constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
-    const ptrdiff_t off = (ptrdiff_t)i * N - (ptrdiff_t)cy * sy - (ptrdiff_t)cz * sz;
-    const typename S::T* ps = fb + off;
+    [[maybe_unused]] constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+    const typename S::T* ps;
+    if constexpr (TAB) {
+      ps = D->in[i] + idx0;
+    } else {
+      const ptrdiff_t off = (ptrdiff_t)i * N - (ptrdiff_t)cy * sy - (ptrdiff_t)cz * sz;
+      ps = fb + off;
+    }
     if constexpr (G == 2) {
       IO::template ld4<COH>(ps, 0u, rp[0][i], rp[1][i]);  // 8- or 16-byte aligned when nx % 4 == 0
     } else {
 #pragma unroll
       for (int g = 0; g < G; g++) rp[g][i] = IO::template ld<COH>(ps, 2 * g);
     }
-    if constexpr (cx > 0) r1[i] = IO::template ld1<COH>(x0 > 0 ? ps - 1 : ps, 0u);     // x - 1
-    if constexpr (cx < 0) r1[i] = IO::template ld1<COH>(ps + (last ? V - 1 : V), 0u);  // x + 1, outlet clamp
+    if constexpr (TAB) {
+      if constexpr (cx > 0) r1[i] = IO::template ld1<COH>(D->in[i] + idxm, 0u);
+      if constexpr (cx < 0) r1[i] = IO::template ld1<COH>(D->in[i] + idxp, 0u);
+    } else {
+      if constexpr (cx > 0) r1[i] = IO::template ld1<COH>(x0 > 0 ? ps - 1 : ps, 0u);     // x - 1
+      if constexpr (cx < 0) r1[i] = IO::template ld1<COH>(ps + (last ? V - 1 : V), 0u);  // x + 1, outlet clamp
+    }
   });
   // phase 2, one pair of cells at a time (the other pairs stay packed in their raw registers):
   // convert and shift into the pulled populations, collide, store
@@ -1256,7 +1293,8 @@ __device__ __forceinline__ void bulk_cells(const wt_kparams& P, const typename S
     PairMoments pm;
     collide_shifted2<L, BGK>(P, h, x0 + 2 * g, [&](auto I, float2 v) {
       constexpr int i = decltype(I)::value;
-      if (clean) IO::st(ob + (ptrdiff_t)i * N, 2 * g, v, (float)Wc<L, i>::v);
+      if constexpr (TAB) IO::st_if(D->out[i] + idx0, 2 * g, v, (float)Wc<L, i>::v, clean);
+      else IO::st_if(ob + (ptrdiff_t)i * N, 2 * g, v, (float)Wc<L, i>::v, clean);
       if constexpr (SMP) pm.template add<L, i>(IO::readback(v, (float)Wc<L, i>::v));
     });
     if constexpr (SMP) {
@@ -1276,11 +1314,12 @@ __global__ void __launch_bounds__(256, MINB > 0 ? MINB : 1) k_stream_collide_v(c
                                                           const typename S::T* __restrict__ fin,
                                                           typename S::T* __restrict__ fout,
                                                           const uint8_t* __restrict__ cls, int gs, int zrev,
-                                                          const __grid_constant__ SampleOut O) {
+                                                          const __grid_constant__ SampleOut O,
+                                                          const __grid_constant__ DirPtrs<typename S::T> D) {
   SampleSums acc;
-  bulk_cells<L, S, V, BGK, SMP>(P, fin, fout, cls, gs, (blockIdx.x * blockDim.x + threadIdx.x) * V,
+  bulk_cells<L, S, V, BGK, SMP, false, true>(P, fin, fout, cls, gs, (blockIdx.x * blockDim.x + threadIdx.x) * V,
                                 blockIdx.y * blockDim.y + threadIdx.y,
-                                zrev ? (int)(gridDim.z - 1u - blockIdx.z) : (int)blockIdx.z, &O, &acc);
+                                zrev ? (int)(gridDim.z - 1u - blockIdx.z) : (int)blockIdx.z, &O, &acc, &D);
   if constexpr (SMP) smp_flush(acc, O.sets, global_warp_id());
 }
 
@@ -1958,7 +1997,7 @@ __global__ void __launch_bounds__(LC_THREADS, LC_BLOCKS_PER_SM) k_stream_collide
     const float2 wd = make_float2(cl_wall_dist(sw.x), cl_wall_dist(sw.y));
     const bool store = inside && (cv & 0x03030303u) == 0u;
     typename S::T* ob = fout + idx0;
-    collide_shifted2x<L, BGK>(
+    collide_shifted2x<L, BGK, SP_TEST>(
         P, h, x0,
         [&](auto I, float2 v) {
           constexpr int i = decltype(I)::value;
@@ -3330,14 +3369,26 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout, const SampleO
       // the bulk kernel on the main stream, concurrently with the auxiliary work; steps writing
       // buffer 1 sweep z upwards, steps writing buffer 0 downwards
       const int zrev = fout == s->f[0] ? 1 : 0;
+      // the vectorised kernel's per-direction plane bases for this step (pointer arithmetic on
+      // integers: a base may lie before the buffer; the cells that use it index into it)
+      DirPtrs<typename S::T> dp;
+      {
+        const int64_t N = (int64_t)s->kp.n, sy = s->dims.nx, sz = (int64_t)s->dims.nx * s->dims.ny;
+        for (int i = 0; i < L::Q; i++) {
+          const int64_t off = (int64_t)i * N - (int64_t)L::c[i][1] * sy - (int64_t)(L::DIM == 3 ? L::c[i][2] : 0) * sz;
+          dp.in[i] = (const typename S::T*)((uintptr_t)fin + (uintptr_t)(off * (int64_t)sizeof(typename S::T)));
+          dp.out[i] = (typename S::T*)fout + (size_t)i * (size_t)N;
+        }
+        for (int i = L::Q; i < 19; i++) dp.in[i] = nullptr, dp.out[i] = nullptr;
+      }
 #define WT_LAUNCH_V(VV, MB)                                                                                     \
   do {                                                                                                             \
     if (s->kp.collision == 1u)                                                                                     \
       k_stream_collide_v<L, S, VV, MB, true><<<grid, block, 0, s->stream>>>(                                       \
-          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, none);                      \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, none, dp);                  \
     else                                                                                                           \
       k_stream_collide_v<L, S, VV, MB, false><<<grid, block, 0, s->stream>>>(                                      \
-          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, none);                      \
+          s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, none, dp);                  \
   } while (0)
       const int mb = s->sc_kernel;
       if constexpr (L::DIM == 3) {
@@ -3387,14 +3438,14 @@ static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout, const SampleO
         const bool bgk = s->kp.collision == 1u;
         if (V == 2) {
           if (bgk) k_stream_collide_v<L, S, 2, 0, true, true><<<grid, block, 0, s->stream>>>(
-                       s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, *smp);
+                       s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, *smp, dp);
           else k_stream_collide_v<L, S, 2, 4, false, true><<<grid, block, 0, s->stream>>>(
-                   s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, *smp);
+                   s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, *smp, dp);
         } else {
           if (bgk) k_stream_collide_v<L, S, 4, 0, true, true><<<grid, block, 0, s->stream>>>(
-                       s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, *smp);
+                       s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, *smp, dp);
           else k_stream_collide_v<L, S, 4, 0, false, true><<<grid, block, 0, s->stream>>>(
-                   s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, *smp);
+                   s->kp, (const typename S::T*)fin, (typename S::T*)fout, s->cls, s->gs, zrev, *smp, dp);
         }
       } else if (V == 2) {
         if (mb == 2) WT_LAUNCH_V(2, 2);
