@@ -199,6 +199,18 @@ int wt_set_wheels(wt_solver* s, const wt_wheel* w, int32_t count);
 int wt_voxelize(wt_solver* s, const float* pos, int64_t nverts, const uint32_t* idx, int64_t ntri,
                 const float m[16], const wt_wheel* wheels, int32_t nwheels, wt_voxel_info* info);
 
+/* The same uploads queued the way the reference queues them (SolverGPU.uploadFlags /
+ * uploadSdf, SolverGPU.ts:312-322, 342-345: device.queue.writeBuffer, which returns before the
+ * copy is done): the copy starts at once on the handle's upload copy stream, overlapping any
+ * steps in flight, and the geometry takes effect for every call that follows, exactly as after
+ * wt_upload_flags / wt_upload_sdf (unchanged geometry keeps the classification and the captured
+ * step graphs). The host buffer must stay valid and unchanged until the next call on the handle
+ * that reads or writes the geometry (a step, sample, geometry read, voxelization, tracer,
+ * streamline or derived-field call, a synchronous upload, or wt_sync) has returned. The copy
+ * overlaps other work only from page-locked host memory. */
+int wt_upload_flags_async(wt_solver* s, const uint32_t* flags, int64_t n);
+int wt_upload_sdf_async(wt_solver* s, const float* d, int64_t n);
+
 /* ---- time stepping ---------------------------------------------------------------------- */
 /* SolverGPU.encodeSteps (SolverGPU.ts:204-222): `steps` fused pull-stream + collide steps. */
 int wt_step(wt_solver* s, int32_t steps);
@@ -207,6 +219,18 @@ int wt_step(wt_solver* s, int32_t steps);
 int wt_sample(wt_solver* s, wt_stats* out);
 /* LbmSolver.stepAndSample (types.ts:14, SolverGPU.ts:292-309). */
 int wt_step_and_sample(wt_solver* s, int32_t steps, wt_stats* out);
+/* The same call in the reference's asynchronous form (stepAndSample returns a Promise that
+ * resolves after sampleBuf.mapAsync, SolverGPU.ts:292-309): wt_step_and_sample_async queues the
+ * steps, the sampling pass and the copy of the statistics and returns at once; wt_sample_wait
+ * blocks until that sample is done and returns it. Uploads, readbacks and further steps may be
+ * queued in between; another sample (wt_sample, wt_step_and_sample, wt_step_and_sample_async,
+ * wt_batch_sample) before wt_sample_wait fails with WT_E_STATE, and wt_sample_wait without a
+ * pending sample fails with WT_E_STATE. */
+int wt_step_and_sample_async(wt_solver* s, int32_t steps);
+int wt_sample_wait(wt_solver* s, wt_stats* out);
+/* Waits until every queued step, sample, upload and readback of the handle has completed
+ * (applying staged asynchronous uploads first). */
+int wt_sync(wt_solver* s);
 
 /* ---- readback / checkpoint -------------------------------------------------------------- */
 /* SolverGPU.readFlags (SolverGPU.ts:347-356). */
@@ -225,6 +249,12 @@ int wt_read_velocity(wt_solver* s, float* out4, int64_t n);
 /* The same field in its storage format, the reference texture's rgba16float: 4 IEEE binary16 per
  * cell (8 bytes), copied without widening. */
 int wt_read_velocity_half4(wt_solver* s, void* out_half4, int64_t n);
+/* The same readback queued (the reference reads its fields through mapAsync, SolverGPU.ts:347-369):
+ * the copy starts on the handle's readback copy stream once everything queued so far has
+ * completed, and the call returns at once. The next sampling pass that rewrites the field waits
+ * for the copy; out_half4 holds the field after wt_sync (or any later call that waits for the
+ * handle's work). Overlaps other work only into page-locked host memory. */
+int wt_read_velocity_half4_async(wt_solver* s, void* out_half4, int64_t n);
 /* meanA (ux, uy, uz, rho EMA, 4 f32 per cell) and meanB (<u.u> EMA, 1 f32 per cell). */
 int wt_read_means(wt_solver* s, float* mean4, float* meanb, int64_t n);
 

@@ -520,8 +520,9 @@ def test_batch_matches_members_stepped_alone(gpu):
 
 def test_reuploading_unchanged_geometry_keeps_the_classification(gpu):
     """Uploads land in a staging buffer and replace the geometry only when it differs: re-uploading
-    the same flags and wall distances adds only the compare (and sdf encode) launches, and the run
-    stays bit-identical to one without the re-upload."""
+    the same flags and wall distances adds only the compare launches (the comparison and the
+    hand-over of its result word; the sdf encode before the sdf comparison), and the run stays
+    bit-identical to one without the re-upload."""
     dims = (48, 20, 16)
     params = dict(PARAM_SETS["freeslip_reg"], precision="f16")
     flags, sdf, wheels = scene(dims)
@@ -536,7 +537,7 @@ def test_reuploading_unchanged_geometry_keeps_the_classification(gpu):
     a.upload_sdf(sdf)
     a.step(12)
     b.step(12)
-    assert a.launches - la == b.launches - lb + 3  # diff (flags), encode + diff (sdf)
+    assert a.launches - la == b.launches - lb + 5  # diff + take (flags), encode + diff + take (sdf)
     np.testing.assert_array_equal(a.read_populations(), b.read_populations())
     a.destroy()
     b.destroy()

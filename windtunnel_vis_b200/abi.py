@@ -171,11 +171,16 @@ def _sig(lib):
         "wt_step_count": ([S], i64),
         "wt_upload_flags": ([S, v, i64], C.c_int),
         "wt_upload_sdf": ([S, v, i64], C.c_int),
+        "wt_upload_flags_async": ([S, v, i64], C.c_int),
+        "wt_upload_sdf_async": ([S, v, i64], C.c_int),
         "wt_set_wheels": ([S, P(Wheel), i32], C.c_int),
         "wt_voxelize": ([S, v, i64, v, i64, v, P(Wheel), i32, P(VoxelInfo)], C.c_int),
         "wt_step": ([S, i32], C.c_int),
         "wt_sample": ([S, P(Stats)], C.c_int),
         "wt_step_and_sample": ([S, i32, P(Stats)], C.c_int),
+        "wt_step_and_sample_async": ([S, i32], C.c_int),
+        "wt_sample_wait": ([S, P(Stats)], C.c_int),
+        "wt_sync": ([S], C.c_int),
         "wt_read_flags": ([S, v, i64], C.c_int),
         "wt_read_sdf": ([S, v, i64], C.c_int),
         "wt_population_bytes": ([S], i64),
@@ -183,6 +188,7 @@ def _sig(lib):
         "wt_write_populations": ([S, v, i64], C.c_int),
         "wt_read_velocity": ([S, v, i64], C.c_int),
         "wt_read_velocity_half4": ([S, v, i64], C.c_int),
+        "wt_read_velocity_half4_async": ([S, v, i64], C.c_int),
         "wt_read_means": ([S, v, v, i64], C.c_int),
         "wt_advect_tracers": ([S, P(TracerParams)], C.c_int),
         "wt_read_tracers": ([S, v, i64, v, i64], C.c_int),

@@ -73,7 +73,7 @@ void free_all(wt_solver* s) {
                   s->partials, s->result_dev, s->err_dev, s->tr_state, s->tr_hist, s->bnd, s->bnd_count,
                   s->bcell, s->brec, s->bgam, s->vox_pos, s->vox_idx, s->vox_info,
                   s->dvort, s->dstat, s->dmean, s->exp_buf, s->probe_buf, s->closure_dev, s->stage,
-                  s->diff_dev, s->lc_rows, s->solids, s->smp_sets, s->ps_bar};
+                  s->diff_dev, s->lc_rows, s->solids, s->smp_sets, s->ps_bar, s->stage_flags, s->stage_sdf};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->result_host) cudaFreeHost(s->result_host);
@@ -88,6 +88,10 @@ void free_all(wt_solver* s) {
     if (g) cudaGraphExecDestroy(g);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
+  for (cudaEvent_t e : {s->ev_up, s->ev_src, s->ev_rd, s->ev_smp, s->ev_swap})
+    if (e) cudaEventDestroy(e);
+  if (s->copy_up) cudaStreamDestroy(s->copy_up);
+  if (s->copy_rd) cudaStreamDestroy(s->copy_rd);
   if (s->aux) cudaStreamDestroy(s->aux);
   if (s->stream) cudaStreamDestroy(s->stream);
 }
@@ -134,6 +138,14 @@ __global__ void k_diff_words(const uint32_t* __restrict__ a, const uint32_t* __r
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     d = d || a[i] != b[i];
   if (__syncthreads_or(d) && threadIdx.x == 0) atomicOr(out, 1u);
+}
+
+// *host = *word, then *word = 0: the difference word reaches the host through mapped page-locked
+// memory (a store over the bus, not a copy-engine transfer, so it never queues behind a large
+// asynchronous readback), and the word is clear for the next comparison
+__global__ void k_take_word(uint32_t* __restrict__ word, volatile uint32_t* host) {
+  *host = *word;
+  *word = 0u;
 }
 
 __global__ void k_clear_stats(float4* __restrict__ meanA, float* __restrict__ meanB, size_t n) {
@@ -261,7 +273,7 @@ void decode(const wt_solver* s, const double* d, wt_stats* out) {
   out->max_u = std::sqrt(d[3] > 0 ? d[3] : 0.0);
   out->rho_ref = d[5] > 0 ? d[4] / d[5] : 1.0;
   out->unstable = (d[6] > 0 || !std::isfinite(d[0]) || d[3] > 0.25) ? 1 : 0;
-  out->step = s->step_count;
+  out->step = s->sample_step;
 }
 
 }  // namespace
@@ -417,7 +429,8 @@ int wt_create(const wt_dims* d, const wt_params* p, wt_solver** out) {
 void wt_destroy(wt_solver* s) {
   if (!s) return;
   DeviceGuard g(s->device);
-  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (cudaStream_t st : {s->stream, s->aux, s->copy_up, s->copy_rd})
+    if (st) cudaStreamSynchronize(st);
   free_all(s);
   delete s;
 }
@@ -465,35 +478,116 @@ int wt_clear_stats(wt_solver* s) {
 
 int64_t wt_step_count(const wt_solver* s) { return s ? s->step_count : -1; }
 
+// The difference words: one per comparison (0: synchronous uploads, 1 and 2: the asynchronous
+// flags and wall-distance uploads), on the device and in mapped page-locked host memory.
+enum { DIFF_SYNC = 0, DIFF_FLAGS = 1, DIFF_SDF = 2, DIFF_WORDS = 4 };
+static int ensure_diff(wt_solver* s) {
+  if (s->diff_host_dev) return WT_OK;
+  if ((!s->diff_dev && cudaMalloc((void**)&s->diff_dev, DIFF_WORDS * 4) != cudaSuccess) ||
+      (!s->diff_host && cudaMallocHost((void**)&s->diff_host, DIFF_WORDS * 4) != cudaSuccess)) {
+    cudaGetLastError();
+    return fail(s, WT_E_OOM, "upload comparison words");
+  }
+  WT_CUDA(s, cudaMemset(s->diff_dev, 0, DIFF_WORDS * 4), "upload comparison words");
+  WT_CUDA(s, cudaHostGetDevicePointer((void**)&s->diff_host_dev, s->diff_host, 0), "upload comparison words");
+  return WT_OK;
+}
+
+// queues the comparison of *staged with *cur on `st`: difference word w lands in diff_host[w]
+static cudaError_t queue_compare(wt_solver* s, const uint32_t* staged, const uint32_t* cur, int w, cudaStream_t st) {
+  k_diff_words<<<grid_for(s->n), 256, 0, st>>>(staged, cur, s->n, s->diff_dev + w);
+  k_take_word<<<1, 1, 0, st>>>(s->diff_dev + w, s->diff_host_dev + w);
+  s->launches += 2;
+  return cudaGetLastError();
+}
+static bool differs(const wt_solver* s, int w) { return reinterpret_cast<volatile uint32_t*>(s->diff_host)[w] != 0u; }
+
 // Compares the staged upload with *cur on the device; when they differ the stage becomes the
 // current buffer (the old one becomes the stage) and `changed` is set.
-int commit_stage(wt_solver* s, uint32_t** cur, bool* changed, const char* what) {
-  WT_CUDA(s, cudaMemsetAsync(s->diff_dev, 0, 4, s->stream), what);
-  k_diff_words<<<grid_for(s->n), 256, 0, s->stream>>>(s->stage, *cur, s->n, s->diff_dev);
-  s->launches++;
-  WT_CUDA(s, cudaGetLastError(), what);
-  WT_CUDA(s, cudaMemcpyAsync(s->diff_host, s->diff_dev, 4, cudaMemcpyDeviceToHost, s->stream), what);
+static int commit_stage(wt_solver* s, uint32_t** cur, bool* changed, const char* what) {
+  WT_CUDA(s, queue_compare(s, s->stage, *cur, DIFF_SYNC, s->stream), what);
   WT_CUDA(s, cudaStreamSynchronize(s->stream), what);
-  *changed = *s->diff_host != 0u;
+  *changed = differs(s, DIFF_SYNC);
   if (*changed) std::swap(*cur, s->stage);
   return WT_OK;
 }
 
-int ensure_stage(wt_solver* s) {
-  if (s->stage) return WT_OK;
-  if (cudaMalloc((void**)&s->stage, s->n * 4) != cudaSuccess || cudaMalloc((void**)&s->diff_dev, 4) != cudaSuccess ||
-      cudaMallocHost((void**)&s->diff_host, 4) != cudaSuccess) {
+static int ensure_stage(wt_solver* s) {
+  int rc = ensure_diff(s);
+  if (rc || s->stage) return rc;
+  if (cudaMalloc((void**)&s->stage, s->n * 4) != cudaSuccess) {
     cudaGetLastError();
     return fail(s, WT_E_OOM, "upload staging buffer");
   }
   return WT_OK;
 }
 
+// Applies the asynchronous uploads staged since the last call. Each was compared with the current
+// buffer on the upload copy stream right after its copy (the comparison runs while the steps
+// before it run), so applying one needs no round trip through the compute stream: once the
+// copies and comparisons are done, a staged buffer that differs becomes the current one (flags
+// first, then wall distances, as the synchronous uploads would have). Every call that reads or
+// writes the geometry runs this first, so an asynchronous upload is seen by everything queued
+// after it. A buffer that stops being current may still be read by steps in flight: the next
+// upload into it waits for them (ev_swap).
+static int settle_uploads(wt_solver* s) {
+  if (!s->up_flags && !s->up_sdf) return WT_OK;
+  WT_CUDA(s, cudaEventSynchronize(s->ev_up), "apply uploads");
+  bool swapped = false;
+  if (s->up_flags) {
+    s->up_flags = false;
+    if (differs(s, DIFF_FLAGS)) {
+      std::swap(s->flags, s->stage_flags);
+      s->cls_dirty = true;
+      swapped = true;
+    }
+  }
+  if (s->up_sdf) {
+    s->up_sdf = false;
+    if (differs(s, DIFF_SDF)) {
+      std::swap(s->sdf, s->stage_sdf);
+      s->tab_dirty = true;  // the wall distances set the link records, and the graphs hold the buffer
+      swapped = true;
+    }
+  }
+  if (swapped) {
+    WT_CUDA(s, cudaEventRecord(s->ev_swap, s->stream), "apply uploads");
+    s->swap_pending = true;
+  }
+  return WT_OK;
+}
+
+// the copy streams and events of the asynchronous calls, created on first use
+static int ensure_async(wt_solver* s) {
+  if (s->copy_up) return WT_OK;
+  cudaError_t e = cudaStreamCreateWithFlags(&s->copy_rd, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_up, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_src, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_rd, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_smp, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_swap, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy_up, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_fail(s, e, "asynchronous copy streams");
+  return WT_OK;
+}
+
+// Kernels that write the velocity field wait for the asynchronous readbacks issued before them.
+static int order_after_reads(wt_solver* s) {
+  if (s->rd_issued) WT_CUDA(s, cudaStreamWaitEvent(s->stream, s->ev_rd, 0), "order after readback");
+  return WT_OK;
+}
+
+static int no_pending_sample(wt_solver* s, const char* what) {
+  if (!s->sample_pending) return WT_OK;
+  return fail(s, WT_E_STATE, std::string(what) + ": an asynchronous sample is pending (call wt_sample_wait first)");
+}
+
 int wt_upload_flags(wt_solver* s, const uint32_t* flags, int64_t n) {
   if (!s || !flags) return WT_E_INVALID;
   if ((size_t)n != s->n) return fail(s, WT_E_INVALID, "wt_upload_flags: n != nx*ny*nz");
   DeviceGuard g(s->device);
-  int rc = ensure_stage(s);
+  int rc = settle_uploads(s);
+  if (!rc) rc = ensure_stage(s);
   if (rc) return rc;
   WT_CUDA(s, cudaMemcpyAsync(s->stage, flags, s->n * 4, cudaMemcpyHostToDevice, s->stream), "upload flags");
   bool changed = false;
@@ -507,7 +601,8 @@ int wt_upload_sdf(wt_solver* s, const float* d, int64_t n) {
   if (!s || !d) return WT_E_INVALID;
   if ((size_t)n != s->n) return fail(s, WT_E_INVALID, "wt_upload_sdf: n != nx*ny*nz");
   DeviceGuard g(s->device);
-  int rc = ensure_stage(s);
+  int rc = settle_uploads(s);
+  if (!rc) rc = ensure_stage(s);
   if (rc) return rc;
   WT_CUDA(s, cudaMemcpyAsync(s->stage, d, s->n * 4, cudaMemcpyHostToDevice, s->stream), "upload sdf");
   k_encode_sdf<<<grid_for(s->n), 256, 0, s->stream>>>(s->stage, s->n);
@@ -520,6 +615,42 @@ int wt_upload_sdf(wt_solver* s, const float* d, int64_t n) {
   // buffer's address
   if (changed) s->tab_dirty = true;
   return WT_OK;
+}
+
+// One staged asynchronous upload, queued on copy_up: the copy into the stage, the sdf encoding
+// (wall distances) and the comparison with the current buffer; settle_uploads applies it.
+static int upload_async(wt_solver* s, bool sdf, const void* src, int64_t n, const char* what) {
+  if ((size_t)n != s->n) return fail(s, WT_E_INVALID, std::string(what) + ": n != nx*ny*nz");
+  DeviceGuard g(s->device);
+  int rc = ensure_async(s);
+  if (!rc) rc = ensure_diff(s);
+  if (rc) return rc;
+  uint32_t** stage = sdf ? &s->stage_sdf : &s->stage_flags;
+  if (!*stage) WT_CUDA(s, cudaMalloc((void**)stage, s->n * 4), "cudaMalloc(upload stage)");
+  // a stage that was the current buffer until the last swap: steps queued before it may read it
+  if (s->swap_pending) {
+    WT_CUDA(s, cudaStreamWaitEvent(s->copy_up, s->ev_swap, 0), what);
+    s->swap_pending = false;
+  }
+  WT_CUDA(s, cudaMemcpyAsync(*stage, src, s->n * 4, cudaMemcpyHostToDevice, s->copy_up), what);
+  if (sdf) {
+    k_encode_sdf<<<grid_for(s->n), 256, 0, s->copy_up>>>(*stage, s->n);
+    s->launches++;
+  }
+  WT_CUDA(s, queue_compare(s, *stage, sdf ? s->sdf : s->flags, sdf ? DIFF_SDF : DIFF_FLAGS, s->copy_up), what);
+  WT_CUDA(s, cudaEventRecord(s->ev_up, s->copy_up), what);
+  (sdf ? s->up_sdf : s->up_flags) = true;
+  return WT_OK;
+}
+
+int wt_upload_flags_async(wt_solver* s, const uint32_t* flags, int64_t n) {
+  if (!s || !flags) return WT_E_INVALID;
+  return upload_async(s, false, flags, n, "wt_upload_flags_async");
+}
+
+int wt_upload_sdf_async(wt_solver* s, const float* d, int64_t n) {
+  if (!s || !d) return WT_E_INVALID;
+  return upload_async(s, true, d, n, "wt_upload_sdf_async");
 }
 
 int wt_set_wheels(wt_solver* s, const wt_wheel* w, int32_t count) {
@@ -585,7 +716,8 @@ int wt_voxelize(wt_solver* s, const float* pos, int64_t nverts, const uint32_t* 
                 const wt_wheel* wheels, int32_t nwheels, wt_voxel_info* info) {
   if (!s || !info || !m || ntri < 0 || nverts < 0 || (ntri > 0 && (!pos || !idx))) return WT_E_INVALID;
   DeviceGuard g(s->device);
-  int rc = wt_set_wheels(s, wheels, nwheels);
+  int rc = settle_uploads(s);  // staged uploads land before the voxelizer overwrites the geometry
+  if (!rc) rc = wt_set_wheels(s, wheels, nwheels);
   if (rc) return rc;
   std::memset(info, 0, sizeof *info);
   if (ntri == 0) {
@@ -655,7 +787,8 @@ int wt_voxelize(wt_solver* s, const float* pos, int64_t nverts, const uint32_t* 
 int wt_step(wt_solver* s, int32_t steps) {
   if (!s || steps < 0) return WT_E_INVALID;
   DeviceGuard g(s->device);
-  int rc = ensure_classified(s);
+  int rc = settle_uploads(s);
+  if (!rc) rc = ensure_classified(s);
   if (!rc) rc = ensure_init(s);
   if (rc) return rc;
   int32_t k = 0;
@@ -705,31 +838,28 @@ int wt_step(wt_solver* s, int32_t steps) {
   return WT_OK;
 }
 
-int wt_sample(wt_solver* s, wt_stats* out) {
-  if (!s || !out) return WT_E_INVALID;
-  DeviceGuard g(s->device);
-  int rc = ensure_init(s);
-  if (rc) return rc;
-  rc = ensure_classified(s);  // the macro pass reads the class byte
+// Queues the macro pass and the copies of its result and of the error word to pinned memory.
+static int enqueue_sample(wt_solver* s) {
+  int rc = settle_uploads(s);
+  if (!rc) rc = ensure_init(s);
+  if (!rc) rc = ensure_classified(s);  // the macro pass reads the class byte
+  if (!rc) rc = order_after_reads(s);
   if (rc) return rc;
   WT_CUDA(s, wt::launch_macro(s), "macro");
   WT_CUDA(s, cudaMemcpyAsync(s->result_host, s->result_dev, RESULT_BYTES, cudaMemcpyDeviceToHost, s->stream), "read result");
   WT_CUDA(s, cudaMemcpyAsync(s->err_host, s->err_dev, 4, cudaMemcpyDeviceToHost, s->stream), "read error word");
-  WT_CUDA(s, cudaStreamSynchronize(s->stream), "sample");
-  if (*s->err_host != 0) return check_err_flag(s);
-  decode(s, s->result_host, out);
+  s->sample_step = s->step_count;
   return WT_OK;
 }
 
-int wt_step_and_sample(wt_solver* s, int32_t steps, wt_stats* out) {
-  if (!s || !out || steps < 0) return WT_E_INVALID;
-  if (steps == 0) return wt_sample(s, out);
-  DeviceGuard g(s->device);
-  int rc = wt_step(s, 0);  // classification and initialisation
+// Queues `steps` steps, the last with the sampling pass fused, and the result copies.
+static int enqueue_step_and_sample(wt_solver* s, int32_t steps) {
+  if (steps == 0) return enqueue_sample(s);
+  int rc = wt_step(s, 0);  // uploads, classification and initialisation
   if (rc) return rc;
   if (!wt::sample_step_ok(s)) {
     rc = wt_step(s, steps);
-    return rc ? rc : wt_sample(s, out);
+    return rc ? rc : enqueue_sample(s);
   }
   // The last step runs the sampling pass's per-cell work on what it stores (no second read of the
   // populations), then the wall force and the solid cells, then the final reduction. With solid
@@ -737,6 +867,7 @@ int wt_step_and_sample(wt_solver* s, int32_t steps, wt_stats* out) {
   // (the persistent launch takes all steps but the last in one launch instead)
   const bool tail = steps >= WT_SAMPLE_TAIL && s->sc_kernel != WT_LAUNCH_PERSISTENT;
   rc = wt_step(s, steps - (tail ? WT_SAMPLE_TAIL : 1));
+  if (!rc) rc = order_after_reads(s);  // the sampling step writes the velocity field
   if (rc) return rc;
   if (tail && s->solid_ok[0] && s->solid_ok[1]) {
     if (!s->sample_graph[s->parity]) {
@@ -759,15 +890,87 @@ int wt_step_and_sample(wt_solver* s, int32_t steps, wt_stats* out) {
   WT_CUDA(s, cudaMemcpyAsync(s->result_host, s->result_dev, RESULT_BYTES, cudaMemcpyDeviceToHost, s->stream),
           "read result");
   WT_CUDA(s, cudaMemcpyAsync(s->err_host, s->err_dev, 4, cudaMemcpyDeviceToHost, s->stream), "read error word");
-  WT_CUDA(s, cudaStreamSynchronize(s->stream), "sample");
+  s->sample_step = s->step_count;
+  return WT_OK;
+}
+
+// the result of a completed sample: error word first, then the decoded statistics
+static int finish_sample(wt_solver* s, wt_stats* out) {
   if (*s->err_host != 0) return check_err_flag(s);
   decode(s, s->result_host, out);
+  return WT_OK;
+}
+
+int wt_sample(wt_solver* s, wt_stats* out) {
+  if (!s || !out) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  int rc = no_pending_sample(s, "wt_sample");
+  if (!rc) rc = enqueue_sample(s);
+  if (rc) return rc;
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "sample");
+  return finish_sample(s, out);
+}
+
+int wt_step_and_sample(wt_solver* s, int32_t steps, wt_stats* out) {
+  if (!s || !out || steps < 0) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  int rc = no_pending_sample(s, "wt_step_and_sample");
+  if (!rc) rc = enqueue_step_and_sample(s, steps);
+  if (rc) return rc;
+  WT_CUDA(s, cudaStreamSynchronize(s->stream), "sample");
+  return finish_sample(s, out);
+}
+
+int wt_step_and_sample_async(wt_solver* s, int32_t steps) {
+  if (!s || steps < 0) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  int rc = no_pending_sample(s, "wt_step_and_sample_async");
+  if (!rc) rc = ensure_async(s);
+  if (!rc) rc = enqueue_step_and_sample(s, steps);
+  if (rc) return rc;
+  WT_CUDA(s, cudaEventRecord(s->ev_smp, s->stream), "sample event");
+  s->sample_pending = true;
+  return WT_OK;
+}
+
+int wt_sample_wait(wt_solver* s, wt_stats* out) {
+  if (!s || !out) return WT_E_INVALID;
+  if (!s->sample_pending) return fail(s, WT_E_STATE, "wt_sample_wait: no asynchronous sample is pending");
+  DeviceGuard g(s->device);
+  s->sample_pending = false;
+  WT_CUDA(s, cudaEventSynchronize(s->ev_smp), "sample");
+  return finish_sample(s, out);
+}
+
+int wt_read_velocity_half4_async(wt_solver* s, void* out_half4, int64_t n) {
+  if (!s || !out_half4 || (size_t)n != s->n) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  int rc = ensure_async(s);
+  if (rc) return rc;
+  // the copy starts once everything queued so far on the compute stream has completed
+  WT_CUDA(s, cudaEventRecord(s->ev_src, s->stream), "read velocity");
+  WT_CUDA(s, cudaStreamWaitEvent(s->copy_rd, s->ev_src, 0), "read velocity");
+  WT_CUDA(s, cudaMemcpyAsync(out_half4, s->vel, s->n * 8, cudaMemcpyDeviceToHost, s->copy_rd), "read velocity");
+  WT_CUDA(s, cudaEventRecord(s->ev_rd, s->copy_rd), "read velocity");
+  s->rd_issued = true;
+  return WT_OK;
+}
+
+int wt_sync(wt_solver* s) {
+  if (!s) return WT_E_INVALID;
+  DeviceGuard g(s->device);
+  int rc = settle_uploads(s);
+  if (rc) return rc;
+  for (cudaStream_t st : {s->stream, s->aux, s->copy_up, s->copy_rd})
+    if (st) WT_CUDA(s, cudaStreamSynchronize(st), "wt_sync");
   return WT_OK;
 }
 
 int wt_read_flags(wt_solver* s, uint32_t* out, int64_t n) {
   if (!s || !out || (size_t)n != s->n) return WT_E_INVALID;
   DeviceGuard g(s->device);
+  int rc = settle_uploads(s);
+  if (rc) return rc;
   WT_CUDA(s, cudaMemcpyAsync(out, s->flags, s->n * 4, cudaMemcpyDeviceToHost, s->stream), "read flags");
   WT_CUDA(s, cudaStreamSynchronize(s->stream), "read flags");
   return WT_OK;
@@ -776,6 +979,8 @@ int wt_read_flags(wt_solver* s, uint32_t* out, int64_t n) {
 int wt_read_sdf(wt_solver* s, uint32_t* out, int64_t n) {
   if (!s || !out || (size_t)n != s->n) return WT_E_INVALID;
   DeviceGuard g(s->device);
+  int rc = settle_uploads(s);
+  if (rc) return rc;
   WT_CUDA(s, cudaMemcpyAsync(out, s->sdf, s->n * 4, cudaMemcpyDeviceToHost, s->stream), "read sdf");
   WT_CUDA(s, cudaStreamSynchronize(s->stream), "read sdf");
   return WT_OK;
@@ -836,6 +1041,7 @@ int wt_read_means(wt_solver* s, float* mean4, float* meanb, int64_t n) {
 int wt_derive_fields(wt_solver* s) {
   if (!s) return WT_E_INVALID;
   DeviceGuard g(s->device);
+  if (int rc = settle_uploads(s)) return rc;
   for (uint2** b : {&s->dvort, &s->dstat, &s->dmean})
     if (!*b) WT_CUDA(s, cudaMalloc((void**)b, s->n * 8), "cudaMalloc(derived fields)");
   WT_CUDA(s, wt::launch_derive(s), "derive fields");
@@ -909,7 +1115,7 @@ int wt_streamlines(wt_solver* s, const wt_streamline_params* p, float* pts4, int
   if (!s || !p || !pts4 || n != (int64_t)p->seeds * (int64_t)p->points) return WT_E_INVALID;
   if (p->seeds == 0 || p->points == 0) return WT_OK;
   DeviceGuard g(s->device);
-  int rc = WT_OK;
+  int rc = settle_uploads(s);
   if (p->use_mean) rc = wt_derive_fields(s);
   if (!rc) rc = ensure_export(s, (size_t)n);
   if (rc) return rc;
@@ -954,6 +1160,7 @@ int wt_advect_tracers(wt_solver* s, const wt_tracer_params* p) {
   if (p->trail == 0 || p->head >= p->trail) return fail(s, WT_E_INVALID, "wt_advect_tracers: need trail >= 1 and head < trail");
   if (p->emitter == 1 && p->nozzles == 0) return fail(s, WT_E_INVALID, "wt_advect_tracers: rake emitter needs nozzles >= 1");
   DeviceGuard g(s->device);
+  if (int rc = settle_uploads(s)) return rc;
   int rc = ensure_tracers(s, p->count, p->trail);
   if (rc) return rc;
   if (p->count == 0) return WT_OK;
@@ -1353,7 +1560,8 @@ int wt_batch_step(wt_batch* b, int32_t steps) {
   if (!b || steps < 0) return WT_E_INVALID;
   DeviceGuard g(b->device);
   for (wt_solver* s : b->m) {
-    int rc = ensure_classified(s);
+    int rc = settle_uploads(s);
+    if (!rc) rc = ensure_classified(s);
     if (!rc) rc = ensure_init(s);
     if (rc) return bfail(b, rc, std::string("member: ") + s->err);
   }
@@ -1420,12 +1628,16 @@ int wt_batch_sample(wt_batch* b, wt_stats* out) {
   DeviceGuard g(b->device);
   // the sampling passes of all members are queued first, then read back together
   for (wt_solver* s : b->m) {
-    int rc = ensure_init(s);
+    int rc = no_pending_sample(s, "wt_batch_sample");
+    if (!rc) rc = settle_uploads(s);
+    if (!rc) rc = ensure_init(s);
     if (!rc) rc = ensure_classified(s);
+    if (!rc) rc = order_after_reads(s);
     if (rc) return bfail(b, rc, std::string("member: ") + s->err);
     cudaError_t e = wt::launch_macro(s);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(s->result_host, s->result_dev, RESULT_BYTES, cudaMemcpyDeviceToHost, s->stream);
+    s->sample_step = s->step_count;
     if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch sample: ") + cudaGetErrorString(e));
   }
   for (size_t k = 0; k < b->m.size(); k++) {

@@ -56,8 +56,9 @@ struct wt_solver {
   // uploads land here first and replace flags / sdf only when their content differs, so that
   // re-uploading unchanged geometry keeps the classification and the captured graphs
   uint32_t* stage = nullptr;
-  uint32_t* diff_dev = nullptr;   // device word: the staged words differ from the current ones
-  uint32_t* diff_host = nullptr;  // pinned copy
+  uint32_t* diff_dev = nullptr;   // device words: a staged buffer differs from the current one
+  uint32_t* diff_host = nullptr;  // pinned copies (written by k_take_word through their mapping)
+  uint32_t* diff_host_dev = nullptr;  // device address of diff_host
   uint8_t* cls = nullptr;
   bool cls_dirty = true;
   bool tab_dirty = false;  // link records need a rebuild (parameters or wheels changed)
@@ -133,6 +134,21 @@ struct wt_solver {
   int* err_dev = nullptr;   // device-side error word written by kernels with bounded waits
   int* err_host = nullptr;  // pinned copy
   int64_t launches = 0;
+  // asynchronous transfers (wt_*_async, created by the first such call): one copy stream per
+  // direction, so that an upload and a readback overlap each other and the compute stream
+  cudaStream_t copy_up = nullptr, copy_rd = nullptr;
+  uint32_t* stage_flags = nullptr;  // staged asynchronous uploads, applied by settle_uploads
+  uint32_t* stage_sdf = nullptr;
+  bool up_flags = false, up_sdf = false;  // a staged upload waits to be applied
+  cudaEvent_t ev_up = nullptr;   // on copy_up: after the last asynchronous upload and its comparison
+  cudaEvent_t ev_swap = nullptr; // on stream: after the steps that may read a buffer swapped out
+  bool swap_pending = false;     // the next asynchronous upload waits for ev_swap
+  cudaEvent_t ev_src = nullptr;  // on stream: the state an asynchronous readback copies
+  cudaEvent_t ev_rd = nullptr;   // on copy_rd: after the last asynchronous readback
+  bool rd_issued = false;        // ev_rd has been recorded: writers of `vel` wait for it
+  cudaEvent_t ev_smp = nullptr;  // on stream: after the result copy of an asynchronous sample
+  bool sample_pending = false;   // wt_step_and_sample_async issued, wt_sample_wait not yet called
+  int64_t sample_step = 0;       // step count of the last queued sample (its statistics' `step`)
   std::string err;
 };
 

@@ -51,6 +51,7 @@ class Solver:
         self.q = 19 if self.is3d else 9
         self.params = dict(params)
         self.precision = abi.PRECISION[self.params.get("precision", "f32") or "f32"]
+        self._async_refs = []  # host arrays of queued copies, released by sync / destroy
         h = C.c_void_p()
         d = abi.Dims(nx, ny, nz)
         rc = self._lib.wt_create(C.byref(d), C.byref(abi.make_params(self.params)), C.byref(h))
@@ -91,8 +92,9 @@ class Solver:
 
     def destroy(self):
         if getattr(self, "_h", None):
-            self._lib.wt_destroy(self._h)
+            self._lib.wt_destroy(self._h)  # waits for the queued copies first
             self._h = None
+        self._async_refs = []
 
     def __del__(self):
         try:
@@ -147,6 +149,21 @@ class Solver:
         a = np.ascontiguousarray(np.asarray(d).ravel(), np.float32)
         self._check(self._lib.wt_upload_sdf(self._h, _ptr(a), a.size))
 
+    def upload_flags_async(self, flags):
+        """uploadFlags queued (device.queue.writeBuffer): the copy overlaps the work in flight and
+        the geometry applies to every later call. The array (kept referenced here until `sync`)
+        must not change until the next call that reads the geometry; page-locked memory (e.g. a
+        pinned torch tensor's numpy view) lets the copy overlap."""
+        f = np.ascontiguousarray(np.asarray(flags).ravel(), np.uint32)
+        self._check(self._lib.wt_upload_flags_async(self._h, _ptr(f), f.size))
+        self._async_refs.append(f)
+
+    def upload_sdf_async(self, d):
+        """uploadSdf queued, as `upload_flags_async`."""
+        a = np.ascontiguousarray(np.asarray(d).ravel(), np.float32)
+        self._check(self._lib.wt_upload_sdf_async(self._h, _ptr(a), a.size))
+        self._async_refs.append(a)
+
     def set_wheels(self, wheels):
         arr, n = abi.make_wheels(list(wheels))
         self._check(self._lib.wt_set_wheels(self._h, arr, n))
@@ -178,6 +195,21 @@ class Solver:
         st = abi.Stats()
         self._check(self._lib.wt_step_and_sample(self._h, int(steps), C.byref(st)))
         return _stats_dict(st)
+
+    def step_and_sample_async(self, steps: int):
+        """stepAndSample in the reference's asynchronous form: queues the chunk and returns; the
+        statistics come from `sample_wait`."""
+        self._check(self._lib.wt_step_and_sample_async(self._h, int(steps)))
+
+    def sample_wait(self):
+        st = abi.Stats()
+        self._check(self._lib.wt_sample_wait(self._h, C.byref(st)))
+        return _stats_dict(st)
+
+    def sync(self):
+        """Waits for every queued step, sample, upload and readback of the handle."""
+        self._check(self._lib.wt_sync(self._h))
+        self._async_refs.clear()
 
     # ---- readback / checkpoint ---------------------------------------------------------------
     def read_flags(self):
@@ -219,6 +251,15 @@ class Solver:
             out = np.empty((self.n, 4), np.float16)
         assert out.dtype == np.float16 and out.shape == (self.n, 4) and out.flags["C_CONTIGUOUS"]
         self._check(self._lib.wt_read_velocity_half4(self._h, _ptr(out), self.n))
+        return out
+
+    def read_velocity_half_async(self, out):
+        """`read_velocity_half` queued: the copy into `out` (a C-contiguous (n, 4) float16 array,
+        page-locked for the copy to overlap) starts once the work queued so far is done; `out`
+        holds the field after `sync`."""
+        assert out.dtype == np.float16 and out.shape == (self.n, 4) and out.flags["C_CONTIGUOUS"]
+        self._check(self._lib.wt_read_velocity_half4_async(self._h, _ptr(out), self.n))
+        self._async_refs.append(out)
         return out
 
     def read_means(self):
