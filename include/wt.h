@@ -355,8 +355,14 @@ int wt_batch_sample(wt_batch* b, wt_stats* out);
  * blocks take the wall-cell chunks, face-row tiles and bulk tiles of every member from an atomic
  * counter, with a grid-wide barrier between steps. Members stay bit-identical to the same handles
  * stepped alone.
+ * on = WT_BATCH_QUEUE: under the same conditions, every step of every member is one launch of the
+ * same work queue (resident blocks taking wall chunks, face tiles and bulk tiles of all members
+ * from an atomic counter), without the grid barrier: the steps are separate launches, captured in
+ * the batch's CUDA graphs, so the population loads keep the read-only cache path. Members stay
+ * bit-identical to the same handles stepped alone.
  * on = 0 (default): the members' own kernels under one graph. */
 #define WT_BATCH_PERSISTENT 2
+#define WT_BATCH_QUEUE 3
 int wt_batch_set_fused(wt_batch* b, int32_t on);
 
 /* ---- learned LES closure (extension; no counterpart in the reference) -----------------------

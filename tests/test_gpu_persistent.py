@@ -89,3 +89,28 @@ def test_persistent_batch_matches_members_stepped_alone(gpu, prec):
     batch.destroy()
     for s in alone + members:
         s.destroy()
+
+
+@pytest.mark.parametrize("prec", ["f16", "f32"])
+def test_queue_batch_matches_members_stepped_alone(gpu, prec):
+    # the work queue launched once per step under the batch graphs (read-only-cache loads, no grid
+    # barrier): bit-identical to the members stepped alone, one launch per step for all members
+    cases = [((32, 14, 12), "belt_periodic_les"), ((48, 16, 14), "freeslip_reg"), ((64, 12, 10), "belt_periodic_les")]
+    alone = [_solver(d, dict(PARAM_SETS[p], precision=prec)) for d, p in cases]
+    members = [_solver(d, dict(PARAM_SETS[p], precision=prec)) for d, p in cases]
+    batch = Batch(members, queue=True)
+    for n in (3, 16, 9, 24):
+        for s in alone:
+            s.step(n)
+        l0 = [t.launches for t in members]
+        batch.step(n)
+        if n == 16:
+            # graph replays: one work-queue launch per step, counted on the first member
+            assert members[0].launches == l0[0] + 16 and [t.launches for t in members[1:]] == l0[1:]
+        for s, t in zip(alone, members):
+            np.testing.assert_array_equal(s.read_populations(), t.read_populations())
+    for s, st in zip(alone, batch.sample()):
+        assert s.sample()["raw"].tolist() == st["raw"].tolist()
+    batch.destroy()
+    for s in alone + members:
+        s.destroy()

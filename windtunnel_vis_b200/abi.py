@@ -17,6 +17,7 @@ WT_E_NO_DEVICE = -6
 WT_LAUNCH_ROW_PIPELINE = 8
 WT_LAUNCH_PERSISTENT = 9
 WT_BATCH_PERSISTENT = 2
+WT_BATCH_QUEUE = 3
 
 GROUND = {"freeslip": 0, "noslip": 1, "moving": 2}
 SIDES = {"freeslip": 0, "periodic": 1}

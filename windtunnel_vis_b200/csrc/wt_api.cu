@@ -1333,6 +1333,7 @@ struct wt_batch {
   std::vector<int64_t> long_per_replay;
   bool fused = false;  // wt_batch_set_fused(b, 1)
   bool persistent = false;  // wt_batch_set_fused(b, WT_BATCH_PERSISTENT)
+  bool queue = false;       // wt_batch_set_fused(b, WT_BATCH_QUEUE)
   unsigned* ps_bar = nullptr;  // the persistent kernel's barrier words
   std::string err;
 };
@@ -1368,16 +1369,20 @@ bool batch_fused(const wt_batch* b) {
   return true;
 }
 
-// Whether the batch's steps run in the persistent kernel: same lattice, storage and collision for
-// every member, each able to take it, and the table holds them all.
-bool batch_persistent(const wt_batch* b) {
-  if (!b->persistent || b->m.size() > 48) return false;
+// Whether the members can share the persistent kernel's work queue: same lattice, storage and
+// collision for every member, each able to take it, and the table holds them all.
+bool batch_queue_ok(const wt_batch* b) {
+  if (b->m.size() > 48) return false;
   const wt_solver* s0 = b->m[0];
   for (const wt_solver* s : b->m)
     if (!wt::persistent_ok(s) || s->is3d != s0->is3d || s->prec != s0->prec || s->kp.collision != s0->kp.collision)
       return false;
   return true;
 }
+// the batch's steps as one cooperative launch per wt_batch_step call (WT_BATCH_PERSISTENT)
+bool batch_persistent(const wt_batch* b) { return b->persistent && batch_queue_ok(b); }
+// the batch's steps as one launch of the work queue per step, under the batch graphs (WT_BATCH_QUEUE)
+bool batch_queue(const wt_batch* b) { return b->queue && batch_queue_ok(b); }
 
 // One step of every member with the bulk rows of all of them in one launch of the batch kernel on
 // the batch stream; each member's face rows and wall cells run on its auxiliary stream alongside,
@@ -1420,7 +1425,14 @@ int batch_capture_pairs(wt_batch* b, int pairs, cudaGraphExec_t* out, std::vecto
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return bfail(b, WT_E_CUDA, std::string("batch capture: ") + cudaGetErrorString(e));
-  if (batch_fused(b)) {
+  if (batch_queue(b)) {
+    // one work-queue launch per step; the item counters start from zero in every replay
+    e = cudaMemsetAsync(b->ps_bar, 0, wt::PS_BAR_WORDS * sizeof(unsigned), b->stream);
+    for (int k = 0; k < 2 * pairs && e == cudaSuccess; k++) {
+      e = wt::launch_queue_step(b->m.data(), (int)n, k, b->ps_bar, b->m[0]->err_dev, b->stream);
+      if (e == cudaSuccess) b->m[0]->launches++;
+    }
+  } else if (batch_fused(b)) {
     for (int k = 0; k < pairs && e == cudaSuccess; k++) {
       e = batch_fused_step(b, 0);
       if (e == cudaSuccess) e = batch_fused_step(b, 1);
@@ -1553,6 +1565,7 @@ int wt_batch_set_fused(wt_batch* b, int32_t on) {
   batch_drop_graph(b);
   b->fused = on == 1;
   b->persistent = on == WT_BATCH_PERSISTENT;
+  b->queue = on == WT_BATCH_QUEUE;
   return WT_OK;
 }
 

@@ -213,6 +213,10 @@ bool batch_fusable(const wt_solver* s);
 constexpr int PS_BAR_WORDS = 4;
 bool persistent_ok(const wt_solver* s);
 cudaError_t launch_persistent(wt_solver* const* ms, int count, int steps, unsigned* bar, int* err, cudaStream_t st);
+// one step of every tunnel in one launch of the persistent kernel's work queue (read-only-cache
+// loads, no grid barrier), step k0 of a graph: the tunnels start at parity parity ^ (k0 & 1), and the
+// launch takes item counter bar[2 + (k0 & 1)] and clears the other
+cudaError_t launch_queue_step(wt_solver* const* ms, int count, int k0, unsigned* bar, int* err, cudaStream_t st);
 // the face-row and wall-cell kernels of one step of `s` on its auxiliary stream, forked from
 // `origin`; s->ev_join is recorded at their end (the caller joins it into `origin`)
 cudaError_t launch_aux_kernels(wt_solver* s, const void* fin, void* fout, cudaStream_t origin);

@@ -2356,36 +2356,39 @@ __device__ __forceinline__ uint32_t ps_find(const PersistTable& T, uint32_t item
 }
 
 // wall cells c of one chunk (one per thread)
-template <class L, class S>
+template <class L, class S, bool COH>
 __device__ __forceinline__ void ps_wall_cells(const PersistTunnel& t, const typename S::T* fin, typename S::T* fout,
                                               uint32_t c) {
   if (c < t.nbnd)
-    boundary_cell<L, S, FM_SMAG, false, true>(t.P, fin, fout, t.bcell, t.brec, t.bgam, c, t.btab_cap, nullptr,
+    boundary_cell<L, S, FM_SMAG, false, COH>(t.P, fin, fout, t.bcell, t.brec, t.bgam, c, t.btab_cap, nullptr,
                                               nullptr, nullptr, nullptr, nullptr);
 }
 
 // face-row cell pair g (row g / (nx / 2), pair g % (nx / 2))
-template <class L, class S>
+template <class L, class S, bool COH>
 __device__ __forceinline__ void ps_face_cells(const PersistTunnel& t, const typename S::T* fin, typename S::T* fout,
                                               uint32_t g) {
   const uint32_t half = t.P.nx / 2u;
-  face_rows<L, S, FM_SMAG, false, true>(t.P, fin, fout, t.cls, t.gs, nullptr, nullptr, nullptr, nullptr, nullptr,
+  face_rows<L, S, FM_SMAG, false, COH>(t.P, fin, fout, t.cls, t.gs, nullptr, nullptr, nullptr, nullptr, nullptr,
                                         (int)(g % half) * 2, (int)(g / half));
 }
 
 // the same, out of line: in D3Q19 their register demand is above the bulk tiles' budget
-template <class L, class S>
+template <class L, class S, bool COH>
 __device__ __noinline__ void ps_wall(const PersistTunnel& t, const typename S::T* fin, typename S::T* fout, uint32_t c) {
-  ps_wall_cells<L, S>(t, fin, fout, c);
+  ps_wall_cells<L, S, COH>(t, fin, fout, c);
 }
-template <class L, class S>
+template <class L, class S, bool COH>
 __device__ __noinline__ void ps_face(const PersistTunnel& t, const typename S::T* fin, typename S::T* fout, uint32_t g) {
-  ps_face_cells<L, S>(t, fin, fout, g);
+  ps_face_cells<L, S, COH>(t, fin, fout, g);
 }
 
-template <class L, class S, bool BGK>
+// COH: the population loads bypass the read-only cache (a launch of several steps reads what its
+// own blocks wrote in the step before); one step per launch (k0 = the step's index in its graph,
+// which alternates the item counters) keeps the read-only path of the per-step kernels.
+template <class L, class S, bool BGK, bool COH>
 __global__ void __launch_bounds__(PS_THREADS, PS_MIN_BLOCKS)
-    k_steps_persistent(const __grid_constant__ PersistTable T, int steps, unsigned* __restrict__ bar,
+    k_steps_persistent(const __grid_constant__ PersistTable T, int steps, int k0, unsigned* __restrict__ bar,
                        int* __restrict__ err) {
   typedef typename S::T ST;
   // A block's first item of a step is its block index; thread 0 takes each further item from the
@@ -2395,9 +2398,9 @@ __global__ void __launch_bounds__(PS_THREADS, PS_MIN_BLOCKS)
   const uint32_t tid = threadIdx.x;
   uint32_t sl = 0;
   for (int k = 0; k < steps; k++) {
-    unsigned* const ctr = bar + 2 + (k & 1);
-    // the next step's counter was last used by step k - 1, which every block has left
-    if (blockIdx.x == 0 && tid == 0) atomicExch(bar + 2 + ((k + 1) & 1), 0u);
+    unsigned* const ctr = bar + 2 + ((k0 + k) & 1);
+    // the next step's counter was last used by the step before this one, which every block has left
+    if (blockIdx.x == 0 && tid == 0) atomicExch(bar + 2 + ((k0 + k + 1) & 1), 0u);
     for (uint32_t item = blockIdx.x; item < T.items; sl ^= 1u) {
       uint32_t nxt = 0;
       if (tid == 0) nxt = atomicAdd(ctr, 1u);  // consumed after this item's cells
@@ -2414,14 +2417,14 @@ __global__ void __launch_bounds__(PS_THREADS, PS_MIN_BLOCKS)
         const uint32_t bx = j % t.ttx, by = (j / t.ttx) % t.tty;
         uint32_t bz = j / (t.ttx * t.tty);
         if (par == 1) bz = (uint32_t)t.P.nz - 1u - bz;  // writing buffer 0: z downwards, as the step kernels
-        bulk_cells<L, S, 2, BGK, false, true>(t.P, fin, fout, t.cls, t.gs, (int)(bx * t.tbx + tid % t.tbx) * 2,
-                                              (int)(by * t.tby + tid / t.tbx), (int)bz);
+        bulk_cells<L, S, 2, BGK, false, COH>(t.P, fin, fout, t.cls, t.gs, (int)(bx * t.tbx + tid % t.tbx) * 2,
+                                             (int)(by * t.tby + tid / t.tbx), (int)bz);
       } else if (item >= T.fseg) {
-        if constexpr (L::DIM == 3) ps_face<L, S>(t, fin, fout, (item - t.fi0) * PS_THREADS + tid);
-        else ps_face_cells<L, S>(t, fin, fout, (item - t.fi0) * PS_THREADS + tid);
+        if constexpr (L::DIM == 3) ps_face<L, S, COH>(t, fin, fout, (item - t.fi0) * PS_THREADS + tid);
+        else ps_face_cells<L, S, COH>(t, fin, fout, (item - t.fi0) * PS_THREADS + tid);
       } else {
-        if constexpr (L::DIM == 3) ps_wall<L, S>(t, fin, fout, (item - t.wi0) * PS_THREADS + tid);
-        else ps_wall_cells<L, S>(t, fin, fout, (item - t.wi0) * PS_THREADS + tid);
+        if constexpr (L::DIM == 3) ps_wall<L, S, COH>(t, fin, fout, (item - t.wi0) * PS_THREADS + tid);
+        else ps_wall_cells<L, S, COH>(t, fin, fout, (item - t.wi0) * PS_THREADS + tid);
       }
       if (tid == 0) s_item[sl] = gridDim.x + nxt;
       __syncthreads();
@@ -3538,57 +3541,74 @@ bool persistent_ok(const wt_solver* s) {
          (s->nbnd == 0 || s->btab_cap >= s->nbnd);
 }
 
+// The step items of `count` tunnels (wall chunks, then face tiles, then bulk tiles of every
+// tunnel); tunnel k starts at parity ms[k]->parity ^ flip.
+static cudaError_t persistent_table(wt_solver* const* ms, int count, int flip, PersistTable& tab) {
+  if (count < 1 || count > PS_MAX_TUNNELS) return cudaErrorInvalidValue;
+  std::memset(&tab, 0, sizeof tab);
+  uint32_t nwall[PS_MAX_TUNNELS], nface[PS_MAX_TUNNELS], nbulk[PS_MAX_TUNNELS];
+  for (int k = 0; k < count; k++) {
+    const wt_solver* s = ms[k];
+    PersistTunnel& t = tab.t[k];
+    t.P = s->kp;
+    t.f[0] = s->f[0];
+    t.f[1] = s->f[1];
+    t.cls = s->cls;
+    t.bcell = s->bcell;
+    t.brec = s->brec;
+    t.bgam = s->bgam;
+    t.nbnd = s->nbnd;
+    t.btab_cap = (uint32_t)s->btab_cap;
+    t.gs = s->gs;
+    t.p0 = s->parity ^ flip;
+    const uint32_t half = (uint32_t)s->dims.nx / 2u;
+    t.tbx = half >= 256 ? 256u : (half >= 128 ? 128u : (half >= 64 ? 64u : 32u));
+    t.tby = (uint32_t)PS_THREADS / t.tbx;
+    t.ttx = (half + t.tbx - 1) / t.tbx;
+    t.tty = ((uint32_t)s->dims.ny + t.tby - 1) / t.tby;
+    nbulk[k] = t.ttx * t.tty * (uint32_t)s->dims.nz;
+    const uint32_t fr = s->is3d ? 2u * (uint32_t)s->dims.ny + 2u * (uint32_t)(s->dims.nz - 2) : 2u;
+    nface[k] = (fr * half + PS_THREADS - 1) / PS_THREADS;
+    nwall[k] = (s->nbnd + PS_THREADS - 1) / PS_THREADS;
+  }
+  uint32_t items = 0;
+  for (int k = 0; k < count; k++) tab.t[k].wi0 = items, items += nwall[k];
+  tab.fseg = items;
+  for (int k = 0; k < count; k++) tab.t[k].fi0 = items, items += nface[k];
+  tab.bseg = items;
+  for (int k = 0; k < count; k++) tab.t[k].bi0 = items, items += nbulk[k];
+  tab.count = (uint32_t)count;
+  tab.items = items;
+  return cudaSuccess;
+}
+
+// resident blocks of `kern` on the device of ms[0], at most `items`
+template <class K>
+static cudaError_t persistent_grid(K kern, wt_solver* const* ms, uint32_t items, unsigned* grid) {
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PS_THREADS, 0);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  *grid = (unsigned)std::min<size_t>(items, (size_t)per_sm * (size_t)ms[0]->num_sms);
+  return cudaSuccess;
+}
+
 template <class L, class S>
 static cudaError_t persistent_t(wt_solver* const* ms, int count, int steps, unsigned* bar, int* err,
                                 cudaStream_t st) {
   if constexpr (S::PREC == WT_PREC_F64) {
     return cudaErrorNotSupported;
   } else {
-    if (count < 1 || count > PS_MAX_TUNNELS || steps < 1) return cudaErrorInvalidValue;
+    if (steps < 1) return cudaErrorInvalidValue;
     PersistTable tab;
-    std::memset(&tab, 0, sizeof tab);
-    // items of a step: every tunnel's wall chunks, then every tunnel's face tiles, then the bulk tiles
-    uint32_t nwall[PS_MAX_TUNNELS], nface[PS_MAX_TUNNELS], nbulk[PS_MAX_TUNNELS];
-    for (int k = 0; k < count; k++) {
-      const wt_solver* s = ms[k];
-      PersistTunnel& t = tab.t[k];
-      t.P = s->kp;
-      t.f[0] = s->f[0];
-      t.f[1] = s->f[1];
-      t.cls = s->cls;
-      t.bcell = s->bcell;
-      t.brec = s->brec;
-      t.bgam = s->bgam;
-      t.nbnd = s->nbnd;
-      t.btab_cap = (uint32_t)s->btab_cap;
-      t.gs = s->gs;
-      t.p0 = s->parity;
-      const uint32_t half = (uint32_t)s->dims.nx / 2u;
-      t.tbx = half >= 256 ? 256u : (half >= 128 ? 128u : (half >= 64 ? 64u : 32u));
-      t.tby = (uint32_t)PS_THREADS / t.tbx;
-      t.ttx = (half + t.tbx - 1) / t.tbx;
-      t.tty = ((uint32_t)s->dims.ny + t.tby - 1) / t.tby;
-      nbulk[k] = t.ttx * t.tty * (uint32_t)s->dims.nz;
-      const uint32_t fr = s->is3d ? 2u * (uint32_t)s->dims.ny + 2u * (uint32_t)(s->dims.nz - 2) : 2u;
-      nface[k] = (fr * half + PS_THREADS - 1) / PS_THREADS;
-      nwall[k] = (s->nbnd + PS_THREADS - 1) / PS_THREADS;
-    }
-    uint32_t items = 0;
-    for (int k = 0; k < count; k++) tab.t[k].wi0 = items, items += nwall[k];
-    tab.fseg = items;
-    for (int k = 0; k < count; k++) tab.t[k].fi0 = items, items += nface[k];
-    tab.bseg = items;
-    for (int k = 0; k < count; k++) tab.t[k].bi0 = items, items += nbulk[k];
-    tab.count = (uint32_t)count;
-    tab.items = items;
-    auto kern = ms[0]->kp.collision == 1u ? k_steps_persistent<L, S, true> : k_steps_persistent<L, S, false>;
-    int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PS_THREADS, 0);
+    cudaError_t e = persistent_table(ms, count, 0, tab);
     if (e != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    const unsigned grid = (unsigned)std::min<size_t>(items, (size_t)per_sm * (size_t)ms[0]->num_sms);
+    auto kern = ms[0]->kp.collision == 1u ? k_steps_persistent<L, S, true, true> : k_steps_persistent<L, S, false, true>;
+    unsigned grid = 0;
+    if ((e = persistent_grid(kern, ms, tab.items, &grid)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(bar, 0, PS_BAR_WORDS * sizeof(unsigned), st)) != cudaSuccess) return e;
-    void* args[] = {(void*)&tab, (void*)&steps, (void*)&bar, (void*)&err};
+    int k0 = 0;
+    void* args[] = {(void*)&tab, (void*)&steps, (void*)&k0, (void*)&bar, (void*)&err};
     return cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(PS_THREADS), args, 0, st);
   }
 }
@@ -3599,6 +3619,31 @@ cudaError_t launch_persistent(wt_solver* const* ms, int count, int steps, unsign
     if (ms[k]->is3d != s->is3d || ms[k]->prec != s->prec || ms[k]->kp.collision != s->kp.collision)
       return cudaErrorInvalidValue;
   WT_DISPATCH(persistent_t, ms, count, steps, bar, err, st);
+}
+
+template <class L, class S>
+static cudaError_t queue_step_t(wt_solver* const* ms, int count, int k0, unsigned* bar, int* err, cudaStream_t st) {
+  if constexpr (S::PREC == WT_PREC_F64) {
+    return cudaErrorNotSupported;
+  } else {
+    PersistTable tab;
+    cudaError_t e = persistent_table(ms, count, k0 & 1, tab);
+    if (e != cudaSuccess) return e;
+    auto kern =
+        ms[0]->kp.collision == 1u ? k_steps_persistent<L, S, true, false> : k_steps_persistent<L, S, false, false>;
+    unsigned grid = 0;
+    if ((e = persistent_grid(kern, ms, tab.items, &grid)) != cudaSuccess) return e;
+    kern<<<grid, PS_THREADS, 0, st>>>(tab, 1, k0, bar, err);
+    return cudaGetLastError();
+  }
+}
+
+cudaError_t launch_queue_step(wt_solver* const* ms, int count, int k0, unsigned* bar, int* err, cudaStream_t st) {
+  const wt_solver* s = ms[0];
+  for (int k = 1; k < count; k++)
+    if (ms[k]->is3d != s->is3d || ms[k]->prec != s->prec || ms[k]->kp.collision != s->kp.collision)
+      return cudaErrorInvalidValue;
+  WT_DISPATCH(queue_step_t, ms, count, k0, bar, err, st);
 }
 
 bool batch_fusable(const wt_solver* s) {

@@ -350,7 +350,7 @@ class Batch:
     holding every member's step kernels, so small tunnels run concurrently. Members stay ordinary
     Solver objects for parameters, geometry and readback, and must outlive the batch."""
 
-    def __init__(self, solvers, fused=False, persistent=False):
+    def __init__(self, solvers, fused=False, persistent=False, queue=False):
         self._lib = abi.load()
         self.members = list(solvers)
         arr = (C.c_void_p * len(self.members))(*[s.handle.value for s in self.members])
@@ -363,6 +363,8 @@ class Batch:
             self.set_fused(True)
         if persistent:
             self.set_persistent(True)
+        if queue:
+            self.set_queue(True)
 
     def set_fused(self, on: bool):
         """Bulk rows of all members in one batch-kernel launch per step (wt_batch_set_fused(b, 1))."""
@@ -372,6 +374,11 @@ class Batch:
         """Every wt_batch_step call of two or more steps as one cooperative launch of the
         persistent kernel over all members (wt_batch_set_fused(b, WT_BATCH_PERSISTENT))."""
         self._check(self._lib.wt_batch_set_fused(self._h, abi.WT_BATCH_PERSISTENT if on else 0))
+
+    def set_queue(self, on: bool):
+        """Every step of every member as one launch of the persistent kernel's work queue, the
+        launches captured in the batch graphs (wt_batch_set_fused(b, WT_BATCH_QUEUE))."""
+        self._check(self._lib.wt_batch_set_fused(self._h, abi.WT_BATCH_QUEUE if on else 0))
 
     def _check(self, rc):
         if rc != 0:

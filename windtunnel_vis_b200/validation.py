@@ -332,7 +332,7 @@ def sweep_cases(count=32):
 
 
 def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, re_l=2e4, target_tris=200_000,
-                closure=None, fused=False, autotune=True, persistent=False):
+                closure=None, fused=False, autotune=True, persistent=False, queue=False):
     """Runs the sweep of sweep_cases as one batch (windtunnel_vis_b200.solver.Batch): every tunnel
     voxelizes the vehicle body at its yaw (moving belt, rotating wheels, Smagorinsky LES, FP16),
     then all advance `steps` lattice updates together. Reports the aggregate MLUPS (device time
@@ -341,7 +341,9 @@ def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, 
     and the per-case C_D, which must agree exactly (the batch replays the same kernels). `closure`
     (a network, see windtunnel_vis_b200.closure) replaces Smagorinsky in every tunnel; with
     `autotune` the project's launch tuner picks each tunnel's block shape and cells per thread;
-    `persistent` runs each batch step call as one launch of the persistent kernel over all tunnels."""
+    `persistent` runs each batch step call as one launch of the persistent kernel over all tunnels;
+    `queue` runs each step of all tunnels as one launch of that kernel's work queue, under the batch
+    graphs."""
     import torch
 
     from . import mesh as Mh
@@ -397,7 +399,7 @@ def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, 
 
     cells = sum(d[0] * d[1] * d[2] for d, _, _ in cases)
     solvers, frontal = build()
-    batch = Batch(solvers, fused=fused, persistent=persistent)
+    batch = Batch(solvers, fused=fused, persistent=persistent, queue=queue)
 
     def step_batch(n):
         batch.step(n)
@@ -405,7 +407,7 @@ def batch_sweep(steps=10000, count=32, chunk=250, compare_alone=False, cs=0.14, 
 
     ms, res = run(step_batch, batch.sample, frontal)
     out = {"id": "batch_sweep", "tunnels": count, "cells": cells, "steps": steps, "closure": closure is not None,
-           "fused": fused, "persistent": persistent, "autotune": autotune and closure is None,
+           "fused": fused, "persistent": persistent, "queue": queue, "autotune": autotune and closure is None,
            "batch_ms": ms,
            "batch_mlups": cells * steps / (ms * 1e-3) / 1e6, "cases": res}
     batch.destroy()
@@ -461,6 +463,7 @@ def main(argv=None):
     ap.add_argument("--save", default=None, help="learned_closure: write the trained network (.npz)")
     ap.add_argument("--fused", action="store_true", help="batch_sweep: bulk rows of all tunnels in one kernel")
     ap.add_argument("--persistent", action="store_true", help="batch_sweep: all tunnels' steps in one persistent launch")
+    ap.add_argument("--queue", action="store_true", help="batch_sweep: each step of all tunnels in one work-queue launch")
     ap.add_argument("--outside-regime", action="store_true",
                     help="batch_sweep: apply --closure outside its stored Reynolds-number regime (throughput only)")
     ap.add_argument("--closure", default=None,
@@ -495,7 +498,8 @@ def main(argv=None):
             # the length): outside the shipped network's regime, allowed only for throughput runs
             model = CL.load_pretrained(2e4 * 0.336, allow_outside=a.outside_regime,
                                        path=CL.PRETRAINED if a.closure == "pretrained" else a.closure)
-        r = batch_sweep(a.steps, compare_alone=True, closure=model, fused=a.fused, persistent=a.persistent)
+        r = batch_sweep(a.steps, compare_alone=True, closure=model, fused=a.fused, persistent=a.persistent,
+                        queue=a.queue)
     else:
         r = CASES[a.case](solver_factory, a.valscale)
     r.pop("series", None)
