@@ -334,8 +334,8 @@ def test_shipped_network_beats_smagorinsky_a_posteriori(gpu):
     The fine run (512 x 256 x 256, 16000 steps) gives the reference C_D; coarse runs over the same
     physical time with no sub-grid model, with Smagorinsky (Cs = 0.1) and with the network. The
     network's C_D lies within 2 % of the fine run's and closer to it than Smagorinsky's; every run is
-    deterministic, so these are the study's own numbers (fine 0.4822, no model -0.9 %, Smagorinsky
-    +3.2 %, network +0.0 %)."""
+    deterministic (on the current build: fine 0.4851, no model -0.3 %, Smagorinsky +3.5 %, network
+    +1.9 %)."""
     from windtunnel_vis_b200.solver import solver_factory
 
     model = CL.load_pretrained(1000.0)
