@@ -1044,8 +1044,8 @@ int wt_derive_fields(wt_solver* s) {
   if (int rc = settle_uploads(s)) return rc;
   for (uint2** b : {&s->dvort, &s->dstat, &s->dmean})
     if (!*b) WT_CUDA(s, cudaMalloc((void**)b, s->n * 8), "cudaMalloc(derived fields)");
+  // queued on the handle's stream like the reference's derive dispatch; the reads that follow wait
   WT_CUDA(s, wt::launch_derive(s), "derive fields");
-  WT_CUDA(s, cudaStreamSynchronize(s->stream), "derive fields");
   return WT_OK;
 }
 

@@ -6,8 +6,9 @@
 //   k_export ... every stride-th cell (clamped to the last cell) of velocity, mean and vorticity
 //                as three float4 arrays (the export pass of src/solver/SolverGPU.ts:374-425)
 //
-// One thread per cell along x-rows; the velocity stencil (six neighbours) is read through L1/L2
-// and the kernel streams 8 + 16 + 4 + 4 B in and 24 B out per cell. Compiled without FMA
+// One thread per cell along x-rows; the velocity stencil (six neighbours) and the solid flags two
+// cells out along each axis are read through L1/L2, all of a cell's loads issued before its
+// arithmetic; the kernel streams 8 + 16 + 4 + 4 B in and 24 B out per cell. Compiled without FMA
 // contraction: every output is bit-identical to the oracle's f32 restatement.
 #include <cuda_fp16.h>
 
@@ -29,12 +30,6 @@ __device__ __forceinline__ float3 vel_at(const uint2* __restrict__ vel, int x, i
   return make_float3(a.x, a.y, b.x);
 }
 
-__device__ __forceinline__ bool solid_at(const uint32_t* __restrict__ flags, int x, int y, int z, int NX, int NY,
-                                         int NZ) {
-  if (x < 0 || y < 0 || z < 0 || x >= NX || y >= NY || z >= NZ) return false;
-  return __ldg(flags + (size_t)x + (size_t)NX * ((size_t)y + (size_t)NY * (size_t)z)) != 0u;
-}
-
 __device__ __forceinline__ uint2 pack_half4(float a, float b, float c, float d) {
   __half2 h0 = __floats2half2_rn(a, b), h1 = __floats2half2_rn(c, d);
   return make_uint2(*reinterpret_cast<uint32_t*>(&h0), *reinterpret_cast<uint32_t*>(&h1));
@@ -44,6 +39,15 @@ __device__ __forceinline__ float4 unpack_half4(uint2 v) {
   const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&v.x));
   const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&v.y));
   return make_float4(a.x, a.y, b.x, b.y);
+}
+
+// the solid flag of cell (x, y, z), false outside the grid; the load is always issued (from a
+// clamped address) so that all of a cell's stencil loads are in flight together
+__device__ __forceinline__ bool solid_near(const uint32_t* __restrict__ flags, int x, int y, int z, int NX, int NY,
+                                           int NZ) {
+  const bool in = x >= 0 && y >= 0 && z >= 0 && x < NX && y < NY && z < NZ;
+  const int cx = min(max(x, 0), NX - 1), cy = min(max(y, 0), NY - 1), cz = min(max(z, 0), NZ - 1);
+  return in && __ldg(flags + (size_t)cx + (size_t)NX * ((size_t)cy + (size_t)NY * (size_t)cz)) != 0u;
 }
 
 template <int DIM>
@@ -57,11 +61,26 @@ __global__ void __launch_bounds__(256) k_derive(const __grid_constant__ wt_kpara
   const int y = blockIdx.y, z = blockIdx.z;
   if (x >= NX) return;
   const size_t idx = (size_t)x + (size_t)NX * ((size_t)y + (size_t)NY * (size_t)z);
-  const bool solid = flags[idx] != 0u;
+  // every load of the cell first (the stencil's velocities and flags, the EMA statistics), then the
+  // arithmetic: no load waits behind a branch on another
+  const bool solid = __ldg(flags + idx) != 0u;
+  const float4 m = __ldg(meanA + idx);
+  const float mb = __ldg(meanB + idx);
+  const float3 xp = vel_at(vel, x + 1, y, z, NX, NY, NZ), xm = vel_at(vel, x - 1, y, z, NX, NY, NZ);
+  const float3 yp = vel_at(vel, x, y + 1, z, NX, NY, NZ), ym = vel_at(vel, x, y - 1, z, NX, NY, NZ);
+  float3 zp = make_float3(0.f, 0.f, 0.f), zm = zp;
+  if (DIM == 3) zp = vel_at(vel, x, y, z + 1, NX, NY, NZ), zm = vel_at(vel, x, y, z - 1, NX, NY, NZ);
+  bool hit[2][3];  // a solid d cells away along axis a, either side
+#pragma unroll
+  for (int d = 1; d <= 2; d++)
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const int ex = a == 0 ? d : 0, ey = a == 1 ? d : 0, ez = a == 2 ? d : 0;
+      hit[d - 1][a] = a < DIM && (solid_near(flags, x + ex, y + ey, z + ez, NX, NY, NZ) |
+                                  solid_near(flags, x - ex, y - ey, z - ez, NX, NY, NZ));
+    }
   float4 vo = make_float4(0.f, 0.f, 0.f, 0.f);
   if (!solid) {
-    const float3 xp = vel_at(vel, x + 1, y, z, NX, NY, NZ), xm = vel_at(vel, x - 1, y, z, NX, NY, NZ);
-    const float3 yp = vel_at(vel, x, y + 1, z, NX, NY, NZ), ym = vel_at(vel, x, y - 1, z, NX, NY, NZ);
     float J[3][3];  // J[j][i] = d u_i / d x_j
     J[0][0] = 0.5f * (xp.x - xm.x);
     J[0][1] = 0.5f * (xp.y - xm.y);
@@ -70,7 +89,6 @@ __global__ void __launch_bounds__(256) k_derive(const __grid_constant__ wt_kpara
     J[1][1] = 0.5f * (yp.y - ym.y);
     J[1][2] = 0.5f * (yp.z - ym.z);
     if (DIM == 3) {
-      const float3 zp = vel_at(vel, x, y, z + 1, NX, NY, NZ), zm = vel_at(vel, x, y, z - 1, NX, NY, NZ);
       J[2][0] = 0.5f * (zp.x - zm.x);
       J[2][1] = 0.5f * (zp.y - zm.y);
       J[2][2] = 0.5f * (zp.z - zm.z);
@@ -95,15 +113,11 @@ __global__ void __launch_bounds__(256) k_derive(const __grid_constant__ wt_kpara
 #pragma unroll
     for (int d = 1; d <= 2; d++)
 #pragma unroll
-      for (int a = 0; a < DIM; a++) {
-        const int ex = a == 0 ? d : 0, ey = a == 1 ? d : 0, ez = a == 2 ? d : 0;
-        if (solid_at(flags, x + ex, y + ey, z + ez, NX, NY, NZ) || solid_at(flags, x - ex, y - ey, z - ez, NX, NY, NZ))
-          near = fmaxf(near, d == 1 ? 1.0f : 0.5f);
-      }
+      for (int a = 0; a < DIM; a++)
+        if (hit[d - 1][a]) near = fmaxf(near, d == 1 ? 1.0f : 0.5f);
     vo = make_float4(wx, wy, wz, 0.5f * (W2 - S2) * (1.0f - near));
   }
-  const float4 m = meanA[idx];
-  const float k = fmaxf(meanB[idx] - (m.x * m.x + m.y * m.y + m.z * m.z), 0.0f);
+  const float k = fmaxf(mb - (m.x * m.x + m.y * m.y + m.z * m.z), 0.0f);
   const float ti = sqrtf(k / 3.0f) / fmaxf(P.u_ref, 1e-6f);
   vort[idx] = pack_half4(vo.x, vo.y, vo.z, vo.w);
   stat[idx] = pack_half4(solid ? 0.0f : ti, solid ? 1.0f : 0.0f, 0.0f, 0.0f);
