@@ -137,3 +137,29 @@ def test_sample_state_errors(gpu):
     assert st["step"] == 4
     assert s.step_and_sample(2)["step"] == 8
     s.destroy()
+
+
+def test_queued_uploads_apply_to_batch_members(gpu):
+    """A queued upload on a batch member applies before the batch's next step, as it does before
+    the member's own next step."""
+    from windtunnel_vis_b200.solver import Batch
+
+    dims = (40, 16, 12)
+    flags, sdf, wheels = scene(dims)
+    params = dict(PARAM_SETS["freeslip_reg"], precision="f16")
+    alone, member = _handles(dims, params, wheels)
+    for s in (alone, member):
+        s.upload_flags(np.zeros_like(flags))
+        s.step(4)
+    alone.upload_flags(flags)
+    alone.upload_sdf(sdf)
+    member.upload_flags_async(flags)
+    member.upload_sdf_async(sdf)
+    batch = Batch([member])
+    batch.step(6)
+    alone.step(6)
+    np.testing.assert_array_equal(member.read_populations(), alone.read_populations())
+    assert batch.sample()[0]["raw"].tolist() == alone.sample()["raw"].tolist()
+    batch.destroy()
+    alone.destroy()
+    member.destroy()
