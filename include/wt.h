@@ -405,8 +405,8 @@ int wt_set_closure(wt_solver* s, const wt_closure* closure);
 int wt_get_closure(const wt_solver* s, wt_closure* out, int32_t* enabled);
 
 /* Trainer of the closure: a device-resident pool of samples (features + target eddy viscosity),
- * the network's f32 master weights and Adam state, and the BF16 training kernels (tcgen05 forward
- * and input-gradient products, f32 accumulation). One trainer per device; calls on one trainer are
+ * the network's f32 master weights and Adam state, and the BF16 training kernels (tcgen05 forward,
+ * input-gradient and weight-gradient products, f32 accumulation). One trainer per device; calls on one trainer are
  * serialized by the caller. */
 typedef struct wt_trainer wt_trainer;
 typedef struct wt_train_params {

@@ -1,7 +1,7 @@
 // wt_closure.cu — trainer of the learned LES closure: the sample pool, the training-data kernels
 // (targets from the box-filtered fine run, selection), the BF16 training and inference kernel
-// (tcgen05 MMAs for the three batch-by-32 products, f32 accumulation), the gradient reduction and
-// Adam. No counterpart in the reference, whose only closure is Smagorinsky (wgslLbm.ts:206-214).
+// (tcgen05 MMAs for the two forward layers, the input gradient of layer 2 and the weight gradients
+// of both layers, f32 accumulation), the gradient reduction and Adam. No counterpart in the reference, whose only closure is Smagorinsky (wgslLbm.ts:206-214).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -44,24 +44,41 @@ namespace {
 
 constexpr int TR_THREADS = 128;
 constexpr int TR_NOUT = CL_NPARAM + 1;  // gradient entries + loss
-constexpr uint32_t TR_TMEM_COLS = 128;
+// tensor-memory columns: z1 (0-31), z2 (32-63), dH1 (64-95); training adds dW2 (96-127) and dW1 (128-159)
+constexpr uint32_t TR_TMEM_COLS_INFER = 128;
+constexpr uint32_t TR_TMEM_COLS_TRAIN = 256;
 constexpr uint32_t TR_WAIT_LIMIT = 1u << 22;
 // shared-memory layout of k_train (bytes)
 constexpr int TS_A = 0;          // inputs x', 128 x 16 bf16, K-major (A of layer 1)
 constexpr int TS_H1 = 4096;      // h1, 128 x 32 bf16, K-major (A of layer 2)
 constexpr int TS_DZ2 = 12288;    // dz2, 128 x 32 bf16, K-major (A of the dH1 product)
-constexpr int TS_DZ1 = 20480;    // dz1, [128][32] bf16
-constexpr int TS_H2 = 28672;     // h2, [128][32] f32
-constexpr int TS_W1 = 45056;     // W1 image (N = 32 hidden, K = 16 inputs)
-constexpr int TS_W2 = 46080;     // W2 image (N = out, K = in)
-constexpr int TS_W2T = 48128;    // W2 transposed image (N = in, K = out)
-constexpr int TS_DZ3 = 50176;    // dz3 [128] f32
-constexpr int TS_LOSS = 50688;   // per-row loss [128] f32
-constexpr int TS_BAR = 51200;    // mbarrier, the tensor-memory address, pad, drain barrier
-// 53 KB of dynamic shared memory: at most 4 blocks per SM, whose 4 x 128 tensor-memory columns fit
-constexpr int TS_BYTES = 53 * 1024;
+constexpr int TS_H2 = 20480;     // h2, [128][32] f32
+constexpr int TS_W1 = 36864;     // W1 image (N = 32 hidden, K = 16 inputs)
+constexpr int TS_W2 = 37888;     // W2 image (N = out, K = in)
+constexpr int TS_W2T = 39936;    // W2 transposed image (N = in, K = out)
+constexpr int TS_DZ3 = 41984;    // dz3 [128] f32
+constexpr int TS_LOSS = 42496;   // per-row loss [128] f32
+constexpr int TS_BAR = 43008;    // mbarrier, the tensor-memory address, pad, drain barrier
 constexpr int TS_DRAIN = TS_BAR + 16;
-static_assert(TS_DRAIN + 8 <= TS_BYTES, "layout");
+// inference: 45 KB of dynamic shared memory, so at most 4 blocks share an SM and their
+// 4 x 128 tensor-memory columns fit in its 512
+constexpr int TS_BYTES_INFER = 45 * 1024;
+// Training adds the operands of the weight-gradient products, summed over the block's 128 samples
+// (the K dimension):
+//   dW2 and db2 = [h1^T ; 1] dz2: A = h1^T in rows 0-31, ones in row 32, zeros below (128 x 128
+//                 bf16, K-major); B = dz2^T (32 x 128)
+//   dW1 and db1 = [x'^T ; 1] dz1: A = x'^T in rows 0-9, ones in row 16, zeros elsewhere; B = dz1^T
+// M = 128 (tensor-memory lane = row), N = 32, eight K = 16 steps each. 125 KB: one block per SM,
+// with 256 tensor-memory columns.
+constexpr int TS_GA2 = 46080;
+constexpr int TS_GA1 = TS_GA2 + 32768;
+constexpr int TS_GB2 = TS_GA1 + 32768;
+constexpr int TS_GB1 = TS_GB2 + 8192;
+constexpr int TS_BYTES_TRAIN = TS_GB1 + 8192;
+constexpr int TR_ONE_K1 = 16;    // the ones row of the dW1 operand (its sums over the samples are db1)
+static_assert(TS_DRAIN + 8 <= TS_BYTES_INFER && TS_BYTES_INFER <= TS_GA2 && 5 * (TS_BYTES_INFER + 1024) > 228 * 1024,
+              "inference layout");
+static_assert(TS_BYTES_TRAIN <= 227 * 1024 && 2 * (TS_BYTES_TRAIN + 1024) > 228 * 1024, "training layout");
 
 // parameter offsets in the master vector
 constexpr int PO_W1 = 0, PO_B1 = 320, PO_W2 = 352, PO_B2 = 1376, PO_W3 = 1408, PO_B3 = 1440;
@@ -96,8 +113,9 @@ __device__ __forceinline__ float sm_bf16(const uint8_t* base, uint32_t off) {
 // layers on tcgen05 (x' W1 into columns 0-31, h1 W2 into 32-63), the output layer on CUDA cores.
 // TRAIN adds the backward pass: dz3 = 2 (nu - y) sigmoid(z3) / nu_scale per sample,
 // dz2 = bf16(dz3 w3 gelu'(z2)), dH1 = dz2 W2^T on tcgen05 (columns 64-95), dz1 = bf16(dH1 gelu'(z1)),
-// then the weight and bias gradients summed over the block's rows on CUDA cores (f32, rows in
-// order) into partials[block].
+// then the block's weight and bias gradients of layers 1 and 2 as two more tcgen05 products over
+// its 128 samples ([h1^T ; 1] dz2 into columns 96-127, [x'^T ; 1] dz1 into 128-159) and those of
+// the output layer on CUDA cores (f32, rows in order), into partials[block].
 template <bool TRAIN>
 __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ TrainArgs A, int* __restrict__ err) {
   extern __shared__ __align__(128) uint8_t sm[];
@@ -132,7 +150,13 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
     umma::mbar_init(mbar, 1);
     umma::mbar_init(dbar, 1);
   }
-  if (warp == 0) umma::tmem_alloc(tslot, TR_TMEM_COLS);
+  constexpr uint32_t TMEM_COLS = TRAIN ? TR_TMEM_COLS_TRAIN : TR_TMEM_COLS_INFER;
+  if (warp == 0) umma::tmem_alloc(tslot, TMEM_COLS);
+  if constexpr (TRAIN) {
+    // the weight-gradient A operands are zero outside their data and ones rows
+    uint4* z = reinterpret_cast<uint4*>(sm + TS_GA2);
+    for (uint32_t e = tid; e < 2u * 32768u / 16u; e += TR_THREADS) z[e] = make_uint4(0u, 0u, 0u, 0u);
+  }
   // x' row (zeros for padding rows)
   {
     uint32_t w[8];
@@ -145,6 +169,16 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
     }
     *reinterpret_cast<uint4*>(sm + TS_A + umma::kmaj_off(tid, 0, CL_K1)) = make_uint4(w[0], w[1], w[2], w[3]);
     *reinterpret_cast<uint4*>(sm + TS_A + umma::kmaj_off(tid, 8, CL_K1)) = make_uint4(w[4], w[5], w[6], w[7]);
+    if constexpr (TRAIN) {
+      // column tid of [x'^T ; 1] and the ones of [h1^T ; 1] (after the zero fill above)
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < CL_IN; k++)
+        *reinterpret_cast<uint16_t*>(sm + TS_GA1 + umma::kmaj_off(k, tid, TR_THREADS)) =
+            (uint16_t)(w[k >> 1] >> (16 * (k & 1)));
+      *reinterpret_cast<uint16_t*>(sm + TS_GA1 + umma::kmaj_off(TR_ONE_K1, tid, TR_THREADS)) = 0x3F80u;
+      *reinterpret_cast<uint16_t*>(sm + TS_GA2 + umma::kmaj_off(CL_H, tid, TR_THREADS)) = 0x3F80u;
+    }
   }
   umma::fence_async_smem();
   umma::fence_before_sync();
@@ -180,6 +214,12 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
       pk[e] = lo | (hi << 16);
     }
     *reinterpret_cast<uint4*>(sm + TS_H1 + umma::kmaj_off(tid, 8 * c, CL_H)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    if constexpr (TRAIN) {
+#pragma unroll
+      for (int e = 0; e < 8; e++)
+        *reinterpret_cast<uint16_t*>(sm + TS_GA2 + umma::kmaj_off(8 * c + e, tid, TR_THREADS)) =
+            (uint16_t)(pk[e >> 1] >> (16 * (e & 1)));
+    }
   }
   umma::fence_before_sync();
   umma::fence_async_smem();
@@ -233,6 +273,10 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
         pk[e] = lo | (hi << 16);
       }
       *reinterpret_cast<uint4*>(sm + TS_DZ2 + umma::kmaj_off(tid, 8 * c, CL_H)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+#pragma unroll
+      for (int e = 0; e < 8; e++)
+        *reinterpret_cast<uint16_t*>(sm + TS_GB2 + umma::kmaj_off(8 * c + e, tid, TR_THREADS)) =
+            (uint16_t)(pk[e >> 1] >> (16 * (e & 1)));
       float4* hrow = reinterpret_cast<float4*>(sm + TS_H2 + (tid * CL_H + 8 * c) * 4);
       hrow[0] = make_float4(h2[8 * c], h2[8 * c + 1], h2[8 * c + 2], h2[8 * c + 3]);
       hrow[1] = make_float4(h2[8 * c + 4], h2[8 * c + 5], h2[8 * c + 6], h2[8 * c + 7]);
@@ -266,35 +310,56 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
         const uint32_t hi = valid ? bf16_bits(dh[2 * e + 1] * g1) : 0u;
         pk[e] = lo | (hi << 16);
       }
-      *reinterpret_cast<uint4*>(sm + TS_DZ1 + (tid * CL_H + 8 * c) * 2) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+#pragma unroll
+      for (int e = 0; e < 8; e++)
+        *reinterpret_cast<uint16_t*>(sm + TS_GB1 + umma::kmaj_off(8 * c + e, tid, TR_THREADS)) =
+            (uint16_t)(pk[e >> 1] >> (16 * (e & 1)));
     }
+    // the weight and bias gradients of layers 1 and 2 on the tensor cores: sums over the block's
+    // 128 samples, eight K = 16 steps per product
+    umma::fence_before_sync();
+    umma::fence_async_smem();
     __syncthreads();
-    // block sums of the weight and bias gradients (rows in order, f32)
+    if (tid == 0) {
+      umma::fence_after_sync();
+      const uint32_t a2 = umma::smem_u32(sm + TS_GA2), b2 = umma::smem_u32(sm + TS_GB2);
+      const uint32_t a1 = umma::smem_u32(sm + TS_GA1), b1 = umma::smem_u32(sm + TS_GB1);
+#pragma unroll
+      for (int k = 0; k < TR_THREADS / 16; k++) {
+        umma::mma_bf16(tmem + 96, umma::sdesc(a2 + 256 * k, 128, 2048), umma::sdesc(b2 + 256 * k, 128, 2048), ID, k > 0);
+        umma::mma_bf16(tmem + 128, umma::sdesc(a1 + 256 * k, 128, 2048), umma::sdesc(b1 + 256 * k, 128, 2048), ID,
+                       k > 0);
+      }
+      umma::commit(mbar);
+    }
+    issue_wait();
     float* out = A.partials + (size_t)blockIdx.x * TR_NOUT;
-    for (int p = (int)tid; p < TR_NOUT; p += TR_THREADS) {
+    // rows 0-31 and 32 of the dW2 product, rows 0-9 and 16 of the dW1 product (lanes of warps 0-1)
+    if (warp < 2) {
+      float v2[32], v1[32];
+      umma::tmem_ld32(umma::tmem_lane_addr(tmem, warp, 96), v2);
+      umma::tmem_ld32(umma::tmem_lane_addr(tmem, warp, 128), v1);
+      umma::tmem_wait_ld();
+      if (tid <= (uint32_t)CL_H) {
+        float* o = tid < (uint32_t)CL_H ? out + PO_W2 + tid * CL_H : out + PO_B2;
+#pragma unroll
+        for (int j = 0; j < CL_H; j++) o[j] = v2[j];
+      }
+      if (tid < (uint32_t)CL_IN || tid == (uint32_t)TR_ONE_K1) {
+        float* o = tid < (uint32_t)CL_IN ? out + PO_W1 + tid * CL_H : out + PO_B1;
+#pragma unroll
+        for (int j = 0; j < CL_H; j++) o[j] = v1[j];
+      }
+    }
+    // the output layer's weights and bias and the loss: block sums on CUDA cores (rows in order, f32)
+    const float* dz = reinterpret_cast<const float*>(sm + TS_DZ3);
+    for (int p = PO_W3 + (int)tid; p < TR_NOUT; p += TR_THREADS) {
       float acc = 0.0f;
-      if (p < PO_B1) {
-        const int k = p / CL_H, j = p % CL_H;
-        for (int r = 0; r < TR_THREADS; r++)
-          acc = __fmaf_rn(sm_bf16(sm + TS_A, umma::kmaj_off(r, k, CL_K1)), sm_bf16(sm + TS_DZ1, (r * CL_H + j) * 2), acc);
-      } else if (p < PO_W2) {
-        const int j = p - PO_B1;
-        for (int r = 0; r < TR_THREADS; r++) acc = __fadd_rn(acc, sm_bf16(sm + TS_DZ1, (r * CL_H + j) * 2));
-      } else if (p < PO_B2) {
-        const int i = (p - PO_W2) / CL_H, j = (p - PO_W2) % CL_H;
-        for (int r = 0; r < TR_THREADS; r++)
-          acc = __fmaf_rn(sm_bf16(sm + TS_H1, umma::kmaj_off(r, i, CL_H)), sm_bf16(sm + TS_DZ2, umma::kmaj_off(r, j, CL_H)),
-                          acc);
-      } else if (p < PO_W3) {
-        const int j = p - PO_B2;
-        for (int r = 0; r < TR_THREADS; r++) acc = __fadd_rn(acc, sm_bf16(sm + TS_DZ2, umma::kmaj_off(r, j, CL_H)));
-      } else if (p < PO_B3) {
+      if (p < PO_B3) {
         const int j = p - PO_W3;
-        const float* dz = reinterpret_cast<const float*>(sm + TS_DZ3);
         const float* h2s = reinterpret_cast<const float*>(sm + TS_H2);
         for (int r = 0; r < TR_THREADS; r++) acc = __fmaf_rn(dz[r], h2s[r * CL_H + j], acc);
       } else if (p == PO_B3) {
-        const float* dz = reinterpret_cast<const float*>(sm + TS_DZ3);
         for (int r = 0; r < TR_THREADS; r++) acc = __fadd_rn(acc, dz[r]);
       } else {
         const float* ls = reinterpret_cast<const float*>(sm + TS_LOSS);
@@ -306,7 +371,7 @@ __global__ void __launch_bounds__(TR_THREADS) k_train(const __grid_constant__ Tr
   // after a timed-out wait, the MMAs finish before their tensor memory is released
   const bool drained = umma::drain_before_free(dbar, !ok, TR_WAIT_LIMIT);
   __syncthreads();
-  if (warp == 0) umma::tmem_free(tmem, TR_TMEM_COLS);
+  if (warp == 0) umma::tmem_free(tmem, TMEM_COLS);
   if (!ok || !drained) atomicOr(err, 4);
 }
 
@@ -534,8 +599,9 @@ int ensure_partials(wt_trainer* t, int64_t blocks) {
 
 // k_train's dynamic shared memory exceeds the 48 KB default: opt in (on the current device)
 cudaError_t train_smem_optin() {
-  cudaError_t r = cudaFuncSetAttribute(k_train<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TS_BYTES);
-  if (r == cudaSuccess) r = cudaFuncSetAttribute(k_train<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TS_BYTES);
+  cudaError_t r = cudaFuncSetAttribute(k_train<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TS_BYTES_TRAIN);
+  if (r == cudaSuccess)
+    r = cudaFuncSetAttribute(k_train<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TS_BYTES_INFER);
   return r;
 }
 
@@ -821,7 +887,7 @@ int wt_trainer_fit(wt_trainer* t, const wt_train_params* p, float* loss) {
   cudaError_t e = cudaSuccess;
   for (int s = 0; s < p->steps && e == cudaSuccess; s++) {
     A.draw = (uint64_t)s;
-    k_train<true><<<(unsigned)blocks, TR_THREADS, TS_BYTES, t->stream>>>(A, derr);
+    k_train<true><<<(unsigned)blocks, TR_THREADS, TS_BYTES_TRAIN, t->stream>>>(A, derr);
     k_grad_reduce<<<(TR_NOUT + 127) / 128, 128, 0, t->stream>>>(t->partials, blocks, t->grad);
     t->adam_t++;
     const float c1 = (float)(1.0 - std::pow((double)p->beta1, (double)t->adam_t));
@@ -858,7 +924,7 @@ int wt_trainer_grad(wt_trainer* t, int64_t offset, int64_t n, wt_closure* grad, 
   A.partials = t->partials;
   std::vector<double> h(TR_NOUT);
   int herr = 0;
-  k_train<true><<<(unsigned)blocks, TR_THREADS, TS_BYTES, t->stream>>>(A, derr);
+  k_train<true><<<(unsigned)blocks, TR_THREADS, TS_BYTES_TRAIN, t->stream>>>(A, derr);
   k_grad_reduce<<<(TR_NOUT + 127) / 128, 128, 0, t->stream>>>(t->partials, blocks, t->grad);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), t->grad, TR_NOUT * sizeof(double), cudaMemcpyDeviceToHost, t->stream);
@@ -895,7 +961,7 @@ int wt_trainer_infer(wt_trainer* t, const float* x, int64_t n, float* nu) {
   int herr = 0;
   cudaError_t e = cudaMemcpyAsync(t->io, x, (size_t)n * CL_IN * sizeof(float), cudaMemcpyHostToDevice, t->stream);
   if (e == cudaSuccess) {
-    k_train<false><<<(unsigned)((n + TR_THREADS - 1) / TR_THREADS), TR_THREADS, TS_BYTES, t->stream>>>(A, derr);
+    k_train<false><<<(unsigned)((n + TR_THREADS - 1) / TR_THREADS), TR_THREADS, TS_BYTES_INFER, t->stream>>>(A, derr);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(nu, A.nu_out, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, t->stream);
