@@ -374,6 +374,8 @@ def components(s, peak, no_cpu):
     from windtunnel_vis_b200 import abi as A
 
     out["d2q9_cylinder_persistent"] = d2q9_cylinder(peak, True, launch=(A.WT_LAUNCH_PERSISTENT, 2, 0, 0))
+    # and through the work queue, one launch per step under the step graphs
+    out["d2q9_cylinder_queue"] = d2q9_cylinder(peak, True, launch=(A.WT_LAUNCH_QUEUE, 2, 0, 0))
 
     # voxelizer (vehicle config, its own 512 x 256 x 256 handle)
     vd = (512, 256, 256)
@@ -450,11 +452,14 @@ def d2q9_cylinder(peak, no_cpu, updates=4000, chunks=20, launch=None):
            "mlups": round(n / ms / 1e3, 1), "steps_per_s": round(1e3 / ms, 1),
            "chunk_mlups": round(n * CHUNK / chunk_s / 1e6, 1),
            "chunk": f"stepAndSample({CHUNK}) incl. the sampling pass and the statistics readback (host clock)",
-           "launch": {"form": "10-step CUDA graphs: bulk kernel, face rows and wall cells per step",
-                      "cells_per_thread": used[1], "block": [used[2], used[3]]}
-           if used[0] != A.WT_LAUNCH_PERSISTENT else
-           {"form": "persistent kernel: one cooperative launch per call, work items from an atomic counter, "
-                    "grid barrier between steps"},
+           "launch": {"form": "persistent kernel: one cooperative launch per call, work items from an atomic counter, "
+                              "grid barrier between steps"}
+           if used[0] == A.WT_LAUNCH_PERSISTENT else
+           {"form": "10-step CUDA graphs: one launch per step of the persistent kernel's work queue (wall, face "
+                    "and bulk items from an atomic counter)"}
+           if used[0] == A.WT_LAUNCH_QUEUE else
+           {"form": "10-step CUDA graphs: bulk kernel, face rows and wall cells per step",
+            "cells_per_thread": used[1], "block": [used[2], used[3]]},
            "bytes_alg_per_update": n * 72, "l2_resident": True,
            "achieved_gbs_equiv": round(n * 72 / ms / 1e6, 1)}
     if not no_cpu:

@@ -315,6 +315,11 @@ int wt_probes(wt_solver* s, const float* pos4, int32_t count, float* out8);
  * as running them. Needs f16 / f32 storage, nx even and the reference's closure; elsewhere the
  * vectorised kernel runs. */
 #define WT_LAUNCH_PERSISTENT 9
+/* kernel = WT_LAUNCH_QUEUE (param 2, bx 0, by 0): every step is one launch of that kernel's work
+ * queue, one step per launch (no grid barrier, read-only-cache loads), captured in the step graphs
+ * like the per-step kernels; the sampling step keeps the per-step kernels. Same conditions and
+ * bit-identical results as WT_LAUNCH_PERSISTENT. */
+#define WT_LAUNCH_QUEUE 10
 int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32_t by);
 int wt_get_launch(const wt_solver* s, int32_t* out4);
 /* The project's launch tuner: times every applicable launch candidate on this handle's

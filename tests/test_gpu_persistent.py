@@ -49,6 +49,30 @@ def test_persistent_steps_match_per_step_kernels(gpu, dims, pset, prec):
     b.destroy()
 
 
+QUEUE = (abi.WT_LAUNCH_QUEUE, 2, 0, 0)
+
+
+@pytest.mark.parametrize("prec", ["f16", "f32"])
+@pytest.mark.parametrize("pset", list(PARAM_SETS))
+@pytest.mark.parametrize("dims", [(32, 14, 12), (34, 14, 10), (48, 16, 1), (160, 12, 1)])
+def test_queue_steps_match_per_step_kernels(gpu, dims, pset, prec):
+    # one work-queue launch per step (captured in the step graphs; the counter clears itself), the
+    # sampling step on the per-step kernels: bit-identical to the per-step kernels throughout
+    params = dict(PARAM_SETS[pset], precision=prec)
+    a = _solver(dims, params)
+    b = _solver(dims, params, QUEUE)
+    assert b.get_launch() == QUEUE
+    for n in (1, 7, 24, 3):
+        a.step(n)
+        b.step(n)
+        np.testing.assert_array_equal(a.read_populations(), b.read_populations())
+        sa, sb = a.step_and_sample(11), b.step_and_sample(11)
+        assert sa["raw"].tolist() == sb["raw"].tolist() and sa["mass"] == sb["mass"]
+    np.testing.assert_array_equal(a.read_velocity_half(), b.read_velocity_half())
+    a.destroy()
+    b.destroy()
+
+
 def test_persistent_channel_matches_graph_steps(gpu):
     # the D2Q9 cylinder channel (512 x 128, FP32, BGK): 500 updates as one launch
     dims = V.CHANNEL_DIMS

@@ -16,6 +16,7 @@ WT_E_UNSUPPORTED = -5
 WT_E_NO_DEVICE = -6
 WT_LAUNCH_ROW_PIPELINE = 8
 WT_LAUNCH_PERSISTENT = 9
+WT_LAUNCH_QUEUE = 10
 WT_BATCH_PERSISTENT = 2
 WT_BATCH_QUEUE = 3
 

@@ -1201,9 +1201,12 @@ int wt_set_launch(wt_solver* s, int32_t kernel, int32_t param, int32_t bx, int32
   if (kernel == WT_LAUNCH_ROW_PIPELINE) {
     if (param != 2 || bx != 0 || by < 0 || by > 16)
       return fail(s, WT_E_INVALID, "wt_set_launch: the row pipeline takes param 2, bx 0 and 0..16 rows per block");
-  } else if (kernel == WT_LAUNCH_PERSISTENT) {
+  } else if (kernel == WT_LAUNCH_PERSISTENT || kernel == WT_LAUNCH_QUEUE) {
     if (param != 2 || bx != 0 || by != 0)
       return fail(s, WT_E_INVALID, "wt_set_launch: the persistent kernel takes param 2, bx 0, by 0");
+    // the work queue's item counter and arrival count start at zero
+    DeviceGuard g(s->device);
+    WT_CUDA(s, cudaMemsetAsync(s->ps_bar, 0, wt::PS_BAR_WORDS * sizeof(unsigned), s->stream), "wt_set_launch");
   } else if (!(kernel == 0 || (kernel >= 2 && kernel <= 4))) {
     return fail(s, WT_E_INVALID, "wt_set_launch: occupancy hint must be 0 or 2..4 CTAs per SM");
   } else if (!(param == 1 || param == 2 || param == 4) || bx < 0 || by < 0 || bx * by > 256 || (bx % 32) != 0 ||

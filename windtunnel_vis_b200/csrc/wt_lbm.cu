@@ -2398,9 +2398,11 @@ __global__ void __launch_bounds__(PS_THREADS, PS_MIN_BLOCKS)
   const uint32_t tid = threadIdx.x;
   uint32_t sl = 0;
   for (int k = 0; k < steps; k++) {
-    unsigned* const ctr = bar + 2 + ((k0 + k) & 1);
-    // the next step's counter was last used by the step before this one, which every block has left
-    if (blockIdx.x == 0 && tid == 0) atomicExch(bar + 2 + ((k0 + k + 1) & 1), 0u);
+    // COH (several steps per launch): two counters alternate, the next step's cleared by block 0
+    // (it was last used by the step before this one, which every block has left). One step per
+    // launch: one counter, cleared by the last block to finish (below).
+    unsigned* const ctr = COH ? bar + 2 + ((k0 + k) & 1) : bar + 2;
+    if (COH && blockIdx.x == 0 && tid == 0) atomicExch(bar + 2 + ((k0 + k + 1) & 1), 0u);
     for (uint32_t item = blockIdx.x; item < T.items; sl ^= 1u) {
       uint32_t nxt = 0;
       if (tid == 0) nxt = atomicAdd(ctr, 1u);  // consumed after this item's cells
@@ -2433,6 +2435,15 @@ __global__ void __launch_bounds__(PS_THREADS, PS_MIN_BLOCKS)
     if (k + 1 < steps && !grid_barrier(bar, gridDim.x)) {
       if (tid == 0) atomicOr(err, 16);
       return;
+    }
+  }
+  if constexpr (!COH) {
+    // every block has taken its last item once it gets here: the last one clears the counter and
+    // the arrival count for the next launch
+    __syncthreads();
+    if (tid == 0 && atomicAdd(bar + 3, 1u) == gridDim.x - 1u) {
+      atomicExch(bar + 2, 0u);
+      atomicExch(bar + 3, 0u);
     }
   }
 }
@@ -3265,9 +3276,19 @@ cudaError_t closure_rows_reserve(wt_solver* s, bool* grown) {
 // One step, fin -> fout. With smp (the fused sampling step, see sample_step_ok) the face, wall-cell
 // and bulk kernels also run the sampling pass's per-cell work on what they store.
 template <class L, class S>
+static cudaError_t queue_step_t(wt_solver* const* ms, int count, int flip, unsigned* bar, int* err, cudaStream_t st);
+
+template <class L, class S>
 static cudaError_t sc_t(wt_solver* s, const void* fin, void* fout, const SampleOut* smp) {
   constexpr bool vec_ok = S::PREC == WT_PREC_F16 || S::PREC == WT_PREC_F32;
   const SampleOut none{};
+  if (s->sc_kernel == WT_LAUNCH_QUEUE && smp == nullptr && persistent_ok(s)) {
+    // the whole step (wall chunks, face tiles, bulk tiles) in one launch of the work queue
+    const int par = fin == s->f[0] ? 0 : 1;
+    wt_solver* one[1] = {s};
+    s->launches++;
+    return queue_step_t<L, S>(one, 1, s->parity ^ par, s->ps_bar, s->err_dev, s->stream);
+  }
   if constexpr (vec_ok) {
     const int V = s->sc_param;
     const bool faces_ok = s->dims.ny >= 2 && (L::DIM == 2 || s->dims.nz >= 2);
@@ -3622,18 +3643,18 @@ cudaError_t launch_persistent(wt_solver* const* ms, int count, int steps, unsign
 }
 
 template <class L, class S>
-static cudaError_t queue_step_t(wt_solver* const* ms, int count, int k0, unsigned* bar, int* err, cudaStream_t st) {
+static cudaError_t queue_step_t(wt_solver* const* ms, int count, int flip, unsigned* bar, int* err, cudaStream_t st) {
   if constexpr (S::PREC == WT_PREC_F64) {
     return cudaErrorNotSupported;
   } else {
     PersistTable tab;
-    cudaError_t e = persistent_table(ms, count, k0 & 1, tab);
+    cudaError_t e = persistent_table(ms, count, flip, tab);
     if (e != cudaSuccess) return e;
     auto kern =
         ms[0]->kp.collision == 1u ? k_steps_persistent<L, S, true, false> : k_steps_persistent<L, S, false, false>;
     unsigned grid = 0;
     if ((e = persistent_grid(kern, ms, tab.items, &grid)) != cudaSuccess) return e;
-    kern<<<grid, PS_THREADS, 0, st>>>(tab, 1, k0, bar, err);
+    kern<<<grid, PS_THREADS, 0, st>>>(tab, 1, 0, bar, err);
     return cudaGetLastError();
   }
 }
@@ -3643,7 +3664,7 @@ cudaError_t launch_queue_step(wt_solver* const* ms, int count, int k0, unsigned*
   for (int k = 1; k < count; k++)
     if (ms[k]->is3d != s->is3d || ms[k]->prec != s->prec || ms[k]->kp.collision != s->kp.collision)
       return cudaErrorInvalidValue;
-  WT_DISPATCH(queue_step_t, ms, count, k0, bar, err, st);
+  WT_DISPATCH(queue_step_t, ms, count, k0 & 1, bar, err, st);
 }
 
 bool batch_fusable(const wt_solver* s) {
