@@ -2397,6 +2397,9 @@ __global__ void __launch_bounds__(PS_THREADS, PS_MIN_BLOCKS)
   __shared__ uint32_t s_item[2];
   const uint32_t tid = threadIdx.x;
   uint32_t sl = 0;
+  // one step per launch: a launch with programmatic stream serialisation may start before the
+  // previous step has finished; wait for it (and its memory) before touching any buffer or counter
+  if constexpr (!COH) asm volatile("griddepcontrol.wait;" ::: "memory");
   for (int k = 0; k < steps; k++) {
     // COH (several steps per launch): two counters alternate, the next step's cleared by block 0
     // (it was last used by the step before this one, which every block has left). One step per
@@ -2438,6 +2441,8 @@ __global__ void __launch_bounds__(PS_THREADS, PS_MIN_BLOCKS)
     }
   }
   if constexpr (!COH) {
+    // the next step's blocks may be scheduled now (they wait for this grid to complete)
+    asm volatile("griddepcontrol.launch_dependents;");
     // every block has taken its last item once it gets here: the last one clears the counter and
     // the arrival count for the next launch
     __syncthreads();
@@ -3654,8 +3659,19 @@ static cudaError_t queue_step_t(wt_solver* const* ms, int count, int flip, unsig
         ms[0]->kp.collision == 1u ? k_steps_persistent<L, S, true, false> : k_steps_persistent<L, S, false, false>;
     unsigned grid = 0;
     if ((e = persistent_grid(kern, ms, tab.items, &grid)) != cudaSuccess) return e;
-    kern<<<grid, PS_THREADS, 0, st>>>(tab, 1, 0, bar, err);
-    return cudaGetLastError();
+    // programmatic stream serialisation: the launch may overlap the end of the previous kernel on
+    // the stream (the kernel waits for it before its first access)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(PS_THREADS);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int one = 1, zero = 0;
+    return cudaLaunchKernelEx(&cfg, kern, tab, one, zero, bar, err);
   }
 }
 
