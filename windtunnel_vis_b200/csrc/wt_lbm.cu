@@ -2564,7 +2564,7 @@ __device__ __forceinline__ void cell_force(const wt_kparams& P, const typename S
   uint32_t gfl[GATHER ? Q : 1], gsd[GATHER ? Q : 1], gflb[GATHER ? Q : 1];
   R gfb[GATHER ? Q : 1];
   if constexpr (GATHER) {
-    // round 1: every neighbour's flags
+    // first wave of loads: every neighbour's flags
     gfl[0] = 0u;
     static_for<Q>([&](auto I) {
       constexpr int i = I;
@@ -2574,7 +2574,7 @@ __device__ __forceinline__ void cell_force(const wt_kparams& P, const typename S
         gfl[i] = sn >= 0 ? __ldg(flags + sn) : 0u;
       }
     });
-    // round 2: the solid links' distances and partners
+    // second wave: the solid links' distances and partners
     static_for<Q>([&](auto I) {
       constexpr int i = I;
       gsd[i] = 0u;
