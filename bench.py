@@ -64,7 +64,12 @@ def measured_traffic(shape, closure=False):
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
-    key = "lc" if closure else ",".join(str(int(v)) for v in shape[1:])
+    cells, bx, by = (int(v) for v in shape[1:])
+    if bx == 0 and by == 0 and cells > 1:
+        # the default block of the vectorised kernel: one row of up to 128 threads
+        runs = DIMS[0] // cells
+        bx, by = (128 if runs >= 128 else ((runs + 31) // 32) * 32), 1
+    key = "lc" if closure else f"{cells},{bx},{by}"
     for m in re.finditer(r"^traffic_bytes_per_step\[([0-9a-z,]+)\]:\s*(\d+)", open(p).read(), flags=re.M):
         if m.group(1) == key:
             return int(m.group(2))
