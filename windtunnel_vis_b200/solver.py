@@ -51,7 +51,10 @@ class Solver:
         self.q = 19 if self.is3d else 9
         self.params = dict(params)
         self.precision = abi.PRECISION[self.params.get("precision", "f32") or "f32"]
-        self._async_refs = []  # host arrays of queued copies, released by sync / destroy
+        # host arrays of queued copies, kept referenced until the library is done with them: uploads
+        # until the next step or sample has applied them, readbacks until a later sample has waited
+        # for them (or sync / destroy)
+        self._up_refs, self._rd_refs, self._rd_before_sample = [], [], 0
         h = C.c_void_p()
         d = abi.Dims(nx, ny, nz)
         rc = self._lib.wt_create(C.byref(d), C.byref(abi.make_params(self.params)), C.byref(h))
@@ -94,7 +97,7 @@ class Solver:
         if getattr(self, "_h", None):
             self._lib.wt_destroy(self._h)  # waits for the queued copies first
             self._h = None
-        self._async_refs = []
+        self._up_refs, self._rd_refs, self._rd_before_sample = [], [], 0
 
     def __del__(self):
         try:
@@ -156,13 +159,13 @@ class Solver:
         pinned torch tensor's numpy view) lets the copy overlap."""
         f = np.ascontiguousarray(np.asarray(flags).ravel(), np.uint32)
         self._check(self._lib.wt_upload_flags_async(self._h, _ptr(f), f.size))
-        self._async_refs.append(f)
+        self._up_refs.append(f)
 
     def upload_sdf_async(self, d):
         """uploadSdf queued, as `upload_flags_async`."""
         a = np.ascontiguousarray(np.asarray(d).ravel(), np.float32)
         self._check(self._lib.wt_upload_sdf_async(self._h, _ptr(a), a.size))
-        self._async_refs.append(a)
+        self._up_refs.append(a)
 
     def set_wheels(self, wheels):
         arr, n = abi.make_wheels(list(wheels))
@@ -200,16 +203,23 @@ class Solver:
         """stepAndSample in the reference's asynchronous form: queues the chunk and returns; the
         statistics come from `sample_wait`."""
         self._check(self._lib.wt_step_and_sample_async(self._h, int(steps)))
+        self._up_refs.clear()  # applied before the chunk was queued
+        # the chunk's sampling step waits for every readback queued before it
+        self._rd_before_sample = len(self._rd_refs)
 
     def sample_wait(self):
         st = abi.Stats()
         self._check(self._lib.wt_sample_wait(self._h, C.byref(st)))
+        del self._rd_refs[:self._rd_before_sample]
+        self._rd_before_sample = 0
         return _stats_dict(st)
 
     def sync(self):
         """Waits for every queued step, sample, upload and readback of the handle."""
         self._check(self._lib.wt_sync(self._h))
-        self._async_refs.clear()
+        self._up_refs.clear()
+        self._rd_refs.clear()
+        self._rd_before_sample = 0
 
     # ---- readback / checkpoint ---------------------------------------------------------------
     def read_flags(self):
@@ -259,7 +269,7 @@ class Solver:
         holds the field after `sync`."""
         assert out.dtype == np.float16 and out.shape == (self.n, 4) and out.flags["C_CONTIGUOUS"]
         self._check(self._lib.wt_read_velocity_half4_async(self._h, _ptr(out), self.n))
-        self._async_refs.append(out)
+        self._rd_refs.append(out)
         return out
 
     def read_means(self):
