@@ -3659,8 +3659,10 @@ static cudaError_t queue_step_t(wt_solver* const* ms, int count, int flip, unsig
         ms[0]->kp.collision == 1u ? k_steps_persistent<L, S, true, false> : k_steps_persistent<L, S, false, false>;
     unsigned grid = 0;
     if ((e = persistent_grid(kern, ms, tab.items, &grid)) != cudaSuccess) return e;
-    // programmatic stream serialisation: the launch may overlap the end of the previous kernel on
-    // the stream (the kernel waits for it before its first access)
+    // Programmatic stream serialisation for steps of at most two item waves (launch-bound steps,
+    // such as small 2-D channels): the launch may overlap the end of the previous kernel on the
+    // stream (the kernel waits for it before its first access). Large steps launch plainly: blocks
+    // scheduled early would only hold slots the previous step's last items need.
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(PS_THREADS);
@@ -3669,7 +3671,7 @@ static cudaError_t queue_step_t(wt_solver* const* ms, int count, int flip, unsig
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = tab.items <= 2u * grid ? 1 : 0;
     int one = 1, zero = 0;
     return cudaLaunchKernelEx(&cfg, kern, tab, one, zero, bar, err);
   }
