@@ -57,3 +57,15 @@ def test_reference_arm_non_zero_rank_exits_quietly():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
                         "--warmup", "0"], env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_measured_traffic_follows_the_launch_shape():
+    # the default block of the vectorised kernel (0, 0) is one row of 128 threads on the bench
+    # tunnel, so it reads the 128 x 1 entry of the committed profile; shapes never captured give None
+    sys.path.insert(0, ROOT)
+    import bench
+
+    assert bench.measured_traffic((4, 2, 0, 0)) == bench.measured_traffic((3, 2, 128, 1)) is not None
+    assert bench.measured_traffic((4, 2, 64, 2)) is not None
+    assert bench.measured_traffic((0, 4, 32, 4)) is None
+    assert bench.measured_traffic((0, 0, 0, 0), closure=True) is not None
