@@ -557,11 +557,16 @@ def run_ours(args, rank, world, local_rank, dist):
             # stepAndSample(CHUNK): wt_step_and_sample runs step(CHUNK - TAIL) and then one graph of
             # the last TAIL steps, the last of them with the sampling pass fused; calling the two
             # parts here does the same work and lets the events bracket the plain updates for the
-            # roofline
+            # roofline. The chunk's statistics are read back through the queued form (the
+            # reference's stepAndSample Promise): chunk k's plain updates are queued before the
+            # host waits for chunk k - 1's statistics, so the device never waits for the host.
             ev[k][0].record(stream)
             s.step(CHUNK - TAIL)
             ev[k][1].record(stream)
-            s.step_and_sample(TAIL)
+            if k > 0:
+                s.sample_wait()
+            s.step_and_sample_async(TAIL)
+        s.sample_wait()
         t_end.record(stream)
         torch.cuda.synchronize()
         barrier()
